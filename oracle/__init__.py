@@ -1,0 +1,301 @@
+"""Test infrastructure: ctypes bindings to the two CPU checkers.
+
+* ``liboracle.so`` -- the plain-C restatement in ``asgard_oracle.c`` of the
+  reference's CPU kronmult, sparse-grid/pair-list builder and GMRES.
+* ``_ref/libasgard_ref.so`` -- the reference itself, compiled from its own
+  sources by ``Makefile`` (target ``ref``), reached through ``ref_shim.cpp``.
+
+Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU legs may
+import this package, and only as the checker or the CPU baseline; the product
+(``asgard_b200``) never does.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "liboracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libasgard_ref.so")
+
+_i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+_f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_f32p = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
+
+_oracle = None
+_ref = None
+
+
+def build_oracle(force: bool = False) -> str:
+    """Compiles liboracle.so (gcc is present wherever the tests run)."""
+    if force or not os.path.exists(ORACLE_SO):
+        subprocess.run(["make", "-C", HERE, "all"], check=True,
+                       stdout=subprocess.DEVNULL)
+    return ORACLE_SO
+
+
+def oracle():
+    global _oracle
+    if _oracle is None:
+        build_oracle()
+        lib = C.CDLL(ORACLE_SO)
+        for name, T in (("f64", _f64p), ("f32", _f32p)):
+            fn = getattr(lib, f"orc_kronmult_sparse_{name}")
+            S = C.c_double if name == "f64" else C.c_float
+            fn.argtypes = [C.c_int, C.c_int, C.c_int, _i32p, _i32p, C.c_int,
+                           _i32p, T, S, T, S, T]
+            fn.restype = C.c_int
+        lib.orc_assemble_dense.argtypes = [C.c_int, C.c_int, C.c_int, _i32p,
+                                           _i32p, C.c_int, _i32p, _f64p, _f64p]
+        lib.orc_connect_1d.argtypes = [C.c_int, C.POINTER(C.c_int),
+                                       C.POINTER(C.c_int), C.c_void_p,
+                                       C.c_void_p]
+        lib.orc_sparse_grid.argtypes = [C.c_int, C.c_int, C.c_void_p]
+        lib.orc_sparse_grid.restype = C.c_int64
+        lib.orc_build_pairs.argtypes = [C.c_int, C.c_int, C.c_int, _i32p,
+                                        C.POINTER(C.c_int64), C.c_void_p,
+                                        C.c_void_p, C.c_void_p]
+        lib.orc_expand_iA.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int64,
+                                      _i32p, _i32p]
+        lib.orc_expand_iA.restype = None
+        lib.orc_rotg.argtypes = [C.POINTER(C.c_double)] * 4
+        lib.orc_rotg.restype = None
+        lib.orc_gmres_euler.argtypes = [C.c_int, C.c_int, C.c_int, _i32p,
+                                        _i32p, C.c_int, _i32p, _f64p,
+                                        C.c_double, _f64p, _f64p, C.c_int,
+                                        C.c_int, C.c_double,
+                                        C.POINTER(C.c_double),
+                                        C.POINTER(C.c_int)]
+        lib.orc_gmres_dense.argtypes = [C.c_int, _f64p, _f64p, _f64p, C.c_int,
+                                        C.c_int, C.c_double,
+                                        C.POINTER(C.c_double),
+                                        C.POINTER(C.c_int)]
+        lib.orc_make_kronmult_data.argtypes = [C.c_int] * 6 + [
+            _i32p, _i32p, _i32p, C.c_void_p, C.c_void_p, C.c_void_p]
+        _oracle = lib
+    return _oracle
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_SO)
+
+
+def ref():
+    """The reference compiled from source; raises if it was not built."""
+    global _ref
+    if _ref is None:
+        if not ref_available():
+            raise FileNotFoundError(REF_SO)
+        # OpenBLAS (linked by the reference build) finds its private
+        # libgfortran only when that is loaded first from the same folder.
+        import glob, site
+        for sp in site.getsitepackages():
+            deps = glob.glob(os.path.join(sp, "opencv_python_headless.libs",
+                                          "lib*.so*"))
+            for key in ("quadmath", "gfortran"):
+                for dep in deps:
+                    if key in os.path.basename(dep):
+                        C.CDLL(dep, mode=C.RTLD_GLOBAL)
+        lib = C.CDLL(REF_SO)
+        for name, T in (("f64", _f64p), ("f32", _f32p)):
+            S = C.c_double if name == "f64" else C.c_float
+            fn = getattr(lib, f"ref_cpu_sparse_{name}")
+            fn.argtypes = [C.c_int, C.c_int, C.c_int, _i32p, _i32p, C.c_int,
+                           _i32p, T, S, T, S, T]
+            fn = getattr(lib, f"ref_make_kronmult_data_{name}")
+            fn.argtypes = [C.c_int] * 5 + [_i32p, _i32p, _i32p, T, T, T, T]
+        lib.ref_gmres_euler_f64.argtypes = [
+            C.c_int, C.c_int, C.c_int, C.c_int, _i32p, _i32p, _i32p, _f64p,
+            C.c_int64, C.c_double, _f64p, _f64p, C.c_int, C.c_int, C.c_double,
+            C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_int)]
+        lib.ref_gmres_dense_f64.argtypes = [
+            C.c_int, _f64p, _f64p, _f64p, C.c_void_p, C.c_int, C.c_int,
+            C.c_double, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_int)]
+        lib.ref_connect_1d.argtypes = [C.c_int, C.POINTER(C.c_int),
+                                       C.POINTER(C.c_int), C.c_void_p,
+                                       C.c_void_p, C.c_void_p]
+        lib.ref_pde_create.argtypes = [C.c_char_p, C.c_char_p, C.c_int]
+        lib.ref_pde_create.restype = C.c_void_p
+        lib.ref_pde_destroy.argtypes = [C.c_void_p]
+        lib.ref_pde_destroy.restype = None
+        lib.ref_pde_info.argtypes = [C.c_void_p] + [C.POINTER(C.c_int)] * 5 + [
+            C.POINTER(C.c_int64)] * 3 + [C.POINTER(C.c_double)]
+        lib.ref_pde_export.argtypes = [C.c_void_p, _i32p, _i32p, _i32p, _f64p,
+                                       _i32p]
+        lib.ref_pde_coefficients.argtypes = [C.c_void_p, C.c_int, C.c_int,
+                                             C.c_void_p, C.POINTER(C.c_int)]
+        lib.ref_pde_apply.argtypes = [C.c_void_p, C.c_double, _f64p,
+                                      C.c_double, _f64p]
+        lib.ref_pde_gmres_euler.argtypes = [
+            C.c_void_p, C.c_double, _f64p, _f64p, C.c_int, C.c_int,
+            C.c_double, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_int)]
+        _ref = lib
+    return _ref
+
+
+# ----------------------------------------------------------------- helpers
+
+def kronmult(d, n, pntr, indx, terms, iA, vA, alpha, x, beta, y, lib=None):
+    """y <- beta*y + alpha*K*x in place (oracle restatement by default)."""
+    f32 = vA.dtype == np.float32
+    rows = len(pntr) - 1
+    if lib is None:
+        fn = getattr(oracle(), "orc_kronmult_sparse_" + ("f32" if f32 else "f64"))
+    else:
+        fn = getattr(lib, "ref_cpu_sparse_" + ("f32" if f32 else "f64"))
+    rc = fn(d, n, rows, pntr, indx, terms, iA, vA, alpha, x, beta, y)
+    if rc != 0:
+        raise RuntimeError(f"kronmult checker returned {rc}")
+    return y
+
+
+def connect_1d(level, lib=None):
+    rows, conn = C.c_int(), C.c_int()
+    if lib is None:
+        f = oracle().orc_connect_1d
+        f(level, C.byref(rows), C.byref(conn), None, None)
+        pntr = np.zeros(rows.value + 1, np.int32)
+        indx = np.zeros(conn.value, np.int32)
+        f(level, C.byref(rows), C.byref(conn), pntr.ctypes.data, indx.ctypes.data)
+    else:
+        f = lib.ref_connect_1d
+        f(level, C.byref(rows), C.byref(conn), None, None, None)
+        pntr = np.zeros(rows.value + 1, np.int32)
+        indx = np.zeros(conn.value, np.int32)
+        f(level, C.byref(rows), C.byref(conn), pntr.ctypes.data,
+          indx.ctypes.data, None)
+    return pntr, indx
+
+
+def sparse_grid(d, L):
+    lib = oracle()
+    cells = lib.orc_sparse_grid(d, L, None)
+    table = np.zeros((cells, 2 * d), np.int32)
+    lib.orc_sparse_grid(d, L, table.ctypes.data)
+    return table
+
+
+def build_pairs(d, L, table):
+    lib = oracle()
+    nnz = C.c_int64()
+    table = np.ascontiguousarray(table, dtype=np.int32)
+    cells = table.shape[0]
+    lib.orc_build_pairs(d, L, cells, table.ravel(), C.byref(nnz), None, None, None)
+    pntr = np.zeros(cells + 1, np.int32)
+    indx = np.zeros(nnz.value, np.int32)
+    conn = np.zeros((nnz.value, d), np.int32)
+    lib.orc_build_pairs(d, L, cells, table.ravel(), C.byref(nnz),
+                        pntr.ctypes.data, indx.ctypes.data, conn.ctypes.data)
+    return pntr, indx, conn
+
+
+def expand_iA(d, n, terms, conn):
+    conn = np.ascontiguousarray(conn, dtype=np.int32)
+    nnz = conn.shape[0]
+    iA = np.zeros(nnz * terms * d, np.int32)
+    oracle().orc_expand_iA(d, n, terms, nnz, conn.ravel(), iA)
+    return iA
+
+
+def gmres_euler(d, n, pntr, indx, terms, iA, vA, dt, x, b, restart, max_outer,
+                tol, lib=None):
+    err, it = C.c_double(), C.c_int()
+    rows = len(pntr) - 1
+    if lib is None:
+        rc = oracle().orc_gmres_euler(d, n, rows, pntr, indx, terms, iA, vA,
+                                      dt, x, b, restart, max_outer, tol,
+                                      C.byref(err), C.byref(it))
+    else:
+        rc = lib.ref_gmres_euler_f64(d, n, rows, terms, pntr, indx, iA, vA,
+                                     len(vA), dt, x, b, restart, max_outer,
+                                     tol, 1, C.byref(err), C.byref(it))
+    if rc != 0:
+        raise RuntimeError(f"gmres checker returned {rc}")
+    return err.value, it.value
+
+
+def gmres_dense(A, x, b, restart, max_outer, tol, lib=None):
+    n = len(b)
+    At = np.asfortranarray(A).ravel(order="F").copy()
+    err, it = C.c_double(), C.c_int()
+    if lib is None:
+        rc = oracle().orc_gmres_dense(n, At, x, b, restart, max_outer, tol,
+                                      C.byref(err), C.byref(it))
+    else:
+        rc = lib.ref_gmres_dense_f64(n, At, x, b, None, restart, max_outer,
+                                     tol, 1, C.byref(err), C.byref(it))
+    if rc != 0:
+        raise RuntimeError(f"gmres checker returned {rc}")
+    return err.value, it.value
+
+
+def make_kronmult_data(d, n, rows, terms, mats, dtype=np.float64):
+    """The reference tests' random kronmult data (minstd_rand(42))."""
+    nb = rows * rows
+    pntr = np.zeros(rows + 1, np.int32)
+    indx = np.zeros(nb, np.int32)
+    iA = np.zeros(nb * terms * d, np.int32)
+    ts = n ** d
+    vA = np.zeros(n * n * mats, dtype)
+    x = np.zeros(ts * rows, dtype)
+    y = np.zeros(ts * rows, dtype)
+    oracle().orc_make_kronmult_data(d, n, rows, terms, mats,
+                                    8 if dtype == np.float64 else 4, pntr,
+                                    indx, iA, vA.ctypes.data, x.ctypes.data,
+                                    y.ctypes.data)
+    return dict(pntr=pntr, indx=indx, iA=iA, vA=vA, x=x, y=y)
+
+
+class RefPDE:
+    """A built-in reference PDE with its sparse kronmult matrix (reference builder)."""
+
+    def __init__(self, name: str, level: int, degree: int, dims: int):
+        self.lib = ref()
+        levels = " ".join([str(level)] * dims)
+        self.h = self.lib.ref_pde_create(name.encode(), levels.encode(), degree)
+        if not self.h:
+            raise RuntimeError(f"reference could not build pde {name}")
+        d, n, rows, terms, L = (C.c_int() for _ in range(5))
+        nnz, ia, va = (C.c_int64() for _ in range(3))
+        dt = C.c_double()
+        rc = self.lib.ref_pde_info(self.h, C.byref(d), C.byref(n), C.byref(rows),
+                                   C.byref(terms), C.byref(L), C.byref(nnz),
+                                   C.byref(ia), C.byref(va), C.byref(dt))
+        if rc != 0:
+            raise RuntimeError("reference matrix is split into several calls")
+        self.d, self.n, self.rows, self.terms = d.value, n.value, rows.value, terms.value
+        self.max_level, self.nnz, self.dt = L.value, nnz.value, dt.value
+        self.pntr = np.zeros(self.rows + 1, np.int32)
+        self.indx = np.zeros(self.nnz, np.int32)
+        self.iA = np.zeros(ia.value, np.int32)
+        self.vA = np.zeros(va.value, np.float64)
+        self.table = np.zeros(self.rows * 2 * self.d, np.int32)
+        self.lib.ref_pde_export(self.h, self.pntr, self.indx, self.iA, self.vA,
+                                self.table)
+        self.table = self.table.reshape(self.rows, 2 * self.d)
+
+    def coefficients(self, term, dim):
+        lda = C.c_int()
+        self.lib.ref_pde_coefficients(self.h, term, dim, None, C.byref(lda))
+        out = np.zeros(lda.value * lda.value, np.float64)
+        self.lib.ref_pde_coefficients(self.h, term, dim, out.ctypes.data,
+                                      C.byref(lda))
+        return out.reshape(lda.value, lda.value, order="F")
+
+    def apply(self, alpha, x, beta, y):
+        self.lib.ref_pde_apply(self.h, alpha, x, beta, y)
+        return y
+
+    def gmres_euler(self, dt, x, b, restart, max_outer, tol):
+        err, it = C.c_double(), C.c_int()
+        self.lib.ref_pde_gmres_euler(self.h, dt, x, b, restart, max_outer, tol,
+                                     1, C.byref(err), C.byref(it))
+        return err.value, it.value
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib.ref_pde_destroy(self.h)
+            self.h = None
