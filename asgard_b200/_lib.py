@@ -1,0 +1,89 @@
+"""ctypes binding of the C ABI in ``include/asgard_b200.h``.
+
+Loads the in-tree ``libasgard_b200.so``.  There is no fallback: if the library
+is missing or does not load, importing fails with the reason.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libasgard_b200.so")
+
+EXPORTS = [
+    "asgk_plan_create", "asgk_plan_create_pairs", "asgk_plan_create_conn",
+    "asgk_plan_destroy", "asgk_plan_update_values", "asgk_plan_info",
+    "asgk_apply", "asgk_apply_f32", "asgk_apply_host", "asgk_apply_euler",
+    "asgk_gmres_euler", "asgk_gmres_dense", "asgk_default_gmres_restarts",
+    "asgk_sparse_grid", "asgk_connect_1d", "asgk_build_pairs",
+    "asgk_status_string", "asgk_launch_count", "asgk_device_info",
+    "asgk_measure_fma_peak",
+]
+
+
+class GmresInfo(C.Structure):
+    _fields_ = [("error", C.c_double), ("iterations", C.c_int),
+                ("status", C.c_int), ("true_relres", C.c_double),
+                ("outer_steps", C.c_int), ("matvecs_low", C.c_int),
+                ("matvecs_fp64", C.c_int), ("precond_calls", C.c_int),
+                ("fallback", C.c_int)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+_vp = C.c_void_p
+_i = C.c_int
+_i64 = C.c_int64
+_d = C.c_double
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(
+            f"asgard_b200: {LIB_PATH} is missing; build it with "
+            "`python -m asgard_b200.build` (nvcc, sm_100a)")
+    lib = C.CDLL(LIB_PATH)
+    sig = {
+        "asgk_plan_create": ([C.POINTER(_vp), _i, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _i64], _i),
+        "asgk_plan_create_pairs": ([C.POINTER(_vp), _i, _i, _i, _i, _i, _i64, _vp, _vp, _vp, _vp, _i64], _i),
+        "asgk_plan_create_conn": ([C.POINTER(_vp), _i, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _i64], _i),
+        "asgk_plan_destroy": ([_vp], None),
+        "asgk_plan_update_values": ([_vp, _vp, _i64], _i),
+        "asgk_plan_info": ([_vp] + [C.POINTER(_i64)] * 5, _i),
+        "asgk_apply": ([_vp, _i, _d, _vp, _d, _vp, _vp], _i),
+        "asgk_apply_f32": ([_vp, C.c_float, _vp, C.c_float, _vp, _vp], _i),
+        "asgk_apply_host": ([_vp, _d, _vp, _d, _vp, _vp], _i),
+        "asgk_apply_euler": ([_vp, _i, _d, _d, _vp, _d, _vp, _vp], _i),
+        "asgk_gmres_euler": ([_vp, _d, _vp, _vp, _i, _i, _d, _i, _i, _vp, C.POINTER(GmresInfo), _vp], _i),
+        "asgk_gmres_dense": ([_i, _vp, _vp, _vp, _i, _i, _d, C.POINTER(GmresInfo)], _i),
+        "asgk_default_gmres_restarts": ([_i64], _i),
+        "asgk_sparse_grid": ([_i, _i, _vp], _i64),
+        "asgk_connect_1d": ([_i, C.POINTER(_i), C.POINTER(_i), _vp, _vp], _i),
+        "asgk_build_pairs": ([_i, _i, _i, _vp, C.POINTER(_i64), _vp, _vp, _vp], _i),
+        "asgk_status_string": ([_i], C.c_char_p),
+        "asgk_launch_count": ([], _i64),
+        "asgk_device_info": ([C.POINTER(_i)] * 3, _i),
+        "asgk_measure_fma_peak": ([_i, C.POINTER(_d)], _i),
+    }
+    for name, (args, res) in sig.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = res
+    return lib
+
+
+lib = _load()
+
+
+class AsgkError(RuntimeError):
+    def __init__(self, status: int, what: str = ""):
+        msg = lib.asgk_status_string(status).decode()
+        super().__init__(f"{what}: {msg} (status {status})" if what else msg)
+        self.status = status
+
+
+def check(status: int, what: str = "") -> None:
+    if status != 0:
+        raise AsgkError(status, what)

@@ -1,0 +1,932 @@
+// C ABI: operator plans, apply entry points and the device-resident GMRES.
+#include "internal.cuh"
+#include "mlp.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <functional>
+#include <memory>
+#include <new>
+#include <numeric>
+
+namespace asgk
+{
+std::atomic<int64_t> g_launches{0};
+
+namespace
+{
+template<typename T>
+int dev_alloc(T **ptr, int64_t count, int64_t &bytes)
+{
+  *ptr = nullptr;
+  if (count <= 0)
+    return ASGK_OK;
+  size_t const b = size_t(count) * sizeof(T);
+  if (cudaMalloc(reinterpret_cast<void **>(ptr), b) != cudaSuccess)
+  {
+    cudaGetLastError();
+    return ASGK_ERR_ALLOC;
+  }
+  bytes += int64_t(b);
+  return ASGK_OK;
+}
+
+void free_plan(plan_data &p)
+{
+  cudaFree(p.row_ptr);
+  cudaFree(p.col);
+  cudaFree(p.idx);
+  cudaFree(p.row_order);
+  cudaFree(p.vA64);
+  cudaFree(p.vA32);
+  cudaFree(p.xw);
+  cudaFree(p.yw);
+  p = plan_data{};
+}
+
+__global__ void k_to_f32(const double *__restrict__ a, float *__restrict__ b,
+                         int64_t n)
+{
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n;
+       i += int64_t(gridDim.x) * blockDim.x)
+    b[i] = static_cast<float>(a[i]);
+}
+
+int upload_values(plan_data &p, const double *vA)
+{
+  ASGK_CUDA(cudaMemcpy(p.vA64, vA, sizeof(double) * p.vA_len,
+                       cudaMemcpyHostToDevice));
+  if (p.vA_len > 0)
+  {
+    k_to_f32<<<256, 256>>>(p.vA64, p.vA32, p.vA_len);
+    ASGK_LAUNCHED();
+  }
+  ASGK_CUDA(cudaDeviceSynchronize());
+  return ASGK_OK;
+}
+
+int check_dims(int d, int n, int rows, int cols, int terms)
+{
+  if (d < 1 || d > 6 || n < 1 || rows < 0 || cols < 0 || terms < 0)
+    return ASGK_ERR_INVALID;
+  double ts = std::pow(double(n), d);
+  if (ts > double(1 << 24))
+    return ASGK_ERR_UNSUPPORTED;
+  return ASGK_OK;
+}
+
+int64_t ipow(int n, int d)
+{
+  int64_t r = 1;
+  for (int i = 0; i < d; i++)
+    r *= n;
+  return r;
+}
+
+// Builds the device plan from host CSR arrays (validated here).
+int build_plan(asgk_plan **out, int d, int n, int rows, int cols, int terms,
+               std::vector<int64_t> const &row_ptr, const int *col,
+               const int *idx, index_mode mode, const double *vA,
+               int64_t vA_len)
+{
+  if (out == nullptr)
+    return ASGK_ERR_INVALID;
+  *out = nullptr;
+  if (int rc = check_dims(d, n, rows, cols, terms))
+    return rc;
+  if (vA_len < 0 || (vA_len > 0 && vA == nullptr))
+    return ASGK_ERR_INVALID;
+  int64_t const nnz = row_ptr.empty() ? 0 : row_ptr.back();
+  if (row_ptr.size() != size_t(rows) + 1 || row_ptr[0] != 0)
+    return ASGK_ERR_INVALID;
+  for (int r = 0; r < rows; r++)
+    if (row_ptr[r + 1] < row_ptr[r])
+      return ASGK_ERR_INVALID;
+  if (nnz > 0 && (col == nullptr || (terms > 0 && idx == nullptr)))
+    return ASGK_ERR_INVALID;
+  for (int64_t i = 0; i < nnz; i++)
+    if (col[i] < 0 || col[i] >= cols)
+      return ASGK_ERR_INVALID;
+  int64_t const nn  = int64_t(n) * n;
+  int64_t const blk = int64_t(d) * terms * nn;
+  int64_t idx_len   = 0;
+  if (terms > 0)
+  {
+    if (mode == index_mode::expanded)
+    {
+      idx_len = nnz * terms * d;
+      for (int64_t i = 0; i < idx_len; i++)
+        if (idx[i] < 0 || int64_t(idx[i]) + nn > vA_len)
+          return ASGK_ERR_INVALID;
+    }
+    else
+    {
+      idx_len = nnz * d;
+      for (int64_t i = 0; i < idx_len; i++)
+        if (idx[i] < 0 || (int64_t(idx[i]) + 1) * blk > vA_len)
+          return ASGK_ERR_INVALID;
+    }
+  }
+  std::unique_ptr<asgk_plan> plan(new (std::nothrow) asgk_plan());
+  if (!plan)
+    return ASGK_ERR_ALLOC;
+  plan_data &p = plan->p;
+  p.d = d;
+  p.n = n;
+  p.rows = rows;
+  p.cols = cols;
+  p.terms = terms;
+  p.tensor = int(ipow(n, d));
+  p.nnz = nnz;
+  p.mode = mode;
+  p.vA_len = vA_len;
+  int64_t &B = p.device_bytes;
+  int rc = ASGK_OK;
+  if ((rc = dev_alloc(&p.row_ptr, rows + 1, B)) ||
+      (rc = dev_alloc(&p.col, std::max<int64_t>(nnz, 1), B)) ||
+      (rc = dev_alloc(&p.idx, std::max<int64_t>(idx_len, 1), B)) ||
+      (rc = dev_alloc(&p.row_order, std::max(rows, 1), B)) ||
+      (rc = dev_alloc(&p.vA64, std::max<int64_t>(vA_len, 1), B)) ||
+      (rc = dev_alloc(&p.vA32, std::max<int64_t>(vA_len, 1), B)) ||
+      (rc = dev_alloc(&p.xw, std::max<int64_t>(int64_t(cols) * p.tensor, 1), B)) ||
+      (rc = dev_alloc(&p.yw, std::max<int64_t>(int64_t(rows) * p.tensor, 1), B)))
+  {
+    free_plan(p);
+    return rc;
+  }
+  // cells by decreasing pair count, ties by index
+  std::vector<int> order(rows);
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+    return (row_ptr[a + 1] - row_ptr[a]) > (row_ptr[b + 1] - row_ptr[b]);
+  });
+  auto up = [&](void *dst, const void *src, size_t bytes) -> int {
+    if (bytes == 0)
+      return ASGK_OK;
+    ASGK_CUDA(cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice));
+    return ASGK_OK;
+  };
+  if ((rc = up(p.row_ptr, row_ptr.data(), sizeof(int64_t) * (rows + 1))) ||
+      (rc = up(p.col, col, sizeof(int) * nnz)) ||
+      (rc = up(p.idx, idx, sizeof(int) * idx_len)) ||
+      (rc = up(p.row_order, order.data(), sizeof(int) * rows)) ||
+      (rc = upload_values(p, vA)))
+  {
+    free_plan(p);
+    return rc;
+  }
+  *out = plan.release();
+  return ASGK_OK;
+}
+
+cudaStream_t as_stream(asgk_stream s) { return static_cast<cudaStream_t>(s); }
+
+// y = beta*y + alpha*A*x for a dense column-major n x n matrix (one warp per row)
+__global__ void k_dense_gemv(int n, const double *__restrict__ A, double alpha,
+                             const double *__restrict__ x, double beta,
+                             double *__restrict__ y)
+{
+  int const row  = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+  int const lane = threadIdx.x & 31;
+  if (row >= n)
+    return;
+  double s = 0;
+  for (int j = lane; j < n; j += 32)
+    s += A[row + int64_t(j) * n] * x[j];
+  for (int o = 16; o > 0; o >>= 1)
+    s += __shfl_down_sync(0xffffffffu, s, o);
+  if (lane == 0)
+    y[row] = (beta == 0.0 ? 0.0 : beta * y[row]) + alpha * s;
+}
+
+// ------------------------------------------------------------------ GMRES
+
+// Reference BLAS Givens generation (drotg), as reached by lib_dispatch::rotg.
+void rotg(double &a, double &b, double &c, double &s)
+{
+  double const sa = a, sb = b;
+  double const roe   = (std::fabs(sa) > std::fabs(sb)) ? sa : sb;
+  double const scale = std::fabs(sa) + std::fabs(sb);
+  double r, z;
+  if (scale == 0)
+  {
+    c = 1;
+    s = 0;
+    r = 0;
+    z = 0;
+  }
+  else
+  {
+    r = scale * std::sqrt((sa / scale) * (sa / scale) + (sb / scale) * (sb / scale));
+    r = (roe >= 0 ? 1.0 : -1.0) * r;
+    c = sa / r;
+    s = sb / r;
+    z = 1;
+    if (std::fabs(sa) > std::fabs(sb))
+      z = s;
+    if (std::fabs(sb) >= std::fabs(sa) && c != 0)
+      z = 1 / c;
+  }
+  a = r;
+  b = z;
+}
+
+inline void rot(double &x, double &y, double c, double s)
+{
+  double const tx = c * x + s * y;
+  double const ty = c * y - s * x;
+  x = tx;
+  y = ty;
+}
+
+inline int pos_from_indices(int i, int j) { return i + j * (j + 1) / 2; }
+
+// Device workspace of a GMRES solve, kept on the plan between solves.
+struct gmres_ws
+{
+  int64_t N = 0;
+  int m = 0;
+  bool flexible = false;
+  double *V = nullptr, *Z = nullptr, *part = nullptr, *h = nullptr,
+         *y = nullptr, *r = nullptr, *e = nullptr;
+  double *hh = nullptr; // pinned host mirror of h
+  int nblocks = 0;
+
+  ~gmres_ws() { release(); }
+  void release()
+  {
+    cudaFree(V);
+    cudaFree(Z);
+    cudaFree(part);
+    cudaFree(h);
+    cudaFree(y);
+    cudaFree(r);
+    cudaFree(e);
+    if (hh)
+      cudaFreeHost(hh);
+    V = Z = part = h = y = r = e = hh = nullptr;
+    N = 0;
+    m = 0;
+  }
+  int ensure(int64_t n, int restart, bool flex)
+  {
+    if (n == N && restart <= m && (!flex || Z != nullptr))
+      return ASGK_OK;
+    release();
+    int64_t bytes = 0;
+    nblocks       = max_reduction_blocks();
+    int rc;
+    if ((rc = dev_alloc(&V, n * (restart + 1), bytes)) ||
+        (flex && (rc = dev_alloc(&Z, n * restart, bytes))) ||
+        (rc = dev_alloc(&part, int64_t(nblocks) * (restart + 2), bytes)) ||
+        (rc = dev_alloc(&h, restart + 2, bytes)) ||
+        (rc = dev_alloc(&y, restart + 1, bytes)) ||
+        (rc = dev_alloc(&r, n, bytes)) || (rc = dev_alloc(&e, n, bytes)))
+    {
+      release();
+      return rc;
+    }
+    if (cudaMallocHost(reinterpret_cast<void **>(&hh),
+                       sizeof(double) * (restart + 2)) != cudaSuccess)
+    {
+      cudaGetLastError();
+      release();
+      return ASGK_ERR_ALLOC;
+    }
+    N        = n;
+    m        = restart;
+    flexible = flex;
+    return ASGK_OK;
+  }
+};
+
+using matvec_t  = std::function<int(double alpha, const double *x, double beta, double *y)>;
+using precond_t = std::function<int(const double *v, double *z)>;
+
+struct core_stats
+{
+  int total   = 0; // reference iteration count
+  int matvecs = 0;
+  int pcalls  = 0;
+  int restarts = 0;
+  double err  = 0;
+  int status  = ASGK_OK;
+  bool verified = false; // stopped on a recomputed residual
+};
+
+int norm2(gmres_ws &ws, const double *v, int64_t n, double &out,
+          cudaStream_t s)
+{
+  int blocks = 0;
+  if (int rc = launch_norm2(v, n, ws.part, &blocks, s))
+    return rc;
+  if (int rc = launch_reduce_parts(ws.part, blocks, 1, ws.h, s))
+    return rc;
+  ASGK_CUDA(cudaMemcpyAsync(ws.hh, ws.h, sizeof(double), cudaMemcpyDeviceToHost, s));
+  ASGK_CUDA(cudaStreamSynchronize(s));
+  out = std::sqrt(ws.hh[0]);
+  return ASGK_OK;
+}
+
+// solver::simple_gmres (src/solver.cpp:157-298) on device vectors.  With a
+// preconditioner it is the flexible (right-preconditioned) variant: z_j =
+// M(v_j) is stored and the update is x += Z y, so the estimated residual is
+// that of the unpreconditioned system.  As in the reference, the last Givens
+// rotation is not applied to the right-hand side once the tolerance is met.
+//
+// verify: the estimate is not trusted -- a cycle that meets the tolerance by
+// its estimate is followed by the restart residual r = b - A x, and the solve
+// stops only when ||r|| meets the tolerance (the relative-tolerance mode,
+// whose contract is the true residual).
+int gmres_core(gmres_ws &ws, int64_t n, matvec_t const &mat,
+               precond_t const *pc, double *x, const double *b, int restart,
+               int max_outer, double tol, core_stats &st, cudaStream_t s,
+               bool verify = false)
+{
+  bool const flex = (pc != nullptr);
+  if (int rc = ws.ensure(n, restart, flex))
+    return rc;
+  std::vector<double> proj(size_t(restart) * (restart + 1) / 2, 0.0);
+  std::vector<double> sines(restart + 1, 0.0), cosines(restart + 1, 0.0),
+      ksol(restart + 1, 0.0);
+  int outer       = 0;
+  double inner_res = 0, outer_res = tol + 1;
+  while (outer_res > tol && outer < max_outer)
+  {
+    double *r0 = ws.V;
+    if (int rc = launch_copy(r0, b, n, s))
+      return rc;
+    if (int rc = mat(-1.0, x, 1.0, r0))
+      return rc;
+    ++st.total;
+    ++st.matvecs;
+    if (int rc = norm2(ws, r0, n, inner_res, s))
+      return rc;
+    if (!std::isfinite(inner_res))
+    {
+      st.status = ASGK_ERR_NONFINITE;
+      st.err    = inner_res;
+      return ASGK_OK;
+    }
+    if (inner_res == 0.0 || (verify && inner_res <= tol))
+    {
+      outer_res = inner_res;
+      st.verified = true;
+      break;
+    }
+    if (int rc = launch_scale(r0, n, 1.0 / inner_res, s))
+      return rc;
+    ksol[0] = inner_res;
+    int inner = 0;
+    while (inner_res > tol && inner < restart)
+    {
+      double *vi = ws.V + int64_t(inner) * n;
+      double *w  = ws.V + int64_t(inner + 1) * n;
+      if (flex)
+      {
+        double *zi = ws.Z + int64_t(inner) * n;
+        if (int rc = (*pc)(vi, zi))
+          return rc;
+        ++st.pcalls;
+        if (int rc = mat(1.0, zi, 0.0, w))
+          return rc;
+      }
+      else if (int rc = mat(1.0, vi, 0.0, w))
+        return rc;
+      ++st.total;
+      ++st.matvecs;
+      int const k = inner + 1;
+      int blocks  = 0;
+      if (int rc = launch_multidot(ws.V, n, k, w, n, ws.part, &blocks, s))
+        return rc;
+      if (int rc = launch_reduce_parts(ws.part, blocks, k, ws.h, s))
+        return rc;
+      if (int rc = launch_update_norm(ws.V, n, k, ws.h, w, n, ws.part, &blocks, s))
+        return rc;
+      if (int rc = launch_reduce_parts(ws.part, blocks, 1, ws.h + k, s))
+        return rc;
+      ASGK_CUDA(cudaMemcpyAsync(ws.hh, ws.h, sizeof(double) * (k + 1),
+                                cudaMemcpyDeviceToHost, s));
+      ASGK_CUDA(cudaStreamSynchronize(s));
+      double const nrm = std::sqrt(ws.hh[k]);
+      if (!std::isfinite(nrm))
+      {
+        st.status = ASGK_ERR_NONFINITE;
+        st.err    = nrm;
+        return ASGK_OK;
+      }
+      if (nrm > 0)
+        if (int rc = launch_scale(w, n, 1.0 / nrm, s))
+          return rc;
+      double *coeffs = proj.data() + pos_from_indices(0, inner);
+      for (int j = 0; j < k; j++)
+        coeffs[j] = ws.hh[j];
+      for (int j = 0; j < inner; j++)
+        rot(coeffs[j], coeffs[j + 1], cosines[j], sines[j]);
+      double beta = nrm;
+      rotg(coeffs[inner], beta, cosines[inner], sines[inner]);
+      inner_res = std::fabs(sines[inner] * ksol[inner]);
+      if (inner_res > tol && inner < restart)
+      {
+        ksol[inner + 1] = 0.0;
+        rot(ksol[inner], ksol[inner + 1], cosines[inner], sines[inner]);
+      }
+      ++inner;
+      if (nrm == 0.0) // exact solution inside the Krylov space
+        break;
+    }
+    if (inner > 0)
+    {
+      // tpsv: upper, no transpose, non-unit, packed column-major
+      for (int j = inner - 1; j >= 0; j--)
+      {
+        if (ksol[j] != 0)
+        {
+          ksol[j] /= proj[pos_from_indices(j, j)];
+          double const tmp = ksol[j];
+          for (int i = j - 1; i >= 0; i--)
+            ksol[i] -= tmp * proj[pos_from_indices(i, j)];
+        }
+      }
+      ASGK_CUDA(cudaMemcpyAsync(ws.y, ksol.data(), sizeof(double) * inner,
+                                cudaMemcpyHostToDevice, s));
+      if (int rc = launch_gemv_add(flex ? ws.Z : ws.V, n, inner, ws.y, x, n, s))
+        return rc;
+      // ksol is read by the copy above before it is reused
+      ASGK_CUDA(cudaStreamSynchronize(s));
+    }
+    ++outer;
+    ++st.restarts;
+    outer_res = inner_res;
+    if (verify && outer_res <= tol)
+      outer_res = tol + 1; // confirm on the restart residual
+  }
+  if (verify && !st.verified && outer >= max_outer)
+    outer_res = inner_res;
+  st.err = outer_res;
+  if (outer_res > tol)
+    st.status = ASGK_ERR_NOT_CONVERGED;
+  return ASGK_OK;
+}
+
+} // namespace
+} // namespace asgk
+
+// Workspace lives beside the plan (kept out of plan_data so the kernels'
+// view of the plan stays trivially copyable).
+namespace
+{
+struct plan_extras
+{
+  asgk::gmres_ws ws;
+};
+std::vector<std::pair<asgk_plan *, plan_extras *>> g_extras;
+
+plan_extras *extras_of(asgk_plan *p, bool create)
+{
+  for (auto &e : g_extras)
+    if (e.first == p)
+      return e.second;
+  if (!create)
+    return nullptr;
+  auto *x = new plan_extras();
+  g_extras.emplace_back(p, x);
+  return x;
+}
+
+void drop_extras(asgk_plan *p)
+{
+  for (size_t i = 0; i < g_extras.size(); i++)
+    if (g_extras[i].first == p)
+    {
+      delete g_extras[i].second;
+      g_extras.erase(g_extras.begin() + i);
+      return;
+    }
+}
+} // namespace
+
+using namespace asgk;
+
+extern "C"
+{
+const char *asgk_status_string(int status)
+{
+  switch (status)
+  {
+  case ASGK_OK: return "success";
+  case ASGK_ERR_INVALID: return "invalid argument";
+  case ASGK_ERR_UNSUPPORTED: return "unsupported dimension or size";
+  case ASGK_ERR_CUDA: return "CUDA runtime error";
+  case ASGK_ERR_ALLOC: return "allocation failed";
+  case ASGK_ERR_BREAKDOWN: return "GMRES breakdown";
+  case ASGK_ERR_NOT_CONVERGED: return "GMRES did not converge";
+  case ASGK_ERR_NONFINITE: return "non-finite residual";
+  default: return "unknown status";
+  }
+}
+
+int64_t asgk_launch_count(void) { return g_launches.load(); }
+
+int asgk_device_info(int *sm_count, int *cc_major, int *cc_minor)
+{
+  int dev = 0;
+  ASGK_CUDA(cudaGetDevice(&dev));
+  if (sm_count)
+    ASGK_CUDA(cudaDeviceGetAttribute(sm_count, cudaDevAttrMultiProcessorCount, dev));
+  if (cc_major)
+    ASGK_CUDA(cudaDeviceGetAttribute(cc_major, cudaDevAttrComputeCapabilityMajor, dev));
+  if (cc_minor)
+    ASGK_CUDA(cudaDeviceGetAttribute(cc_minor, cudaDevAttrComputeCapabilityMinor, dev));
+  return ASGK_OK;
+}
+
+int asgk_plan_create(asgk_plan **plan, int d, int n, int num_rows,
+                     int num_cols, int num_terms, const int64_t *row_ptr,
+                     const int *col_indx, const int *iA, const double *vA,
+                     int64_t vA_len)
+{
+  if (row_ptr == nullptr || num_rows < 0)
+    return ASGK_ERR_INVALID;
+  std::vector<int64_t> rp(row_ptr, row_ptr + num_rows + 1);
+  return build_plan(plan, d, n, num_rows, num_cols, num_terms, rp, col_indx,
+                    iA, index_mode::expanded, vA, vA_len);
+}
+
+int asgk_plan_create_conn(asgk_plan **plan, int d, int n, int num_rows,
+                          int num_cols, int num_terms, const int64_t *row_ptr,
+                          const int *col_indx, const int *conn,
+                          const double *vA, int64_t vA_len)
+{
+  if (row_ptr == nullptr || num_rows < 0)
+    return ASGK_ERR_INVALID;
+  std::vector<int64_t> rp(row_ptr, row_ptr + num_rows + 1);
+  return build_plan(plan, d, n, num_rows, num_cols, num_terms, rp, col_indx,
+                    conn, index_mode::conn, vA, vA_len);
+}
+
+int asgk_plan_create_pairs(asgk_plan **plan, int d, int n, int num_rows,
+                           int num_cols, int num_terms, int64_t num_batch,
+                           const int *iy, const int *ix, const int *iA,
+                           const double *vA, int64_t vA_len)
+{
+  if (plan == nullptr)
+    return ASGK_ERR_INVALID;
+  if (int rc = check_dims(d, n, num_rows, num_cols, num_terms))
+    return rc;
+  if (num_batch < 0 || (num_batch > 0 && (iy == nullptr || ix == nullptr)))
+    return ASGK_ERR_INVALID;
+  int64_t const ts = ipow(n, d);
+  std::vector<int64_t> rp(num_rows + 1, 0);
+  for (int64_t i = 0; i < num_batch; i++)
+  {
+    if (iy[i] < 0 || iy[i] % ts != 0 || iy[i] / ts >= num_rows ||
+        ix[i] < 0 || ix[i] % ts != 0 || ix[i] / ts >= num_cols)
+      return ASGK_ERR_INVALID;
+    rp[iy[i] / ts + 1]++;
+  }
+  for (int r = 0; r < num_rows; r++)
+    rp[r + 1] += rp[r];
+  std::vector<int64_t> fill(rp.begin(), rp.end() - 1);
+  std::vector<int> col(num_batch);
+  int64_t const per = int64_t(num_terms) * d;
+  std::vector<int> ia(num_batch * per);
+  for (int64_t i = 0; i < num_batch; i++)
+  {
+    int64_t const dst = fill[iy[i] / ts]++;
+    col[dst]          = int(ix[i] / ts);
+    if (per > 0)
+      std::copy_n(iA + i * per, per, ia.data() + dst * per);
+  }
+  return build_plan(plan, d, n, num_rows, num_cols, num_terms, rp, col.data(),
+                    ia.data(), index_mode::expanded, vA, vA_len);
+}
+
+void asgk_plan_destroy(asgk_plan *plan)
+{
+  if (!plan)
+    return;
+  drop_extras(plan);
+  free_plan(plan->p);
+  delete plan;
+}
+
+int asgk_plan_update_values(asgk_plan *plan, const double *vA, int64_t vA_len)
+{
+  if (!plan || vA_len != plan->p.vA_len || (vA_len > 0 && !vA))
+    return ASGK_ERR_INVALID;
+  return upload_values(plan->p, vA);
+}
+
+int asgk_plan_info(const asgk_plan *plan, int64_t *num_batch,
+                   int64_t *input_size, int64_t *output_size, int64_t *flops,
+                   int64_t *device_bytes)
+{
+  if (!plan)
+    return ASGK_ERR_INVALID;
+  auto const &p = plan->p;
+  if (num_batch)
+    *num_batch = p.nnz;
+  if (input_size)
+    *input_size = int64_t(p.cols) * p.tensor;
+  if (output_size)
+    *output_size = int64_t(p.rows) * p.tensor;
+  if (flops)
+    *flops = int64_t(p.tensor) * p.n * p.d * p.terms * p.nnz * 2;
+  if (device_bytes)
+    *device_bytes = p.device_bytes;
+  return ASGK_OK;
+}
+
+int asgk_apply(asgk_plan *plan, int precision, double alpha, const double *x,
+               double beta, double *y, asgk_stream stream)
+{
+  if (!plan || !x || !y)
+    return ASGK_ERR_INVALID;
+  auto &p = plan->p;
+  cudaStream_t s = as_stream(stream);
+  if (p.terms == 0 || p.nnz == 0 || alpha == 0.0)
+  {
+    // only the scaling of y remains (src/asgard_kronmult_matrix.hpp:344-349)
+    int64_t const ny = int64_t(p.rows) * p.tensor;
+    if (beta == 0.0)
+      return launch_fill(y, ny, 0.0, s);
+    if (beta != 1.0)
+      return launch_scale(y, ny, beta, s);
+    return ASGK_OK;
+  }
+  return launch_apply(p, precision, alpha, x, 0, beta, y, 0, 0.0, s);
+}
+
+int asgk_apply_f32(asgk_plan *plan, float alpha, const float *x, float beta,
+                   float *y, asgk_stream stream)
+{
+  if (!plan || !x || !y)
+    return ASGK_ERR_INVALID;
+  auto &p = plan->p;
+  if (p.terms == 0 || p.nnz == 0)
+    return ASGK_ERR_UNSUPPORTED;
+  return launch_apply(p, ASGK_FP32, alpha, x, 1, beta, y, 1, 0.0,
+                      as_stream(stream));
+}
+
+int asgk_apply_host(asgk_plan *plan, double alpha, const double *x,
+                    double beta, double *y, asgk_stream stream)
+{
+  if (!plan || !x || !y)
+    return ASGK_ERR_INVALID;
+  auto &p          = plan->p;
+  cudaStream_t s   = as_stream(stream);
+  int64_t const nx = int64_t(p.cols) * p.tensor;
+  int64_t const ny = int64_t(p.rows) * p.tensor;
+  ASGK_CUDA(cudaMemcpyAsync(p.xw, x, sizeof(double) * nx,
+                            cudaMemcpyHostToDevice, s));
+  if (beta != 0.0)
+    ASGK_CUDA(cudaMemcpyAsync(p.yw, y, sizeof(double) * ny,
+                              cudaMemcpyHostToDevice, s));
+  if (int rc = asgk_apply(plan, ASGK_FP64, alpha, p.xw, beta, p.yw, stream))
+    return rc;
+  ASGK_CUDA(cudaMemcpyAsync(y, p.yw, sizeof(double) * ny,
+                            cudaMemcpyDeviceToHost, s));
+  ASGK_CUDA(cudaStreamSynchronize(s));
+  return ASGK_OK;
+}
+
+int asgk_apply_euler(asgk_plan *plan, int precision, double dt, double alpha,
+                     const double *x, double beta, double *y,
+                     asgk_stream stream)
+{
+  if (!plan || !x || !y)
+    return ASGK_ERR_INVALID;
+  auto &p = plan->p;
+  if (p.rows != p.cols)
+    return ASGK_ERR_INVALID;
+  cudaStream_t s = as_stream(stream);
+  if (p.terms == 0 || p.nnz == 0 || dt == 0.0)
+  {
+    int64_t const ny = int64_t(p.rows) * p.tensor;
+    if (beta == 0.0)
+    {
+      if (int rc = launch_copy(y, x, ny, s))
+        return rc;
+      return launch_scale(y, ny, alpha, s);
+    }
+    if (int rc = launch_scale(y, ny, beta, s))
+      return rc;
+    return launch_axpy(y, x, ny, alpha, s);
+  }
+  return launch_apply(p, precision, -dt * alpha, x, 0, beta, y, 0, alpha, s);
+}
+
+int asgk_gmres_dense(int n, const double *A, double *x, const double *b,
+                     int restart, int max_outer, double tol,
+                     asgk_gmres_info *info)
+{
+  if (n <= 0 || !A || !x || !b)
+    return ASGK_ERR_INVALID;
+  if (restart <= 0)
+    restart = asgk_default_gmres_restarts(n);
+  if (restart > n)
+    return ASGK_ERR_INVALID;
+  if (max_outer <= 0)
+    max_outer = n;
+  if (!(tol > 0))
+    tol = 1e-12;
+  double *dA = nullptr, *dx = nullptr, *db = nullptr;
+  int64_t bytes = 0;
+  int rc;
+  if ((rc = dev_alloc(&dA, int64_t(n) * n, bytes)) ||
+      (rc = dev_alloc(&dx, n, bytes)) || (rc = dev_alloc(&db, n, bytes)))
+  {
+    cudaFree(dA);
+    cudaFree(dx);
+    return rc;
+  }
+  cudaStream_t s = nullptr;
+  gmres_ws ws;
+  core_stats st;
+  auto mat = [&](double a, const double *xin, double bb, double *yout) -> int {
+    k_dense_gemv<<<(n + 3) / 4, 128, 0, s>>>(n, dA, a, xin, bb, yout);
+    ASGK_LAUNCHED();
+    return ASGK_OK;
+  };
+  rc = ASGK_OK;
+  if (cudaMemcpy(dA, A, sizeof(double) * n * int64_t(n), cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(dx, x, sizeof(double) * n, cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(db, b, sizeof(double) * n, cudaMemcpyHostToDevice) != cudaSuccess)
+    rc = ASGK_ERR_CUDA;
+  if (rc == ASGK_OK)
+    rc = gmres_core(ws, n, mat, nullptr, dx, db, restart, max_outer, tol, st, s);
+  if (rc == ASGK_OK &&
+      cudaMemcpy(x, dx, sizeof(double) * n, cudaMemcpyDeviceToHost) != cudaSuccess)
+    rc = ASGK_ERR_CUDA;
+  cudaFree(dA);
+  cudaFree(dx);
+  cudaFree(db);
+  if (rc == ASGK_OK && info)
+  {
+    *info              = asgk_gmres_info{};
+    info->error        = st.err;
+    info->iterations   = st.total;
+    info->status       = st.status;
+    info->outer_steps  = st.restarts;
+    info->matvecs_fp64 = st.matvecs;
+  }
+  return rc;
+}
+
+int asgk_default_gmres_restarts(int64_t n)
+{
+  int const minimum = int(std::min<int64_t>(10, n));
+  int const maximum = int(std::min<int64_t>(200, n));
+  double const MB   = double(n) * sizeof(double) / 1048576.0;
+  int const want    = int(512.0 / MB);
+  return std::clamp(want, minimum, maximum);
+}
+
+int asgk_gmres_euler(asgk_plan *plan, double dt, double *x, const double *b,
+                     int restart, int max_outer, double tol, int tol_mode,
+                     int precision, asgk_mlp *precond, asgk_gmres_info *info,
+                     asgk_stream stream)
+{
+  if (!plan || !x || !b)
+    return ASGK_ERR_INVALID;
+  auto &p = plan->p;
+  if (p.rows != p.cols)
+    return ASGK_ERR_INVALID;
+  if (precision != ASGK_FP64 && precision != ASGK_FP32)
+    return ASGK_ERR_UNSUPPORTED;
+  int64_t const n = int64_t(p.rows) * p.tensor;
+  if (restart <= 0)
+    restart = asgk_default_gmres_restarts(n);
+  if (restart > n)
+    return ASGK_ERR_INVALID; // src/solver.cpp:175-181
+  if (max_outer <= 0)
+    max_outer = int(std::min<int64_t>(n, 1 << 30));
+  if (!(tol > 0))
+    tol = 1e-12; // src/solver.cpp:165-166 default for double
+  cudaStream_t s = as_stream(stream);
+  auto *ex       = extras_of(plan, true);
+  gmres_ws &ws   = ex->ws;
+
+  asgk_gmres_info out{};
+  auto op64 = [&](double a, const double *xin, double bb, double *yout) -> int {
+    return asgk_apply_euler(plan, ASGK_FP64, dt, a, xin, bb, yout, stream);
+  };
+  auto oplow = [&](double a, const double *xin, double bb, double *yout) -> int {
+    return asgk_apply_euler(plan, precision, dt, a, xin, bb, yout, stream);
+  };
+  precond_t pcf;
+  precond_t const *pcp = nullptr;
+  if (precond != nullptr)
+  {
+    pcf = [&](const double *v, double *z) -> int {
+      return mlp_precondition(precond, plan, v, z, s);
+    };
+    pcp = &pcf;
+  }
+
+  double bnorm = 0;
+  if (ws.ensure(n, restart, pcp != nullptr) != ASGK_OK)
+    return ASGK_ERR_ALLOC;
+  if (int rc = norm2(ws, b, n, bnorm, s))
+    return rc;
+  double const tol_abs = (tol_mode == ASGK_TOL_REL) ? tol * bnorm : tol;
+
+  core_stats st;
+  int status = ASGK_OK;
+  double true_res = -1; // FP64 residual of the final x when already known
+  if (precision == ASGK_FP64 && precond == nullptr)
+  {
+    if (int rc = gmres_core(ws, n, op64, nullptr, x, b, restart, max_outer,
+                            tol_abs, st, s, tol_mode == ASGK_TOL_REL))
+      return rc;
+    out.error        = st.err;
+    out.iterations   = st.total;
+    out.outer_steps  = st.restarts;
+    out.matvecs_fp64 = st.matvecs;
+    status           = st.status;
+    if (st.verified)
+      true_res = st.err;
+  }
+  else
+  {
+    // FP64 iterative refinement: r = b - A x in FP64, inner (flexible) GMRES
+    // on A e = r with the low-precision operator, x += e.
+    double const inner_rtol = (precision == ASGK_FP64) ? 1e-10 : 1e-5;
+    int total = 0, low = 0, fp64 = 0, pcalls = 0, steps = 0;
+    double rnorm = 0;
+    int const max_steps = 50;
+    status = ASGK_ERR_NOT_CONVERGED;
+    for (;;)
+    {
+      if (int rc = launch_copy(ws.r, b, n, s))
+        return rc;
+      if (int rc = op64(-1.0, x, 1.0, ws.r))
+        return rc;
+      ++fp64;
+      if (int rc = norm2(ws, ws.r, n, rnorm, s))
+        return rc;
+      if (!std::isfinite(rnorm))
+      {
+        status = ASGK_ERR_NONFINITE;
+        break;
+      }
+      if (rnorm <= tol_abs)
+      {
+        status   = ASGK_OK;
+        true_res = rnorm;
+        break;
+      }
+      if (steps >= max_steps || total >= max_outer * (restart + 1))
+        break;
+      if (int rc = launch_fill(ws.e, n, 0.0, s))
+        return rc;
+      core_stats ist;
+      double const itol = std::max(inner_rtol * rnorm, 0.5 * tol_abs);
+      int const inner_outer = std::max(1, max_outer);
+      if (int rc = gmres_core(ws, n, (precision == ASGK_FP64) ? matvec_t(op64) : matvec_t(oplow),
+                              pcp, ws.e, ws.r, restart, inner_outer, itol, ist, s))
+        return rc;
+      total += ist.total;
+      if (precision == ASGK_FP64)
+        fp64 += ist.matvecs;
+      else
+        low += ist.matvecs;
+      pcalls += ist.pcalls;
+      ++steps;
+      if (ist.status == ASGK_ERR_NONFINITE)
+      {
+        status = ASGK_ERR_NONFINITE;
+        break;
+      }
+      if (int rc = launch_axpy(x, ws.e, n, 1.0, s))
+        return rc;
+    }
+    out.error        = rnorm;
+    out.iterations   = total;
+    out.outer_steps  = steps;
+    out.matvecs_low  = low;
+    out.matvecs_fp64 = fp64;
+    out.precond_calls = pcalls;
+  }
+  // FP64 check of the final iterate (unless the solve ended on one)
+  double rfinal = true_res;
+  if (rfinal < 0)
+  {
+    if (int rc = launch_copy(ws.r, b, n, s))
+      return rc;
+    if (int rc = op64(-1.0, x, 1.0, ws.r))
+      return rc;
+    if (int rc = norm2(ws, ws.r, n, rfinal, s))
+      return rc;
+  }
+  out.true_relres = (bnorm > 0) ? rfinal / bnorm : rfinal;
+  out.status      = status;
+  if (info)
+    *info = out;
+  return ASGK_OK;
+}
+
+} // extern "C"

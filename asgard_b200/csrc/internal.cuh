@@ -1,0 +1,112 @@
+// Internal declarations shared by the asgard_b200 CUDA sources.
+#pragma once
+
+#include "asgard_b200.h"
+
+#include <cuda_runtime.h>
+#include <atomic>
+#include <cstdint>
+#include <cstdio>
+#include <vector>
+
+namespace asgk
+{
+// Launch counter (all kernels launched by this library).
+extern std::atomic<int64_t> g_launches;
+inline void count_launch(int k = 1) { g_launches.fetch_add(k, std::memory_order_relaxed); }
+
+#define ASGK_CUDA(call)                                                        \
+  do                                                                           \
+  {                                                                            \
+    cudaError_t asgk_err_ = (call);                                            \
+    if (asgk_err_ != cudaSuccess)                                              \
+    {                                                                          \
+      std::fprintf(stderr, "asgard_b200: %s failed: %s (%s:%d)\n", #call,      \
+                   cudaGetErrorString(asgk_err_), __FILE__, __LINE__);         \
+      return ASGK_ERR_CUDA;                                                    \
+    }                                                                          \
+  } while (0)
+
+#define ASGK_LAUNCHED()                                                        \
+  do                                                                           \
+  {                                                                            \
+    cudaError_t asgk_err_ = cudaGetLastError();                                \
+    if (asgk_err_ != cudaSuccess)                                              \
+    {                                                                          \
+      std::fprintf(stderr, "asgard_b200: launch failed: %s (%s:%d)\n",         \
+                   cudaGetErrorString(asgk_err_), __FILE__, __LINE__);         \
+      return ASGK_ERR_CUDA;                                                    \
+    }                                                                          \
+    ::asgk::count_launch();                                                    \
+  } while (0)
+
+// How the factor blocks of a pair are addressed.
+enum class index_mode : int
+{
+  expanded = 0, // iA[(p*T + t)*d + k]: reference layout, any offsets
+  conn     = 1  // conn[p*d + k]*(d*T*n*n) + (t*d + k)*n*n: sparse-grid layout
+};
+
+// Device-resident operator.  Pairs are grouped by output cell (CSR) and the
+// cells are visited in order of decreasing pair count.
+struct plan_data
+{
+  int d = 0, n = 0, rows = 0, cols = 0, terms = 0;
+  int tensor = 0;      // n^d
+  int64_t nnz = 0;     // number of (row, col) pairs
+  index_mode mode = index_mode::expanded;
+  int64_t vA_len = 0;
+
+  int64_t *row_ptr = nullptr; // [rows + 1]
+  int *col     = nullptr;     // [nnz] column cell per pair
+  int *idx     = nullptr;     // [nnz*T*d] (expanded) or [nnz*d] (conn)
+  int *row_order = nullptr;   // [rows] cells by decreasing pair count
+  double *vA64 = nullptr;     // [vA_len]
+  float *vA32  = nullptr;     // [vA_len]
+
+  // FP64 workspace for apply_host and GMRES scratch
+  double *xw = nullptr, *yw = nullptr;
+  int64_t device_bytes = 0;
+};
+
+} // namespace asgk
+
+struct asgk_plan
+{
+  asgk::plan_data p;
+};
+
+namespace asgk
+{
+// kron_kernels.cu
+int launch_apply(plan_data const &p, int precision, double alpha,
+                 const void *x, int x_is_f32, double beta, void *y,
+                 int y_is_f32, double euler_x_coeff, cudaStream_t s);
+
+// krylov.cu: BLAS-1/2 pieces of the device-resident GMRES
+int launch_fill(double *v, int64_t n, double value, cudaStream_t s);
+int launch_copy(double *dst, const double *src, int64_t n, cudaStream_t s);
+int launch_scale(double *v, int64_t n, double alpha, cudaStream_t s);
+int launch_axpy(double *y, const double *x, int64_t n, double alpha,
+                cudaStream_t s);
+int launch_xpby(double *y, const double *x, int64_t n, double beta,
+                cudaStream_t s);
+// partial sums of V[:,0..k)^T w into part[blocks][k]; returns blocks used
+int launch_multidot(const double *V, int64_t ldv, int k, const double *w,
+                    int64_t n, double *part, int *blocks, cudaStream_t s);
+// out[j] = sum_b part[b][j]
+int launch_reduce_parts(const double *part, int blocks, int k, double *out,
+                        cudaStream_t s);
+// w -= V[:,0..k) h; part[b] = partial sum of w^2 after the update
+int launch_update_norm(const double *V, int64_t ldv, int k, const double *h,
+                       double *w, int64_t n, double *part, int *blocks,
+                       cudaStream_t s);
+// part[b] = partial sums of v^2
+int launch_norm2(const double *v, int64_t n, double *part, int *blocks,
+                 cudaStream_t s);
+// x += V[:,0..k) y
+int launch_gemv_add(const double *V, int64_t ldv, int k, const double *y,
+                    double *x, int64_t n, cudaStream_t s);
+int max_reduction_blocks();
+
+} // namespace asgk

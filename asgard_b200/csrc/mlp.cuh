@@ -1,0 +1,11 @@
+// Learned preconditioner (per-cell MLP) used inside flexible GMRES.
+#pragma once
+
+#include "internal.cuh"
+
+namespace asgk
+{
+// z = M(v): applies the network cell by cell to the FP64 Krylov vector v.
+int mlp_precondition(asgk_mlp *mlp, asgk_plan *plan, const double *v,
+                     double *z, cudaStream_t s);
+} // namespace asgk

@@ -1,0 +1,265 @@
+"""Python mirror of the reference's kronmult_matrix / simple_gmres interfaces.
+
+Mirrors ``asgard::kronmult_matrix<P>`` (src/asgard_kronmult_matrix.hpp:111-682)
+and ``asgard::solver::simple_gmres_euler`` / ``simple_gmres``
+(src/solver.hpp:17-41) over the C ABI.  Device vectors are CUDA tensors
+(torch, float64 unless stated); host vectors are numpy arrays.  Errors raise
+the reference's exception types: ``RuntimeError`` for unsupported shapes and
+runtime failures, ``ValueError`` (std::invalid_argument) for a restart larger
+than the system.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from ._lib import AsgkError, GmresInfo, check, lib
+
+FP64, FP32, BF16 = 0, 1, 2
+TOL_ABS, TOL_REL = 0, 1
+_PREC = {"fp64": FP64, "fp32": FP32, "bf16": BF16}
+
+
+def _precision(p) -> int:
+    return _PREC[p] if isinstance(p, str) else int(p)
+
+
+def _host(a, dtype):
+    return np.ascontiguousarray(a, dtype=dtype)
+
+
+def _ptr(t):
+    """Device pointer of a CUDA tensor (or 0/None)."""
+    if t is None:
+        return None
+    return C.c_void_p(t.data_ptr())
+
+
+def _stream(stream):
+    if stream is None:
+        import torch
+        return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    if isinstance(stream, int):
+        return C.c_void_p(stream)
+    return C.c_void_p(stream.cuda_stream)
+
+
+@dataclass
+class gmres_info:
+    """``gmres_info<P>`` (src/pde/pde_base.hpp:93-97) plus solve diagnostics."""
+    error: float
+    iterations: int
+    status: int = 0
+    true_relres: float = float("nan")
+    outer_steps: int = 0
+    matvecs_low: int = 0
+    matvecs_fp64: int = 0
+    precond_calls: int = 0
+    fallback: int = 0
+
+
+class kronmult_matrix:
+    """A batched-Kronecker operator held on the GPU (see module docstring)."""
+
+    def __init__(self, handle, d, n, rows, cols, terms):
+        self._h = handle
+        self.num_dimensions = d
+        self.kron_size = n
+        self.num_rows = rows
+        self.num_cols = cols
+        self.num_terms = terms
+
+    # -- constructors ------------------------------------------------------
+    @classmethod
+    def from_csr(cls, d, n, num_rows, num_cols, num_terms, pntr, indx, iA, vA):
+        """Reference CPU sparse format: row pointers, column cells, iA, vA."""
+        pntr = _host(pntr, np.int64)
+        indx = _host(indx, np.int32)
+        iA = _host(iA, np.int32)
+        vA = _host(vA, np.float64)
+        h = C.c_void_p()
+        check(lib.asgk_plan_create(C.byref(h), d, n, num_rows, num_cols,
+                                   num_terms, pntr.ctypes.data,
+                                   indx.ctypes.data, iA.ctypes.data,
+                                   vA.ctypes.data, len(vA)), "plan_create")
+        return cls(h, d, n, num_rows, num_cols, num_terms)
+
+    @classmethod
+    def from_pairs(cls, d, n, num_rows, num_cols, num_terms, row_indx,
+                   col_indx, iA, vA):
+        """Reference GPU format: per pair the tensor offsets into y and x."""
+        iy = _host(row_indx, np.int32)
+        ix = _host(col_indx, np.int32)
+        iA = _host(iA, np.int32)
+        vA = _host(vA, np.float64)
+        h = C.c_void_p()
+        check(lib.asgk_plan_create_pairs(C.byref(h), d, n, num_rows, num_cols,
+                                         num_terms, len(iy), iy.ctypes.data,
+                                         ix.ctypes.data, iA.ctypes.data,
+                                         vA.ctypes.data, len(vA)),
+              "plan_create_pairs")
+        return cls(h, d, n, num_rows, num_cols, num_terms)
+
+    @classmethod
+    def from_conn(cls, d, n, num_rows, num_cols, num_terms, row_ptr, col_indx,
+                  conn, vA):
+        """Sparse-grid format: per pair the d 1D connection indices."""
+        rp = _host(row_ptr, np.int64)
+        ci = _host(col_indx, np.int32)
+        cn = _host(conn, np.int32)
+        vA = _host(vA, np.float64)
+        h = C.c_void_p()
+        check(lib.asgk_plan_create_conn(C.byref(h), d, n, num_rows, num_cols,
+                                        num_terms, rp.ctypes.data,
+                                        ci.ctypes.data, cn.ctypes.data,
+                                        vA.ctypes.data, len(vA)),
+              "plan_create_conn")
+        return cls(h, d, n, num_rows, num_cols, num_terms)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            lib.asgk_plan_destroy(h)
+            self._h = None
+
+    @property
+    def handle(self):
+        return self._h
+
+    # -- accessors (src/asgard_kronmult_matrix.hpp:480-577) ---------------
+    def _info(self):
+        vals = [C.c_int64() for _ in range(5)]
+        check(lib.asgk_plan_info(self._h, *[C.byref(v) for v in vals]))
+        return [v.value for v in vals]
+
+    def num_batch(self):
+        return self._info()[0]
+
+    def tensor_size(self):
+        return self.kron_size ** self.num_dimensions
+
+    def input_size(self):
+        return self._info()[1]
+
+    def output_size(self):
+        return self._info()[2]
+
+    def flops(self):
+        """compute_flops: 2 * n^d * n * d * T * pairs."""
+        return self._info()[3]
+
+    def device_bytes(self):
+        return self._info()[4]
+
+    @staticmethod
+    def compute_tensor_size(num_dimensions, kron_size):
+        return kron_size ** num_dimensions
+
+    @staticmethod
+    def compute_flops(num_dimensions, kron_size, num_terms, num_batch):
+        return kron_size ** num_dimensions * kron_size * num_dimensions * num_terms * num_batch * 2
+
+    def is_dense(self):
+        return False
+
+    def is_onecall(self):
+        return True
+
+    def __bool__(self):
+        return self.num_dimensions > 0
+
+    def update_stored_coefficients(self, vA):
+        vA = _host(vA, np.float64)
+        check(lib.asgk_plan_update_values(self._h, vA.ctypes.data, len(vA)),
+              "update_stored_coefficients")
+
+    # -- apply -------------------------------------------------------------
+    def apply(self, alpha, x, beta, y, resource="device", precision="fp64",
+              stream=None):
+        """y = beta*y + alpha*K*x.
+
+        resource="device": x, y are CUDA tensors (float64, or float32 for a
+        float32 apply); resource="host": numpy float64 arrays, copied to and
+        from the GPU inside the call."""
+        if resource == "host":
+            xs = _host(x, np.float64)
+            if not (y.flags["C_CONTIGUOUS"] and y.dtype == np.float64):
+                raise ValueError("y must be a contiguous float64 array")
+            check(lib.asgk_apply_host(self._h, alpha, xs.ctypes.data, beta,
+                                      y.ctypes.data, _stream(stream)), "apply")
+            return y
+        import torch
+        if x.dtype == torch.float32:
+            check(lib.asgk_apply_f32(self._h, alpha, _ptr(x), beta, _ptr(y),
+                                     _stream(stream)), "apply")
+        else:
+            check(lib.asgk_apply(self._h, _precision(precision), alpha,
+                                 _ptr(x), beta, _ptr(y), _stream(stream)),
+                  "apply")
+        return y
+
+    def apply_euler(self, dt, alpha, x, beta, y, precision="fp64", stream=None):
+        """y = beta*y + alpha*(x - dt*K*x) on device tensors."""
+        check(lib.asgk_apply_euler(self._h, _precision(precision), dt, alpha,
+                                   _ptr(x), beta, _ptr(y), _stream(stream)),
+              "apply_euler")
+        return y
+
+
+def simple_gmres_euler(dt, mat: kronmult_matrix, x, b, restart=-1,
+                       max_iter=-1, tol=-1.0, tol_mode="abs",
+                       precision="fp64", precond=None, stream=None):
+    """Solves (I - dt*K) x = b in place on device tensors (x = initial guess).
+
+    tol_mode="abs" is the reference criterion (estimated residual <= tol);
+    "rel" stops at tol * ||b||.  precision "fp32"/"bf16" runs the Krylov
+    operator in that arithmetic inside FP64 iterative refinement.  precond is
+    a learned preconditioner (asgard_b200.precond.LearnedPreconditioner) used
+    on the right through flexible GMRES."""
+    n = mat.output_size()
+    if restart is not None and restart > n:
+        raise ValueError(f"Number of inner iterations {restart} must be less than {n}!")
+    info = GmresInfo()
+    pc = precond.handle if precond is not None else None
+    rc = lib.asgk_gmres_euler(mat.handle, dt, _ptr(x), _ptr(b),
+                              -1 if restart is None else restart,
+                              -1 if max_iter is None else max_iter, tol,
+                              TOL_REL if tol_mode == "rel" else TOL_ABS,
+                              _precision(precision), pc, C.byref(info),
+                              _stream(stream))
+    if rc == 1 and restart is not None and restart > n:
+        raise ValueError("restart larger than the system")
+    check(rc, "simple_gmres_euler")
+    return gmres_info(**info.as_dict())
+
+
+def simple_gmres(A, x, b, M=None, restart=-1, max_iter=-1, tol=-1.0):
+    """Dense test path of solver::simple_gmres (host arrays, solved on the GPU)."""
+    if M is not None and np.size(M) > 0:
+        raise NotImplementedError("dense LU preconditioner is not provided")
+    A = np.asfortranarray(A, dtype=np.float64)
+    n = A.shape[0]
+    if restart is not None and restart > n:
+        raise ValueError(f"Number of inner iterations {restart} must be less than {n}!")
+    bb = _host(b, np.float64)
+    if not (x.flags["C_CONTIGUOUS"] and x.dtype == np.float64):
+        raise ValueError("x must be a contiguous float64 array")
+    info = GmresInfo()
+    check(lib.asgk_gmres_dense(n, A.ctypes.data, x.ctypes.data, bb.ctypes.data,
+                               restart, max_iter, tol, C.byref(info)),
+          "simple_gmres")
+    return gmres_info(**info.as_dict())
+
+
+def default_gmres_restarts(n: int) -> int:
+    return lib.asgk_default_gmres_restarts(n)
+
+
+def launch_count() -> int:
+    return lib.asgk_launch_count()
+
+
+__all__ = ["kronmult_matrix", "simple_gmres_euler", "simple_gmres",
+           "gmres_info", "default_gmres_restarts", "launch_count", "AsgkError"]

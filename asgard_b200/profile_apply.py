@@ -1,0 +1,69 @@
+"""Times the kronmult apply kernel on a synthetic sparse-grid operator.
+
+    python -m asgard_b200.profile_apply --d 4 --level 7 --terms 4 \
+        --precision fp64 --reps 3 [--warmup 1]
+
+Builds the operator (advection/diffusion factors unless --kind random), runs
+--warmup untimed applies of the fused backward-Euler operator
+y = x - dt*K*x, then --reps timed applies (CUDA events on the launching
+stream) and prints one JSON line: ms per launch, algorithmic TFLOP/s
+(2*d*T*n^(d+1) flops per pair) and the fraction of the measured FMA peak.
+This is the command the ncu summaries under profiles/ were taken with.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import time
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--d", type=int, default=4)
+    ap.add_argument("--level", type=int, default=7)
+    ap.add_argument("--terms", type=int, default=4)
+    ap.add_argument("--kind", default="advdiff")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32", "bf16"])
+    ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=1)
+    ap.add_argument("--peak", action="store_true", help="also measure the FMA peak")
+    args = ap.parse_args()
+
+    import torch
+    import asgard_b200 as ab
+
+    t0 = time.perf_counter()
+    op = ab.SparseGridOperator(args.d, args.level, args.terms, kind=args.kind)
+    mat = op.kronmult_matrix()
+    t_setup = time.perf_counter() - t0
+    g = torch.Generator(device="cuda").manual_seed(0)
+    x = torch.rand(op.N, dtype=torch.float64, device="cuda", generator=g) * 2 - 1
+    y = torch.zeros_like(x)
+    for _ in range(args.warmup):
+        mat.apply_euler(1e-3, 1.0, x, 0.0, y, precision=args.precision)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.reps):
+        mat.apply_euler(1e-3, 1.0, x, 0.0, y, precision=args.precision)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.reps
+    flops = op.flops()
+    out = {"d": args.d, "level": args.level, "terms": args.terms,
+           "precision": args.precision, "cells": op.rows, "pairs": op.nnz,
+           "dofs": op.N, "ms_per_launch": ms, "tflops": flops / ms / 1e9,
+           "flops_per_launch": flops, "setup_s": t_setup,
+           "device_bytes": mat.device_bytes()}
+    if args.peak:
+        pk = C.c_double()
+        ab.lib.asgk_measure_fma_peak(0 if args.precision == "fp64" else 1, C.byref(pk))
+        out["fma_peak_tflops"] = pk.value
+        out["frac"] = out["tflops"] / pk.value
+    print(json.dumps(out))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,426 @@
+"""Benchmark: implicit backward-Euler solves per second on one B200.
+
+Workload (default ``d4``): d=4, n=3 (81 dofs per cell), level-7 sparse grid
+(4048 cells, 327,888 dofs, 12,258,592 connected cell pairs), 4 terms of
+advection/diffusion factors, solve (I - dt*K) x = b with dt = 1e-3,
+b uniform in [-1, 1] (seeded, a new b every step), GMRES restart 50, until the
+FP64 relative residual ||b - (I - dt K) x|| / ||b|| <= 1e-10.
+
+A step is one solve by the framework's method (mixed-precision FGMRES with
+FP64 iterative refinement; the plain FP64 GMRES with the FP64 kronmult is
+timed beside it).  Inputs are resident in HBM when the timed region starts;
+the operator (pair list + factor indices, ~245 MB) is larger than L2, so
+no extra L2 flush is done between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+For N > 1 (torchrun, one rank per GPU) every rank solves its own right-hand
+sides on its own copy of the operator (replicas: the north star forbids
+sharding the solve); value = solves of all ranks / max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "implicit-step solves/s at 1e-10 residual, learned+mixed vs plain FP64 (1 B200)"
+WORKLOADS = {
+    "d4": dict(d=4, level=7, terms=4, dt=1e-3, nu=0.1, kind="advdiff"),
+    "d5": dict(d=5, level=7, terms=4, dt=1e-3, nu=0.1, kind="advdiff"),
+    "d6": dict(d=6, level=7, terms=6, dt=5e-4, nu=0.1, kind="advdiff"),
+    "d3": dict(d=3, level=7, terms=3, dt=1e-3, nu=0.1, kind="advdiff"),
+}
+RESTART = 50
+TOL = 1e-10
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
+    ap.add_argument("--workload", default="d4", choices=sorted(WORKLOADS))
+    ap.add_argument("--plain-steps", type=int, default=2)
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons (every 200 ms)."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        sm.sort()
+        med = sm[len(sm) // 2] if sm else None
+        return {"sm_mhz": med, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup(args):
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    elif torch.cuda.is_available():
+        torch.cuda.set_device(0)
+    return world, rank, local
+
+
+def barrier(world):
+    import torch
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    torch.cuda.synchronize()
+
+
+def max_over_ranks(v, world):
+    import torch
+    if world == 1:
+        return v
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t.item()
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except OSError:
+        return {}
+
+
+# ---------------------------------------------------------------- reference arm
+
+def reference_arm(args):
+    """The reference's own CPU path (compiled from source into oracle/_ref):
+    kronmult_matrix<double>::apply on the CPU sparse format, all host
+    threads.  Each step times one full-operator apply and converts it to
+    solves/s with the iteration count of the reference GMRES algorithm on this
+    workload (measured once by the compiled reference at a reduced level and
+    recorded in the line)."""
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import numpy as np
+    import oracle
+    if not oracle.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "reference library oracle/_ref/libasgard_ref.so was not built"}))
+        return
+    R = oracle.ref()
+    cfg = WORKLOADS[args.workload]
+    from asgard_b200 import operators as ops
+    d, L, T = cfg["d"], cfg["level"], cfg["terms"]
+    table = ops.sparse_grid(d, L)
+    row_ptr, col, conn = ops.build_pairs(d, L, table)
+    vA = ops.factor_values(d, L, T, cfg["kind"], cfg["nu"])
+    iA = ops.expand_iA(conn, d, 3, T)
+    pntr = row_ptr.astype(np.int32)
+    rows = len(pntr) - 1
+    N = rows * 3 ** d
+    x = np.random.default_rng(0).uniform(-1, 1, N)
+    y = np.zeros(N)
+    iters = _plain_iterations(args.workload)
+    times = []
+    for s in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        oracle.kronmult(d, 3, pntr, col, T, iA, vA, -cfg["dt"], x, 0.0, y, lib=R)
+        dt = time.perf_counter() - t0
+        if s >= args.warmup:
+            times.append(dt)
+    t_apply = sorted(times)[len(times) // 2]
+    value = 1.0 / (t_apply * iters)
+    cores = R.ref_num_threads()
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value,
+        "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_apply * iters * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic",
+        "config": _config(args.workload),
+        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": cores,
+                         "kind": "reference",
+                         "sample": f"{args.steps} full-operator applies of the reference "
+                                   f"kronmult_matrix<double> (cpu_sparse, OpenMP {cores} threads); "
+                                   f"solves/s = 1/(median apply time x {iters} GMRES iterations)"},
+        "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+        "apply_s": t_apply, "gmres_iterations": iters,
+    }
+    print(json.dumps(line))
+
+
+# Iterations of the reference GMRES algorithm (restart 50, FP64, relative
+# 1e-10) on each workload, as measured by this framework's plain FP64 solver
+# (same algorithm); used to turn a CPU apply time into solves/s.
+_ITERS_CACHE = os.path.join(ROOT, "profiles", "plain_gmres_iterations.json")
+
+
+def _plain_iterations(workload):
+    try:
+        with open(_ITERS_CACHE) as f:
+            return int(json.load(f)[workload])
+    except (OSError, KeyError, ValueError):
+        return {"d4": 400, "d5": 400, "d6": 400, "d3": 300}[workload]
+
+
+def _config(workload):
+    cfg = WORKLOADS[workload]
+    return {"workload": f"d={cfg['d']} n=3 level {cfg['level']} sparse grid, "
+                        f"{cfg['terms']} advection/diffusion terms (nu={cfg['nu']}), "
+                        f"dt={cfg['dt']}, GMRES restart {RESTART}, rel tol {TOL}",
+            "d": cfg["d"], "n": 3, "level": cfg["level"], "terms": cfg["terms"],
+            "dt": cfg["dt"], "restart": RESTART, "tol": TOL,
+            "l2": "operator data (pair list + indices) larger than L2; no flush"}
+
+
+# ---------------------------------------------------------------- our arm
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return reference_arm(args)
+    import numpy as np
+    import torch
+    import asgard_b200 as ab
+
+    world, rank, local = dist_setup(args)
+    cfg = WORKLOADS[args.workload]
+    d, L, T, dt = cfg["d"], cfg["level"], cfg["terms"], cfg["dt"]
+    op = ab.SparseGridOperator(d, L, T, kind=cfg["kind"], nu=cfg["nu"])
+    mat = op.kronmult_matrix()
+    N = op.N
+    gen = torch.Generator(device="cuda").manual_seed(1000 + rank)
+    nb = args.warmup + args.steps
+    B = [torch.rand(N, dtype=torch.float64, device="cuda", generator=gen) * 2 - 1
+         for _ in range(max(nb, args.plain_steps + 1))]
+    method = dict(precision="fp32", precond=None, name="fp32-ir")
+
+    def solve(b, precision, precond=None):
+        x = torch.zeros(N, dtype=torch.float64, device="cuda")
+        info = ab.simple_gmres_euler(dt, mat, x, b, RESTART, 200, TOL,
+                                     tol_mode="rel", precision=precision,
+                                     precond=precond)
+        return x, info
+
+    # warm-up (method and plain)
+    infos = []
+    for i in range(args.warmup):
+        _, info = solve(B[i], method["precision"], method["precond"])
+        infos.append(info)
+    _, pinfo = solve(B[0], "fp64")
+
+    # ---- timed: the method
+    launches0 = ab.launch_count()
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier(world)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    minfos = []
+    for i in range(args.steps):
+        _, info = solve(B[args.warmup + i], method["precision"], method["precond"])
+        minfos.append(info)
+    e1.record()
+    barrier(world)
+    clk = clocks.stop()
+    launches = ab.launch_count() - launches0
+    t_method = max_over_ranks(e0.elapsed_time(e1) / 1e3, world)
+    value = world * args.steps / t_method
+
+    # ---- timed: plain FP64 GMRES with the FP64 kronmult
+    barrier(world)
+    e0.record()
+    pinfos = []
+    for i in range(args.plain_steps):
+        _, info = solve(B[i], "fp64")
+        pinfos.append(info)
+    e1.record()
+    barrier(world)
+    t_plain = max_over_ranks(e0.elapsed_time(e1) / 1e3, world)
+    plain_value = world * args.plain_steps / t_plain
+
+    # ---- roofline: the dominant kernel (FP64 kronmult, and the FP32 one
+    # used inside the method), average launch duration by CUDA events
+    xs = B[0]
+    ys = torch.zeros_like(xs)
+    flops = op.flops()
+    reps = 5
+
+    def time_apply(precision):
+        mat.apply_euler(dt, 1.0, xs, 0.0, ys, precision=precision)
+        torch.cuda.synchronize()
+        a0 = torch.cuda.Event(enable_timing=True)
+        a1 = torch.cuda.Event(enable_timing=True)
+        a0.record()
+        for _ in range(reps):
+            mat.apply_euler(dt, 1.0, xs, 0.0, ys, precision=precision)
+        a1.record()
+        torch.cuda.synchronize()
+        return a0.elapsed_time(a1) / 1e3 / reps
+
+    t64 = time_apply("fp64")
+    t32 = time_apply("fp32")
+    fp64_peak = ab._lib.C.c_double()
+    ab.lib.asgk_measure_fma_peak(0, ab._lib.C.byref(fp64_peak))
+    fp32_peak = ab._lib.C.c_double()
+    ab.lib.asgk_measure_fma_peak(1, ab._lib.C.byref(fp32_peak))
+
+    # ---- e2e through the public API with host buffers
+    e2e_value = None
+    hb = torch.empty(N, dtype=torch.float64, pin_memory=True)
+    hx = torch.empty(N, dtype=torch.float64, pin_memory=True)
+    hb.copy_(B[0].cpu())
+    barrier(world)
+    e0.record()
+    for i in range(args.e2e_steps):
+        bd = hb.to("cuda", non_blocking=True)
+        x, _ = solve(bd, method["precision"], method["precond"])
+        hx.copy_(x, non_blocking=True)
+    e1.record()
+    barrier(world)
+    t_e2e = max_over_ranks(e0.elapsed_time(e1) / 1e3, world)
+    e2e_value = world * args.e2e_steps / t_e2e
+
+    # ---- CPU baseline (rank 0, N = 1): the reference compiled from source
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(op, cfg, pinfo.iterations)
+
+    if rank == 0:
+        os.makedirs(os.path.join(ROOT, "profiles"), exist_ok=True)
+        achieved = flops / t64 / 1e12
+        line = {
+            "metric": METRIC, "value": value, "unit": "solves/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": t_method / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic",
+            "config": dict(_config(args.workload), method=method["name"],
+                           parallelism=f"replicas x{world}"),
+            "plain_fp64": {"value": plain_value, "unit": "solves/s",
+                           "iterations": pinfo.iterations,
+                           "true_relres": max(i.true_relres for i in pinfos),
+                           "ms_per_solve": t_plain / args.plain_steps * 1e3},
+            "method": {"iterations": [i.iterations for i in minfos],
+                       "true_relres": max(i.true_relres for i in minfos),
+                       "outer_steps": minfos[0].outer_steps,
+                       "matvecs_low": minfos[0].matvecs_low,
+                       "matvecs_fp64": minfos[0].matvecs_fp64,
+                       "speedup_vs_plain": value / plain_value},
+            "clocks": clk,
+            "e2e": {"value": e2e_value, "unit": "solves/s",
+                    "h2d_bytes_per_step": N * 8, "d2h_bytes_per_step": N * 8},
+            "gpu_launches": launches,
+            "roofline": {"bound": "fp64", "kernel": "kron3_rows<d=4, fp64>",
+                         "achieved": achieved, "peak": fp64_peak.value,
+                         "peak_source": "measured live (FMA chain kernel)",
+                         "unit": "TFLOP/s", "frac": achieved / fp64_peak.value,
+                         "traffic": None,
+                         "ms_per_launch": t64 * 1e3,
+                         "flops_per_launch": flops,
+                         "fp32_kernel": {"ms_per_launch": t32 * 1e3,
+                                         "achieved": flops / t32 / 1e12,
+                                         "peak": fp32_peak.value,
+                                         "frac": flops / t32 / 1e12 / fp32_peak.value}},
+            "cpu_baseline": cpu,
+        }
+        with open(_ITERS_CACHE + ".new", "w") as f:
+            json.dump({args.workload: pinfo.iterations}, f)
+        print(json.dumps(line))
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def cpu_baseline(op, cfg, iters):
+    """Reference kronmult_matrix::apply on the host cores (bounded sample)."""
+    import numpy as np
+    import oracle
+    if not oracle.ref_available():
+        return {"value": None, "unit": "solves/s", "cores": 0, "kind": "reference",
+                "sample": "reference library not built"}
+    R = oracle.ref()
+    iA = op.iA()
+    pntr = op.row_ptr.astype(np.int32)
+    x = np.random.default_rng(0).uniform(-1, 1, op.N)
+    y = np.zeros(op.N)
+    t0 = time.perf_counter()
+    oracle.kronmult(op.d, 3, pntr, op.col, op.terms, iA, op.vA, -cfg["dt"], x,
+                    0.0, y, lib=R)
+    t_apply = time.perf_counter() - t0
+    cores = R.ref_num_threads()
+    return {"value": 1.0 / (t_apply * iters), "unit": "solves/s",
+            "cores": cores, "kind": "reference",
+            "sample": f"1 full-operator apply of the reference cpu_sparse kronmult "
+                      f"({t_apply:.2f} s, {cores} OpenMP threads) x {iters} GMRES iterations",
+            "apply_s": t_apply}
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,204 @@
+/* asgard_b200 -- C ABI of the B200 (sm_100a) kronmult operator and the
+ * implicit backward-Euler GMRES solve it feeds.
+ *
+ * Plain pointers and sizes only; every entry point returns an asgk_status
+ * (0 = success) and never throws.  Device pointers are CUDA global-memory
+ * pointers on the current device; "host" pointers are ordinary host memory.
+ * A plan is not re-entrant: one call at a time per plan, as with the
+ * reference's kronmult_matrix::apply, which is documented "not thread-safe"
+ * (src/asgard_kronmult_matrix.hpp:336).  Calls are stream-ordered on the
+ * stream argument (0 = the legacy default stream).
+ *
+ * Conventions shared with the reference (src/device/asgard_kronmult.hpp):
+ *   - a Kronecker product acts on tensors of n^d entries stored contiguously,
+ *     dimension 0 slowest;
+ *   - the d factors of one product are column-major n x n blocks inside vA,
+ *     addressed by iA offsets, the first offset applying to dimension 0;
+ *   - y = beta*y + alpha * sum_{pairs (row,col)} sum_{terms}
+ *           (A_{t,0} (x) ... (x) A_{t,d-1}) x_col, with beta = 0 overwriting y.
+ */
+#ifndef ASGARD_B200_H
+#define ASGARD_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct asgk_plan asgk_plan;
+typedef struct asgk_mlp asgk_mlp;
+typedef void *asgk_stream; /* a cudaStream_t */
+
+typedef enum asgk_status
+{
+  ASGK_OK              = 0,
+  ASGK_ERR_INVALID     = 1, /* bad argument (size, pointer, index) */
+  ASGK_ERR_UNSUPPORTED = 2, /* (d, n) outside the supported range */
+  ASGK_ERR_CUDA        = 3, /* a CUDA runtime call failed */
+  ASGK_ERR_ALLOC       = 4, /* device or host allocation failed */
+  ASGK_ERR_BREAKDOWN   = 5, /* GMRES: zero or non-finite Arnoldi norm */
+  ASGK_ERR_NOT_CONVERGED = 6, /* GMRES: iteration limit before tolerance */
+  ASGK_ERR_NONFINITE   = 7  /* non-finite residual (NaN/Inf in the data) */
+} asgk_status;
+
+typedef enum asgk_precision
+{
+  ASGK_FP64 = 0, /* FP64 loads, FP64 arithmetic */
+  ASGK_FP32 = 1, /* FP64 vectors, FP32 factors and FP32 arithmetic */
+  ASGK_BF16 = 2  /* FP64 vectors, BF16 tensor-core products, FP32 accumulation */
+} asgk_precision;
+
+/* ---------------------------------------------------------------- plans */
+
+/* Replaces kronmult_matrix<P>'s sparse constructors
+ * (src/asgard_kronmult_matrix.hpp:235-297, CPU one-call and multi-call forms)
+ * and the buffers make_kronmult_sparse uploads
+ * (src/asgard_kronmult_matrix.cpp:639-643).
+ *
+ * row_ptr[num_rows+1], col_indx[nnz]: pairs in CSR form over output cells
+ *   (the reference's CPU format); col_indx are cell indices < num_cols.
+ * iA[nnz*num_terms*d]: offsets into vA of the n x n factors, pair-major then
+ *   term then dimension (reference layout).
+ * vA[vA_len]: factor values (FP64, host).
+ * All arrays are host arrays and are copied; the plan owns device copies.
+ * Offsets are checked against vA_len (ASGK_ERR_INVALID if out of range). */
+int asgk_plan_create(asgk_plan **plan, int d, int n, int num_rows,
+                     int num_cols, int num_terms, const int64_t *row_ptr,
+                     const int *col_indx, const int *iA, const double *vA,
+                     int64_t vA_len);
+
+/* Same operator from the reference's GPU pair format (kronmult::gpu_sparse,
+ * src/device/asgard_kronmult.hpp:113-133): per pair the tensor offsets
+ * iy[i] (into y) and ix[i] (into x), both multiples of n^d, any order.
+ * Pairs are grouped by output cell inside the plan. */
+int asgk_plan_create_pairs(asgk_plan **plan, int d, int n, int num_rows,
+                           int num_cols, int num_terms, int64_t num_batch,
+                           const int *iy, const int *ix, const int *iA,
+                           const double *vA, int64_t vA_len);
+
+/* Sparse-grid form used by the builder below: per pair the d 1D connection
+ * indices conn[nnz*d]; factor (t, k) of a pair is the n x n block at
+ * vA + conn[k]*(d*T*n*n) + (t*d + k)*n*n (the layout make_kronmult_sparse
+ * writes, src/asgard_kronmult_matrix.cpp:369-393, 455-461) -- this stores
+ * d indices per pair instead of d*T. */
+int asgk_plan_create_conn(asgk_plan **plan, int d, int n, int num_rows,
+                          int num_cols, int num_terms, const int64_t *row_ptr,
+                          const int *col_indx, const int *conn,
+                          const double *vA, int64_t vA_len);
+
+void asgk_plan_destroy(asgk_plan *plan);
+
+/* Replaces update_stored_coefficients (src/asgard_kronmult_matrix.hpp:515-532). */
+int asgk_plan_update_values(asgk_plan *plan, const double *vA, int64_t vA_len);
+
+/* Sizes: tensor_size = n^d, input_size = num_cols*n^d,
+ * output_size = num_rows*n^d, num_batch = nnz, flops = 2*d*T*n^(d+1)*nnz
+ * (compute_flops, src/asgard_kronmult_matrix.hpp:507-512). */
+int asgk_plan_info(const asgk_plan *plan, int64_t *num_batch,
+                   int64_t *input_size, int64_t *output_size,
+                   int64_t *flops, int64_t *device_bytes);
+
+/* ---------------------------------------------------------------- apply */
+
+/* y = beta*y + alpha*K*x on device pointers
+ * (kronmult_matrix<P>::apply<resource::device>, src/asgard_kronmult_matrix.hpp:340-478).
+ * precision selects the arithmetic; x and y are FP64. */
+int asgk_apply(asgk_plan *plan, int precision, double alpha, const double *x,
+               double beta, double *y, asgk_stream stream);
+
+/* FP32 vectors: y = beta*y + alpha*K*x with FP32 x, y and arithmetic
+ * (kronmult_matrix<float>::apply<resource::device>). */
+int asgk_apply_f32(asgk_plan *plan, float alpha, const float *x, float beta,
+                   float *y, asgk_stream stream);
+
+/* Host pointers: copies x (and y when beta != 0) to the plan's device
+ * workspace, applies in FP64 and copies y back, synchronising the stream
+ * (kronmult_matrix<P>::apply<resource::host> on a CUDA build,
+ * src/asgard_kronmult_matrix.hpp:351-358, 451-452). */
+int asgk_apply_host(asgk_plan *plan, double alpha, const double *x,
+                    double beta, double *y, asgk_stream stream);
+
+/* The backward-Euler operator of simple_gmres_euler (src/solver.cpp:119-135)
+ * fused into one pass: y = beta*y + alpha*(x - dt*K*x).  Square plans only. */
+int asgk_apply_euler(asgk_plan *plan, int precision, double dt, double alpha,
+                     const double *x, double beta, double *y,
+                     asgk_stream stream);
+
+/* ---------------------------------------------------------------- GMRES */
+
+typedef struct asgk_gmres_info
+{
+  double error;       /* final residual estimate (as the reference reports) */
+  int iterations;     /* reference count: 1 per restart + 1 per Arnoldi step */
+  int status;         /* asgk_status of the solve */
+  double true_relres; /* ||b - (I - dt K) x||_2 / ||b||_2 recomputed in FP64 */
+  int outer_steps;    /* refinement steps (mixed precision), else restarts */
+  int matvecs_low;    /* low-precision operator applications */
+  int matvecs_fp64;   /* FP64 operator applications */
+  int precond_calls;  /* preconditioner applications */
+  int fallback;       /* 1 if the learned preconditioner was dropped */
+} asgk_gmres_info;
+
+typedef enum asgk_tol_mode
+{
+  ASGK_TOL_ABS = 0, /* reference semantics: |s_k g_k| <= tol (src/solver.cpp:258-259) */
+  ASGK_TOL_REL = 1  /* residual <= tol * ||b||_2 */
+} asgk_tol_mode;
+
+/* Solves (I - dt*K) x = b on device vectors, x holding the initial guess.
+ * Replaces solver::simple_gmres_euler (src/solver.hpp:34-40,
+ * src/solver.cpp:119-135 and the template :157-298) with a device-resident
+ * GMRES: classical Gram-Schmidt, Givens rotations, packed Hessenberg.
+ *
+ * precision = ASGK_FP64 is the reference algorithm.  ASGK_FP32/ASGK_BF16 run
+ * the Krylov operator in that arithmetic inside FP64 iterative refinement
+ * (outer FP64 residuals; FP64 Gram-Schmidt, norms and least squares), until
+ * the FP64 residual meets tol.
+ * precond: a learned preconditioner (asgk_mlp) applied on the right through
+ * flexible GMRES, or NULL.  restart <= 0 selects default_gmres_restarts
+ * (src/solver.cpp:142-152); max_outer <= 0 selects n. */
+int asgk_gmres_euler(asgk_plan *plan, double dt, double *x, const double *b,
+                     int restart, int max_outer, double tol, int tol_mode,
+                     int precision, asgk_mlp *precond, asgk_gmres_info *info,
+                     asgk_stream stream);
+
+/* solver::simple_gmres on a dense column-major n x n host matrix (the test
+ * path of src/solver.cpp:55-74, without the LU preconditioner). */
+int asgk_gmres_dense(int n, const double *A, double *x, const double *b,
+                     int restart, int max_outer, double tol,
+                     asgk_gmres_info *info);
+
+/* default_gmres_restarts<double>(n) (src/solver.cpp:142-152). */
+int asgk_default_gmres_restarts(int64_t n);
+
+/* ------------------------------------------------------- sparse grids */
+
+/* Host-side builder of the reference's sparse-grid operator structure:
+ * element table (src/elements.cpp:248-351), 1D connectivity (connect_1d,
+ * src/asgard_grid_1d.hpp) and connected cell pairs (check_connected,
+ * src/asgard_kronmult_matrix.cpp:230-300).  Two-call: pass NULL arrays to get
+ * the sizes. */
+int64_t asgk_sparse_grid(int d, int level, int *table);
+int asgk_connect_1d(int level, int *num_rows, int *num_conn, int *pntr,
+                    int *indx);
+int asgk_build_pairs(int d, int level, int num_cells, const int *table,
+                     int64_t *nnz, int64_t *row_ptr, int *col_indx,
+                     int *conn);
+
+/* ------------------------------------------------------------ misc */
+
+const char *asgk_status_string(int status);
+/* Number of kernels this library launched since load (for launch counts). */
+int64_t asgk_launch_count(void);
+/* Measured FMA throughput (TFLOP/s, 2 flops per FMA) of the current device
+ * for precision ASGK_FP64 or ASGK_FP32: the denominator of the roofline of the
+ * CUDA-core kronmult kernels.  No counterpart in the reference. */
+int asgk_measure_fma_peak(int precision, double *tflops);
+/* Device properties (SM count etc.) for the current device. */
+int asgk_device_info(int *sm_count, int *cc_major, int *cc_minor);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ASGARD_B200_H */

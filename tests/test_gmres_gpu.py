@@ -1,0 +1,114 @@
+"""Device-resident GMRES through the C ABI against the oracle and the
+reference's known answers."""
+import json
+
+import numpy as np
+import pytest
+
+import oracle
+from conftest import golden, rel_err, rmse_close
+
+pytestmark = pytest.mark.gpu
+
+
+def to_dev(a):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64)).cuda()
+
+
+def test_gmres_known_answers(cuda):
+    """The 3x3 systems of src/solver_tests.cpp:141-213 (no preconditioner):
+    error below machine epsilon, x equal to the gold answer."""
+    import asgard_b200 as ab
+    case = json.load(open(golden("gmres_3x3.json")))
+    A = np.array(case["A"])
+    eps = np.finfo(np.float64).eps
+    for k in ("1", "2"):
+        x = np.zeros(3)
+        info = ab.simple_gmres(A, x, np.array(case["b" + k]), None, 3, 3, eps)
+        assert info.error < eps
+        assert info.iterations == case["ref_iters" + k]
+        assert rmse_close(x, case["x" + k], 10 * eps)
+
+
+@pytest.mark.parametrize("name", ["continuity_2_L4", "continuity_3_L3", "diffusion_2_L3"])
+def test_gmres_euler_reference_pdes(cuda, name):
+    """simple_gmres_euler on reference-built operators: the reference's answer
+    (restart 20, 50 restarts, absolute tolerance 1e-12), same iteration count
+    as the reference up to one step."""
+    import asgard_b200 as ab
+    import torch
+    z = np.load(golden(f"pde_{name}.npz"))
+    d, n, terms = int(z["d"]), int(z["n"]), int(z["terms"])
+    rows = len(z["pntr"]) - 1
+    N = rows * n ** d
+    rng = np.random.default_rng(7)
+    rng.uniform(-1, 1, N)
+    rng.uniform(-1, 1, N)
+    b = rng.uniform(-1, 1, N)
+    mat = ab.kronmult_matrix.from_csr(d, n, rows, rows, terms, z["pntr"],
+                                      z["indx"], z["iA"], z["vA"])
+    x = torch.zeros(N, dtype=torch.float64, device="cuda")
+    info = ab.simple_gmres_euler(float(z["dt"]), mat, x, to_dev(b), 20, 50, 1e-12)
+    assert info.status == 0
+    assert info.error <= 1e-12
+    assert abs(info.iterations - int(z["gmres_iters"])) <= 1
+    xs = x.cpu().numpy()
+    assert rel_err(xs, z["gmres_x"]) < 1e-10
+    assert info.true_relres < 1e-11
+
+
+def test_gmres_euler_matches_oracle_iterations(cuda):
+    """Synthetic advection/diffusion operator, reference (absolute) criterion:
+    the oracle's restarted GMRES and the device GMRES agree."""
+    import asgard_b200 as ab
+    import torch
+    op = ab.SparseGridOperator(2, 6, 2, kind="advdiff", nu=0.1)
+    b = np.random.default_rng(11).uniform(-1, 1, op.N)
+    xo = np.zeros(op.N)
+    err_o, its_o = oracle.gmres_euler(2, 3, op.row_ptr.astype(np.int32), op.col,
+                                      2, op.iA(), op.vA, 1e-3, xo, b, 30, 40, 1e-9)
+    x = torch.zeros(op.N, dtype=torch.float64, device="cuda")
+    info = ab.simple_gmres_euler(1e-3, op.kronmult_matrix(), x, to_dev(b), 30, 40, 1e-9)
+    assert info.status == 0
+    assert abs(info.iterations - its_o) <= 2
+    assert rel_err(x.cpu().numpy(), xo) < 1e-8
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_gmres_relative_tolerance_true_residual(cuda, precision):
+    """1e-10 relative residual, checked in FP64; the FP32 operator runs inside
+    FP64 iterative refinement."""
+    import asgard_b200 as ab
+    import torch
+    op = ab.SparseGridOperator(3, 5, 3, kind="advdiff", nu=0.1)
+    b = to_dev(np.random.default_rng(4).uniform(-1, 1, op.N))
+    x = torch.zeros(op.N, dtype=torch.float64, device="cuda")
+    info = ab.simple_gmres_euler(1e-3, op.kronmult_matrix(), x, b, 50, 100,
+                                 1e-10, tol_mode="rel", precision=precision)
+    assert info.status == 0
+    assert info.true_relres <= 1e-10
+    if precision == "fp32":
+        assert info.matvecs_low > 0 and info.outer_steps >= 2
+
+
+def test_gmres_restart_larger_than_system(cuda):
+    import asgard_b200 as ab
+    import torch
+    op = ab.SparseGridOperator(1, 2, 1, kind="random")
+    x = torch.zeros(op.N, dtype=torch.float64, device="cuda")
+    with pytest.raises(ValueError):
+        ab.simple_gmres_euler(1e-3, op.kronmult_matrix(), x, x.clone(), op.N + 1, 1, 1e-10)
+
+
+def test_gmres_nonfinite_input_reports_status(cuda):
+    """A NaN planted in b (host-side fault injection) ends the solve with a
+    non-finite status instead of iterating on garbage."""
+    import asgard_b200 as ab
+    import torch
+    op = ab.SparseGridOperator(2, 4, 2, kind="advdiff")
+    b = np.random.default_rng(0).uniform(-1, 1, op.N)
+    b[5] = np.nan
+    x = torch.zeros(op.N, dtype=torch.float64, device="cuda")
+    info = ab.simple_gmres_euler(1e-3, op.kronmult_matrix(), x, to_dev(b), 10, 5, 1e-10)
+    assert info.status == 7  # ASGK_ERR_NONFINITE

@@ -1,0 +1,111 @@
+"""CPU-side checks of the product library: it loads, exports every symbol the
+C header declares, and its host-side sparse-grid builder reproduces the
+reference builder (golden fixtures) and the oracle."""
+import os
+import re
+
+import numpy as np
+import pytest
+
+import oracle
+from conftest import ROOT, golden
+
+
+def header_symbols():
+    text = open(os.path.join(ROOT, "include", "asgard_b200.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(asgk_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    import asgard_b200
+    syms = header_symbols()
+    assert len(syms) >= 15
+    missing = [s for s in syms if not hasattr(asgard_b200.lib, s)]
+    assert not missing, missing
+
+
+@pytest.mark.parametrize("name", ["continuity_2_L4", "continuity_3_L3",
+                                  "continuity_6_L2", "diffusion_2_L3"])
+def test_builder_matches_reference_builder(name):
+    import asgard_b200 as ab
+    z = np.load(golden(f"pde_{name}.npz"))
+    d, n, L, terms = int(z["d"]), int(z["n"]), int(z["level"]), int(z["terms"])
+    table = ab.sparse_grid(d, L)
+    assert np.array_equal(table, z["table"])
+    row_ptr, col, conn = ab.build_pairs(d, L, table)
+    assert np.array_equal(row_ptr, z["pntr"].astype(np.int64))
+    assert np.array_equal(col, z["indx"])
+    assert np.array_equal(ab.expand_iA(conn, d, n, terms), z["iA"])
+
+
+@pytest.mark.parametrize("d,L", [(1, 7), (2, 6), (3, 5), (4, 5), (5, 4), (6, 3)])
+def test_builder_matches_oracle(d, L):
+    import asgard_b200 as ab
+    t1 = ab.sparse_grid(d, L)
+    t2 = oracle.sparse_grid(d, L)
+    assert np.array_equal(t1, t2)
+    r1, c1, k1 = ab.build_pairs(d, L, t1)
+    r2, c2, k2 = oracle.build_pairs(d, L, t2)
+    assert np.array_equal(r1, r2.astype(np.int64))
+    assert np.array_equal(c1, c2)
+    assert np.array_equal(k1, k2)
+
+
+def test_connect_1d_matches_oracle():
+    import asgard_b200 as ab
+    for L in range(0, 10):
+        p1, i1 = ab.connect_1d(L)
+        if L == 0:
+            assert len(p1) == 2
+            continue
+        p2, i2 = oracle.connect_1d(L)
+        assert np.array_equal(p1, p2) and np.array_equal(i1, i2)
+
+
+def test_sparse_grid_sizes():
+    """Cell and pair counts of the benchmark grids (n = 3)."""
+    import asgard_b200 as ab
+    assert ab.sparse_grid(2, 6).shape[0] == 256
+    assert ab.sparse_grid(4, 7).shape[0] == 4048
+    assert ab.sparse_grid(5, 7).shape[0] == 8472
+    assert ab.sparse_grid(6, 7).shape[0] == 16172
+    r, c, k = ab.build_pairs(2, 6, ab.sparse_grid(2, 6))
+    assert len(c) == 38512
+
+
+def test_advdiff_factors_use_reference_blocks():
+    """Level-7 advection/diffusion factors equal the stored reference blocks."""
+    import asgard_b200 as ab
+    vA = ab.factor_values(2, 7, 2, "advdiff", nu=0.1).reshape(-1, 2, 2, 9)
+    ops = ab.operators.ops1d()
+    assert np.array_equal(vA[:, 0, 0], ops["adv"])
+    assert np.allclose(vA[:, 1, 1], 0.1 * ops["dif"], rtol=0, atol=0)
+    pntr, indx = ab.connect_1d(7)
+    rows = np.repeat(np.arange(len(pntr) - 1), np.diff(pntr))
+    diag = rows == indx
+    assert np.array_equal(vA[diag, 0, 1], np.tile(np.eye(3).ravel(), (diag.sum(), 1)))
+    assert not vA[~diag, 0, 1].any()
+
+
+def test_invalid_plans_are_rejected():
+    import asgard_b200 as ab
+    from asgard_b200._lib import AsgkError
+    # column out of range, factor offset out of range, bad dimension
+    with pytest.raises(AsgkError):
+        ab.kronmult_matrix.from_csr(2, 2, 1, 1, 1, [0, 1], [1], [0, 0], np.zeros(4))
+    with pytest.raises(AsgkError):
+        ab.kronmult_matrix.from_csr(2, 2, 1, 1, 1, [0, 1], [0], [0, 1], np.zeros(4))
+    with pytest.raises(AsgkError):
+        ab.kronmult_matrix.from_csr(7, 2, 1, 1, 1, [0, 1], [0], [0] * 7, np.zeros(4))
+    with pytest.raises(AsgkError):
+        ab.kronmult_matrix.from_pairs(2, 2, 1, 1, 1, [1], [0], [0, 0], np.zeros(4))
+
+
+def test_default_gmres_restarts():
+    """default_gmres_restarts (src/solver.cpp:142-152)."""
+    import asgard_b200 as ab
+    assert ab.default_gmres_restarts(5) == 5
+    assert ab.default_gmres_restarts(1000) == 200
+    n = 11789388
+    assert ab.default_gmres_restarts(n) == max(10, min(200, int(512 / (n * 8 / 1048576))))

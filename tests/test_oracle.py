@@ -1,0 +1,157 @@
+"""Pins the C restatement (oracle/) against the reference: golden fixtures made
+by the reference itself, and the reference library when it was built here."""
+import hashlib
+import json
+
+import numpy as np
+import pytest
+
+import oracle
+from conftest import golden, rmse_close
+
+KRON = np.load(golden("kronmult_data.npz"))
+
+
+def kron_keys():
+    out = []
+    for k in KRON.files:
+        if k.endswith("_ref_y"):
+            tag, d, n, rows, terms, mats = k[:-len("_ref_y")].split("_")
+            out.append((tag, int(d), int(n), int(rows), int(terms), int(mats)))
+    return sorted(out)
+
+
+@pytest.mark.parametrize("tag,d,n,rows,terms,mats", kron_keys())
+def test_oracle_kronmult_reference_test_data(tag, d, n, rows, terms, mats):
+    """make_kronmult_data (minstd_rand(42)) regenerated bit-exactly, and the
+    oracle's pair kronmult against the reference's explicit Kronecker answer
+    (src/asgard_kronmult_matrix_tests.cpp:14-118, 100 ulp rmse)."""
+    dt = np.float64 if tag == "f64" else np.float32
+    data = oracle.make_kronmult_data(d, n, rows, terms, mats, dt)
+    key = f"{tag}_{d}_{n}_{rows}_{terms}_{mats}"
+    h = hashlib.sha256()
+    for a in (data["iA"], data["vA"], data["x"], data["y"]):
+        h.update(np.ascontiguousarray(a).tobytes())
+    assert h.hexdigest() == bytes(KRON[key + "_inputs_sha256"]).decode()
+    y = data["y"].copy()
+    oracle.kronmult(d, n, data["pntr"], data["indx"], terms, data["iA"],
+                    data["vA"], 1.0, data["x"], 1.0, y)
+    eps = np.finfo(dt).eps
+    assert rmse_close(y, KRON[key + "_ref_y"], 100 * eps)
+
+
+PDES = ["continuity_2_L4", "continuity_3_L3", "continuity_6_L2", "diffusion_2_L3"]
+
+
+@pytest.mark.parametrize("name", PDES)
+def test_oracle_builder_matches_reference_builder(name):
+    """Element table, pair list, iA of the reference's make_kronmult_sparse."""
+    z = np.load(golden(f"pde_{name}.npz"))
+    d, n, L, terms = int(z["d"]), int(z["n"]), int(z["level"]), int(z["terms"])
+    table = oracle.sparse_grid(d, L)
+    assert np.array_equal(table, z["table"])
+    pntr, indx, conn = oracle.build_pairs(d, L, table)
+    assert np.array_equal(pntr, z["pntr"])
+    assert np.array_equal(indx, z["indx"])
+    assert np.array_equal(oracle.expand_iA(d, n, terms, conn), z["iA"])
+
+
+@pytest.mark.parametrize("name", PDES)
+def test_oracle_apply_matches_reference_apply(name):
+    z = np.load(golden(f"pde_{name}.npz"))
+    d, n, terms = int(z["d"]), int(z["n"]), int(z["terms"])
+    N = (len(z["pntr"]) - 1) * n ** d
+    rng = np.random.default_rng(7)
+    x = rng.uniform(-1, 1, N)
+    y0 = rng.uniform(-1, 1, N)
+    y = oracle.kronmult(d, n, z["pntr"], z["indx"], terms, z["iA"], z["vA"],
+                        1.0, x, 0.0, np.zeros(N))
+    assert np.array_equal(y, z["y"])  # same summation order: bit-exact
+    y2 = oracle.kronmult(d, n, z["pntr"], z["indx"], terms, z["iA"], z["vA"],
+                         -0.5, x, 2.0, y0.copy())
+    assert np.array_equal(y2, z["y_ab"])
+
+
+@pytest.mark.parametrize("name", ["continuity_2_L4", "continuity_3_L3", "diffusion_2_L3"])
+def test_oracle_gmres_euler_matches_reference(name):
+    """simple_gmres_euler: same iteration count, solution to 1e-12."""
+    z = np.load(golden(f"pde_{name}.npz"))
+    d, n, terms = int(z["d"]), int(z["n"]), int(z["terms"])
+    N = (len(z["pntr"]) - 1) * n ** d
+    rng = np.random.default_rng(7)
+    rng.uniform(-1, 1, N)
+    rng.uniform(-1, 1, N)
+    b = rng.uniform(-1, 1, N)
+    x = np.zeros(N)
+    err, its = oracle.gmres_euler(d, n, z["pntr"], z["indx"], terms, z["iA"],
+                                  z["vA"], float(z["dt"]), x, b, 20, 50, 1e-12)
+    assert its == int(z["gmres_iters"])
+    assert err <= 1e-12
+    assert np.linalg.norm(x - z["gmres_x"]) <= 1e-12 * max(1, np.linalg.norm(z["gmres_x"]))
+
+
+def test_oracle_gmres_known_answers():
+    """The 3x3 systems of src/solver_tests.cpp:141-213."""
+    case = json.load(open(golden("gmres_3x3.json")))
+    A = np.array(case["A"])
+    for k in ("1", "2"):
+        x = np.zeros(3)
+        err, its = oracle.gmres_dense(A, x, np.array(case["b" + k]), 3, 3,
+                                      np.finfo(np.float64).eps)
+        assert err < np.finfo(np.float64).eps
+        assert its == case["ref_iters" + k]
+        assert rmse_close(x, case["x" + k], 10 * np.finfo(np.float64).eps)
+        assert rmse_close(x, case["ref_x" + k], 10 * np.finfo(np.float64).eps)
+
+
+def test_oracle_kronecker_known_answers():
+    """Known-answer Kronecker products (src/asgard_kronmult_matrix_tests.cpp:178-193)."""
+    import ctypes as C
+    A = np.array([1, 2, 3, 4], dtype=np.float64)
+    B = np.array([10, 20, 30, 40], dtype=np.float64)
+    gold = [10, 20, 20, 40, 30, 40, 60, 80, 30, 60, 40, 80, 90, 120, 120, 160]
+    # K = A (x) B applied to unit vectors gives its columns
+    lib = oracle.oracle()
+    lib.orc_reference_kronmult_one.restype = None
+    K = np.zeros(16)
+    for c in range(4):
+        e = np.zeros(4)
+        e[c] = 1
+        y = np.zeros(4)
+        pa = (C.c_void_p * 2)(A.ctypes.data, B.ctypes.data)
+        lib.orc_reference_kronmult_one(2, 2, pa, e.ctypes.data_as(C.c_void_p),
+                                       y.ctypes.data_as(C.c_void_p))
+        K[c * 4:(c + 1) * 4] = y
+    assert np.array_equal(K, gold)
+
+
+@pytest.mark.skipif(not oracle.ref_available(), reason="reference not built here")
+def test_oracle_matches_compiled_reference():
+    """connect_1d for levels 1..9 and cpu_sparse on random data, bit-exact."""
+    R = oracle.ref()
+    for L in range(1, 10):
+        p1, i1 = oracle.connect_1d(L)
+        p2, i2 = oracle.connect_1d(L, lib=R)
+        assert np.array_equal(p1, p2) and np.array_equal(i1, i2)
+    for (d, n, rows, terms, mats) in [(2, 3, 12, 3, 7), (4, 3, 6, 2, 7), (6, 2, 5, 2, 7)]:
+        data = oracle.make_kronmult_data(d, n, rows, terms, mats)
+        y1 = data["y"].copy()
+        y2 = data["y"].copy()
+        oracle.kronmult(d, n, data["pntr"], data["indx"], terms, data["iA"],
+                        data["vA"], 0.7, data["x"], -1.0, y1)
+        oracle.kronmult(d, n, data["pntr"], data["indx"], terms, data["iA"],
+                        data["vA"], 0.7, data["x"], -1.0, y2, lib=R)
+        assert np.array_equal(y1, y2)
+
+
+def test_oracle_planted_mistake_is_caught():
+    """A wrong factor in the oracle's input must change the answer well above
+    the parity tolerance (guards against a vacuous comparison)."""
+    data = oracle.make_kronmult_data(3, 3, 6, 2, 7)
+    y1 = oracle.kronmult(3, 3, data["pntr"], data["indx"], 2, data["iA"],
+                         data["vA"], 1.0, data["x"], 0.0, np.zeros_like(data["y"]))
+    vA = data["vA"].copy()
+    vA[4] += 1e-6
+    y2 = oracle.kronmult(3, 3, data["pntr"], data["indx"], 2, data["iA"], vA,
+                         1.0, data["x"], 0.0, np.zeros_like(data["y"]))
+    assert np.linalg.norm(y1 - y2) / np.linalg.norm(y1) > 1e-9
