@@ -6,14 +6,14 @@ The compute path is the in-tree CUDA library ``libasgard_b200.so`` (C ABI in
 fails if the library is missing -- there is no CPU fallback.
 """
 from ._lib import AsgkError, lib  # noqa: F401  (loads the CUDA library)
-from .kronmult import (BF16, FP32, FP64, default_gmres_restarts, gmres_info,
+from .kronmult import (BF16, FP32, FP64, cgs_step, default_gmres_restarts, gmres_info,
                        kronmult_matrix, launch_count, simple_gmres,
                        simple_gmres_euler)
 from .operators import (SparseGridOperator, build_pairs, connect_1d,
                         expand_iA, factor_values, sparse_grid)
 
 __all__ = [
-    "kronmult_matrix", "simple_gmres_euler", "simple_gmres", "gmres_info",
+    "kronmult_matrix", "simple_gmres_euler", "simple_gmres", "gmres_info", "cgs_step",
     "default_gmres_restarts", "launch_count", "SparseGridOperator",
     "sparse_grid", "connect_1d", "build_pairs", "expand_iA", "factor_values",
     "FP64", "FP32", "BF16", "AsgkError",

@@ -776,6 +776,39 @@ int asgk_gmres_dense(int n, const double *A, double *x, const double *b,
   return rc;
 }
 
+int asgk_cgs_step(const double *V, int64_t ldv, int k, double *w, int64_t n,
+                  double *h, double *norm, asgk_stream stream)
+{
+  if (!V || !w || !h || !norm || k < 1 || n < 1 || ldv < n)
+    return ASGK_ERR_INVALID;
+  cudaStream_t s   = as_stream(stream);
+  int const blocks = max_reduction_blocks();
+  double *part     = nullptr;
+  size_t const cnt = size_t(blocks) * (k + 1) + 1;
+  ASGK_CUDA(cudaMallocAsync(reinterpret_cast<void **>(&part),
+                            sizeof(double) * cnt, s));
+  double *nrm2 = part + size_t(blocks) * (k + 1);
+  int used     = 0;
+  int rc       = launch_multidot(V, ldv, k, w, n, part, &used, s);
+  if (!rc)
+    rc = launch_reduce_parts(part, used, k, h, s);
+  if (!rc)
+    rc = launch_update_norm(V, ldv, k, h, w, n, part, &used, s);
+  if (!rc)
+    rc = launch_reduce_parts(part, used, 1, nrm2, s);
+  double host = 0;
+  if (!rc && cudaMemcpyAsync(&host, nrm2, sizeof(double),
+                             cudaMemcpyDeviceToHost, s) != cudaSuccess)
+    rc = ASGK_ERR_CUDA;
+  if (cudaFreeAsync(part, s) != cudaSuccess && !rc)
+    rc = ASGK_ERR_CUDA;
+  if (!rc && cudaStreamSynchronize(s) != cudaSuccess)
+    rc = ASGK_ERR_CUDA;
+  if (!rc)
+    *norm = std::sqrt(host);
+  return rc;
+}
+
 int asgk_default_gmres_restarts(int64_t n)
 {
   int const minimum = int(std::min<int64_t>(10, n));

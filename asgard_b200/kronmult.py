@@ -253,6 +253,21 @@ def simple_gmres(A, x, b, M=None, restart=-1, max_iter=-1, tol=-1.0):
     return gmres_info(**info.as_dict())
 
 
+def cgs_step(V, k, w, h=None, stream=None):
+    """One classical Gram-Schmidt step of the device GMRES on CUDA tensors:
+    h = V[:, :k]^T w, w -= V[:, :k] h (in place); returns (h, ||w||).
+    V is (k_cols, n) row-major in torch terms, i.e. column-major n x k_cols
+    with leading dimension n."""
+    import torch
+    n = w.numel()
+    if h is None:
+        h = torch.empty(k, dtype=torch.float64, device=w.device)
+    nrm = C.c_double()
+    check(lib.asgk_cgs_step(_ptr(V), V.stride(0), k, _ptr(w), n, _ptr(h),
+                            C.byref(nrm), _stream(stream)), "cgs_step")
+    return h, nrm.value
+
+
 def default_gmres_restarts(n: int) -> int:
     return lib.asgk_default_gmres_restarts(n)
 
@@ -261,5 +276,5 @@ def launch_count() -> int:
     return lib.asgk_launch_count()
 
 
-__all__ = ["kronmult_matrix", "simple_gmres_euler", "simple_gmres",
+__all__ = ["kronmult_matrix", "simple_gmres_euler", "simple_gmres", "cgs_step",
            "gmres_info", "default_gmres_restarts", "launch_count", "AsgkError"]

@@ -169,6 +169,15 @@ int asgk_gmres_dense(int n, const double *A, double *x, const double *b,
                      int restart, int max_outer, double tol,
                      asgk_gmres_info *info);
 
+/* One classical Gram-Schmidt step of the device GMRES, the two GEMVs and the
+ * norm of src/solver.cpp:233-245:
+ *   h[0..k) = V[:, 0..k)^T w;   w -= V[:, 0..k) h;   *norm = ||w||_2.
+ * V is column-major with leading dimension ldv >= n; V, w and h are device
+ * pointers, norm a host pointer.  Deterministic (fixed-order reductions).
+ * The partial sums live in scratch allocated on the stream for the call. */
+int asgk_cgs_step(const double *V, int64_t ldv, int k, double *w, int64_t n,
+                  double *h, double *norm, asgk_stream stream);
+
 /* default_gmres_restarts<double>(n) (src/solver.cpp:142-152). */
 int asgk_default_gmres_restarts(int64_t n);
 

@@ -112,3 +112,21 @@ def test_gmres_nonfinite_input_reports_status(cuda):
     x = torch.zeros(op.N, dtype=torch.float64, device="cuda")
     info = ab.simple_gmres_euler(1e-3, op.kronmult_matrix(), x, to_dev(b), 10, 5, 1e-10)
     assert info.status == 7  # ASGK_ERR_NONFINITE
+
+
+@pytest.mark.parametrize("n,k", [(1000, 1), (327888, 7), (50001, 51)])
+def test_cgs_step_against_fp64_reference(cuda, n, k):
+    """One Gram-Schmidt step (src/solver.cpp:233-245) against numpy in FP64."""
+    import asgard_b200 as ab
+    import torch
+    rng = np.random.default_rng(n + k)
+    V = rng.uniform(-1, 1, (k, n))
+    w = rng.uniform(-1, 1, n)
+    h_ref = V @ w
+    w_ref = w - V.T @ h_ref
+    Vd = torch.from_numpy(V).cuda()
+    wd = torch.from_numpy(w).cuda()
+    h, nrm = ab.cgs_step(Vd, k, wd)
+    assert rel_err(h.cpu().numpy(), h_ref) < 1e-13
+    assert rel_err(wd.cpu().numpy(), w_ref) < 1e-13
+    assert abs(nrm - np.linalg.norm(w_ref)) <= 1e-13 * np.linalg.norm(w_ref)
