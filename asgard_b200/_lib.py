@@ -16,7 +16,7 @@ EXPORTS = [
     "asgk_plan_destroy", "asgk_plan_update_values", "asgk_plan_info",
     "asgk_apply", "asgk_apply_f32", "asgk_apply_host", "asgk_apply_euler",
     "asgk_gmres_euler", "asgk_gmres_dense", "asgk_default_gmres_restarts",
-    "asgk_cgs_step",
+    "asgk_cgs_step", "asgk_cgs_step_noalloc",
     "asgk_sparse_grid", "asgk_connect_1d", "asgk_build_pairs",
     "asgk_status_string", "asgk_launch_count", "asgk_device_info",
     "asgk_measure_fma_peak",
@@ -61,6 +61,7 @@ def _load():
         "asgk_gmres_dense": ([_i, _vp, _vp, _vp, _i, _i, _d, C.POINTER(GmresInfo)], _i),
         "asgk_default_gmres_restarts": ([_i64], _i),
         "asgk_cgs_step": ([_vp, _i64, _i, _vp, _i64, _vp, C.POINTER(_d), _vp], _i),
+        "asgk_cgs_step_noalloc": ([_vp, _i64, _i, _vp, _i64, _vp, C.POINTER(_d), _vp], _i),
         "asgk_sparse_grid": ([_i, _i, _vp], _i64),
         "asgk_connect_1d": ([_i, C.POINTER(_i), C.POINTER(_i), _vp, _vp], _i),
         "asgk_build_pairs": ([_i, _i, _i, _vp, C.POINTER(_i64), _vp, _vp, _vp], _i),

@@ -523,6 +523,8 @@ const char *asgk_status_string(int status)
   case ASGK_ERR_BREAKDOWN: return "GMRES breakdown";
   case ASGK_ERR_NOT_CONVERGED: return "GMRES did not converge";
   case ASGK_ERR_NONFINITE: return "non-finite residual";
+  case ASGK_ERR_NOALLOC_LIMIT:
+    return "size exceeds the fixed scratch of the allocation-free entry point";
   default: return "unknown status";
   }
 }

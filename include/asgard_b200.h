@@ -39,7 +39,8 @@ typedef enum asgk_status
   ASGK_ERR_ALLOC       = 4, /* device or host allocation failed */
   ASGK_ERR_BREAKDOWN   = 5, /* GMRES: zero or non-finite Arnoldi norm */
   ASGK_ERR_NOT_CONVERGED = 6, /* GMRES: iteration limit before tolerance */
-  ASGK_ERR_NONFINITE   = 7  /* non-finite residual (NaN/Inf in the data) */
+  ASGK_ERR_NONFINITE   = 7, /* non-finite residual (NaN/Inf in the data) */
+  ASGK_ERR_NOALLOC_LIMIT = 8 /* request exceeds an allocation-free entry's fixed scratch */
 } asgk_status;
 
 typedef enum asgk_precision
@@ -177,6 +178,19 @@ int asgk_gmres_dense(int n, const double *A, double *x, const double *b,
  * The partial sums live in scratch allocated on the stream for the call. */
 int asgk_cgs_step(const double *V, int64_t ldv, int k, double *w, int64_t n,
                   double *h, double *norm, asgk_stream stream);
+
+/* asgk_cgs_step without any device allocation, for callers that must not
+ * allocate once their solve runs (all device memory handed to their own pool
+ * at start-up, or no device-wide synchronisation allowed).  No counterpart in
+ * the reference.  Same arguments and result as asgk_cgs_step; the partial
+ * sums use a fixed array of about 1 MiB inside the library (held on every
+ * GPU that loads it until exit).  k <= 256 columns and at most 512 reduction
+ * blocks (GPUs up to 256 SMs), else ASGK_ERR_NOALLOC_LIMIT.  All calls share
+ * the array: calls that overlap on the GPU race.  The first call on a device
+ * looks up the array's address (make it before any stream capture). */
+int asgk_cgs_step_noalloc(const double *V, int64_t ldv, int k, double *w,
+                          int64_t n, double *h, double *norm,
+                          asgk_stream stream);
 
 /* default_gmres_restarts<double>(n) (src/solver.cpp:142-152). */
 int asgk_default_gmres_restarts(int64_t n);
