@@ -42,6 +42,8 @@ void free_plan(plan_data &p)
   cudaFree(p.vA32);
   cudaFree(p.xw);
   cudaFree(p.yw);
+  cudaFree(p.vP64);
+  cudaFree(p.vP32);
   p = plan_data{};
 }
 
@@ -53,6 +55,26 @@ __global__ void k_to_f32(const double *__restrict__ a, float *__restrict__ b,
     b[i] = static_cast<float>(a[i]);
 }
 
+// vP[((c*d + k)*T + t)*PAD + e] = vA[c*d*T*9 + (t*d + k)*9 + e] (e < 9), 0 pad
+__global__ void k_repack(const double *__restrict__ vA, int64_t nconn, int d,
+                         int T, double *__restrict__ v64,
+                         float *__restrict__ v32)
+{
+  int64_t const total = nconn * d * T;
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < total;
+       i += int64_t(gridDim.x) * blockDim.x)
+  {
+    int64_t const c = i / (d * T);
+    int const k     = int((i / T) % d);
+    int const t     = int(i % T);
+    const double *src = vA + c * d * T * 9 + (t * d + k) * 9;
+    for (int e = 0; e < 10; e++)
+      v64[i * 10 + e] = (e < 9) ? src[e] : 0.0;
+    for (int e = 0; e < 12; e++)
+      v32[i * 12 + e] = (e < 9) ? float(src[e]) : 0.0f;
+  }
+}
+
 int upload_values(plan_data &p, const double *vA)
 {
   ASGK_CUDA(cudaMemcpy(p.vA64, vA, sizeof(double) * p.vA_len,
@@ -60,6 +82,11 @@ int upload_values(plan_data &p, const double *vA)
   if (p.vA_len > 0)
   {
     k_to_f32<<<256, 256>>>(p.vA64, p.vA32, p.vA_len);
+    ASGK_LAUNCHED();
+  }
+  if (p.nconn > 0)
+  {
+    k_repack<<<256, 256>>>(p.vA64, p.nconn, p.d, p.terms, p.vP64, p.vP32);
     ASGK_LAUNCHED();
   }
   ASGK_CUDA(cudaDeviceSynchronize());
@@ -141,6 +168,8 @@ int build_plan(asgk_plan **out, int d, int n, int rows, int cols, int terms,
   p.nnz = nnz;
   p.mode = mode;
   p.vA_len = vA_len;
+  if (mode == index_mode::conn && n == 3 && terms > 0)
+    p.nconn = vA_len / blk;
   int64_t &B = p.device_bytes;
   int rc = ASGK_OK;
   if ((rc = dev_alloc(&p.row_ptr, rows + 1, B)) ||
@@ -150,7 +179,9 @@ int build_plan(asgk_plan **out, int d, int n, int rows, int cols, int terms,
       (rc = dev_alloc(&p.vA64, std::max<int64_t>(vA_len, 1), B)) ||
       (rc = dev_alloc(&p.vA32, std::max<int64_t>(vA_len, 1), B)) ||
       (rc = dev_alloc(&p.xw, std::max<int64_t>(int64_t(cols) * p.tensor, 1), B)) ||
-      (rc = dev_alloc(&p.yw, std::max<int64_t>(int64_t(rows) * p.tensor, 1), B)))
+      (rc = dev_alloc(&p.yw, std::max<int64_t>(int64_t(rows) * p.tensor, 1), B)) ||
+      (rc = dev_alloc(&p.vP64, p.nconn * d * terms * 10, B)) ||
+      (rc = dev_alloc(&p.vP32, p.nconn * d * terms * 12, B)))
   {
     free_plan(p);
     return rc;
@@ -890,9 +921,10 @@ int asgk_gmres_euler(asgk_plan *plan, double dt, double *x, const double *b,
     // FP64 iterative refinement: r = b - A x in FP64, inner (flexible) GMRES
     // on A e = r with the low-precision operator, x += e.
     double const inner_rtol = (precision == ASGK_FP64) ? 1e-10 : 1e-5;
-    int total = 0, low = 0, fp64 = 0, pcalls = 0, steps = 0;
-    double rnorm = 0;
+    int total = 0, low = 0, fp64 = 0, pcalls = 0, steps = 0, fallback = 0;
+    double rnorm = 0, prev_rnorm = 0;
     int const max_steps = 50;
+    precond_t const *use_pc = pcp;
     status = ASGK_ERR_NOT_CONVERGED;
     for (;;)
     {
@@ -916,13 +948,21 @@ int asgk_gmres_euler(asgk_plan *plan, double dt, double *x, const double *b,
       }
       if (steps >= max_steps || total >= max_outer * (restart + 1))
         break;
+      // The learned preconditioner is dropped (plain GMRES from the current
+      // iterate) when a refinement step did not halve the FP64 residual.
+      if (use_pc && steps > 0 && rnorm > 0.5 * prev_rnorm)
+      {
+        use_pc   = nullptr;
+        fallback = 1;
+      }
+      prev_rnorm = rnorm;
       if (int rc = launch_fill(ws.e, n, 0.0, s))
         return rc;
       core_stats ist;
       double const itol = std::max(inner_rtol * rnorm, 0.5 * tol_abs);
       int const inner_outer = std::max(1, max_outer);
       if (int rc = gmres_core(ws, n, (precision == ASGK_FP64) ? matvec_t(op64) : matvec_t(oplow),
-                              pcp, ws.e, ws.r, restart, inner_outer, itol, ist, s))
+                              use_pc, ws.e, ws.r, restart, inner_outer, itol, ist, s))
         return rc;
       total += ist.total;
       if (precision == ASGK_FP64)
@@ -933,6 +973,13 @@ int asgk_gmres_euler(asgk_plan *plan, double dt, double *x, const double *b,
       ++steps;
       if (ist.status == ASGK_ERR_NONFINITE)
       {
+        if (use_pc)
+        {
+          // a non-finite network output: retry the step without it
+          use_pc   = nullptr;
+          fallback = 1;
+          continue;
+        }
         status = ASGK_ERR_NONFINITE;
         break;
       }
@@ -945,6 +992,7 @@ int asgk_gmres_euler(asgk_plan *plan, double dt, double *x, const double *b,
     out.matvecs_low  = low;
     out.matvecs_fp64 = fp64;
     out.precond_calls = pcalls;
+    out.fallback      = fallback;
   }
   // FP64 check of the final iterate (unless the solve ended on one)
   double rfinal = true_res;

@@ -63,6 +63,12 @@ struct plan_data
   int *row_order = nullptr;   // [rows] cells by decreasing pair count
   double *vA64 = nullptr;     // [vA_len]
   float *vA32  = nullptr;     // [vA_len]
+  // sparse-grid plans with n = 3: the factors repacked per (connection,
+  // dimension) with the T terms contiguous, each 3 x 3 block padded to a
+  // 16-byte multiple (10 doubles / 12 floats) for vector loads
+  int64_t nconn = 0;
+  double *vP64  = nullptr;    // [nconn][d][T][10]
+  float *vP32   = nullptr;    // [nconn][d][T][12]
 
   // FP64 workspace for apply_host and GMRES scratch
   double *xw = nullptr, *yw = nullptr;

@@ -34,24 +34,34 @@ namespace
 {
 constexpr int ipow3(int k) { return k == 0 ? 1 : 3 * ipow3(k - 1); }
 
-template<int D>
+template<int D, int HL>
 struct shape3
 {
-  static constexpr int H    = D / 2;               // dimensions on lanes
+  static constexpr int H    = HL;                  // dimensions on lanes
   static constexpr int LG   = ipow3(H);            // lanes per group
   static constexpr int R    = ipow3(D - H);        // registers per lane
-  static constexpr int TS   = ipow3(D);            // tensor size
+  static constexpr int TS   = ipow3(D);            // tensor size (odd)
   static constexpr int G    = 32 / LG;             // groups per warp
-  static constexpr int LOWB = ipow3(D - 2 * H);    // 1 (d even) or 3 (d odd)
-  static constexpr int BUF  = TS + ((TS % 2 == 0) ? 1 : 0) + ((TS % 2 == 0) ? 0 : 0);
+  static constexpr int LOWB = ipow3(D - 2 * H);    // register block below the lane dims in B
+  static constexpr int BUF  = TS;                  // odd stride: conflict-free transposes
   // layout A: lane q <-> dims [0, H), register m <-> dims [H, D)
   // layout B: lane q <-> dims [H, 2H), register m <-> dims [0, H) ++ [2H, D)
+  // A pair's tensor is read in layout B, dims [0, H) are contracted, one
+  // transpose moves it to layout A, dims [H, D) are contracted.
   static constexpr int strideA(int k) { return ipow3(D - 1 - k); }
   static constexpr int strideB(int k) { return ipow3(H - 1 - k) * LOWB; }
   __device__ static constexpr int idxB(int q, int m)
   {
     return (m / LOWB) * ipow3(D - H) + q * LOWB + (m % LOWB);
   }
+};
+
+// lane dimensions per d: 3 x 27 registers for d = 4, 9 x 27 for d = 5,
+// 27 x 27 for d = 6 (27 values per lane along every contracted fibre set)
+template<int D>
+struct lanes3
+{
+  static constexpr int value = (D <= 4) ? 1 : (D == 5 ? 2 : 3);
 };
 
 template<int B, int E, typename F>
@@ -64,15 +74,42 @@ __device__ __forceinline__ void static_for(F &&f)
   }
 }
 
-// w <- (I (x) A (x) I) w along the register dimension with stride S:
-// out_j = sum_i A(j, i) w_i, A column-major (A(j, i) = A[j + 3 i]).
-template<int R, int S, typename TC>
-__device__ __forceinline__ void contract3(TC (&w)[R], const TC *__restrict__ A)
+// The 9 entries of a column-major 3 x 3 factor (A(j, i) = a[j + 3 i]).
+template<typename TC>
+__device__ __forceinline__ void load9(const TC *__restrict__ A, TC (&a)[9])
 {
-  TC a[9];
 #pragma unroll
   for (int i = 0; i < 9; i++)
     a[i] = __ldg(A + i);
+}
+
+// Padded block (16-byte aligned, 10 doubles or 12 floats): vector loads.
+__device__ __forceinline__ void load9p(const double *__restrict__ A, double (&a)[9])
+{
+  const double2 *v = reinterpret_cast<const double2 *>(A);
+#pragma unroll
+  for (int i = 0; i < 4; i++)
+  {
+    double2 const t = __ldg(v + i);
+    a[2 * i]        = t.x;
+    a[2 * i + 1]    = t.y;
+  }
+  a[8] = __ldg(A + 8);
+}
+__device__ __forceinline__ void load9p(const float *__restrict__ A, float (&a)[9])
+{
+  const float4 *v = reinterpret_cast<const float4 *>(A);
+  float4 const t0 = __ldg(v), t1 = __ldg(v + 1);
+  a[0] = t0.x; a[1] = t0.y; a[2] = t0.z; a[3] = t0.w;
+  a[4] = t1.x; a[5] = t1.y; a[6] = t1.z; a[7] = t1.w;
+  a[8] = __ldg(A + 8);
+}
+
+// w <- (I (x) A (x) I) w along the register dimension with stride S:
+// out_j = sum_i A(j, i) w_i.
+template<int R, int S, typename TC>
+__device__ __forceinline__ void contract3(TC (&w)[R], TC const (&a)[9])
+{
 #pragma unroll
   for (int b = 0; b < R; b++)
   {
@@ -86,14 +123,36 @@ __device__ __forceinline__ void contract3(TC (&w)[R], const TC *__restrict__ A)
   }
 }
 
+// acc += (I (x) A (x) I) w along the register dimension with stride S.
+template<int R, int S, typename TC>
+__device__ __forceinline__ void contract3_acc(TC const (&w)[R], TC const (&a)[9],
+                                              TC (&acc)[R])
+{
+#pragma unroll
+  for (int b = 0; b < R; b++)
+  {
+    if ((b / S) % 3 == 0)
+    {
+      TC const w0 = w[b], w1 = w[b + S], w2 = w[b + 2 * S];
+      acc[b]         = fma(a[6], w2, fma(a[3], w1, fma(a[0], w0, acc[b])));
+      acc[b + S]     = fma(a[7], w2, fma(a[4], w1, fma(a[1], w0, acc[b + S])));
+      acc[b + 2 * S] = fma(a[8], w2, fma(a[5], w1, fma(a[2], w0, acc[b + 2 * S])));
+    }
+  }
+}
+
+template<typename TC> struct pad3;
+template<> struct pad3<double> { static constexpr int value = 10; };
+template<> struct pad3<float> { static constexpr int value = 12; };
+
 template<typename T>
 __device__ __forceinline__ double to_f64(T v)
 {
   return static_cast<double>(v);
 }
 
-template<int D, typename TC, typename TX, typename TY, index_mode MODE,
-         bool EULER, int NW>
+template<int D, int HL, typename TC, typename TX, typename TY,
+         index_mode MODE, bool EULER, int NW>
 __global__ void __launch_bounds__(NW * 32)
     kron3_rows(int terms, const int64_t *__restrict__ row_ptr,
                const int *__restrict__ row_order, const int *__restrict__ col,
@@ -101,7 +160,8 @@ __global__ void __launch_bounds__(NW * 32)
                double alpha, const TX *__restrict__ x, double beta,
                TY *__restrict__ y, double ex)
 {
-  using S = shape3<D>;
+  // conn mode: vA is the repacked [conn][d][T][pad] array
+  using S = shape3<D, HL>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   TC *smem = reinterpret_cast<TC *>(smem_raw);
 
@@ -115,7 +175,7 @@ __global__ void __launch_bounds__(NW * 32)
   int const row       = row_order[blockIdx.x];
   int64_t const pbeg  = row_ptr[row];
   int64_t const pend  = row_ptr[row + 1];
-  int const blk       = D * terms * 9;
+  constexpr int PAD   = pad3<TC>::value;
 
   TC acc[S::R];
 #pragma unroll
@@ -128,12 +188,14 @@ __global__ void __launch_bounds__(NW * 32)
     bool const act   = laneok && (p < pend);
     int64_t const pc = act ? p : pbeg;
 
-    TC xa[S::R];
+    // x in layout B: for a fixed register, the lanes of a group read
+    // consecutive entries (coalesced)
+    TC xb[S::R];
     {
-      const TX *xs = x + int64_t(col[pc]) * S::TS + q * S::R;
+      const TX *xs = x + int64_t(col[pc]) * S::TS;
 #pragma unroll
       for (int m = 0; m < S::R; m++)
-        xa[m] = act ? static_cast<TC>(xs[m]) : TC(0);
+        xb[m] = act ? static_cast<TC>(xs[S::idxB(q, m)]) : TC(0);
     }
     int cn[D];
     if constexpr (MODE == index_mode::conn)
@@ -145,46 +207,56 @@ __global__ void __launch_bounds__(NW * 32)
 
     for (int t = 0; t < terms; t++)
     {
-      auto factor = [&](int k) -> const TC * {
+      auto factor = [&](int k, TC(&a)[9]) {
         if constexpr (MODE == index_mode::conn)
-          return vA + int64_t(cn[k]) * blk + (t * D + k) * 9;
+          load9p(vA + ((int64_t(cn[k]) * D + k) * terms + t) * PAD, a);
         else
-          return vA + __ldg(idx + (pc * terms + t) * D + k);
+          load9(vA + __ldg(idx + (pc * terms + t) * D + k), a);
       };
       TC w[S::R];
 #pragma unroll
       for (int m = 0; m < S::R; m++)
-        w[m] = xa[m];
-      // dimensions [H, D) are in registers in layout A
-      static_for<S::H, D>([&](auto kc) {
-        constexpr int k = decltype(kc)::value;
-        contract3<S::R, S::strideA(k)>(w, factor(k));
-      });
-      // transpose to layout B through shared memory
-      __syncwarp();
-      if (laneok)
-      {
-#pragma unroll
-        for (int m = 0; m < S::R; m++)
-          buf[q * S::R + m] = w[m];
-      }
-      __syncwarp();
-      if (laneok)
-      {
-#pragma unroll
-        for (int m = 0; m < S::R; m++)
-          w[m] = buf[S::idxB(q, m)];
-      }
+        w[m] = xb[m];
       // dimensions [0, H) are in registers in layout B
       static_for<0, S::H>([&](auto kc) {
         constexpr int k = decltype(kc)::value;
-        contract3<S::R, S::strideB(k)>(w, factor(k));
+        TC a[9];
+        factor(k, a);
+        contract3<S::R, S::strideB(k)>(w, a);
       });
-      if (act)
+      // transpose to layout A through shared memory
+      __syncwarp();
+      if (laneok)
       {
 #pragma unroll
         for (int m = 0; m < S::R; m++)
-          acc[m] += w[m];
+          buf[S::idxB(q, m)] = w[m];
+      }
+      __syncwarp();
+      if (laneok)
+      {
+#pragma unroll
+        for (int m = 0; m < S::R; m++)
+          w[m] = buf[q * S::R + m];
+      }
+      // dimensions [H, D) are in registers in layout A; the last one
+      // accumulates straight into acc
+      static_for<S::H, D - 1>([&](auto kc) {
+        constexpr int k = decltype(kc)::value;
+        TC a[9];
+        factor(k, a);
+        contract3<S::R, S::strideA(k)>(w, a);
+      });
+      {
+        TC a[9];
+        factor(D - 1, a);
+        if (!act)
+        {
+#pragma unroll
+          for (int i = 0; i < 9; i++)
+            a[i] = TC(0);
+        }
+        contract3_acc<S::R, S::strideA(D - 1)>(w, a, acc);
       }
     }
   }
@@ -195,7 +267,7 @@ __global__ void __launch_bounds__(NW * 32)
   {
 #pragma unroll
     for (int m = 0; m < S::R; m++)
-      buf[S::idxB(q, m)] = acc[m];
+      buf[q * S::R + m] = acc[m];
   }
   __syncthreads();
   int64_t const base = int64_t(row) * S::TS;
@@ -304,9 +376,17 @@ template<int D, typename TC, typename TX, typename TY, index_mode MODE,
 int launch3(plan_data const &p, const TC *vA, double alpha, const TX *x,
             double beta, TY *y, double ex, cudaStream_t s)
 {
-  using S          = shape3<D>;
+  constexpr int HL = lanes3<D>::value;
+  using S          = shape3<D, HL>;
   size_t const shm = size_t(kWarps) * S::G * S::BUF * sizeof(TC);
-  auto kern        = kron3_rows<D, TC, TX, TY, MODE, EULER, kWarps>;
+  auto kern        = kron3_rows<D, HL, TC, TX, TY, MODE, EULER, kWarps>;
+  if constexpr (MODE == index_mode::conn)
+  {
+    if constexpr (std::is_same_v<TC, double>)
+      vA = reinterpret_cast<const TC *>(p.vP64);
+    else
+      vA = reinterpret_cast<const TC *>(p.vP32);
+  }
   static bool configured = false;
   if (!configured)
   {

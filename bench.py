@@ -52,6 +52,10 @@ def parse():
     ap.add_argument("--plain-steps", type=int, default=2)
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--method", default="learned-fp32",
+                    choices=["learned-fp32", "learned-fp64", "fp32", "fp64"])
+    ap.add_argument("--train-solves", type=int, default=5)
+    ap.add_argument("--train-epochs", type=int, default=60)
     return ap.parse_args()
 
 
@@ -258,7 +262,24 @@ def main():
     nb = args.warmup + args.steps
     B = [torch.rand(N, dtype=torch.float64, device="cuda", generator=gen) * 2 - 1
          for _ in range(max(nb, args.plain_steps + 1))]
-    method = dict(precision="fp32", precond=None, name="fp32-ir")
+    precision = "fp64" if args.method.endswith("fp64") else "fp32"
+    pc, train_info = None, None
+    if args.method.startswith("learned"):
+        # setup, not timed (like building the operator): plain FP64 GMRES
+        # solves of random right-hand sides give (v, e) pairs, one row per
+        # cell, and the network trains on them on this GPU
+        t0 = time.perf_counter()
+        pc = ab.LearnedPreconditioner(op, seed=rank)
+        train_info = pc.train(mat, dt, num_solves=args.train_solves,
+                              epochs=args.train_epochs, batch=1024, lr=1e-3,
+                              seed=rank)
+        torch.cuda.synchronize()
+        train_info["setup_s"] = time.perf_counter() - t0
+    method = dict(precision=precision, precond=pc,
+                  name={"learned-fp32": "learned preconditioner + FP32 operator, FP64 refinement",
+                        "learned-fp64": "learned preconditioner, FP64",
+                        "fp32": "FP32 operator, FP64 refinement",
+                        "fp64": "plain FP64 GMRES"}[args.method])
 
     def solve(b, precision, precond=None):
         x = torch.zeros(N, dtype=torch.float64, device="cuda")
@@ -361,17 +382,21 @@ def main():
             "ms_per_step": t_method / args.steps * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic",
-            "config": dict(_config(args.workload), method=method["name"],
+            "config": dict(_config(args.workload), method=args.method,
                            parallelism=f"replicas x{world}"),
             "plain_fp64": {"value": plain_value, "unit": "solves/s",
                            "iterations": pinfo.iterations,
                            "true_relres": max(i.true_relres for i in pinfos),
                            "ms_per_solve": t_plain / args.plain_steps * 1e3},
-            "method": {"iterations": [i.iterations for i in minfos],
+            "method": {"name": method["name"],
+                       "iterations": [i.iterations for i in minfos],
                        "true_relres": max(i.true_relres for i in minfos),
                        "outer_steps": minfos[0].outer_steps,
                        "matvecs_low": minfos[0].matvecs_low,
                        "matvecs_fp64": minfos[0].matvecs_fp64,
+                       "precond_calls": minfos[0].precond_calls,
+                       "fallback": max(i.fallback for i in minfos),
+                       "training": train_info,
                        "speedup_vs_plain": value / plain_value},
             "clocks": clk,
             "e2e": {"value": e2e_value, "unit": "solves/s",

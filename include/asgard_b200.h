@@ -195,6 +195,40 @@ int asgk_cgs_step_noalloc(const double *V, int64_t ldv, int k, double *w,
 /* default_gmres_restarts<double>(n) (src/solver.cpp:142-152). */
 int asgk_default_gmres_restarts(int64_t n);
 
+/* ------------------------------------------------ learned preconditioner */
+
+/* A per-cell MLP preconditioner (no counterpart in the reference, which has
+ * none on this path; BASELINE's learned form).  4 layers, widths
+ * (n^d + d) -> hidden -> hidden -> hidden -> n^d, GELU, FP32 master weights,
+ * BF16 tensor-core GEMMs with FP32 accumulation.  As a preconditioner,
+ * z_c = ||v_c|| * f([v_c / ||v_c||, levels_c / max_level]) for every cell c.
+ * cell_levels: num_cells x d host ints (the element table's level columns).
+ * Weights are initialised from seed. */
+int asgk_mlp_create(asgk_mlp **mlp, int d, int n, int num_cells,
+                    const int *cell_levels, int max_level, int hidden,
+                    uint64_t seed);
+void asgk_mlp_destroy(asgk_mlp *mlp);
+int asgk_mlp_num_params(const asgk_mlp *mlp, int64_t *count);
+/* Flat FP32 host layout: per layer W (row-major fan_in x fan_out) then b. */
+int asgk_mlp_get_params(const asgk_mlp *mlp, float *params);
+int asgk_mlp_set_params(asgk_mlp *mlp, const float *params);
+/* One forward and backward pass on host rows (X: rows x (n^d + d), targets
+ * T: rows x n^d, FP32): outputs Y, loss = 0.5*sum((Y - T)^2) and the
+ * gradients in the parameter layout.  Used to check the kernels' gradients. */
+int asgk_mlp_forward_backward(asgk_mlp *mlp, int rows, const float *X,
+                              const float *T, float *Y, float *grads,
+                              double *loss);
+/* Trains on num_samples (v, e) vector pairs on the device (sample-major,
+ * num_cells*n^d FP64 each, e = (I - dt K)^{-1} v): one row per (sample,
+ * cell), mini-batches of `batch` rows, `epochs` passes, Adam(lr).  Reports
+ * the last epoch's mean squared error. */
+int asgk_mlp_train(asgk_mlp *mlp, const double *v, const double *e,
+                   int num_samples, int epochs, int batch, float lr,
+                   uint64_t seed, double *final_loss, asgk_stream stream);
+/* z = M(v) on device vectors of the plan's size. */
+int asgk_mlp_apply(asgk_mlp *mlp, asgk_plan *plan, const double *v, double *z,
+                   asgk_stream stream);
+
 /* ------------------------------------------------------- sparse grids */
 
 /* Host-side builder of the reference's sparse-grid operator structure:

@@ -155,3 +155,24 @@ def test_oracle_planted_mistake_is_caught():
     y2 = oracle.kronmult(3, 3, data["pntr"], data["indx"], 2, data["iA"], vA,
                          1.0, data["x"], 0.0, np.zeros_like(data["y"]))
     assert np.linalg.norm(y1 - y2) / np.linalg.norm(y1) > 1e-9
+
+
+def test_mlp_oracle_gradient_matches_finite_differences():
+    """The float64 network oracle's backward pass against central finite
+    differences (it is the checker of the GPU gradients)."""
+    from oracle import mlp_oracle
+    rng = np.random.default_rng(0)
+    dims = [5, 6, 6, 6, 3]
+    nparams = sum(dims[l] * dims[l + 1] + dims[l + 1] for l in range(4))
+    p = rng.normal(0, 0.5, nparams)
+    X = rng.normal(0, 1, (4, 5))
+    T = rng.normal(0, 1, (4, 3))
+    _, _, g = mlp_oracle.forward_backward(p, dims, X, T)
+    h = 1e-6
+    for i in rng.choice(nparams, 25, replace=False):
+        pp, pm = p.copy(), p.copy()
+        pp[i] += h
+        pm[i] -= h
+        fd = (mlp_oracle.forward_backward(pp, dims, X, T)[1] -
+              mlp_oracle.forward_backward(pm, dims, X, T)[1]) / (2 * h)
+        assert abs(fd - g[i]) <= 1e-6 * max(1.0, abs(fd))
