@@ -22,6 +22,7 @@ EXPORTS = [
     "asgk_measure_fma_peak", "asgk_mlp_create", "asgk_mlp_destroy",
     "asgk_mlp_num_params", "asgk_mlp_get_params", "asgk_mlp_set_params",
     "asgk_mlp_forward_backward", "asgk_mlp_train", "asgk_mlp_apply",
+    "asgk_mlp_train_residual",
 ]
 
 
@@ -79,6 +80,7 @@ def _load():
         "asgk_mlp_forward_backward": ([_vp, _i, _vp, _vp, _vp, _vp, C.POINTER(_d)], _i),
         "asgk_mlp_train": ([_vp, _vp, _vp, _i, _i, _i, C.c_float, C.c_uint64, C.POINTER(_d), _vp], _i),
         "asgk_mlp_apply": ([_vp, _vp, _vp, _vp, _vp], _i),
+        "asgk_mlp_train_residual": ([_vp, _vp, _vp, _d, _vp, _vp, _i, _i, C.c_float, _i, C.c_uint64, C.POINTER(_d), _vp], _i),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)

@@ -343,7 +343,8 @@ struct core_stats
   int restarts = 0;
   double err  = 0;
   int status  = ASGK_OK;
-  bool verified = false; // stopped on a recomputed residual
+  bool verified = false;  // stopped on a recomputed residual
+  bool stagnated = false; // a preconditioned cycle reduced the residual < 10%
 };
 
 int norm2(gmres_ws &ws, const double *v, int64_t n, double &out,
@@ -382,7 +383,7 @@ int gmres_core(gmres_ws &ws, int64_t n, matvec_t const &mat,
   std::vector<double> sines(restart + 1, 0.0), cosines(restart + 1, 0.0),
       ksol(restart + 1, 0.0);
   int outer       = 0;
-  double inner_res = 0, outer_res = tol + 1;
+  double inner_res = 0, outer_res = tol + 1, cycle_start = -1;
   while (outer_res > tol && outer < max_outer)
   {
     double *r0 = ws.V;
@@ -406,6 +407,14 @@ int gmres_core(gmres_ws &ws, int64_t n, matvec_t const &mat,
       st.verified = true;
       break;
     }
+    if (flex && cycle_start >= 0 && inner_res > 0.9 * cycle_start)
+    {
+      // the preconditioned cycle did not reduce the residual by 10%
+      st.stagnated = true;
+      outer_res    = inner_res;
+      break;
+    }
+    cycle_start = inner_res;
     if (int rc = launch_scale(r0, n, 1.0 / inner_res, s))
       return rc;
     ksol[0] = inner_res;
@@ -971,6 +980,16 @@ int asgk_gmres_euler(asgk_plan *plan, double dt, double *x, const double *b,
         low += ist.matvecs;
       pcalls += ist.pcalls;
       ++steps;
+      if (ist.stagnated && use_pc)
+      {
+        // keep the progress made (e is a valid correction), then continue
+        // without the learned preconditioner
+        if (int rc = launch_axpy(x, ws.e, n, 1.0, s))
+          return rc;
+        use_pc   = nullptr;
+        fallback = 1;
+        continue;
+      }
       if (ist.status == ASGK_ERR_NONFINITE)
       {
         if (use_pc)

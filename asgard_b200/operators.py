@@ -124,6 +124,26 @@ def factor_values(d: int, level: int, terms: int, kind: str = "advdiff",
     return vA.reshape(-1)
 
 
+def transpose_factor_values(vA: np.ndarray, d: int, level: int, terms: int,
+                            n: int = 3) -> np.ndarray:
+    """Factor values of the transposed operator K^T on the same pair list.
+
+    The connected-pair set is symmetric, so K^T has the same CSR structure;
+    its pair (c, r) needs (A_{t,k} at the 1D connection (r_k, c_k))^T.  With
+    factors addressed by the pair's own connection (c_k, r_k), block j of the
+    result is the transposed block of the mirror connection of j."""
+    pntr, indx = connect_1d(level)
+    rows = np.repeat(np.arange(len(pntr) - 1), np.diff(pntr))
+    R = len(pntr) - 1
+    lut = np.full((R, R), -1, np.int64)
+    lut[rows, indx] = np.arange(len(indx))
+    mirror = lut[indx, rows]
+    if (mirror < 0).any():
+        raise ValueError("1D connectivity is not symmetric")
+    blocks = vA.reshape(len(indx), terms, d, n, n)     # [..., col j, row i]
+    return np.ascontiguousarray(blocks[mirror].transpose(0, 1, 2, 4, 3)).reshape(-1)
+
+
 class SparseGridOperator:
     """Structure + values of a synthetic sparse-grid operator."""
 
@@ -152,6 +172,15 @@ class SparseGridOperator:
         return kronmult_matrix.from_conn(self.d, self.n, self.rows, self.rows,
                                          self.terms, self.row_ptr, self.col,
                                          self.conn, self.vA)
+
+    def kronmult_matrix_transposed(self):
+        """K^T as a plan (same pair list, transposed mirror factors)."""
+        from .kronmult import kronmult_matrix
+        vT = transpose_factor_values(self.vA, self.d, self.level, self.terms,
+                                     self.n)
+        return kronmult_matrix.from_conn(self.d, self.n, self.rows, self.rows,
+                                         self.terms, self.row_ptr, self.col,
+                                         self.conn, vT)
 
     def flops(self) -> int:
         return 2 * self.d * self.terms * self.n ** (self.d + 1) * self.nnz

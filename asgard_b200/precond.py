@@ -1,12 +1,16 @@
-"""Learned preconditioner: a per-cell MLP trained on the GPU from plain GMRES
-solves, used on the right inside flexible GMRES.
+"""Learned preconditioner: a per-cell network trained on the GPU from plain
+GMRES solves, used on the right inside (flexible) GMRES.  The network is
+linear in the residual block and gated by the cell's levels (see
+include/asgard_b200.h), so the preconditioner is a fixed linear operator.
 
     pc = LearnedPreconditioner(op)                  # op: SparseGridOperator
     stats = pc.train(mat, dt, num_solves=5)         # 5 x cells training rows
     info = simple_gmres_euler(dt, mat, x, b, ..., precond=pc)
 
-Training data follow BASELINE's recipe: random right-hand sides v, the plain
-FP64 GMRES solution e of (I - dt K) e = v, and one (v_c, e_c) row per cell.
+Training data: (residual, GMRES-correction) pairs from plain FP64 GMRES solves
+of random right-hand sides -- each restart cycle's residual r_k and the exact
+correction x* - x_k -- one row per (pair, cell).  A solve with ~5 restart
+cycles gives ~5 x cells rows (about 20k at d=4, level 7).
 """
 from __future__ import annotations
 
@@ -34,7 +38,8 @@ class LearnedPreconditioner:
                                   levels.ctypes.data, level, hidden, seed),
               "mlp_create")
         self._h = h
-        self.dims = [n ** d + d, hidden, hidden, hidden, n ** d]
+        self.dims = [n ** d, hidden, hidden, hidden, n ** d]
+        self.useful = None   # set by validate()
 
     def __del__(self):
         h = getattr(self, "_h", None)
@@ -96,26 +101,47 @@ class LearnedPreconditioner:
         return Y, loss.value, g
 
     # -- training ----------------------------------------------------------
-    def generate(self, mat, dt, num_solves=5, restart=50, tol=1e-10, seed=0):
-        """(v, e) sample pairs from plain FP64 GMRES solves (device tensors)."""
+    def generate(self, mat, dt, num_solves=5, restart=50, tol=1e-10, seed=0,
+                 max_cycles=40, white_only=False):
+        """(residual, GMRES-correction) pairs from plain FP64 GMRES solves of
+        random right-hand sides: every restart cycle k of a solve gives the
+        residual r_k = b - A x_k and the correction e_k = x* - x_k that solves
+        A e_k = r_k exactly (x* the converged solution).  Device tensors."""
         import torch
         from .kronmult import simple_gmres_euler
         N = mat.output_size()
         g = torch.Generator(device="cuda").manual_seed(seed)
-        V = torch.empty(num_solves, N, dtype=torch.float64, device="cuda")
-        E = torch.zeros(num_solves, N, dtype=torch.float64, device="cuda")
-        its = []
+        Vs, Es, its = [], [], []
         for s in range(num_solves):
-            V[s] = torch.rand(N, dtype=torch.float64, device="cuda", generator=g) * 2 - 1
-            info = simple_gmres_euler(dt, mat, E[s], V[s], restart, 400, tol,
-                                      tol_mode="rel")
-            its.append(info.iterations)
-        return V, E, its
+            b = torch.rand(N, dtype=torch.float64, device="cuda", generator=g) * 2 - 1
+            x = torch.zeros(N, dtype=torch.float64, device="cuda")
+            iterates, total = [], 0
+            for _ in range(max_cycles):
+                iterates.append(x.clone())
+                info = simple_gmres_euler(dt, mat, x, b, restart, 1, tol,
+                                          tol_mode="rel")
+                total += info.iterations
+                if info.true_relres <= tol:
+                    break
+            its.append(total)
+            if white_only:
+                iterates = iterates[:1]   # only (b, x*): uncorrelated residuals
+            for xk in iterates:
+                r = b.clone()
+                mat.apply_euler(dt, -1.0, xk, 1.0, r)   # r = b - A x_k
+                Vs.append(r)
+                Es.append(x - xk)
+        return torch.stack(Vs), torch.stack(Es), its
 
     def train(self, mat, dt, num_solves=5, epochs=60, batch=1024, lr=1e-3,
-              seed=0, samples=None):
-        """Generates the samples (unless given as (V, E)) and trains."""
+              seed=0, samples=None, mat_T=None, residual_epochs=30,
+              residual_lr=3e-4, precision="fp32"):
+        """Generates the samples (unless given as (V, E)) and trains: first
+        on the correction itself (mean squared error of e_c, cell rows), then,
+        when mat_T (K^T) is given, on the preconditioned residual
+        ||A M r - r|| / ||r|| of every sample (asgk_mlp_train_residual)."""
         import torch
+        from .kronmult import _precision
         if samples is None:
             V, E, its = self.generate(mat, dt, num_solves, seed=seed)
         else:
@@ -127,8 +153,41 @@ class LearnedPreconditioner:
                                  C.c_void_p(E.data_ptr()), V.shape[0], epochs,
                                  batch, lr, seed, C.byref(loss), stream),
               "mlp_train")
-        return {"loss": loss.value, "rows": V.shape[0] * self.cells,
-                "solve_iterations": its}
+        out = {"loss": loss.value, "rows": V.shape[0] * self.cells,
+               "samples": V.shape[0], "solve_iterations": its}
+        if mat_T is not None and residual_epochs > 0:
+            rl = C.c_double()
+            check(lib.asgk_mlp_train_residual(
+                self._h, mat.handle, mat_T.handle, dt, C.c_void_p(V.data_ptr()),
+                C.c_void_p(E.data_ptr()), V.shape[0], residual_epochs,
+                residual_lr, _precision(precision), seed, C.byref(rl), stream),
+                "mlp_train_residual")
+            out["residual_loss"] = rl.value
+        out["validation"] = self.validate(mat, dt, seed=seed + 7919)
+        return out
+
+    def validate(self, mat, dt, seed=0, restart=50, tol=1e-10):
+        """Solves one held-out right-hand side with and without the network
+        (FP64, relative tolerance) and records whether it reduced the
+        iteration count; ``useful`` is False when it did not, and callers
+        then fall back to plain GMRES (the solver also drops a network that
+        stalls a solve)."""
+        import torch
+        from .kronmult import simple_gmres_euler
+        N = mat.output_size()
+        g = torch.Generator(device="cuda").manual_seed(seed)
+        b = torch.rand(N, dtype=torch.float64, device="cuda", generator=g) * 2 - 1
+        plain = simple_gmres_euler(dt, mat, torch.zeros_like(b), b, restart,
+                                   400, tol, tol_mode="rel")
+        learned = simple_gmres_euler(dt, mat, torch.zeros_like(b), b, restart,
+                                     400, tol, tol_mode="rel", precond=self)
+        self.useful = (learned.status == 0 and learned.fallback == 0 and
+                       learned.iterations < plain.iterations)
+        return {"plain_iterations": plain.iterations,
+                "learned_iterations": learned.iterations,
+                "learned_fallback": learned.fallback,
+                "gain": plain.iterations / max(learned.iterations, 1),
+                "useful": self.useful}
 
     def apply(self, mat, v, z):
         import torch

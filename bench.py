@@ -54,7 +54,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--method", default="learned-fp32",
                     choices=["learned-fp32", "learned-fp64", "fp32", "fp64"])
-    ap.add_argument("--train-solves", type=int, default=5)
+    ap.add_argument("--train-solves", type=int, default=1)
     ap.add_argument("--train-epochs", type=int, default=60)
     return ap.parse_args()
 
@@ -272,9 +272,13 @@ def main():
         pc = ab.LearnedPreconditioner(op, seed=rank)
         train_info = pc.train(mat, dt, num_solves=args.train_solves,
                               epochs=args.train_epochs, batch=1024, lr=1e-3,
-                              seed=rank)
+                              seed=rank, mat_T=op.kronmult_matrix_transposed(),
+                              residual_epochs=20)
         torch.cuda.synchronize()
         train_info["setup_s"] = time.perf_counter() - t0
+        if not pc.useful:
+            # the validation solve showed no gain: plain GMRES is the fallback
+            pc = None
     method = dict(precision=precision, precond=pc,
                   name={"learned-fp32": "learned preconditioner + FP32 operator, FP64 refinement",
                         "learned-fp64": "learned preconditioner, FP64",

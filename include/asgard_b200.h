@@ -197,11 +197,15 @@ int asgk_default_gmres_restarts(int64_t n);
 
 /* ------------------------------------------------ learned preconditioner */
 
-/* A per-cell MLP preconditioner (no counterpart in the reference, which has
- * none on this path; BASELINE's learned form).  4 layers, widths
- * (n^d + d) -> hidden -> hidden -> hidden -> n^d, GELU, FP32 master weights,
- * BF16 tensor-core GEMMs with FP32 accumulation.  As a preconditioner,
- * z_c = ||v_c|| * f([v_c / ||v_c||, levels_c / max_level]) for every cell c.
+/* A per-cell learned preconditioner (no counterpart in the reference, which
+ * has none on this path; BASELINE's learned form).  4 layers of width
+ * `hidden` with GELU: the cell's residual block (scaled to unit norm) passes
+ * through 4 linear layers whose hidden activations are gated elementwise by
+ * GELU gates computed from the cell's level multi-index, so the network is
+ * linear in the residual and the preconditioner
+ *   z_c = ||v_c|| * f(v_c / ||v_c||, levels_c / max_level)
+ * is a fixed linear operator, an approximation of (I - dt K)^{-1}.  FP32
+ * master weights, BF16 tensor-core GEMMs with FP32 accumulation.
  * cell_levels: num_cells x d host ints (the element table's level columns).
  * Weights are initialised from seed. */
 int asgk_mlp_create(asgk_mlp **mlp, int d, int n, int num_cells,
@@ -209,22 +213,36 @@ int asgk_mlp_create(asgk_mlp **mlp, int d, int n, int num_cells,
                     uint64_t seed);
 void asgk_mlp_destroy(asgk_mlp *mlp);
 int asgk_mlp_num_params(const asgk_mlp *mlp, int64_t *count);
-/* Flat FP32 host layout: per layer W (row-major fan_in x fan_out) then b. */
+/* Flat FP32 host layout: W1 (n^d x hidden), W2, W3 (hidden x hidden),
+ * W4 (hidden x n^d), then per gated layer l = 1..3 the gate weights
+ * (d x hidden) and gate biases (hidden); matrices row-major. */
 int asgk_mlp_get_params(const asgk_mlp *mlp, float *params);
 int asgk_mlp_set_params(asgk_mlp *mlp, const float *params);
-/* One forward and backward pass on host rows (X: rows x (n^d + d), targets
- * T: rows x n^d, FP32): outputs Y, loss = 0.5*sum((Y - T)^2) and the
- * gradients in the parameter layout.  Used to check the kernels' gradients. */
+/* One forward and backward pass on host rows (X: rows x (n^d + d), the
+ * residual block then the level features; targets T: rows x n^d; FP32):
+ * outputs Y, loss = 0.5*sum((Y - T)^2) and the gradients in the parameter
+ * layout.  Used to check the kernels' gradients. */
 int asgk_mlp_forward_backward(asgk_mlp *mlp, int rows, const float *X,
                               const float *T, float *Y, float *grads,
                               double *loss);
 /* Trains on num_samples (v, e) vector pairs on the device (sample-major,
  * num_cells*n^d FP64 each, e = (I - dt K)^{-1} v): one row per (sample,
  * cell), mini-batches of `batch` rows, `epochs` passes, Adam(lr).  Reports
- * the last epoch's mean squared error. */
+ * the last epoch's mean squared error.  Targets are e_c/||v_c||. */
 int asgk_mlp_train(asgk_mlp *mlp, const double *v, const double *e,
                    int num_samples, int epochs, int batch, float lr,
                    uint64_t seed, double *final_loss, asgk_stream stream);
+/* Residual-space training on the same (residual, GMRES-correction) pairs
+ * (r_k, e_k), A e_k = r_k, A = I - dt K: minimises
+ * ||A (M r_k - e_k)||^2 / ||r_k||^2 = ||A M r_k - r_k||^2 / ||r_k||^2 per
+ * sample (one Adam step per sample, all cells in one batch).  plan_T holds
+ * K^T on the same pair list (its gradient needs A^T); the operator applies
+ * run in `precision`.  Reports the last epoch's mean loss. */
+int asgk_mlp_train_residual(asgk_mlp *mlp, asgk_plan *plan, asgk_plan *plan_T,
+                            double dt, const double *r, const double *e,
+                            int num_samples, int epochs, float lr,
+                            int precision, uint64_t seed, double *final_loss,
+                            asgk_stream stream);
 /* z = M(v) on device vectors of the plan's size. */
 int asgk_mlp_apply(asgk_mlp *mlp, asgk_plan *plan, const double *v, double *z,
                    asgk_stream stream);

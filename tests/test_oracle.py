@@ -162,17 +162,30 @@ def test_mlp_oracle_gradient_matches_finite_differences():
     differences (it is the checker of the GPU gradients)."""
     from oracle import mlp_oracle
     rng = np.random.default_rng(0)
-    dims = [5, 6, 6, 6, 3]
-    nparams = sum(dims[l] * dims[l + 1] + dims[l + 1] for l in range(4))
+    ts, d, H = 5, 3, 6
+    nparams = sum(int(np.prod(s)) for _, s in mlp_oracle.layout(ts, d, H))
     p = rng.normal(0, 0.5, nparams)
-    X = rng.normal(0, 1, (4, 5))
-    T = rng.normal(0, 1, (4, 3))
-    _, _, g = mlp_oracle.forward_backward(p, dims, X, T)
+    X = rng.normal(0, 1, (4, ts + d))
+    T = rng.normal(0, 1, (4, ts))
+    _, _, g = mlp_oracle.forward_backward(p, ts, d, H, X, T)
     h = 1e-6
-    for i in rng.choice(nparams, 25, replace=False):
+    for i in rng.choice(nparams, 40, replace=False):
         pp, pm = p.copy(), p.copy()
         pp[i] += h
         pm[i] -= h
-        fd = (mlp_oracle.forward_backward(pp, dims, X, T)[1] -
-              mlp_oracle.forward_backward(pm, dims, X, T)[1]) / (2 * h)
+        fd = (mlp_oracle.forward_backward(pp, ts, d, H, X, T)[1] -
+              mlp_oracle.forward_backward(pm, ts, d, H, X, T)[1]) / (2 * h)
         assert abs(fd - g[i]) <= 1e-6 * max(1.0, abs(fd))
+
+
+def test_mlp_oracle_is_linear_in_the_residual():
+    from oracle import mlp_oracle
+    rng = np.random.default_rng(1)
+    ts, d, H = 9, 2, 8
+    nparams = sum(int(np.prod(s)) for _, s in mlp_oracle.layout(ts, d, H))
+    p = rng.normal(0, 0.5, nparams)
+    lam = rng.uniform(0, 1, (3, d))
+    u1, u2 = rng.normal(0, 1, (3, ts)), rng.normal(0, 1, (3, ts))
+    Z = np.zeros((3, ts))
+    f = lambda u: mlp_oracle.forward_backward(p, ts, d, H, np.hstack([u, lam]), Z)[0]
+    assert np.allclose(f(2 * u1 - 3 * u2), 2 * f(u1) - 3 * f(u2), atol=1e-12)
