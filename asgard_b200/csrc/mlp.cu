@@ -228,17 +228,17 @@ __global__ void k_gates(const float *__restrict__ L, int rows, int d,
 }
 
 // Gate gradients: dq = dG * gelu'(Q); gP[k][c] = sum_r L[r][k] dq[r][c],
-// gp[c] = sum_r dq[r][c] (one thread per column c).
-__global__ void k_gate_grad(const float *__restrict__ L, int rows, int d,
-                            const float *__restrict__ Q,
-                            const float *__restrict__ dG, int H,
-                            float *__restrict__ gP, float *__restrict__ gp)
+// gp[c] = sum_r dq[r][c].  One block per column c, the rows split over the
+// block's threads and reduced in shared memory (fixed order).
+__global__ void __launch_bounds__(128)
+    k_gate_grad(const float *__restrict__ L, int rows, int d,
+                const float *__restrict__ Q, const float *__restrict__ dG,
+                int H, float *__restrict__ gP, float *__restrict__ gp)
 {
-  int const c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= H)
-    return;
+  __shared__ float sh[7][128];
+  int const c = blockIdx.x;
   float acc[7] = {0, 0, 0, 0, 0, 0, 0};
-  for (int r = 0; r < rows; r++)
+  for (int r = threadIdx.x; r < rows; r += blockDim.x)
   {
     int64_t const i = int64_t(r) * H + c;
     float const dq  = dG[i] * dgelu(Q[i]);
@@ -246,9 +246,22 @@ __global__ void k_gate_grad(const float *__restrict__ L, int rows, int d,
       acc[k] += L[int64_t(r) * d + k] * dq;
     acc[6] += dq;
   }
-  for (int k = 0; k < d; k++)
-    gP[k * H + c] = acc[k];
-  gp[c] = acc[6];
+  for (int k = 0; k < 7; k++)
+    sh[k][threadIdx.x] = acc[k];
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1)
+  {
+    if (threadIdx.x < o)
+      for (int k = 0; k < 7; k++)
+        sh[k][threadIdx.x] += sh[k][threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+  {
+    for (int k = 0; k < d; k++)
+      gP[k * H + c] = sh[k][0];
+    gp[c] = sh[6][0];
+  }
 }
 
 // dY = (Y - T) * scale as bf16; partial sums of (Y - T)^2 per block
@@ -586,7 +599,7 @@ struct mlp_state
     }
     for (int l = 0; l < 3; l++)
     {
-      k_gate_grad<<<(hidden + 127) / 128, 128, 0, s>>>(
+      k_gate_grad<<<hidden, 128, 0, s>>>(
           Lr, rows, d, Q[l], dG[l], hidden, grads + off_P[l], grads + off_p[l]);
       ASGK_LAUNCHED();
     }

@@ -3,6 +3,8 @@
 // independent FMA chains; the grid covers every SM several times.
 #include "internal.cuh"
 
+#include <algorithm>
+
 namespace asgk
 {
 namespace
@@ -46,15 +48,20 @@ int measure(double *tflops, int iters)
   int const blocks = sms * 8;
   k_fma_peak<T><<<blocks, 256>>>(out, iters / 4, T(0.999999), T(1e-7)); // warm-up
   ASGK_LAUNCHED();
-  ASGK_CUDA(cudaEventRecord(e0));
-  k_fma_peak<T><<<blocks, 256>>>(out, iters, T(0.999999), T(1e-7));
-  ASGK_LAUNCHED();
-  ASGK_CUDA(cudaEventRecord(e1));
-  ASGK_CUDA(cudaEventSynchronize(e1));
-  float ms = 0;
-  ASGK_CUDA(cudaEventElapsedTime(&ms, e0, e1));
   double const flop = 2.0 * 8 * 16 * double(iters) * blocks * 256;
-  *tflops           = flop / (ms * 1e-3) / 1e12;
+  double best = 0;
+  for (int rep = 0; rep < 5; rep++) // best of 5 launches
+  {
+    ASGK_CUDA(cudaEventRecord(e0));
+    k_fma_peak<T><<<blocks, 256>>>(out, iters, T(0.999999), T(1e-7));
+    ASGK_LAUNCHED();
+    ASGK_CUDA(cudaEventRecord(e1));
+    ASGK_CUDA(cudaEventSynchronize(e1));
+    float ms = 0;
+    ASGK_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    best = std::max(best, flop / (ms * 1e-3) / 1e12);
+  }
+  *tflops = best;
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   cudaFree(out);
