@@ -47,7 +47,7 @@ def _load():
     if not os.path.exists(LIB_PATH):
         raise ImportError(
             f"asgard_b200: {LIB_PATH} is missing; build it with "
-            "`python -m asgard_b200.build` (nvcc, sm_100a)")
+            "`python asgard_b200/build.py` (nvcc, sm_100a)")
     lib = C.CDLL(LIB_PATH)
     sig = {
         "asgk_plan_create": ([C.POINTER(_vp), _i, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _i64], _i),

@@ -1,6 +1,6 @@
 """Builds the in-tree CUDA library ``asgard_b200/libasgard_b200.so`` for sm_100a.
 
-    python -m asgard_b200.build          (or: python asgard_b200/build.py)
+    python asgard_b200/build.py
 
 Each source is compiled by nvcc (``-gencode arch=compute_100a,code=sm_100a
 -lineinfo -O3``) in parallel, then linked into one shared library exporting
