@@ -114,40 +114,6 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def dist_setup(args):
-    import torch
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
-                                device_id=torch.device("cuda", local))
-    elif torch.cuda.is_available():
-        torch.cuda.set_device(0)
-    return world, rank, local
-
-
-def barrier(world):
-    import torch
-    if world > 1:
-        import torch.distributed as dist
-        dist.barrier()
-    torch.cuda.synchronize()
-
-
-def max_over_ranks(v, world):
-    import torch
-    if world == 1:
-        return v
-    import torch.distributed as dist
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return t.item()
-
-
 def peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -254,13 +220,14 @@ def main():
     import torch
     import asgard_b200 as ab
 
-    world, rank, local = dist_setup(args)
+    from asgard_b200 import replicas
+    world, rank, local = replicas.init("nccl")
     cfg = WORKLOADS[args.workload]
     d, L, T, dt = cfg["d"], cfg["level"], cfg["terms"], cfg["dt"]
     op = ab.SparseGridOperator(d, L, T, kind=cfg["kind"], nu=cfg["nu"])
     mat = op.kronmult_matrix()
     N = op.N
-    gen = torch.Generator(device="cuda").manual_seed(1000 + rank)
+    gen = torch.Generator(device="cuda").manual_seed(replicas.rhs_seed(rank))
     nb = args.warmup + args.steps
     B = [torch.rand(N, dtype=torch.float64, device="cuda", generator=gen) * 2 - 1
          for _ in range(max(nb, args.plain_steps + 1))]
@@ -305,7 +272,7 @@ def main():
     launches0 = ab.launch_count()
     clocks = ClockSampler(local)
     clocks.start()
-    barrier(world)
+    replicas.barrier()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record()
@@ -314,23 +281,25 @@ def main():
         _, info = solve(B[args.warmup + i], method["precision"], method["precond"])
         minfos.append(info)
     e1.record()
-    barrier(world)
+    replicas.barrier()
     clk = clocks.stop()
     launches = ab.launch_count() - launches0
-    t_method = max_over_ranks(e0.elapsed_time(e1) / 1e3, world)
-    value = world * args.steps / t_method
+    t_local = e0.elapsed_time(e1) / 1e3
+    t_method = replicas.max_over_ranks(t_local)
+    value = replicas.throughput(args.steps, t_local)
 
     # ---- timed: plain FP64 GMRES with the FP64 kronmult
-    barrier(world)
+    replicas.barrier()
     e0.record()
     pinfos = []
     for i in range(args.plain_steps):
         _, info = solve(B[i], "fp64")
         pinfos.append(info)
     e1.record()
-    barrier(world)
-    t_plain = max_over_ranks(e0.elapsed_time(e1) / 1e3, world)
-    plain_value = world * args.plain_steps / t_plain
+    replicas.barrier()
+    t_local = e0.elapsed_time(e1) / 1e3
+    t_plain = replicas.max_over_ranks(t_local)
+    plain_value = replicas.throughput(args.plain_steps, t_local)
 
     # ---- roofline: the dominant kernel (FP64 kronmult, and the FP32 one
     # used inside the method), average launch duration by CUDA events
@@ -363,16 +332,16 @@ def main():
     hb = torch.empty(N, dtype=torch.float64, pin_memory=True)
     hx = torch.empty(N, dtype=torch.float64, pin_memory=True)
     hb.copy_(B[0].cpu())
-    barrier(world)
+    replicas.barrier()
     e0.record()
     for i in range(args.e2e_steps):
         bd = hb.to("cuda", non_blocking=True)
         x, _ = solve(bd, method["precision"], method["precond"])
         hx.copy_(x, non_blocking=True)
     e1.record()
-    barrier(world)
-    t_e2e = max_over_ranks(e0.elapsed_time(e1) / 1e3, world)
-    e2e_value = world * args.e2e_steps / t_e2e
+    replicas.barrier()
+    t_local = e0.elapsed_time(e1) / 1e3
+    e2e_value = replicas.throughput(args.e2e_steps, t_local)
 
     # ---- CPU baseline (rank 0, N = 1): the reference compiled from source
     cpu = None
@@ -422,9 +391,7 @@ def main():
             "cpu_baseline": cpu,
         }
         print(json.dumps(line))
-    if world > 1:
-        import torch.distributed as dist
-        dist.destroy_process_group()
+    replicas.shutdown()
 
 
 def cpu_baseline(op, cfg, iters):
