@@ -1,0 +1,208 @@
+// C++ mirror of the reference's kronmult_matrix<P> and simple_gmres_euler
+// (src/asgard_kronmult_matrix.hpp:111-682, src/solver.hpp:17-41) over the C
+// ABI of asgard_b200.h.  Header-only; link libasgard_b200.so.
+//
+// Differences from the reference types: vectors are std::vector (host) or raw
+// device pointers instead of fk::vector, and only P = double is provided (the
+// FP32 operator is reached through precision arguments).  Errors raise the
+// reference's exception types: std::runtime_error, and std::invalid_argument
+// for a restart larger than the system (src/solver.cpp:175-181).
+#pragma once
+
+#include "asgard_b200.h"
+
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <utility>
+#include <vector>
+
+namespace asgard_b200
+{
+enum class resource
+{
+  host,
+  device
+};
+
+//! gmres_info<P> of src/pde/pde_base.hpp:93-97
+template<typename P>
+struct gmres_info
+{
+  P error;
+  int iterations;
+};
+
+inline void check(int status, char const *what)
+{
+  if (status != ASGK_OK)
+    throw std::runtime_error(std::string(what) + ": " + asgk_status_string(status));
+}
+
+template<typename P>
+class kronmult_matrix;
+
+template<>
+class kronmult_matrix<double>
+{
+public:
+  kronmult_matrix() = default;
+
+  //! Sparse CPU form (src/asgard_kronmult_matrix.hpp:284-297, one chunk):
+  //! CSR over output cells, per-pair factor offsets iA into vA.
+  kronmult_matrix(int num_dimensions, int kron_size, int num_rows,
+                  int num_cols, int num_terms, std::vector<int> const &pntr,
+                  std::vector<int> const &indx, std::vector<int> const &iA,
+                  std::vector<double> const &vA)
+      : d_(num_dimensions), n_(kron_size), rows_(num_rows), cols_(num_cols),
+        terms_(num_terms)
+  {
+    if (pntr.size() != size_t(num_rows) + 1)
+      throw std::runtime_error("kronmult_matrix: pntr must have num_rows + 1 entries");
+    std::vector<int64_t> rp(pntr.begin(), pntr.end());
+    check(asgk_plan_create(&plan_, d_, n_, rows_, cols_, terms_, rp.data(),
+                           indx.data(), iA.data(), vA.data(),
+                           int64_t(vA.size())),
+          "kronmult_matrix");
+  }
+
+  //! Sparse GPU form (src/asgard_kronmult_matrix.hpp:235-272): per pair the
+  //! tensor offsets into y (row_indx) and x (col_indx).
+  static kronmult_matrix from_pairs(int num_dimensions, int kron_size,
+                                    int num_rows, int num_cols, int num_terms,
+                                    std::vector<int> const &row_indx,
+                                    std::vector<int> const &col_indx,
+                                    std::vector<int> const &iA,
+                                    std::vector<double> const &vA)
+  {
+    kronmult_matrix m;
+    m.d_     = num_dimensions;
+    m.n_     = kron_size;
+    m.rows_  = num_rows;
+    m.cols_  = num_cols;
+    m.terms_ = num_terms;
+    if (row_indx.size() != col_indx.size())
+      throw std::runtime_error("kronmult_matrix: row/col index sizes differ");
+    check(asgk_plan_create_pairs(&m.plan_, m.d_, m.n_, m.rows_, m.cols_,
+                                 m.terms_, int64_t(row_indx.size()),
+                                 row_indx.data(), col_indx.data(), iA.data(),
+                                 vA.data(), int64_t(vA.size())),
+          "kronmult_matrix");
+    return m;
+  }
+
+  kronmult_matrix(kronmult_matrix const &) = delete;
+  kronmult_matrix &operator=(kronmult_matrix const &) = delete;
+  kronmult_matrix(kronmult_matrix &&o) noexcept { swap(o); }
+  kronmult_matrix &operator=(kronmult_matrix &&o) noexcept
+  {
+    swap(o);
+    return *this;
+  }
+  ~kronmult_matrix() { asgk_plan_destroy(plan_); }
+
+  //! y = beta*y + alpha*K*x; rec says where x and y live
+  //! (src/asgard_kronmult_matrix.hpp:340-478).  Not thread-safe, as there.
+  template<resource rec = resource::host>
+  void apply(double alpha, double const x[], double beta, double y[]) const
+  {
+    if constexpr (rec == resource::host)
+      check(asgk_apply_host(plan_, alpha, x, beta, y, nullptr), "apply");
+    else
+      check(asgk_apply(plan_, ASGK_FP64, alpha, x, beta, y, nullptr), "apply");
+  }
+
+  int64_t num_batch() const { return info(0); }
+  int tensor_size() const { return compute_tensor_size(d_, n_); }
+  int input_size() const { return int(info(1)); }
+  int output_size() const { return int(info(2)); }
+  //! as the reference's flops(): n^d * n * |iA| (multiply-add counted once)
+  int64_t flops() const { return info(3) / 2; }
+  explicit operator bool() const { return d_ > 0; }
+  bool is_dense() const { return false; }
+  bool is_onecall() const { return true; }
+
+  static int compute_tensor_size(int num_dimensions, int kron_size)
+  {
+    int t = kron_size;
+    for (int i = 1; i < num_dimensions; i++)
+      t *= kron_size;
+    return t;
+  }
+  static int64_t compute_flops(int num_dimensions, int kron_size,
+                               int num_terms, int64_t num_batch)
+  {
+    return int64_t(compute_tensor_size(num_dimensions, kron_size)) *
+           kron_size * num_dimensions * num_terms * num_batch * 2;
+  }
+
+  void update_stored_coefficients(std::vector<double> const &vA)
+  {
+    check(asgk_plan_update_values(plan_, vA.data(), int64_t(vA.size())),
+          "update_stored_coefficients");
+  }
+
+  asgk_plan *plan() const { return plan_; }
+
+private:
+  int64_t info(int which) const
+  {
+    int64_t v[5] = {0, 0, 0, 0, 0};
+    check(asgk_plan_info(plan_, &v[0], &v[1], &v[2], &v[3], &v[4]), "info");
+    return v[which];
+  }
+  void swap(kronmult_matrix &o) noexcept
+  {
+    std::swap(plan_, o.plan_);
+    std::swap(d_, o.d_);
+    std::swap(n_, o.n_);
+    std::swap(rows_, o.rows_);
+    std::swap(cols_, o.cols_);
+    std::swap(terms_, o.terms_);
+  }
+
+  asgk_plan *plan_ = nullptr;
+  int d_ = 0, n_ = 0, rows_ = 0, cols_ = 0, terms_ = 0;
+};
+
+namespace solver
+{
+//! Solves (I - dt*K) x = b on device vectors (x holds the initial guess),
+//! the reference's criterion (absolute tolerance on the estimated residual)
+//! -- src/solver.cpp:119-135.
+inline gmres_info<double>
+simple_gmres_euler(double dt, kronmult_matrix<double> const &mat, double *x,
+                   double const *b, int restart, int max_iter, double tol)
+{
+  int64_t const n = mat.output_size();
+  if (restart > n)
+    throw std::invalid_argument("Number of inner iterations " +
+                                std::to_string(restart) + " must be less than " +
+                                std::to_string(n) + "!");
+  asgk_gmres_info info{};
+  check(asgk_gmres_euler(mat.plan(), dt, x, b, restart, max_iter, tol,
+                         ASGK_TOL_ABS, ASGK_FP64, nullptr, &info, nullptr),
+        "simple_gmres_euler");
+  if (info.status == ASGK_ERR_NONFINITE)
+    throw std::runtime_error("simple_gmres_euler: non-finite residual");
+  return gmres_info<double>{info.error, info.iterations};
+}
+
+//! solver::simple_gmres on a dense column-major host matrix (no
+//! preconditioner) -- src/solver.cpp:55-74.
+inline gmres_info<double> simple_gmres(std::vector<double> const &A,
+                                       std::vector<double> &x,
+                                       std::vector<double> const &b,
+                                       int restart, int max_iter, double tol)
+{
+  int const n = int(b.size());
+  if (restart > n)
+    throw std::invalid_argument("restart larger than the system");
+  asgk_gmres_info info{};
+  check(asgk_gmres_dense(n, A.data(), x.data(), b.data(), restart, max_iter,
+                         tol, &info),
+        "simple_gmres");
+  return gmres_info<double>{info.error, info.iterations};
+}
+} // namespace solver
+} // namespace asgard_b200

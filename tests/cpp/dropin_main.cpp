@@ -1,0 +1,130 @@
+// Drives the C++ drop-in header (include/asgard_b200/kronmult_matrix.hpp) the
+// way reference code would: builds a sparse-grid operator (d = 3, level 4,
+// 2 terms, seeded random factors) in the reference's CPU CSR format, applies
+// it on host and device vectors, solves one backward-Euler step with
+// simple_gmres_euler and one dense system with simple_gmres, and writes
+// inputs and results to a binary file for tests/test_cpp_dropin_gpu.py.
+#include "asgard_b200/kronmult_matrix.hpp"
+
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <fstream>
+#include <random>
+#include <vector>
+
+using namespace asgard_b200;
+
+template<typename T>
+void put(std::ofstream &o, std::vector<T> const &v)
+{
+  int64_t const n = int64_t(v.size());
+  o.write(reinterpret_cast<char const *>(&n), sizeof(n));
+  o.write(reinterpret_cast<char const *>(v.data()), sizeof(T) * v.size());
+}
+
+int main(int argc, char **argv)
+{
+  if (argc < 2)
+    return 2;
+  int const d = 3, L = 4, n = 3, T = 2;
+  int64_t const cells = asgk_sparse_grid(d, L, nullptr);
+  std::vector<int> table(cells * 2 * d);
+  asgk_sparse_grid(d, L, table.data());
+  int64_t nnz = 0;
+  check(asgk_build_pairs(d, L, int(cells), table.data(), &nnz, nullptr,
+                         nullptr, nullptr),
+        "build_pairs");
+  std::vector<int64_t> rp(cells + 1);
+  std::vector<int> col(nnz), conn(nnz * d);
+  check(asgk_build_pairs(d, L, int(cells), table.data(), &nnz, rp.data(),
+                         col.data(), conn.data()),
+        "build_pairs");
+  int nrows1d = 0, nconn = 0;
+  asgk_connect_1d(L, &nrows1d, &nconn, nullptr, nullptr);
+  // reference layout: iA = conn*(d*T*n*n) + (t*d + k)*n*n
+  std::vector<int> iA(nnz * T * d);
+  for (int64_t p = 0; p < nnz; p++)
+    for (int t = 0; t < T; t++)
+      for (int k = 0; k < d; k++)
+        iA[(p * T + t) * d + k] = conn[p * d + k] * d * T * n * n + (t * d + k) * n * n;
+  std::mt19937_64 rng(17);
+  std::uniform_real_distribution<double> U(-1.0, 1.0);
+  std::vector<double> vA(int64_t(nconn) * d * T * n * n);
+  for (auto &v : vA)
+    v = 0.2 * U(rng);
+  std::vector<int> pntr(rp.begin(), rp.end());
+  kronmult_matrix<double> mat(d, n, int(cells), int(cells), T, pntr, col, iA, vA);
+  int const N = mat.output_size();
+
+  std::vector<double> x(N), y_host(N), b(N);
+  for (auto &v : x)
+    v = U(rng);
+  for (auto &v : b)
+    v = U(rng);
+  for (auto &v : y_host)
+    v = U(rng);
+  std::vector<double> y0 = y_host;
+  mat.apply<resource::host>(0.5, x.data(), -2.0, y_host.data());
+
+  double *dx = nullptr, *dy = nullptr, *db = nullptr;
+  cudaMalloc(&dx, sizeof(double) * N);
+  cudaMalloc(&dy, sizeof(double) * N);
+  cudaMalloc(&db, sizeof(double) * N);
+  cudaMemcpy(dx, x.data(), sizeof(double) * N, cudaMemcpyHostToDevice);
+  cudaMemcpy(dy, y0.data(), sizeof(double) * N, cudaMemcpyHostToDevice);
+  mat.apply<resource::device>(0.5, dx, -2.0, dy);
+  std::vector<double> y_dev(N);
+  cudaMemcpy(y_dev.data(), dy, sizeof(double) * N, cudaMemcpyDeviceToHost);
+
+  // one implicit step: (I - dt K) sol = b
+  cudaMemcpy(db, b.data(), sizeof(double) * N, cudaMemcpyHostToDevice);
+  cudaMemset(dx, 0, sizeof(double) * N);
+  auto info = solver::simple_gmres_euler(1e-2, mat, dx, db, 20, 50, 1e-12);
+  std::vector<double> sol(N);
+  cudaMemcpy(sol.data(), dx, sizeof(double) * N, cudaMemcpyDeviceToHost);
+
+  // restart larger than the system must throw std::invalid_argument
+  int threw = 0;
+  try
+  {
+    solver::simple_gmres_euler(1e-2, mat, dx, db, N + 1, 1, 1e-12);
+  }
+  catch (std::invalid_argument const &)
+  {
+    threw = 1;
+  }
+
+  // the 3x3 known answer of the reference solver tests (column-major A)
+  std::vector<double> A = {3.383861628748717e+00, 3.210305545769361e+00, 1.723479266939425e+00,
+                           1.113343240310116e-02, 3.412141162288144e+00, 1.710451084172946e+00,
+                           2.920740795411032e+00, 3.934494120167269e+00, 4.450671104482062e+00};
+  std::vector<double> b3 = {2.084406360034887e-01, 6.444769305362776e-01, 3.687335330031937e-01};
+  std::vector<double> x3(3, 0.0);
+  auto info3 = solver::simple_gmres(A, x3, b3, 3, 3, 2.220446049250313e-16);
+
+  std::ofstream o(argv[1], std::ios::binary);
+  put(o, pntr);
+  put(o, col);
+  put(o, iA);
+  put(o, vA);
+  put(o, x);
+  put(o, y0);
+  put(o, y_host);
+  put(o, y_dev);
+  put(o, b);
+  put(o, sol);
+  put(o, x3);
+  std::vector<double> meta = {double(d), double(n), double(T), double(cells),
+                              info.error, double(info.iterations), double(threw),
+                              info3.error, double(mat.num_batch()),
+                              double(mat.flops()),
+                              double(kronmult_matrix<double>::compute_flops(d, n, T, mat.num_batch()))};
+  put(o, meta);
+  cudaFree(dx);
+  cudaFree(dy);
+  cudaFree(db);
+  std::printf("dropin ok: %d cells, %lld pairs, gmres %d its\n", int(cells),
+              (long long)nnz, info.iterations);
+  return 0;
+}

@@ -1,0 +1,61 @@
+"""The C++ drop-in header, compiled and run as reference code would use it
+(tests/cpp/dropin_main.cpp), checked against the oracle."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import oracle
+from conftest import ROOT, rel_err, rmse_close
+
+pytestmark = pytest.mark.gpu
+
+
+def compile_dropin(exe):
+    libdir = os.path.join(ROOT, "asgard_b200")
+    cuda = "/usr/local/cuda"
+    cmd = ["g++", "-std=c++17", "-O2", os.path.join(ROOT, "tests", "cpp", "dropin_main.cpp"),
+           "-I", os.path.join(ROOT, "include"), "-I", os.path.join(cuda, "include"),
+           "-L", libdir, "-lasgard_b200", "-L", os.path.join(cuda, "lib64"),
+           "-lcudart", f"-Wl,-rpath,{libdir}", f"-Wl,-rpath,{cuda}/lib64",
+           "-o", str(exe)]
+    return subprocess.run(cmd, capture_output=True, text=True)
+
+
+def _read(path):
+    out = []
+    with open(path, "rb") as f:
+        data = f.read()
+    o = 0
+    for dt in [np.int32] * 3 + [np.float64] * 9:
+        n = int(np.frombuffer(data, np.int64, 1, o)[0])
+        o += 8
+        out.append(np.frombuffer(data, dt, n, o).copy())
+        o += n * np.dtype(dt).itemsize
+    return out
+
+
+def test_cpp_dropin_header(cuda, tmp_path):
+    exe = tmp_path / "dropin"
+    r = compile_dropin(exe)
+    assert r.returncode == 0, r.stderr
+    out = tmp_path / "out.bin"
+    subprocess.run([str(exe), str(out)], check=True)
+    pntr, col, iA, vA, x, y0, y_host, y_dev, b, sol, x3, meta = _read(out)
+    d, n, T = int(meta[0]), int(meta[1]), int(meta[2])
+    expect = oracle.kronmult(d, n, pntr, col, T, iA, vA, 0.5, x, -2.0, y0.copy())
+    assert rel_err(y_host, expect) < 1e-13
+    assert rel_err(y_dev, expect) < 1e-13
+    # implicit step: the oracle's GMRES on the same system
+    xo = np.zeros_like(b)
+    _, its_o = oracle.gmres_euler(d, n, pntr, col, T, iA, vA, 1e-2, xo, b,
+                                  20, 50, 1e-12)
+    assert meta[4] <= 1e-12
+    assert abs(int(meta[5]) - its_o) <= 1
+    assert rel_err(sol, xo) < 1e-10
+    assert meta[6] == 1.0                         # std::invalid_argument thrown
+    gold = [4.715561567725287e-02, 1.257695999382253e-01, 1.625351700791827e-02]
+    assert rmse_close(x3, gold, 10 * np.finfo(np.float64).eps)
+    # flops(): reference convention (multiply-add once), compute_flops() x2
+    assert meta[10] == 2 * meta[9]

@@ -109,3 +109,11 @@ def test_default_gmres_restarts():
     assert ab.default_gmres_restarts(1000) == 200
     n = 11789388
     assert ab.default_gmres_restarts(n) == max(10, min(200, int(512 / (n * 8 / 1048576))))
+
+
+def test_cpp_dropin_header_compiles(tmp_path):
+    """The C++ drop-in header and its driver compile and link against the
+    library (running them needs a GPU: tests/test_cpp_dropin_gpu.py)."""
+    from test_cpp_dropin_gpu import compile_dropin
+    r = compile_dropin(tmp_path / "dropin")
+    assert r.returncode == 0, r.stderr
