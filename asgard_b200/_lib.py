@@ -19,6 +19,7 @@ EXPORTS = [
     "asgk_cgs_step", "asgk_cgs_step_noalloc",
     "asgk_sparse_grid", "asgk_connect_1d", "asgk_build_pairs",
     "asgk_status_string", "asgk_launch_count", "asgk_device_info",
+    "asgk_device_status",
     "asgk_measure_fma_peak", "asgk_mlp_create", "asgk_mlp_destroy",
     "asgk_mlp_num_params", "asgk_mlp_get_params", "asgk_mlp_set_params",
     "asgk_mlp_forward_backward", "asgk_mlp_train", "asgk_mlp_apply",
@@ -71,6 +72,7 @@ def _load():
         "asgk_status_string": ([_i], C.c_char_p),
         "asgk_launch_count": ([], _i64),
         "asgk_device_info": ([C.POINTER(_i)] * 3, _i),
+        "asgk_device_status": ([_i], _i),
         "asgk_measure_fma_peak": ([_i, C.POINTER(_d)], _i),
         "asgk_mlp_create": ([C.POINTER(_vp), _i, _i, _i, _vp, _i, _i, C.c_uint64], _i),
         "asgk_mlp_destroy": ([_vp], None),

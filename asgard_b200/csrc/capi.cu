@@ -42,6 +42,7 @@ void free_plan(plan_data &p)
   cudaFree(p.vA32);
   cudaFree(p.xw);
   cudaFree(p.yw);
+  cudaFree(p.xs);
   cudaFree(p.vP64);
   cudaFree(p.vP32);
   p = plan_data{};
@@ -180,6 +181,7 @@ int build_plan(asgk_plan **out, int d, int n, int rows, int cols, int terms,
       (rc = dev_alloc(&p.vA32, std::max<int64_t>(vA_len, 1), B)) ||
       (rc = dev_alloc(&p.xw, std::max<int64_t>(int64_t(cols) * p.tensor, 1), B)) ||
       (rc = dev_alloc(&p.yw, std::max<int64_t>(int64_t(rows) * p.tensor, 1), B)) ||
+      (rc = dev_alloc(&p.xs, int64_t(cols) * p.tensor + 2, B)) ||
       (rc = dev_alloc(&p.vP64, p.nconn * d * terms * 10, B)) ||
       (rc = dev_alloc(&p.vP32, p.nconn * d * terms * 12, B)))
   {
@@ -565,11 +567,22 @@ const char *asgk_status_string(int status)
   case ASGK_ERR_NONFINITE: return "non-finite residual";
   case ASGK_ERR_NOALLOC_LIMIT:
     return "size exceeds the fixed scratch of the allocation-free entry point";
+  case ASGK_ERR_DEVICE_TIMEOUT:
+    return "a kernel's bounded wait on its shared-memory copies expired";
   default: return "unknown status";
   }
 }
 
 int64_t asgk_launch_count(void) { return g_launches.load(); }
+
+int asgk_device_status(int reset)
+{
+  int code = ASGK_OK;
+  ASGK_CUDA(cudaDeviceSynchronize());
+  if (int rc = read_device_error(reset, &code))
+    return rc;
+  return code;
+}
 
 int asgk_device_info(int *sm_count, int *cc_major, int *cc_minor)
 {

@@ -72,6 +72,9 @@ struct plan_data
 
   // FP64 workspace for apply_host and GMRES scratch
   double *xw = nullptr, *yw = nullptr;
+  // 16-byte aligned copy of x (cols*tensor + 2 doubles) for the staged
+  // kernel when the caller's x is not aligned or cols is odd
+  double *xs = nullptr;
   int64_t device_bytes = 0;
 };
 
@@ -88,6 +91,14 @@ namespace asgk
 int launch_apply(plan_data const &p, int precision, double alpha,
                  const void *x, int x_is_f32, double beta, void *y,
                  int y_is_f32, double euler_x_coeff, cudaStream_t s);
+
+// kron_staged.cu: n = 3, d = 3/4 apply with bulk-copied x tensors
+bool staged_supported(plan_data const &p);
+int launch_staged(plan_data const &p, int precision, double alpha,
+                  const double *x, double beta, double *y, double ex,
+                  cudaStream_t s);
+// the device-side error word written by bounded waits that expired
+int read_device_error(int reset, int *code);
 
 // krylov.cu: BLAS-1/2 pieces of the device-resident GMRES
 int launch_fill(double *v, int64_t n, double value, cudaStream_t s);

@@ -468,6 +468,9 @@ int launch_apply(plan_data const &p, int precision, double alpha,
                                          static_cast<float *>(y), ex, euler, s);
   if (x_is_f32 || y_is_f32)
     return ASGK_ERR_INVALID;
+  if (staged_supported(p) && (precision == ASGK_FP64 || precision == ASGK_FP32))
+    return launch_staged(p, precision, alpha, static_cast<const double *>(x),
+                         beta, static_cast<double *>(y), ex, s);
   if (precision == ASGK_FP64)
     return dispatch<double, double, double>(p, p.vA64, alpha,
                                             static_cast<const double *>(x),

@@ -1,0 +1,493 @@
+// Staged kronmult apply for n = 3, d = 3 and 4 (the d = 4, level 7 operator
+// of the implicit-step benchmark runs here).
+//
+// Same operator and row ownership as kron3_rows (kron_kernels.cu); what
+// differs is how data reaches the FMA pipe:
+//
+//   * x tensors are staged in shared memory by the bulk-copy engine
+//     (cp.async.bulk, completion on an mbarrier), two stages per warp, so x
+//     never passes through the load/store unit: the copy of batch b + 2 is in
+//     flight while batch b is contracted.  Every wait is bounded.
+//   * no per-term exchange between lanes.  A pair's tensor is held by a
+//     group of three lanes; lane q holds the slice x[q, :] (dimension 0 = q,
+//     3^(d-1) registers).  Dimensions 1..d-1 are contracted in registers; the
+//     dimension-0 factor is applied as a column: lane q adds A0(i, q) * v to
+//     its partial sums of all three output slices i.  The sum over q (and
+//     over the pairs held by other lanes) is taken once per row, after the
+//     pair loop, by a warp butterfly and a shared-memory sum over warps.
+//     This does the same 2*d*T*3^(d+1) flops per pair as the reference's
+//     kronmult, with 3^d accumulators per lane instead of a transpose of
+//     every pair tensor for every term.
+//
+// Reference operator: kronmult::cpu_sparse, src/device/asgard_spkronmult_cpu.cpp:84-433.
+#include "internal.cuh"
+
+#include <type_traits>
+
+namespace asgk
+{
+__device__ int g_device_error = 0;
+
+namespace
+{
+constexpr int ipow3s(int k) { return k == 0 ? 1 : 3 * ipow3s(k - 1); }
+
+constexpr long long kWaitCycles = 1ll << 31; // about one second at 2 GHz
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p)
+{
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count)
+{
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(count)
+               : "memory");
+}
+
+__device__ __forceinline__ void mbar_init_fence()
+{
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar,
+                                                      uint32_t bytes)
+{
+  asm volatile(
+      "mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(
+          smem_u32(bar)),
+      "r"(bytes)
+      : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
+{
+  uint32_t ok;
+  asm volatile("{\n\t.reg .pred p;\n\t"
+               "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+               "selp.u32 %0, 1, 0, p;\n\t}"
+               : "=r"(ok)
+               : "r"(smem_u32(bar)), "r"(parity)
+               : "memory");
+  return ok != 0;
+}
+
+// Waits until the phase with the given parity has completed, or gives up
+// after kWaitCycles.  The decision is warp-uniform.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar,
+                                                  uint32_t parity)
+{
+  long long const t0 = clock64();
+  while (true)
+  {
+    bool const ok = mbar_try_wait(bar, parity);
+    if (__all_sync(0xffffffffu, ok))
+      return true;
+    if (__any_sync(0xffffffffu, clock64() - t0 > kWaitCycles))
+      return false;
+  }
+}
+
+// global -> shared bulk copy (no multicast), completion counted on bar
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src,
+                                         uint32_t bytes, uint64_t *bar)
+{
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::"
+               "bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+
+// orders this thread's earlier shared-memory accesses before later
+// async-proxy (bulk copy) accesses
+__device__ __forceinline__ void fence_proxy_async_smem()
+{
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+template<int B, int E, typename F>
+__device__ __forceinline__ void sfor(F &&f)
+{
+  if constexpr (B < E)
+  {
+    f(std::integral_constant<int, B>{});
+    sfor<B + 1, E>(f);
+  }
+}
+
+template<typename TC> struct padS;
+template<> struct padS<double> { static constexpr int value = 10; };
+template<> struct padS<float> { static constexpr int value = 12; };
+
+template<typename TC>
+__device__ __forceinline__ void ld9(const TC *__restrict__ A, TC (&a)[9])
+{
+#pragma unroll
+  for (int i = 0; i < 9; i++)
+    a[i] = __ldg(A + i);
+}
+
+__device__ __forceinline__ void ld9p(const double *__restrict__ A, double (&a)[9])
+{
+  const double2 *v = reinterpret_cast<const double2 *>(A);
+#pragma unroll
+  for (int i = 0; i < 4; i++)
+  {
+    double2 const t = __ldg(v + i);
+    a[2 * i]        = t.x;
+    a[2 * i + 1]    = t.y;
+  }
+  a[8] = __ldg(A + 8);
+}
+
+__device__ __forceinline__ void ld9p(const float *__restrict__ A, float (&a)[9])
+{
+  const float4 *v = reinterpret_cast<const float4 *>(A);
+  float4 const t0 = __ldg(v), t1 = __ldg(v + 1);
+  a[0] = t0.x; a[1] = t0.y; a[2] = t0.z; a[3] = t0.w;
+  a[4] = t1.x; a[5] = t1.y; a[6] = t1.z; a[7] = t1.w;
+  a[8] = __ldg(A + 8);
+}
+
+// w <- (I (x) A (x) I) w along the register dimension of stride S
+template<int R, int S, typename TC>
+__device__ __forceinline__ void fibre3(TC (&w)[R], TC const (&a)[9])
+{
+#pragma unroll
+  for (int b = 0; b < R; b++)
+  {
+    if ((b / S) % 3 == 0)
+    {
+      TC const w0 = w[b], w1 = w[b + S], w2 = w[b + 2 * S];
+      w[b]         = fma(a[6], w2, fma(a[3], w1, a[0] * w0));
+      w[b + S]     = fma(a[7], w2, fma(a[4], w1, a[1] * w0));
+      w[b + 2 * S] = fma(a[8], w2, fma(a[5], w1, a[2] * w0));
+    }
+  }
+}
+
+template<int D, int NW, int NS>
+struct staged_shape
+{
+  static constexpr int TS   = ipow3s(D);     // tensor entries (odd)
+  static constexpr int R    = ipow3s(D - 1); // registers per lane
+  static constexpr int G    = 10;            // three-lane groups per warp
+  static constexpr int SLOT = TS + 1;        // doubles per staged tensor (even)
+  static constexpr uint32_t SLOT_BYTES = 8u * SLOT;
+  static constexpr size_t bar_bytes  = size_t(NW) * NS * 8;
+  static constexpr size_t red_off    = (bar_bytes + 127) / 128 * 128;
+  static constexpr size_t xs_off     = (red_off + size_t(NW) * TS * 8 + 127) / 128 * 128;
+  static constexpr size_t smem_bytes = xs_off + size_t(NW) * NS * G * SLOT * 8;
+};
+
+// x must be 16-byte aligned with an even number of column cells: the staged
+// copy of tensor c covers the 16-byte aligned range [x_c rounded down,
+// + 8*(3^d + 1)), which then stays inside x (the launcher copies x to an
+// aligned workspace otherwise).
+template<int D, typename TC, index_mode MODE, bool EULER, int NW, int NS>
+__global__ void __launch_bounds__(NW * 32, 2)
+    kron3_staged(int terms, const int64_t *__restrict__ row_ptr,
+                 const int *__restrict__ row_order, const int *__restrict__ col,
+                 const int *__restrict__ idx, const TC *__restrict__ vF,
+                 double alpha, const double *__restrict__ x, double beta,
+                 double *__restrict__ y, double ex)
+{
+  using S = staged_shape<D, NW, NS>;
+  constexpr int R  = S::R;
+  constexpr int TS = S::TS;
+  constexpr int G  = S::G;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw);
+  TC *red        = reinterpret_cast<TC *>(smem_raw + S::red_off);
+  double *xs     = reinterpret_cast<double *>(smem_raw + S::xs_off);
+
+  int const warp    = threadIdx.x >> 5;
+  int const lane    = threadIdx.x & 31;
+  int const g       = lane / 3;
+  int const q       = lane - 3 * g;
+  bool const laneok = g < G;
+  uint64_t *wbar    = bars + warp * NS;
+  double *wxs       = xs + size_t(warp) * NS * G * S::SLOT;
+
+  int const row      = row_order[blockIdx.x];
+  int64_t const pbeg = row_ptr[row];
+  int64_t const pend = row_ptr[row + 1];
+  int64_t const np   = pend - pbeg;
+  // batches of G consecutive pairs, interleaved over the warps
+  int64_t const first = int64_t(warp) * G;
+  int const nb = (np > first) ? int((np - first + int64_t(NW) * G - 1) / (int64_t(NW) * G)) : 0;
+
+  if (lane == 0)
+  {
+#pragma unroll
+    for (int s = 0; s < NS; s++)
+      mbar_init(wbar + s, 1);
+    mbar_init_fence();
+  }
+  __syncwarp();
+
+  auto issue = [&](int bb) {
+    int const st       = bb % NS;
+    int64_t const pb   = pbeg + (int64_t(bb) * NW + warp) * G;
+    int const nact     = (pend - pb < G) ? int(pend - pb) : G;
+    fence_proxy_async_smem();
+    __syncwarp();
+    if (lane == 0)
+      mbar_arrive_expect_tx(wbar + st, uint32_t(nact) * S::SLOT_BYTES);
+    __syncwarp();
+    if (laneok && q == 0 && g < nact)
+    {
+      const double *src = x + int64_t(__ldg(col + pb + g)) * TS;
+      auto const a0     = reinterpret_cast<uintptr_t>(src) & ~uintptr_t(15);
+      bulk_g2s(wxs + (st * G + g) * S::SLOT,
+               reinterpret_cast<const void *>(a0), S::SLOT_BYTES, wbar + st);
+    }
+  };
+
+  TC acc[3 * R];
+#pragma unroll
+  for (int e = 0; e < 3 * R; e++)
+    acc[e] = TC(0);
+
+  int issued = 0;
+  for (; issued < NS && issued < nb; issued++)
+    issue(issued);
+
+  constexpr int PAD = padS<TC>::value;
+  for (int b = 0; b < nb; b++)
+  {
+    int const st = b % NS;
+    if (!mbar_wait_bounded(wbar + st, uint32_t((b / NS) & 1)))
+    {
+      if (lane == 0)
+        atomicExch(&g_device_error, int(ASGK_ERR_DEVICE_TIMEOUT));
+      // let the copies still in flight land before the CTA's shared memory
+      // is released (bounded as well), then skip the remaining pairs
+      for (int bb = b; bb < issued; bb++)
+        mbar_wait_bounded(wbar + bb % NS, uint32_t((bb / NS) & 1));
+      break;
+    }
+    int64_t const p = pbeg + (int64_t(b) * NW + warp) * G + g;
+    bool const act  = laneok && p < pend;
+    // FP32: the slice lives in registers for all terms and the stage is
+    // refilled at once; FP64 (two registers per value, 3^d accumulators):
+    // the slice is read from the stage at every term, which is refilled
+    // after the batch
+    constexpr bool XREG = sizeof(TC) == 4;
+    TC xr[XREG ? R : 1];
+    int cn[D];
+    const double *sl = wxs;
+    if (act)
+    {
+      int const c = __ldg(col + p);
+      sl          = wxs + (st * G + g) * S::SLOT + (c & 1) + q * R;
+      if constexpr (XREG)
+      {
+#pragma unroll
+        for (int m = 0; m < R; m++)
+          xr[m] = static_cast<TC>(sl[m]);
+      }
+      if constexpr (MODE == index_mode::conn)
+      {
+#pragma unroll
+        for (int k = 0; k < D; k++)
+          cn[k] = __ldg(idx + p * D + k);
+      }
+    }
+    if constexpr (XREG)
+    {
+      if (issued < nb)
+      {
+        issue(issued);
+        issued++;
+      }
+    }
+    if (act)
+    {
+#pragma unroll 1
+      for (int t = 0; t < terms; t++)
+      {
+        TC w[R];
+        if constexpr (XREG)
+        {
+#pragma unroll
+          for (int m = 0; m < R; m++)
+            w[m] = xr[m];
+        }
+        else
+        {
+          volatile const double *vs = sl;
+#pragma unroll
+          for (int m = 0; m < R; m++)
+            w[m] = vs[m];
+        }
+        auto blk = [&](int k) -> const TC * {
+          if constexpr (MODE == index_mode::conn)
+            return vF + ((int64_t(cn[k]) * D + k) * terms + t) * PAD;
+          else
+            return vF + __ldg(idx + (p * terms + t) * D + k);
+        };
+        // dimensions 1..D-1 live in registers: register m <-> (i_1 .. i_{D-1})
+        sfor<1, D>([&](auto kc) {
+          constexpr int k = decltype(kc)::value;
+          TC a[9];
+          // FP64: one factor block live at a time (register budget)
+          if constexpr (!XREG)
+            asm volatile("" ::: "memory");
+          if constexpr (MODE == index_mode::conn)
+            ld9p(blk(k), a);
+          else
+            ld9(blk(k), a);
+          fibre3<R, ipow3s(D - 1 - k)>(w, a);
+        });
+        // dimension 0: this lane holds input slice q; column q of A0
+        // scatters it to the three output slices
+        if constexpr (!XREG)
+          asm volatile("" ::: "memory");
+        const TC *a0 = blk(0) + 3 * q;
+        TC const c0 = __ldg(a0), c1 = __ldg(a0 + 1), c2 = __ldg(a0 + 2);
+#pragma unroll
+        for (int m = 0; m < R; m++)
+        {
+          acc[m]         = fma(c0, w[m], acc[m]);
+          acc[R + m]     = fma(c1, w[m], acc[R + m]);
+          acc[2 * R + m] = fma(c2, w[m], acc[2 * R + m]);
+        }
+      }
+    }
+    if constexpr (!XREG)
+    {
+      // every lane is done with this stage: refill it with batch b + NS
+      if (issued < nb)
+      {
+        issue(issued);
+        issued++;
+      }
+    }
+  }
+
+  // sum the row's partial tensors over the lanes of the warp (through the
+  // warp's stage buffers, idle now: all copies have landed), one output
+  // slice at a time, then over the warps
+  static_assert(32 * R <= NS * G * S::SLOT, "stage buffers too small for the reduction");
+  TC *wred = reinterpret_cast<TC *>(wxs);
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+  {
+    __syncwarp();
+#pragma unroll
+    for (int m = 0; m < R; m++)
+      wred[lane * R + m] = acc[i * R + m]; // odd stride: no bank conflicts
+    __syncwarp();
+    if (lane < R)
+    {
+      TC s = TC(0);
+#pragma unroll 6
+      for (int l = 0; l < 3 * G; l++)
+        s += wred[l * R + lane];
+      red[warp * TS + i * R + lane] = s;
+    }
+  }
+  __syncthreads();
+  int64_t const base = int64_t(row) * TS;
+  for (int i = threadIdx.x; i < TS; i += NW * 32)
+  {
+    TC s = TC(0);
+#pragma unroll
+    for (int ww = 0; ww < NW; ww++)
+      s += red[ww * TS + i];
+    double v = alpha * static_cast<double>(s);
+    if constexpr (EULER)
+      v += ex * x[base + i];
+    if (beta != 0.0)
+      v += beta * y[base + i];
+    y[base + i] = v;
+  }
+}
+
+constexpr int kStagedWarps  = 4;
+constexpr int kStagedStages = 2;
+
+template<int D, typename TC, index_mode MODE, bool EULER>
+int launch_staged_t(plan_data const &p, const TC *vF, double alpha,
+                    const double *x, double beta, double *y, double ex,
+                    cudaStream_t s)
+{
+  using S     = staged_shape<D, kStagedWarps, kStagedStages>;
+  auto kern   = kron3_staged<D, TC, MODE, EULER, kStagedWarps, kStagedStages>;
+  static bool configured = false;
+  if (!configured)
+  {
+    ASGK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   int(S::smem_bytes)));
+    configured = true;
+  }
+  kern<<<p.rows, kStagedWarps * 32, S::smem_bytes, s>>>(
+      p.terms, p.row_ptr, p.row_order, p.col, p.idx, vF, alpha, x, beta, y, ex);
+  ASGK_LAUNCHED();
+  return ASGK_OK;
+}
+
+template<int D, typename TC>
+int launch_staged_d(plan_data const &p, double alpha, const double *x,
+                    double beta, double *y, double ex, cudaStream_t s)
+{
+  const TC *vF;
+  bool const conn = p.mode == index_mode::conn;
+  if constexpr (std::is_same_v<TC, double>)
+    vF = conn ? p.vP64 : p.vA64;
+  else
+    vF = conn ? p.vP32 : p.vA32;
+  bool const euler = ex != 0.0;
+  if (conn)
+    return euler ? launch_staged_t<D, TC, index_mode::conn, true>(p, vF, alpha, x, beta, y, ex, s)
+                 : launch_staged_t<D, TC, index_mode::conn, false>(p, vF, alpha, x, beta, y, ex, s);
+  return euler ? launch_staged_t<D, TC, index_mode::expanded, true>(p, vF, alpha, x, beta, y, ex, s)
+               : launch_staged_t<D, TC, index_mode::expanded, false>(p, vF, alpha, x, beta, y, ex, s);
+}
+
+} // namespace
+
+bool staged_supported(plan_data const &p)
+{
+  return p.n == 3 && (p.d == 3 || p.d == 4) && p.terms > 0 && p.xs != nullptr;
+}
+
+int launch_staged(plan_data const &p, int precision, double alpha,
+                  const double *x, double beta, double *y, double ex,
+                  cudaStream_t s)
+{
+  // the staged copies need a 16-byte aligned x whose last tensor starts on
+  // an odd 8-byte boundary (an even number of column cells); otherwise x is
+  // copied once to the plan's aligned workspace
+  bool const aligned = (reinterpret_cast<uintptr_t>(x) & 15) == 0;
+  if (!aligned || (p.cols & 1))
+  {
+    ASGK_CUDA(cudaMemcpyAsync(p.xs, x, sizeof(double) * int64_t(p.cols) * p.tensor,
+                              cudaMemcpyDeviceToDevice, s));
+    x = p.xs;
+  }
+  if (precision == ASGK_FP64)
+    return (p.d == 3) ? launch_staged_d<3, double>(p, alpha, x, beta, y, ex, s)
+                      : launch_staged_d<4, double>(p, alpha, x, beta, y, ex, s);
+  if (precision == ASGK_FP32)
+    return (p.d == 3) ? launch_staged_d<3, float>(p, alpha, x, beta, y, ex, s)
+                      : launch_staged_d<4, float>(p, alpha, x, beta, y, ex, s);
+  return ASGK_ERR_UNSUPPORTED;
+}
+
+int read_device_error(int reset, int *code)
+{
+  int v = 0;
+  ASGK_CUDA(cudaMemcpyFromSymbol(&v, g_device_error, sizeof(int)));
+  if (reset && v != 0)
+  {
+    int const zero = 0;
+    ASGK_CUDA(cudaMemcpyToSymbol(g_device_error, &zero, sizeof(int)));
+  }
+  *code = v;
+  return ASGK_OK;
+}
+
+} // namespace asgk

@@ -40,7 +40,9 @@ typedef enum asgk_status
   ASGK_ERR_BREAKDOWN   = 5, /* GMRES: zero or non-finite Arnoldi norm */
   ASGK_ERR_NOT_CONVERGED = 6, /* GMRES: iteration limit before tolerance */
   ASGK_ERR_NONFINITE   = 7, /* non-finite residual (NaN/Inf in the data) */
-  ASGK_ERR_NOALLOC_LIMIT = 8 /* request exceeds an allocation-free entry's fixed scratch */
+  ASGK_ERR_NOALLOC_LIMIT = 8, /* request exceeds an allocation-free entry's fixed scratch */
+  ASGK_ERR_DEVICE_TIMEOUT = 9 /* a kernel's bounded wait on its own copies expired;
+                                 the outputs of that launch are invalid */
 } asgk_status;
 
 typedef enum asgk_precision
@@ -270,6 +272,12 @@ int64_t asgk_launch_count(void);
  * for precision ASGK_FP64 or ASGK_FP32: the denominator of the roofline of the
  * CUDA-core kronmult kernels.  No counterpart in the reference. */
 int asgk_measure_fma_peak(int precision, double *tflops);
+/* Reads (and, if reset != 0, clears) the library's device-side error word:
+ * ASGK_OK, or ASGK_ERR_DEVICE_TIMEOUT when a kernel gave up a bounded wait on
+ * its shared-memory copies (it then skips its remaining work and returns,
+ * so the GPU stays usable).  Synchronises the device.  No counterpart in the
+ * reference, whose kernels have no waits. */
+int asgk_device_status(int reset);
 /* Device properties (SM count etc.) for the current device. */
 int asgk_device_info(int *sm_count, int *cc_major, int *cc_minor);
 

@@ -264,3 +264,32 @@ def test_full_size_properties(cuda):
     ye = torch.zeros_like(x1)
     mat.apply_euler(1e-3, 1.0, x1, 0.0, ye)
     assert (torch.linalg.norm(ye - (x1 - 1e-3 * y1)) / torch.linalg.norm(ye)).item() < 1e-14
+
+
+@pytest.mark.parametrize("d,L", [(3, 4), (4, 3), (4, 4)])
+def test_staged_kernel_alignment_and_status(cuda, d, L):
+    """The n = 3, d = 3/4 kernel copies x tensors to shared memory in 16-byte
+    aligned pieces: x views offset by one double and odd or even cell counts
+    (63 / 104 / 192 cells here) take the same result, in FP64 and FP32, and
+    no bounded wait in the kernel expires."""
+    import asgard_b200 as ab
+    import torch
+    op = ab.SparseGridOperator(d, L, d, kind="advdiff", seed=1)
+    rng = np.random.default_rng(11)
+    x = rng.uniform(-1, 1, op.N)
+    y0 = rng.uniform(-1, 1, op.N)
+    expect = oracle.kronmult(d, 3, op.row_ptr.astype(np.int32), op.col, d,
+                             op.iA(), op.vA, -0.4, x, 0.5, y0.copy())
+    for mat in (op.kronmult_matrix(), op.kronmult_matrix(expanded=True)):
+        for off in (0, 1):
+            buf = torch.zeros(op.N + 2, dtype=torch.float64, device="cuda")
+            xd = buf[off:off + op.N]
+            xd.copy_(torch.from_numpy(x))
+            for prec, tol in (("fp64", FP64_TOL), ("fp32", FP32_TOL)):
+                yd = to_dev(y0)
+                mat.apply(-0.4, xd, 0.5, yd, precision=prec)
+                torch.cuda.synchronize()
+                assert rel_err(yd.cpu().numpy(), expect) < tol, (off, prec)
+            # the input is left untouched
+            assert torch.equal(xd.cpu(), torch.from_numpy(x))
+    assert ab.lib.asgk_device_status(1) == 0
