@@ -181,9 +181,9 @@ int build_plan(asgk_plan **out, int d, int n, int rows, int cols, int terms,
       (rc = dev_alloc(&p.vA32, std::max<int64_t>(vA_len, 1), B)) ||
       (rc = dev_alloc(&p.xw, std::max<int64_t>(int64_t(cols) * p.tensor, 1), B)) ||
       (rc = dev_alloc(&p.yw, std::max<int64_t>(int64_t(rows) * p.tensor, 1), B)) ||
-      (rc = dev_alloc(&p.xs, int64_t(cols) * p.tensor + 2, B)) ||
       (rc = dev_alloc(&p.vP64, p.nconn * d * terms * 10, B)) ||
-      (rc = dev_alloc(&p.vP32, p.nconn * d * terms * 12, B)))
+      (rc = dev_alloc(&p.vP32, p.nconn * d * terms * 12, B)) ||
+      (rc = dev_alloc(&p.xs, terms > 0 ? staged_x_doubles(d, n, cols) : 0, B)))
   {
     free_plan(p);
     return rc;

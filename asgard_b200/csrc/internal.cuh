@@ -72,8 +72,7 @@ struct plan_data
 
   // FP64 workspace for apply_host and GMRES scratch
   double *xw = nullptr, *yw = nullptr;
-  // 16-byte aligned copy of x (cols*tensor + 2 doubles) for the staged
-  // kernel when the caller's x is not aligned or cols is odd
+  // x repacked for the staged kernel (n = 3, d = 3/4): padded slices
   double *xs = nullptr;
   int64_t device_bytes = 0;
 };
@@ -94,6 +93,7 @@ int launch_apply(plan_data const &p, int precision, double alpha,
 
 // kron_staged.cu: n = 3, d = 3/4 apply with bulk-copied x tensors
 bool staged_supported(plan_data const &p);
+int64_t staged_x_doubles(int d, int n, int cols); // 0: no staged kernel
 int launch_staged(plan_data const &p, int precision, double alpha,
                   const double *x, double beta, double *y, double ex,
                   cudaStream_t s);

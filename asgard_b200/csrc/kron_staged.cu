@@ -4,10 +4,13 @@
 // Same operator and row ownership as kron3_rows (kron_kernels.cu); what
 // differs is how data reaches the FMA pipe:
 //
-//   * x tensors are staged in shared memory by the bulk-copy engine
-//     (cp.async.bulk, completion on an mbarrier), two stages per warp, so x
-//     never passes through the load/store unit: the copy of batch b + 2 is in
-//     flight while batch b is contracted.  Every wait is bounded.
+//   * x is first repacked (one pass, padded dimension-0 slices, every slice
+//     16-byte aligned), then each pair's tensor is staged in shared memory
+//     by the bulk-copy engine (cp.async.bulk, completion on an mbarrier),
+//     two stages per warp, so x never passes through the load/store unit
+//     and lanes read their slices with conflict-free 128-bit loads; the copy
+//     of the next batch is in flight while a batch is contracted.  Every
+//     wait is bounded.
 //   * no per-term exchange between lanes.  A pair's tensor is held by a
 //     group of three lanes; lane q holds the slice x[q, :] (dimension 0 = q,
 //     3^(d-1) registers).  Dimensions 1..d-1 are contracted in registers; the
@@ -167,48 +170,118 @@ __device__ __forceinline__ void fibre3(TC (&w)[R], TC const (&a)[9])
   }
 }
 
+__device__ __forceinline__ double2 lds_f64x2(uint32_t addr)
+{
+  double2 v;
+  asm volatile("ld.shared.v2.f64 {%0, %1}, [%2];"
+               : "=d"(v.x), "=d"(v.y)
+               : "r"(addr));
+  return v;
+}
+
+// Layout of the staged x tensors.  A tensor's three dimension-0 slices
+// (3^(d-1) doubles each) are stored SP doubles apart (SP even, padded), so
+// every slice starts on a 16-byte boundary and a lane reads its slice with
+// 128-bit loads.  In a shared-memory stage the slot of group g starts at
+// chunk (16-byte unit) slot(g): the slots are packed back to back, each
+// placed at the first chunk whose residue mod 8 is RES[g].  With the three
+// lanes of a group reading slices SP/2 chunks apart, these residues make the
+// eight lanes of every quarter-warp of a 128-bit load hit eight distinct
+// bank groups (no conflicts); they were found by exhaustive search.
+template<int D> struct xlayout;
+template<> struct xlayout<4>
+{
+  static constexpr int SP       = 30;
+  static constexpr int STAGE_CH = 496; // chunks per stage of 10 slots
+  // residues {0, 3, 5, 1, 6, 2, 4, 7, 0, 3}: slot(g) = 45 g + offset(g),
+  // offsets {0, 6, 11, 18, 18, 25, 30, 36, 40, 46} in six bits each
+  __device__ static int slot(int g)
+  {
+    return 45 * g + int((0xba891e65248b180ull >> (6 * g)) & 63);
+  }
+};
+template<> struct xlayout<3>
+{
+  static constexpr int SP       = 10;
+  static constexpr int STAGE_CH = 184;
+  // residues {0, 1, 7, 2, 3, 6, 4, 5, 0, 1}: slot(g) = 15 g + offset(g),
+  // offsets {0, 2, 9, 13, 15, 19, 26, 28, 32, 34}
+  __device__ static int slot(int g)
+  {
+    return 15 * g + int((0x8a071a4cf349080ull >> (6 * g)) & 63);
+  }
+};
+
 template<int D, int NW, int NS>
 struct staged_shape
 {
-  static constexpr int TS   = ipow3s(D);     // tensor entries (odd)
-  static constexpr int R    = ipow3s(D - 1); // registers per lane
-  static constexpr int G    = 10;            // three-lane groups per warp
-  static constexpr int SLOT = TS + 1;        // doubles per staged tensor (even)
-  static constexpr uint32_t SLOT_BYTES = 8u * SLOT;
+  using L = xlayout<D>;
+  static constexpr int TS    = ipow3s(D);     // tensor entries (odd)
+  static constexpr int R     = ipow3s(D - 1); // registers per lane
+  static constexpr int G     = 10;            // three-lane groups per warp
+  static constexpr int SP    = L::SP;
+  static constexpr int XP    = 3 * SP;        // doubles per repacked tensor
+  static constexpr int NCH   = (R + 1) / 2;   // 128-bit reads per slice
+  static constexpr uint32_t COPY_BYTES = 8u * XP;
+  static constexpr int STAGE_CH = L::STAGE_CH; // chunks per stage
+  static_assert(SP >= 2 * NCH, "slice padding too small");
   static constexpr size_t bar_bytes  = size_t(NW) * NS * 8;
   static constexpr size_t red_off    = (bar_bytes + 127) / 128 * 128;
   static constexpr size_t xs_off     = (red_off + size_t(NW) * TS * 8 + 127) / 128 * 128;
-  static constexpr size_t smem_bytes = xs_off + size_t(NW) * NS * G * SLOT * 8;
+  static constexpr size_t smem_bytes = xs_off + size_t(NW) * NS * STAGE_CH * 16;
 };
 
-// x must be 16-byte aligned with an even number of column cells: the staged
-// copy of tensor c covers the 16-byte aligned range [x_c rounded down,
-// + 8*(3^d + 1)), which then stays inside x (the launcher copies x to an
-// aligned workspace otherwise).
+// x (cols tensors of 3^d doubles) -> xp (cols tensors of 3*SP doubles, each
+// dimension-0 slice padded to SP with zeros)
+template<int D>
+__global__ void k_repack_x(const double *__restrict__ x, int64_t cols,
+                           double *__restrict__ xp)
+{
+  constexpr int R  = ipow3s(D - 1);
+  constexpr int SP = xlayout<D>::SP;
+  int64_t const total = cols * 3 * SP;
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < total;
+       i += int64_t(gridDim.x) * blockDim.x)
+  {
+    int64_t const c = i / (3 * SP);
+    int const r     = int(i - c * 3 * SP);
+    int const q     = r / SP;
+    int const m     = r - q * SP;
+    xp[i]           = (m < R) ? x[c * 3 * R + q * R + m] : 0.0;
+  }
+}
+
 template<int D, typename TC, index_mode MODE, bool EULER, int NW, int NS>
 __global__ void __launch_bounds__(NW * 32, 2)
     kron3_staged(int terms, const int64_t *__restrict__ row_ptr,
                  const int *__restrict__ row_order, const int *__restrict__ col,
                  const int *__restrict__ idx, const TC *__restrict__ vF,
-                 double alpha, const double *__restrict__ x, double beta,
+                 double alpha, const double *__restrict__ xp,
+                 const double *__restrict__ x, double beta,
                  double *__restrict__ y, double ex)
 {
   using S = staged_shape<D, NW, NS>;
+  using L = typename S::L;
   constexpr int R  = S::R;
   constexpr int TS = S::TS;
   constexpr int G  = S::G;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw);
   TC *red        = reinterpret_cast<TC *>(smem_raw + S::red_off);
-  double *xs     = reinterpret_cast<double *>(smem_raw + S::xs_off);
+  unsigned char *xs = smem_raw + S::xs_off;
 
   int const warp    = threadIdx.x >> 5;
   int const lane    = threadIdx.x & 31;
   int const g       = lane / 3;
   int const q       = lane - 3 * g;
   bool const laneok = g < G;
+  int const gg      = laneok ? g : 0;
   uint64_t *wbar    = bars + warp * NS;
-  double *wxs       = xs + size_t(warp) * NS * G * S::SLOT;
+  unsigned char *wxs = xs + size_t(warp) * NS * S::STAGE_CH * 16;
+  // this lane's slot and slice, as a byte offset inside a stage
+  uint32_t const slot_off  = uint32_t(L::slot(gg)) * 16u;
+  uint32_t const slice_off = slot_off + uint32_t(q * S::SP) * 8u;
+  uint32_t const wxs_u32   = smem_u32(wxs);
 
   int const row      = row_order[blockIdx.x];
   int64_t const pbeg = row_ptr[row];
@@ -228,20 +301,19 @@ __global__ void __launch_bounds__(NW * 32, 2)
   __syncwarp();
 
   auto issue = [&](int bb) {
-    int const st       = bb % NS;
-    int64_t const pb   = pbeg + (int64_t(bb) * NW + warp) * G;
-    int const nact     = (pend - pb < G) ? int(pend - pb) : G;
+    int const st     = bb % NS;
+    int64_t const pb = pbeg + (int64_t(bb) * NW + warp) * G;
+    int const nact   = (pend - pb < G) ? int(pend - pb) : G;
     fence_proxy_async_smem();
     __syncwarp();
     if (lane == 0)
-      mbar_arrive_expect_tx(wbar + st, uint32_t(nact) * S::SLOT_BYTES);
+      mbar_arrive_expect_tx(wbar + st, uint32_t(nact) * S::COPY_BYTES);
     __syncwarp();
     if (laneok && q == 0 && g < nact)
     {
-      const double *src = x + int64_t(__ldg(col + pb + g)) * TS;
-      auto const a0     = reinterpret_cast<uintptr_t>(src) & ~uintptr_t(15);
-      bulk_g2s(wxs + (st * G + g) * S::SLOT,
-               reinterpret_cast<const void *>(a0), S::SLOT_BYTES, wbar + st);
+      const double *src = xp + int64_t(__ldcs(col + pb + g)) * S::XP;
+      bulk_g2s(wxs + size_t(st) * S::STAGE_CH * 16 + slot_off, src,
+               S::COPY_BYTES, wbar + st);
     }
   };
 
@@ -250,11 +322,19 @@ __global__ void __launch_bounds__(NW * 32, 2)
   for (int e = 0; e < 3 * R; e++)
     acc[e] = TC(0);
 
+  // FP32: a lane's slice lives in registers for all terms, so a stage is
+  // refilled as soon as it has been read (NS batches ahead).  FP64 (two
+  // registers per value, 3^d accumulators): the slice is re-read from the
+  // stage at every term, so the refill targets the stage consumed in the
+  // previous batch (NS - 1 ahead), issued before the contraction.
+  constexpr bool XREG = sizeof(TC) == 4;
+  constexpr int PRE   = XREG ? NS : NS - 1;
+  static_assert(PRE >= 1, "at least one batch of look-ahead");
   int issued = 0;
-  for (; issued < NS && issued < nb; issued++)
+  for (; issued < PRE && issued < nb; issued++)
     issue(issued);
 
-  constexpr int PAD = padS<TC>::value;
+  constexpr int PAD  = padS<TC>::value;
   for (int b = 0; b < nb; b++)
   {
     int const st = b % NS;
@@ -268,31 +348,37 @@ __global__ void __launch_bounds__(NW * 32, 2)
         mbar_wait_bounded(wbar + bb % NS, uint32_t((bb / NS) & 1));
       break;
     }
+    if constexpr (!XREG)
+    {
+      if (issued < nb)
+      {
+        issue(issued);
+        issued++;
+      }
+    }
     int64_t const p = pbeg + (int64_t(b) * NW + warp) * G + g;
     bool const act  = laneok && p < pend;
-    // FP32: the slice lives in registers for all terms and the stage is
-    // refilled at once; FP64 (two registers per value, 3^d accumulators):
-    // the slice is read from the stage at every term, which is refilled
-    // after the batch
-    constexpr bool XREG = sizeof(TC) == 4;
+    uint32_t const sl = wxs_u32 + uint32_t(st) * S::STAGE_CH * 16u + slice_off;
     TC xr[XREG ? R : 1];
     int cn[D];
-    const double *sl = wxs;
     if (act)
     {
-      int const c = __ldg(col + p);
-      sl          = wxs + (st * G + g) * S::SLOT + (c & 1) + q * R;
       if constexpr (XREG)
       {
 #pragma unroll
-        for (int m = 0; m < R; m++)
-          xr[m] = static_cast<TC>(sl[m]);
+        for (int j = 0; j < S::NCH; j++)
+        {
+          double2 const v = lds_f64x2(sl + 16u * j);
+          xr[2 * j] = static_cast<TC>(v.x);
+          if (2 * j + 1 < R)
+            xr[2 * j + 1] = static_cast<TC>(v.y);
+        }
       }
       if constexpr (MODE == index_mode::conn)
       {
 #pragma unroll
         for (int k = 0; k < D; k++)
-          cn[k] = __ldg(idx + p * D + k);
+          cn[k] = __ldcs(idx + p * D + k); // streamed: keep L1 for factors
       }
     }
     if constexpr (XREG)
@@ -317,24 +403,25 @@ __global__ void __launch_bounds__(NW * 32, 2)
         }
         else
         {
-          volatile const double *vs = sl;
 #pragma unroll
-          for (int m = 0; m < R; m++)
-            w[m] = vs[m];
+          for (int j = 0; j < S::NCH; j++)
+          {
+            double2 const v = lds_f64x2(sl + 16u * j);
+            w[2 * j] = v.x;
+            if (2 * j + 1 < R)
+              w[2 * j + 1] = v.y;
+          }
         }
         auto blk = [&](int k) -> const TC * {
           if constexpr (MODE == index_mode::conn)
-            return vF + ((int64_t(cn[k]) * D + k) * terms + t) * PAD;
+            return vF + uint32_t(((cn[k] * D + k) * terms + t) * PAD);
           else
-            return vF + __ldg(idx + (p * terms + t) * D + k);
+            return vF + __ldcs(idx + (p * terms + t) * D + k);
         };
         // dimensions 1..D-1 live in registers: register m <-> (i_1 .. i_{D-1})
         sfor<1, D>([&](auto kc) {
           constexpr int k = decltype(kc)::value;
           TC a[9];
-          // FP64: one factor block live at a time (register budget)
-          if constexpr (!XREG)
-            asm volatile("" ::: "memory");
           if constexpr (MODE == index_mode::conn)
             ld9p(blk(k), a);
           else
@@ -343,8 +430,6 @@ __global__ void __launch_bounds__(NW * 32, 2)
         });
         // dimension 0: this lane holds input slice q; column q of A0
         // scatters it to the three output slices
-        if constexpr (!XREG)
-          asm volatile("" ::: "memory");
         const TC *a0 = blk(0) + 3 * q;
         TC const c0 = __ldg(a0), c1 = __ldg(a0 + 1), c2 = __ldg(a0 + 2);
 #pragma unroll
@@ -356,21 +441,12 @@ __global__ void __launch_bounds__(NW * 32, 2)
         }
       }
     }
-    if constexpr (!XREG)
-    {
-      // every lane is done with this stage: refill it with batch b + NS
-      if (issued < nb)
-      {
-        issue(issued);
-        issued++;
-      }
-    }
   }
 
   // sum the row's partial tensors over the lanes of the warp (through the
   // warp's stage buffers, idle now: all copies have landed), one output
   // slice at a time, then over the warps
-  static_assert(32 * R <= NS * G * S::SLOT, "stage buffers too small for the reduction");
+  static_assert(32 * R * 8 <= NS * S::STAGE_CH * 16, "stage buffers too small for the reduction");
   TC *wred = reinterpret_cast<TC *>(wxs);
 #pragma unroll
   for (int i = 0; i < 3; i++)
@@ -406,16 +482,19 @@ __global__ void __launch_bounds__(NW * 32, 2)
   }
 }
 
-constexpr int kStagedWarps  = 4;
+constexpr int kStagedWarps = 4;
+// two stages per warp: shared memory is carved out of L1, which holds the
+// factor blocks (about 100 KB per output cell at d = 4, level 7)
+template<typename TC>
 constexpr int kStagedStages = 2;
 
 template<int D, typename TC, index_mode MODE, bool EULER>
 int launch_staged_t(plan_data const &p, const TC *vF, double alpha,
-                    const double *x, double beta, double *y, double ex,
-                    cudaStream_t s)
+                    const double *xp, const double *x, double beta, double *y,
+                    double ex, cudaStream_t s)
 {
-  using S     = staged_shape<D, kStagedWarps, kStagedStages>;
-  auto kern   = kron3_staged<D, TC, MODE, EULER, kStagedWarps, kStagedStages>;
+  using S     = staged_shape<D, kStagedWarps, kStagedStages<TC>>;
+  auto kern   = kron3_staged<D, TC, MODE, EULER, kStagedWarps, kStagedStages<TC>>;
   static bool configured = false;
   if (!configured)
   {
@@ -424,7 +503,8 @@ int launch_staged_t(plan_data const &p, const TC *vF, double alpha,
     configured = true;
   }
   kern<<<p.rows, kStagedWarps * 32, S::smem_bytes, s>>>(
-      p.terms, p.row_ptr, p.row_order, p.col, p.idx, vF, alpha, x, beta, y, ex);
+      p.terms, p.row_ptr, p.row_order, p.col, p.idx, vF, alpha, xp, x, beta,
+      y, ex);
   ASGK_LAUNCHED();
   return ASGK_OK;
 }
@@ -433,6 +513,11 @@ template<int D, typename TC>
 int launch_staged_d(plan_data const &p, double alpha, const double *x,
                     double beta, double *y, double ex, cudaStream_t s)
 {
+  using S = staged_shape<D, kStagedWarps, kStagedStages<TC>>;
+  int64_t const total = int64_t(p.cols) * S::XP;
+  int const blocks    = int(std::min<int64_t>((total + 255) / 256, 4096));
+  k_repack_x<D><<<blocks, 256, 0, s>>>(x, p.cols, p.xs);
+  ASGK_LAUNCHED();
   const TC *vF;
   bool const conn = p.mode == index_mode::conn;
   if constexpr (std::is_same_v<TC, double>)
@@ -441,33 +526,36 @@ int launch_staged_d(plan_data const &p, double alpha, const double *x,
     vF = conn ? p.vP32 : p.vA32;
   bool const euler = ex != 0.0;
   if (conn)
-    return euler ? launch_staged_t<D, TC, index_mode::conn, true>(p, vF, alpha, x, beta, y, ex, s)
-                 : launch_staged_t<D, TC, index_mode::conn, false>(p, vF, alpha, x, beta, y, ex, s);
-  return euler ? launch_staged_t<D, TC, index_mode::expanded, true>(p, vF, alpha, x, beta, y, ex, s)
-               : launch_staged_t<D, TC, index_mode::expanded, false>(p, vF, alpha, x, beta, y, ex, s);
+    return euler ? launch_staged_t<D, TC, index_mode::conn, true>(p, vF, alpha, p.xs, x, beta, y, ex, s)
+                 : launch_staged_t<D, TC, index_mode::conn, false>(p, vF, alpha, p.xs, x, beta, y, ex, s);
+  return euler ? launch_staged_t<D, TC, index_mode::expanded, true>(p, vF, alpha, p.xs, x, beta, y, ex, s)
+               : launch_staged_t<D, TC, index_mode::expanded, false>(p, vF, alpha, p.xs, x, beta, y, ex, s);
 }
 
 } // namespace
 
+int64_t staged_x_doubles(int d, int n, int cols)
+{
+  if (n != 3)
+    return 0;
+  if (d == 4)
+    return int64_t(cols) * 3 * xlayout<4>::SP;
+  if (d == 3)
+    return int64_t(cols) * 3 * xlayout<3>::SP;
+  return 0;
+}
+
 bool staged_supported(plan_data const &p)
 {
-  return p.n == 3 && (p.d == 3 || p.d == 4) && p.terms > 0 && p.xs != nullptr;
+  // factor offsets of the repacked blocks are computed in 32 bits
+  return p.n == 3 && (p.d == 3 || p.d == 4) && p.terms > 0 && p.xs != nullptr &&
+         p.nconn * p.d * p.terms * 12 < (int64_t(1) << 31);
 }
 
 int launch_staged(plan_data const &p, int precision, double alpha,
                   const double *x, double beta, double *y, double ex,
                   cudaStream_t s)
 {
-  // the staged copies need a 16-byte aligned x whose last tensor starts on
-  // an odd 8-byte boundary (an even number of column cells); otherwise x is
-  // copied once to the plan's aligned workspace
-  bool const aligned = (reinterpret_cast<uintptr_t>(x) & 15) == 0;
-  if (!aligned || (p.cols & 1))
-  {
-    ASGK_CUDA(cudaMemcpyAsync(p.xs, x, sizeof(double) * int64_t(p.cols) * p.tensor,
-                              cudaMemcpyDeviceToDevice, s));
-    x = p.xs;
-  }
   if (precision == ASGK_FP64)
     return (p.d == 3) ? launch_staged_d<3, double>(p, alpha, x, beta, y, ex, s)
                       : launch_staged_d<4, double>(p, alpha, x, beta, y, ex, s);
