@@ -200,6 +200,40 @@ int build_plan(asgk_plan **out, int d, int n, int rows, int cols, int terms,
     ASGK_CUDA(cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice));
     return ASGK_OK;
   };
+  // For the staged n = 3, d = 3/4 kernel, each row's pairs are ordered by
+  // their factor blocks, the last dimension slowest and dimension 0 fastest:
+  // the ten pairs a warp contracts together then mostly share the blocks of
+  // dimensions 1..d-1 (read whole) and differ in dimension 0 (read as one
+  // column per lane), and a block's reuse distance stays within L1.  The
+  // result changes only by the order of the floating-point sums.
+  std::vector<int> col_sorted, idx_sorted;
+  if (n == 3 && (d == 3 || d == 4) && terms > 0 && nnz > 0)
+  {
+    int64_t const per = (mode == index_mode::conn) ? d : int64_t(terms) * d;
+    col_sorted.resize(nnz);
+    idx_sorted.resize(idx_len);
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int r = 0; r < rows; r++)
+    {
+      int64_t const b = row_ptr[r], e = row_ptr[r + 1];
+      std::vector<int64_t> ord(e - b);
+      std::iota(ord.begin(), ord.end(), b);
+      std::stable_sort(ord.begin(), ord.end(), [&](int64_t u, int64_t v) {
+        for (int k = d - 1; k >= 0; k--)
+          if (idx[u * per + k] != idx[v * per + k])
+            return idx[u * per + k] < idx[v * per + k];
+        return col[u] < col[v];
+      });
+      for (int64_t i = 0; i < e - b; i++)
+      {
+        col_sorted[b + i] = col[ord[i]];
+        std::copy(idx + ord[i] * per, idx + (ord[i] + 1) * per,
+                  idx_sorted.begin() + (b + i) * per);
+      }
+    }
+    col = col_sorted.data();
+    idx = idx_sorted.data();
+  }
   if ((rc = up(p.row_ptr, row_ptr.data(), sizeof(int64_t) * (rows + 1))) ||
       (rc = up(p.col, col, sizeof(int) * nnz)) ||
       (rc = up(p.idx, idx, sizeof(int) * idx_len)) ||

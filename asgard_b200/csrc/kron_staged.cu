@@ -188,10 +188,10 @@ __device__ __forceinline__ double2 lds_f64x2(uint32_t addr)
 // lanes of a group reading slices SP/2 chunks apart, these residues make the
 // eight lanes of every quarter-warp of a 128-bit load hit eight distinct
 // bank groups (no conflicts); they were found by exhaustive search.
-template<int D> struct xlayout;
-template<> struct xlayout<4>
+template<int D, typename T> struct xlayout;
+template<> struct xlayout<4, double>
 {
-  static constexpr int SP       = 30;
+  static constexpr int SP       = 30;  // doubles per slice (15 chunks)
   static constexpr int STAGE_CH = 496; // chunks per stage of 10 slots
   // residues {0, 3, 5, 1, 6, 2, 4, 7, 0, 3}: slot(g) = 45 g + offset(g),
   // offsets {0, 6, 11, 18, 18, 25, 30, 36, 40, 46} in six bits each
@@ -200,7 +200,17 @@ template<> struct xlayout<4>
     return 45 * g + int((0xba891e65248b180ull >> (6 * g)) & 63);
   }
 };
-template<> struct xlayout<3>
+template<> struct xlayout<4, float>
+{
+  static constexpr int SP       = 28;  // floats per slice (7 chunks = 15 mod 8)
+  static constexpr int STAGE_CH = 256;
+  // the same residues and offsets as the FP64 layout
+  __device__ static int slot(int g)
+  {
+    return 21 * g + int((0xba891e65248b180ull >> (6 * g)) & 63);
+  }
+};
+template<> struct xlayout<3, double>
 {
   static constexpr int SP       = 10;
   static constexpr int STAGE_CH = 184;
@@ -211,34 +221,42 @@ template<> struct xlayout<3>
     return 15 * g + int((0x8a071a4cf349080ull >> (6 * g)) & 63);
   }
 };
+template<> struct xlayout<3, float>
+{
+  static constexpr int SP       = 12;  // 3 chunks: residues 0..7, 0, 1
+  static constexpr int STAGE_CH = 96;
+  __device__ static int slot(int g) { return 9 * g; }
+};
 
-template<int D, int NW, int NS>
+template<int D, typename TC, int NW, int NS>
 struct staged_shape
 {
-  using L = xlayout<D>;
+  using L = xlayout<D, TC>;
   static constexpr int TS    = ipow3s(D);     // tensor entries (odd)
   static constexpr int R     = ipow3s(D - 1); // registers per lane
   static constexpr int G     = 10;            // three-lane groups per warp
   static constexpr int SP    = L::SP;
-  static constexpr int XP    = 3 * SP;        // doubles per repacked tensor
-  static constexpr int NCH   = (R + 1) / 2;   // 128-bit reads per slice
-  static constexpr uint32_t COPY_BYTES = 8u * XP;
+  static constexpr int XP    = 3 * SP;        // elements per repacked tensor
+  static constexpr int EPC   = 16 / int(sizeof(TC)); // elements per chunk
+  static constexpr int NCH   = (R + EPC - 1) / EPC;  // 128-bit reads per slice
+  static constexpr uint32_t COPY_BYTES = uint32_t(sizeof(TC)) * XP;
   static constexpr int STAGE_CH = L::STAGE_CH; // chunks per stage
-  static_assert(SP >= 2 * NCH, "slice padding too small");
+  static_assert(SP >= NCH * EPC && (SP * sizeof(TC)) % 16 == 0, "slice padding");
+  static_assert(COPY_BYTES % 16 == 0, "bulk copies move 16-byte multiples");
   static constexpr size_t bar_bytes  = size_t(NW) * NS * 8;
   static constexpr size_t red_off    = (bar_bytes + 127) / 128 * 128;
-  static constexpr size_t xs_off     = (red_off + size_t(NW) * TS * 8 + 127) / 128 * 128;
+  static constexpr size_t xs_off     = (red_off + size_t(NW) * TS * sizeof(TC) + 127) / 128 * 128;
   static constexpr size_t smem_bytes = xs_off + size_t(NW) * NS * STAGE_CH * 16;
 };
 
-// x (cols tensors of 3^d doubles) -> xp (cols tensors of 3*SP doubles, each
-// dimension-0 slice padded to SP with zeros)
-template<int D>
+// x (cols tensors of 3^d doubles) -> xp (cols tensors of 3*SP values of the
+// compute type, each dimension-0 slice padded to SP with zeros)
+template<int D, typename T>
 __global__ void k_repack_x(const double *__restrict__ x, int64_t cols,
-                           double *__restrict__ xp)
+                           T *__restrict__ xp)
 {
   constexpr int R  = ipow3s(D - 1);
-  constexpr int SP = xlayout<D>::SP;
+  constexpr int SP = xlayout<D, T>::SP;
   int64_t const total = cols * 3 * SP;
   for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < total;
        i += int64_t(gridDim.x) * blockDim.x)
@@ -247,20 +265,56 @@ __global__ void k_repack_x(const double *__restrict__ x, int64_t cols,
     int const r     = int(i - c * 3 * SP);
     int const q     = r / SP;
     int const m     = r - q * SP;
-    xp[i]           = (m < R) ? x[c * 3 * R + q * R + m] : 0.0;
+    xp[i]           = (m < R) ? static_cast<T>(x[c * 3 * R + q * R + m]) : T(0);
+  }
+}
+
+__device__ __forceinline__ float4 lds_f32x4(uint32_t addr)
+{
+  float4 v;
+  asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];"
+               : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+               : "r"(addr));
+  return v;
+}
+
+// the R values of a slice at shared address a (128-bit loads)
+template<int R, int NCH>
+__device__ __forceinline__ void load_slice(uint32_t a, double (&w)[R])
+{
+#pragma unroll
+  for (int j = 0; j < NCH; j++)
+  {
+    double2 const v = lds_f64x2(a + 16u * j);
+    w[2 * j] = v.x;
+    if (2 * j + 1 < R)
+      w[2 * j + 1] = v.y;
+  }
+}
+template<int R, int NCH>
+__device__ __forceinline__ void load_slice(uint32_t a, float (&w)[R])
+{
+#pragma unroll
+  for (int j = 0; j < NCH; j++)
+  {
+    float4 const v = lds_f32x4(a + 16u * j);
+    w[4 * j] = v.x;
+    if (4 * j + 1 < R) w[4 * j + 1] = v.y;
+    if (4 * j + 2 < R) w[4 * j + 2] = v.z;
+    if (4 * j + 3 < R) w[4 * j + 3] = v.w;
   }
 }
 
 template<int D, typename TC, index_mode MODE, bool EULER, int NW, int NS>
-__global__ void __launch_bounds__(NW * 32, 2)
+__global__ void __launch_bounds__(NW * 32, sizeof(TC) == 4 ? 3 : 2)
     kron3_staged(int terms, const int64_t *__restrict__ row_ptr,
                  const int *__restrict__ row_order, const int *__restrict__ col,
                  const int *__restrict__ idx, const TC *__restrict__ vF,
-                 double alpha, const double *__restrict__ xp,
+                 double alpha, const TC *__restrict__ xp,
                  const double *__restrict__ x, double beta,
                  double *__restrict__ y, double ex)
 {
-  using S = staged_shape<D, NW, NS>;
+  using S = staged_shape<D, TC, NW, NS>;
   using L = typename S::L;
   constexpr int R  = S::R;
   constexpr int TS = S::TS;
@@ -280,7 +334,7 @@ __global__ void __launch_bounds__(NW * 32, 2)
   unsigned char *wxs = xs + size_t(warp) * NS * S::STAGE_CH * 16;
   // this lane's slot and slice, as a byte offset inside a stage
   uint32_t const slot_off  = uint32_t(L::slot(gg)) * 16u;
-  uint32_t const slice_off = slot_off + uint32_t(q * S::SP) * 8u;
+  uint32_t const slice_off = slot_off + uint32_t(q * S::SP * sizeof(TC));
   uint32_t const wxs_u32   = smem_u32(wxs);
 
   int const row      = row_order[blockIdx.x];
@@ -311,7 +365,7 @@ __global__ void __launch_bounds__(NW * 32, 2)
     __syncwarp();
     if (laneok && q == 0 && g < nact)
     {
-      const double *src = xp + int64_t(__ldcs(col + pb + g)) * S::XP;
+      const TC *src = xp + int64_t(__ldcs(col + pb + g)) * S::XP;
       bulk_g2s(wxs + size_t(st) * S::STAGE_CH * 16 + slot_off, src,
                S::COPY_BYTES, wbar + st);
     }
@@ -364,16 +418,7 @@ __global__ void __launch_bounds__(NW * 32, 2)
     if (act)
     {
       if constexpr (XREG)
-      {
-#pragma unroll
-        for (int j = 0; j < S::NCH; j++)
-        {
-          double2 const v = lds_f64x2(sl + 16u * j);
-          xr[2 * j] = static_cast<TC>(v.x);
-          if (2 * j + 1 < R)
-            xr[2 * j + 1] = static_cast<TC>(v.y);
-        }
-      }
+        load_slice<R, S::NCH>(sl, xr);
       if constexpr (MODE == index_mode::conn)
       {
 #pragma unroll
@@ -402,16 +447,7 @@ __global__ void __launch_bounds__(NW * 32, 2)
             w[m] = xr[m];
         }
         else
-        {
-#pragma unroll
-          for (int j = 0; j < S::NCH; j++)
-          {
-            double2 const v = lds_f64x2(sl + 16u * j);
-            w[2 * j] = v.x;
-            if (2 * j + 1 < R)
-              w[2 * j + 1] = v.y;
-          }
-        }
+          load_slice<R, S::NCH>(sl, w);
         auto blk = [&](int k) -> const TC * {
           if constexpr (MODE == index_mode::conn)
             return vF + uint32_t(((cn[k] * D + k) * terms + t) * PAD);
@@ -446,7 +482,7 @@ __global__ void __launch_bounds__(NW * 32, 2)
   // sum the row's partial tensors over the lanes of the warp (through the
   // warp's stage buffers, idle now: all copies have landed), one output
   // slice at a time, then over the warps
-  static_assert(32 * R * 8 <= NS * S::STAGE_CH * 16, "stage buffers too small for the reduction");
+  static_assert(32 * R * sizeof(TC) <= NS * S::STAGE_CH * 16, "stage buffers too small for the reduction");
   TC *wred = reinterpret_cast<TC *>(wxs);
 #pragma unroll
   for (int i = 0; i < 3; i++)
@@ -484,16 +520,17 @@ __global__ void __launch_bounds__(NW * 32, 2)
 
 constexpr int kStagedWarps = 4;
 // two stages per warp: shared memory is carved out of L1, which holds the
-// factor blocks (about 100 KB per output cell at d = 4, level 7)
+// factor blocks (about 100 KB per output cell at d = 4, level 7); FP32 stages
+// are half the size and three CTAs share an SM
 template<typename TC>
 constexpr int kStagedStages = 2;
 
 template<int D, typename TC, index_mode MODE, bool EULER>
 int launch_staged_t(plan_data const &p, const TC *vF, double alpha,
-                    const double *xp, const double *x, double beta, double *y,
+                    const TC *xp, const double *x, double beta, double *y,
                     double ex, cudaStream_t s)
 {
-  using S     = staged_shape<D, kStagedWarps, kStagedStages<TC>>;
+  using S     = staged_shape<D, TC, kStagedWarps, kStagedStages<TC>>;
   auto kern   = kron3_staged<D, TC, MODE, EULER, kStagedWarps, kStagedStages<TC>>;
   static bool configured = false;
   if (!configured)
@@ -513,10 +550,11 @@ template<int D, typename TC>
 int launch_staged_d(plan_data const &p, double alpha, const double *x,
                     double beta, double *y, double ex, cudaStream_t s)
 {
-  using S = staged_shape<D, kStagedWarps, kStagedStages<TC>>;
+  using S = staged_shape<D, TC, kStagedWarps, kStagedStages<TC>>;
   int64_t const total = int64_t(p.cols) * S::XP;
   int const blocks    = int(std::min<int64_t>((total + 255) / 256, 4096));
-  k_repack_x<D><<<blocks, 256, 0, s>>>(x, p.cols, p.xs);
+  TC *xp              = reinterpret_cast<TC *>(p.xs);
+  k_repack_x<D, TC><<<blocks, 256, 0, s>>>(x, p.cols, xp);
   ASGK_LAUNCHED();
   const TC *vF;
   bool const conn = p.mode == index_mode::conn;
@@ -526,10 +564,10 @@ int launch_staged_d(plan_data const &p, double alpha, const double *x,
     vF = conn ? p.vP32 : p.vA32;
   bool const euler = ex != 0.0;
   if (conn)
-    return euler ? launch_staged_t<D, TC, index_mode::conn, true>(p, vF, alpha, p.xs, x, beta, y, ex, s)
-                 : launch_staged_t<D, TC, index_mode::conn, false>(p, vF, alpha, p.xs, x, beta, y, ex, s);
-  return euler ? launch_staged_t<D, TC, index_mode::expanded, true>(p, vF, alpha, p.xs, x, beta, y, ex, s)
-               : launch_staged_t<D, TC, index_mode::expanded, false>(p, vF, alpha, p.xs, x, beta, y, ex, s);
+    return euler ? launch_staged_t<D, TC, index_mode::conn, true>(p, vF, alpha, xp, x, beta, y, ex, s)
+                 : launch_staged_t<D, TC, index_mode::conn, false>(p, vF, alpha, xp, x, beta, y, ex, s);
+  return euler ? launch_staged_t<D, TC, index_mode::expanded, true>(p, vF, alpha, xp, x, beta, y, ex, s)
+               : launch_staged_t<D, TC, index_mode::expanded, false>(p, vF, alpha, xp, x, beta, y, ex, s);
 }
 
 } // namespace
@@ -538,10 +576,11 @@ int64_t staged_x_doubles(int d, int n, int cols)
 {
   if (n != 3)
     return 0;
+  // sized for the FP64 staging (the FP32 one is smaller)
   if (d == 4)
-    return int64_t(cols) * 3 * xlayout<4>::SP;
+    return int64_t(cols) * 3 * xlayout<4, double>::SP;
   if (d == 3)
-    return int64_t(cols) * 3 * xlayout<3>::SP;
+    return int64_t(cols) * 3 * xlayout<3, double>::SP;
   return 0;
 }
 
