@@ -23,7 +23,9 @@ EXPORTS = [
     "asgk_measure_fma_peak", "asgk_mlp_create", "asgk_mlp_destroy",
     "asgk_mlp_num_params", "asgk_mlp_get_params", "asgk_mlp_set_params",
     "asgk_mlp_forward_backward", "asgk_mlp_train", "asgk_mlp_apply",
-    "asgk_mlp_train_residual",
+    "asgk_mlp_train_residual", "asgk_jacobi_create", "asgk_jacobi_destroy",
+    "asgk_jacobi_apply", "asgk_jacobi_info", "asgk_gmres_euler_jacobi",
+    "asgk_mlp_set_base",
 ]
 
 
@@ -82,6 +84,12 @@ def _load():
         "asgk_mlp_forward_backward": ([_vp, _i, _vp, _vp, _vp, _vp, C.POINTER(_d)], _i),
         "asgk_mlp_train": ([_vp, _vp, _vp, _i, _i, _i, C.c_float, C.c_uint64, C.POINTER(_d), _vp], _i),
         "asgk_mlp_apply": ([_vp, _vp, _vp, _vp, _vp], _i),
+        "asgk_jacobi_create": ([C.POINTER(_vp), _vp, _d, _i], _i),
+        "asgk_jacobi_destroy": ([_vp], None),
+        "asgk_mlp_set_base": ([_vp, _vp], _i),
+        "asgk_jacobi_apply": ([_vp, _vp, _vp, _vp], _i),
+        "asgk_jacobi_info": ([_vp, C.POINTER(_i), C.POINTER(_d), C.POINTER(_i64)], _i),
+        "asgk_gmres_euler_jacobi": ([_vp, _d, _vp, _vp, _i, _i, _d, _i, _i, _vp, C.POINTER(GmresInfo), _vp], _i),
         "asgk_mlp_train_residual": ([_vp, _vp, _vp, _d, _vp, _vp, _i, _i, C.c_float, _i, C.c_uint64, C.POINTER(_d), _vp], _i),
     }
     for name, (args, res) in sig.items():

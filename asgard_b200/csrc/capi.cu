@@ -907,10 +907,19 @@ int asgk_default_gmres_restarts(int64_t n)
   return std::clamp(want, minimum, maximum);
 }
 
-int asgk_gmres_euler(asgk_plan *plan, double dt, double *x, const double *b,
+} // extern "C"
+
+namespace asgk
+{
+// The solve behind asgk_gmres_euler*: pc (or nullptr) is the right
+// preconditioner of the flexible GMRES, given whether the inner operator is
+// the low-precision one.
+using make_pc_t = std::function<precond_t(bool low)>;
+
+int gmres_euler_impl(asgk_plan *plan, double dt, double *x, const double *b,
                      int restart, int max_outer, double tol, int tol_mode,
-                     int precision, asgk_mlp *precond, asgk_gmres_info *info,
-                     asgk_stream stream)
+                     int precision, make_pc_t const *make_pc,
+                     asgk_gmres_info *info, asgk_stream stream)
 {
   if (!plan || !x || !b)
     return ASGK_ERR_INVALID;
@@ -941,13 +950,12 @@ int asgk_gmres_euler(asgk_plan *plan, double dt, double *x, const double *b,
   };
   precond_t pcf;
   precond_t const *pcp = nullptr;
-  if (precond != nullptr)
+  if (make_pc != nullptr)
   {
-    pcf = [&](const double *v, double *z) -> int {
-      return mlp_precondition(precond, plan, v, z, s);
-    };
+    pcf = (*make_pc)(precision != ASGK_FP64);
     pcp = &pcf;
   }
+  bool const precond = pcp != nullptr;
 
   double bnorm = 0;
   if (ws.ensure(n, restart, pcp != nullptr) != ASGK_OK)
@@ -959,7 +967,7 @@ int asgk_gmres_euler(asgk_plan *plan, double dt, double *x, const double *b,
   core_stats st;
   int status = ASGK_OK;
   double true_res = -1; // FP64 residual of the final x when already known
-  if (precision == ASGK_FP64 && precond == nullptr)
+  if (precision == ASGK_FP64 && !precond)
   {
     if (int rc = gmres_core(ws, n, op64, nullptr, x, b, restart, max_outer,
                             tol_abs, st, s, tol_mode == ASGK_TOL_REL))
@@ -1076,6 +1084,47 @@ int asgk_gmres_euler(asgk_plan *plan, double dt, double *x, const double *b,
   if (info)
     *info = out;
   return ASGK_OK;
+}
+
+} // namespace asgk
+
+extern "C"
+{
+
+int asgk_gmres_euler(asgk_plan *plan, double dt, double *x, const double *b,
+                     int restart, int max_outer, double tol, int tol_mode,
+                     int precision, asgk_mlp *precond, asgk_gmres_info *info,
+                     asgk_stream stream)
+{
+  if (precond == nullptr)
+    return gmres_euler_impl(plan, dt, x, b, restart, max_outer, tol, tol_mode,
+                            precision, nullptr, info, stream);
+  cudaStream_t s = as_stream(stream);
+  make_pc_t const mk = [&](bool low) -> precond_t {
+    return [=](const double *v, double *z) -> int {
+      return mlp_precondition(precond, plan, v, z, s, low);
+    };
+  };
+  return gmres_euler_impl(plan, dt, x, b, restart, max_outer, tol, tol_mode,
+                          precision, &mk, info, stream);
+}
+
+int asgk_gmres_euler_jacobi(asgk_plan *plan, double dt, double *x,
+                            const double *b, int restart, int max_outer,
+                            double tol, int tol_mode, int precision,
+                            asgk_jacobi *precond, asgk_gmres_info *info,
+                            asgk_stream stream)
+{
+  if (precond == nullptr)
+    return ASGK_ERR_INVALID;
+  cudaStream_t s = as_stream(stream);
+  make_pc_t const mk = [&](bool low) -> precond_t {
+    return [=](const double *v, double *z) -> int {
+      return jacobi_apply_handle(precond, low, v, z, s);
+    };
+  };
+  return gmres_euler_impl(plan, dt, x, b, restart, max_outer, tol, tol_mode,
+                          precision, &mk, info, stream);
 }
 
 } // extern "C"

@@ -91,6 +91,13 @@ int launch_apply(plan_data const &p, int precision, double alpha,
                  const void *x, int x_is_f32, double beta, void *y,
                  int y_is_f32, double euler_x_coeff, cudaStream_t s);
 
+// jacobi.cu
+struct jacobi_data;
+int jacobi_apply(jacobi_data const &jd, bool low, const double *v, double *z,
+                 cudaStream_t s);
+int jacobi_apply_handle(asgk_jacobi *pc, bool low, const double *v, double *z,
+                        cudaStream_t s);
+
 // kron_staged.cu: n = 3, d = 3/4 apply with bulk-copied x tensors
 bool staged_supported(plan_data const &p);
 int64_t staged_x_doubles(int d, int n, int cols); // 0: no staged kernel

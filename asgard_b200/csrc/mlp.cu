@@ -345,20 +345,21 @@ __global__ void k_pc_features(const double *__restrict__ v, int cells, int ts,
     s[c] = (nrm > 0) ? nrm : 0.0;
 }
 
-// z_c = s_c * y_c.  The network predicts the correction itself, not its
-// difference from v: for a stiff cell the correction is a small multiple of
-// v_c, and forming it as v_c + (a BF16 quantity close to -v_c) would cancel
-// away all of its digits.
+// z_c = s_c * y_c (+ z_c when a base preconditioner's output is already in
+// z).  The network predicts the correction itself, not its difference from
+// v: for a stiff cell the correction is a small multiple of v_c, and forming
+// it as v_c + (a BF16 quantity close to -v_c) would cancel away all of its
+// digits.
 __global__ void k_pc_output(const float *__restrict__ y, int cells, int ts,
                             const double *__restrict__ s,
                             const double *__restrict__ v,
-                            double *__restrict__ z)
+                            double *__restrict__ z, int accumulate)
 {
   (void)v;
   int64_t const n = int64_t(cells) * ts;
   for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n;
        i += int64_t(gridDim.x) * blockDim.x)
-    z[i] = s[i / ts] * double(y[i]);
+    z[i] = (accumulate ? z[i] : 0.0) + s[i / ts] * double(y[i]);
 }
 
 // Training rows from (v, e) cell pairs: U = v_c/s_c, levels, and the target
@@ -471,6 +472,7 @@ struct mlp_state
   int *rows_cell = nullptr;          // identity map cell -> row for inference
   int64_t step = 0;
   float weight_decay = 0.05f;
+  asgk_jacobi *base = nullptr;       // z = base(v) + network(v) when set
   std::vector<void *> owned;
 
   float *W(int l) { return params + off_W[l]; }
@@ -620,20 +622,24 @@ struct mlp_state
 };
 
 int mlp_precondition(asgk_mlp *mlp, asgk_plan *plan, const double *v,
-                     double *z, cudaStream_t s)
+                     double *z, cudaStream_t s, bool low)
 {
   auto *m = reinterpret_cast<mlp_state *>(mlp);
   if (!m || !plan || plan->p.rows != m->cells || plan->p.tensor != m->ts)
     return ASGK_ERR_INVALID;
   if (int rc = m->ensure_rows(m->cells))
     return rc;
+  if (m->base)
+    if (int rc = jacobi_apply_handle(m->base, low, v, z, s))
+      return rc;
   k_pc_features<<<m->cells, 128, 0, s>>>(v, m->cells, m->ts, m->d, m->lev,
                                          m->U, m->Lr, m->scale);
   ASGK_LAUNCHED();
   if (int rc = m->forward(m->cells, s))
     return rc;
   int64_t const n = int64_t(m->cells) * m->ts;
-  k_pc_output<<<grid1(n), 256, 0, s>>>(m->Y, m->cells, m->ts, m->scale, v, z);
+  k_pc_output<<<grid1(n), 256, 0, s>>>(m->Y, m->cells, m->ts, m->scale, v, z,
+                                       m->base != nullptr);
   ASGK_LAUNCHED();
   return ASGK_OK;
 }
@@ -960,7 +966,7 @@ int asgk_mlp_train_residual(asgk_mlp *mlp, asgk_plan *plan, asgk_plan *plan_T,
       count_launch();
       if ((rc = m->forward(m->cells, s)))
         break;
-      k_pc_output<<<gb, 256, 0, s>>>(m->Y, m->cells, m->ts, m->scale, rk, z);
+      k_pc_output<<<gb, 256, 0, s>>>(m->Y, m->cells, m->ts, m->scale, rk, z, 0);
       k_sub<<<gb, 256, 0, s>>>(z, ek, dv, N);
       if (cudaGetLastError() != cudaSuccess)
       {
@@ -994,11 +1000,21 @@ int asgk_mlp_train_residual(asgk_mlp *mlp, asgk_plan *plan, asgk_plan *plan_T,
   return rc;
 }
 
+int asgk_mlp_set_base(asgk_mlp *mlp, asgk_jacobi *base)
+{
+  auto *m = reinterpret_cast<mlp_state *>(mlp);
+  if (!m)
+    return ASGK_ERR_INVALID;
+  m->base = base;
+  return ASGK_OK;
+}
+
 // z = M(v) for a full vector of cells*n^d values (device pointers).
 int asgk_mlp_apply(asgk_mlp *mlp, asgk_plan *plan, const double *v, double *z,
                    asgk_stream stream)
 {
-  return mlp_precondition(mlp, plan, v, z, static_cast<cudaStream_t>(stream));
+  return mlp_precondition(mlp, plan, v, z, static_cast<cudaStream_t>(stream),
+                          false);
 }
 
 } // extern "C"

@@ -5,7 +5,8 @@
 
 namespace asgk
 {
-// z = M(v): applies the network cell by cell to the FP64 Krylov vector v.
+// z = M(v): applies the network cell by cell to the FP64 Krylov vector v
+// (plus its base preconditioner, from its FP32 copy when low is set).
 int mlp_precondition(asgk_mlp *mlp, asgk_plan *plan, const double *v,
-                     double *z, cudaStream_t s);
+                     double *z, cudaStream_t s, bool low);
 } // namespace asgk

@@ -216,14 +216,17 @@ def simple_gmres_euler(dt, mat: kronmult_matrix, x, b, restart=-1,
     tol_mode="abs" is the reference criterion (estimated residual <= tol);
     "rel" stops at tol * ||b||.  precision "fp32"/"bf16" runs the Krylov
     operator in that arithmetic inside FP64 iterative refinement.  precond is
-    a learned preconditioner (asgard_b200.precond.LearnedPreconditioner) used
-    on the right through flexible GMRES."""
+    a preconditioner of asgard_b200.precond (JacobiPreconditioner or
+    LearnedPreconditioner) used on the right through flexible GMRES."""
+    from .precond import JacobiPreconditioner
     n = mat.output_size()
     if restart is not None and restart > n:
         raise ValueError(f"Number of inner iterations {restart} must be less than {n}!")
     info = GmresInfo()
     pc = precond.handle if precond is not None else None
-    rc = lib.asgk_gmres_euler(mat.handle, dt, _ptr(x), _ptr(b),
+    entry = (lib.asgk_gmres_euler_jacobi if isinstance(precond, JacobiPreconditioner)
+             else lib.asgk_gmres_euler)
+    rc = entry(mat.handle, dt, _ptr(x), _ptr(b),
                               -1 if restart is None else restart,
                               -1 if max_iter is None else max_iter, tol,
                               TOL_REL if tol_mode == "rel" else TOL_ABS,

@@ -1,5 +1,15 @@
-"""Learned preconditioner: a per-cell network trained on the GPU from plain
-GMRES solves, used on the right inside (flexible) GMRES.  The network is
+"""Preconditioners of the backward-Euler operator, used on the right inside
+(flexible) GMRES.
+
+JacobiPreconditioner: the reference's diagonal preconditioner
+(build_preconditioner, src/asgard_kronmult_matrix.cpp:1015-1067) or the
+inverse of each cell's whole diagonal block, built on the device.
+
+    pc = JacobiPreconditioner(mat, dt, kind="block")
+    info = simple_gmres_euler(dt, mat, x, b, ..., precond=pc)
+
+LearnedPreconditioner: a per-cell network trained on the GPU from plain
+GMRES solves.  The network is
 linear in the residual block and gated by the cell's levels (see
 include/asgard_b200.h), so the preconditioner is a fixed linear operator.
 
@@ -23,6 +33,44 @@ from ._lib import check, lib
 
 _MAGIC = b"ASGKMLP1"
 
+JACOBI_KINDS = {"point": 0, "block": 1}
+
+
+class JacobiPreconditioner:
+    """Point or cell-block Jacobi preconditioner of I - dt*K for a square
+    kronmult_matrix (see asgk_jacobi_create in include/asgard_b200.h)."""
+
+    def __init__(self, mat, dt, kind="block"):
+        if kind not in JACOBI_KINDS:
+            raise ValueError(f"kind must be one of {sorted(JACOBI_KINDS)}")
+        h = C.c_void_p()
+        check(lib.asgk_jacobi_create(C.byref(h), mat.handle, float(dt),
+                                     JACOBI_KINDS[kind]), "jacobi_create")
+        self._h = h
+        self.kind, self.dt = kind, float(dt)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            lib.asgk_jacobi_destroy(h)
+            self._h = None
+
+    @property
+    def handle(self):
+        return self._h
+
+    def device_bytes(self):
+        b = C.c_int64()
+        check(lib.asgk_jacobi_info(self._h, None, None, C.byref(b)))
+        return b.value
+
+    def apply(self, v, z, stream=None):
+        """z = M v on CUDA float64 tensors."""
+        from .kronmult import _ptr, _stream
+        check(lib.asgk_jacobi_apply(self._h, _ptr(v), _ptr(z), _stream(stream)),
+              "jacobi_apply")
+        return z
+
 
 class LearnedPreconditioner:
     def __init__(self, op=None, *, d=None, n=3, table=None, level=None,
@@ -40,6 +88,14 @@ class LearnedPreconditioner:
         self._h = h
         self.dims = [n ** d, hidden, hidden, hidden, n ** d]
         self.useful = None   # set by validate()
+        self.base = None
+
+    def set_base(self, base):
+        """Preconditioner base(v) + network(v): the network learns a
+        correction to a JacobiPreconditioner (None removes it)."""
+        check(lib.asgk_mlp_set_base(self._h, base.handle if base is not None else None),
+              "mlp_set_base")
+        self.base = base      # kept alive with the network
 
     def __del__(self):
         h = getattr(self, "_h", None)
@@ -147,6 +203,13 @@ class LearnedPreconditioner:
         else:
             V, E = samples
             its = []
+        if self.base is not None:
+            # the network learns what the base misses: e - base(r)
+            E = E.clone()
+            z = torch.empty_like(E[0])
+            for i in range(V.shape[0]):
+                self.base.apply(V[i], z)
+                E[i] -= z
         loss = C.c_double()
         stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
         check(lib.asgk_mlp_train(self._h, C.c_void_p(V.data_ptr()),
@@ -168,22 +231,24 @@ class LearnedPreconditioner:
 
     def validate(self, mat, dt, seed=0, restart=50, tol=1e-10):
         """Solves one held-out right-hand side with and without the network
-        (FP64, relative tolerance) and records whether it reduced the
-        iteration count; ``useful`` is False when it did not, and callers
-        then fall back to plain GMRES (the solver also drops a network that
-        stalls a solve)."""
+        (FP64, relative tolerance; "without" keeps the base preconditioner
+        when one is set) and records whether it reduced the iteration count;
+        ``useful`` is False when it did not, and callers then fall back to
+        the method without it (the solver also drops a network that stalls a
+        solve)."""
         import torch
         from .kronmult import simple_gmres_euler
         N = mat.output_size()
         g = torch.Generator(device="cuda").manual_seed(seed)
         b = torch.rand(N, dtype=torch.float64, device="cuda", generator=g) * 2 - 1
         plain = simple_gmres_euler(dt, mat, torch.zeros_like(b), b, restart,
-                                   400, tol, tol_mode="rel")
+                                   400, tol, tol_mode="rel", precond=self.base)
         learned = simple_gmres_euler(dt, mat, torch.zeros_like(b), b, restart,
                                      400, tol, tol_mode="rel", precond=self)
         self.useful = (learned.status == 0 and learned.fallback == 0 and
                        learned.iterations < plain.iterations)
-        return {"plain_iterations": plain.iterations,
+        return {"baseline": "block-jacobi" if self.base is not None else "none",
+                "plain_iterations": plain.iterations,
                 "learned_iterations": learned.iterations,
                 "learned_fallback": learned.fallback,
                 "gain": plain.iterations / max(learned.iterations, 1),

@@ -52,8 +52,10 @@ def parse():
     ap.add_argument("--plain-steps", type=int, default=2)
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--method", default="learned-fp32",
-                    choices=["learned-fp32", "learned-fp64", "fp32", "fp64"])
+    ap.add_argument("--method", default="learned-block-fp32",
+                    choices=["learned-block-fp32", "learned-block-fp64",
+                             "block-fp32", "block-fp64", "learned-fp32",
+                             "learned-fp64", "fp32", "fp64"])
     ap.add_argument("--train-solves", type=int, default=1)
     ap.add_argument("--train-epochs", type=int, default=60)
     return ap.parse_args()
@@ -191,8 +193,8 @@ def reference_arm(args):
 PLAIN_ITERATIONS = {"d4": 230}
 
 # DRAM bytes per launch of the dominant kernel from one ncu capture
-# (profiles/kron3_rows_d4_L7_fp64.md); None where none was taken.
-KERNEL_TRAFFIC = {"d4": 251_761_664 + 5_670_144}
+# (profiles/kron3_staged_d4_L7_fp64.md); None where none was taken.
+KERNEL_TRAFFIC = {"d4": 254_243_328 + 4_232_704}
 
 
 def _plain_iterations(workload):
@@ -232,27 +234,41 @@ def main():
     B = [torch.rand(N, dtype=torch.float64, device="cuda", generator=gen) * 2 - 1
          for _ in range(max(nb, args.plain_steps + 1))]
     precision = "fp64" if args.method.endswith("fp64") else "fp32"
-    pc, train_info = None, None
+    # setup, not timed (like building the operator): the block-Jacobi
+    # inverses (cells with n^d <= 81) and the learned network's training
+    base = None
+    if "block" in args.method and 3 ** d <= 81:
+        base = ab.JacobiPreconditioner(mat, dt, kind="block")
+    pc, train_info = base, None
     if args.method.startswith("learned"):
-        # setup, not timed (like building the operator): plain FP64 GMRES
-        # solves of random right-hand sides give (v, e) pairs, one row per
-        # cell, and the network trains on them on this GPU
+        # plain FP64 GMRES solves of random right-hand sides give (v, e)
+        # pairs, one row per cell, and the network trains on them on this
+        # GPU; with a base it learns the correction e - base(v)
         t0 = time.perf_counter()
-        pc = ab.LearnedPreconditioner(op, seed=rank)
-        train_info = pc.train(mat, dt, num_solves=args.train_solves,
-                              epochs=args.train_epochs, batch=1024, lr=1e-3,
-                              seed=rank, mat_T=op.kronmult_matrix_transposed(),
-                              residual_epochs=20)
+        net = ab.LearnedPreconditioner(op, seed=rank)
+        if base is not None:
+            net.set_base(base)
+        train_info = net.train(mat, dt, num_solves=args.train_solves,
+                               epochs=args.train_epochs, batch=1024, lr=1e-3,
+                               seed=rank, mat_T=op.kronmult_matrix_transposed(),
+                               residual_epochs=20)
         torch.cuda.synchronize()
         train_info["setup_s"] = time.perf_counter() - t0
-        if not pc.useful:
-            # the validation solve showed no gain: plain GMRES is the fallback
-            pc = None
-    method = dict(precision=precision, precond=pc,
-                  name={"learned-fp32": "learned preconditioner + FP32 operator, FP64 refinement",
-                        "learned-fp64": "learned preconditioner, FP64",
-                        "fp32": "FP32 operator, FP64 refinement",
-                        "fp64": "plain FP64 GMRES"}[args.method])
+        # the validation solve decides: without a gain the method continues
+        # without the network (the base preconditioner, or none)
+        if net.useful:
+            pc = net
+    learned = args.method.startswith("learned")
+    dropped = " (learned correction dropped: no gain in its validation solve)"
+    parts = []
+    if learned and pc is not None and pc is not base:
+        parts.append("learned preconditioner" + (" on block-Jacobi" if base is not None else ""))
+    elif base is not None:
+        parts.append("block-Jacobi preconditioner" + (dropped if learned else ""))
+    elif learned:
+        parts.append("no preconditioner" + dropped)
+    parts.append("FP32 operator, FP64 refinement" if precision == "fp32" else "FP64")
+    method = dict(precision=precision, precond=pc, name=", ".join(parts))
 
     def solve(b, precision, precond=None):
         x = torch.zeros(N, dtype=torch.float64, device="cuda")
@@ -376,7 +392,7 @@ def main():
             "e2e": {"value": e2e_value, "unit": "solves/s",
                     "h2d_bytes_per_step": N * 8, "d2h_bytes_per_step": N * 8},
             "gpu_launches": launches,
-            "roofline": {"bound": "fp64", "kernel": "kron3_rows<d=4, fp64>",
+            "roofline": {"bound": "fp64", "kernel": "kron3_staged<d=4, fp64> (+ x repack)",
                          "achieved": achieved, "peak": fp64_peak.value,
                          "peak_source": "measured live (FMA chain kernel)",
                          "unit": "TFLOP/s", "frac": achieved / fp64_peak.value,

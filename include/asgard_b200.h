@@ -28,6 +28,7 @@ extern "C" {
 
 typedef struct asgk_plan asgk_plan;
 typedef struct asgk_mlp asgk_mlp;
+typedef struct asgk_jacobi asgk_jacobi;
 typedef void *asgk_stream; /* a cudaStream_t */
 
 typedef enum asgk_status
@@ -197,6 +198,40 @@ int asgk_cgs_step_noalloc(const double *V, int64_t ldv, int k, double *w,
 /* default_gmres_restarts<double>(n) (src/solver.cpp:142-152). */
 int asgk_default_gmres_restarts(int64_t n);
 
+/* ------------------------------------------------ Jacobi preconditioners */
+
+typedef enum asgk_jacobi_kind
+{
+  ASGK_JACOBI_POINT = 0, /* the reference's diagonal preconditioner */
+  ASGK_JACOBI_BLOCK = 1  /* inverse of each cell's n^d x n^d diagonal block */
+} asgk_jacobi_kind;
+
+/* Builds a Jacobi preconditioner of I - dt*K for a square plan, on the
+ * device.  ASGK_JACOBI_POINT is build_preconditioner
+ * (src/asgard_kronmult_matrix.cpp:1015-1067): pc_i = sum_t prod_k
+ * A_{t,k}(i_k, i_k) over the factors of each cell's own pair, applied as
+ * z_i = v_i / (1 - dt*pc_i) (apply_diagonal_precond, src/solver.cpp:76-91;
+ * the reference has it in its global-kron mode only).  ASGK_JACOBI_BLOCK
+ * inverts the whole diagonal block (I - dt*sum_t (x)_k A_{t,k}) of every
+ * cell (Gauss-Jordan with partial pivoting; n^d <= 81, else
+ * ASGK_ERR_UNSUPPORTED); ASGK_ERR_BREAKDOWN if a block is singular.  The
+ * preconditioner keeps no reference to the plan. */
+int asgk_jacobi_create(asgk_jacobi **pc, asgk_plan *plan, double dt, int kind);
+void asgk_jacobi_destroy(asgk_jacobi *pc);
+/* z = M v on device vectors of the plan's size (z != v). */
+int asgk_jacobi_apply(asgk_jacobi *pc, const double *v, double *z,
+                      asgk_stream stream);
+int asgk_jacobi_info(asgk_jacobi *pc, int *kind, double *dt,
+                     int64_t *device_bytes);
+/* asgk_gmres_euler with a Jacobi preconditioner applied on the right
+ * (flexible GMRES; the reference applies its diagonal one to the residual).
+ * With ASGK_FP32 the block inverses are applied from an FP32 copy. */
+int asgk_gmres_euler_jacobi(asgk_plan *plan, double dt, double *x,
+                            const double *b, int restart, int max_outer,
+                            double tol, int tol_mode, int precision,
+                            asgk_jacobi *precond, asgk_gmres_info *info,
+                            asgk_stream stream);
+
 /* ------------------------------------------------ learned preconditioner */
 
 /* A per-cell learned preconditioner (no counterpart in the reference, which
@@ -245,7 +280,12 @@ int asgk_mlp_train_residual(asgk_mlp *mlp, asgk_plan *plan, asgk_plan *plan_T,
                             int num_samples, int epochs, float lr,
                             int precision, uint64_t seed, double *final_loss,
                             asgk_stream stream);
-/* z = M(v) on device vectors of the plan's size. */
+/* Makes the preconditioner base(v) + network(v): the network then learns a
+ * correction to base (a Jacobi preconditioner, which must outlive this use;
+ * NULL removes it).  The training entries are unchanged: pass them the
+ * corrections e - base(r) as targets.  No counterpart in the reference. */
+int asgk_mlp_set_base(asgk_mlp *mlp, asgk_jacobi *base);
+/* z = M(v) on device vectors of the plan's size (base included). */
 int asgk_mlp_apply(asgk_mlp *mlp, asgk_plan *plan, const double *v, double *z,
                    asgk_stream stream);
 

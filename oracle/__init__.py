@@ -299,3 +299,58 @@ class RefPDE:
         if getattr(self, "h", None):
             self.lib.ref_pde_destroy(self.h)
             self.h = None
+
+
+# ---------------------------------------------------------------- Jacobi
+# numpy restatements (small sizes only) of the diagonal preconditioner data
+
+
+def _self_pair(pntr, indx, row):
+    b, e = int(pntr[row]), int(pntr[row + 1])
+    hit = np.nonzero(np.asarray(indx[b:e]) == row)[0]
+    return b + int(hit[0]) if len(hit) else -1
+
+
+def point_jacobi_diag(d, n, pntr, indx, terms, iA, vA):
+    """pc_i = sum_t prod_k A_{t,k}(i_k, i_k) over each cell's own pair:
+    build_preconditioner (src/asgard_kronmult_matrix.cpp:1015-1067, the loop
+    at :1046-1063), with the factors addressed by the local-mode iA of the
+    cell's diagonal pair instead of the global 1D coefficient matrices."""
+    rows = len(pntr) - 1
+    ts = n ** d
+    pc = np.zeros(rows * ts)
+    for r in range(rows):
+        p = _self_pair(pntr, indx, r)
+        if p < 0:
+            continue
+        for i in range(ts):
+            s = 0.0
+            for t in range(terms):
+                a, ii = 1.0, i
+                for k in range(d - 1, -1, -1):
+                    ik = ii % n
+                    ii //= n
+                    a *= vA[iA[(p * terms + t) * d + k] + ik + ik * n]
+                s += a
+            pc[r * ts + i] = s
+    return pc
+
+
+def diagonal_blocks(d, n, pntr, indx, terms, iA, vA):
+    """K_cc = sum_t (x)_k A_{t,k} over each cell's own pair (dimension 0
+    slowest, column-major factors), rows x ts x ts."""
+    rows = len(pntr) - 1
+    ts = n ** d
+    out = np.zeros((rows, ts, ts))
+    for r in range(rows):
+        p = _self_pair(pntr, indx, r)
+        if p < 0:
+            continue
+        for t in range(terms):
+            m = np.ones((1, 1))
+            for k in range(d):
+                off = int(iA[(p * terms + t) * d + k])
+                A = np.asarray(vA[off:off + n * n]).reshape(n, n).T  # A(i, j)
+                m = np.kron(m, A)
+            out[r] += m
+    return out

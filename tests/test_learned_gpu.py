@@ -113,3 +113,42 @@ def test_broken_network_falls_back_to_plain_gmres(cuda):
     assert info.status == 0
     assert info.true_relres <= 1e-10
     assert info.fallback == 1
+
+
+def test_learned_correction_on_block_jacobi(cuda):
+    """With a block-Jacobi base the preconditioner is base(v) + network(v)
+    and the network trains on e - base(r).  An untrained (zero-output)
+    network leaves the base's solve unchanged up to rounding; after
+    training, the validation solve compares against the base alone and the
+    preconditioned solve still reaches the tolerance."""
+    import asgard_b200 as ab
+    import torch
+    op = ab.SparseGridOperator(3, 6, 3, kind="advdiff", nu=0.1)
+    mat = op.kronmult_matrix()
+    dt = 4e-3
+    base = ab.JacobiPreconditioner(mat, dt, kind="block")
+    pc = ab.LearnedPreconditioner(op, seed=0)
+    pc.set_base(base)
+    # the apply is base + network: with zero weights it is exactly the base
+    pc.set_params(np.zeros(pc.num_params(), np.float32))
+    v = torch.rand(op.N, dtype=torch.float64, device="cuda") * 2 - 1
+    z0, z1 = torch.empty_like(v), torch.empty_like(v)
+    base.apply(v, z0)
+    pc.apply(mat, v, z1)
+    torch.cuda.synchronize()
+    assert torch.equal(z0, z1)
+    pc2 = ab.LearnedPreconditioner(op, seed=0)
+    pc2.set_base(base)
+    stats = pc2.train(mat, dt, num_solves=2, epochs=20, batch=512, lr=1e-3,
+                      mat_T=op.kronmult_matrix_transposed(), residual_epochs=10)
+    val = stats["validation"]
+    assert val["baseline"] == "block-jacobi"
+    assert val["useful"] == (val["learned_iterations"] < val["plain_iterations"]
+                             and val["learned_fallback"] == 0)
+    b = torch.rand(op.N, dtype=torch.float64, device="cuda",
+                   generator=torch.Generator(device="cuda").manual_seed(3)) * 2 - 1
+    for prec in ("fp64", "fp32"):
+        x = torch.zeros_like(b)
+        info = ab.simple_gmres_euler(dt, mat, x, b, 50, 200, 1e-10,
+                                     tol_mode="rel", precision=prec, precond=pc2)
+        assert info.status == 0 and info.true_relres <= 1e-10, (prec, info)

@@ -189,3 +189,24 @@ def test_mlp_oracle_is_linear_in_the_residual():
     Z = np.zeros((3, ts))
     f = lambda u: mlp_oracle.forward_backward(p, ts, d, H, np.hstack([u, lam]), Z)[0]
     assert np.allclose(f(2 * u1 - 3 * u2), 2 * f(u1) - 3 * f(u2), atol=1e-12)
+
+
+def test_jacobi_restatements_against_dense_assembly():
+    """The point-Jacobi diagonal and the cell-diagonal blocks of the oracle
+    equal the diagonal entries / blocks of K assembled column by column from
+    the oracle's kronmult (d = 2, level 3, random factors)."""
+    import asgard_b200.operators as O
+    d, L, T = 2, 3, 2
+    op = O.SparseGridOperator(d, L, T, kind="random", seed=4)
+    pntr, iA = op.row_ptr.astype(np.int32), op.iA()
+    ts, N = 3 ** d, op.N
+    K = np.zeros((N, N))
+    for j in range(N):
+        e = np.zeros(N)
+        e[j] = 1.0
+        K[:, j] = oracle.kronmult(d, 3, pntr, op.col, T, iA, op.vA, 1.0, e, 0.0, np.zeros(N))
+    blocks = oracle.diagonal_blocks(d, 3, pntr, op.col, T, iA, op.vA)
+    for c in range(op.rows):
+        assert np.allclose(blocks[c], K[c * ts:(c + 1) * ts, c * ts:(c + 1) * ts], rtol=0, atol=1e-14)
+    pc = oracle.point_jacobi_diag(d, 3, pntr, op.col, T, iA, op.vA)
+    assert np.allclose(pc, np.diag(K), rtol=0, atol=1e-14)
