@@ -96,6 +96,14 @@ class LearnedPreconditioner:
         check(lib.asgk_mlp_set_base(self._h, base.handle if base is not None else None),
               "mlp_set_base")
         self.base = base      # kept alive with the network
+        if base is not None:
+            # start as the base itself: output layer W4 (hidden x n^d, after
+            # W1 and two hidden x hidden layers in the flat parameters) zero
+            ts, H = self.dims[0], self.hidden
+            p = self.get_params()
+            o = ts * H + 2 * H * H
+            p[o:o + H * ts] = 0.0
+            self.set_params(p)
 
     def __del__(self):
         h = getattr(self, "_h", None)
