@@ -13,11 +13,13 @@ LIB_PATH = os.path.join(HERE, "libasgard_b200.so")
 
 EXPORTS = [
     "asgk_plan_create", "asgk_plan_create_pairs", "asgk_plan_create_conn",
+    "asgk_plan_create_global",
     "asgk_plan_destroy", "asgk_plan_update_values", "asgk_plan_info",
     "asgk_apply", "asgk_apply_f32", "asgk_apply_host", "asgk_apply_euler",
     "asgk_gmres_euler", "asgk_gmres_dense", "asgk_default_gmres_restarts",
     "asgk_cgs_step", "asgk_cgs_step_noalloc",
     "asgk_sparse_grid", "asgk_connect_1d", "asgk_build_pairs",
+    "asgk_direction_pairs",
     "asgk_status_string", "asgk_launch_count", "asgk_device_info",
     "asgk_device_status",
     "asgk_measure_fma_peak", "asgk_mlp_create", "asgk_mlp_destroy",
@@ -56,6 +58,7 @@ def _load():
         "asgk_plan_create": ([C.POINTER(_vp), _i, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _i64], _i),
         "asgk_plan_create_pairs": ([C.POINTER(_vp), _i, _i, _i, _i, _i, _i64, _vp, _vp, _vp, _vp, _i64], _i),
         "asgk_plan_create_conn": ([C.POINTER(_vp), _i, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _i64], _i),
+        "asgk_plan_create_global": ([C.POINTER(_vp), _i, _i, _i, _i, _vp, _i, _vp, _i64], _i),
         "asgk_plan_destroy": ([_vp], None),
         "asgk_plan_update_values": ([_vp, _vp, _i64], _i),
         "asgk_plan_info": ([_vp] + [C.POINTER(_i64)] * 5, _i),
@@ -71,6 +74,7 @@ def _load():
         "asgk_sparse_grid": ([_i, _i, _vp], _i64),
         "asgk_connect_1d": ([_i, C.POINTER(_i), C.POINTER(_i), _vp, _vp], _i),
         "asgk_build_pairs": ([_i, _i, _i, _vp, C.POINTER(_i64), _vp, _vp, _vp], _i),
+        "asgk_direction_pairs": ([_i, _i, _i, _vp, C.POINTER(_i64), _vp, _vp, _vp, _vp], _i),
         "asgk_status_string": ([_i], C.c_char_p),
         "asgk_launch_count": ([], _i64),
         "asgk_device_info": ([C.POINTER(_i)] * 3, _i),

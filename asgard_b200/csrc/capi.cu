@@ -43,6 +43,11 @@ void free_plan(plan_data &p)
   cudaFree(p.xw);
   cudaFree(p.yw);
   cudaFree(p.xs);
+  cudaFree(p.gptr);
+  cudaFree(p.gcol);
+  cudaFree(p.gkb);
+  cudaFree(p.gB64);
+  cudaFree(p.gB32);
   cudaFree(p.vP64);
   cudaFree(p.vP32);
   p = plan_data{};
@@ -74,6 +79,70 @@ __global__ void k_repack(const double *__restrict__ vA, int64_t nconn, int d,
     for (int e = 0; e < 12; e++)
       v32[i * 12 + e] = (e < 9) ? float(src[e]) : 0.0f;
   }
+}
+
+// Global mode: checks that every term is the identity in all but at most
+// one dimension (identity: the block of a self-connection is I and every
+// other block is 0, exactly), and sums each dimension's blocks over the terms
+// acting there.  B: [nconn*d][10] (9 values + pad).
+int global_blocks(int d, int terms, std::vector<int> const &conn_row,
+                  std::vector<int> const &conn_col, const double *vA,
+                  std::vector<double> &B, int &n_identity)
+{
+  int64_t const nconn = int64_t(conn_row.size());
+  auto blk = [&](int64_t j, int t, int k) {
+    return vA + j * d * terms * 9 + int64_t(t * d + k) * 9;
+  };
+  std::vector<int> active(terms, -1);
+  n_identity = 0;
+  for (int t = 0; t < terms; t++)
+  {
+    int nact = 0;
+    for (int k = 0; k < d; k++)
+    {
+      bool ident = true;
+      for (int64_t j = 0; j < nconn && ident; j++)
+      {
+        bool const self = conn_row[j] == conn_col[j];
+        const double *a = blk(j, t, k);
+        for (int e = 0; e < 9 && ident; e++)
+          ident = a[e] == ((self && e % 4 == 0) ? 1.0 : 0.0);
+      }
+      if (!ident)
+      {
+        active[t] = k;
+        ++nact;
+      }
+    }
+    if (nact > 1)
+      return ASGK_ERR_UNSUPPORTED; // needs the multi-direction form
+    if (nact == 0)
+      ++n_identity;
+  }
+  B.assign(size_t(nconn) * d * 10, 0.0);
+  for (int t = 0; t < terms; t++)
+  {
+    int const k = active[t];
+    if (k < 0)
+      continue;
+    for (int64_t j = 0; j < nconn; j++)
+      for (int e = 0; e < 9; e++)
+        B[(j * d + k) * 10 + e] += blk(j, t, k)[e];
+  }
+  return ASGK_OK;
+}
+
+int upload_global_blocks(plan_data &p, std::vector<double> const &B)
+{
+  std::vector<float> B32(B.size() / 10 * 12, 0.0f);
+  for (size_t i = 0; i < B.size() / 10; i++)
+    for (int e = 0; e < 9; e++)
+      B32[i * 12 + e] = float(B[i * 10 + e]);
+  ASGK_CUDA(cudaMemcpy(p.gB64, B.data(), sizeof(double) * B.size(),
+                       cudaMemcpyHostToDevice));
+  ASGK_CUDA(cudaMemcpy(p.gB32, B32.data(), sizeof(float) * B32.size(),
+                       cudaMemcpyHostToDevice));
+  return ASGK_OK;
 }
 
 int upload_values(plan_data &p, const double *vA)
@@ -705,7 +774,117 @@ int asgk_plan_update_values(asgk_plan *plan, const double *vA, int64_t vA_len)
 {
   if (!plan || vA_len != plan->p.vA_len || (vA_len > 0 && !vA))
     return ASGK_ERR_INVALID;
-  return upload_values(plan->p, vA);
+  auto &p = plan->p;
+  if (p.global)
+  {
+    std::vector<double> B;
+    int n_identity = 0;
+    if (int rc = global_blocks(p.d, p.terms, p.g_conn_row, p.g_conn_col, vA, B,
+                               n_identity))
+      return rc;
+    if (int rc = upload_global_blocks(p, B))
+      return rc;
+    p.g_identity = n_identity;
+  }
+  return upload_values(p, vA);
+}
+
+int asgk_plan_create_global(asgk_plan **plan, int d, int n, int level,
+                            int num_cells, const int *table, int num_terms,
+                            const double *vA, int64_t vA_len)
+{
+  if (plan == nullptr)
+    return ASGK_ERR_INVALID;
+  *plan = nullptr;
+  if (n != 3)
+    return ASGK_ERR_UNSUPPORTED;
+  if (num_terms < 1 || vA == nullptr || table == nullptr || num_cells < 1)
+    return ASGK_ERR_INVALID;
+  direction_pairs dp;
+  if (int rc = build_direction_pairs(d, level, num_cells, table, dp))
+    return rc;
+  if (vA_len != int64_t(dp.nconn) * d * num_terms * 9)
+    return ASGK_ERR_INVALID;
+  std::vector<double> B;
+  int n_identity = 0;
+  if (int rc = global_blocks(d, num_terms, dp.conn_row, dp.conn_col, vA, B,
+                             n_identity))
+    return rc;
+  // entries of dimensions some term acts in
+  std::vector<char> used(d, 0);
+  for (int64_t j = 0; j < dp.nconn; j++)
+    for (int k = 0; k < d; k++)
+      for (int e = 0; e < 9; e++)
+        if (B[(j * d + k) * 10 + e] != 0.0)
+          used[k] = 1;
+  std::vector<int64_t> gptr(num_cells + 1, 0);
+  std::vector<int> gcol, gkb;
+  for (int r = 0; r < num_cells; r++)
+  {
+    for (int64_t e = dp.ptr[r]; e < dp.ptr[r + 1]; e++)
+      if (used[dp.dim[e]])
+      {
+        gcol.push_back(dp.col[e]);
+        gkb.push_back(dp.conn[e] * d + dp.dim[e]);
+      }
+    gptr[r + 1] = int64_t(gcol.size());
+  }
+  // the diagonal pairs (one per cell) for the Jacobi preconditioners
+  std::vector<int64_t> rp(num_cells + 1);
+  std::vector<int> col(num_cells), conn(size_t(num_cells) * d);
+  for (int r = 0; r <= num_cells; r++)
+    rp[r] = r;
+  for (int r = 0; r < num_cells; r++)
+  {
+    col[r] = r;
+    for (int k = 0; k < d; k++)
+      conn[size_t(r) * d + k] = dp.self_conn[size_t(r) * d + k];
+  }
+  if (int rc = build_plan(plan, d, n, num_cells, num_cells, num_terms, rp,
+                          col.data(), conn.data(), index_mode::conn, vA, vA_len))
+    return rc;
+  auto &p = (*plan)->p;
+  p.global     = true;
+  p.gnnz       = int64_t(gcol.size());
+  p.g_identity = n_identity;
+  p.g_conn_row = dp.conn_row;
+  p.g_conn_col = dp.conn_col;
+  int64_t &bytes = p.device_bytes;
+  int rc = ASGK_OK;
+  if ((rc = dev_alloc(&p.gptr, num_cells + 1, bytes)) ||
+      (rc = dev_alloc(&p.gcol, std::max<int64_t>(p.gnnz, 1), bytes)) ||
+      (rc = dev_alloc(&p.gkb, std::max<int64_t>(p.gnnz, 1), bytes)) ||
+      (rc = dev_alloc(&p.gB64, int64_t(B.size()), bytes)) ||
+      (rc = dev_alloc(&p.gB32, int64_t(B.size() / 10 * 12), bytes)))
+  {
+    asgk_plan_destroy(*plan);
+    *plan = nullptr;
+    return rc;
+  }
+  auto up = [&](void *dst, const void *src, size_t b) -> int {
+    if (b == 0)
+      return ASGK_OK;
+    ASGK_CUDA(cudaMemcpy(dst, src, b, cudaMemcpyHostToDevice));
+    return ASGK_OK;
+  };
+  // cells with the most single-direction neighbours first (coarse cells
+  // reach every cell of a dimension: up to 2^level per dimension)
+  std::vector<int> order(num_cells);
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+    return (gptr[a + 1] - gptr[a]) > (gptr[b + 1] - gptr[b]);
+  });
+  if ((rc = up(p.row_order, order.data(), sizeof(int) * order.size())) ||
+      (rc = up(p.gptr, gptr.data(), sizeof(int64_t) * gptr.size())) ||
+      (rc = up(p.gcol, gcol.data(), sizeof(int) * gcol.size())) ||
+      (rc = up(p.gkb, gkb.data(), sizeof(int) * gkb.size())) ||
+      (rc = upload_global_blocks(p, B)))
+  {
+    asgk_plan_destroy(*plan);
+    *plan = nullptr;
+    return rc;
+  }
+  return ASGK_OK;
 }
 
 int asgk_plan_info(const asgk_plan *plan, int64_t *num_batch,
@@ -716,13 +895,15 @@ int asgk_plan_info(const asgk_plan *plan, int64_t *num_batch,
     return ASGK_ERR_INVALID;
   auto const &p = plan->p;
   if (num_batch)
-    *num_batch = p.nnz;
+    *num_batch = p.global ? p.gnnz : p.nnz;
   if (input_size)
     *input_size = int64_t(p.cols) * p.tensor;
   if (output_size)
     *output_size = int64_t(p.rows) * p.tensor;
+  // global mode: one contraction in one dimension per entry
   if (flops)
-    *flops = int64_t(p.tensor) * p.n * p.d * p.terms * p.nnz * 2;
+    *flops = p.global ? int64_t(p.tensor) * p.n * p.gnnz * 2
+                      : int64_t(p.tensor) * p.n * p.d * p.terms * p.nnz * 2;
   if (device_bytes)
     *device_bytes = p.device_bytes;
   return ASGK_OK;

@@ -19,7 +19,10 @@
 #include <algorithm>
 #include <cstdint>
 #include <cstdlib>
+#include <unordered_map>
 #include <vector>
+
+#include "internal.cuh"
 
 #include <omp.h>
 
@@ -100,6 +103,86 @@ inline int index_1d(int level, int pos)
 }
 
 } // namespace
+
+namespace asgk
+{
+// Neighbours of every cell along one dimension at a time: cell c is listed
+// for row r and dimension k when c agrees with r in every other dimension
+// and the 1D cells of r and c in dimension k are connected (c == r, with
+// the self-connection, for every k).  These are the cell pairs of the
+// connected-pair list that differ in at most one dimension -- the only
+// pairs a term acting in a single dimension couples.
+int build_direction_pairs(int d, int level, int num_cells, const int *table,
+                          direction_pairs &out)
+{
+  if (d < 1 || d > 6 || level < 0 || level > 12 || num_cells < 0 || !table)
+    return ASGK_ERR_INVALID;
+  conn1d const c(level);
+  int const R = c.rows;
+  std::vector<int> oned(size_t(num_cells) * d);
+  for (int i = 0; i < num_cells; i++)
+    for (int k = 0; k < d; k++)
+    {
+      int const L = table[int64_t(i) * 2 * d + k];
+      int const p = table[int64_t(i) * 2 * d + d + k];
+      if (L < 0 || L > level || p < 0 || (L > 1 && p >= (1 << (L - 1))) ||
+          (L <= 1 && p != 0))
+        return ASGK_ERR_INVALID;
+      oned[size_t(i) * d + k] = index_1d(L, p);
+    }
+  // 1D-index tuple -> cell (1D indices < 2^level: level bits each)
+  int const bits = std::max(level, 1);
+  if (d * bits > 64)
+    return ASGK_ERR_UNSUPPORTED;
+  auto key = [&](const int *t) {
+    uint64_t h = 0;
+    for (int k = 0; k < d; k++)
+      h = (h << bits) | uint64_t(t[k]);
+    return h;
+  };
+  std::unordered_map<uint64_t, int> where;
+  where.reserve(size_t(num_cells) * 2);
+  for (int i = 0; i < num_cells; i++)
+    if (!where.emplace(key(&oned[size_t(i) * d]), i).second)
+      return ASGK_ERR_INVALID; // a cell listed twice
+  out.d = d;
+  out.ptr.assign(num_cells + 1, 0);
+  out.col.clear();
+  out.dim.clear();
+  out.conn.clear();
+  out.self_conn.assign(size_t(num_cells) * d, -1);
+  std::vector<int> t(d);
+  for (int r = 0; r < num_cells; r++)
+  {
+    const int *ro = &oned[size_t(r) * d];
+    for (int k = 0; k < d; k++)
+    {
+      std::copy(ro, ro + d, t.begin());
+      int const rk = ro[k];
+      for (int j = c.pntr[rk]; j < c.pntr[rk + 1]; j++)
+      {
+        t[k]          = c.indx[j];
+        auto const it = where.find(key(t.data()));
+        if (it == where.end())
+          continue;
+        out.col.push_back(it->second);
+        out.dim.push_back(k);
+        out.conn.push_back(j);
+        if (it->second == r)
+          out.self_conn[size_t(r) * d + k] = j;
+      }
+    }
+    out.ptr[r + 1] = int64_t(out.col.size());
+  }
+  out.nconn = int(c.indx.size());
+  out.conn_row.resize(c.indx.size());
+  out.conn_col = c.indx;
+  for (int r = 0; r < R; r++)
+    for (int j = c.pntr[r]; j < c.pntr[r + 1]; j++)
+      out.conn_row[j] = r;
+  return ASGK_OK;
+}
+} // namespace asgk
 
 extern "C"
 {
@@ -249,6 +332,27 @@ int asgk_build_pairs(int d, int level, int num_cells, const int *table,
       ++pos;
     }
   }
+  return ASGK_OK;
+}
+
+int asgk_direction_pairs(int d, int level, int num_cells, const int *table,
+                         int64_t *nnz, int64_t *row_ptr, int *col_indx,
+                         int *dim, int *conn)
+{
+  if (!nnz)
+    return ASGK_ERR_INVALID;
+  asgk::direction_pairs dp;
+  if (int rc = asgk::build_direction_pairs(d, level, num_cells, table, dp))
+    return rc;
+  *nnz = int64_t(dp.col.size());
+  if (row_ptr)
+    std::copy(dp.ptr.begin(), dp.ptr.end(), row_ptr);
+  if (col_indx)
+    std::copy(dp.col.begin(), dp.col.end(), col_indx);
+  if (dim)
+    std::copy(dp.dim.begin(), dp.dim.end(), dim);
+  if (conn)
+    std::copy(dp.conn.begin(), dp.conn.end(), conn);
   return ASGK_OK;
 }
 

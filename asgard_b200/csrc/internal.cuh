@@ -74,6 +74,20 @@ struct plan_data
   double *xw = nullptr, *yw = nullptr;
   // x repacked for the staged kernel (n = 3, d = 3/4): padded slices
   double *xs = nullptr;
+
+  // global mode (every term acts in at most one dimension; n = 3): per
+  // output cell its neighbours along one dimension (gptr/gcol), each with
+  // the index conn*d + k of a 3x3 block pre-summed over the terms acting in
+  // dimension k (gkb); the pair list above then holds only the diagonal
+  // pairs, for the Jacobi preconditioners
+  bool global = false;
+  int64_t gnnz = 0;
+  int64_t *gptr = nullptr;
+  int *gcol = nullptr, *gkb = nullptr;
+  double *gB64 = nullptr; // [nconn*d][10]
+  float *gB32  = nullptr; // [nconn*d][12]
+  double g_identity = 0;  // number of terms that are the identity
+  std::vector<int> g_conn_row, g_conn_col; // 1D cells of each 1D connection
   int64_t device_bytes = 0;
 };
 
@@ -91,12 +105,29 @@ int launch_apply(plan_data const &p, int precision, double alpha,
                  const void *x, int x_is_f32, double beta, void *y,
                  int y_is_f32, double euler_x_coeff, cudaStream_t s);
 
+// grid.cpp: cell pairs that differ in at most one dimension
+struct direction_pairs
+{
+  int d = 0, nconn = 0;
+  std::vector<int64_t> ptr;     // [cells + 1]
+  std::vector<int> col, dim, conn; // per entry: neighbour cell, dimension, 1D connection
+  std::vector<int> self_conn;   // [cells][d] the self-connection index
+  std::vector<int> conn_row, conn_col; // 1D cells of each 1D connection
+};
+int build_direction_pairs(int d, int level, int num_cells, const int *table,
+                          direction_pairs &out);
+
 // jacobi.cu
 struct jacobi_data;
 int jacobi_apply(jacobi_data const &jd, bool low, const double *v, double *z,
                  cudaStream_t s);
 int jacobi_apply_handle(asgk_jacobi *pc, bool low, const double *v, double *z,
                         cudaStream_t s);
+
+// kron_global.cu: global-mode apply
+int launch_global(plan_data const &p, int precision, double alpha,
+                  const double *x, double beta, double *y, double ex,
+                  cudaStream_t s);
 
 // kron_staged.cu: n = 3, d = 3/4 apply with bulk-copied x tensors
 bool staged_supported(plan_data const &p);

@@ -461,6 +461,13 @@ int launch_apply(plan_data const &p, int precision, double alpha,
 {
   if (p.rows == 0)
     return ASGK_OK;
+  if (p.global)
+  {
+    if (x_is_f32 || y_is_f32)
+      return ASGK_ERR_UNSUPPORTED;
+    return launch_global(p, precision, alpha, static_cast<const double *>(x),
+                         beta, static_cast<double *>(y), ex, s);
+  }
   bool const euler = (ex != 0.0);
   if (x_is_f32 && y_is_f32)
     return dispatch<float, float, float>(p, p.vA32, alpha,

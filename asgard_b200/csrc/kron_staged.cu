@@ -228,6 +228,24 @@ template<> struct xlayout<3, float>
   __device__ static int slot(int g) { return 9 * g; }
 };
 
+// out <- (I (x) A (x) I) in along the register dimension of stride S
+template<int R, int S, typename TC>
+__device__ __forceinline__ void fibre3_from(TC const (&in)[R], TC (&out)[R],
+                                            TC const (&a)[9])
+{
+#pragma unroll
+  for (int b = 0; b < R; b++)
+  {
+    if ((b / S) % 3 == 0)
+    {
+      TC const w0 = in[b], w1 = in[b + S], w2 = in[b + 2 * S];
+      out[b]         = fma(a[6], w2, fma(a[3], w1, a[0] * w0));
+      out[b + S]     = fma(a[7], w2, fma(a[4], w1, a[1] * w0));
+      out[b + 2 * S] = fma(a[8], w2, fma(a[5], w1, a[2] * w0));
+    }
+  }
+}
+
 template<int D, typename TC, int NW, int NS>
 struct staged_shape
 {
@@ -440,13 +458,7 @@ __global__ void __launch_bounds__(NW * 32, sizeof(TC) == 4 ? 3 : 2)
       for (int t = 0; t < terms; t++)
       {
         TC w[R];
-        if constexpr (XREG)
-        {
-#pragma unroll
-          for (int m = 0; m < R; m++)
-            w[m] = xr[m];
-        }
-        else
+        if constexpr (!XREG)
           load_slice<R, S::NCH>(sl, w);
         auto blk = [&](int k) -> const TC * {
           if constexpr (MODE == index_mode::conn)
@@ -455,6 +467,8 @@ __global__ void __launch_bounds__(NW * 32, sizeof(TC) == 4 ? 3 : 2)
             return vF + __ldcs(idx + (p * terms + t) * D + k);
         };
         // dimensions 1..D-1 live in registers: register m <-> (i_1 .. i_{D-1})
+        // (FP32: the first one reads the slice registers, so they need no
+        // copy per term)
         sfor<1, D>([&](auto kc) {
           constexpr int k = decltype(kc)::value;
           TC a[9];
@@ -462,7 +476,10 @@ __global__ void __launch_bounds__(NW * 32, sizeof(TC) == 4 ? 3 : 2)
             ld9p(blk(k), a);
           else
             ld9(blk(k), a);
-          fibre3<R, ipow3s(D - 1 - k)>(w, a);
+          if constexpr (XREG && k == 1)
+            fibre3_from<R, ipow3s(D - 1 - k)>(xr, w, a);
+          else
+            fibre3<R, ipow3s(D - 1 - k)>(w, a);
         });
         // dimension 0: this lane holds input slice q; column q of A0
         // scatters it to the three output slices

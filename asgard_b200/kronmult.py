@@ -118,6 +118,22 @@ class kronmult_matrix:
               "plan_create_conn")
         return cls(h, d, n, num_rows, num_cols, num_terms)
 
+    @classmethod
+    def from_global(cls, d, n, level, table, num_terms, vA):
+        """Global Kronecker form of the sparse grid's operator (terms acting in
+        one dimension each): the element table (cells x 2d) and vA in the
+        per-1D-connection layout; raises AsgkError (unsupported) when a term
+        acts in more than one dimension."""
+        tb = _host(table, np.int32)
+        vA = _host(vA, np.float64)
+        cells = tb.shape[0]
+        h = C.c_void_p()
+        check(lib.asgk_plan_create_global(C.byref(h), d, n, level, cells,
+                                          tb.ctypes.data, num_terms,
+                                          vA.ctypes.data, len(vA)),
+              "plan_create_global")
+        return cls(h, d, n, cells, cells, num_terms)
+
     def __del__(self):
         h = getattr(self, "_h", None)
         if h:

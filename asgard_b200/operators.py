@@ -162,8 +162,16 @@ class SparseGridOperator:
     def iA(self) -> np.ndarray:
         return expand_iA(self.conn, self.d, self.n, self.terms)
 
-    def kronmult_matrix(self, expanded: bool = False):
+    def kronmult_matrix(self, expanded: bool = False, mode: str = "pairs"):
+        """mode "pairs": the connected-pair kronmult (expanded: the
+        reference's iA offsets instead of connection indices); "global": the
+        global Kronecker form (terms acting in one dimension each)."""
         from .kronmult import kronmult_matrix
+        if mode == "global":
+            return kronmult_matrix.from_global(self.d, self.n, self.level,
+                                               self.table, self.terms, self.vA)
+        if mode != "pairs":
+            raise ValueError(mode)
         if expanded:
             return kronmult_matrix.from_csr(self.d, self.n, self.rows,
                                             self.rows, self.terms,

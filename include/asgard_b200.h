@@ -91,6 +91,21 @@ int asgk_plan_create_conn(asgk_plan **plan, int d, int n, int num_rows,
                           const int *col_indx, const int *conn,
                           const double *vA, int64_t vA_len);
 
+/* Global Kronecker form (the reference's global_kron_matrix,
+ * src/asgard_kronmult_matrix.cpp:1196-1334, for its single-direction terms):
+ * the same operator as the connected-pair plan of this sparse grid (the
+ * element table `table`, num_cells x 2d, as asgk_sparse_grid writes it; vA
+ * in the per-1D-connection layout of asgk_plan_create_conn), applied through
+ * the cell pairs that differ in at most one dimension.  Every term must be
+ * the identity (self-connection blocks I, all others 0) in all but at most
+ * one dimension, else ASGK_ERR_UNSUPPORTED; n = 3 only.  The plan works with
+ * asgk_apply / asgk_apply_euler / the GMRES and Jacobi entries like any
+ * other; num_batch reports the single-direction pairs and flops
+ * 2 * n^(d+1) per pair.  No counterpart for the reference's multi-direction
+ * terms (its upper/lower permutations). */
+int asgk_plan_create_global(asgk_plan **plan, int d, int n, int level,
+                            int num_cells, const int *table, int num_terms,
+                            const double *vA, int64_t vA_len);
 void asgk_plan_destroy(asgk_plan *plan);
 
 /* Replaces update_stored_coefficients (src/asgard_kronmult_matrix.hpp:515-532). */
@@ -302,6 +317,13 @@ int asgk_connect_1d(int level, int *num_rows, int *num_conn, int *pntr,
 int asgk_build_pairs(int d, int level, int num_cells, const int *table,
                      int64_t *nnz, int64_t *row_ptr, int *col_indx,
                      int *conn);
+/* The pairs of the global form: per cell r, every cell c that agrees with r
+ * in all dimensions but one (dim[i] = k, or c = r once per dimension) and
+ * whose 1D cell in dimension k is connected to r's (conn[i] = that 1D
+ * connection).  Two-call like asgk_build_pairs (NULL arrays: size only). */
+int asgk_direction_pairs(int d, int level, int num_cells, const int *table,
+                         int64_t *nnz, int64_t *row_ptr, int *col_indx,
+                         int *dim, int *conn);
 
 /* ------------------------------------------------------------ misc */
 

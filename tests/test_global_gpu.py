@@ -1,0 +1,112 @@
+"""Global Kronecker form (terms acting in one dimension each): the same
+operator as the connected-pair kronmult, checked against the oracle and the
+pair plan, inside GMRES, and its error cases."""
+import numpy as np
+import pytest
+
+import oracle
+from conftest import rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+def _dev(a):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def _apply(mat, alpha, x, beta, y, precision="fp64"):
+    import torch
+    yd = _dev(y)
+    mat.apply(alpha, _dev(x), beta, yd, precision=precision)
+    torch.cuda.synchronize()
+    return yd.cpu().numpy()
+
+
+@pytest.mark.parametrize("d,L,T", [(1, 6, 2), (2, 6, 3), (3, 5, 3), (4, 4, 4),
+                                   (5, 3, 5), (6, 3, 6), (4, 7, 4)])
+def test_global_matches_oracle_and_pairs(cuda, d, L, T):
+    import asgard_b200 as ab
+    op = ab.SparseGridOperator(d, L, T, kind="advdiff")
+    g = op.kronmult_matrix(mode="global")
+    rng = np.random.default_rng(d)
+    x = rng.uniform(-1, 1, op.N)
+    y0 = rng.uniform(-1, 1, op.N)
+    if op.nnz < 3_000_000:
+        expect = oracle.kronmult(d, 3, op.row_ptr.astype(np.int32), op.col, T,
+                                 op.iA(), op.vA, 0.7, x, -1.3, y0.copy())
+    else:   # d=4 level 7: the pair plan is the reference
+        expect = _apply(op.kronmult_matrix(), 0.7, x, -1.3, y0)
+    assert rel_err(_apply(g, 0.7, x, -1.3, y0), expect) < 1e-13
+    assert rel_err(_apply(g, 0.7, x, 0.0, y0), _apply(op.kronmult_matrix(), 0.7, x, 0.0, y0)) < 1e-13
+    assert rel_err(_apply(g, 0.7, x, -1.3, y0, "fp32"), expect) < 1e-5
+    # num_batch: the single-direction pairs; flops: one contraction each
+    assert g.num_batch() < op.nnz or d == 1
+    assert g.flops() == 2 * 3 ** (d + 1) * g.num_batch()
+
+
+def test_global_euler_identity_term_and_update(cuda):
+    """The fused Euler form, a term that is the identity in every dimension
+    (it adds x), and update_stored_coefficients."""
+    import asgard_b200 as ab
+    import torch
+    d, L, T = 3, 5, 4
+    op = ab.SparseGridOperator(d, L, T, kind="advdiff")
+    pntr, indx = ab.connect_1d(L)
+    rows = np.repeat(np.arange(len(pntr) - 1), np.diff(pntr))
+    vA = op.vA.reshape(len(indx), T, d, 9).copy()
+    eye = np.where((rows == indx)[:, None], np.eye(3).ravel(order="F")[None, :], 0.0)
+    vA[:, 3, 3 % d] = eye          # term 3 is now the identity everywhere
+    vA = vA.ravel()
+    g = ab.kronmult_matrix.from_global(d, 3, L, op.table, T, vA)
+    rng = np.random.default_rng(3)
+    x, y0 = rng.uniform(-1, 1, op.N), rng.uniform(-1, 1, op.N)
+    kx = oracle.kronmult(d, 3, op.row_ptr.astype(np.int32), op.col, T, op.iA(),
+                         vA, 1.0, x, 0.0, np.zeros(op.N))
+    dt, alpha, beta = 1e-3, -1.0, 0.5
+    yd = _dev(y0)
+    g.apply_euler(dt, alpha, _dev(x), beta, yd)
+    torch.cuda.synchronize()
+    assert rel_err(yd.cpu().numpy(), beta * y0 + alpha * (x - dt * kx)) < 1e-13
+    # new values: 2x the factors of the acting dimensions
+    vA2 = vA.reshape(len(indx), T, d, 9).copy()
+    for t in range(3):
+        vA2[:, t, t % d] *= 2.0
+    vA2 = vA2.ravel()
+    g.update_stored_coefficients(vA2)
+    kx2 = oracle.kronmult(d, 3, op.row_ptr.astype(np.int32), op.col, T, op.iA(),
+                          vA2, 1.0, x, 0.0, np.zeros(op.N))
+    assert rel_err(_apply(g, 1.0, x, 0.0, y0), kx2) < 1e-13
+
+
+def test_global_gmres_matches_pair_gmres(cuda):
+    """Solves with the global plan take the pair plan's iterations (+-1) and
+    reach the same solution, plain and with block Jacobi (built from the
+    global plan's diagonal pairs)."""
+    import asgard_b200 as ab
+    import torch
+    d, L, T, dt = 3, 6, 3, 4e-3
+    op = ab.SparseGridOperator(d, L, T, kind="advdiff")
+    pm, gm = op.kronmult_matrix(), op.kronmult_matrix(mode="global")
+    b = _dev(np.random.default_rng(1).uniform(-1, 1, op.N))
+    for kind in (None, "block"):
+        infos, xs = [], []
+        for mat in (pm, gm):
+            pc = ab.JacobiPreconditioner(mat, dt, kind=kind) if kind else None
+            x = torch.zeros_like(b)
+            info = ab.simple_gmres_euler(dt, mat, x, b, 50, 200, 1e-10,
+                                         tol_mode="rel", precond=pc)
+            assert info.status == 0 and info.true_relres <= 1e-10
+            infos.append(info)
+            xs.append(x)
+        assert abs(infos[0].iterations - infos[1].iterations) <= 1, (kind, infos)
+        assert (torch.linalg.norm(xs[0] - xs[1]) / torch.linalg.norm(xs[0])).item() < 1e-9
+
+
+def test_global_rejects_multi_direction_terms(cuda):
+    import asgard_b200 as ab
+    op = ab.SparseGridOperator(2, 3, 2, kind="random")
+    with pytest.raises(ab.AsgkError):
+        op.kronmult_matrix(mode="global")
+    with pytest.raises(ValueError):
+        op.kronmult_matrix(mode="dense")

@@ -117,3 +117,38 @@ def test_cpp_dropin_header_compiles(tmp_path):
     from test_cpp_dropin_gpu import compile_dropin
     r = compile_dropin(tmp_path / "dropin")
     assert r.returncode == 0, r.stderr
+
+
+@pytest.mark.parametrize("d,L", [(2, 5), (3, 4), (4, 3)])
+def test_direction_pairs_are_the_single_dimension_pairs(d, L):
+    """asgk_direction_pairs lists, per cell, exactly the connected pairs whose
+    cells differ in at most one dimension (the diagonal pair once per
+    dimension), with that dimension's 1D connection."""
+    import ctypes as C
+    from asgard_b200 import lib, operators as O
+    table = np.ascontiguousarray(O.sparse_grid(d, L), dtype=np.int32)
+    cells = table.shape[0]
+    rp, col, conn = O.build_pairs(d, L, table)
+    conn = conn.reshape(-1, d)
+    nnz = C.c_int64()
+    assert lib.asgk_direction_pairs(d, L, cells, table.ctypes.data, C.byref(nnz),
+                                    None, None, None, None) == 0
+    n = nnz.value
+    ptr = np.zeros(cells + 1, np.int64)
+    gcol, gdim, gconn = (np.zeros(n, np.int32) for _ in range(3))
+    assert lib.asgk_direction_pairs(d, L, cells, table.ctypes.data, C.byref(nnz),
+                                    ptr.ctypes.data, gcol.ctypes.data,
+                                    gdim.ctypes.data, gconn.ctypes.data) == 0
+    lv, ps = table[:, :d], table[:, d:]
+    for r in range(cells):
+        got = {(int(c), int(k), int(j)) for c, k, j in
+               zip(gcol[ptr[r]:ptr[r + 1]], gdim[ptr[r]:ptr[r + 1]], gconn[ptr[r]:ptr[r + 1]])}
+        want = set()
+        for p in range(rp[r], rp[r + 1]):
+            c = int(col[p])
+            diff = [k for k in range(d) if lv[r, k] != lv[c, k] or ps[r, k] != ps[c, k]]
+            if len(diff) == 1:
+                want.add((c, diff[0], int(conn[p, diff[0]])))
+            elif not diff:
+                want |= {(c, k, int(conn[p, k])) for k in range(d)}
+        assert got == want, r
