@@ -1,13 +1,14 @@
 """Times the kronmult apply kernel on a synthetic sparse-grid operator.
 
     python -m asgard_b200.profile_apply --d 4 --level 7 --terms 4 \
-        --precision fp64 --reps 3 [--warmup 1]
+        --precision fp64 --reps 3 [--warmup 1] [--mode global]
 
 Builds the operator (advection/diffusion factors unless --kind random), runs
 --warmup untimed applies of the fused backward-Euler operator
 y = x - dt*K*x, then --reps timed applies (CUDA events on the launching
 stream) and prints one JSON line: ms per launch, algorithmic TFLOP/s
-(2*d*T*n^(d+1) flops per pair) and the fraction of the measured FMA peak.
+(2*d*T*n^(d+1) flops per pair; 2*n^(d+1) per single-direction pair in the
+global form) and the fraction of the measured FMA peak.
 This is the command the ncu summaries under profiles/ were taken with.
 """
 from __future__ import annotations
@@ -28,6 +29,8 @@ def main():
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=1)
     ap.add_argument("--peak", action="store_true", help="also measure the FMA peak")
+    ap.add_argument("--mode", default="pairs", choices=["pairs", "global"],
+                    help="connected-pair kronmult or the global Kronecker form")
     args = ap.parse_args()
 
     import torch
@@ -35,7 +38,7 @@ def main():
 
     t0 = time.perf_counter()
     op = ab.SparseGridOperator(args.d, args.level, args.terms, kind=args.kind)
-    mat = op.kronmult_matrix()
+    mat = op.kronmult_matrix(mode=args.mode)
     t_setup = time.perf_counter() - t0
     g = torch.Generator(device="cuda").manual_seed(0)
     x = torch.rand(op.N, dtype=torch.float64, device="cuda", generator=g) * 2 - 1
@@ -51,8 +54,9 @@ def main():
     e1.record()
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / args.reps
-    flops = op.flops()
-    out = {"d": args.d, "level": args.level, "terms": args.terms,
+    flops = mat.flops()
+    out = {"d": args.d, "level": args.level, "terms": args.terms, "mode": args.mode,
+           "num_batch": mat.num_batch(),
            "precision": args.precision, "cells": op.rows, "pairs": op.nnz,
            "dofs": op.N, "ms_per_launch": ms, "tflops": flops / ms / 1e9,
            "flops_per_launch": flops, "setup_s": t_setup,

@@ -6,11 +6,17 @@ advection/diffusion factors, solve (I - dt*K) x = b with dt = 1e-3,
 b uniform in [-1, 1] (seeded, a new b every step), GMRES restart 50, until the
 FP64 relative residual ||b - (I - dt K) x|| / ||b|| <= 1e-10.
 
-A step is one solve by the framework's method (mixed-precision FGMRES with
-FP64 iterative refinement; the plain FP64 GMRES with the FP64 kronmult is
-timed beside it).  Inputs are resident in HBM when the timed region starts;
-the operator (pair list + factor indices, ~245 MB) is larger than L2, so
-no extra L2 flush is done between steps.
+A step is one solve by the framework's method: the operator in its global
+Kronecker form (the reference's global_kron_matrix; the same operator as
+the connected-pair kronmult, its terms acting in one dimension each),
+block-Jacobi right preconditioning (the learned correction on top of it is
+trained and kept only if its validation solve gains), FP32 operator inside
+FP64 iterative refinement.  Timed beside it: the north star's plain
+baseline -- FP64 GMRES with the connected-pair FP64 kronmult -- and the same
+method on the connected-pair operator.  Inputs are resident in HBM when the
+timed region starts; the plain baseline's operator (pair list + factor
+indices, ~245 MB) is larger than L2; no extra L2 flush is done between
+steps (the method's working set is L2-sized by design).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
@@ -56,6 +62,8 @@ def parse():
                     choices=["learned-block-fp32", "learned-block-fp64",
                              "block-fp32", "block-fp64", "learned-fp32",
                              "learned-fp64", "fp32", "fp64"])
+    ap.add_argument("--operator", default="global", choices=["global", "pairs"],
+                    help="the method's operator form (plain FP64 always uses pairs)")
     ap.add_argument("--train-solves", type=int, default=1)
     ap.add_argument("--train-epochs", type=int, default=60)
     return ap.parse_args()
@@ -195,6 +203,16 @@ PLAIN_ITERATIONS = {"d4": 230}
 # DRAM bytes per launch of the dominant kernel from one ncu capture
 # (profiles/kron3_staged_d4_L7_fp64.md); None where none was taken.
 KERNEL_TRAFFIC = {"d4": 254_243_328 + 4_232_704}
+# the same for the global form's kernel (profiles/kron_global_rows_d4_L7.md)
+GLOBAL_TRAFFIC = {"d4": 3_874_560 + 0}
+
+
+def _measured_hbm_gbs():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"])
+    except (OSError, KeyError, ValueError):
+        return 6650.0
 
 
 def _plain_iterations(workload):
@@ -227,8 +245,17 @@ def main():
     cfg = WORKLOADS[args.workload]
     d, L, T, dt = cfg["d"], cfg["level"], cfg["terms"], cfg["dt"]
     op = ab.SparseGridOperator(d, L, T, kind=cfg["kind"], nu=cfg["nu"])
-    mat = op.kronmult_matrix()
+    mat = op.kronmult_matrix()          # connected pairs: the plain baseline
     N = op.N
+    # the method's operator: the global Kronecker form of the same operator
+    # (terms acting in one dimension each) unless --operator pairs
+    gmat = None
+    if args.operator == "global":
+        try:
+            gmat = op.kronmult_matrix(mode="global")
+        except ab.AsgkError:
+            gmat = None
+    mmat = gmat if gmat is not None else mat
     gen = torch.Generator(device="cuda").manual_seed(replicas.rhs_seed(rank))
     nb = args.warmup + args.steps
     B = [torch.rand(N, dtype=torch.float64, device="cuda", generator=gen) * 2 - 1
@@ -238,7 +265,7 @@ def main():
     # inverses (cells with n^d <= 81) and the learned network's training
     base = None
     if "block" in args.method and 3 ** d <= 81:
-        base = ab.JacobiPreconditioner(mat, dt, kind="block")
+        base = ab.JacobiPreconditioner(mmat, dt, kind="block")
     pc, train_info = base, None
     if args.method.startswith("learned"):
         # plain FP64 GMRES solves of random right-hand sides give (v, e)
@@ -248,10 +275,15 @@ def main():
         net = ab.LearnedPreconditioner(op, seed=rank)
         if base is not None:
             net.set_base(base)
-        train_info = net.train(mat, dt, num_solves=args.train_solves,
+        if gmat is not None:
+            from asgard_b200.operators import transpose_factor_values
+            mat_T = ab.kronmult_matrix.from_global(
+                d, 3, L, op.table, T, transpose_factor_values(op.vA, d, L, T))
+        else:
+            mat_T = op.kronmult_matrix_transposed()
+        train_info = net.train(mmat, dt, num_solves=args.train_solves,
                                epochs=args.train_epochs, batch=1024, lr=1e-3,
-                               seed=rank, mat_T=op.kronmult_matrix_transposed(),
-                               residual_epochs=20)
+                               seed=rank, mat_T=mat_T, residual_epochs=20)
         torch.cuda.synchronize()
         train_info["setup_s"] = time.perf_counter() - t0
         # the validation solve decides: without a gain the method continues
@@ -268,11 +300,14 @@ def main():
     elif learned:
         parts.append("no preconditioner" + dropped)
     parts.append("FP32 operator, FP64 refinement" if precision == "fp32" else "FP64")
+    parts.insert(0, "global Kronecker operator" if gmat is not None
+                 else "connected-pair operator")
     method = dict(precision=precision, precond=pc, name=", ".join(parts))
 
-    def solve(b, precision, precond=None):
+    def solve(b, precision, precond=None, m=None):
         x = torch.zeros(N, dtype=torch.float64, device="cuda")
-        info = ab.simple_gmres_euler(dt, mat, x, b, RESTART, 200, TOL,
+        info = ab.simple_gmres_euler(dt, m if m is not None else mmat, x, b,
+                                     RESTART, 200, TOL,
                                      tol_mode="rel", precision=precision,
                                      precond=precond)
         return x, info
@@ -282,7 +317,7 @@ def main():
     for i in range(args.warmup):
         _, info = solve(B[i], method["precision"], method["precond"])
         infos.append(info)
-    _, pinfo = solve(B[0], "fp64")
+    _, pinfo = solve(B[0], "fp64", None, mat)
 
     # ---- timed: the method
     launches0 = ab.launch_count()
@@ -309,7 +344,7 @@ def main():
     e0.record()
     pinfos = []
     for i in range(args.plain_steps):
-        _, info = solve(B[i], "fp64")
+        _, info = solve(B[i], "fp64", None, mat)
         pinfos.append(info)
     e1.record()
     replicas.barrier()
@@ -317,31 +352,80 @@ def main():
     t_plain = replicas.max_over_ranks(t_local)
     plain_value = replicas.throughput(args.plain_steps, t_local)
 
-    # ---- roofline: the dominant kernel (FP64 kronmult, and the FP32 one
-    # used inside the method), average launch duration by CUDA events
+    # ---- timed: the same method on the connected-pair operator
+    pair_method = None
+    if gmat is not None:
+        replicas.barrier()
+        e0.record()
+        qinfos = []
+        for i in range(args.plain_steps):
+            _, info = solve(B[i], method["precision"], method["precond"], mat)
+            qinfos.append(info)
+        e1.record()
+        replicas.barrier()
+        t_local = e0.elapsed_time(e1) / 1e3
+        pair_method = {"value": replicas.throughput(args.plain_steps, t_local),
+                       "unit": "solves/s",
+                       "iterations": [i.iterations for i in qinfos],
+                       "true_relres": max(i.true_relres for i in qinfos)}
+
+    # ---- rooflines by CUDA events (average launch duration): the
+    # connected-pair kronmult (FP64, the plain baseline's kernel, and FP32)
+    # and the method's operator kernel
     xs = B[0]
     ys = torch.zeros_like(xs)
     flops = op.flops()
     reps = 5
 
-    def time_apply(precision):
-        mat.apply_euler(dt, 1.0, xs, 0.0, ys, precision=precision)
+    def time_apply(m, precision):
+        m.apply_euler(dt, 1.0, xs, 0.0, ys, precision=precision)
         torch.cuda.synchronize()
         a0 = torch.cuda.Event(enable_timing=True)
         a1 = torch.cuda.Event(enable_timing=True)
         a0.record()
         for _ in range(reps):
-            mat.apply_euler(dt, 1.0, xs, 0.0, ys, precision=precision)
+            m.apply_euler(dt, 1.0, xs, 0.0, ys, precision=precision)
         a1.record()
         torch.cuda.synchronize()
         return a0.elapsed_time(a1) / 1e3 / reps
 
-    t64 = time_apply("fp64")
-    t32 = time_apply("fp32")
+    t64 = time_apply(mat, "fp64")
+    t32 = time_apply(mat, "fp32")
     fp64_peak = ab._lib.C.c_double()
     ab.lib.asgk_measure_fma_peak(0, ab._lib.C.byref(fp64_peak))
     fp32_peak = ab._lib.C.c_double()
     ab.lib.asgk_measure_fma_peak(1, ab._lib.C.byref(fp32_peak))
+    pair_roof = {"bound": "fp64", "kernel": "kron3_staged<d=4, fp64> (+ x repack)",
+                 "achieved": flops / t64 / 1e12, "peak": fp64_peak.value,
+                 "peak_source": "measured live (FMA chain kernel)",
+                 "unit": "TFLOP/s", "frac": flops / t64 / 1e12 / fp64_peak.value,
+                 "traffic": KERNEL_TRAFFIC.get(args.workload),
+                 "traffic_source": "ncu dram__bytes_read+write, one launch",
+                 "ms_per_launch": t64 * 1e3, "flops_per_launch": flops,
+                 "fp32_kernel": {"ms_per_launch": t32 * 1e3,
+                                 "achieved": flops / t32 / 1e12,
+                                 "peak": fp32_peak.value,
+                                 "frac": flops / t32 / 1e12 / fp32_peak.value}}
+    if gmat is not None:
+        # the method's operator kernel: algorithmic bytes per launch are x
+        # read once, y written, the neighbour lists and the pre-summed blocks
+        tg = time_apply(gmat, method["precision"])
+        nbytes = (16 * N + 8 * gmat.num_batch() + 8 * (op.rows + 1)
+                  + 48 * len(op.vA) // (9 * T))
+        hbm = _measured_hbm_gbs()
+        roofline = {"bound": "hbm",
+                    "kernel": f"kron_global_rows<d={d}, {method['precision']}>",
+                    "achieved": nbytes / tg / 1e9, "peak": hbm,
+                    "peak_source": "MEASURED_PEAKS.json hbm_gbs" if hbm != 6650.0
+                                   else "fallback 6.65 TB/s",
+                    "unit": "GB/s", "frac": nbytes / tg / 1e9 / hbm,
+                    "traffic": GLOBAL_TRAFFIC.get(args.workload),
+                    "traffic_source": "ncu dram__bytes_read+write, one launch",
+                    "bytes_per_launch": nbytes, "ms_per_launch": tg * 1e3,
+                    "note": "working set L2-resident; launch/latency bound",
+                    "pair_kernel": pair_roof}
+    else:
+        roofline = pair_roof
 
     # ---- e2e through the public API with host buffers
     e2e_value = None
@@ -365,7 +449,6 @@ def main():
         cpu = cpu_baseline(op, cfg, pinfo.iterations)
 
     if rank == 0:
-        achieved = flops / t64 / 1e12
         line = {
             "metric": METRIC, "value": value, "unit": "solves/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -392,18 +475,8 @@ def main():
             "e2e": {"value": e2e_value, "unit": "solves/s",
                     "h2d_bytes_per_step": N * 8, "d2h_bytes_per_step": N * 8},
             "gpu_launches": launches,
-            "roofline": {"bound": "fp64", "kernel": "kron3_staged<d=4, fp64> (+ x repack)",
-                         "achieved": achieved, "peak": fp64_peak.value,
-                         "peak_source": "measured live (FMA chain kernel)",
-                         "unit": "TFLOP/s", "frac": achieved / fp64_peak.value,
-                         "traffic": KERNEL_TRAFFIC.get(args.workload),
-                         "traffic_source": "ncu dram__bytes_read+write, one launch",
-                         "ms_per_launch": t64 * 1e3,
-                         "flops_per_launch": flops,
-                         "fp32_kernel": {"ms_per_launch": t32 * 1e3,
-                                         "achieved": flops / t32 / 1e12,
-                                         "peak": fp32_peak.value,
-                                         "frac": flops / t32 / 1e12 / fp32_peak.value}},
+            "pair_operator_method": pair_method,
+            "roofline": roofline,
             "cpu_baseline": cpu,
         }
         print(json.dumps(line))
