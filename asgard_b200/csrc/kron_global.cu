@@ -29,8 +29,10 @@ template<typename TC> struct padG;
 template<> struct padG<double> { static constexpr int value = 10; };
 template<> struct padG<float> { static constexpr int value = 12; };
 
-// One CTA per output cell; its NW warps take the cell's entries in turn (two
-// in flight per warp), each warp holding a partial output tensor (PER
+// One CTA per output cell.  The cell's neighbour list is staged in shared
+// memory (coalesced, CAP entries at a time) so that the neighbours' tensor
+// loads do not wait on their indices; the NW warps take the entries in turn,
+// four in flight per warp, each warp holding a partial output tensor (PER
 // entries per lane), summed over the warps in shared memory at the end.
 template<int D, typename TC, int NW>
 __global__ void __launch_bounds__(NW * 32)
@@ -43,8 +45,12 @@ __global__ void __launch_bounds__(NW * 32)
   constexpr int TS  = ipow3g(D);
   constexpr int PER = (TS + 31) / 32; // outputs per lane
   constexpr int PAD = padG<TC>::value;
+  constexpr int CAP = 512;
+  constexpr int NT  = NW * 32;
   extern __shared__ __align__(16) unsigned char smem_g[];
-  TC *red = reinterpret_cast<TC *>(smem_g); // [NW][TS]
+  TC *red    = reinterpret_cast<TC *>(smem_g);          // [NW][TS]
+  int *s_col = reinterpret_cast<int *>(red + NW * TS);  // [CAP]
+  int *s_kb  = s_col + CAP;                             // [CAP]
 
   int const warp     = threadIdx.x >> 5;
   int const lane     = threadIdx.x & 31;
@@ -57,9 +63,9 @@ __global__ void __launch_bounds__(NW * 32)
   for (int o = 0; o < PER; o++)
     acc[o] = TC(0);
 
-  auto entry = [&](int64_t e) {
-    int const c  = __ldg(gcol + e);
-    int const kb = __ldg(gkb + e);
+  auto entry = [&](int j) {
+    int const c  = s_col[j];
+    int const kb = s_kb[j];
     int const k  = kb % D;
     const TC *b  = B + int64_t(kb) * PAD;
     const double *xc = x + int64_t(c) * TS;
@@ -85,11 +91,26 @@ __global__ void __launch_bounds__(NW * 32)
       }
     }
   };
-  for (int64_t e = ebeg + warp; e < eend; e += 2 * NW)
+  for (int64_t cb = ebeg; cb < eend; cb += CAP)
   {
-    entry(e);
-    if (e + NW < eend)
-      entry(e + NW);
+    int const n = int((eend - cb < CAP) ? (eend - cb) : CAP);
+    __syncthreads(); // the previous chunk's entries are consumed
+    for (int i = threadIdx.x; i < n; i += NT)
+    {
+      s_col[i] = __ldg(gcol + cb + i);
+      s_kb[i]  = __ldg(gkb + cb + i);
+    }
+    __syncthreads();
+    for (int j = warp; j < n; j += 4 * NW)
+    {
+      entry(j);
+      if (j + NW < n)
+        entry(j + NW);
+      if (j + 2 * NW < n)
+        entry(j + 2 * NW);
+      if (j + 3 * NW < n)
+        entry(j + 3 * NW);
+    }
   }
 #pragma unroll
   for (int o = 0; o < PER; o++)
@@ -100,7 +121,7 @@ __global__ void __launch_bounds__(NW * 32)
   }
   __syncthreads();
   int64_t const base = int64_t(row) * TS;
-  for (int i = threadIdx.x; i < TS; i += NW * 32)
+  for (int i = threadIdx.x; i < TS; i += NT)
   {
     TC s = TC(0);
 #pragma unroll
@@ -119,22 +140,19 @@ int launch_global_d(plan_data const &p, double alpha, const double *x,
 {
   constexpr int TS = ipow3g(D);
   constexpr int NW = TS <= 27 ? 4 : 8;
-  size_t const shm = size_t(NW) * TS * sizeof(TC);
+  size_t const shm = size_t(NW) * TS * sizeof(TC) + 2 * 512 * sizeof(int);
   const TC *B;
   if constexpr (sizeof(TC) == 8)
     B = p.gB64;
   else
     B = p.gB32;
   auto kern = kron_global_rows<D, TC, NW>;
-  if (shm > 48 * 1024)
+  static bool configured = false;
+  if (!configured)
   {
-    static bool configured = false;
-    if (!configured)
-    {
-      ASGK_CUDA(cudaFuncSetAttribute(
-          kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shm)));
-      configured = true;
-    }
+    ASGK_CUDA(cudaFuncSetAttribute(
+        kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shm)));
+    configured = true;
   }
   kern<<<p.rows, NW * 32, shm, s>>>(p.gptr, p.gcol, p.gkb, B, p.row_order,
                                     alpha, x, beta, y, ex);

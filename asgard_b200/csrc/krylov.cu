@@ -109,33 +109,37 @@ __global__ void k_xpby(double *__restrict__ y, const double *__restrict__ x,
     y[i] = x[i] + b * y[i];
 }
 
-// part[b*k + j] = sum over block b's rows of V[r, j] * w[r]
+// part[b*k + j] = sum over row chunk b of V[r, j] * w[r]; block (b, g)
+// takes the columns 8g .. 8g+7 of chunk b (one block reduction each)
+constexpr int kDotCols = 8;
 __global__ void __launch_bounds__(kThreads)
     k_multidot(const double *__restrict__ V, int64_t ldv, int k,
                const double *__restrict__ w, int64_t n,
                double *__restrict__ part)
 {
-  __shared__ double sh[4 * 32];
+  __shared__ double sh[kDotCols * 32];
   int64_t const chunk = (n + gridDim.x - 1) / gridDim.x;
   int64_t const beg   = blockIdx.x * chunk;
   int64_t const end   = min(n, beg + chunk);
-  for (int j0 = 0; j0 < k; j0 += 4)
-  {
-    double a[4] = {0, 0, 0, 0};
-    int const nj = min(4, k - j0);
-    for (int64_t r = beg + threadIdx.x; r < end; r += blockDim.x)
-    {
-      double const wr = w[r];
+  int const j0        = blockIdx.y * kDotCols;
+  int const nj        = min(kDotCols, k - j0);
+  double a[kDotCols];
 #pragma unroll
-      for (int j = 0; j < 4; j++)
-        if (j < nj)
-          a[j] += V[r + (j0 + j) * ldv] * wr;
-    }
-    block_sum<4>(a, sh);
-    if (threadIdx.x == 0)
-      for (int j = 0; j < nj; j++)
-        part[int64_t(blockIdx.x) * k + j0 + j] = a[j];
+  for (int j = 0; j < kDotCols; j++)
+    a[j] = 0.0;
+  const double *Vj = V + int64_t(j0) * ldv;
+  for (int64_t r = beg + threadIdx.x; r < end; r += blockDim.x)
+  {
+    double const wr = w[r];
+#pragma unroll
+    for (int j = 0; j < kDotCols; j++)
+      if (j < nj)
+        a[j] = fma(Vj[r + j * ldv], wr, a[j]);
   }
+  block_sum<kDotCols>(a, sh);
+  if (threadIdx.x == 0)
+    for (int j = 0; j < nj; j++)
+      part[int64_t(blockIdx.x) * k + j0 + j] = a[j];
 }
 
 __global__ void k_reduce_parts(const double *__restrict__ part, int blocks,
@@ -151,7 +155,26 @@ __global__ void k_reduce_parts(const double *__restrict__ part, int blocks,
     out[j] = v[0];
 }
 
-// w -= V[:, :k] h ; part[b] = sum of w^2 over block b's rows
+// w -= V[:, :k] h ; part[b] = sum of w^2 over block b's rows.  Four
+// independent partial sums per row keep four basis loads in flight.
+__device__ __forceinline__ double dot_row(const double *__restrict__ V,
+                                          int64_t ldv, int k, int64_t r,
+                                          const double *hs)
+{
+  double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+  int j = 0;
+  for (; j + 4 <= k; j += 4)
+  {
+    s0 = fma(V[r + j * ldv], hs[j], s0);
+    s1 = fma(V[r + (j + 1) * ldv], hs[j + 1], s1);
+    s2 = fma(V[r + (j + 2) * ldv], hs[j + 2], s2);
+    s3 = fma(V[r + (j + 3) * ldv], hs[j + 3], s3);
+  }
+  for (; j < k; j++)
+    s0 = fma(V[r + j * ldv], hs[j], s0);
+  return (s0 + s1) + (s2 + s3);
+}
+
 __global__ void __launch_bounds__(kThreads)
     k_update_norm(const double *__restrict__ V, int64_t ldv, int k,
                   const double *__restrict__ h, double *__restrict__ w,
@@ -168,10 +191,7 @@ __global__ void __launch_bounds__(kThreads)
   double v[1]         = {0.0};
   for (int64_t r = beg + threadIdx.x; r < end; r += blockDim.x)
   {
-    double s = 0.0;
-    for (int j = 0; j < k; j++)
-      s += V[r + j * ldv] * hs[j];
-    double const wr = w[r] - s;
+    double const wr = w[r] - dot_row(V, ldv, k, r, hs);
     w[r]            = wr;
     v[0] += wr * wr;
   }
@@ -206,12 +226,7 @@ __global__ void __launch_bounds__(kThreads)
   __syncthreads();
   for (int64_t r = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; r < n;
        r += int64_t(gridDim.x) * blockDim.x)
-  {
-    double s = 0.0;
-    for (int j = 0; j < k; j++)
-      s += V[r + j * ldv] * ys[j];
-    x[r] += s;
-  }
+    x[r] += dot_row(V, ldv, k, r, ys);
 }
 
 } // namespace
@@ -257,7 +272,8 @@ int launch_multidot(const double *V, int64_t ldv, int k, const double *w,
                     int64_t n, double *part, int *blocks, cudaStream_t s)
 {
   int const g = grid_for(n);
-  k_multidot<<<g, kThreads, 0, s>>>(V, ldv, k, w, n, part);
+  dim3 const grid(g, (k + kDotCols - 1) / kDotCols);
+  k_multidot<<<grid, kThreads, 0, s>>>(V, ldv, k, w, n, part);
   ASGK_LAUNCHED();
   *blocks = g;
   return ASGK_OK;

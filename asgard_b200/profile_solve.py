@@ -1,0 +1,75 @@
+"""Times implicit-step GMRES solves on a synthetic sparse-grid operator.
+
+    python -m asgard_b200.profile_solve --d 4 --level 7 --terms 4 --dt 1e-3 \
+        --mode global --precond block --precision fp32 --solves 3 [--warmup 1]
+
+Builds the operator (connected pairs or the global Kronecker form), the
+preconditioner (none, point or block Jacobi), runs --warmup untimed and
+--solves timed solves of (I - dt K) x = b to a 1e-10 FP64 relative residual
+(GMRES restart 50, a new seeded b per solve) and prints one JSON line with
+the seconds per solve (CUDA events), iterations and residuals.  Used for
+per-kernel captures of a solve (`ncu ... python -m asgard_b200.profile_solve`).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import time
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--d", type=int, default=4)
+    ap.add_argument("--level", type=int, default=7)
+    ap.add_argument("--terms", type=int, default=4)
+    ap.add_argument("--dt", type=float, default=1e-3)
+    ap.add_argument("--mode", default="global", choices=["pairs", "global"])
+    ap.add_argument("--precond", default="block", choices=["none", "point", "block"])
+    ap.add_argument("--precision", default="fp32", choices=["fp64", "fp32"])
+    ap.add_argument("--restart", type=int, default=50)
+    ap.add_argument("--tol", type=float, default=1e-10)
+    ap.add_argument("--solves", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=1)
+    args = ap.parse_args()
+
+    import torch
+    import asgard_b200 as ab
+
+    t0 = time.perf_counter()
+    op = ab.SparseGridOperator(args.d, args.level, args.terms)
+    mat = op.kronmult_matrix(mode=args.mode)
+    pc = None if args.precond == "none" else ab.JacobiPreconditioner(mat, args.dt, kind=args.precond)
+    torch.cuda.synchronize()
+    setup = time.perf_counter() - t0
+    g = torch.Generator(device="cuda").manual_seed(0)
+    bs = [torch.rand(op.N, dtype=torch.float64, device="cuda", generator=g) * 2 - 1
+          for _ in range(args.warmup + args.solves)]
+
+    def solve(b):
+        x = torch.zeros_like(b)
+        return ab.simple_gmres_euler(args.dt, mat, x, b, args.restart, 400, args.tol,
+                                     tol_mode="rel", precision=args.precision,
+                                     precond=pc)
+
+    for i in range(args.warmup):
+        solve(bs[i])
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    infos = [solve(bs[args.warmup + i]) for i in range(args.solves)]
+    e1.record()
+    torch.cuda.synchronize()
+    s = e0.elapsed_time(e1) / 1e3 / args.solves
+    print(json.dumps({"d": args.d, "level": args.level, "terms": args.terms,
+                      "mode": args.mode, "precond": args.precond,
+                      "precision": args.precision, "dofs": op.N,
+                      "s_per_solve": s, "solves_per_s": 1.0 / s,
+                      "iterations": [i.iterations for i in infos],
+                      "true_relres": max(i.true_relres for i in infos),
+                      "ms_per_iteration": s * 1e3 / (sum(i.iterations for i in infos) / len(infos)),
+                      "setup_s": setup}))
+
+
+if __name__ == "__main__":
+    main()

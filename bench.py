@@ -395,7 +395,9 @@ def main():
     ab.lib.asgk_measure_fma_peak(0, ab._lib.C.byref(fp64_peak))
     fp32_peak = ab._lib.C.c_double()
     ab.lib.asgk_measure_fma_peak(1, ab._lib.C.byref(fp32_peak))
-    pair_roof = {"bound": "fp64", "kernel": "kron3_staged<d=4, fp64> (+ x repack)",
+    pair_kernel = (f"kron3_staged<d={d}, fp64> (+ x repack)" if d in (3, 4)
+                   else f"kron3_rows<d={d}, fp64>")
+    pair_roof = {"bound": "fp64", "kernel": pair_kernel,
                  "achieved": flops / t64 / 1e12, "peak": fp64_peak.value,
                  "peak_source": "measured live (FMA chain kernel)",
                  "unit": "TFLOP/s", "frac": flops / t64 / 1e12 / fp64_peak.value,
