@@ -48,6 +48,13 @@ void free_plan(plan_data &p)
   cudaFree(p.gkb);
   cudaFree(p.gB64);
   cudaFree(p.gB32);
+  cudaFree(p.slice_row);
+  cudaFree(p.slice_len);
+  cudaFree(p.slice_beg);
+  cudaFree(p.row_slice0);
+  cudaFree(p.row_nslice);
+  cudaFree(p.gscratch);
+  cudaFree(p.gtickets);
   cudaFree(p.vP64);
   cudaFree(p.vP32);
   p = plan_data{};
@@ -868,13 +875,49 @@ int asgk_plan_create_global(asgk_plan **plan, int d, int n, int level,
     return ASGK_OK;
   };
   // cells with the most single-direction neighbours first (coarse cells
-  // reach every cell of a dimension: up to 2^level per dimension)
+  // reach every cell of a dimension: up to 2^level per dimension), each
+  // cell's list cut into slices of at most kGlobalSlice entries
   std::vector<int> order(num_cells);
   std::iota(order.begin(), order.end(), 0);
   std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
     return (gptr[a + 1] - gptr[a]) > (gptr[b + 1] - gptr[b]);
   });
+  std::vector<int> srow, slen, rs0(num_cells), rns(num_cells);
+  std::vector<int64_t> sbeg;
+  for (int r : order)
+  {
+    int64_t const e = gptr[r + 1] - gptr[r];
+    int const ns    = int(std::max<int64_t>(1, (e + kGlobalSlice - 1) / kGlobalSlice));
+    rs0[r] = int(srow.size());
+    rns[r] = ns;
+    for (int q = 0; q < ns; q++)
+    {
+      srow.push_back(r);
+      sbeg.push_back(gptr[r] + int64_t(q) * kGlobalSlice);
+      slen.push_back(int(std::min<int64_t>(kGlobalSlice, e - int64_t(q) * kGlobalSlice)));
+    }
+  }
+  p.gslices = int(srow.size());
+  if ((rc = dev_alloc(&p.slice_row, p.gslices, bytes)) ||
+      (rc = dev_alloc(&p.slice_len, p.gslices, bytes)) ||
+      (rc = dev_alloc(&p.slice_beg, p.gslices, bytes)) ||
+      (rc = dev_alloc(&p.row_slice0, num_cells, bytes)) ||
+      (rc = dev_alloc(&p.row_nslice, num_cells, bytes)) ||
+      (rc = dev_alloc(&p.gscratch, int64_t(p.gslices) * p.tensor, bytes)) ||
+      (rc = dev_alloc(&p.gtickets, num_cells, bytes)))
+  {
+    asgk_plan_destroy(*plan);
+    *plan = nullptr;
+    return rc;
+  }
+  std::vector<unsigned> zeros(num_cells, 0u);
   if ((rc = up(p.row_order, order.data(), sizeof(int) * order.size())) ||
+      (rc = up(p.slice_row, srow.data(), sizeof(int) * srow.size())) ||
+      (rc = up(p.slice_len, slen.data(), sizeof(int) * slen.size())) ||
+      (rc = up(p.slice_beg, sbeg.data(), sizeof(int64_t) * sbeg.size())) ||
+      (rc = up(p.row_slice0, rs0.data(), sizeof(int) * rs0.size())) ||
+      (rc = up(p.row_nslice, rns.data(), sizeof(int) * rns.size())) ||
+      (rc = up(p.gtickets, zeros.data(), sizeof(unsigned) * zeros.size())) ||
       (rc = up(p.gptr, gptr.data(), sizeof(int64_t) * gptr.size())) ||
       (rc = up(p.gcol, gcol.data(), sizeof(int) * gcol.size())) ||
       (rc = up(p.gkb, gkb.data(), sizeof(int) * gkb.size())) ||

@@ -40,6 +40,9 @@ inline void count_launch(int k = 1) { g_launches.fetch_add(k, std::memory_order_
     ::asgk::count_launch();                                                    \
   } while (0)
 
+// Entries of a global-form neighbour list handled by one CTA.
+constexpr int kGlobalSlice = 64;
+
 // How the factor blocks of a pair are addressed.
 enum class index_mode : int
 {
@@ -88,6 +91,14 @@ struct plan_data
   float *gB32  = nullptr; // [nconn*d][12]
   double g_identity = 0;  // number of terms that are the identity
   std::vector<int> g_conn_row, g_conn_col; // 1D cells of each 1D connection
+  // the neighbour lists cut into slices of at most kGlobalSlice entries, one
+  // CTA each; slices of one cell have consecutive ids (heavy cells first)
+  int gslices = 0;
+  int *slice_row = nullptr, *slice_len = nullptr;  // [gslices]
+  int64_t *slice_beg = nullptr;                    // [gslices]
+  int *row_slice0 = nullptr, *row_nslice = nullptr; // [rows]
+  double *gscratch = nullptr;  // [gslices * n^d] partial tensors
+  unsigned *gtickets = nullptr; // [rows], zero between launches
   int64_t device_bytes = 0;
 };
 

@@ -25,92 +25,125 @@ namespace
 {
 constexpr int ipow3g(int k) { return k == 0 ? 1 : 3 * ipow3g(k - 1); }
 
+constexpr int kSlice = kGlobalSlice; // neighbour-list entries per CTA
+
 template<typename TC> struct padG;
 template<> struct padG<double> { static constexpr int value = 10; };
 template<> struct padG<float> { static constexpr int value = 12; };
 
-// One CTA per output cell.  The cell's neighbour list is staged in shared
-// memory (coalesced, CAP entries at a time) so that the neighbours' tensor
-// loads do not wait on their indices; the NW warps take the entries in turn,
-// four in flight per warp, each warp holding a partial output tensor (PER
-// entries per lane), summed over the warps in shared memory at the end.
+// Stride of dimension k in a 3^D tensor (dimension 0 slowest), 3^(D-1-k):
+// byte k of the packed constant.
+template<int D>
+__device__ __forceinline__ int dim_stride(int k)
+{
+  constexpr unsigned long long packed =
+      D == 1 ? 0x01ull : D == 2 ? 0x0103ull : D == 3 ? 0x010309ull
+      : D == 4 ? 0x0103091bull : D == 5 ? 0x0103091b51ull : 0x0103091b51f3ull;
+  return int((packed >> (8 * k)) & 0xff);
+}
+
+// One CTA per slice of at most kSlice entries of an output cell's
+// neighbour list.  The NW warps take the slice's entries in turn (four in
+// flight per warp), each warp holding a partial output tensor (PER entries
+// per lane, with their base-3 digits packed two bits per dimension), summed
+// over the warps in shared memory.  A cell with one slice writes y at once;
+// the slices of a cell with several write partial tensors to scratch, and
+// the last of them to finish (an atomic ticket, no waiting) adds them in
+// slice order and writes y -- deterministic whichever slice ends last.
 template<int D, typename TC, int NW>
 __global__ void __launch_bounds__(NW * 32)
-    kron_global_rows(const int64_t *__restrict__ gptr,
+    kron_global_rows(const int *__restrict__ slice_row,
+                     const int64_t *__restrict__ slice_beg,
+                     const int *__restrict__ slice_len,
+                     const int *__restrict__ row_slice0,
+                     const int *__restrict__ row_nslice,
                      const int *__restrict__ gcol, const int *__restrict__ gkb,
-                     const TC *__restrict__ B, const int *__restrict__ row_order,
-                     double alpha, const double *__restrict__ x, double beta,
+                     const TC *__restrict__ B, double *__restrict__ scratch,
+                     unsigned *__restrict__ tickets, double alpha,
+                     const double *__restrict__ x, double beta,
                      double *__restrict__ y, double ex)
 {
   constexpr int TS  = ipow3g(D);
   constexpr int PER = (TS + 31) / 32; // outputs per lane
   constexpr int PAD = padG<TC>::value;
-  constexpr int CAP = 512;
   constexpr int NT  = NW * 32;
-  extern __shared__ __align__(16) unsigned char smem_g[];
-  TC *red    = reinterpret_cast<TC *>(smem_g);          // [NW][TS]
-  int *s_col = reinterpret_cast<int *>(red + NW * TS);  // [CAP]
-  int *s_kb  = s_col + CAP;                             // [CAP]
+  __shared__ TC red[NW * TS];
+  __shared__ int s_col[kSlice], s_kb[kSlice];
+  __shared__ unsigned s_ticket;
 
-  int const warp     = threadIdx.x >> 5;
-  int const lane     = threadIdx.x & 31;
-  int const row      = row_order[blockIdx.x];
-  int64_t const ebeg = gptr[row];
-  int64_t const eend = gptr[row + 1];
+  int const warp   = threadIdx.x >> 5;
+  int const lane   = threadIdx.x & 31;
+  int const sl     = blockIdx.x;
+  int const row    = slice_row[sl];
+  int const s0     = row_slice0[row];
+  int const ns     = row_nslice[row];
+  int64_t const eb = slice_beg[sl];
+  int const n      = slice_len[sl];
 
+  for (int i = threadIdx.x; i < n; i += NT)
+  {
+    s_col[i] = __ldg(gcol + eb + i);
+    s_kb[i]  = __ldg(gkb + eb + i);
+  }
+  // base-3 digits of this lane's outputs, two bits per dimension
+  unsigned dig[PER];
+#pragma unroll
+  for (int o = 0; o < PER; o++)
+  {
+    int v = lane + 32 * o;
+    unsigned pk = 0;
+#pragma unroll
+    for (int k = D - 1; k >= 0; k--)
+    {
+      pk |= unsigned(v % 3) << (2 * k);
+      v /= 3;
+    }
+    dig[o] = pk;
+  }
   TC acc[PER];
 #pragma unroll
   for (int o = 0; o < PER; o++)
     acc[o] = TC(0);
+  __syncthreads();
 
   auto entry = [&](int j) {
-    int const c  = s_col[j];
-    int const kb = s_kb[j];
-    int const k  = kb % D;
-    const TC *b  = B + int64_t(kb) * PAD;
+    int const c      = s_col[j];
+    int const kb     = s_kb[j];
+    int const k      = kb % D;
+    int const stride = dim_stride<D>(k);
+    const TC *b      = B + int64_t(kb) * PAD;
     const double *xc = x + int64_t(c) * TS;
-    int stride = 1; // of dimension k in the tensor (dimension 0 slowest)
-#pragma unroll
-    for (int q = D - 1; q > 0; q--)
-      if (q > k)
-        stride *= 3;
+    TC const b0 = __ldg(b), b1 = __ldg(b + 1), b2 = __ldg(b + 2);
+    TC const b3 = __ldg(b + 3), b4 = __ldg(b + 4), b5 = __ldg(b + 5);
+    TC const b6 = __ldg(b + 6), b7 = __ldg(b + 7), b8 = __ldg(b + 8);
 #pragma unroll
     for (int o = 0; o < PER; o++)
     {
       int const i = lane + 32 * o;
       if (i < TS)
       {
-        int const ik   = (i / stride) % 3;
+        int const ik   = int((dig[o] >> (2 * k)) & 3u);
         int const base = i - ik * stride;
-        // row ik of the column-major block: b[ik + 3 j]
         TC const v0 = static_cast<TC>(__ldg(xc + base));
         TC const v1 = static_cast<TC>(__ldg(xc + base + stride));
         TC const v2 = static_cast<TC>(__ldg(xc + base + 2 * stride));
-        acc[o] = fma(__ldg(b + ik + 6), v2,
-                     fma(__ldg(b + ik + 3), v1, fma(__ldg(b + ik), v0, acc[o])));
+        // row ik of the column-major block
+        TC const a0 = ik == 0 ? b0 : (ik == 1 ? b1 : b2);
+        TC const a1 = ik == 0 ? b3 : (ik == 1 ? b4 : b5);
+        TC const a2 = ik == 0 ? b6 : (ik == 1 ? b7 : b8);
+        acc[o] = fma(a2, v2, fma(a1, v1, fma(a0, v0, acc[o])));
       }
     }
   };
-  for (int64_t cb = ebeg; cb < eend; cb += CAP)
+  for (int j = warp; j < n; j += 4 * NW)
   {
-    int const n = int((eend - cb < CAP) ? (eend - cb) : CAP);
-    __syncthreads(); // the previous chunk's entries are consumed
-    for (int i = threadIdx.x; i < n; i += NT)
-    {
-      s_col[i] = __ldg(gcol + cb + i);
-      s_kb[i]  = __ldg(gkb + cb + i);
-    }
-    __syncthreads();
-    for (int j = warp; j < n; j += 4 * NW)
-    {
-      entry(j);
-      if (j + NW < n)
-        entry(j + NW);
-      if (j + 2 * NW < n)
-        entry(j + 2 * NW);
-      if (j + 3 * NW < n)
-        entry(j + 3 * NW);
-    }
+    entry(j);
+    if (j + NW < n)
+      entry(j + NW);
+    if (j + 2 * NW < n)
+      entry(j + 2 * NW);
+    if (j + 3 * NW < n)
+      entry(j + 3 * NW);
   }
 #pragma unroll
   for (int o = 0; o < PER; o++)
@@ -121,17 +154,52 @@ __global__ void __launch_bounds__(NW * 32)
   }
   __syncthreads();
   int64_t const base = int64_t(row) * TS;
+  if (ns == 1)
+  {
+    for (int i = threadIdx.x; i < TS; i += NT)
+    {
+      TC s = TC(0);
+#pragma unroll
+      for (int w = 0; w < NW; w++)
+        s += red[w * TS + i];
+      double v = alpha * static_cast<double>(s) + ex * x[base + i];
+      if (beta != 0.0)
+        v += beta * y[base + i];
+      y[base + i] = v;
+    }
+    return;
+  }
+  // several slices: publish this slice's partial tensor
+  double *mine = scratch + int64_t(sl) * TS;
   for (int i = threadIdx.x; i < TS; i += NT)
   {
     TC s = TC(0);
 #pragma unroll
     for (int w = 0; w < NW; w++)
       s += red[w * TS + i];
-    double v = alpha * static_cast<double>(s) + ex * x[base + i];
+    mine[i] = static_cast<double>(s);
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0)
+    s_ticket = atomicAdd(tickets + row, 1u);
+  __syncthreads();
+  if (s_ticket != unsigned(ns - 1))
+    return;
+  // the last slice of the row: add the slices in order, finish the row
+  __threadfence();
+  for (int i = threadIdx.x; i < TS; i += NT)
+  {
+    double s = 0.0;
+    for (int q = 0; q < ns; q++)
+      s += __ldcg(scratch + int64_t(s0 + q) * TS + i);
+    double v = alpha * s + ex * x[base + i];
     if (beta != 0.0)
       v += beta * y[base + i];
     y[base + i] = v;
   }
+  if (threadIdx.x == 0)
+    tickets[row] = 0u; // ready for the next launch
 }
 
 template<int D, typename TC>
@@ -140,22 +208,14 @@ int launch_global_d(plan_data const &p, double alpha, const double *x,
 {
   constexpr int TS = ipow3g(D);
   constexpr int NW = TS <= 27 ? 4 : 8;
-  size_t const shm = size_t(NW) * TS * sizeof(TC) + 2 * 512 * sizeof(int);
   const TC *B;
   if constexpr (sizeof(TC) == 8)
     B = p.gB64;
   else
     B = p.gB32;
-  auto kern = kron_global_rows<D, TC, NW>;
-  static bool configured = false;
-  if (!configured)
-  {
-    ASGK_CUDA(cudaFuncSetAttribute(
-        kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shm)));
-    configured = true;
-  }
-  kern<<<p.rows, NW * 32, shm, s>>>(p.gptr, p.gcol, p.gkb, B, p.row_order,
-                                    alpha, x, beta, y, ex);
+  kron_global_rows<D, TC, NW><<<p.gslices, NW * 32, 0, s>>>(
+      p.slice_row, p.slice_beg, p.slice_len, p.row_slice0, p.row_nslice, p.gcol, p.gkb, B,
+      p.gscratch, p.gtickets, alpha, x, beta, y, ex);
   ASGK_LAUNCHED();
   return ASGK_OK;
 }
