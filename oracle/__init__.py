@@ -20,6 +20,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libasgard_ref.so")
+REF_GLOBAL_SO = os.path.join(HERE, "_ref", "libasgard_ref_global.so")
 
 _i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
 _f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
@@ -27,6 +28,7 @@ _f32p = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
 
 _oracle = None
 _ref = None
+_ref_global = None
 
 
 def build_oracle(force: bool = False) -> str:
@@ -81,6 +83,70 @@ def oracle():
 
 def ref_available() -> bool:
     return os.path.exists(REF_SO)
+
+
+def _load_blas_deps():
+    # OpenBLAS (linked by the reference builds) finds its private
+    # libgfortran only when that is loaded first from the same folder.
+    import glob, site
+    for sp in site.getsitepackages():
+        deps = glob.glob(os.path.join(sp, "opencv_python_headless.libs", "lib*.so*"))
+        for key in ("quadmath", "gfortran"):
+            for dep in deps:
+                if key in os.path.basename(dep):
+                    C.CDLL(dep, mode=C.RTLD_GLOBAL)
+
+
+def ref_global_available() -> bool:
+    return os.path.exists(REF_GLOBAL_SO)
+
+
+class RefGlobal:
+    """The reference's global Kronecker product (global_cpu,
+    src/device/asgard_glkronmult_cpu.cpp:150-188; built by `make -C oracle
+    ref_global`) on a sparse-grid operator: build once, apply many times."""
+
+    def __init__(self, d, n, level, table, terms, vA):
+        global _ref_global
+        if _ref_global is None:
+            if not ref_global_available():
+                raise FileNotFoundError(REF_GLOBAL_SO)
+            _load_blas_deps()
+            lib = C.CDLL(REF_GLOBAL_SO)
+            lib.ref_global_create.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int,
+                                              _i32p, C.c_int, _f64p]
+            lib.ref_global_create.restype = C.c_void_p
+            lib.ref_global_run.argtypes = [C.c_void_p, C.c_int, _f64p, _f64p,
+                                           C.POINTER(C.c_double)]
+            lib.ref_global_run.restype = C.c_int
+            lib.ref_global_destroy.argtypes = [C.c_void_p]
+            _ref_global = lib
+        self._lib = _ref_global
+        table = np.ascontiguousarray(table, dtype=np.int32)
+        self.N = table.shape[0] * n ** d
+        self._h = self._lib.ref_global_create(d, n, level, table.shape[0], table,
+                                              terms, np.ascontiguousarray(vA, dtype=np.float64))
+        if not self._h:
+            raise ValueError("ref_global_create rejected its input")
+
+    def apply(self, x, reps=1):
+        """y = K x; returns (y, best seconds of one product)."""
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.zeros(self.N)
+        sec = C.c_double()
+        if self._lib.ref_global_run(self._h, reps, x, y, C.byref(sec)) != 0:
+            raise ValueError("ref_global_run failed")
+        return y, sec.value
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            self._lib.ref_global_destroy(self._h)
+            self._h = None
+
+
+def ref_global_apply(d, n, level, table, terms, vA, x, reps=1):
+    """One-shot RefGlobal(...).apply(x, reps)."""
+    return RefGlobal(d, n, level, table, terms, vA).apply(x, reps)
 
 
 def ref():

@@ -110,3 +110,17 @@ def test_global_rejects_multi_direction_terms(cuda):
         op.kronmult_matrix(mode="global")
     with pytest.raises(ValueError):
         op.kronmult_matrix(mode="dense")
+
+
+@pytest.mark.skipif(not oracle.ref_global_available(),
+                    reason="reference global-kron library not built")
+@pytest.mark.parametrize("d,L,T", [(2, 6, 3), (3, 5, 3), (4, 5, 4)])
+def test_global_matches_reference_global_kron(cuda, d, L, T):
+    """The GPU global form against the reference's own global Kronecker
+    product (global_cpu compiled from its sources)."""
+    import asgard_b200 as ab
+    op = ab.SparseGridOperator(d, L, T, kind="advdiff")
+    x = np.random.default_rng(7).uniform(-1, 1, op.N)
+    y_ref, _ = oracle.ref_global_apply(d, 3, L, op.table, T, op.vA, x)
+    g = op.kronmult_matrix(mode="global")
+    assert rel_err(_apply(g, 1.0, x, 0.0, np.zeros(op.N)), y_ref) < 1e-13

@@ -210,3 +210,20 @@ def test_jacobi_restatements_against_dense_assembly():
         assert np.allclose(blocks[c], K[c * ts:(c + 1) * ts, c * ts:(c + 1) * ts], rtol=0, atol=1e-14)
     pc = oracle.point_jacobi_diag(d, 3, pntr, op.col, T, iA, op.vA)
     assert np.allclose(pc, np.diag(K), rtol=0, atol=1e-14)
+
+
+@pytest.mark.skipif(not oracle.ref_global_available(),
+                    reason="reference global-kron library not built (make -C oracle ref_global)")
+@pytest.mark.parametrize("d,L,T", [(1, 5, 2), (2, 5, 3), (3, 4, 3), (4, 3, 4)])
+def test_reference_global_kron_equals_pair_kronmult(d, L, T):
+    """The reference's global Kronecker product (compiled from its sources in
+    KRON_MODE_GLOBAL) and the connected-pair kronmult give the same operator
+    on advection/diffusion factors (terms acting in one dimension each) --
+    the identity the global form of this library rests on."""
+    import asgard_b200.operators as O
+    op = O.SparseGridOperator(d, L, T, kind="advdiff")
+    x = np.random.default_rng(d).uniform(-1, 1, op.N)
+    y_ref, _ = oracle.ref_global_apply(d, 3, L, op.table, T, op.vA, x)
+    y_pair = oracle.kronmult(d, 3, op.row_ptr.astype(np.int32), op.col, T,
+                             op.iA(), op.vA, 1.0, x, 0.0, np.zeros(op.N))
+    assert np.linalg.norm(y_ref - y_pair) <= 1e-13 * np.linalg.norm(y_pair)
