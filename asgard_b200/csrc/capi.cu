@@ -876,7 +876,7 @@ int asgk_plan_create_global(asgk_plan **plan, int d, int n, int level,
   };
   // cells with the most single-direction neighbours first (coarse cells
   // reach every cell of a dimension: up to 2^level per dimension), each
-  // cell's list cut into slices of at most kGlobalSlice entries
+  // cell's list cut into slices of at most global_slice(d) entries
   std::vector<int> order(num_cells);
   std::iota(order.begin(), order.end(), 0);
   std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
@@ -887,14 +887,15 @@ int asgk_plan_create_global(asgk_plan **plan, int d, int n, int level,
   for (int r : order)
   {
     int64_t const e = gptr[r + 1] - gptr[r];
-    int const ns    = int(std::max<int64_t>(1, (e + kGlobalSlice - 1) / kGlobalSlice));
+    int const sz    = global_slice(d);
+    int const ns    = int(std::max<int64_t>(1, (e + sz - 1) / sz));
     rs0[r] = int(srow.size());
     rns[r] = ns;
     for (int q = 0; q < ns; q++)
     {
       srow.push_back(r);
-      sbeg.push_back(gptr[r] + int64_t(q) * kGlobalSlice);
-      slen.push_back(int(std::min<int64_t>(kGlobalSlice, e - int64_t(q) * kGlobalSlice)));
+      sbeg.push_back(gptr[r] + int64_t(q) * sz);
+      slen.push_back(int(std::min<int64_t>(sz, e - int64_t(q) * sz)));
     }
   }
   p.gslices = int(srow.size());

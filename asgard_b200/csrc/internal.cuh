@@ -40,8 +40,10 @@ inline void count_launch(int k = 1) { g_launches.fetch_add(k, std::memory_order_
     ::asgk::count_launch();                                                    \
   } while (0)
 
-// Entries of a global-form neighbour list handled by one CTA.
-constexpr int kGlobalSlice = 64;
+// Entries of a global-form neighbour list handled by one CTA: 32 for
+// tensors of up to 81 entries (4-warp CTAs), 64 above (8 warps).
+constexpr int kGlobalSliceMax = 64;
+constexpr int global_slice(int d) { return d <= 4 ? 32 : 64; }
 
 // How the factor blocks of a pair are addressed.
 enum class index_mode : int
@@ -91,7 +93,7 @@ struct plan_data
   float *gB32  = nullptr; // [nconn*d][12]
   double g_identity = 0;  // number of terms that are the identity
   std::vector<int> g_conn_row, g_conn_col; // 1D cells of each 1D connection
-  // the neighbour lists cut into slices of at most kGlobalSlice entries, one
+  // the neighbour lists cut into slices of at most global_slice(d) entries, one
   // CTA each; slices of one cell have consecutive ids (heavy cells first)
   int gslices = 0;
   int *slice_row = nullptr, *slice_len = nullptr;  // [gslices]

@@ -25,7 +25,6 @@ namespace
 {
 constexpr int ipow3g(int k) { return k == 0 ? 1 : 3 * ipow3g(k - 1); }
 
-constexpr int kSlice = kGlobalSlice; // neighbour-list entries per CTA
 
 template<typename TC> struct padG;
 template<> struct padG<double> { static constexpr int value = 10; };
@@ -43,14 +42,15 @@ __device__ __forceinline__ int dim_stride(int k)
 }
 
 // One CTA per slice of at most kSlice entries of an output cell's
-// neighbour list.  The NW warps take the slice's entries in turn (four in
+// neighbour list (32 up to d = 4, 64 above).  The NW warps take the slice's
+// entries in turn (four in
 // flight per warp), each warp holding a partial output tensor (PER entries
 // per lane, with their base-3 digits packed two bits per dimension), summed
 // over the warps in shared memory.  A cell with one slice writes y at once;
 // the slices of a cell with several write partial tensors to scratch, and
 // the last of them to finish (an atomic ticket, no waiting) adds them in
 // slice order and writes y -- deterministic whichever slice ends last.
-template<int D, typename TC, int NW>
+template<int D, typename TC, int NW, int kSlice>
 __global__ void __launch_bounds__(NW * 32)
     kron_global_rows(const int *__restrict__ slice_row,
                      const int64_t *__restrict__ slice_beg,
@@ -206,14 +206,16 @@ template<int D, typename TC>
 int launch_global_d(plan_data const &p, double alpha, const double *x,
                     double beta, double *y, double ex, cudaStream_t s)
 {
-  constexpr int TS = ipow3g(D);
-  constexpr int NW = TS <= 27 ? 4 : 8;
+  constexpr int TS    = ipow3g(D);
+  constexpr int NW    = TS <= 81 ? 4 : 8;
+  constexpr int SLICE = global_slice(D);
+  static_assert(SLICE <= kGlobalSliceMax, "slice");
   const TC *B;
   if constexpr (sizeof(TC) == 8)
     B = p.gB64;
   else
     B = p.gB32;
-  kron_global_rows<D, TC, NW><<<p.gslices, NW * 32, 0, s>>>(
+  kron_global_rows<D, TC, NW, SLICE><<<p.gslices, NW * 32, 0, s>>>(
       p.slice_row, p.slice_beg, p.slice_len, p.row_slice0, p.row_nslice, p.gcol, p.gkb, B,
       p.gscratch, p.gtickets, alpha, x, beta, y, ex);
   ASGK_LAUNCHED();

@@ -70,18 +70,58 @@ def parse():
 
 
 class ClockSampler:
-    """nvidia-smi samples of SM clock and throttle reasons (every 200 ms)."""
+    """SM clock and throttle reasons during the timed region: NVML read every
+    10 ms from a thread (the timed region of a short run lasts well under a
+    second); `nvidia-smi -lms 200` when NVML is unavailable.  Read-only."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    # NVML clock-event reason bits
+    BITS = {"sw_power_cap": 0x4, "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20,
+            "hw_thermal_slowdown": 0x40}
 
     def __init__(self, index: int):
         self.index = index
         self.proc = None
         self.lines = []
+        self.nvml = None
+        self.samples = []
+
+    def _nvml_handle(self):
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        props = torch.cuda.get_device_properties(self.index)
+        uuid = getattr(props, "uuid", None)
+        if uuid is not None:
+            try:
+                return pynvml, pynvml.nvmlDeviceGetHandleByUUID("GPU-" + str(uuid))
+            except Exception:
+                pass
+        return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.index)
 
     def start(self):
+        try:
+            self.nvml, self.h = self._nvml_handle()
+            get_reasons = getattr(self.nvml, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+                self.nvml.nvmlDeviceGetCurrentClocksThrottleReasons
+            self.max_mhz = float(self.nvml.nvmlDeviceGetMaxClockInfo(self.h, self.nvml.NVML_CLOCK_SM))
+            self.stop_evt = threading.Event()
+
+            def poll():
+                while not self.stop_evt.is_set():
+                    try:
+                        sm = self.nvml.nvmlDeviceGetClockInfo(self.h, self.nvml.NVML_CLOCK_SM)
+                        self.samples.append((float(sm), int(get_reasons(self.h))))
+                    except Exception:
+                        pass
+                    time.sleep(0.01)
+            self.t = threading.Thread(target=poll, daemon=True)
+            self.t.start()
+            return
+        except Exception:
+            self.nvml = None
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
@@ -97,6 +137,15 @@ class ClockSampler:
             self.lines.append(line.strip())
 
     def stop(self):
+        if self.nvml is not None:
+            self.stop_evt.set()
+            self.t.join(timeout=2)
+            sm = sorted(s for s, _ in self.samples)
+            reasons = sorted({nm for _, r in self.samples
+                              for nm, bit in self.BITS.items() if r & bit})
+            return {"sm_mhz": sm[len(sm) // 2] if sm else None,
+                    "sm_max_mhz": self.max_mhz, "reasons": reasons,
+                    "samples": len(sm), "source": "NVML every 10 ms"}
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.proc.terminate()
@@ -121,7 +170,7 @@ class ClockSampler:
         sm.sort()
         med = sm[len(sm) // 2] if sm else None
         return {"sm_mhz": med, "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "source": "nvidia-smi every 200 ms"}
 
 
 def peaks():
