@@ -91,6 +91,31 @@ public:
     return m;
   }
 
+  //! Global Kronecker form of a sparse-grid operator (the reference's
+  //! global_kron_matrix, src/asgard_kronmult_matrix.cpp:1196-1334, for terms
+  //! that act in one dimension each): the element table (num_cells x 2d
+  //! levels then positions, asgk_sparse_grid's layout) and the factors per
+  //! 1D connection (asgk_plan_create_conn's layout).  Throws
+  //! std::runtime_error (unsupported) when a term acts in several dimensions.
+  static kronmult_matrix global_form(int num_dimensions, int kron_size,
+                                     int level, std::vector<int> const &table,
+                                     int num_terms,
+                                     std::vector<double> const &vA)
+  {
+    kronmult_matrix m;
+    int const cells = int(table.size() / (2 * size_t(num_dimensions)));
+    m.d_     = num_dimensions;
+    m.n_     = kron_size;
+    m.rows_  = cells;
+    m.cols_  = cells;
+    m.terms_ = num_terms;
+    check(asgk_plan_create_global(&m.plan_, num_dimensions, kron_size, level,
+                                  cells, table.data(), num_terms, vA.data(),
+                                  int64_t(vA.size())),
+          "kronmult_matrix");
+    return m;
+  }
+
   kronmult_matrix(kronmult_matrix const &) = delete;
   kronmult_matrix &operator=(kronmult_matrix const &) = delete;
   kronmult_matrix(kronmult_matrix &&o) noexcept { swap(o); }

@@ -8,6 +8,7 @@
 
 #include <cuda_runtime.h>
 
+#include <cmath>
 #include <cstdio>
 #include <fstream>
 #include <random>
@@ -84,6 +85,48 @@ int main(int argc, char **argv)
   std::vector<double> sol(N);
   cudaMemcpy(sol.data(), dx, sizeof(double) * N, cudaMemcpyDeviceToHost);
 
+  // the same operator in the global Kronecker form (every term here acts in
+  // all dimensions, so the form is refused), then a single-direction operator
+  int global_refused = 0;
+  try
+  {
+    std::vector<int> tb(table.begin(), table.end());
+    auto g = kronmult_matrix<double>::global_form(d, n, L, tb, T, vA);
+  }
+  catch (std::runtime_error const &)
+  {
+    global_refused = 1;
+  }
+  // advection-like factors in dimension t only (identity elsewhere)
+  std::vector<double> vS(vA.size(), 0.0);
+  std::vector<int> c1p(nrows1d + 1), c1i(nconn);
+  asgk_connect_1d(L, &nrows1d, &nconn, c1p.data(), c1i.data());
+  for (int r = 0; r < nrows1d; r++)
+    for (int j = c1p[r]; j < c1p[r + 1]; j++)
+      for (int t = 0; t < T; t++)
+        for (int k = 0; k < d; k++)
+          for (int e = 0; e < 9; e++)
+          {
+            double &v = vS[((int64_t(j) * T + t) * d + k) * 9 + e];
+            if (k == t % d)
+              v = 0.2 * U(rng);
+            else
+              v = (c1i[j] == r && e % 4 == 0) ? 1.0 : 0.0;
+          }
+  std::vector<int> tb(table.begin(), table.end());
+  auto gS = kronmult_matrix<double>::global_form(d, n, L, tb, T, vS);
+  kronmult_matrix<double> pS(d, n, int(cells), int(cells), T, pntr, col, iA, vS);
+  std::vector<double> yg(N), yp(N);
+  gS.apply<resource::host>(1.0, x.data(), 0.0, yg.data());
+  pS.apply<resource::host>(1.0, x.data(), 0.0, yp.data());
+  double num = 0, den = 0;
+  for (int i = 0; i < N; i++)
+  {
+    num += (yg[i] - yp[i]) * (yg[i] - yp[i]);
+    den += yp[i] * yp[i];
+  }
+  double const global_rel = std::sqrt(num / den);
+
   // restart larger than the system must throw std::invalid_argument
   int threw = 0;
   try
@@ -119,7 +162,8 @@ int main(int argc, char **argv)
                               info.error, double(info.iterations), double(threw),
                               info3.error, double(mat.num_batch()),
                               double(mat.flops()),
-                              double(kronmult_matrix<double>::compute_flops(d, n, T, mat.num_batch()))};
+                              double(kronmult_matrix<double>::compute_flops(d, n, T, mat.num_batch())),
+                              double(global_refused), global_rel};
   put(o, meta);
   cudaFree(dx);
   cudaFree(dy);
