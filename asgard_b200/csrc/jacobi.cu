@@ -12,6 +12,8 @@
 //   cell-local map that contains the point preconditioner as its diagonal.
 #include "internal.cuh"
 
+#include <cuda_fp16.h>
+
 #include <algorithm>
 #include <cmath>
 #include <memory>
@@ -175,6 +177,10 @@ __global__ void k_block_jacobi(int rows, int d, int n, int ts, int T,
   }
 }
 
+__device__ __forceinline__ double to_d(double v) { return v; }
+__device__ __forceinline__ double to_d(float v) { return v; }
+__device__ __forceinline__ double to_d(__half v) { return __half2float(v); }
+
 // z_c = M_c v_c, one CTA per cell; M column-major so the threads of a CTA
 // read consecutive entries
 template<typename TM>
@@ -192,9 +198,17 @@ __global__ void k_block_apply(int rows, int ts, const TM *__restrict__ M,
   {
     double s = 0.0;
     for (int j = 0; j < ts; j++)
-      s = fma(static_cast<double>(Mc[int64_t(j) * ts + i]), vs[j], s);
+      s = fma(to_d(Mc[int64_t(j) * ts + i]), vs[j], s);
     z[int64_t(row) * ts + i] = s;
   }
+}
+
+__global__ void k_to_f16(const float *__restrict__ a, __half *__restrict__ b,
+                         int64_t n)
+{
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n;
+       i += int64_t(gridDim.x) * blockDim.x)
+    b[i] = __float2half_rn(a[i]);
 }
 
 __global__ void k_point_apply(int64_t n, const double *__restrict__ inv_diag,
@@ -217,12 +231,14 @@ struct jacobi_data
   double *inv_diag = nullptr; // point: rows*ts
   double *M64      = nullptr; // block: rows*ts*ts, column-major per cell
   float *M32       = nullptr;
+  __half *M16      = nullptr; // applied inside the FP32 solves
   int64_t device_bytes = 0;
   ~jacobi_data()
   {
     cudaFree(inv_diag);
     cudaFree(M64);
     cudaFree(M32);
+    cudaFree(M16);
   }
 };
 
@@ -260,7 +276,8 @@ int jacobi_build(plan_data const &p, double dt, int kind, jacobi_data &jd)
     size_t const b = size_t(p.rows) * ts * ts;
     ASGK_CUDA(cudaMalloc(&jd.M64, sizeof(double) * b));
     ASGK_CUDA(cudaMalloc(&jd.M32, sizeof(float) * b));
-    jd.device_bytes = int64_t(b * (sizeof(double) + sizeof(float)));
+    ASGK_CUDA(cudaMalloc(&jd.M16, sizeof(__half) * b));
+    jd.device_bytes = int64_t(b * (sizeof(double) + sizeof(float) + sizeof(__half)));
     size_t const shm = sizeof(double) * size_t(ts) * 2 * ts;
     ASGK_CUDA(cudaFuncSetAttribute(k_block_jacobi,
                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -268,6 +285,9 @@ int jacobi_build(plan_data const &p, double dt, int kind, jacobi_data &jd)
     k_block_jacobi<<<p.rows, 256, shm>>>(p.rows, p.d, p.n, ts, p.terms, p.mode,
                                          p.row_ptr, p.col, p.idx, vA, dt,
                                          jd.M64, jd.M32, err);
+    ASGK_LAUNCHED();
+    int const blocks = int(std::min<int64_t>((int64_t(b) + 255) / 256, 4096));
+    k_to_f16<<<blocks, 256>>>(jd.M32, jd.M16, int64_t(b));
     ASGK_LAUNCHED();
   }
   int herr = 0;
@@ -289,7 +309,7 @@ int jacobi_apply(jacobi_data const &jd, bool low, const double *v, double *z,
   int const threads = jd.ts <= 32 ? 32 : (jd.ts <= 64 ? 64 : 128);
   size_t const shm  = sizeof(double) * jd.ts;
   if (low)
-    k_block_apply<float><<<jd.rows, threads, shm, s>>>(jd.rows, jd.ts, jd.M32, v, z);
+    k_block_apply<__half><<<jd.rows, threads, shm, s>>>(jd.rows, jd.ts, jd.M16, v, z);
   else
     k_block_apply<double><<<jd.rows, threads, shm, s>>>(jd.rows, jd.ts, jd.M64, v, z);
   ASGK_LAUNCHED();

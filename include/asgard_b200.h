@@ -240,7 +240,8 @@ int asgk_jacobi_info(asgk_jacobi *pc, int *kind, double *dt,
                      int64_t *device_bytes);
 /* asgk_gmres_euler with a Jacobi preconditioner applied on the right
  * (flexible GMRES; the reference applies its diagonal one to the residual).
- * With ASGK_FP32 the block inverses are applied from an FP32 copy. */
+ * With ASGK_FP32 the block inverses are applied from an FP16 copy (FP64
+ * accumulation): an inexact preconditioner, which flexible GMRES allows. */
 int asgk_gmres_euler_jacobi(asgk_plan *plan, double dt, double *x,
                             const double *b, int restart, int max_outer,
                             double tol, int tol_mode, int precision,
