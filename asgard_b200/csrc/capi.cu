@@ -170,6 +170,25 @@ int upload_values(plan_data &p, const double *vA)
   return ASGK_OK;
 }
 
+// Dense-mode factors to the per-connection layout of a conn-mode plan: the
+// caller's terms[t] hold, per dimension k, num_1d_blocks^2 column-major n x n
+// blocks ordered by (column cell, row cell) (make_kronmult_dense,
+// src/asgard_kronmult_matrix.cpp:95-113); connection c = ic*nb + ir keeps
+// the d*T blocks of that 1D pair together.
+std::vector<double> dense_values(int d, int n, int terms, int nb,
+                                 const double *const *tv)
+{
+  int64_t const nn = int64_t(n) * n;
+  int64_t const nc = int64_t(nb) * nb;
+  std::vector<double> vA(size_t(nc * d * terms * nn));
+  for (int t = 0; t < terms; t++)
+    for (int k = 0; k < d; k++)
+      for (int64_t c = 0; c < nc; c++)
+        std::copy_n(tv[t] + (k * nc + c) * nn, nn,
+                    vA.data() + (c * d * terms + t * d + k) * nn);
+  return vA;
+}
+
 int check_dims(int d, int n, int rows, int cols, int terms)
 {
   if (d < 1 || d > 6 || n < 1 || rows < 0 || cols < 0 || terms < 0)
@@ -768,6 +787,96 @@ int asgk_plan_create_pairs(asgk_plan **plan, int d, int n, int num_rows,
                     ia.data(), index_mode::expanded, vA, vA_len);
 }
 
+int asgk_plan_create_dense(asgk_plan **plan, int d, int n, int num_rows,
+                           int num_cols, int num_terms,
+                           const double *const *terms, const int *elem,
+                           int64_t elem_len, int row_offset, int col_offset,
+                           int num_1d_blocks)
+{
+  if (plan == nullptr)
+    return ASGK_ERR_INVALID;
+  *plan = nullptr;
+  if (int rc = check_dims(d, n, num_rows, num_cols, num_terms))
+    return rc;
+  if (row_offset < 0 || col_offset < 0)
+    return ASGK_ERR_INVALID;
+  int64_t const npairs = (num_terms > 0) ? int64_t(num_rows) * num_cols : 0;
+  int const nb         = (num_terms > 0) ? num_1d_blocks : 0;
+  if (num_terms > 0)
+  {
+    if (terms == nullptr || num_1d_blocks < 1 ||
+        int64_t(num_1d_blocks) * num_1d_blocks > (int64_t(1) << 30))
+      return ASGK_ERR_INVALID;
+    for (int t = 0; t < num_terms; t++)
+      if (terms[t] == nullptr)
+        return ASGK_ERR_INVALID;
+  }
+  if (npairs > 0)
+  {
+    int64_t const need =
+        int64_t(d) * std::max(int64_t(row_offset) + num_rows,
+                              int64_t(col_offset) + num_cols);
+    if (elem == nullptr || elem_len < need)
+      return ASGK_ERR_INVALID;
+    for (int64_t i = 0; i < need; i++)
+      if (elem[i] < 0 || elem[i] >= nb)
+        return ASGK_ERR_INVALID;
+  }
+  // every (row, col) pair, columns in order; per pair the d connections
+  // elem_col[k]*nb + elem_row[k]
+  std::vector<int64_t> rp(size_t(num_rows) + 1);
+  for (int r = 0; r <= num_rows; r++)
+    rp[r] = (npairs > 0) ? int64_t(r) * num_cols : 0;
+  std::vector<int> col(static_cast<size_t>(npairs));
+  std::vector<int> conn(static_cast<size_t>(npairs) * d);
+#pragma omp parallel for schedule(static)
+  for (int r = 0; r < (npairs > 0 ? num_rows : 0); r++)
+  {
+    const int *er = elem + int64_t(r + row_offset) * d;
+    for (int c = 0; c < num_cols; c++)
+    {
+      int64_t const p = int64_t(r) * num_cols + c;
+      const int *ec   = elem + int64_t(c + col_offset) * d;
+      col[p]          = c;
+      for (int k = 0; k < d; k++)
+        conn[p * d + k] = ec[k] * nb + er[k];
+    }
+  }
+  std::vector<double> vA;
+  if (num_terms > 0)
+    vA = dense_values(d, n, num_terms, nb, terms);
+  if (int rc = build_plan(plan, d, n, num_rows, num_cols, num_terms, rp,
+                          col.data(), conn.data(), index_mode::conn,
+                          vA.data(), int64_t(vA.size())))
+    return rc;
+  (*plan)->p.dense    = true;
+  (*plan)->p.dense_nb = nb;
+  return ASGK_OK;
+}
+
+int asgk_plan_kind(const asgk_plan *plan)
+{
+  if (!plan)
+    return -ASGK_ERR_INVALID;
+  return plan->p.global ? 2 : (plan->p.dense ? 1 : 0);
+}
+
+int asgk_plan_update_terms(asgk_plan *plan, const double *const *terms,
+                           int num_terms)
+{
+  if (!plan || !plan->p.dense || num_terms != plan->p.terms ||
+      (num_terms > 0 && terms == nullptr))
+    return ASGK_ERR_INVALID;
+  for (int t = 0; t < num_terms; t++)
+    if (terms[t] == nullptr)
+      return ASGK_ERR_INVALID;
+  auto &p = plan->p;
+  if (num_terms == 0)
+    return ASGK_OK;
+  std::vector<double> vA = dense_values(p.d, p.n, p.terms, p.dense_nb, terms);
+  return upload_values(p, vA.data());
+}
+
 void asgk_plan_destroy(asgk_plan *plan)
 {
   if (!plan)
@@ -779,7 +888,7 @@ void asgk_plan_destroy(asgk_plan *plan)
 
 int asgk_plan_update_values(asgk_plan *plan, const double *vA, int64_t vA_len)
 {
-  if (!plan || vA_len != plan->p.vA_len || (vA_len > 0 && !vA))
+  if (!plan || plan->p.dense || vA_len != plan->p.vA_len || (vA_len > 0 && !vA))
     return ASGK_ERR_INVALID;
   auto &p = plan->p;
   if (p.global)

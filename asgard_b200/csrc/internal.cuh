@@ -101,6 +101,12 @@ struct plan_data
   int *row_slice0 = nullptr, *row_nslice = nullptr; // [rows]
   double *gscratch = nullptr;  // [gslices * n^d] partial tensors
   unsigned *gtickets = nullptr; // [rows], zero between launches
+
+  // dense mode (every (row, col) pair): a conn-mode plan whose connection
+  // index in dimension k is elem_col[k] * dense_nb + elem_row[k], the factors
+  // of the caller's per-term arrays repacked to the per-connection layout
+  bool dense   = false;
+  int dense_nb = 0;
   int64_t device_bytes = 0;
 };
 

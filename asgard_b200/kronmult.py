@@ -134,6 +134,27 @@ class kronmult_matrix:
               "plan_create_global")
         return cls(h, d, n, cells, cells, num_terms)
 
+    @classmethod
+    def from_dense(cls, d, n, num_rows, num_cols, num_terms, terms, elem,
+                   row_offset=0, col_offset=0, num_1d_blocks=1):
+        """Dense form (the reference's dense constructor): every output cell
+        with every input cell; terms is a list of num_terms arrays of
+        d*num_1d_blocks^2*n^2 values (per dimension the column-major n x n
+        blocks ordered by column cell, then row cell), elem the 1D cell
+        indices of every cell (cells x d), rows starting at row_offset and
+        columns at col_offset."""
+        tv = [_host(t, np.float64) for t in terms]
+        if len(tv) != num_terms:
+            raise ValueError("terms must hold num_terms arrays")
+        el = _host(elem, np.int32).ravel()
+        ptrs = (C.c_void_p * max(num_terms, 1))(*[t.ctypes.data for t in tv])
+        h = C.c_void_p()
+        check(lib.asgk_plan_create_dense(C.byref(h), d, n, num_rows, num_cols,
+                                         num_terms, ptrs, el.ctypes.data,
+                                         len(el), row_offset, col_offset,
+                                         num_1d_blocks), "plan_create_dense")
+        return cls(h, d, n, num_rows, num_cols, num_terms)
+
     def __del__(self):
         h = getattr(self, "_h", None)
         if h:
@@ -151,6 +172,14 @@ class kronmult_matrix:
         return [v.value for v in vals]
 
     def num_batch(self):
+        """num_rows * num_cols, as the reference's num_batch()
+        (src/asgard_kronmult_matrix.hpp:481) returns for every matrix."""
+        return self.num_rows * self.num_cols
+
+    def num_pairs(self):
+        """The (row, col) products one apply computes: the stored pairs
+        (rows*cols for a dense plan, the single-direction entries for the
+        global form)."""
         return self._info()[0]
 
     def tensor_size(self):
@@ -163,7 +192,9 @@ class kronmult_matrix:
         return self._info()[2]
 
     def flops(self):
-        """compute_flops: 2 * n^d * n * d * T * pairs."""
+        """Flops of one apply, multiply and add counted apart:
+        compute_flops(d, n, T, num_pairs()) = 2 * n^d * n * d * T * pairs
+        (2 * n^(d+1) per entry for the global form)."""
         return self._info()[3]
 
     def device_bytes(self):
@@ -177,8 +208,12 @@ class kronmult_matrix:
     def compute_flops(num_dimensions, kron_size, num_terms, num_batch):
         return kron_size ** num_dimensions * kron_size * num_dimensions * num_terms * num_batch * 2
 
+    def kind(self):
+        """"sparse", "dense" or "global"."""
+        return ("sparse", "dense", "global")[lib.asgk_plan_kind(self._h)]
+
     def is_dense(self):
-        return False
+        return lib.asgk_plan_kind(self._h) == 1
 
     def is_onecall(self):
         return True
@@ -187,6 +222,14 @@ class kronmult_matrix:
         return self.num_dimensions > 0
 
     def update_stored_coefficients(self, vA):
+        """New factor values in the layout the plan was made from: one vA
+        array, or for a dense plan the list of per-term arrays."""
+        if self.is_dense():
+            tv = [_host(t, np.float64) for t in vA]
+            ptrs = (C.c_void_p * max(len(tv), 1))(*[t.ctypes.data for t in tv])
+            check(lib.asgk_plan_update_terms(self._h, ptrs, len(tv)),
+                  "update_stored_coefficients")
+            return
         vA = _host(vA, np.float64)
         check(lib.asgk_plan_update_values(self._h, vA.ctypes.data, len(vA)),
               "update_stored_coefficients")

@@ -162,14 +162,45 @@ class SparseGridOperator:
     def iA(self) -> np.ndarray:
         return expand_iA(self.conn, self.d, self.n, self.terms)
 
+    def elem(self) -> np.ndarray:
+        """1D cell index of every cell in every dimension (cells x d): 0 at
+        level 0, else 2^(level-1) + position (the dense form's elem,
+        src/asgard_kronmult_matrix.cpp:116-131)."""
+        lev = self.table[:, :self.d].astype(np.int64)
+        pos = self.table[:, self.d:].astype(np.int64)
+        idx = np.where(lev == 0, 0, (1 << np.maximum(lev - 1, 0)) + pos)
+        return np.ascontiguousarray(idx, dtype=np.int32)
+
+    def dense_terms(self):
+        """The factors as the dense form holds them: per term, per dimension
+        the full 1D operator cut into 2^level x 2^level blocks of n x n,
+        ordered by column cell then row cell, zero where two 1D cells are not
+        connected (make_kronmult_dense, src/asgard_kronmult_matrix.cpp:95-113)."""
+        pntr, indx = connect_1d(self.level)
+        nb, d, T, nn = len(pntr) - 1, self.d, self.terms, self.n * self.n
+        rows = np.repeat(np.arange(nb), np.diff(pntr))
+        blocks = self.vA.reshape(len(indx), T, d, nn)
+        out = []
+        for t in range(T):
+            a = np.zeros((d, nb * nb, nn))
+            a[:, indx * nb + rows, :] = blocks[:, t].transpose(1, 0, 2)
+            out.append(a.reshape(-1))
+        return out, nb
+
     def kronmult_matrix(self, expanded: bool = False, mode: str = "pairs"):
         """mode "pairs": the connected-pair kronmult (expanded: the
         reference's iA offsets instead of connection indices); "global": the
-        global Kronecker form (terms acting in one dimension each)."""
+        global Kronecker form (terms acting in one dimension each); "dense":
+        the reference's dense form (every cell pair, full 1D operators)."""
         from .kronmult import kronmult_matrix
         if mode == "global":
             return kronmult_matrix.from_global(self.d, self.n, self.level,
                                                self.table, self.terms, self.vA)
+        if mode == "dense":
+            terms, nb = self.dense_terms()
+            return kronmult_matrix.from_dense(self.d, self.n, self.rows,
+                                              self.rows, self.terms, terms,
+                                              self.elem(), 0, 0, nb)
         if mode != "pairs":
             raise ValueError(mode)
         if expanded:

@@ -1,14 +1,14 @@
 """Times the kronmult apply kernel on a synthetic sparse-grid operator.
 
     python -m asgard_b200.profile_apply --d 4 --level 7 --terms 4 \
-        --precision fp64 --reps 3 [--warmup 1] [--mode global]
+        --precision fp64 --reps 3 [--warmup 1] [--mode global|dense]
 
 Builds the operator (advection/diffusion factors unless --kind random), runs
 --warmup untimed applies of the fused backward-Euler operator
 y = x - dt*K*x, then --reps timed applies (CUDA events on the launching
 stream) and prints one JSON line: ms per launch, algorithmic TFLOP/s
-(2*d*T*n^(d+1) flops per pair; 2*n^(d+1) per single-direction pair in the
-global form) and the fraction of the measured FMA peak.
+(2*d*T*n^(d+1) flops per pair -- every cell pair in the dense form;
+2*n^(d+1) per single-direction pair in the global form) and the fraction of the measured FMA peak.
 This is the command the ncu summaries under profiles/ were taken with.
 """
 from __future__ import annotations
@@ -29,8 +29,9 @@ def main():
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=1)
     ap.add_argument("--peak", action="store_true", help="also measure the FMA peak")
-    ap.add_argument("--mode", default="pairs", choices=["pairs", "global"],
-                    help="connected-pair kronmult or the global Kronecker form")
+    ap.add_argument("--mode", default="pairs", choices=["pairs", "global", "dense"],
+                    help="connected-pair kronmult, the global Kronecker form, "
+                         "or the dense form (every cell pair)")
     args = ap.parse_args()
 
     import torch
@@ -56,7 +57,7 @@ def main():
     ms = e0.elapsed_time(e1) / args.reps
     flops = mat.flops()
     out = {"d": args.d, "level": args.level, "terms": args.terms, "mode": args.mode,
-           "num_batch": mat.num_batch(),
+           "num_pairs": mat.num_pairs(),
            "precision": args.precision, "cells": op.rows, "pairs": op.nnz,
            "dofs": op.N, "ms_per_launch": ms, "tflops": flops / ms / 1e9,
            "flops_per_launch": flops, "setup_s": t_setup,

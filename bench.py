@@ -482,7 +482,7 @@ def main():
         # the method's operator kernel: algorithmic bytes per launch are x
         # read once, y written, the neighbour lists and the pre-summed blocks
         tg = time_apply(gmat, method["precision"])
-        nbytes = (16 * N + 8 * gmat.num_batch() + 8 * (op.rows + 1)
+        nbytes = (16 * N + 8 * gmat.num_pairs() + 8 * (op.rows + 1)
                   + 48 * len(op.vA) // (9 * T))
         hbm = _measured_hbm_gbs()
         roofline = {"bound": "hbm",

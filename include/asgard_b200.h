@@ -91,6 +91,34 @@ int asgk_plan_create_conn(asgk_plan **plan, int d, int n, int num_rows,
                           const int *col_indx, const int *conn,
                           const double *vA, int64_t vA_len);
 
+/* Dense form: replaces kronmult_matrix<P>'s dense constructor
+ * (src/asgard_kronmult_matrix.hpp:132-176, filled by make_kronmult_dense,
+ * src/asgard_kronmult_matrix.cpp:64-163) and kronmult::gpu_dense /
+ * cpu_dense (src/device/asgard_kronmult.hpp:81-125,
+ * src/device/asgard_kronmult_cpu.cpp:160-530): every output cell r <
+ * num_rows with every input cell c < num_cols,
+ *   y_r = beta y_r + alpha sum_c sum_t (A_{t,0} (x) ... (x) A_{t,d-1}) x_c,
+ * A_{t,k} the n x n column-major block of terms[t] at
+ *   terms[t] + ((k*num_1d_blocks + ic)*num_1d_blocks + ir)*n*n,
+ * ir = elem[(r + row_offset)*d + k], ic = elem[(c + col_offset)*d + k]
+ * (1D cell indices < num_1d_blocks).
+ * terms[num_terms]: host arrays of d*num_1d_blocks^2*n^2 values each;
+ * elem[elem_len]: host array, elem_len >= d*(max(row_offset + num_rows,
+ * col_offset + num_cols)).  num_terms == 0 makes the reference's empty
+ * matrix (apply only scales y).  The plan holds every (row, col) pair (the
+ * reference's num_batch() = rows*cols products per apply).  Indices out of
+ * range: ASGK_ERR_INVALID. */
+int asgk_plan_create_dense(asgk_plan **plan, int d, int n, int num_rows,
+                           int num_cols, int num_terms,
+                           const double *const *terms, const int *elem,
+                           int64_t elem_len, int row_offset, int col_offset,
+                           int num_1d_blocks);
+
+/* What kind of plan this is: 0 sparse (pair list), 1 dense, 2 global
+ * Kronecker form; negative on a null plan.  kronmult_matrix::is_dense()
+ * (src/asgard_kronmult_matrix.hpp:514-517) is kind == 1. */
+int asgk_plan_kind(const asgk_plan *plan);
+
 /* Global Kronecker form (the reference's global_kron_matrix,
  * src/asgard_kronmult_matrix.cpp:1196-1334, for its single-direction terms):
  * the same operator as the connected-pair plan of this sparse grid (the
@@ -108,11 +136,20 @@ int asgk_plan_create_global(asgk_plan **plan, int d, int n, int level,
                             const double *vA, int64_t vA_len);
 void asgk_plan_destroy(asgk_plan *plan);
 
-/* Replaces update_stored_coefficients (src/asgard_kronmult_matrix.hpp:515-532). */
+/* Replaces update_stored_coefficients (src/asgard_kronmult_matrix.hpp:519-536):
+ * vA in the layout the plan was created with (same length).  For a dense
+ * plan use asgk_plan_update_terms. */
 int asgk_plan_update_values(asgk_plan *plan, const double *vA, int64_t vA_len);
 
+/* Dense plans: replaces the per-term overload of update_stored_coefficients
+ * (src/asgard_kronmult_matrix.hpp:538-561); terms[num_terms] as for
+ * asgk_plan_create_dense.  ASGK_ERR_INVALID on other plans. */
+int asgk_plan_update_terms(asgk_plan *plan, const double *const *terms,
+                           int num_terms);
+
 /* Sizes: tensor_size = n^d, input_size = num_cols*n^d,
- * output_size = num_rows*n^d, num_batch = nnz, flops = 2*d*T*n^(d+1)*nnz
+ * output_size = num_rows*n^d, num_batch = the (row, col) products one apply
+ * computes (nnz; rows*cols for a dense plan), flops = 2*d*T*n^(d+1)*num_batch
  * (compute_flops, src/asgard_kronmult_matrix.hpp:507-512). */
 int asgk_plan_info(const asgk_plan *plan, int64_t *num_batch,
                    int64_t *input_size, int64_t *output_size,

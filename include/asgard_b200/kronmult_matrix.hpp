@@ -91,6 +91,30 @@ public:
     return m;
   }
 
+  //! Dense form (src/asgard_kronmult_matrix.hpp:132-176): every output cell
+  //! with every input cell; terms[t] holds d * num_1d_blocks^2 column-major
+  //! n x n blocks (per dimension ordered by column cell, then row cell, as
+  //! make_kronmult_dense writes them), elem the d 1D cell indices of every
+  //! cell; rows start at elem entry row_offset, columns at col_offset.
+  kronmult_matrix(int num_dimensions, int kron_size, int num_rows,
+                  int num_cols, int num_terms,
+                  std::vector<std::vector<double>> const &terms,
+                  std::vector<int> const &elem, int row_offset, int col_offset,
+                  int num_1d_blocks)
+      : d_(num_dimensions), n_(kron_size), rows_(num_rows), cols_(num_cols),
+        terms_(num_terms)
+  {
+    if (terms.size() != size_t(num_terms))
+      throw std::runtime_error("kronmult_matrix: terms must hold num_terms arrays");
+    std::vector<double const *> tp;
+    for (auto const &t : terms)
+      tp.push_back(t.data());
+    check(asgk_plan_create_dense(&plan_, d_, n_, rows_, cols_, terms_,
+                                 tp.data(), elem.data(), int64_t(elem.size()),
+                                 row_offset, col_offset, num_1d_blocks),
+          "kronmult_matrix");
+  }
+
   //! Global Kronecker form of a sparse-grid operator (the reference's
   //! global_kron_matrix, src/asgard_kronmult_matrix.cpp:1196-1334, for terms
   //! that act in one dimension each): the element table (num_cells x 2d
@@ -137,14 +161,18 @@ public:
       check(asgk_apply(plan_, ASGK_FP64, alpha, x, beta, y, nullptr), "apply");
   }
 
-  int64_t num_batch() const { return info(0); }
+  //! num_rows * num_cols, as the reference returns for every matrix
+  //! (src/asgard_kronmult_matrix.hpp:481)
+  int64_t num_batch() const { return int64_t(rows_) * int64_t(cols_); }
+  //! the (row, col) products one apply computes (stored pairs)
+  int64_t num_pairs() const { return info(0); }
   int tensor_size() const { return compute_tensor_size(d_, n_); }
   int input_size() const { return int(info(1)); }
   int output_size() const { return int(info(2)); }
   //! as the reference's flops(): n^d * n * |iA| (multiply-add counted once)
   int64_t flops() const { return info(3) / 2; }
   explicit operator bool() const { return d_ > 0; }
-  bool is_dense() const { return false; }
+  bool is_dense() const { return plan_ != nullptr && asgk_plan_kind(plan_) == 1; }
   bool is_onecall() const { return true; }
 
   static int compute_tensor_size(int num_dimensions, int kron_size)
@@ -164,6 +192,15 @@ public:
   void update_stored_coefficients(std::vector<double> const &vA)
   {
     check(asgk_plan_update_values(plan_, vA.data(), int64_t(vA.size())),
+          "update_stored_coefficients");
+  }
+  //! dense matrices: new per-term arrays (src/asgard_kronmult_matrix.hpp:538-561)
+  void update_stored_coefficients(std::vector<std::vector<double>> const &terms)
+  {
+    std::vector<double const *> tp;
+    for (auto const &t : terms)
+      tp.push_back(t.data());
+    check(asgk_plan_update_terms(plan_, tp.data(), int(terms.size())),
           "update_stored_coefficients");
   }
 

@@ -77,6 +77,14 @@ def oracle():
                                         C.POINTER(C.c_int)]
         lib.orc_make_kronmult_data.argtypes = [C.c_int] * 6 + [
             _i32p, _i32p, _i32p, C.c_void_p, C.c_void_p, C.c_void_p]
+        for name, T in (("f64", _f64p), ("f32", _f32p)):
+            S = C.c_double if name == "f64" else C.c_float
+            fn = getattr(lib, f"orc_kronmult_dense_{name}")
+            fn.argtypes = [C.c_int] * 5 + [_i32p, C.c_int, C.c_int, C.c_void_p,
+                                           C.c_int, S, T, S, T]
+            fn.restype = C.c_int
+        lib.orc_make_kronmult_welem.argtypes = [C.c_int] * 5 + [
+            _i32p, C.c_void_p, C.c_void_p, C.c_void_p]
         _oracle = lib
     return _oracle
 
@@ -173,6 +181,10 @@ def ref():
                            _i32p, T, S, T, S, T]
             fn = getattr(lib, f"ref_make_kronmult_data_{name}")
             fn.argtypes = [C.c_int] * 5 + [_i32p, _i32p, _i32p, T, T, T, T]
+            fn = getattr(lib, f"ref_make_welem_{name}")
+            fn.argtypes = [C.c_int] * 5 + [_i32p, T, T, T, T]
+            fn = getattr(lib, f"ref_dense_apply_{name}")
+            fn.argtypes = [C.c_int] * 5 + [T, _i32p] + [C.c_int] * 4 + [S, T, S, T]
         lib.ref_gmres_euler_f64.argtypes = [
             C.c_int, C.c_int, C.c_int, C.c_int, _i32p, _i32p, _i32p, _f64p,
             C.c_int64, C.c_double, _f64p, _f64p, C.c_int, C.c_int, C.c_double,
@@ -313,6 +325,75 @@ def make_kronmult_data(d, n, rows, terms, mats, dtype=np.float64):
                                     indx, iA, vA.ctypes.data, x.ctypes.data,
                                     y.ctypes.data)
     return dict(pntr=pntr, indx=indx, iA=iA, vA=vA, x=x, y=y)
+
+
+def _term_pointers(terms):
+    return (C.c_void_p * max(len(terms), 1))(*[t.ctypes.data for t in terms])
+
+
+def kronmult_dense(d, n, rows, cols, terms, elem, row_offset, col_offset, nb,
+                   alpha, x, beta, y, lib=None):
+    """Dense form y <- beta*y + alpha*K*x in place (kronmult::cpu_dense):
+    terms is a list of per-term coefficient arrays (d*nb^2*n^2 each), elem
+    the cells' 1D indices (d per cell).  lib=ref() runs the reference's own
+    kronmult_matrix (dense constructor) instead of the restatement."""
+    f32 = x.dtype == np.float32
+    dt = np.float32 if f32 else np.float64
+    tv = [np.ascontiguousarray(t, dtype=dt) for t in terms]
+    el = np.ascontiguousarray(elem, dtype=np.int32).ravel()
+    if lib is None:
+        fn = getattr(oracle(), "orc_kronmult_dense_" + ("f32" if f32 else "f64"))
+        rc = fn(d, n, rows, cols, len(tv), el, row_offset, col_offset,
+                _term_pointers(tv), nb, alpha, x, beta, y)
+    else:
+        fn = getattr(lib, "ref_dense_apply_" + ("f32" if f32 else "f64"))
+        rc = fn(d, n, rows, cols, len(tv), np.concatenate(tv) if tv else
+                np.zeros(1, dt), el, len(el), row_offset, col_offset, nb,
+                alpha, x, beta, y)
+    if rc != 0:
+        raise RuntimeError(f"dense kronmult checker returned {rc}")
+    return y
+
+
+def ref_make_kronmult_welem(d, n, terms, index_range, dtype=np.float64,
+                            want_ref=True):
+    """The reference's own make_kronmult_welem (compiled from its sources):
+    the same fields as make_kronmult_welem plus ref_y, its explicit
+    Kronecker-product answer of y + K x (when want_ref)."""
+    rows = index_range ** d
+    ts = n ** d
+    per = d * index_range * index_range * n * n
+    elem = np.zeros(rows * d, np.int32)
+    coeff = np.zeros(max(terms * per, 1), dtype)
+    x = np.zeros(rows * ts, dtype)
+    y = np.zeros(rows * ts, dtype)
+    ref_y = np.zeros(rows * ts, dtype)
+    fn = getattr(ref(), "ref_make_welem_" + ("f64" if dtype == np.float64 else "f32"))
+    fn(d, n, terms, index_range, int(want_ref), elem, coeff, x, y, ref_y)
+    return dict(rows=rows, elem=elem.reshape(rows, d),
+                terms=[coeff[t * per:(t + 1) * per] for t in range(terms)],
+                x=x, y=y, ref_y=ref_y)
+
+
+def make_kronmult_welem(d, n, terms, index_range, dtype=np.float64):
+    """The reference's dense-test data (kronmult_intputs_welem,
+    minstd_rand(42)): elem, the list of per-term coefficient arrays, x, y."""
+    rows = index_range ** d
+    ts = n ** d
+    per = d * index_range * index_range * n * n
+    elem = np.zeros(rows * d, np.int32)
+    coeff = np.zeros(terms * per, dtype)
+    x = np.zeros(rows * ts, dtype)
+    y = np.zeros(rows * ts, dtype)
+    rc = oracle().orc_make_kronmult_welem(d, n, terms, index_range,
+                                          8 if dtype == np.float64 else 4,
+                                          elem, coeff.ctypes.data,
+                                          x.ctypes.data, y.ctypes.data)
+    if rc != 0:
+        raise RuntimeError("make_kronmult_welem failed")
+    return dict(rows=rows, elem=elem.reshape(rows, d),
+                terms=[coeff[t * per:(t + 1) * per] for t in range(terms)],
+                x=x, y=y)
 
 
 class RefPDE:

@@ -99,6 +99,65 @@ DEFINE_CONTRACT(float, contract_f32)
 DEFINE_SPARSE(double, orc_kronmult_sparse_f64, contract_f64)
 DEFINE_SPARSE(float, orc_kronmult_sparse_f32, contract_f32)
 
+/* kronmult::cpu_dense<T> (src/device/asgard_kronmult_cpu.cpp:160-507,
+ * dispatch :517-700): one output cell per iteration, beta applied to its
+ * block first, then every (column cell, term) product in column order.
+ * Factor (t, k) of the pair (r, c) is the column-major n x n block of
+ * vA[t] at k*nb^2*n^2 + (ic*nb + ir)*n^2 with ir = elem[(r + row_offset)*d
+ * + k], ic = elem[(c + col_offset)*d + k] (the reference's dense layout,
+ * src/asgard_kronmult_matrix.cpp:95-113). */
+#define DEFINE_DENSE(T, NAME, CONTRACT)                                       \
+  int NAME(int d, int n, int rows, int cols, int terms, const int *elem,      \
+           int row_offset, int col_offset, const T *const *vA, int nb,        \
+           T alpha, const T *x, T beta, T *y)                                 \
+  {                                                                           \
+    if (d < 1 || d > 6 || n < 1)                                              \
+      return 1;                                                               \
+    int const ts       = ipow_i(n, d);                                        \
+    int64_t const nn   = (int64_t)n * n;                                      \
+    int64_t const vstr = (int64_t)nb * nb * nn;                               \
+    _Pragma("omp parallel")                                                   \
+    {                                                                         \
+      T *w0 = (T *)malloc(sizeof(T) * ts);                                    \
+      T *w1 = (T *)malloc(sizeof(T) * ts);                                    \
+      _Pragma("omp for schedule(dynamic, 4)")                                 \
+      for (int r = 0; r < rows; r++)                                          \
+      {                                                                       \
+        T *yr = y + (int64_t)r * ts;                                          \
+        const int *iy = elem + (int64_t)(r + row_offset) * d;                 \
+        for (int j = 0; j < ts; j++)                                          \
+          yr[j] = (beta == 0) ? (T)0 : ((beta == 1) ? yr[j] : beta * yr[j]);  \
+        for (int c = 0; c < cols; c++)                                        \
+        {                                                                     \
+          const int *ix = elem + (int64_t)(c + col_offset) * d;               \
+          const T *xc   = x + (int64_t)c * ts;                                \
+          for (int t = 0; t < terms; t++)                                     \
+          {                                                                   \
+            const T *src = xc;                                                \
+            T *cur = w0, *nxt = w1;                                           \
+            for (int k = 0; k < d; k++)                                       \
+            {                                                                 \
+              const T *A = vA[t] + k * vstr +                                 \
+                           ((int64_t)ix[k] * nb + iy[k]) * nn;                \
+              CONTRACT(d, n, k, A, src, cur);                                 \
+              src = cur;                                                      \
+              T *tmp = cur;                                                   \
+              cur = nxt;                                                      \
+              nxt = tmp;                                                      \
+            }                                                                 \
+            for (int j = 0; j < ts; j++)                                      \
+              yr[j] += alpha * src[j];                                        \
+          }                                                                   \
+        }                                                                     \
+      }                                                                       \
+      free(w0);                                                               \
+      free(w1);                                                               \
+    }                                                                         \
+    return 0;                                                                 \
+  }
+DEFINE_DENSE(double, orc_kronmult_dense_f64, contract_f64)
+DEFINE_DENSE(float, orc_kronmult_dense_f32, contract_f32)
+
 /* kronecker() and reference_kronmult_one() of the reference tests
  * (src/asgard_kronmult_tests.hpp:39-76): explicit product with pA[0] the
  * outermost factor, then a dense GEMV y += K x. */
@@ -712,6 +771,54 @@ int orc_make_kronmult_data(int d, int n, int rows, int terms, int mats,
       xx[i] = orc_uniform_f32(&g, -1.0f, 1.0f);
       yy[i] = orc_uniform_f32(&g, -1.0f, 1.0f);
     }
+  }
+  return 0;
+}
+
+/* kronmult_intputs_welem<P>(d, n, terms, range) of the reference's dense
+ * tests (src/asgard_kronmult_tests.hpp:236-300): range^d cells whose 1D
+ * indices are the base-d digits of the cell number (the digit base there is
+ * the number of dimensions, not range), then from minstd_rand(42) every
+ * coefficient of every term (d*range^2*n^2 each, term after term), all of x,
+ * all of y.  precision 8 = double, 4 = float. */
+int orc_make_kronmult_welem(int d, int n, int terms, int range, int precision,
+                            int *elem, void *coeff, void *x, void *y)
+{
+  if (d < 1 || n < 1 || terms < 0 || range < 1)
+    return 1;
+  int const rows = ipow_i(range, d);
+  for (int i = 0; i < rows; i++)
+  {
+    int t = i;
+    for (int k = 0; k < d; k++)
+    {
+      elem[i * d + k] = t % d;
+      t /= d;
+    }
+  }
+  orc_minstd g;
+  orc_minstd_seed(&g, 42);
+  int64_t const nc = (int64_t)terms * d * range * range * n * n;
+  int64_t const nx = (int64_t)ipow_i(n, d) * rows;
+  if (precision == 8)
+  {
+    double *c = (double *)coeff, *xx = (double *)x, *yy = (double *)y;
+    for (int64_t i = 0; i < nc; i++)
+      c[i] = orc_uniform_f64(&g, -1.0, 1.0);
+    for (int64_t i = 0; i < nx; i++)
+      xx[i] = orc_uniform_f64(&g, -1.0, 1.0);
+    for (int64_t i = 0; i < nx; i++)
+      yy[i] = orc_uniform_f64(&g, -1.0, 1.0);
+  }
+  else
+  {
+    float *c = (float *)coeff, *xx = (float *)x, *yy = (float *)y;
+    for (int64_t i = 0; i < nc; i++)
+      c[i] = orc_uniform_f32(&g, -1.0f, 1.0f);
+    for (int64_t i = 0; i < nx; i++)
+      xx[i] = orc_uniform_f32(&g, -1.0f, 1.0f);
+    for (int64_t i = 0; i < nx; i++)
+      yy[i] = orc_uniform_f32(&g, -1.0f, 1.0f);
   }
   return 0;
 }

@@ -24,6 +24,19 @@ int orc_kronmult_sparse_f32(int d, int n, int rows, const int *pntr,
                             const float *vA, float alpha, const float *x,
                             float beta, float *y);
 
+/* Dense form of kronmult::cpu_dense: every output cell r < rows with every
+ * input cell c < cols; factor (t, k) of the pair is the n x n block of vA[t]
+ * at k*nb^2*n^2 + (ic*nb + ir)*n^2, ir / ic the 1D indices of cells
+ * r + row_offset / c + col_offset in elem (d ints per cell). */
+int orc_kronmult_dense_f64(int d, int n, int rows, int cols, int terms,
+                           const int *elem, int row_offset, int col_offset,
+                           const double *const *vA, int nb, double alpha,
+                           const double *x, double beta, double *y);
+int orc_kronmult_dense_f32(int d, int n, int rows, int cols, int terms,
+                           const int *elem, int row_offset, int col_offset,
+                           const float *const *vA, int nb, float alpha,
+                           const float *x, float beta, float *y);
+
 /* Explicit Kronecker product of the d factors (pA[0] outermost) applied by a
  * dense GEMV: y += K x. */
 void orc_reference_kronmult_one(int d, int n, const double *const *pA,
@@ -80,6 +93,11 @@ float orc_uniform_f32(orc_minstd *g, float a, float b);
 int orc_make_kronmult_data(int d, int n, int rows, int terms, int mats,
                            int precision, int *pntr, int *indx, int *iA,
                            void *vA, void *x, void *y);
+
+/* make_kronmult_welem(d, n, terms, range) of the dense tests: elem[range^d
+ * * d], coeff[terms * d*range^2*n^2] (term-major), x and y [range^d * n^d]. */
+int orc_make_kronmult_welem(int d, int n, int terms, int range, int precision,
+                            int *elem, void *coeff, void *x, void *y);
 
 #ifdef __cplusplus
 }

@@ -7,6 +7,7 @@
 // Everything here forwards to the reference code unchanged:
 //   * kronmult::cpu_sparse               src/device/asgard_spkronmult_cpu.cpp:606-768
 //   * kronmult_matrix<P> (CPU, sparse)   src/asgard_kronmult_matrix.hpp:235-297, 340-478
+//   * kronmult_matrix<P> (CPU, dense)    src/asgard_kronmult_matrix.hpp:132-176 (cpu_dense)
 //   * solver::simple_gmres_euler         src/solver.cpp:119-135
 //   * solver::simple_gmres (dense)       src/solver.cpp:55-74
 //   * connect_1d                         src/asgard_grid_1d.hpp:19-330
@@ -126,6 +127,53 @@ int make_data(int d, int n, int rows, int terms, int mats, int *pntr,
   std::copy(data->input_x.begin(), data->input_x.end(), x);
   std::copy(data->output_y.begin(), data->output_y.end(), y);
   std::copy(data->reference_y.begin(), data->reference_y.end(), ref_y);
+  return 0;
+}
+
+// make_kronmult_welem<T>(d, n, terms, range) of the reference's dense tests
+// (src/asgard_kronmult_tests.hpp:236-353): elem, the term coefficients
+// (concatenated), x, y, and -- with want_ref -- its explicit
+// Kronecker-product answer of y <- y + K x.
+template<typename T>
+int make_welem(int d, int n, int terms, int range, int want_ref, int *elem,
+               T *coeff, T *x, T *y, T *ref_y)
+{
+  std::unique_ptr<kronmult_intputs_welem<T>> data;
+  if (want_ref)
+    data = make_kronmult_welem<T, true>(d, n, terms, range);
+  else
+    data = make_kronmult_welem<T, false>(d, n, terms, range);
+  std::copy(data->elem.begin(), data->elem.end(), elem);
+  for (auto const &c : data->coefficients)
+    coeff = std::copy_n(c.data(), c.size(), coeff);
+  std::copy(data->input_x.begin(), data->input_x.end(), x);
+  std::copy(data->output_y.begin(), data->output_y.end(), y);
+  std::copy(data->reference_y.begin(), data->reference_y.end(), ref_y);
+  return 0;
+}
+
+// kronmult_matrix<T> through its dense constructor
+// (src/asgard_kronmult_matrix.hpp:132-176) and apply (cpu_dense).
+template<typename T>
+int dense_apply(int d, int n, int rows, int cols, int terms, T const *coeff,
+                int const *elem, int elem_len, int row_offset, int col_offset,
+                int nb, T alpha, T const *x, T beta, T *y)
+{
+  try
+  {
+    int64_t const per = int64_t(d) * nb * nb * n * n;
+    std::vector<fk::vector<T>> tv;
+    for (int t = 0; t < terms; t++)
+      tv.push_back(fk::vector<T>(std::vector<T>(coeff + t * per, coeff + (t + 1) * per)));
+    fk::vector<int> el(std::vector<int>(elem, elem + elem_len));
+    kronmult_matrix<T> mat(d, n, rows, cols, terms, std::move(tv), std::move(el),
+                           row_offset, col_offset, nb);
+    mat.apply(alpha, x, beta, y);
+  }
+  catch (std::exception const &)
+  {
+    return 1;
+  }
   return 0;
 }
 
@@ -418,6 +466,38 @@ int ref_make_kronmult_data_f32(int d, int n, int rows, int terms, int mats,
 {
   return make_data<float>(d, n, rows, terms, mats, pntr, indx, iA, vA, x, y,
                           ref_y);
+}
+
+int ref_make_welem_f64(int d, int n, int terms, int range, int want_ref,
+                       int *elem, double *coeff, double *x, double *y,
+                       double *ref_y)
+{
+  return make_welem<double>(d, n, terms, range, want_ref, elem, coeff, x, y, ref_y);
+}
+
+int ref_make_welem_f32(int d, int n, int terms, int range, int want_ref,
+                       int *elem, float *coeff, float *x, float *y,
+                       float *ref_y)
+{
+  return make_welem<float>(d, n, terms, range, want_ref, elem, coeff, x, y, ref_y);
+}
+
+int ref_dense_apply_f64(int d, int n, int rows, int cols, int terms,
+                        double const *coeff, int const *elem, int elem_len,
+                        int row_offset, int col_offset, int nb, double alpha,
+                        double const *x, double beta, double *y)
+{
+  return dense_apply<double>(d, n, rows, cols, terms, coeff, elem, elem_len,
+                             row_offset, col_offset, nb, alpha, x, beta, y);
+}
+
+int ref_dense_apply_f32(int d, int n, int rows, int cols, int terms,
+                        float const *coeff, int const *elem, int elem_len,
+                        int row_offset, int col_offset, int nb, float alpha,
+                        float const *x, float beta, float *y)
+{
+  return dense_apply<float>(d, n, rows, cols, terms, coeff, elem, elem_len,
+                            row_offset, col_offset, nb, alpha, x, beta, y);
 }
 
 } // extern "C"

@@ -1,7 +1,8 @@
 // Drives the C++ drop-in header (include/asgard_b200/kronmult_matrix.hpp) the
 // way reference code would: builds a sparse-grid operator (d = 3, level 4,
-// 2 terms, seeded random factors) in the reference's CPU CSR format, applies
-// it on host and device vectors, solves one backward-Euler step with
+// 2 terms, seeded random factors) in the reference's CPU CSR format and in
+// its dense form, applies it on host and device vectors, solves one
+// backward-Euler step with
 // simple_gmres_euler and one dense system with simple_gmres, and writes
 // inputs and results to a binary file for tests/test_cpp_dropin_gpu.py.
 #include "asgard_b200/kronmult_matrix.hpp"
@@ -127,6 +128,48 @@ int main(int argc, char **argv)
   }
   double const global_rel = std::sqrt(num / den);
 
+  // the same operator in the reference's dense form (make_kronmult_dense's
+  // layout): full 1D operators with the connection blocks, zero elsewhere,
+  // and the cells' 1D indices; every (row, col) pair is then computed
+  int const nb = nrows1d;
+  std::vector<std::vector<double>> dterms(T, std::vector<double>(size_t(d) * nb * nb * 9, 0.0));
+  for (int r = 0; r < nrows1d; r++)
+    for (int j = c1p[r]; j < c1p[r + 1]; j++)
+      for (int t = 0; t < T; t++)
+        for (int k = 0; k < d; k++)
+          for (int e = 0; e < 9; e++)
+            dterms[t][((size_t(k) * nb + c1i[j]) * nb + r) * 9 + e] =
+                vA[((int64_t(j) * T + t) * d + k) * 9 + e];
+  std::vector<int> elem(size_t(cells) * d);
+  for (int64_t c = 0; c < cells; c++)
+    for (int k = 0; k < d; k++)
+    {
+      int const lev = table[c * 2 * d + k], pos = table[c * 2 * d + d + k];
+      elem[c * d + k] = (lev == 0) ? 0 : (1 << (lev - 1)) + pos;
+    }
+  kronmult_matrix<double> dmat(d, n, int(cells), int(cells), T, dterms, elem, 0, 0, nb);
+  std::vector<double> y_dense = y0;
+  dmat.apply<resource::host>(0.5, x.data(), -2.0, y_dense.data());
+  auto rel = [&](std::vector<double> const &a, std::vector<double> const &ref) {
+    double nu = 0, de = 0;
+    for (size_t i = 0; i < a.size(); i++)
+    {
+      nu += (a[i] - ref[i]) * (a[i] - ref[i]);
+      de += ref[i] * ref[i];
+    }
+    return std::sqrt(nu / de);
+  };
+  double const dense_rel = rel(y_dense, y_host);
+  // new per-term coefficients: twice the factors of dimension 0 doubles K x
+  for (auto &tv : dterms)
+    for (size_t e = 0; e < size_t(nb) * nb * 9; e++)
+      tv[e] *= 2.0;
+  std::vector<double> ya(N, 0.0), yb(N, 0.0);
+  mat.apply<resource::host>(2.0, x.data(), 0.0, ya.data());
+  dmat.update_stored_coefficients(dterms);
+  dmat.apply<resource::host>(1.0, x.data(), 0.0, yb.data());
+  double const dense_update_rel = rel(yb, ya);
+
   // restart larger than the system must throw std::invalid_argument
   int threw = 0;
   try
@@ -160,10 +203,13 @@ int main(int argc, char **argv)
   put(o, x3);
   std::vector<double> meta = {double(d), double(n), double(T), double(cells),
                               info.error, double(info.iterations), double(threw),
-                              info3.error, double(mat.num_batch()),
+                              info3.error, double(mat.num_pairs()),
                               double(mat.flops()),
-                              double(kronmult_matrix<double>::compute_flops(d, n, T, mat.num_batch())),
-                              double(global_refused), global_rel};
+                              double(kronmult_matrix<double>::compute_flops(d, n, T, mat.num_pairs())),
+                              double(global_refused), global_rel,
+                              double(mat.num_batch()), double(mat.is_dense()),
+                              double(dmat.is_dense()), double(dmat.num_batch()),
+                              double(dmat.flops()), dense_rel, dense_update_rel};
   put(o, meta);
   cudaFree(dx);
   cudaFree(dy);

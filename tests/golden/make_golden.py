@@ -3,7 +3,7 @@
 Run from the repository root, with the reference tree available and the
 reference oracle built (``make -C oracle ref``):
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [kron dense ops1d pde gmres]
 
 Every fixture is produced by reference code compiled from the reference's own
 sources (``oracle/_ref/libasgard_ref.so``), so the tests can pin the C
@@ -21,6 +21,12 @@ Fixtures:
   kronmult_data.npz   make_kronmult_data answers (explicit Kronecker products,
                       src/asgard_kronmult_tests.hpp) for the reference test
                       shapes of src/asgard_kronmult_matrix_tests.cpp.
+  dense_data.npz      make_kronmult_welem answers of the dense tests
+                      (src/asgard_kronmult_matrix_tests.cpp:118-176, 197-305)
+                      for the shapes whose element table stays inside the
+                      coefficient arrays: the explicit Kronecker answer and
+                      the reference kronmult_matrix (dense, cpu_dense) answer,
+                      plus one non-square case with row/column offsets.
   pde_*.npz           sparse kronmult matrices made by make_kronmult_sparse
                       for built-in PDEs, with an apply and a GMRES solve.
   gmres_3x3.json      the known-answer systems of src/solver_tests.cpp:141-213.
@@ -48,6 +54,23 @@ KRON_SHAPES = [
     (5, 2, 8, 2, 7), (5, 3, 10, 2, 7), (5, 4, 8, 2, 7),
     (6, 1, 6, 2, 7), (6, 2, 6, 2, 7), (6, 3, 8, 2, 7), (6, 4, 6, 2, 7),
 ]
+
+
+# dense-test shapes (d, n, terms, index_range) of the reference whose
+# element table stays inside the coefficient arrays: make_kronmult_welem
+# writes the cells' 1D indices as base-d digits, so for (4, n, 2, 3) and
+# (6, n, 2, 2) they reach index_range and the reference test reads past the
+# blocks of each dimension (those shapes have no defined answer)
+DENSE_SHAPES = ([(1, 2, 1, 1), (1, 2, 1, 5), (1, 2, 2, 5), (1, 2, 2, 7)]
+                + [(1, n, 3, 7) for n in range(1, 7)]
+                + [(2, n, 3, 5) for n in range(1, 6)]
+                + [(3, n, 3, 3) for n in range(1, 6)]
+                + [(5, n, 2, 1) for n in range(1, 6)]
+                + [(6, 4, 2, 1)])
+# non-square with offsets: cells [5, 15) against cells [9, 21) of a d = 2,
+# n = 3, index_range 5 table (25 cells), alpha 0.7, beta -1.3
+DENSE_OFFSET = dict(d=2, n=3, terms=2, index_range=5, rows=10, cols=12,
+                    row_offset=5, col_offset=9, alpha=0.7, beta=-1.3)
 
 
 def digest(*arrays):
@@ -78,6 +101,36 @@ def kron_data():
             out[key + "_inputs_sha256"] = np.frombuffer(
                 digest(iA, vA, x, y).encode(), dtype=np.uint8)
     np.savez_compressed(os.path.join(OUT, "kronmult_data.npz"), **out)
+
+
+def dense_data():
+    R = oracle.ref()
+    out = {}
+    for (d, n, terms, rg) in DENSE_SHAPES:
+        for dt, tag in ((np.float64, "f64"), (np.float32, "f32")):
+            a = oracle.ref_make_kronmult_welem(d, n, terms, rg, dt)
+            y = a["y"].copy()
+            oracle.kronmult_dense(d, n, a["rows"], a["rows"], a["terms"],
+                                  a["elem"], 0, 0, rg, dt(1.0), a["x"],
+                                  dt(1.0), y, lib=R)
+            key = f"{tag}_{d}_{n}_{terms}_{rg}"
+            out[key + "_ref_y"] = a["ref_y"]
+            out[key + "_cpu_dense_y"] = y
+            out[key + "_inputs_sha256"] = np.frombuffer(
+                digest(a["elem"], *a["terms"], a["x"], a["y"]).encode(),
+                dtype=np.uint8)
+    c = DENSE_OFFSET
+    a = oracle.ref_make_kronmult_welem(c["d"], c["n"], c["terms"],
+                                       c["index_range"], np.float64,
+                                       want_ref=False)
+    ts = c["n"] ** c["d"]
+    x = a["x"][c["col_offset"] * ts:(c["col_offset"] + c["cols"]) * ts].copy()
+    y = a["y"][c["row_offset"] * ts:(c["row_offset"] + c["rows"]) * ts].copy()
+    oracle.kronmult_dense(c["d"], c["n"], c["rows"], c["cols"], a["terms"],
+                          a["elem"], c["row_offset"], c["col_offset"],
+                          c["index_range"], c["alpha"], x, c["beta"], y, lib=R)
+    out["offset_y"] = y
+    np.savez_compressed(os.path.join(OUT, "dense_data.npz"), **out)
 
 
 def ops1d():
@@ -145,10 +198,11 @@ def gmres_3x3():
 
 
 if __name__ == "__main__":
+    # optional names restrict the run: kron dense ops1d pde gmres
+    parts = {"kron": kron_data, "dense": dense_data, "ops1d": ops1d,
+             "pde": pde_cases, "gmres": gmres_3x3}
     oracle.ref()
-    kron_data()
-    ops1d()
-    pde_cases()
-    gmres_3x3()
+    for name in (sys.argv[1:] or list(parts)):
+        parts[name]()
     for f in sorted(os.listdir(OUT)):
         print(f, os.path.getsize(os.path.join(OUT, f)))

@@ -63,3 +63,13 @@ def test_cpp_dropin_header(cuda, tmp_path):
     # for single-direction ones
     assert meta[11] == 1.0
     assert meta[12] < 1e-13
+    # num_batch() is rows*cols for every matrix, as in the reference
+    cells = int(meta[3])
+    assert meta[13] == cells * cells and meta[14] == 0.0
+    # dense form of the same operator: is_dense, rows*cols products, the
+    # reference's flops_ (n^d * n * rows * cols * T * d), the sparse result,
+    # and update_stored_coefficients with per-term arrays
+    assert meta[15] == 1.0 and meta[16] == cells * cells
+    assert meta[17] == n ** d * n * cells * cells * T * d
+    assert meta[18] < 1e-13
+    assert meta[19] < 1e-13

@@ -40,9 +40,10 @@ def test_global_matches_oracle_and_pairs(cuda, d, L, T):
     assert rel_err(_apply(g, 0.7, x, -1.3, y0), expect) < 1e-13
     assert rel_err(_apply(g, 0.7, x, 0.0, y0), _apply(op.kronmult_matrix(), 0.7, x, 0.0, y0)) < 1e-13
     assert rel_err(_apply(g, 0.7, x, -1.3, y0, "fp32"), expect) < 1e-5
-    # num_batch: the single-direction pairs; flops: one contraction each
-    assert g.num_batch() < op.nnz or d == 1
-    assert g.flops() == 2 * 3 ** (d + 1) * g.num_batch()
+    # num_pairs: the single-direction pairs; flops: one contraction each
+    assert g.num_pairs() < op.nnz or d == 1
+    assert g.flops() == 2 * 3 ** (d + 1) * g.num_pairs()
+    assert g.num_batch() == op.rows * op.rows
 
 
 def test_global_euler_identity_term_and_update(cuda):
@@ -109,7 +110,7 @@ def test_global_rejects_multi_direction_terms(cuda):
     with pytest.raises(ab.AsgkError):
         op.kronmult_matrix(mode="global")
     with pytest.raises(ValueError):
-        op.kronmult_matrix(mode="dense")
+        op.kronmult_matrix(mode="blocked")
 
 
 @pytest.mark.skipif(not oracle.ref_global_available(),
