@@ -66,6 +66,67 @@ public:
           "kronmult_matrix");
   }
 
+  //! Multi-call CPU form (src/asgard_kronmult_matrix.hpp:284-297, 580-627):
+  //! consecutive blocks of output rows, chunk i a CSR over its own rows
+  //! (list_pntr[i] has rows_i + 1 entries, sum rows_i = num_rows) with its
+  //! iA.  The reference applies the chunks one call each (the split bounds
+  //! its 32-bit offsets); here they form one plan, the same operator.
+  kronmult_matrix(int num_dimensions, int kron_size, int num_rows,
+                  int num_cols, int num_terms,
+                  std::vector<std::vector<int>> const &list_pntr,
+                  std::vector<std::vector<int>> const &list_indx,
+                  std::vector<std::vector<int>> const &list_iA,
+                  std::vector<double> const &vA)
+      : d_(num_dimensions), n_(kron_size), rows_(num_rows), cols_(num_cols),
+        terms_(num_terms)
+  {
+    if (list_pntr.size() != list_indx.size() || list_pntr.size() != list_iA.size())
+      throw std::runtime_error("kronmult_matrix: chunk lists differ in length");
+    std::vector<int64_t> rp(1, 0);
+    std::vector<int> indx, iA;
+    for (size_t c = 0; c < list_pntr.size(); c++)
+    {
+      auto const &p = list_pntr[c];
+      if (p.empty() || p.front() != 0 || size_t(p.back()) != list_indx[c].size())
+        throw std::runtime_error("kronmult_matrix: bad chunk row pointers");
+      int64_t const base = rp.back();
+      for (size_t r = 1; r < p.size(); r++)
+        rp.push_back(base + p[r]);
+      indx.insert(indx.end(), list_indx[c].begin(), list_indx[c].end());
+      iA.insert(iA.end(), list_iA[c].begin(), list_iA[c].end());
+    }
+    if (rp.size() != size_t(num_rows) + 1)
+      throw std::runtime_error("kronmult_matrix: chunks must cover num_rows rows");
+    check(asgk_plan_create(&plan_, d_, n_, rows_, cols_, terms_, rp.data(),
+                           indx.data(), iA.data(), vA.data(),
+                           int64_t(vA.size())),
+          "kronmult_matrix");
+  }
+
+  //! Multi-call GPU form (src/asgard_kronmult_matrix.hpp:284-297, 372-449):
+  //! chunks of pairs in the GPU format, all acting on the whole of y (beta
+  //! once, as the reference passes it to the first chunk only).
+  static kronmult_matrix from_pair_lists(int num_dimensions, int kron_size,
+                                         int num_rows, int num_cols, int num_terms,
+                                         std::vector<std::vector<int>> const &list_row_indx,
+                                         std::vector<std::vector<int>> const &list_col_indx,
+                                         std::vector<std::vector<int>> const &list_iA,
+                                         std::vector<double> const &vA)
+  {
+    if (list_row_indx.size() != list_col_indx.size() ||
+        list_row_indx.size() != list_iA.size())
+      throw std::runtime_error("kronmult_matrix: chunk lists differ in length");
+    std::vector<int> ri, ci, ia;
+    for (size_t c = 0; c < list_row_indx.size(); c++)
+    {
+      ri.insert(ri.end(), list_row_indx[c].begin(), list_row_indx[c].end());
+      ci.insert(ci.end(), list_col_indx[c].begin(), list_col_indx[c].end());
+      ia.insert(ia.end(), list_iA[c].begin(), list_iA[c].end());
+    }
+    return from_pairs(num_dimensions, kron_size, num_rows, num_cols, num_terms,
+                      ri, ci, ia, vA);
+  }
+
   //! Sparse GPU form (src/asgard_kronmult_matrix.hpp:235-272): per pair the
   //! tensor offsets into y (row_indx) and x (col_indx).
   static kronmult_matrix from_pairs(int num_dimensions, int kron_size,

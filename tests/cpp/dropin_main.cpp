@@ -1,7 +1,8 @@
 // Drives the C++ drop-in header (include/asgard_b200/kronmult_matrix.hpp) the
 // way reference code would: builds a sparse-grid operator (d = 3, level 4,
-// 2 terms, seeded random factors) in the reference's CPU CSR format and in
-// its dense form, applies it on host and device vectors, solves one
+// 2 terms, seeded random factors) in the reference's CPU CSR format, its
+// multi-call chunk forms and its dense form, applies it on host and device
+// vectors, solves one
 // backward-Euler step with
 // simple_gmres_euler and one dense system with simple_gmres, and writes
 // inputs and results to a binary file for tests/test_cpp_dropin_gpu.py.
@@ -170,6 +171,43 @@ int main(int argc, char **argv)
   dmat.apply<resource::host>(1.0, x.data(), 0.0, yb.data());
   double const dense_update_rel = rel(yb, ya);
 
+  // the multi-call forms: three CSR row blocks, and the GPU pair format in
+  // two interleaved chunks
+  std::vector<std::vector<int>> lp, li, la;
+  int const cuts[4] = {0, int(cells) / 3, 2 * int(cells) / 3, int(cells)};
+  for (int c = 0; c < 3; c++)
+  {
+    std::vector<int> p(1, 0), ix, ia;
+    for (int r = cuts[c]; r < cuts[c + 1]; r++)
+    {
+      for (int j = pntr[r]; j < pntr[r + 1]; j++)
+      {
+        ix.push_back(col[j]);
+        ia.insert(ia.end(), iA.begin() + int64_t(j) * T * d, iA.begin() + int64_t(j + 1) * T * d);
+      }
+      p.push_back(int(ix.size()));
+    }
+    lp.push_back(p);
+    li.push_back(ix);
+    la.push_back(ia);
+  }
+  kronmult_matrix<double> chunked(d, n, int(cells), int(cells), T, lp, li, la, vA);
+  std::vector<std::vector<int>> gr(2), gc(2), ga(2);
+  int const ts = mat.tensor_size();
+  for (int r = 0; r < int(cells); r++)
+    for (int j = pntr[r]; j < pntr[r + 1]; j++)
+    {
+      gr[j % 2].push_back(r * ts);
+      gc[j % 2].push_back(col[j] * ts);
+      ga[j % 2].insert(ga[j % 2].end(), iA.begin() + int64_t(j) * T * d,
+                       iA.begin() + int64_t(j + 1) * T * d);
+    }
+  auto paired = kronmult_matrix<double>::from_pair_lists(d, n, int(cells), int(cells), T, gr, gc, ga, vA);
+  std::vector<double> y_chunk = y0, y_pairs = y0;
+  chunked.apply<resource::host>(0.5, x.data(), -2.0, y_chunk.data());
+  paired.apply<resource::host>(0.5, x.data(), -2.0, y_pairs.data());
+  double const chunk_rel = rel(y_chunk, y_host), pairs_rel = rel(y_pairs, y_host);
+
   // restart larger than the system must throw std::invalid_argument
   int threw = 0;
   try
@@ -209,7 +247,8 @@ int main(int argc, char **argv)
                               double(global_refused), global_rel,
                               double(mat.num_batch()), double(mat.is_dense()),
                               double(dmat.is_dense()), double(dmat.num_batch()),
-                              double(dmat.flops()), dense_rel, dense_update_rel};
+                              double(dmat.flops()), dense_rel, dense_update_rel,
+                              chunk_rel, pairs_rel, double(chunked.num_pairs())};
   put(o, meta);
   cudaFree(dx);
   cudaFree(dy);

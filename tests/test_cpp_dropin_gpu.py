@@ -73,3 +73,6 @@ def test_cpp_dropin_header(cuda, tmp_path):
     assert meta[17] == n ** d * n * cells * cells * T * d
     assert meta[18] < 1e-13
     assert meta[19] < 1e-13
+    # multi-call forms (CSR row blocks, GPU pair chunks): the same operator
+    assert meta[20] < 1e-13 and meta[21] < 1e-13
+    assert meta[22] == len(col)
