@@ -40,8 +40,11 @@ void free_plan(plan_data &p)
   cudaFree(p.row_order);
   cudaFree(p.vA64);
   cudaFree(p.vA32);
-  cudaFree(p.xw);
-  cudaFree(p.yw);
+  if (p.ws_owned)
+  {
+    cudaFree(p.xw);
+    cudaFree(p.yw);
+  }
   cudaFree(p.xs);
   cudaFree(p.gptr);
   cudaFree(p.gcol);
@@ -274,8 +277,6 @@ int build_plan(asgk_plan **out, int d, int n, int rows, int cols, int terms,
       (rc = dev_alloc(&p.row_order, std::max(rows, 1), B)) ||
       (rc = dev_alloc(&p.vA64, std::max<int64_t>(vA_len, 1), B)) ||
       (rc = dev_alloc(&p.vA32, std::max<int64_t>(vA_len, 1), B)) ||
-      (rc = dev_alloc(&p.xw, std::max<int64_t>(int64_t(cols) * p.tensor, 1), B)) ||
-      (rc = dev_alloc(&p.yw, std::max<int64_t>(int64_t(rows) * p.tensor, 1), B)) ||
       (rc = dev_alloc(&p.vP64, p.nconn * d * terms * 10, B)) ||
       (rc = dev_alloc(&p.vP32, p.nconn * d * terms * 12, B)) ||
       (rc = dev_alloc(&p.xs, terms > 0 ? staged_x_doubles(d, n, cols) : 0, B)))
@@ -854,6 +855,28 @@ int asgk_plan_create_dense(asgk_plan **plan, int d, int n, int num_rows,
   return ASGK_OK;
 }
 
+int asgk_plan_set_workspace(asgk_plan *plan, double *x, int64_t x_len,
+                            double *y, int64_t y_len)
+{
+  if (!plan || !x || !y)
+    return ASGK_ERR_INVALID;
+  auto &p = plan->p;
+  if (x_len < int64_t(p.cols) * p.tensor || y_len < int64_t(p.rows) * p.tensor)
+    return ASGK_ERR_INVALID;
+  if (p.ws_owned && p.xw)
+  {
+    ASGK_CUDA(cudaDeviceSynchronize()); // an apply_host may still use them
+    cudaFree(p.xw);
+    cudaFree(p.yw);
+    p.device_bytes -= sizeof(double) * (std::max<int64_t>(int64_t(p.cols) * p.tensor, 1) +
+                                        std::max<int64_t>(int64_t(p.rows) * p.tensor, 1));
+  }
+  p.xw       = x;
+  p.yw       = y;
+  p.ws_owned = false;
+  return ASGK_OK;
+}
+
 int asgk_plan_kind(const asgk_plan *plan)
 {
   if (!plan)
@@ -1103,6 +1126,18 @@ int asgk_apply_host(asgk_plan *plan, double alpha, const double *x,
   cudaStream_t s   = as_stream(stream);
   int64_t const nx = int64_t(p.cols) * p.tensor;
   int64_t const ny = int64_t(p.rows) * p.tensor;
+  if (p.xw == nullptr)
+  {
+    int rc = ASGK_OK;
+    if ((rc = dev_alloc(&p.xw, std::max<int64_t>(nx, 1), p.device_bytes)) ||
+        (rc = dev_alloc(&p.yw, std::max<int64_t>(ny, 1), p.device_bytes)))
+    {
+      cudaFree(p.xw);
+      p.xw = nullptr;
+      return rc;
+    }
+    p.ws_owned = true;
+  }
   ASGK_CUDA(cudaMemcpyAsync(p.xw, x, sizeof(double) * nx,
                             cudaMemcpyHostToDevice, s));
   if (beta != 0.0)

@@ -75,8 +75,10 @@ struct plan_data
   double *vP64  = nullptr;    // [nconn][d][T][10]
   float *vP32   = nullptr;    // [nconn][d][T][12]
 
-  // FP64 workspace for apply_host and GMRES scratch
+  // FP64 staging buffers of apply_host: allocated on first use, or the
+  // caller's (set_workspace; then not owned)
   double *xw = nullptr, *yw = nullptr;
+  bool ws_owned = true;
   // x repacked for the staged kernel (n = 3, d = 3/4): padded slices
   double *xs = nullptr;
 

@@ -234,6 +234,14 @@ class kronmult_matrix:
         check(lib.asgk_plan_update_values(self._h, vA.ctypes.data, len(vA)),
               "update_stored_coefficients")
 
+    def set_workspace(self, x, y):
+        """Device tensors (float64, at least input_size / output_size) that
+        host applies stage x and y in (kronmult_matrix::set_workspace);
+        the caller keeps them alive."""
+        check(lib.asgk_plan_set_workspace(self._h, _ptr(x), x.numel(), _ptr(y),
+                                          y.numel()), "set_workspace")
+        self._workspace = (x, y)
+
     # -- apply -------------------------------------------------------------
     def apply(self, alpha, x, beta, y, resource="device", precision="fp64",
               stream=None):

@@ -114,6 +114,15 @@ int asgk_plan_create_dense(asgk_plan **plan, int d, int n, int num_rows,
                            int64_t elem_len, int row_offset, int col_offset,
                            int num_1d_blocks);
 
+/* Replaces kronmult_matrix<P>::set_workspace
+ * (src/asgard_kronmult_matrix.hpp:301-307): device buffers of at least
+ * input_size / output_size doubles that asgk_apply_host stages x and y in
+ * (the caller keeps them alive and may share them between plans that are
+ * not applied at the same time).  Without it a plan allocates its own on
+ * its first host apply. */
+int asgk_plan_set_workspace(asgk_plan *plan, double *x, int64_t x_len,
+                            double *y, int64_t y_len);
+
 /* What kind of plan this is: 0 sparse (pair list), 1 dense, 2 global
  * Kronecker form; negative on a null plan.  kronmult_matrix::is_dense()
  * (src/asgard_kronmult_matrix.hpp:514-517) is kind == 1. */

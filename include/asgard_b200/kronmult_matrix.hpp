@@ -235,6 +235,12 @@ public:
   explicit operator bool() const { return d_ > 0; }
   bool is_dense() const { return plan_ != nullptr && asgk_plan_kind(plan_) == 1; }
   bool is_onecall() const { return true; }
+  //! device buffers for apply<resource::host> (src/asgard_kronmult_matrix.hpp:301-307)
+  void set_workspace(double *xdev, double *ydev)
+  {
+    check(asgk_plan_set_workspace(plan_, xdev, input_size(), ydev, output_size()),
+          "set_workspace");
+  }
 
   static int compute_tensor_size(int num_dimensions, int kron_size)
   {

@@ -208,6 +208,17 @@ int main(int argc, char **argv)
   paired.apply<resource::host>(0.5, x.data(), -2.0, y_pairs.data());
   double const chunk_rel = rel(y_chunk, y_host), pairs_rel = rel(y_pairs, y_host);
 
+  // caller-owned staging buffers for host applies (set_workspace)
+  double *wx = nullptr, *wy = nullptr;
+  cudaMalloc(&wx, sizeof(double) * N);
+  cudaMalloc(&wy, sizeof(double) * N);
+  mat.set_workspace(wx, wy);
+  std::vector<double> y_ws = y0, x_staged(N);
+  mat.apply<resource::host>(0.5, x.data(), -2.0, y_ws.data());
+  cudaMemcpy(x_staged.data(), wx, sizeof(double) * N, cudaMemcpyDeviceToHost);
+  double const ws_rel = rel(y_ws, y_host);
+  double const ws_used = (x_staged == x) ? 1.0 : 0.0;
+
   // restart larger than the system must throw std::invalid_argument
   int threw = 0;
   try
@@ -248,11 +259,14 @@ int main(int argc, char **argv)
                               double(mat.num_batch()), double(mat.is_dense()),
                               double(dmat.is_dense()), double(dmat.num_batch()),
                               double(dmat.flops()), dense_rel, dense_update_rel,
-                              chunk_rel, pairs_rel, double(chunked.num_pairs())};
+                              chunk_rel, pairs_rel, double(chunked.num_pairs()),
+                              ws_rel, ws_used};
   put(o, meta);
   cudaFree(dx);
   cudaFree(dy);
   cudaFree(db);
+  cudaFree(wx);
+  cudaFree(wy);
   std::printf("dropin ok: %d cells, %lld pairs, gmres %d its\n", int(cells),
               (long long)nnz, info.iterations);
   return 0;

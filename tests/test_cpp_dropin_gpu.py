@@ -76,3 +76,5 @@ def test_cpp_dropin_header(cuda, tmp_path):
     # multi-call forms (CSR row blocks, GPU pair chunks): the same operator
     assert meta[20] < 1e-13 and meta[21] < 1e-13
     assert meta[22] == len(col)
+    # set_workspace: host applies stage x in the caller's device buffer
+    assert meta[23] < 1e-13 and meta[24] == 1.0

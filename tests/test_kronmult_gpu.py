@@ -216,6 +216,31 @@ def test_host_resource_apply(cuda):
     assert rel_err(y, expect) < FP64_TOL
 
 
+def test_host_apply_in_caller_workspace(cuda):
+    """set_workspace (src/asgard_kronmult_matrix.hpp:301-307): host applies
+    stage x and y in the caller's device buffers, which two plans share;
+    buffers shorter than input_size / output_size are refused."""
+    import asgard_b200 as ab
+    import torch
+    op = ab.SparseGridOperator(3, 4, 3, kind="advdiff")
+    m1, m2 = op.kronmult_matrix(), op.kronmult_matrix(mode="dense")
+    wx = torch.zeros(op.N, dtype=torch.float64, device="cuda")
+    wy = torch.zeros(op.N, dtype=torch.float64, device="cuda")
+    m1.set_workspace(wx, wy)
+    m2.set_workspace(wx, wy)
+    rng = np.random.default_rng(4)
+    x, y0 = rng.uniform(-1, 1, op.N), rng.uniform(-1, 1, op.N)
+    expect = oracle.kronmult(3, 3, op.row_ptr.astype(np.int32), op.col, 3,
+                             op.iA(), op.vA, 0.5, x, -2.0, y0.copy())
+    for m in (m1, m2):
+        y = y0.copy()
+        m.apply(0.5, x, -2.0, y, resource="host")
+        assert rel_err(y, expect) < FP64_TOL
+        assert np.array_equal(wx.cpu().numpy(), x)
+    with pytest.raises(ab.AsgkError):
+        m1.set_workspace(wx[:-1], wy)
+
+
 def test_empty_rows_and_no_terms(cuda):
     import asgard_b200 as ab
     # 3 output cells, the middle one without pairs
