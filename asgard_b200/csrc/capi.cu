@@ -1496,4 +1496,51 @@ int asgk_gmres_euler_jacobi(asgk_plan *plan, double dt, double *x,
                           precision, &mk, info, stream);
 }
 
+int asgk_implicit_advance(asgk_plan *plan, double dt, double *x, int steps,
+                          const double *forcing, int64_t forcing_stride,
+                          int restart, int max_outer, double tol, int tol_mode,
+                          int precision, int pc_kind, void *precond,
+                          asgk_gmres_info *info, asgk_stream stream)
+{
+  if (!plan || !x || steps < 0 || (steps > 0 && !info) || forcing_stride < 0 ||
+      pc_kind < 0 || pc_kind > 2 || (pc_kind != 0 && !precond))
+    return ASGK_ERR_INVALID;
+  auto &p = plan->p;
+  if (p.rows != p.cols)
+    return ASGK_ERR_INVALID;
+  int64_t const n = int64_t(p.rows) * p.tensor;
+  if (forcing && forcing_stride != 0 && forcing_stride < n)
+    return ASGK_ERR_INVALID;
+  cudaStream_t s = as_stream(stream);
+  double *b      = nullptr;
+  int64_t unused = 0;
+  if (int rc = dev_alloc(&b, std::max<int64_t>(n, 1), unused))
+    return rc;
+  int status = ASGK_OK;
+  for (int k = 0; k < steps && status == ASGK_OK; k++)
+  {
+    // right-hand side x + dt * f(t + dt); the solve starts from it, as the
+    // reference starts from a copy of its right-hand side
+    if (forcing)
+      status = launch_axpy(x, forcing + k * forcing_stride, n, dt, s);
+    if (status == ASGK_OK)
+      status = launch_copy(b, x, n, s);
+    if (status != ASGK_OK)
+      break;
+    if (pc_kind == 1)
+      status = asgk_gmres_euler_jacobi(plan, dt, x, b, restart, max_outer, tol,
+                                       tol_mode, precision,
+                                       static_cast<asgk_jacobi *>(precond),
+                                       info + k, stream);
+    else
+      status = asgk_gmres_euler(plan, dt, x, b, restart, max_outer, tol,
+                                tol_mode, precision,
+                                static_cast<asgk_mlp *>(pc_kind == 2 ? precond : nullptr),
+                                info + k, stream);
+  }
+  cudaStreamSynchronize(s);
+  cudaFree(b);
+  return status;
+}
+
 } // extern "C"

@@ -305,6 +305,38 @@ def simple_gmres_euler(dt, mat: kronmult_matrix, x, b, restart=-1,
     return gmres_info(**info.as_dict())
 
 
+def implicit_advance(dt, mat: kronmult_matrix, x, steps, forcing=None,
+                     restart=-1, max_iter=-1, tol=-1.0, tol_mode="abs",
+                     precision="fp64", precond=None, stream=None):
+    """`steps` backward-Euler steps with x resident on the device (the GMRES
+    branch of the reference's implicit_advance, src/time_advance.cpp:308-470):
+    per step x += dt*f_k, then (I - dt*K) x_new = x from the initial guess x.
+    forcing: None, one device vector (every step) or a (steps, N) device
+    tensor (one per step).  Returns the per-step gmres_info list."""
+    from .precond import JacobiPreconditioner
+    n = mat.output_size()
+    if restart is not None and restart > n:
+        raise ValueError(f"Number of inner iterations {restart} must be less than {n}!")
+    infos = (GmresInfo * max(steps, 1))()
+    stride = 0
+    if forcing is not None and forcing.dim() == 2:
+        if forcing.shape[0] < steps:
+            raise ValueError("forcing must hold one vector per step")
+        stride = forcing.stride(0)
+    kind = (0 if precond is None else
+            1 if isinstance(precond, JacobiPreconditioner) else 2)
+    rc = lib.asgk_implicit_advance(mat.handle, dt, _ptr(x), steps,
+                                   _ptr(forcing), stride,
+                                   -1 if restart is None else restart,
+                                   -1 if max_iter is None else max_iter, tol,
+                                   TOL_REL if tol_mode == "rel" else TOL_ABS,
+                                   _precision(precision), kind,
+                                   precond.handle if precond is not None else None,
+                                   infos, _stream(stream))
+    check(rc, "implicit_advance")
+    return [gmres_info(**infos[k].as_dict()) for k in range(steps)]
+
+
 def simple_gmres(A, x, b, M=None, restart=-1, max_iter=-1, tol=-1.0):
     """Dense test path of solver::simple_gmres (host arrays, solved on the GPU)."""
     if M is not None and np.size(M) > 0:
@@ -347,4 +379,5 @@ def launch_count() -> int:
 
 
 __all__ = ["kronmult_matrix", "simple_gmres_euler", "simple_gmres", "cgs_step",
+           "implicit_advance",
            "gmres_info", "default_gmres_restarts", "launch_count", "AsgkError"]

@@ -2,12 +2,15 @@
 
     python -m asgard_b200.profile_solve --d 4 --level 7 --terms 4 --dt 1e-3 \
         --mode global --precond block --precision fp32 --solves 3 [--warmup 1]
+        [--advance K]
 
 Builds the operator (connected pairs or the global Kronecker form), the
 preconditioner (none, point or block Jacobi), runs --warmup untimed and
 --solves timed solves of (I - dt K) x = b to a 1e-10 FP64 relative residual
 (GMRES restart 50, a new seeded b per solve) and prints one JSON line with
-the seconds per solve (CUDA events), iterations and residuals.  Used for
+the seconds per solve (CUDA events), iterations and residuals.  --advance K
+times K steps of the implicit time loop instead (x_{k+1} from x_k plus a
+fixed forcing, each solve started from its right-hand side).  Used for
 per-kernel captures of a solve (`ncu ... python -m asgard_b200.profile_solve`).
 """
 from __future__ import annotations
@@ -30,6 +33,10 @@ def main():
     ap.add_argument("--tol", type=float, default=1e-10)
     ap.add_argument("--solves", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=1)
+    ap.add_argument("--advance", type=int, default=0,
+                    help="time that many steps of the implicit time loop "
+                         "(implicit_advance, state resident) instead of "
+                         "independent solves")
     args = ap.parse_args()
 
     import torch
@@ -50,6 +57,34 @@ def main():
         return ab.simple_gmres_euler(args.dt, mat, x, b, args.restart, 400, args.tol,
                                      tol_mode="rel", precision=args.precision,
                                      precond=pc)
+
+    if args.advance > 0:
+        x = bs[0].clone()
+        f = bs[1] if len(bs) > 1 else None
+
+        def advance(k):
+            return ab.implicit_advance(args.dt, mat, x, k, forcing=f,
+                                       restart=args.restart, max_iter=400,
+                                       tol=args.tol, tol_mode="rel",
+                                       precision=args.precision, precond=pc)
+        advance(args.warmup)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        infos = advance(args.advance)
+        e1.record()
+        torch.cuda.synchronize()
+        s = e0.elapsed_time(e1) / 1e3 / args.advance
+        print(json.dumps({"d": args.d, "level": args.level, "terms": args.terms,
+                          "mode": args.mode, "precond": args.precond,
+                          "precision": args.precision, "dofs": op.N,
+                          "steps": args.advance, "s_per_step": s,
+                          "steps_per_s": 1.0 / s,
+                          "iterations": [i.iterations for i in infos],
+                          "true_relres": max(i.true_relres for i in infos),
+                          "setup_s": setup}))
+        return
 
     for i in range(args.warmup):
         solve(bs[i])

@@ -294,6 +294,33 @@ int asgk_gmres_euler_jacobi(asgk_plan *plan, double dt, double *x,
                             asgk_jacobi *precond, asgk_gmres_info *info,
                             asgk_stream stream);
 
+/* ------------------------------------------------ implicit time loop */
+
+typedef enum asgk_pc_kind
+{
+  ASGK_PC_NONE    = 0,
+  ASGK_PC_JACOBI  = 1, /* precond is an asgk_jacobi * */
+  ASGK_PC_LEARNED = 2  /* precond is an asgk_mlp * */
+} asgk_pc_kind;
+
+/* `steps` backward-Euler steps of the implicit time loop, the GMRES branch of
+ * implicit_advance (src/time_advance.cpp:308-470) with x resident on the
+ * device between steps: per step, x += dt * f_k (sources and boundary terms
+ * at t + dt, as the reference adds them; f_k = forcing + k*forcing_stride,
+ * forcing_stride 0 reuses one vector, forcing NULL adds nothing), then
+ * (I - dt*K) x_new = x by simple_gmres_euler starting from the right-hand
+ * side (the reference's initial guess), x_new overwriting x.  Solver
+ * arguments as asgk_gmres_euler / asgk_gmres_euler_jacobi; info[k] receives
+ * step k, including a solve that stopped short of the tolerance
+ * (info[k].status, the loop goes on as the reference's does).  An error
+ * return of a solve (invalid argument, CUDA, allocation) stops the loop and
+ * is returned.  A device buffer of one vector is allocated for the call. */
+int asgk_implicit_advance(asgk_plan *plan, double dt, double *x, int steps,
+                          const double *forcing, int64_t forcing_stride,
+                          int restart, int max_outer, double tol, int tol_mode,
+                          int precision, int pc_kind, void *precond,
+                          asgk_gmres_info *info, asgk_stream stream);
+
 /* ------------------------------------------------ learned preconditioner */
 
 /* A per-cell learned preconditioner (no counterpart in the reference, which
