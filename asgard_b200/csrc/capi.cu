@@ -1,4 +1,5 @@
 // C ABI: operator plans, apply entry points and the device-resident GMRES.
+#include "gmres_device.cuh"
 #include "internal.cuh"
 #include "mlp.cuh"
 
@@ -405,6 +406,24 @@ inline void rot(double &x, double &y, double c, double s)
 
 inline int pos_from_indices(int i, int j) { return i + j * (j + 1) / 2; }
 
+// What a recorded GMRES cycle depends on besides the workspace buffers: the
+// operator (plan, dt, arithmetic), the preconditioner, the restart length.
+struct graph_key
+{
+  const void *plan = nullptr; // the workspace dies with its plan
+  double dt        = 0;
+  int precision    = 0;
+  uint64_t pc      = 0;       // preconditioner serial (never reused), 0: none
+  int restart      = 0;
+  bool operator==(graph_key const &o) const
+  {
+    return plan == o.plan && dt == o.dt && precision == o.precision &&
+           pc == o.pc && restart == o.restart;
+  }
+};
+
+bool g_gmres_graphs = true; // asgk_set_gmres_graphs
+
 // Device workspace of a GMRES solve, kept on the plan between solves.
 struct gmres_ws
 {
@@ -414,11 +433,45 @@ struct gmres_ws
   double *V = nullptr, *Z = nullptr, *part = nullptr, *h = nullptr,
          *y = nullptr, *r = nullptr, *e = nullptr;
   double *hh = nullptr; // pinned host mirror of h
+  // reduction tickets: [0] update-norm, [1] norm, [2..] multi-dot groups
+  unsigned *tickets = nullptr;
   int nblocks = 0;
+  // recorded restart cycles (one graph per operator/preconditioner/restart)
+  double *dstate = nullptr, *hstate = nullptr; // device state, pinned mirror
+  struct cycle_graph
+  {
+    graph_key key;
+    cudaGraph_t graph      = nullptr;
+    cudaGraphExec_t exec   = nullptr;
+    int kernels_per_step   = 0;
+  };
+  std::vector<cycle_graph> graphs;
+  bool graphs_broken       = false; // a graph call failed: host-driven cycles
+  cudaStream_t capture     = nullptr;
 
   ~gmres_ws() { release(); }
+  void drop_graphs()
+  {
+    for (auto &g : graphs)
+    {
+      if (g.exec)
+        cudaGraphExecDestroy(g.exec);
+      if (g.graph)
+        cudaGraphDestroy(g.graph);
+    }
+    graphs.clear();
+  }
   void release()
   {
+    drop_graphs();
+    if (capture)
+      cudaStreamDestroy(capture);
+    capture = nullptr;
+    cudaFree(dstate);
+    dstate = nullptr;
+    if (hstate)
+      cudaFreeHost(hstate);
+    hstate = nullptr;
     cudaFree(V);
     cudaFree(Z);
     cudaFree(part);
@@ -426,6 +479,8 @@ struct gmres_ws
     cudaFree(y);
     cudaFree(r);
     cudaFree(e);
+    cudaFree(tickets);
+    tickets = nullptr;
     if (hh)
       cudaFreeHost(hh);
     V = Z = part = h = y = r = e = hh = nullptr;
@@ -438,20 +493,35 @@ struct gmres_ws
       return ASGK_OK;
     release();
     int64_t bytes = 0;
-    nblocks       = max_reduction_blocks();
+    nblocks       = max_reduction_blocks_wide();
     int rc;
     if ((rc = dev_alloc(&V, n * (restart + 1), bytes)) ||
         (flex && (rc = dev_alloc(&Z, n * restart, bytes))) ||
         (rc = dev_alloc(&part, int64_t(nblocks) * (restart + 2), bytes)) ||
         (rc = dev_alloc(&h, restart + 2, bytes)) ||
         (rc = dev_alloc(&y, restart + 1, bytes)) ||
-        (rc = dev_alloc(&r, n, bytes)) || (rc = dev_alloc(&e, n, bytes)))
+        (rc = dev_alloc(&r, n, bytes)) || (rc = dev_alloc(&e, n, bytes)) ||
+        (rc = dev_alloc(&tickets, 2 + (restart + 2 + 7) / 8, bytes)))
+    {
+      release();
+      return rc;
+    }
+    if (cudaMemset(tickets, 0, sizeof(unsigned) * (2 + (restart + 2 + 7) / 8)) !=
+        cudaSuccess)
+    {
+      cudaGetLastError();
+      release();
+      return ASGK_ERR_CUDA;
+    }
+    if ((rc = dev_alloc(&dstate, state_len(restart), bytes)))
     {
       release();
       return rc;
     }
     if (cudaMallocHost(reinterpret_cast<void **>(&hh),
-                       sizeof(double) * (restart + 2)) != cudaSuccess)
+                       sizeof(double) * (restart + 2)) != cudaSuccess ||
+        cudaMallocHost(reinterpret_cast<void **>(&hstate),
+                       sizeof(double) * state_len(restart)) != cudaSuccess)
     {
       cudaGetLastError();
       release();
@@ -464,8 +534,14 @@ struct gmres_ws
   }
 };
 
-using matvec_t  = std::function<int(double alpha, const double *x, double beta, double *y)>;
-using precond_t = std::function<int(const double *v, double *z)>;
+// operator and preconditioner callbacks take the stream they launch on (the
+// solve's stream, or the capture stream while a cycle graph is recorded)
+using matvec_t  = std::function<int(double alpha, const double *x, double beta,
+                                    double *y, cudaStream_t s)>;
+// (with scale_state, v *= scale_state[1] in place first: a recorded step's
+// normalisation of its basis vector, fused into the preconditioner)
+using precond_t = std::function<int(double *v, double *z,
+                                    const double *scale_state, cudaStream_t s)>;
 
 struct core_stats
 {
@@ -479,18 +555,165 @@ struct core_stats
   bool stagnated = false; // a preconditioned cycle reduced the residual < 10%
 };
 
+// start of a recorded cycle: the residual estimate, g[0] and the tolerance
+__global__ void k_cycle_start(double *st, double inner_res, double tol)
+{
+  if (blockIdx.x == 0 && threadIdx.x == 0)
+  {
+    st[0]          = inner_res;
+    st[1]          = 1.0;
+    st[2]          = 0.0;
+    st[3]          = 0.0;
+    st[4]          = ASGK_OK;
+    st[5]          = tol;
+    st[kStateHead] = inner_res;
+  }
+}
+
 int norm2(gmres_ws &ws, const double *v, int64_t n, double &out,
           cudaStream_t s)
 {
-  int blocks = 0;
-  if (int rc = launch_norm2(v, n, ws.part, &blocks, s))
-    return rc;
-  if (int rc = launch_reduce_parts(ws.part, blocks, 1, ws.h, s))
+  if (int rc = launch_norm2_h(v, n, ws.part, ws.tickets + 1, ws.h, s))
     return rc;
   ASGK_CUDA(cudaMemcpyAsync(ws.hh, ws.h, sizeof(double), cudaMemcpyDeviceToHost, s));
   ASGK_CUDA(cudaStreamSynchronize(s));
   out = std::sqrt(ws.hh[0]);
   return ASGK_OK;
+}
+
+// Records one restart cycle: a chain of `restart` conditional nodes, Arnoldi
+// step i in the body of node i with its basis columns fixed at record time
+// (preconditioner, operator, the two Gram-Schmidt passes, the second ending
+// in the Givens step, and the scaling of the new basis vector, folded into
+// the next step's preconditioner when there is one).  Node 0 always runs; step i's Givens
+// kernel opens node i + 1 only while the cycle goes on, so a cycle runs with
+// no host round trip and stops where the host-driven loop would.
+int record_cycle(gmres_ws &ws, int64_t n, matvec_t const &mat,
+                 precond_t const *pc, int restart, gmres_ws::cycle_graph &out)
+{
+  if (!ws.capture &&
+      cudaStreamCreateWithFlags(&ws.capture, cudaStreamNonBlocking) != cudaSuccess)
+    return ASGK_ERR_CUDA;
+  cudaStream_t const cs = ws.capture;
+  cudaGraph_t graph     = nullptr;
+  if (cudaGraphCreate(&graph, 0) != cudaSuccess)
+    return ASGK_ERR_CUDA;
+  int64_t const launches0 = g_launches.load();
+  std::vector<cudaGraphConditionalHandle> hs(restart);
+  int rc = ASGK_OK;
+  for (int i = 0; i < restart && rc == ASGK_OK; i++)
+    if (cudaGraphConditionalHandleCreate(&hs[i], graph, i == 0 ? 1u : 0u,
+                                         cudaGraphCondAssignDefault) != cudaSuccess)
+      rc = ASGK_ERR_CUDA;
+  cudaGraphNode_t prev = nullptr;
+  int kps              = 0;
+  for (int i = 0; i < restart && rc == ASGK_OK; i++)
+  {
+    cudaGraphNodeParams np{};
+    np.type                = cudaGraphNodeTypeConditional;
+    np.conditional.handle  = hs[i];
+    np.conditional.type    = cudaGraphCondTypeIf;
+    np.conditional.size    = 1;
+    cudaGraphNode_t node   = nullptr;
+    if (cudaGraphAddNode(&node, graph, prev ? &prev : nullptr, prev ? 1 : 0, &np) !=
+        cudaSuccess)
+    {
+      rc = ASGK_ERR_CUDA;
+      break;
+    }
+    cudaGraph_t body = np.conditional.phGraph_out[0];
+    if (cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0,
+                                      cudaStreamCaptureModeRelaxed) != cudaSuccess)
+    {
+      rc = ASGK_ERR_CUDA;
+      break;
+    }
+    int64_t const before = g_launches.load();
+    double *vi  = ws.V + int64_t(i) * n;
+    double *w   = ws.V + int64_t(i + 1) * n;
+    int const k = i + 1;
+    if (pc)
+    {
+      // the preconditioner also normalises v_i (step i-1 left 1/||w|| in the
+      // state; v_0 was normalised before the cycle)
+      double *zi = ws.Z + int64_t(i) * n;
+      rc         = (*pc)(vi, zi, i > 0 ? ws.dstate : nullptr, cs);
+      if (rc == ASGK_OK)
+        rc = mat(1.0, zi, 0.0, w, cs);
+    }
+    else
+      rc = mat(1.0, vi, 0.0, w, cs);
+    if (rc == ASGK_OK)
+      rc = launch_multidot_h(ws.V, n, k, w, n, ws.part, ws.tickets + 2, ws.h, cs);
+    if (rc == ASGK_OK)
+    {
+      givens_args ga;
+      ga.state    = ws.dstate;
+      ga.step     = i;
+      ga.restart  = restart;
+      ga.has_next = (i + 1 < restart) ? 1 : 0;
+      ga.next     = ga.has_next ? hs[i + 1] : hs[i];
+      rc = launch_update_norm_h(ws.V, n, k, ws.h, w, n, ws.part, ws.tickets,
+                                ws.h + k, cs, &ga);
+    }
+    // without a preconditioner to fold it into, w is normalised here (the
+    // last step's w is never read: the solution update uses v_0..v_{k-1})
+    if (rc == ASGK_OK && !pc)
+      rc = launch_scale_by(w, n, ws.dstate, cs);
+    cudaGraph_t captured = nullptr;
+    if (cudaStreamEndCapture(cs, &captured) != cudaSuccess && rc == ASGK_OK)
+      rc = ASGK_ERR_CUDA;
+    if (i == 0)
+      kps = int(g_launches.load() - before);
+    prev = node;
+  }
+  // what was launched while recording runs later, counted per executed step
+  g_launches.store(launches0);
+  cudaGraphExec_t exec = nullptr;
+  if (rc == ASGK_OK && cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess)
+    rc = ASGK_ERR_CUDA;
+  if (rc != ASGK_OK)
+  {
+    cudaGetLastError();
+    cudaGraphDestroy(graph);
+    return rc;
+  }
+  out.graph            = graph;
+  out.exec             = exec;
+  out.kernels_per_step = kps;
+  return ASGK_OK;
+}
+
+// The recorded cycle for this operator/preconditioner/restart (recorded on
+// first use, up to four kept), or null: recording is off or failed once.
+gmres_ws::cycle_graph const *cycle_graph_for(gmres_ws &ws, int64_t n,
+                                             matvec_t const &mat,
+                                             precond_t const *pc, int restart,
+                                             graph_key const &key)
+{
+  if (ws.graphs_broken || !g_gmres_graphs)
+    return nullptr;
+  for (auto &g : ws.graphs)
+    if (g.key == key)
+      return &g;
+  if (ws.graphs.size() >= 4)
+  {
+    auto &old = ws.graphs.front();
+    cudaGraphExecDestroy(old.exec);
+    cudaGraphDestroy(old.graph);
+    ws.graphs.erase(ws.graphs.begin());
+  }
+  gmres_ws::cycle_graph cg;
+  cg.key = key;
+  if (record_cycle(ws, n, mat, pc, restart, cg) != ASGK_OK)
+  {
+    std::fprintf(stderr, "asgard_b200: recording a GMRES cycle failed; "
+                         "cycles are driven from the host\n");
+    ws.graphs_broken = true;
+    return nullptr;
+  }
+  ws.graphs.push_back(cg);
+  return &ws.graphs.back();
 }
 
 // solver::simple_gmres (src/solver.cpp:157-298) on device vectors.  With a
@@ -506,7 +729,7 @@ int norm2(gmres_ws &ws, const double *v, int64_t n, double &out,
 int gmres_core(gmres_ws &ws, int64_t n, matvec_t const &mat,
                precond_t const *pc, double *x, const double *b, int restart,
                int max_outer, double tol, core_stats &st, cudaStream_t s,
-               bool verify = false)
+               bool verify = false, graph_key const *gk = nullptr)
 {
   bool const flex = (pc != nullptr);
   if (int rc = ws.ensure(n, restart, flex))
@@ -521,7 +744,7 @@ int gmres_core(gmres_ws &ws, int64_t n, matvec_t const &mat,
     double *r0 = ws.V;
     if (int rc = launch_copy(r0, b, n, s))
       return rc;
-    if (int rc = mat(-1.0, x, 1.0, r0))
+    if (int rc = mat(-1.0, x, 1.0, r0, s))
       return rc;
     ++st.total;
     ++st.matvecs;
@@ -551,32 +774,62 @@ int gmres_core(gmres_ws &ws, int64_t n, matvec_t const &mat,
       return rc;
     ksol[0] = inner_res;
     int inner = 0;
-    while (inner_res > tol && inner < restart)
+    gmres_ws::cycle_graph const *cg =
+        (gk != nullptr && inner_res > tol)
+            ? cycle_graph_for(ws, n, mat, pc, restart, *gk)
+            : nullptr;
+    if (cg != nullptr)
+    {
+      // the recorded cycle: one launch, one read of its state
+      k_cycle_start<<<1, 32, 0, s>>>(ws.dstate, inner_res, tol);
+      ASGK_LAUNCHED();
+      ASGK_CUDA(cudaGraphLaunch(cg->exec, s));
+      ASGK_CUDA(cudaMemcpyAsync(ws.hstate, ws.dstate,
+                                sizeof(double) * state_len(restart),
+                                cudaMemcpyDeviceToHost, s));
+      ASGK_CUDA(cudaStreamSynchronize(s));
+      const double *hs = ws.hstate;
+      inner            = int(hs[3]);
+      count_launch(int64_t(inner) * cg->kernels_per_step);
+      st.total += inner;
+      st.matvecs += inner;
+      if (flex)
+        st.pcalls += inner;
+      if (int(hs[4]) == ASGK_ERR_NONFINITE)
+      {
+        st.status = ASGK_ERR_NONFINITE;
+        st.err    = hs[2];
+        return ASGK_OK;
+      }
+      inner_res         = hs[0];
+      const double *g   = hs + kStateHead;
+      const double *Hp  = g + 3 * int64_t(restart + 1);
+      std::copy(g, g + inner, ksol.begin());
+      std::copy(Hp, Hp + int64_t(inner) * (inner + 1) / 2, proj.begin());
+    }
+    while (cg == nullptr && inner_res > tol && inner < restart)
     {
       double *vi = ws.V + int64_t(inner) * n;
       double *w  = ws.V + int64_t(inner + 1) * n;
       if (flex)
       {
         double *zi = ws.Z + int64_t(inner) * n;
-        if (int rc = (*pc)(vi, zi))
+        if (int rc = (*pc)(vi, zi, nullptr, s))
           return rc;
         ++st.pcalls;
-        if (int rc = mat(1.0, zi, 0.0, w))
+        if (int rc = mat(1.0, zi, 0.0, w, s))
           return rc;
       }
-      else if (int rc = mat(1.0, vi, 0.0, w))
+      else if (int rc = mat(1.0, vi, 0.0, w, s))
         return rc;
       ++st.total;
       ++st.matvecs;
       int const k = inner + 1;
-      int blocks  = 0;
-      if (int rc = launch_multidot(ws.V, n, k, w, n, ws.part, &blocks, s))
+      if (int rc = launch_multidot_h(ws.V, n, k, w, n, ws.part, ws.tickets + 2,
+                                     ws.h, s))
         return rc;
-      if (int rc = launch_reduce_parts(ws.part, blocks, k, ws.h, s))
-        return rc;
-      if (int rc = launch_update_norm(ws.V, n, k, ws.h, w, n, ws.part, &blocks, s))
-        return rc;
-      if (int rc = launch_reduce_parts(ws.part, blocks, 1, ws.h + k, s))
+      if (int rc = launch_update_norm_h(ws.V, n, k, ws.h, w, n, ws.part,
+                                        ws.tickets, ws.h + k, s))
         return rc;
       ASGK_CUDA(cudaMemcpyAsync(ws.hh, ws.h, sizeof(double) * (k + 1),
                                 cudaMemcpyDeviceToHost, s));
@@ -1204,8 +1457,9 @@ int asgk_gmres_dense(int n, const double *A, double *x, const double *b,
   cudaStream_t s = nullptr;
   gmres_ws ws;
   core_stats st;
-  auto mat = [&](double a, const double *xin, double bb, double *yout) -> int {
-    k_dense_gemv<<<(n + 3) / 4, 128, 0, s>>>(n, dA, a, xin, bb, yout);
+  auto mat = [&](double a, const double *xin, double bb, double *yout,
+                 cudaStream_t ss) -> int {
+    k_dense_gemv<<<(n + 3) / 4, 128, 0, ss>>>(n, dA, a, xin, bb, yout);
     ASGK_LAUNCHED();
     return ASGK_OK;
   };
@@ -1285,10 +1539,13 @@ namespace asgk
 // the low-precision one.
 using make_pc_t = std::function<precond_t(bool low)>;
 
+// pc_serial identifies the preconditioner for the recorded-cycle cache (0:
+// none); pc_graph_ok says whether its launches may be recorded.
 int gmres_euler_impl(asgk_plan *plan, double dt, double *x, const double *b,
                      int restart, int max_outer, double tol, int tol_mode,
                      int precision, make_pc_t const *make_pc,
-                     asgk_gmres_info *info, asgk_stream stream)
+                     asgk_gmres_info *info, asgk_stream stream,
+                     uint64_t pc_serial = 0, bool pc_graph_ok = false)
 {
   if (!plan || !x || !b)
     return ASGK_ERR_INVALID;
@@ -1311,11 +1568,13 @@ int gmres_euler_impl(asgk_plan *plan, double dt, double *x, const double *b,
   gmres_ws &ws   = ex->ws;
 
   asgk_gmres_info out{};
-  auto op64 = [&](double a, const double *xin, double bb, double *yout) -> int {
-    return asgk_apply_euler(plan, ASGK_FP64, dt, a, xin, bb, yout, stream);
+  auto op64 = [&](double a, const double *xin, double bb, double *yout,
+                  cudaStream_t ss) -> int {
+    return asgk_apply_euler(plan, ASGK_FP64, dt, a, xin, bb, yout, ss);
   };
-  auto oplow = [&](double a, const double *xin, double bb, double *yout) -> int {
-    return asgk_apply_euler(plan, precision, dt, a, xin, bb, yout, stream);
+  auto oplow = [&](double a, const double *xin, double bb, double *yout,
+                   cudaStream_t ss) -> int {
+    return asgk_apply_euler(plan, precision, dt, a, xin, bb, yout, ss);
   };
   precond_t pcf;
   precond_t const *pcp = nullptr;
@@ -1338,8 +1597,9 @@ int gmres_euler_impl(asgk_plan *plan, double dt, double *x, const double *b,
   double true_res = -1; // FP64 residual of the final x when already known
   if (precision == ASGK_FP64 && !precond)
   {
+    graph_key const gk{plan, dt, ASGK_FP64, 0, restart};
     if (int rc = gmres_core(ws, n, op64, nullptr, x, b, restart, max_outer,
-                            tol_abs, st, s, tol_mode == ASGK_TOL_REL))
+                            tol_abs, st, s, tol_mode == ASGK_TOL_REL, &gk))
       return rc;
     out.error        = st.err;
     out.iterations   = st.total;
@@ -1363,7 +1623,7 @@ int gmres_euler_impl(asgk_plan *plan, double dt, double *x, const double *b,
     {
       if (int rc = launch_copy(ws.r, b, n, s))
         return rc;
-      if (int rc = op64(-1.0, x, 1.0, ws.r))
+      if (int rc = op64(-1.0, x, 1.0, ws.r, s))
         return rc;
       ++fp64;
       if (int rc = norm2(ws, ws.r, n, rnorm, s))
@@ -1394,8 +1654,11 @@ int gmres_euler_impl(asgk_plan *plan, double dt, double *x, const double *b,
       core_stats ist;
       double const itol = std::max(inner_rtol * rnorm, 0.5 * tol_abs);
       int const inner_outer = std::max(1, max_outer);
+      graph_key const gk{plan, dt, precision, use_pc ? pc_serial : 0, restart};
+      bool const recordable = (use_pc == nullptr || pc_graph_ok);
       if (int rc = gmres_core(ws, n, (precision == ASGK_FP64) ? matvec_t(op64) : matvec_t(oplow),
-                              use_pc, ws.e, ws.r, restart, inner_outer, itol, ist, s))
+                              use_pc, ws.e, ws.r, restart, inner_outer, itol, ist, s,
+                              false, recordable ? &gk : nullptr))
         return rc;
       total += ist.total;
       if (precision == ASGK_FP64)
@@ -1443,7 +1706,7 @@ int gmres_euler_impl(asgk_plan *plan, double dt, double *x, const double *b,
   {
     if (int rc = launch_copy(ws.r, b, n, s))
       return rc;
-    if (int rc = op64(-1.0, x, 1.0, ws.r))
+    if (int rc = op64(-1.0, x, 1.0, ws.r, s))
       return rc;
     if (int rc = norm2(ws, ws.r, n, rfinal, s))
       return rc;
@@ -1470,8 +1733,11 @@ int asgk_gmres_euler(asgk_plan *plan, double dt, double *x, const double *b,
                             precision, nullptr, info, stream);
   cudaStream_t s = as_stream(stream);
   make_pc_t const mk = [&](bool low) -> precond_t {
-    return [=](const double *v, double *z) -> int {
-      return mlp_precondition(precond, plan, v, z, s, low);
+    return [=](double *v, double *z, const double *sc, cudaStream_t ss) -> int {
+      if (sc)
+        if (int rc = launch_scale_by(v, int64_t(plan->p.rows) * plan->p.tensor, sc, ss))
+          return rc;
+      return mlp_precondition(precond, plan, v, z, ss, low);
     };
   };
   return gmres_euler_impl(plan, dt, x, b, restart, max_outer, tol, tol_mode,
@@ -1488,12 +1754,20 @@ int asgk_gmres_euler_jacobi(asgk_plan *plan, double dt, double *x,
     return ASGK_ERR_INVALID;
   cudaStream_t s = as_stream(stream);
   make_pc_t const mk = [&](bool low) -> precond_t {
-    return [=](const double *v, double *z) -> int {
-      return jacobi_apply_handle(precond, low, v, z, s);
+    return [=](double *v, double *z, const double *sc, cudaStream_t ss) -> int {
+      return jacobi_apply_handle(precond, low, v, z, sc, ss);
     };
   };
   return gmres_euler_impl(plan, dt, x, b, restart, max_outer, tol, tol_mode,
-                          precision, &mk, info, stream);
+                          precision, &mk, info, stream, jacobi_serial(precond),
+                          true);
+}
+
+int asgk_set_gmres_graphs(int enable)
+{
+  int const old  = g_gmres_graphs ? 1 : 0;
+  g_gmres_graphs = (enable != 0);
+  return old;
 }
 
 int asgk_implicit_advance(asgk_plan *plan, double dt, double *x, int steps,

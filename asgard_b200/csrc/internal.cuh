@@ -140,10 +140,14 @@ int build_direction_pairs(int d, int level, int num_cells, const int *table,
 
 // jacobi.cu
 struct jacobi_data;
-int jacobi_apply(jacobi_data const &jd, bool low, const double *v, double *z,
-                 cudaStream_t s);
-int jacobi_apply_handle(asgk_jacobi *pc, bool low, const double *v, double *z,
-                        cudaStream_t s);
+// z = M v; with scale_state, v *= scale_state[1] in place first (the
+// normalisation of a recorded GMRES step's new basis vector, fused)
+int jacobi_apply(jacobi_data const &jd, bool low, double *v, double *z,
+                 const double *scale_state, cudaStream_t s);
+int jacobi_apply_handle(asgk_jacobi *pc, bool low, double *v, double *z,
+                        const double *scale_state, cudaStream_t s);
+// never reused within a process: identifies a preconditioner in caches
+uint64_t jacobi_serial(const asgk_jacobi *pc);
 
 // kron_global.cu: global-mode apply
 int launch_global(plan_data const &p, int precision, double alpha,
@@ -165,6 +169,22 @@ int launch_copy(double *dst, const double *src, int64_t n, cudaStream_t s);
 int launch_scale(double *v, int64_t n, double alpha, cudaStream_t s);
 int launch_axpy(double *y, const double *x, int64_t n, double alpha,
                 cudaStream_t s);
+// Gram-Schmidt passes that finish their reductions in their last block:
+// h[0..k) = V^T w; w -= V h with *out = ||w||^2; *out = ||v||^2.  tickets:
+// zero-initialised counters, (k+7)/8 of them for the multi-dot, one for
+// the others (left at zero after each launch)
+int launch_multidot_h(const double *V, int64_t ldv, int k, const double *w,
+                      int64_t n, double *part, unsigned *tickets, double *h,
+                      cudaStream_t s);
+struct givens_args; // gmres_device.cuh: the Givens update of a recorded step
+int launch_update_norm_h(const double *V, int64_t ldv, int k, const double *h,
+                         double *w, int64_t n, double *part, unsigned *ticket,
+                         double *out, cudaStream_t s,
+                         givens_args const *ga = nullptr);
+int launch_norm2_h(const double *v, int64_t n, double *part, unsigned *ticket,
+                   double *out, cudaStream_t s);
+// v *= state[1], the scale a recorded GMRES step computed on the device
+int launch_scale_by(double *v, int64_t n, const double *state, cudaStream_t s);
 int launch_xpby(double *y, const double *x, int64_t n, double beta,
                 cudaStream_t s);
 // partial sums of V[:,0..k)^T w into part[blocks][k]; returns blocks used
@@ -184,5 +204,7 @@ int launch_norm2(const double *v, int64_t n, double *part, int *blocks,
 int launch_gemv_add(const double *V, int64_t ldv, int k, const double *y,
                     double *x, int64_t n, cudaStream_t s);
 int max_reduction_blocks();
+// partial sums per column of the self-reducing Gram-Schmidt passes
+int max_reduction_blocks_wide();
 
 } // namespace asgk

@@ -99,7 +99,7 @@ __global__ void k_block_jacobi(int rows, int d, int n, int ts, int T,
                                index_mode mode, const int64_t *row_ptr,
                                const int *col, const int *idx,
                                const double *vA, double dt, double *M,
-                               float *M32, int *err)
+                               __half *M16, int ps16, int *err)
 {
   extern __shared__ double aug[]; // ts x 2ts
   __shared__ int piv;
@@ -167,13 +167,18 @@ __global__ void k_block_jacobi(int rows, int d, int n, int ts, int T,
     return;
   }
   double *Mc = M + int64_t(row) * ts * ts;
-  float *Mf  = M32 + int64_t(row) * ts * ts;
-  for (int e = threadIdx.x; e < ts * ts; e += blockDim.x)
+  __half *Mh = M16 + int64_t(row) * ps16;
+  for (int e = threadIdx.x; e < ps16; e += blockDim.x)
   {
+    if (e >= ts * ts)
+    {
+      Mh[e] = __float2half_rn(0.0f); // padding to a 16-byte multiple
+      continue;
+    }
     int const j = e / ts, i = e - (e / ts) * ts; // column-major
     double const v = aug[i * w + ts + j];
     Mc[e] = v;
-    Mf[e] = float(v);
+    Mh[e] = __float2half_rn(float(v));
   }
 }
 
@@ -185,13 +190,25 @@ __device__ __forceinline__ double to_d(__half v) { return __half2float(v); }
 // read consecutive entries
 template<typename TM>
 __global__ void k_block_apply(int rows, int ts, const TM *__restrict__ M,
-                              const double *__restrict__ v,
-                              double *__restrict__ z)
+                              double *__restrict__ v,
+                              double *__restrict__ z,
+                              const double *__restrict__ scale_state)
 {
   extern __shared__ double vs[];
   int const row = blockIdx.x;
-  for (int i = threadIdx.x; i < ts; i += blockDim.x)
-    vs[i] = v[int64_t(row) * ts + i];
+  if (scale_state)
+  {
+    double const f = scale_state[1];
+    for (int i = threadIdx.x; i < ts; i += blockDim.x)
+    {
+      double const vv          = v[int64_t(row) * ts + i] * f;
+      v[int64_t(row) * ts + i] = vv;
+      vs[i]                    = vv;
+    }
+  }
+  else
+    for (int i = threadIdx.x; i < ts; i += blockDim.x)
+      vs[i] = v[int64_t(row) * ts + i];
   __syncthreads();
   const TM *Mc = M + int64_t(row) * ts * ts;
   for (int i = threadIdx.x; i < ts; i += blockDim.x)
@@ -203,41 +220,108 @@ __global__ void k_block_apply(int rows, int ts, const TM *__restrict__ M,
   }
 }
 
-__global__ void k_to_f16(const float *__restrict__ a, __half *__restrict__ b,
-                         int64_t n)
+// FP16 inverses (the FP32 solves' preconditioner): z_c = M_c v_c with the
+// cell's block (ps halves, ps a multiple of 8 so every block starts on 16
+// bytes) streamed into shared memory by 16-byte loads, all issued before the
+// first is used, and FP32 accumulation (the FP16 entries carry ~5e-4
+// relative error; the sums add ~1e-7).  Blocks are read once per apply:
+// evict-first loads keep L2 for the Krylov basis.
+constexpr int kApply16Threads = 128;
+constexpr int kApply16Loads   = 8; // 16-byte loads per thread: ps <= 8192
+
+__global__ void __launch_bounds__(kApply16Threads)
+    k_block_apply16(int ts, int ps, const __half *__restrict__ M,
+                    double *__restrict__ v, double *__restrict__ z,
+                    const double *__restrict__ scale_state)
 {
-  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n;
-       i += int64_t(gridDim.x) * blockDim.x)
-    b[i] = __float2half_rn(a[i]);
+  extern __shared__ __align__(16) unsigned char smem16[];
+  __half *Ms = reinterpret_cast<__half *>(smem16);
+  float *vs  = reinterpret_cast<float *>(smem16 + sizeof(__half) * ps);
+  int const row = blockIdx.x;
+  int const nv  = ps / 8;
+  const uint4 *src = reinterpret_cast<const uint4 *>(M + int64_t(row) * ps);
+  uint4 r[kApply16Loads];
+#pragma unroll
+  for (int l = 0; l < kApply16Loads; l++)
+  {
+    int const e = threadIdx.x + l * kApply16Threads;
+    if (e < nv)
+      r[l] = __ldcs(src + e);
+  }
+  if (scale_state)
+  {
+    double const f = scale_state[1];
+    for (int i = threadIdx.x; i < ts; i += kApply16Threads)
+    {
+      double const vv          = v[int64_t(row) * ts + i] * f;
+      v[int64_t(row) * ts + i] = vv;
+      vs[i]                    = static_cast<float>(vv);
+    }
+  }
+  else
+    for (int i = threadIdx.x; i < ts; i += kApply16Threads)
+      vs[i] = static_cast<float>(v[int64_t(row) * ts + i]);
+  uint4 *dst = reinterpret_cast<uint4 *>(Ms);
+#pragma unroll
+  for (int l = 0; l < kApply16Loads; l++)
+  {
+    int const e = threadIdx.x + l * kApply16Threads;
+    if (e < nv)
+      dst[e] = r[l];
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < ts; i += kApply16Threads)
+  {
+    float s0 = 0.0f, s1 = 0.0f;
+    int j = 0;
+    for (; j + 2 <= ts; j += 2)
+    {
+      s0 = fmaf(__half2float(Ms[j * ts + i]), vs[j], s0);
+      s1 = fmaf(__half2float(Ms[(j + 1) * ts + i]), vs[j + 1], s1);
+    }
+    if (j < ts)
+      s0 = fmaf(__half2float(Ms[j * ts + i]), vs[j], s0);
+    z[int64_t(row) * ts + i] = static_cast<double>(s0 + s1);
+  }
 }
 
 __global__ void k_point_apply(int64_t n, const double *__restrict__ inv_diag,
-                              const double *__restrict__ v,
-                              double *__restrict__ z)
+                              double *__restrict__ v,
+                              double *__restrict__ z,
+                              const double *__restrict__ scale_state)
 {
+  double const f = scale_state ? scale_state[1] : 1.0;
   for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n;
        i += int64_t(gridDim.x) * blockDim.x)
-    z[i] = v[i] * inv_diag[i];
+  {
+    double vv = v[i];
+    if (scale_state)
+    {
+      vv   = vv * f;
+      v[i] = vv;
+    }
+    z[i] = vv * inv_diag[i];
+  }
 }
 
 } // namespace
 
 struct jacobi_data
 {
+  uint64_t serial = 0; // unique per preconditioner built in this process
   int kind  = 0;
   int rows  = 0;
   int ts    = 0;
   double dt = 0;
   double *inv_diag = nullptr; // point: rows*ts
   double *M64      = nullptr; // block: rows*ts*ts, column-major per cell
-  float *M32       = nullptr;
-  __half *M16      = nullptr; // applied inside the FP32 solves
+  __half *M16      = nullptr; // applied inside the FP32 solves, ps16 per cell
+  int ps16         = 0;       // ts*ts rounded up to a multiple of 8
   int64_t device_bytes = 0;
   ~jacobi_data()
   {
     cudaFree(inv_diag);
     cudaFree(M64);
-    cudaFree(M32);
     cudaFree(M16);
   }
 };
@@ -251,6 +335,8 @@ int jacobi_build(plan_data const &p, double dt, int kind, jacobi_data &jd)
   int const ts = p.tensor;
   if (kind == ASGK_JACOBI_BLOCK && ts > 81)
     return ASGK_ERR_UNSUPPORTED; // the shared-memory inverse holds ts x 2ts
+  static std::atomic<uint64_t> next_serial{1};
+  jd.serial = next_serial.fetch_add(1);
   jd.kind = kind;
   jd.rows = p.rows;
   jd.ts   = ts;
@@ -274,20 +360,18 @@ int jacobi_build(plan_data const &p, double dt, int kind, jacobi_data &jd)
   else
   {
     size_t const b = size_t(p.rows) * ts * ts;
+    jd.ps16         = (ts * ts + 7) / 8 * 8;
+    size_t const bh = size_t(p.rows) * jd.ps16;
     ASGK_CUDA(cudaMalloc(&jd.M64, sizeof(double) * b));
-    ASGK_CUDA(cudaMalloc(&jd.M32, sizeof(float) * b));
-    ASGK_CUDA(cudaMalloc(&jd.M16, sizeof(__half) * b));
-    jd.device_bytes = int64_t(b * (sizeof(double) + sizeof(float) + sizeof(__half)));
+    ASGK_CUDA(cudaMalloc(&jd.M16, sizeof(__half) * bh));
+    jd.device_bytes = int64_t(b * sizeof(double) + bh * sizeof(__half));
     size_t const shm = sizeof(double) * size_t(ts) * 2 * ts;
     ASGK_CUDA(cudaFuncSetAttribute(k_block_jacobi,
                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    int(shm)));
     k_block_jacobi<<<p.rows, 256, shm>>>(p.rows, p.d, p.n, ts, p.terms, p.mode,
                                          p.row_ptr, p.col, p.idx, vA, dt,
-                                         jd.M64, jd.M32, err);
-    ASGK_LAUNCHED();
-    int const blocks = int(std::min<int64_t>((int64_t(b) + 255) / 256, 4096));
-    k_to_f16<<<blocks, 256>>>(jd.M32, jd.M16, int64_t(b));
+                                         jd.M64, jd.M16, jd.ps16, err);
     ASGK_LAUNCHED();
   }
   int herr = 0;
@@ -295,23 +379,32 @@ int jacobi_build(plan_data const &p, double dt, int kind, jacobi_data &jd)
   return herr ? ASGK_ERR_BREAKDOWN : ASGK_OK;
 }
 
-int jacobi_apply(jacobi_data const &jd, bool low, const double *v, double *z,
-                 cudaStream_t s)
+int jacobi_apply(jacobi_data const &jd, bool low, double *v, double *z,
+                 const double *scale_state, cudaStream_t s)
 {
   int64_t const n = int64_t(jd.rows) * jd.ts;
   if (jd.kind == ASGK_JACOBI_POINT)
   {
     int const blocks = int(std::min<int64_t>((n + 255) / 256, 4096));
-    k_point_apply<<<blocks, 256, 0, s>>>(n, jd.inv_diag, v, z);
+    k_point_apply<<<blocks, 256, 0, s>>>(n, jd.inv_diag, v, z, scale_state);
     ASGK_LAUNCHED();
     return ASGK_OK;
   }
-  int const threads = jd.ts <= 32 ? 32 : (jd.ts <= 64 ? 64 : 128);
-  size_t const shm  = sizeof(double) * jd.ts;
   if (low)
-    k_block_apply<__half><<<jd.rows, threads, shm, s>>>(jd.rows, jd.ts, jd.M16, v, z);
+  {
+    if (jd.ps16 / 8 > kApply16Threads * kApply16Loads)
+      return ASGK_ERR_UNSUPPORTED;
+    size_t const shm = sizeof(__half) * jd.ps16 + sizeof(float) * jd.ts;
+    k_block_apply16<<<jd.rows, kApply16Threads, shm, s>>>(jd.ts, jd.ps16, jd.M16, v, z,
+                                                          scale_state);
+  }
   else
-    k_block_apply<double><<<jd.rows, threads, shm, s>>>(jd.rows, jd.ts, jd.M64, v, z);
+  {
+    int const threads = jd.ts <= 32 ? 32 : (jd.ts <= 64 ? 64 : 128);
+    size_t const shm  = sizeof(double) * jd.ts;
+    k_block_apply<double><<<jd.rows, threads, shm, s>>>(jd.rows, jd.ts, jd.M64, v, z,
+                                                        scale_state);
+  }
   ASGK_LAUNCHED();
   return ASGK_OK;
 }
@@ -344,13 +437,17 @@ int asgk_jacobi_apply(asgk_jacobi *pc, const double *v, double *z,
 {
   if (pc == nullptr || v == nullptr || z == nullptr)
     return ASGK_ERR_INVALID;
-  return asgk::jacobi_apply(pc->jd, false, v, z, static_cast<cudaStream_t>(stream));
+  // without a scale state v is only read
+  return asgk::jacobi_apply(pc->jd, false, const_cast<double *>(v), z, nullptr,
+                            static_cast<cudaStream_t>(stream));
 }
 
-int asgk::jacobi_apply_handle(asgk_jacobi *pc, bool low, const double *v,
-                              double *z, cudaStream_t s)
+uint64_t asgk::jacobi_serial(const asgk_jacobi *pc) { return pc ? pc->jd.serial : 0; }
+
+int asgk::jacobi_apply_handle(asgk_jacobi *pc, bool low, double *v, double *z,
+                              const double *scale_state, cudaStream_t s)
 {
-  return asgk::jacobi_apply(pc->jd, low, v, z, s);
+  return asgk::jacobi_apply(pc->jd, low, v, z, scale_state, s);
 }
 
 int asgk_jacobi_info(asgk_jacobi *pc, int *kind, double *dt,

@@ -5,7 +5,7 @@
 // the classical Gram-Schmidt step reads the Krylov basis exactly twice (one
 // multi-dot pass, one fused "w -= V h" + norm pass) and every reduction is
 // deterministic: fixed grid, per-block partial sums, then an ordered sum.
-#include "internal.cuh"
+#include "gmres_device.cuh"
 
 #include <algorithm>
 
@@ -229,9 +229,293 @@ __global__ void __launch_bounds__(kThreads)
     x[r] += dot_row(V, ldv, k, r, ys);
 }
 
+// ---- Gram-Schmidt kernels that finish their own reductions -------------
+//
+// Each block writes its partial sums, then the last block to finish (an
+// atomic ticket; the ticket is reset for the next launch) adds them in block
+// order -- the same fixed order whichever block ends last, so results are
+// deterministic -- and writes the totals.  This saves the separate
+// reduction launch after every pass.  VEC = 2 reads two rows per 16-byte
+// load (n and the leading dimension even, 16-byte aligned vectors).
+
+// out[c0 + c] = sum_b part[b*stride + c0 + c], c < nc: one warp per column,
+// lanes over the blocks in a fixed assignment, a fixed shuffle tree
+__device__ __forceinline__ void ordered_column_sums(const double *part, int nb,
+                                                    int stride, int c0, int nc,
+                                                    double *out)
+{
+  int const warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int c = warp; c < nc; c += blockDim.x >> 5)
+  {
+    double s = 0.0;
+    for (int b = lane; b < nb; b += 32)
+      s += __ldcg(part + int64_t(b) * stride + c0 + c);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+      s += __shfl_down_sync(0xffffffffu, s, o);
+    if (lane == 0)
+      out[c0 + c] = s;
+  }
+}
+
+// thread 0 publishes this block's partials (already in part) and takes a
+// ticket; true in every thread of the block that finished last
+__device__ __forceinline__ bool last_block(unsigned *ticket, unsigned nblocks)
+{
+  __shared__ unsigned s_last;
+  if (threadIdx.x == 0)
+  {
+    __threadfence();
+    s_last = (atomicAdd(ticket, 1u) == nblocks - 1) ? 1u : 0u;
+  }
+  __syncthreads();
+  if (s_last)
+    __threadfence();
+  return s_last != 0;
+}
+
+template<int VEC> struct vload;
+template<> struct vload<1>
+{
+  using T = double;
+};
+template<> struct vload<2>
+{
+  using T = double2;
+};
+
+// h[j] = V[:, j] . w for j < k; grid (row chunks, column groups of 8)
+template<int VEC>
+__global__ void __launch_bounds__(kThreads)
+    k_multidot_h(const double *__restrict__ V, int64_t ldv, int k,
+                 const double *__restrict__ w, int64_t n,
+                 double *__restrict__ part, unsigned *__restrict__ tickets,
+                 double *__restrict__ h)
+{
+  using T = typename vload<VEC>::T;
+  __shared__ double sh[kDotCols * 32];
+  int64_t const nu    = n / VEC;
+  int64_t const chunk = (nu + gridDim.x - 1) / gridDim.x;
+  int64_t const beg   = blockIdx.x * chunk;
+  int64_t const end   = min(nu, beg + chunk);
+  int const j0        = blockIdx.y * kDotCols;
+  int const nj        = min(kDotCols, k - j0);
+  int64_t const ldu   = ldv / VEC;
+  double a[kDotCols];
+#pragma unroll
+  for (int j = 0; j < kDotCols; j++)
+    a[j] = 0.0;
+  const T *Vj = reinterpret_cast<const T *>(V + int64_t(j0) * ldv);
+  const T *wu = reinterpret_cast<const T *>(w);
+  for (int64_t r = beg + threadIdx.x; r < end; r += blockDim.x)
+  {
+    T const wr = wu[r];
+#pragma unroll
+    for (int j = 0; j < kDotCols; j++)
+      if (j < nj)
+      {
+        T const v = Vj[r + j * ldu];
+        if constexpr (VEC == 1)
+          a[j] = fma(v, wr, a[j]);
+        else
+          a[j] = fma(v.y, wr.y, fma(v.x, wr.x, a[j]));
+      }
+  }
+  block_sum<kDotCols>(a, sh);
+  if (threadIdx.x == 0)
+    for (int j = 0; j < nj; j++)
+      part[int64_t(blockIdx.x) * k + j0 + j] = a[j];
+  if (!last_block(tickets + blockIdx.y, gridDim.x))
+    return;
+  ordered_column_sums(part, gridDim.x, k, j0, nj, h);
+  if (threadIdx.x == 0)
+    tickets[blockIdx.y] = 0u;
+}
+
+// w -= V[:, :k] h;  *out = ||w||^2; with ga.state set (a recorded GMRES
+// step), the last block then performs the step's Givens update.  Dynamic
+// shared memory: k doubles, plus 3*(restart+1) with a Givens update.
+template<int VEC>
+__global__ void __launch_bounds__(kThreads)
+    k_update_norm_h(const double *__restrict__ V, int64_t ldv, int k,
+                    const double *__restrict__ h, double *__restrict__ w,
+                    int64_t n, double *__restrict__ part,
+                    unsigned *__restrict__ ticket, double *__restrict__ out,
+                    givens_args ga)
+{
+  using T = typename vload<VEC>::T;
+  extern __shared__ double hs[];
+  __shared__ double sh[32];
+  for (int j = threadIdx.x; j < k; j += blockDim.x)
+    hs[j] = h[j];
+  __syncthreads();
+  int64_t const nu    = n / VEC;
+  int64_t const chunk = (nu + gridDim.x - 1) / gridDim.x;
+  int64_t const beg   = blockIdx.x * chunk;
+  int64_t const end   = min(nu, beg + chunk);
+  int64_t const ldu   = ldv / VEC;
+  const T *Vu = reinterpret_cast<const T *>(V);
+  T *wu       = reinterpret_cast<T *>(w);
+  double v[1] = {0.0};
+  for (int64_t r = beg + threadIdx.x; r < end; r += blockDim.x)
+  {
+    if constexpr (VEC == 1)
+    {
+      double const wr = wu[r] - dot_row(V, ldv, k, r, hs);
+      wu[r]           = wr;
+      v[0] += wr * wr;
+    }
+    else
+    {
+      // two rows, four basis loads in flight (four partial sums per row)
+      double x0 = 0.0, x1 = 0.0, x2 = 0.0, x3 = 0.0;
+      double y0 = 0.0, y1 = 0.0, y2 = 0.0, y3 = 0.0;
+      int j = 0;
+      for (; j + 4 <= k; j += 4)
+      {
+        T const a = Vu[r + j * ldu], b = Vu[r + (j + 1) * ldu];
+        T const c = Vu[r + (j + 2) * ldu], d = Vu[r + (j + 3) * ldu];
+        x0 = fma(a.x, hs[j], x0);
+        y0 = fma(a.y, hs[j], y0);
+        x1 = fma(b.x, hs[j + 1], x1);
+        y1 = fma(b.y, hs[j + 1], y1);
+        x2 = fma(c.x, hs[j + 2], x2);
+        y2 = fma(c.y, hs[j + 2], y2);
+        x3 = fma(d.x, hs[j + 3], x3);
+        y3 = fma(d.y, hs[j + 3], y3);
+      }
+      for (; j < k; j++)
+      {
+        T const a = Vu[r + j * ldu];
+        x0 = fma(a.x, hs[j], x0);
+        y0 = fma(a.y, hs[j], y0);
+      }
+      T wr = wu[r];
+      wr.x -= (x0 + x1) + (x2 + x3);
+      wr.y -= (y0 + y1) + (y2 + y3);
+      wu[r] = wr;
+      v[0] += wr.x * wr.x + wr.y * wr.y;
+    }
+  }
+  block_sum<1>(v, sh);
+  if (threadIdx.x == 0)
+    part[blockIdx.x] = v[0];
+  if (!last_block(ticket, gridDim.x))
+    return;
+  ordered_column_sums(part, gridDim.x, 1, 0, 1, out);
+  if (threadIdx.x == 0)
+    *ticket = 0u;
+  if (ga.state == nullptr)
+    return;
+  // the Givens update: earlier rotations staged in shared memory, then one
+  // thread (the serial part touches shared memory only)
+  double *csn    = hs + k;                   // cosines, sines: 2*(restart+1)
+  double *coeffs = csn + 2 * (ga.restart + 1); // k
+  const double *cs_g = ga.state + kStateHead + ga.restart + 1;
+  for (int j = threadIdx.x; j < 2 * (ga.restart + 1); j += blockDim.x)
+    csn[j] = (j % (ga.restart + 1) < ga.step) ? cs_g[j] : 0.0;
+  __syncthreads();
+  if (threadIdx.x == 0)
+    givens_step(ga, hs, *out, coeffs, csn);
+}
+
+// *out = ||x||^2
+__global__ void __launch_bounds__(kThreads)
+    k_norm2_h(const double *__restrict__ x, int64_t n,
+              double *__restrict__ part, unsigned *__restrict__ ticket,
+              double *__restrict__ out)
+{
+  __shared__ double sh[32];
+  int64_t const chunk = (n + gridDim.x - 1) / gridDim.x;
+  int64_t const beg   = blockIdx.x * chunk;
+  int64_t const end   = min(n, beg + chunk);
+  double v[1]         = {0.0};
+  for (int64_t r = beg + threadIdx.x; r < end; r += blockDim.x)
+    v[0] += x[r] * x[r];
+  block_sum<1>(v, sh);
+  if (threadIdx.x == 0)
+    part[blockIdx.x] = v[0];
+  if (!last_block(ticket, gridDim.x))
+    return;
+  ordered_column_sums(part, gridDim.x, 1, 0, 1, out);
+  if (threadIdx.x == 0)
+    *ticket = 0u;
+}
+
+// blocks of the self-reducing passes: up to eight per SM (full occupancy at
+// 256 threads), so enough basis loads are in flight; the multi-dot shares
+// them among its column groups
+int grid_wide(int64_t n, int groups = 1)
+{
+  int64_t const want = (n + kThreads - 1) / kThreads;
+  int64_t const cap  = std::max<int64_t>(2 * sm_count(), 8 * int64_t(sm_count()) / groups);
+  return int(std::max<int64_t>(1, std::min(want, cap)));
+}
+
+// v *= a[1] (the 1/||w|| a recorded GMRES step leaves in its device state)
+__global__ void k_scale_by(double *v, int64_t n, const double *__restrict__ a)
+{
+  double const f = a[1];
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n;
+       i += int64_t(gridDim.x) * blockDim.x)
+    v[i] *= f;
+}
+
+bool vec2_ok(const double *a, int64_t ld, const double *b)
+{
+  return (ld % 2 == 0) && (reinterpret_cast<uintptr_t>(a) % 16 == 0) &&
+         (reinterpret_cast<uintptr_t>(b) % 16 == 0);
+}
+
 } // namespace
 
 int max_reduction_blocks() { return 2 * sm_count(); }
+int max_reduction_blocks_wide() { return 8 * sm_count(); }
+
+int launch_multidot_h(const double *V, int64_t ldv, int k, const double *w,
+                      int64_t n, double *part, unsigned *tickets, double *h,
+                      cudaStream_t s)
+{
+  int const groups = (k + kDotCols - 1) / kDotCols;
+  dim3 const grid(grid_for(n), groups);
+  if (vec2_ok(V, ldv, w) && n % 2 == 0)
+    k_multidot_h<2><<<grid, kThreads, 0, s>>>(V, ldv, k, w, n, part, tickets, h);
+  else
+    k_multidot_h<1><<<grid, kThreads, 0, s>>>(V, ldv, k, w, n, part, tickets, h);
+  ASGK_LAUNCHED();
+  return ASGK_OK;
+}
+
+int launch_update_norm_h(const double *V, int64_t ldv, int k, const double *h,
+                         double *w, int64_t n, double *part, unsigned *ticket,
+                         double *out, cudaStream_t s, givens_args const *ga)
+{
+  int const g        = grid_wide(n);
+  givens_args const a = ga ? *ga : givens_args{};
+  size_t const shm   = sizeof(double) *
+                     (std::max(k, 1) + (ga ? 3 * int64_t(a.restart + 1) : 0));
+  if (vec2_ok(V, ldv, w) && n % 2 == 0)
+    k_update_norm_h<2><<<g, kThreads, shm, s>>>(V, ldv, k, h, w, n, part, ticket, out, a);
+  else
+    k_update_norm_h<1><<<g, kThreads, shm, s>>>(V, ldv, k, h, w, n, part, ticket, out, a);
+  ASGK_LAUNCHED();
+  return ASGK_OK;
+}
+
+int launch_scale_by(double *v, int64_t n, const double *state, cudaStream_t s)
+{
+  k_scale_by<<<grid_for(n), kThreads, 0, s>>>(v, n, state);
+  ASGK_LAUNCHED();
+  return ASGK_OK;
+}
+
+int launch_norm2_h(const double *v, int64_t n, double *part, unsigned *ticket,
+                   double *out, cudaStream_t s)
+{
+  k_norm2_h<<<grid_wide(n), kThreads, 0, s>>>(v, n, part, ticket, out);
+  ASGK_LAUNCHED();
+  return ASGK_OK;
+}
 
 int launch_fill(double *v, int64_t n, double a, cudaStream_t s)
 {
