@@ -33,6 +33,9 @@ def main():
     ap.add_argument("--tol", type=float, default=1e-10)
     ap.add_argument("--solves", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=1)
+    ap.add_argument("--no-graphs", action="store_true",
+                    help="drive every GMRES cycle from the host (no recorded "
+                         "cycles; the same kernels, for per-kernel captures)")
     ap.add_argument("--advance", type=int, default=0,
                     help="time that many steps of the implicit time loop "
                          "(implicit_advance, state resident) instead of "
@@ -42,6 +45,8 @@ def main():
     import torch
     import asgard_b200 as ab
 
+    if args.no_graphs:
+        ab.lib.asgk_set_gmres_graphs(0)
     t0 = time.perf_counter()
     op = ab.SparseGridOperator(args.d, args.level, args.terms)
     mat = op.kronmult_matrix(mode=args.mode)
