@@ -2,7 +2,7 @@
 
     python -m asgard_b200.profile_solve --d 4 --level 7 --terms 4 --dt 1e-3 \
         --mode global --precond block --precision fp32 --solves 3 [--warmup 1]
-        [--advance K]
+        [--advance K] [--trace] [--no-graphs]
 
 Builds the operator (connected pairs or the global Kronecker form), the
 preconditioner (none, point or block Jacobi), runs --warmup untimed and
@@ -36,6 +36,11 @@ def main():
     ap.add_argument("--no-graphs", action="store_true",
                     help="drive every GMRES cycle from the host (no recorded "
                          "cycles; the same kernels, for per-kernel captures)")
+    ap.add_argument("--trace", action="store_true",
+                    help="also run one solve under torch.profiler (CUPTI) and "
+                         "print its kernels: launches, device time, share, and "
+                         "device-busy against wall time (sees the kernels of "
+                         "recorded cycles, which ncu's launch list does not)")
     ap.add_argument("--advance", type=int, default=0,
                     help="time that many steps of the implicit time loop "
                          "(implicit_advance, state resident) instead of "
@@ -91,6 +96,9 @@ def main():
                           "setup_s": setup}))
         return
 
+    if args.trace:
+        trace(solve, bs[0])
+
     for i in range(args.warmup):
         solve(bs[i])
     torch.cuda.synchronize()
@@ -109,6 +117,40 @@ def main():
                       "true_relres": max(i.true_relres for i in infos),
                       "ms_per_iteration": s * 1e3 / (sum(i.iterations for i in infos) / len(infos)),
                       "setup_s": setup}))
+
+
+def trace(solve, b):
+    """One solve under torch.profiler: per-kernel launches and device time,
+    device-busy time against the solve's wall time."""
+    import re
+    import torch
+    from torch.profiler import ProfilerActivity, profile
+    solve(b)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    solve(b)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    with profile(activities=[ProfilerActivity.CUDA]) as prof:
+        info = solve(b)
+        torch.cuda.synchronize()
+    evs = [e for e in prof.events() if e.device_type.name == "CUDA"]
+    spans = sorted((e.time_range.start, e.time_range.end) for e in evs)
+    busy = sum(e - s for s, e in spans)
+    per = {}
+    for e in evs:
+        name = e.name.replace("(anonymous namespace)::", "").replace("asgk::", "")
+        name = re.sub(r"\(.*", "", name)
+        c = per.setdefault(name, [0, 0.0])
+        c[0] += 1
+        c[1] += e.time_range.end - e.time_range.start
+    print(json.dumps({"trace": {
+        "iterations": info.iterations, "wall_ms": wall * 1e3,
+        "device_busy_ms": busy / 1e3,
+        "first_to_last_ms": (spans[-1][1] - spans[0][0]) / 1e3,
+        "kernels": [{"name": k, "launches": c, "ms": t / 1e3,
+                     "us_per_launch": t / c, "share": t / busy}
+                    for k, (c, t) in sorted(per.items(), key=lambda kv: -kv[1][1])]}}))
 
 
 if __name__ == "__main__":
