@@ -59,6 +59,13 @@ void free_plan(plan_data &p)
   cudaFree(p.row_nslice);
   cudaFree(p.gscratch);
   cudaFree(p.gtickets);
+  cudaFree(p.gjobs);
+  cudaFree(p.gchain_last);
+  cudaFree(p.gd_ptr);
+  cudaFree(p.gd_col);
+  cudaFree(p.gd_conn);
+  cudaFree(p.gd_rel);
+  cudaFree(p.gwork);
   cudaFree(p.vP64);
   cudaFree(p.vP32);
   p = plan_data{};
@@ -92,13 +99,16 @@ __global__ void k_repack(const double *__restrict__ vA, int64_t nconn, int d,
   }
 }
 
-// Global mode: checks that every term is the identity in all but at most
-// one dimension (identity: the block of a self-connection is I and every
-// other block is 0, exactly), and sums each dimension's blocks over the terms
-// acting there.  B: [nconn*d][10] (9 values + pad).
+// Global mode: finds the dimensions each term acts in (a dimension is
+// inactive when its blocks are the identity: I for a self-connection, 0 for
+// every other, exactly) and sums each dimension's blocks over the terms
+// acting in that dimension alone.  B: [nconn*d][10] (9 values + pad).
+// multi: the terms acting in several dimensions, each as (term, its active
+// dimensions in increasing order), applied as chains of 1D passes.
 int global_blocks(int d, int terms, std::vector<int> const &conn_row,
                   std::vector<int> const &conn_col, const double *vA,
-                  std::vector<double> &B, int &n_identity)
+                  std::vector<double> &B, int &n_identity,
+                  std::vector<std::vector<int>> &multi)
 {
   int64_t const nconn = int64_t(conn_row.size());
   auto blk = [&](int64_t j, int t, int k) {
@@ -106,9 +116,10 @@ int global_blocks(int d, int terms, std::vector<int> const &conn_row,
   };
   std::vector<int> active(terms, -1);
   n_identity = 0;
+  multi.clear();
   for (int t = 0; t < terms; t++)
   {
-    int nact = 0;
+    std::vector<int> dims;
     for (int k = 0; k < d; k++)
     {
       bool ident = true;
@@ -120,15 +131,17 @@ int global_blocks(int d, int terms, std::vector<int> const &conn_row,
           ident = a[e] == ((self && e % 4 == 0) ? 1.0 : 0.0);
       }
       if (!ident)
-      {
-        active[t] = k;
-        ++nact;
-      }
+        dims.push_back(k);
     }
-    if (nact > 1)
-      return ASGK_ERR_UNSUPPORTED; // needs the multi-direction form
-    if (nact == 0)
+    if (dims.empty())
       ++n_identity;
+    else if (dims.size() == 1)
+      active[t] = dims[0];
+    else
+    {
+      dims.insert(dims.begin(), t);
+      multi.push_back(dims);
+    }
   }
   B.assign(size_t(nconn) * d * 10, 0.0);
   for (int t = 0; t < terms; t++)
@@ -141,6 +154,33 @@ int global_blocks(int d, int terms, std::vector<int> const &conn_row,
         B[(j * d + k) * 10 + e] += blk(j, t, k)[e];
   }
   return ASGK_OK;
+}
+
+// The chains of a term acting in m >= 2 dimensions a_0 < ... < a_{m-1}, as
+// the reference's permutes (src/device/asgard_kronmult.hpp:152-224) builds
+// them: 2^(m-1) chains; in chain c, dimension a_s (s >= 1) takes the lower
+// part of its operator when bit s-1 of c is 0, the upper part (diagonal
+// included) when 1; a chain applies its upper parts first (in decreasing
+// order of s), then the whole operator of a_0, then its lower parts (in
+// increasing order of s).  The chains' sum is the term's operator on the
+// sparse grid.  Stage entries: (dimension, fill) with fill 0 = upper,
+// 1 = both, 2 = lower.
+std::vector<std::vector<std::pair<int, int>>> term_chains(std::vector<int> const &dims)
+{
+  int const m = int(dims.size());
+  std::vector<std::vector<std::pair<int, int>>> out;
+  for (int c = 0; c < (1 << (m - 1)); c++)
+  {
+    std::vector<int> signed_dir(m, 0); // -s: upper, +s: lower, 0: both
+    for (int s = 1; s < m; s++)
+      signed_dir[s] = ((c >> (s - 1)) & 1) ? -s : s;
+    std::sort(signed_dir.begin(), signed_dir.end());
+    std::vector<std::pair<int, int>> chain;
+    for (int v : signed_dir)
+      chain.emplace_back(dims[std::abs(v)], v < 0 ? 0 : (v > 0 ? 2 : 1));
+    out.push_back(chain);
+  }
+  return out;
 }
 
 int upload_global_blocks(plan_data &p, std::vector<double> const &B)
@@ -1171,9 +1211,13 @@ int asgk_plan_update_values(asgk_plan *plan, const double *vA, int64_t vA_len)
   {
     std::vector<double> B;
     int n_identity = 0;
+    std::vector<std::vector<int>> multi;
     if (int rc = global_blocks(p.d, p.terms, p.g_conn_row, p.g_conn_col, vA, B,
-                               n_identity))
+                               n_identity, multi))
       return rc;
+    // the chains are built for the dimensions each term acts in
+    if (multi != p.g_multi)
+      return ASGK_ERR_INVALID;
     if (int rc = upload_global_blocks(p, B))
       return rc;
     p.g_identity = n_identity;
@@ -1199,8 +1243,9 @@ int asgk_plan_create_global(asgk_plan **plan, int d, int n, int level,
     return ASGK_ERR_INVALID;
   std::vector<double> B;
   int n_identity = 0;
+  std::vector<std::vector<int>> multi;
   if (int rc = global_blocks(d, num_terms, dp.conn_row, dp.conn_col, vA, B,
-                             n_identity))
+                             n_identity, multi))
     return rc;
   // entries of dimensions some term acts in
   std::vector<char> used(d, 0);
@@ -1296,6 +1341,80 @@ int asgk_plan_create_global(asgk_plan **plan, int d, int n, int level,
     *plan = nullptr;
     return rc;
   }
+  // chains of the terms acting in several dimensions
+  p.g_multi = multi;
+  if (!multi.empty())
+  {
+    std::vector<std::vector<std::pair<int, int>>> chains;
+    std::vector<int> chain_term;
+    for (auto const &m : multi)
+      for (auto &c : term_chains(std::vector<int>(m.begin() + 1, m.end())))
+      {
+        chains.push_back(c);
+        chain_term.push_back(m[0]);
+      }
+    p.gchains = int(chains.size());
+    int stages = 0;
+    for (auto const &c : chains)
+      stages = std::max(stages, int(c.size()));
+    // per-dimension neighbour lists (every entry of the direction pairs)
+    std::vector<int64_t> dptr(size_t(d) * (num_cells + 1), 0);
+    std::vector<int> dcol, dconn;
+    std::vector<unsigned char> drel;
+    std::vector<int64_t> per_dim(d, 0);
+    for (int k = 0; k < d; k++)
+    {
+      for (int r = 0; r < num_cells; r++)
+      {
+        for (int64_t e = dp.ptr[r]; e < dp.ptr[r + 1]; e++)
+          if (dp.dim[e] == k)
+          {
+            int const j = dp.conn[e];
+            dcol.push_back(dp.col[e]);
+            dconn.push_back(j);
+            drel.push_back(dp.conn_col[j] < dp.conn_row[j] ? 0 : (dp.conn_col[j] == dp.conn_row[j] ? 1 : 2));
+          }
+        dptr[size_t(k) * (num_cells + 1) + r + 1] = int64_t(dcol.size());
+      }
+      per_dim[k] = int64_t(dcol.size()) - dptr[size_t(k) * (num_cells + 1)];
+      if (k + 1 < d)
+        dptr[size_t(k + 1) * (num_cells + 1)] = int64_t(dcol.size());
+    }
+    std::vector<int4> jobs;
+    for (int s = 0; s < stages; s++)
+    {
+      p.stage_job0.push_back(int(jobs.size()));
+      for (int c = 0; c < p.gchains; c++)
+        if (int(chains[c].size()) > s)
+        {
+          jobs.push_back(make_int4(c, chains[c][s].first, chains[c][s].second, chain_term[c]));
+          p.gchain_entries += per_dim[chains[c][s].first];
+        }
+      p.stage_njobs.push_back(int(jobs.size()) - p.stage_job0.back());
+    }
+    std::vector<int> last(p.gchains);
+    for (int c = 0; c < p.gchains; c++)
+      last[c] = (int(chains[c].size()) - 1) % 2;
+    int64_t const N = int64_t(num_cells) * p.tensor;
+    if ((rc = dev_alloc(&p.gjobs, int64_t(jobs.size()), bytes)) ||
+        (rc = dev_alloc(&p.gchain_last, p.gchains, bytes)) ||
+        (rc = dev_alloc(&p.gd_ptr, int64_t(dptr.size()), bytes)) ||
+        (rc = dev_alloc(&p.gd_col, std::max<int64_t>(int64_t(dcol.size()), 1), bytes)) ||
+        (rc = dev_alloc(&p.gd_conn, std::max<int64_t>(int64_t(dconn.size()), 1), bytes)) ||
+        (rc = dev_alloc(&p.gd_rel, std::max<int64_t>(int64_t(drel.size()), 1), bytes)) ||
+        (rc = dev_alloc(&p.gwork, 2 * int64_t(p.gchains) * N, bytes)) ||
+        (rc = up(p.gjobs, jobs.data(), sizeof(int4) * jobs.size())) ||
+        (rc = up(p.gchain_last, last.data(), sizeof(int) * last.size())) ||
+        (rc = up(p.gd_ptr, dptr.data(), sizeof(int64_t) * dptr.size())) ||
+        (rc = up(p.gd_col, dcol.data(), sizeof(int) * dcol.size())) ||
+        (rc = up(p.gd_conn, dconn.data(), sizeof(int) * dconn.size())) ||
+        (rc = up(p.gd_rel, drel.data(), drel.size())))
+    {
+      asgk_plan_destroy(*plan);
+      *plan = nullptr;
+      return rc;
+    }
+  }
   std::vector<unsigned> zeros(num_cells, 0u);
   if ((rc = up(p.row_order, order.data(), sizeof(int) * order.size())) ||
       (rc = up(p.slice_row, srow.data(), sizeof(int) * srow.size())) ||
@@ -1324,14 +1443,14 @@ int asgk_plan_info(const asgk_plan *plan, int64_t *num_batch,
     return ASGK_ERR_INVALID;
   auto const &p = plan->p;
   if (num_batch)
-    *num_batch = p.global ? p.gnnz : p.nnz;
+    *num_batch = p.global ? p.gnnz + p.gchain_entries : p.nnz;
   if (input_size)
     *input_size = int64_t(p.cols) * p.tensor;
   if (output_size)
     *output_size = int64_t(p.rows) * p.tensor;
   // global mode: one contraction in one dimension per entry
   if (flops)
-    *flops = p.global ? int64_t(p.tensor) * p.n * p.gnnz * 2
+    *flops = p.global ? int64_t(p.tensor) * p.n * (p.gnnz + p.gchain_entries) * 2
                       : int64_t(p.tensor) * p.n * p.d * p.terms * p.nnz * 2;
   if (device_bytes)
     *device_bytes = p.device_bytes;

@@ -103,6 +103,22 @@ struct plan_data
   int *row_slice0 = nullptr, *row_nslice = nullptr; // [rows]
   double *gscratch = nullptr;  // [gslices * n^d] partial tensors
   unsigned *gtickets = nullptr; // [rows], zero between launches
+  // terms acting in several dimensions (the reference's upper/lower
+  // permutations): chains of masked 1D passes over per-dimension neighbour
+  // lists.  Stage s runs the jobs gjobs[stage_job0[s] ..] (chain, dimension,
+  // fill 0 upper / 1 both / 2 lower, term); chain outputs alternate between
+  // two buffers of gchains vectors, chain c's result is in buffer
+  // gchain_last[c].
+  std::vector<std::vector<int>> g_multi; // (term, its dimensions) per such term
+  int gchains = 0;
+  std::vector<int> stage_job0, stage_njobs;
+  int4 *gjobs = nullptr;
+  int *gchain_last = nullptr;
+  int64_t *gd_ptr = nullptr;       // [d][rows + 1]
+  int *gd_col = nullptr, *gd_conn = nullptr;
+  unsigned char *gd_rel = nullptr; // neighbour's 1D cell: 0 before, 1 same, 2 after
+  double *gwork = nullptr;         // 2 * gchains * rows * n^d values
+  int64_t gchain_entries = 0;      // neighbour entries the chains' stages visit
 
   // dense mode (every (row, col) pair): a conn-mode plan whose connection
   // index in dimension k is elem_col[k] * dense_nb + elem_row[k], the factors

@@ -1,6 +1,7 @@
-// Global-mode kronmult apply (n = 3): the operator of terms that act in one
-// dimension each, applied through the cell pairs that differ in at most one
-// dimension.
+// Global-mode kronmult apply (n = 3): the operator applied through the cell
+// pairs that differ in at most one dimension -- terms acting in one
+// dimension in one pass, terms acting in several as chains of masked 1D
+// passes (the reference's upper/lower permutations).
 //
 // Reference: the global Kronecker form (global_kron_matrix,
 // src/asgard_kronmult_matrix.cpp:1196-1334; global_cpu_one,
@@ -202,6 +203,120 @@ __global__ void __launch_bounds__(NW * 32)
     tickets[row] = 0u; // ready for the next launch
 }
 
+// One stage of the chains of the terms acting in several dimensions
+// (src/device/asgard_glkronmult_cpu.cpp:103-181): for job (chain, dimension
+// k, fill, term) and output cell r,
+//   out_r = sum over r's neighbours c along k of block(r, c), masked by the
+//           fill, applied along k to in_c,
+// where block(r, c) is the term's 3x3 factor of dimension k for the 1D pair
+// (r_k, c_k).  The fill splits the 1D operator at its diagonal, in the
+// order (1D cell, polynomial) of the reference's sparsity pattern: upper
+// keeps the neighbours after r_k and, on r_k itself, the columns p >= q of
+// row q; lower keeps the neighbours before r_k and the columns p < q.
+// in_stride 0: every job reads the same input (stage 0 reads x).
+template<int D, typename TC, typename TX>
+__global__ void __launch_bounds__(128)
+    kron_global_chain(const int4 *__restrict__ jobs, int rows,
+                      const int64_t *__restrict__ dptr,
+                      const int *__restrict__ dcol,
+                      const int *__restrict__ dconn,
+                      const unsigned char *__restrict__ drel,
+                      const TC *__restrict__ P, int T,
+                      const TX *__restrict__ in, int64_t in_stride,
+                      TC *__restrict__ out, int64_t N)
+{
+  constexpr int TS  = ipow3g(D);
+  constexpr int PAD = padG<TC>::value;
+  int4 const job    = jobs[blockIdx.y];
+  int const chain   = job.x, k = job.y, fill = job.z, t = job.w;
+  int const r       = blockIdx.x;
+  const TX *src     = in + int64_t(chain) * in_stride;
+  TC *o             = out + int64_t(chain) * N + int64_t(r) * TS;
+  int64_t const b0  = dptr[int64_t(k) * (rows + 1) + r];
+  int64_t const b1  = dptr[int64_t(k) * (rows + 1) + r + 1];
+  int const stride  = dim_stride<D>(k);
+  for (int i = threadIdx.x; i < TS; i += blockDim.x)
+  {
+    int const q    = (i / stride) % 3;
+    int const base = i - q * stride;
+    TC acc         = TC(0);
+    for (int64_t e = b0; e < b1; e++)
+    {
+      int const rel = drel[e];
+      int plo = 0, phi = 3;
+      if (fill == 0) // upper
+      {
+        if (rel == 0)
+          continue;
+        if (rel == 1)
+          plo = q;
+      }
+      else if (fill == 2) // lower
+      {
+        if (rel == 2)
+          continue;
+        if (rel == 1)
+          phi = q;
+      }
+      const TC *b  = P + ((int64_t(dconn[e]) * D + k) * T + t) * PAD;
+      const TX *xc = src + int64_t(dcol[e]) * TS + base;
+      for (int pp = plo; pp < phi; pp++)
+        acc = fma(__ldg(b + q + 3 * pp), static_cast<TC>(xc[pp * stride]), acc);
+    }
+    o[i] = acc;
+  }
+}
+
+// y += alpha * (sum of the chains' results), chains in order
+template<typename TC>
+__global__ void k_chain_sum(int chains, const int *__restrict__ last,
+                            const TC *__restrict__ work, int64_t N,
+                            double alpha, double *__restrict__ y)
+{
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < N;
+       i += int64_t(gridDim.x) * blockDim.x)
+  {
+    double s = 0.0;
+    for (int c = 0; c < chains; c++)
+      s += static_cast<double>(work[(int64_t(last[c]) * chains + c) * N + i]);
+    y[i] += alpha * s;
+  }
+}
+
+template<int D, typename TC>
+int launch_chains(plan_data const &p, double alpha, const double *x, double *y,
+                  cudaStream_t s)
+{
+  constexpr int TS  = ipow3g(D);
+  int const threads = TS >= 128 ? 128 : (TS + 31) / 32 * 32;
+  const TC *P;
+  if constexpr (sizeof(TC) == 8)
+    P = p.vP64;
+  else
+    P = p.vP32;
+  int64_t const N = int64_t(p.rows) * TS;
+  TC *work        = reinterpret_cast<TC *>(p.gwork);
+  for (size_t st = 0; st < p.stage_njobs.size(); st++)
+  {
+    dim3 const grid(p.rows, p.stage_njobs[st]);
+    const int4 *jobs = p.gjobs + p.stage_job0[st];
+    TC *out          = work + int64_t(st % 2) * p.gchains * N;
+    if (st == 0)
+      kron_global_chain<D, TC, double><<<grid, threads, 0, s>>>(
+          jobs, p.rows, p.gd_ptr, p.gd_col, p.gd_conn, p.gd_rel, P, p.terms, x,
+          0, out, N);
+    else
+      kron_global_chain<D, TC, TC><<<grid, threads, 0, s>>>(
+          jobs, p.rows, p.gd_ptr, p.gd_col, p.gd_conn, p.gd_rel, P, p.terms,
+          work + int64_t((st - 1) % 2) * p.gchains * N, N, out, N);
+    ASGK_LAUNCHED();
+  }
+  int const blocks = int(std::min<int64_t>((N + 255) / 256, 4096));
+  k_chain_sum<TC><<<blocks, 256, 0, s>>>(p.gchains, p.gchain_last, work, N, alpha, y);
+  ASGK_LAUNCHED();
+  return ASGK_OK;
+}
+
 template<int D, typename TC>
 int launch_global_d(plan_data const &p, double alpha, const double *x,
                     double beta, double *y, double ex, cudaStream_t s)
@@ -219,6 +334,8 @@ int launch_global_d(plan_data const &p, double alpha, const double *x,
       p.slice_row, p.slice_beg, p.slice_len, p.row_slice0, p.row_nslice, p.gcol, p.gkb, B,
       p.gscratch, p.gtickets, alpha, x, beta, y, ex);
   ASGK_LAUNCHED();
+  if (p.gchains > 0)
+    return launch_chains<D, TC>(p, alpha, x, y, s);
   return ASGK_OK;
 }
 

@@ -120,10 +120,10 @@ class kronmult_matrix:
 
     @classmethod
     def from_global(cls, d, n, level, table, num_terms, vA):
-        """Global Kronecker form of the sparse grid's operator (terms acting in
-        one dimension each): the element table (cells x 2d) and vA in the
-        per-1D-connection layout; raises AsgkError (unsupported) when a term
-        acts in more than one dimension."""
+        """Global Kronecker form of the sparse grid's operator: the element
+        table (cells x 2d) and vA in the per-1D-connection layout.  Terms
+        acting in one dimension are applied in one pass, terms acting in
+        several as the reference's chains of upper/lower 1D passes."""
         tb = _host(table, np.int32)
         vA = _host(vA, np.float64)
         cells = tb.shape[0]

@@ -190,7 +190,8 @@ class SparseGridOperator:
     def kronmult_matrix(self, expanded: bool = False, mode: str = "pairs"):
         """mode "pairs": the connected-pair kronmult (expanded: the
         reference's iA offsets instead of connection indices); "global": the
-        global Kronecker form (terms acting in one dimension each); "dense":
+        global Kronecker form (one pass per term acting in one dimension,
+        upper/lower chains for terms acting in several); "dense":
         the reference's dense form (every cell pair, full 1D operators)."""
         from .kronmult import kronmult_matrix
         if mode == "global":

@@ -129,17 +129,21 @@ int asgk_plan_set_workspace(asgk_plan *plan, double *x, int64_t x_len,
 int asgk_plan_kind(const asgk_plan *plan);
 
 /* Global Kronecker form (the reference's global_kron_matrix,
- * src/asgard_kronmult_matrix.cpp:1196-1334, for its single-direction terms):
- * the same operator as the connected-pair plan of this sparse grid (the
- * element table `table`, num_cells x 2d, as asgk_sparse_grid writes it; vA
- * in the per-1D-connection layout of asgk_plan_create_conn), applied through
- * the cell pairs that differ in at most one dimension.  Every term must be
- * the identity (self-connection blocks I, all others 0) in all but at most
- * one dimension, else ASGK_ERR_UNSUPPORTED; n = 3 only.  The plan works with
- * asgk_apply / asgk_apply_euler / the GMRES and Jacobi entries like any
- * other; num_batch reports the single-direction pairs and flops
- * 2 * n^(d+1) per pair.  No counterpart for the reference's multi-direction
- * terms (its upper/lower permutations). */
+ * src/asgard_kronmult_matrix.cpp:1196-1334, and global_cpu,
+ * src/device/asgard_glkronmult_cpu.cpp:103-181): the same operator as the
+ * connected-pair plan of this sparse grid (the element table `table`,
+ * num_cells x 2d, as asgk_sparse_grid writes it; vA in the per-1D-connection
+ * layout of asgk_plan_create_conn), applied through the cell pairs that
+ * differ in at most one dimension.  A term that is the identity
+ * (self-connection blocks I, all others 0) in all dimensions but one is
+ * applied in one pass with the others; a term acting in m >= 2 dimensions
+ * as the reference does it: 2^(m-1) chains of m 1D passes over the upper or
+ * lower parts of its 1D operators (its permutes), summed.  n = 3 only.  The
+ * plan works with asgk_apply / asgk_apply_euler / the GMRES and Jacobi
+ * entries like any other; asgk_plan_info's num_batch reports the neighbour
+ * entries one apply visits and flops 2 * n^(d+1) per entry.
+ * asgk_plan_update_values keeps the dimensions each term acts in
+ * (ASGK_ERR_INVALID if they change). */
 int asgk_plan_create_global(asgk_plan **plan, int d, int n, int level,
                             int num_cells, const int *table, int num_terms,
                             const double *vA, int64_t vA_len);

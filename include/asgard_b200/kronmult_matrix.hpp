@@ -177,11 +177,11 @@ public:
   }
 
   //! Global Kronecker form of a sparse-grid operator (the reference's
-  //! global_kron_matrix, src/asgard_kronmult_matrix.cpp:1196-1334, for terms
-  //! that act in one dimension each): the element table (num_cells x 2d
-  //! levels then positions, asgk_sparse_grid's layout) and the factors per
-  //! 1D connection (asgk_plan_create_conn's layout).  Throws
-  //! std::runtime_error (unsupported) when a term acts in several dimensions.
+  //! global_kron_matrix, src/asgard_kronmult_matrix.cpp:1196-1334): the
+  //! element table (num_cells x 2d levels then positions, asgk_sparse_grid's
+  //! layout) and the factors per 1D connection (asgk_plan_create_conn's
+  //! layout).  Terms acting in one dimension are applied in one pass, terms
+  //! acting in several by the reference's upper/lower permutations.
   static kronmult_matrix global_form(int num_dimensions, int kron_size,
                                      int level, std::vector<int> const &table,
                                      int num_terms,

@@ -1,6 +1,8 @@
-"""Global Kronecker form (terms acting in one dimension each): the same
-operator as the connected-pair kronmult, checked against the oracle and the
-pair plan, inside GMRES, and its error cases."""
+"""Global Kronecker form: the same operator as the connected-pair
+kronmult -- terms acting in one dimension in one pass, terms acting in
+several as chains of masked 1D passes -- checked against the oracle, the
+pair plan and the reference's own global product, inside GMRES, and its
+error cases."""
 import numpy as np
 import pytest
 
@@ -104,23 +106,89 @@ def test_global_gmres_matches_pair_gmres(cuda):
         assert (torch.linalg.norm(xs[0] - xs[1]) / torch.linalg.norm(xs[0])).item() < 1e-9
 
 
-def test_global_rejects_multi_direction_terms(cuda):
+@pytest.mark.parametrize("d,L,T", [(1, 5, 2), (2, 5, 2), (3, 4, 3), (4, 3, 2), (5, 2, 2)])
+def test_global_multi_direction_terms(cuda, d, L, T):
+    """Terms acting in every dimension (random factors): the chains of
+    masked 1D passes (the reference's upper/lower permutations) give the
+    connected-pair operator, FP64 and FP32, and the Euler form."""
     import asgard_b200 as ab
-    op = ab.SparseGridOperator(2, 3, 2, kind="random")
+    import torch
+    op = ab.SparseGridOperator(d, L, T, kind="random")
+    g = op.kronmult_matrix(mode="global")
+    rng = np.random.default_rng(d + 10)
+    x, y0 = rng.uniform(-1, 1, op.N), rng.uniform(-1, 1, op.N)
+    expect = oracle.kronmult(d, 3, op.row_ptr.astype(np.int32), op.col, T,
+                             op.iA(), op.vA, 0.7, x, -1.3, y0.copy())
+    assert rel_err(_apply(g, 0.7, x, -1.3, y0), expect) < 1e-13
+    assert rel_err(_apply(g, 0.7, x, -1.3, y0, "fp32"), expect) < 1e-5
+    pm = op.kronmult_matrix()
+    ya, yb = _dev(y0), _dev(y0)
+    g.apply_euler(1e-3, -1.0, _dev(x), 0.5, ya)
+    pm.apply_euler(1e-3, -1.0, _dev(x), 0.5, yb)
+    torch.cuda.synchronize()
+    assert rel_err(ya.cpu().numpy(), yb.cpu().numpy()) < 1e-13
+    assert g.num_pairs() > 0 and g.flops() == 2 * 3 ** (d + 1) * g.num_pairs()
+
+
+def test_global_mixed_terms_gmres_and_updates(cuda):
+    """Single-direction (advection/diffusion), all-direction (random) and
+    identity terms in one operator; GMRES with block-Jacobi matches the pair
+    plan; new values with the same active dimensions are taken, a term that
+    changes its active dimensions is refused; unknown modes raise."""
+    import asgard_b200 as ab
+    import torch
+    d, L, dt = 3, 5, 4e-3
+    a = ab.SparseGridOperator(d, L, 3, kind="advdiff")
+    r = ab.SparseGridOperator(d, L, 2, kind="random")
+    nconn = len(ab.connect_1d(L)[1])
+    va = a.vA.reshape(nconn, 3, d, 9)
+    vr = 0.05 * r.vA.reshape(nconn, 2, d, 9)
+    vA = np.concatenate([va, vr], axis=1).ravel()
+    T = 5
+    g = ab.kronmult_matrix.from_global(d, 3, L, a.table, T, vA)
+    pm = ab.kronmult_matrix.from_conn(d, 3, a.rows, a.rows, T, a.row_ptr, a.col, a.conn, vA)
+    rng = np.random.default_rng(4)
+    x = rng.uniform(-1, 1, a.N)
+    assert rel_err(_apply(g, 1.0, x, 0.0, np.zeros(a.N)),
+                   _apply(pm, 1.0, x, 0.0, np.zeros(a.N))) < 1e-13
+    b = _dev(rng.uniform(-1, 1, a.N))
+    infos, xs = [], []
+    for mat in (pm, g):
+        pc = ab.JacobiPreconditioner(mat, dt, kind="block")
+        xx = torch.zeros_like(b)
+        info = ab.simple_gmres_euler(dt, mat, xx, b, 50, 200, 1e-10, tol_mode="rel",
+                                     precision="fp32", precond=pc)
+        assert info.status == 0 and info.true_relres <= 1e-10
+        infos.append(info)
+        xs.append(xx)
+    assert abs(infos[0].iterations - infos[1].iterations) <= 1
+    assert (torch.linalg.norm(xs[0] - xs[1]) / torch.linalg.norm(xs[0])).item() < 1e-9
+    v2 = vA.reshape(nconn, T, d, 9).copy()
+    v2[:, 3:] *= 1.5                       # same active dimensions
+    v2 = v2.ravel()
+    g.update_stored_coefficients(v2)
+    pm.update_stored_coefficients(v2)
+    assert rel_err(_apply(g, 1.0, x, 0.0, np.zeros(a.N)),
+                   _apply(pm, 1.0, x, 0.0, np.zeros(a.N))) < 1e-13
+    v3 = v2.reshape(nconn, T, d, 9).copy()
+    v3[:, 0, (0 + 1) % d] = v3[:, 1, 1 % d]  # term 0 now acts in two dimensions
     with pytest.raises(ab.AsgkError):
-        op.kronmult_matrix(mode="global")
+        g.update_stored_coefficients(v3.ravel())
     with pytest.raises(ValueError):
-        op.kronmult_matrix(mode="blocked")
+        a.kronmult_matrix(mode="blocked")
 
 
 @pytest.mark.skipif(not oracle.ref_global_available(),
                     reason="reference global-kron library not built")
-@pytest.mark.parametrize("d,L,T", [(2, 6, 3), (3, 5, 3), (4, 5, 4)])
-def test_global_matches_reference_global_kron(cuda, d, L, T):
+@pytest.mark.parametrize("d,L,T,kind", [(2, 6, 3, "advdiff"), (3, 5, 3, "advdiff"),
+                                        (4, 5, 4, "advdiff"), (2, 5, 2, "random"),
+                                        (3, 4, 2, "random"), (4, 3, 2, "random")])
+def test_global_matches_reference_global_kron(cuda, d, L, T, kind):
     """The GPU global form against the reference's own global Kronecker
-    product (global_cpu compiled from its sources)."""
+    product (global_cpu compiled from its sources), single-direction terms
+    and terms acting in every dimension (its upper/lower permutations)."""
     import asgard_b200 as ab
-    op = ab.SparseGridOperator(d, L, T, kind="advdiff")
+    op = ab.SparseGridOperator(d, L, T, kind=kind)
     x = np.random.default_rng(7).uniform(-1, 1, op.N)
     y_ref, _ = oracle.ref_global_apply(d, 3, L, op.table, T, op.vA, x)
     g = op.kronmult_matrix(mode="global")

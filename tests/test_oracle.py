@@ -214,14 +214,18 @@ def test_jacobi_restatements_against_dense_assembly():
 
 @pytest.mark.skipif(not oracle.ref_global_available(),
                     reason="reference global-kron library not built (make -C oracle ref_global)")
-@pytest.mark.parametrize("d,L,T", [(1, 5, 2), (2, 5, 3), (3, 4, 3), (4, 3, 4)])
-def test_reference_global_kron_equals_pair_kronmult(d, L, T):
+@pytest.mark.parametrize("d,L,T,kind", [(1, 5, 2, "advdiff"), (2, 5, 3, "advdiff"),
+                                        (3, 4, 3, "advdiff"), (4, 3, 4, "advdiff"),
+                                        (2, 4, 2, "random"), (3, 4, 2, "random"),
+                                        (4, 3, 2, "random")])
+def test_reference_global_kron_equals_pair_kronmult(d, L, T, kind):
     """The reference's global Kronecker product (compiled from its sources in
-    KRON_MODE_GLOBAL) and the connected-pair kronmult give the same operator
-    on advection/diffusion factors (terms acting in one dimension each) --
-    the identity the global form of this library rests on."""
+    KRON_MODE_GLOBAL) and the connected-pair kronmult give the same operator,
+    for terms acting in one dimension each (advection/diffusion factors) and
+    for terms acting in every dimension (random factors, its upper/lower
+    permutations) -- the identity the global form of this library rests on."""
     import asgard_b200.operators as O
-    op = O.SparseGridOperator(d, L, T, kind="advdiff")
+    op = O.SparseGridOperator(d, L, T, kind=kind)
     x = np.random.default_rng(d).uniform(-1, 1, op.N)
     y_ref, _ = oracle.ref_global_apply(d, 3, L, op.table, T, op.vA, x)
     y_pair = oracle.kronmult(d, 3, op.row_ptr.astype(np.int32), op.col, T,
