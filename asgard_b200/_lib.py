@@ -14,7 +14,7 @@ LIB_PATH = os.path.join(HERE, "libasgard_b200.so")
 EXPORTS = [
     "asgk_plan_create", "asgk_plan_create_pairs", "asgk_plan_create_conn",
     "asgk_plan_create_global", "asgk_plan_create_dense", "asgk_plan_kind",
-    "asgk_plan_update_terms", "asgk_plan_set_workspace",
+    "asgk_plan_update_terms", "asgk_plan_set_workspace", "asgk_plan_create_grid",
     "asgk_plan_destroy", "asgk_plan_update_values", "asgk_plan_info",
     "asgk_apply", "asgk_apply_f32", "asgk_apply_host", "asgk_apply_euler",
     "asgk_gmres_euler", "asgk_gmres_dense", "asgk_default_gmres_restarts",
@@ -62,6 +62,7 @@ def _load():
         "asgk_plan_create_global": ([C.POINTER(_vp), _i, _i, _i, _i, _vp, _i, _vp, _i64], _i),
         "asgk_plan_create_dense": ([C.POINTER(_vp), _i, _i, _i, _i, _i, _vp, _vp, _i64, _i, _i, _i], _i),
         "asgk_plan_kind": ([_vp], _i),
+        "asgk_plan_create_grid": ([C.POINTER(_vp), _i, _i, _i, _i, _vp, _i64], _i),
         "asgk_plan_set_workspace": ([_vp, _vp, _i64, _vp, _i64], _i),
         "asgk_plan_update_terms": ([_vp, _vp, _i], _i),
         "asgk_plan_destroy": ([_vp], None),

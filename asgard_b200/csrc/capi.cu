@@ -251,6 +251,43 @@ int64_t ipow(int n, int d)
   return r;
 }
 
+// Sets a plan's sizes and allocates its device arrays: CSR pairs with idx_len
+// factor indices, the factors (FP64, FP32, repacked per connection for
+// n = 3 conn plans) and the staged kernel's x scratch.  Frees what it
+// allocated on failure.
+int alloc_plan(plan_data &p, int d, int n, int rows, int cols, int terms,
+               int64_t nnz, index_mode mode, int64_t vA_len, int64_t idx_len)
+{
+  int64_t const blk = int64_t(d) * terms * n * n;
+  p.d      = d;
+  p.n      = n;
+  p.rows   = rows;
+  p.cols   = cols;
+  p.terms  = terms;
+  p.tensor = int(ipow(n, d));
+  p.nnz    = nnz;
+  p.mode   = mode;
+  p.vA_len = vA_len;
+  if (mode == index_mode::conn && n == 3 && terms > 0)
+    p.nconn = vA_len / blk;
+  int64_t &B = p.device_bytes;
+  int rc     = ASGK_OK;
+  if ((rc = dev_alloc(&p.row_ptr, rows + 1, B)) ||
+      (rc = dev_alloc(&p.col, std::max<int64_t>(nnz, 1), B)) ||
+      (rc = dev_alloc(&p.idx, std::max<int64_t>(idx_len, 1), B)) ||
+      (rc = dev_alloc(&p.row_order, std::max(rows, 1), B)) ||
+      (rc = dev_alloc(&p.vA64, std::max<int64_t>(vA_len, 1), B)) ||
+      (rc = dev_alloc(&p.vA32, std::max<int64_t>(vA_len, 1), B)) ||
+      (rc = dev_alloc(&p.vP64, p.nconn * d * terms * 10, B)) ||
+      (rc = dev_alloc(&p.vP32, p.nconn * d * terms * 12, B)) ||
+      (rc = dev_alloc(&p.xs, terms > 0 ? staged_x_doubles(d, n, cols) : 0, B)))
+  {
+    free_plan(p);
+    return rc;
+  }
+  return ASGK_OK;
+}
+
 // Builds the device plan from host CSR arrays (validated here).
 int build_plan(asgk_plan **out, int d, int n, int rows, int cols, int terms,
                std::vector<int64_t> const &row_ptr, const int *col,
@@ -299,32 +336,9 @@ int build_plan(asgk_plan **out, int d, int n, int rows, int cols, int terms,
   if (!plan)
     return ASGK_ERR_ALLOC;
   plan_data &p = plan->p;
-  p.d = d;
-  p.n = n;
-  p.rows = rows;
-  p.cols = cols;
-  p.terms = terms;
-  p.tensor = int(ipow(n, d));
-  p.nnz = nnz;
-  p.mode = mode;
-  p.vA_len = vA_len;
-  if (mode == index_mode::conn && n == 3 && terms > 0)
-    p.nconn = vA_len / blk;
-  int64_t &B = p.device_bytes;
-  int rc = ASGK_OK;
-  if ((rc = dev_alloc(&p.row_ptr, rows + 1, B)) ||
-      (rc = dev_alloc(&p.col, std::max<int64_t>(nnz, 1), B)) ||
-      (rc = dev_alloc(&p.idx, std::max<int64_t>(idx_len, 1), B)) ||
-      (rc = dev_alloc(&p.row_order, std::max(rows, 1), B)) ||
-      (rc = dev_alloc(&p.vA64, std::max<int64_t>(vA_len, 1), B)) ||
-      (rc = dev_alloc(&p.vA32, std::max<int64_t>(vA_len, 1), B)) ||
-      (rc = dev_alloc(&p.vP64, p.nconn * d * terms * 10, B)) ||
-      (rc = dev_alloc(&p.vP32, p.nconn * d * terms * 12, B)) ||
-      (rc = dev_alloc(&p.xs, terms > 0 ? staged_x_doubles(d, n, cols) : 0, B)))
-  {
-    free_plan(p);
+  int rc       = alloc_plan(p, d, n, rows, cols, terms, nnz, mode, vA_len, idx_len);
+  if (rc)
     return rc;
-  }
   // cells by decreasing pair count, ties by index
   std::vector<int> order(rows);
   std::iota(order.begin(), order.end(), 0);
@@ -1167,6 +1181,127 @@ int asgk_plan_set_workspace(asgk_plan *plan, double *x, int64_t x_len,
   p.xw       = x;
   p.yw       = y;
   p.ws_owned = false;
+  return ASGK_OK;
+}
+
+int asgk_plan_create_grid(asgk_plan **plan, int d, int n, int level,
+                          int num_terms, const double *vA, int64_t vA_len)
+{
+  if (plan == nullptr)
+    return ASGK_ERR_INVALID;
+  *plan = nullptr;
+  if (d < 1 || d > 6 || level < 0 || level > 12 || num_terms < 0 ||
+      (num_terms > 0 && vA == nullptr))
+    return ASGK_ERR_INVALID;
+  if (int rc = check_dims(d, n, 0, 0, num_terms))
+    return rc;
+  int64_t const ncells = asgk_sparse_grid(d, level, nullptr);
+  if (ncells <= 0 || ncells > (int64_t(1) << 30))
+    return ASGK_ERR_UNSUPPORTED;
+  int const cells = int(ncells);
+  std::vector<int> table(size_t(cells) * 2 * d);
+  asgk_sparse_grid(d, level, table.data());
+  int R = 0, nconn = 0;
+  if (int rc = asgk_connect_1d(level, &R, &nconn, nullptr, nullptr))
+    return rc;
+  std::vector<int> pntr(R + 1), indx(nconn);
+  asgk_connect_1d(level, &R, &nconn, pntr.data(), indx.data());
+  int64_t const blk = int64_t(d) * num_terms * n * n;
+  if (vA_len != int64_t(nconn) * blk)
+    return ASGK_ERR_INVALID;
+  std::vector<int> lut(size_t(R) * R, -1), oned(size_t(cells) * d);
+  for (int r = 0; r < R; r++)
+    for (int j = pntr[r]; j < pntr[r + 1]; j++)
+      lut[size_t(r) * R + indx[j]] = j;
+  for (int c = 0; c < cells; c++)
+    for (int k = 0; k < d; k++)
+    {
+      int const lv = table[size_t(c) * 2 * d + k], ps = table[size_t(c) * 2 * d + d + k];
+      oned[size_t(c) * d + k] = (lv == 0) ? 0 : (1 << (lv - 1)) + ps;
+    }
+  // candidates in the order each row's pairs are kept: the staged n = 3,
+  // d = 3/4 kernel wants them by factor blocks, last dimension slowest (the
+  // order build_plan sorts host lists into); table order otherwise
+  std::vector<int> cand(cells);
+  std::iota(cand.begin(), cand.end(), 0);
+  if (n == 3 && (d == 3 || d == 4) && num_terms > 0)
+    std::stable_sort(cand.begin(), cand.end(), [&](int a, int b) {
+      for (int k = d - 1; k >= 0; k--)
+        if (oned[size_t(a) * d + k] != oned[size_t(b) * d + k])
+          return oned[size_t(a) * d + k] < oned[size_t(b) * d + k];
+      return a < b;
+    });
+  int *d_oned = nullptr, *d_cand = nullptr, *d_lut = nullptr;
+  int64_t *d_counts = nullptr;
+  int64_t scratch   = 0;
+  auto release = [&]() {
+    cudaFree(d_oned);
+    cudaFree(d_cand);
+    cudaFree(d_lut);
+    cudaFree(d_counts);
+  };
+  int rc = ASGK_OK;
+  if ((rc = dev_alloc(&d_oned, int64_t(oned.size()), scratch)) ||
+      (rc = dev_alloc(&d_cand, cells, scratch)) ||
+      (rc = dev_alloc(&d_lut, int64_t(lut.size()), scratch)) ||
+      (rc = dev_alloc(&d_counts, cells, scratch)))
+  {
+    release();
+    return rc;
+  }
+  std::vector<int64_t> counts(cells), row_ptr(size_t(cells) + 1, 0);
+  if (cudaMemcpy(d_oned, oned.data(), sizeof(int) * oned.size(), cudaMemcpyHostToDevice) ||
+      cudaMemcpy(d_cand, cand.data(), sizeof(int) * cand.size(), cudaMemcpyHostToDevice) ||
+      cudaMemcpy(d_lut, lut.data(), sizeof(int) * lut.size(), cudaMemcpyHostToDevice))
+    rc = ASGK_ERR_CUDA;
+  if (!rc)
+    rc = launch_count_pairs(d, cells, d_oned, d_cand, d_lut, R, d_counts, nullptr);
+  if (!rc && cudaMemcpy(counts.data(), d_counts, sizeof(int64_t) * cells,
+                        cudaMemcpyDeviceToHost) != cudaSuccess)
+    rc = ASGK_ERR_CUDA;
+  if (rc)
+  {
+    release();
+    return rc;
+  }
+  for (int r = 0; r < cells; r++)
+    row_ptr[r + 1] = row_ptr[r] + counts[r];
+  int64_t const nnz = row_ptr[cells];
+  std::unique_ptr<asgk_plan> pl(new (std::nothrow) asgk_plan());
+  if (!pl)
+  {
+    release();
+    return ASGK_ERR_ALLOC;
+  }
+  plan_data &p = pl->p;
+  // every pair carries its d connection indices (written by the fill)
+  if ((rc = alloc_plan(p, d, n, cells, cells, num_terms, nnz, index_mode::conn,
+                       vA_len, nnz * d)))
+  {
+    release();
+    return rc;
+  }
+  std::vector<int> order(cells);
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(),
+                   [&](int a, int b) { return counts[a] > counts[b]; });
+  if (cudaMemcpy(p.row_ptr, row_ptr.data(), sizeof(int64_t) * row_ptr.size(),
+                 cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(p.row_order, order.data(), sizeof(int) * order.size(),
+                 cudaMemcpyHostToDevice) != cudaSuccess)
+    rc = ASGK_ERR_CUDA;
+  if (!rc && nnz > 0)
+    rc = launch_fill_pairs(d, cells, d_oned, d_cand, d_lut, R, p.row_ptr, p.col,
+                           p.idx, nullptr);
+  if (!rc)
+    rc = upload_values(p, vA);
+  release();
+  if (rc)
+  {
+    free_plan(p);
+    return rc;
+  }
+  *plan = pl.release();
   return ASGK_OK;
 }
 

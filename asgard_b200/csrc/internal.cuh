@@ -154,6 +154,15 @@ struct direction_pairs
 int build_direction_pairs(int d, int level, int num_cells, const int *table,
                           direction_pairs &out);
 
+// grid_device.cu: connected cell pairs on the device.  oned: [cells][d] 1D
+// cell indices; cand: the candidate cells in the order each row's pairs are
+// written; lut: [R][R] 1D connection index or -1
+int launch_count_pairs(int d, int cells, const int *oned, const int *cand,
+                       const int *lut, int R, int64_t *counts, cudaStream_t s);
+int launch_fill_pairs(int d, int cells, const int *oned, const int *cand,
+                      const int *lut, int R, const int64_t *row_ptr, int *col,
+                      int *conn, cudaStream_t s);
+
 // jacobi.cu
 struct jacobi_data;
 // z = M v; with scale_state, v *= scale_state[1] in place first (the

@@ -119,6 +119,18 @@ class kronmult_matrix:
         return cls(h, d, n, num_rows, num_cols, num_terms)
 
     @classmethod
+    def from_grid(cls, d, n, level, num_terms, vA):
+        """The sparse grid of dimension d and this level with its connected
+        cell pairs found on the GPU (vA in the per-1D-connection layout):
+        the plan from_conn makes from the host-built pair list."""
+        vA = _host(vA, np.float64)
+        h = C.c_void_p()
+        check(lib.asgk_plan_create_grid(C.byref(h), d, n, level, num_terms,
+                                        vA.ctypes.data, len(vA)), "plan_create_grid")
+        cells = lib.asgk_sparse_grid(d, level, None)
+        return cls(h, d, n, cells, cells, num_terms)
+
+    @classmethod
     def from_global(cls, d, n, level, table, num_terms, vA):
         """Global Kronecker form of the sparse grid's operator: the element
         table (cells x 2d) and vA in the per-1D-connection layout.  Terms

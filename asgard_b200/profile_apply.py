@@ -29,6 +29,9 @@ def main():
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=1)
     ap.add_argument("--peak", action="store_true", help="also measure the FMA peak")
+    ap.add_argument("--device-build", action="store_true",
+                    help="connected pairs found on the GPU (from_grid) instead of "
+                         "by the host builder; mode pairs only")
     ap.add_argument("--mode", default="pairs", choices=["pairs", "global", "dense"],
                     help="connected-pair kronmult, the global Kronecker form, "
                          "or the dense form (every cell pair)")
@@ -38,8 +41,17 @@ def main():
     import asgard_b200 as ab
 
     t0 = time.perf_counter()
-    op = ab.SparseGridOperator(args.d, args.level, args.terms, kind=args.kind)
-    mat = op.kronmult_matrix(mode=args.mode)
+    if args.device_build:
+        from asgard_b200.operators import factor_values
+        from types import SimpleNamespace
+        vA = factor_values(args.d, args.level, args.terms, args.kind)
+        mat = ab.kronmult_matrix.from_grid(args.d, 3, args.level, args.terms, vA)
+        op = SimpleNamespace(rows=mat.num_rows, nnz=mat.num_pairs(),
+                             N=mat.output_size())
+    else:
+        op = ab.SparseGridOperator(args.d, args.level, args.terms, kind=args.kind)
+        mat = op.kronmult_matrix(mode=args.mode)
+    torch.cuda.synchronize()
     t_setup = time.perf_counter() - t0
     g = torch.Generator(device="cuda").manual_seed(0)
     x = torch.rand(op.N, dtype=torch.float64, device="cuda", generator=g) * 2 - 1

@@ -26,6 +26,9 @@ def main():
     ap.add_argument("--level", type=int, default=7)
     ap.add_argument("--terms", type=int, default=4)
     ap.add_argument("--dt", type=float, default=1e-3)
+    ap.add_argument("--device-build", action="store_true",
+                    help="connected pairs found on the GPU (from_grid) instead of "
+                         "by the host builder; mode pairs only")
     ap.add_argument("--mode", default="global", choices=["pairs", "global"])
     ap.add_argument("--precond", default="block", choices=["none", "point", "block"])
     ap.add_argument("--precision", default="fp32", choices=["fp64", "fp32"])
@@ -53,8 +56,15 @@ def main():
     if args.no_graphs:
         ab.lib.asgk_set_gmres_graphs(0)
     t0 = time.perf_counter()
-    op = ab.SparseGridOperator(args.d, args.level, args.terms)
-    mat = op.kronmult_matrix(mode=args.mode)
+    if args.device_build:
+        from asgard_b200.operators import factor_values
+        from types import SimpleNamespace
+        vA = factor_values(args.d, args.level, args.terms)
+        mat = ab.kronmult_matrix.from_grid(args.d, 3, args.level, args.terms, vA)
+        op = SimpleNamespace(N=mat.output_size())
+    else:
+        op = ab.SparseGridOperator(args.d, args.level, args.terms)
+        mat = op.kronmult_matrix(mode=args.mode)
     pc = None if args.precond == "none" else ab.JacobiPreconditioner(mat, args.dt, kind=args.precond)
     torch.cuda.synchronize()
     setup = time.perf_counter() - t0

@@ -91,6 +91,18 @@ int asgk_plan_create_conn(asgk_plan **plan, int d, int n, int num_rows,
                           const int *col_indx, const int *conn,
                           const double *vA, int64_t vA_len);
 
+/* The sparse-grid operator with its connected pairs found on the device:
+ * the element table of dimension d and level `level` (asgk_sparse_grid),
+ * every cell pair tested against the 1D connectivity (the reference's
+ * check_connected rule, src/asgard_kronmult_matrix.cpp:230-300, which
+ * make_kronmult_sparse applies on the host, :406-466) by a kernel, the pair
+ * list written straight into the plan.  vA in the per-1D-connection layout
+ * of asgk_plan_create_conn.  The same plan as asgk_build_pairs followed by
+ * asgk_plan_create_conn (the same pairs in the same order), without the
+ * host pass and the copy of the pair list. */
+int asgk_plan_create_grid(asgk_plan **plan, int d, int n, int level,
+                          int num_terms, const double *vA, int64_t vA_len);
+
 /* Dense form: replaces kronmult_matrix<P>'s dense constructor
  * (src/asgard_kronmult_matrix.hpp:132-176, filled by make_kronmult_dense,
  * src/asgard_kronmult_matrix.cpp:64-163) and kronmult::gpu_dense /

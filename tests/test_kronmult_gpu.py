@@ -318,3 +318,31 @@ def test_staged_kernel_alignment_and_status(cuda, d, L):
             # the input is left untouched
             assert torch.equal(xd.cpu(), torch.from_numpy(x))
     assert ab.lib.asgk_device_status(1) == 0
+
+
+@pytest.mark.parametrize("d,L,T", [(1, 6, 2), (2, 5, 2), (3, 5, 3), (4, 4, 4),
+                                   (5, 3, 3), (6, 3, 2), (4, 7, 4)])
+def test_device_built_pairs_match_host_built(cuda, d, L, T):
+    """asgk_plan_create_grid (connected pairs found on the GPU) makes the
+    plan the host builder makes: the same pairs in the same order, so the
+    applies agree bit for bit, FP64, FP32 and Euler."""
+    import asgard_b200 as ab
+    import torch
+    op = ab.SparseGridOperator(d, L, T, kind="advdiff")
+    mh = op.kronmult_matrix()
+    md = ab.kronmult_matrix.from_grid(d, 3, L, T, op.vA)
+    assert md.num_pairs() == mh.num_pairs() == op.nnz
+    assert md.num_rows == op.rows and md.output_size() == op.N
+    rng = np.random.default_rng(d)
+    x, y0 = to_dev(rng.uniform(-1, 1, op.N)), rng.uniform(-1, 1, op.N)
+    for prec in ("fp64", "fp32"):
+        ya, yb = to_dev(y0), to_dev(y0)
+        mh.apply(0.7, x, -1.3, ya, precision=prec)
+        md.apply(0.7, x, -1.3, yb, precision=prec)
+        torch.cuda.synchronize()
+        assert np.array_equal(ya.cpu().numpy(), yb.cpu().numpy()), prec
+    ya, yb = to_dev(y0), to_dev(y0)
+    mh.apply_euler(1e-3, -1.0, x, 0.5, ya)
+    md.apply_euler(1e-3, -1.0, x, 0.5, yb)
+    torch.cuda.synchronize()
+    assert np.array_equal(ya.cpu().numpy(), yb.cpu().numpy())
