@@ -1014,24 +1014,46 @@ int64_t asgk_launch_count(void) { return g_launches.load(); }
 
 int asgk_device_status(int reset)
 {
-  int code = ASGK_OK;
-  ASGK_CUDA(cudaDeviceSynchronize());
-  if (int rc = read_device_error(reset, &code))
-    return rc;
-  return code;
+  try
+  {
+    int code = ASGK_OK;
+    ASGK_CUDA(cudaDeviceSynchronize());
+    if (int rc = read_device_error(reset, &code))
+      return rc;
+    return code;
+  }
+  catch (std::bad_alloc const &)
+  {
+    return ASGK_ERR_ALLOC;
+  }
+  catch (...)
+  {
+    return ASGK_ERR_INVALID;
+  }
 }
 
 int asgk_device_info(int *sm_count, int *cc_major, int *cc_minor)
 {
-  int dev = 0;
-  ASGK_CUDA(cudaGetDevice(&dev));
-  if (sm_count)
-    ASGK_CUDA(cudaDeviceGetAttribute(sm_count, cudaDevAttrMultiProcessorCount, dev));
-  if (cc_major)
-    ASGK_CUDA(cudaDeviceGetAttribute(cc_major, cudaDevAttrComputeCapabilityMajor, dev));
-  if (cc_minor)
-    ASGK_CUDA(cudaDeviceGetAttribute(cc_minor, cudaDevAttrComputeCapabilityMinor, dev));
-  return ASGK_OK;
+  try
+  {
+    int dev = 0;
+    ASGK_CUDA(cudaGetDevice(&dev));
+    if (sm_count)
+      ASGK_CUDA(cudaDeviceGetAttribute(sm_count, cudaDevAttrMultiProcessorCount, dev));
+    if (cc_major)
+      ASGK_CUDA(cudaDeviceGetAttribute(cc_major, cudaDevAttrComputeCapabilityMajor, dev));
+    if (cc_minor)
+      ASGK_CUDA(cudaDeviceGetAttribute(cc_minor, cudaDevAttrComputeCapabilityMinor, dev));
+    return ASGK_OK;
+  }
+  catch (std::bad_alloc const &)
+  {
+    return ASGK_ERR_ALLOC;
+  }
+  catch (...)
+  {
+    return ASGK_ERR_INVALID;
+  }
 }
 
 int asgk_plan_create(asgk_plan **plan, int d, int n, int num_rows,
@@ -1039,11 +1061,22 @@ int asgk_plan_create(asgk_plan **plan, int d, int n, int num_rows,
                      const int *col_indx, const int *iA, const double *vA,
                      int64_t vA_len)
 {
-  if (row_ptr == nullptr || num_rows < 0)
+  try
+  {
+    if (row_ptr == nullptr || num_rows < 0)
+      return ASGK_ERR_INVALID;
+    std::vector<int64_t> rp(row_ptr, row_ptr + num_rows + 1);
+    return build_plan(plan, d, n, num_rows, num_cols, num_terms, rp, col_indx,
+                      iA, index_mode::expanded, vA, vA_len);
+  }
+  catch (std::bad_alloc const &)
+  {
+    return ASGK_ERR_ALLOC;
+  }
+  catch (...)
+  {
     return ASGK_ERR_INVALID;
-  std::vector<int64_t> rp(row_ptr, row_ptr + num_rows + 1);
-  return build_plan(plan, d, n, num_rows, num_cols, num_terms, rp, col_indx,
-                    iA, index_mode::expanded, vA, vA_len);
+  }
 }
 
 int asgk_plan_create_conn(asgk_plan **plan, int d, int n, int num_rows,
@@ -1051,11 +1084,22 @@ int asgk_plan_create_conn(asgk_plan **plan, int d, int n, int num_rows,
                           const int *col_indx, const int *conn,
                           const double *vA, int64_t vA_len)
 {
-  if (row_ptr == nullptr || num_rows < 0)
+  try
+  {
+    if (row_ptr == nullptr || num_rows < 0)
+      return ASGK_ERR_INVALID;
+    std::vector<int64_t> rp(row_ptr, row_ptr + num_rows + 1);
+    return build_plan(plan, d, n, num_rows, num_cols, num_terms, rp, col_indx,
+                      conn, index_mode::conn, vA, vA_len);
+  }
+  catch (std::bad_alloc const &)
+  {
+    return ASGK_ERR_ALLOC;
+  }
+  catch (...)
+  {
     return ASGK_ERR_INVALID;
-  std::vector<int64_t> rp(row_ptr, row_ptr + num_rows + 1);
-  return build_plan(plan, d, n, num_rows, num_cols, num_terms, rp, col_indx,
-                    conn, index_mode::conn, vA, vA_len);
+  }
 }
 
 int asgk_plan_create_pairs(asgk_plan **plan, int d, int n, int num_rows,
@@ -1063,36 +1107,47 @@ int asgk_plan_create_pairs(asgk_plan **plan, int d, int n, int num_rows,
                            const int *iy, const int *ix, const int *iA,
                            const double *vA, int64_t vA_len)
 {
-  if (plan == nullptr)
-    return ASGK_ERR_INVALID;
-  if (int rc = check_dims(d, n, num_rows, num_cols, num_terms))
-    return rc;
-  if (num_batch < 0 || (num_batch > 0 && (iy == nullptr || ix == nullptr)))
-    return ASGK_ERR_INVALID;
-  int64_t const ts = ipow(n, d);
-  std::vector<int64_t> rp(num_rows + 1, 0);
-  for (int64_t i = 0; i < num_batch; i++)
+  try
   {
-    if (iy[i] < 0 || iy[i] % ts != 0 || iy[i] / ts >= num_rows ||
-        ix[i] < 0 || ix[i] % ts != 0 || ix[i] / ts >= num_cols)
+    if (plan == nullptr)
       return ASGK_ERR_INVALID;
-    rp[iy[i] / ts + 1]++;
+    if (int rc = check_dims(d, n, num_rows, num_cols, num_terms))
+      return rc;
+    if (num_batch < 0 || (num_batch > 0 && (iy == nullptr || ix == nullptr)))
+      return ASGK_ERR_INVALID;
+    int64_t const ts = ipow(n, d);
+    std::vector<int64_t> rp(num_rows + 1, 0);
+    for (int64_t i = 0; i < num_batch; i++)
+    {
+      if (iy[i] < 0 || iy[i] % ts != 0 || iy[i] / ts >= num_rows ||
+          ix[i] < 0 || ix[i] % ts != 0 || ix[i] / ts >= num_cols)
+        return ASGK_ERR_INVALID;
+      rp[iy[i] / ts + 1]++;
+    }
+    for (int r = 0; r < num_rows; r++)
+      rp[r + 1] += rp[r];
+    std::vector<int64_t> fill(rp.begin(), rp.end() - 1);
+    std::vector<int> col(num_batch);
+    int64_t const per = int64_t(num_terms) * d;
+    std::vector<int> ia(num_batch * per);
+    for (int64_t i = 0; i < num_batch; i++)
+    {
+      int64_t const dst = fill[iy[i] / ts]++;
+      col[dst]          = int(ix[i] / ts);
+      if (per > 0)
+        std::copy_n(iA + i * per, per, ia.data() + dst * per);
+    }
+    return build_plan(plan, d, n, num_rows, num_cols, num_terms, rp, col.data(),
+                      ia.data(), index_mode::expanded, vA, vA_len);
   }
-  for (int r = 0; r < num_rows; r++)
-    rp[r + 1] += rp[r];
-  std::vector<int64_t> fill(rp.begin(), rp.end() - 1);
-  std::vector<int> col(num_batch);
-  int64_t const per = int64_t(num_terms) * d;
-  std::vector<int> ia(num_batch * per);
-  for (int64_t i = 0; i < num_batch; i++)
+  catch (std::bad_alloc const &)
   {
-    int64_t const dst = fill[iy[i] / ts]++;
-    col[dst]          = int(ix[i] / ts);
-    if (per > 0)
-      std::copy_n(iA + i * per, per, ia.data() + dst * per);
+    return ASGK_ERR_ALLOC;
   }
-  return build_plan(plan, d, n, num_rows, num_cols, num_terms, rp, col.data(),
-                    ia.data(), index_mode::expanded, vA, vA_len);
+  catch (...)
+  {
+    return ASGK_ERR_INVALID;
+  }
 }
 
 int asgk_plan_create_dense(asgk_plan **plan, int d, int n, int num_rows,
@@ -1101,208 +1156,241 @@ int asgk_plan_create_dense(asgk_plan **plan, int d, int n, int num_rows,
                            int64_t elem_len, int row_offset, int col_offset,
                            int num_1d_blocks)
 {
-  if (plan == nullptr)
-    return ASGK_ERR_INVALID;
-  *plan = nullptr;
-  if (int rc = check_dims(d, n, num_rows, num_cols, num_terms))
-    return rc;
-  if (row_offset < 0 || col_offset < 0)
-    return ASGK_ERR_INVALID;
-  int64_t const npairs = (num_terms > 0) ? int64_t(num_rows) * num_cols : 0;
-  int const nb         = (num_terms > 0) ? num_1d_blocks : 0;
-  if (num_terms > 0)
+  try
   {
-    if (terms == nullptr || num_1d_blocks < 1 ||
-        int64_t(num_1d_blocks) * num_1d_blocks > (int64_t(1) << 30))
+    if (plan == nullptr)
       return ASGK_ERR_INVALID;
-    for (int t = 0; t < num_terms; t++)
-      if (terms[t] == nullptr)
-        return ASGK_ERR_INVALID;
-  }
-  if (npairs > 0)
-  {
-    int64_t const need =
-        int64_t(d) * std::max(int64_t(row_offset) + num_rows,
-                              int64_t(col_offset) + num_cols);
-    if (elem == nullptr || elem_len < need)
+    *plan = nullptr;
+    if (int rc = check_dims(d, n, num_rows, num_cols, num_terms))
+      return rc;
+    if (row_offset < 0 || col_offset < 0)
       return ASGK_ERR_INVALID;
-    for (int64_t i = 0; i < need; i++)
-      if (elem[i] < 0 || elem[i] >= nb)
-        return ASGK_ERR_INVALID;
-  }
-  // every (row, col) pair, columns in order; per pair the d connections
-  // elem_col[k]*nb + elem_row[k]
-  std::vector<int64_t> rp(size_t(num_rows) + 1);
-  for (int r = 0; r <= num_rows; r++)
-    rp[r] = (npairs > 0) ? int64_t(r) * num_cols : 0;
-  std::vector<int> col(static_cast<size_t>(npairs));
-  std::vector<int> conn(static_cast<size_t>(npairs) * d);
-#pragma omp parallel for schedule(static)
-  for (int r = 0; r < (npairs > 0 ? num_rows : 0); r++)
-  {
-    const int *er = elem + int64_t(r + row_offset) * d;
-    for (int c = 0; c < num_cols; c++)
+    int64_t const npairs = (num_terms > 0) ? int64_t(num_rows) * num_cols : 0;
+    int const nb         = (num_terms > 0) ? num_1d_blocks : 0;
+    if (num_terms > 0)
     {
-      int64_t const p = int64_t(r) * num_cols + c;
-      const int *ec   = elem + int64_t(c + col_offset) * d;
-      col[p]          = c;
-      for (int k = 0; k < d; k++)
-        conn[p * d + k] = ec[k] * nb + er[k];
+      if (terms == nullptr || num_1d_blocks < 1 ||
+          int64_t(num_1d_blocks) * num_1d_blocks > (int64_t(1) << 30))
+        return ASGK_ERR_INVALID;
+      for (int t = 0; t < num_terms; t++)
+        if (terms[t] == nullptr)
+          return ASGK_ERR_INVALID;
     }
+    if (npairs > 0)
+    {
+      int64_t const need =
+          int64_t(d) * std::max(int64_t(row_offset) + num_rows,
+                                int64_t(col_offset) + num_cols);
+      if (elem == nullptr || elem_len < need)
+        return ASGK_ERR_INVALID;
+      for (int64_t i = 0; i < need; i++)
+        if (elem[i] < 0 || elem[i] >= nb)
+          return ASGK_ERR_INVALID;
+    }
+    // every (row, col) pair, columns in order; per pair the d connections
+    // elem_col[k]*nb + elem_row[k]
+    std::vector<int64_t> rp(size_t(num_rows) + 1);
+    for (int r = 0; r <= num_rows; r++)
+      rp[r] = (npairs > 0) ? int64_t(r) * num_cols : 0;
+    std::vector<int> col(static_cast<size_t>(npairs));
+    std::vector<int> conn(static_cast<size_t>(npairs) * d);
+  #pragma omp parallel for schedule(static)
+    for (int r = 0; r < (npairs > 0 ? num_rows : 0); r++)
+    {
+      const int *er = elem + int64_t(r + row_offset) * d;
+      for (int c = 0; c < num_cols; c++)
+      {
+        int64_t const p = int64_t(r) * num_cols + c;
+        const int *ec   = elem + int64_t(c + col_offset) * d;
+        col[p]          = c;
+        for (int k = 0; k < d; k++)
+          conn[p * d + k] = ec[k] * nb + er[k];
+      }
+    }
+    std::vector<double> vA;
+    if (num_terms > 0)
+      vA = dense_values(d, n, num_terms, nb, terms);
+    if (int rc = build_plan(plan, d, n, num_rows, num_cols, num_terms, rp,
+                            col.data(), conn.data(), index_mode::conn,
+                            vA.data(), int64_t(vA.size())))
+      return rc;
+    (*plan)->p.dense    = true;
+    (*plan)->p.dense_nb = nb;
+    return ASGK_OK;
   }
-  std::vector<double> vA;
-  if (num_terms > 0)
-    vA = dense_values(d, n, num_terms, nb, terms);
-  if (int rc = build_plan(plan, d, n, num_rows, num_cols, num_terms, rp,
-                          col.data(), conn.data(), index_mode::conn,
-                          vA.data(), int64_t(vA.size())))
-    return rc;
-  (*plan)->p.dense    = true;
-  (*plan)->p.dense_nb = nb;
-  return ASGK_OK;
+  catch (std::bad_alloc const &)
+  {
+    return ASGK_ERR_ALLOC;
+  }
+  catch (...)
+  {
+    return ASGK_ERR_INVALID;
+  }
 }
 
 int asgk_plan_set_workspace(asgk_plan *plan, double *x, int64_t x_len,
                             double *y, int64_t y_len)
 {
-  if (!plan || !x || !y)
-    return ASGK_ERR_INVALID;
-  auto &p = plan->p;
-  if (x_len < int64_t(p.cols) * p.tensor || y_len < int64_t(p.rows) * p.tensor)
-    return ASGK_ERR_INVALID;
-  if (p.ws_owned && p.xw)
+  try
   {
-    ASGK_CUDA(cudaDeviceSynchronize()); // an apply_host may still use them
-    cudaFree(p.xw);
-    cudaFree(p.yw);
-    p.device_bytes -= sizeof(double) * (std::max<int64_t>(int64_t(p.cols) * p.tensor, 1) +
-                                        std::max<int64_t>(int64_t(p.rows) * p.tensor, 1));
+    if (!plan || !x || !y)
+      return ASGK_ERR_INVALID;
+    auto &p = plan->p;
+    if (x_len < int64_t(p.cols) * p.tensor || y_len < int64_t(p.rows) * p.tensor)
+      return ASGK_ERR_INVALID;
+    if (p.ws_owned && p.xw)
+    {
+      ASGK_CUDA(cudaDeviceSynchronize()); // an apply_host may still use them
+      cudaFree(p.xw);
+      cudaFree(p.yw);
+      p.device_bytes -= sizeof(double) * (std::max<int64_t>(int64_t(p.cols) * p.tensor, 1) +
+                                          std::max<int64_t>(int64_t(p.rows) * p.tensor, 1));
+    }
+    p.xw       = x;
+    p.yw       = y;
+    p.ws_owned = false;
+    return ASGK_OK;
   }
-  p.xw       = x;
-  p.yw       = y;
-  p.ws_owned = false;
-  return ASGK_OK;
+  catch (std::bad_alloc const &)
+  {
+    return ASGK_ERR_ALLOC;
+  }
+  catch (...)
+  {
+    return ASGK_ERR_INVALID;
+  }
 }
 
 int asgk_plan_create_grid(asgk_plan **plan, int d, int n, int level,
                           int num_terms, const double *vA, int64_t vA_len)
 {
-  if (plan == nullptr)
-    return ASGK_ERR_INVALID;
-  *plan = nullptr;
-  if (d < 1 || d > 6 || level < 0 || level > 12 || num_terms < 0 ||
-      (num_terms > 0 && vA == nullptr))
-    return ASGK_ERR_INVALID;
-  if (int rc = check_dims(d, n, 0, 0, num_terms))
-    return rc;
-  int64_t const ncells = asgk_sparse_grid(d, level, nullptr);
-  if (ncells <= 0 || ncells > (int64_t(1) << 30))
-    return ASGK_ERR_UNSUPPORTED;
-  int const cells = int(ncells);
-  std::vector<int> table(size_t(cells) * 2 * d);
-  asgk_sparse_grid(d, level, table.data());
-  int R = 0, nconn = 0;
-  if (int rc = asgk_connect_1d(level, &R, &nconn, nullptr, nullptr))
-    return rc;
-  std::vector<int> pntr(R + 1), indx(nconn);
-  asgk_connect_1d(level, &R, &nconn, pntr.data(), indx.data());
-  int64_t const blk = int64_t(d) * num_terms * n * n;
-  if (vA_len != int64_t(nconn) * blk)
-    return ASGK_ERR_INVALID;
-  std::vector<int> lut(size_t(R) * R, -1), oned(size_t(cells) * d);
-  for (int r = 0; r < R; r++)
-    for (int j = pntr[r]; j < pntr[r + 1]; j++)
-      lut[size_t(r) * R + indx[j]] = j;
-  for (int c = 0; c < cells; c++)
-    for (int k = 0; k < d; k++)
+  try
+  {
+    if (plan == nullptr)
+      return ASGK_ERR_INVALID;
+    *plan = nullptr;
+    if (d < 1 || d > 6 || level < 0 || level > 12 || num_terms < 0 ||
+        (num_terms > 0 && vA == nullptr))
+      return ASGK_ERR_INVALID;
+    if (int rc = check_dims(d, n, 0, 0, num_terms))
+      return rc;
+    int64_t const ncells = asgk_sparse_grid(d, level, nullptr);
+    if (ncells <= 0 || ncells > (int64_t(1) << 30))
+      return ASGK_ERR_UNSUPPORTED;
+    int const cells = int(ncells);
+    std::vector<int> table(size_t(cells) * 2 * d);
+    asgk_sparse_grid(d, level, table.data());
+    int R = 0, nconn = 0;
+    if (int rc = asgk_connect_1d(level, &R, &nconn, nullptr, nullptr))
+      return rc;
+    std::vector<int> pntr(R + 1), indx(nconn);
+    asgk_connect_1d(level, &R, &nconn, pntr.data(), indx.data());
+    int64_t const blk = int64_t(d) * num_terms * n * n;
+    if (vA_len != int64_t(nconn) * blk)
+      return ASGK_ERR_INVALID;
+    std::vector<int> lut(size_t(R) * R, -1), oned(size_t(cells) * d);
+    for (int r = 0; r < R; r++)
+      for (int j = pntr[r]; j < pntr[r + 1]; j++)
+        lut[size_t(r) * R + indx[j]] = j;
+    for (int c = 0; c < cells; c++)
+      for (int k = 0; k < d; k++)
+      {
+        int const lv = table[size_t(c) * 2 * d + k], ps = table[size_t(c) * 2 * d + d + k];
+        oned[size_t(c) * d + k] = (lv == 0) ? 0 : (1 << (lv - 1)) + ps;
+      }
+    // candidates in the order each row's pairs are kept: the staged n = 3,
+    // d = 3/4 kernel wants them by factor blocks, last dimension slowest (the
+    // order build_plan sorts host lists into); table order otherwise
+    std::vector<int> cand(cells);
+    std::iota(cand.begin(), cand.end(), 0);
+    if (n == 3 && (d == 3 || d == 4) && num_terms > 0)
+      std::stable_sort(cand.begin(), cand.end(), [&](int a, int b) {
+        for (int k = d - 1; k >= 0; k--)
+          if (oned[size_t(a) * d + k] != oned[size_t(b) * d + k])
+            return oned[size_t(a) * d + k] < oned[size_t(b) * d + k];
+        return a < b;
+      });
+    int *d_oned = nullptr, *d_cand = nullptr, *d_lut = nullptr;
+    int64_t *d_counts = nullptr;
+    int64_t scratch   = 0;
+    auto release = [&]() {
+      cudaFree(d_oned);
+      cudaFree(d_cand);
+      cudaFree(d_lut);
+      cudaFree(d_counts);
+    };
+    int rc = ASGK_OK;
+    if ((rc = dev_alloc(&d_oned, int64_t(oned.size()), scratch)) ||
+        (rc = dev_alloc(&d_cand, cells, scratch)) ||
+        (rc = dev_alloc(&d_lut, int64_t(lut.size()), scratch)) ||
+        (rc = dev_alloc(&d_counts, cells, scratch)))
     {
-      int const lv = table[size_t(c) * 2 * d + k], ps = table[size_t(c) * 2 * d + d + k];
-      oned[size_t(c) * d + k] = (lv == 0) ? 0 : (1 << (lv - 1)) + ps;
+      release();
+      return rc;
     }
-  // candidates in the order each row's pairs are kept: the staged n = 3,
-  // d = 3/4 kernel wants them by factor blocks, last dimension slowest (the
-  // order build_plan sorts host lists into); table order otherwise
-  std::vector<int> cand(cells);
-  std::iota(cand.begin(), cand.end(), 0);
-  if (n == 3 && (d == 3 || d == 4) && num_terms > 0)
-    std::stable_sort(cand.begin(), cand.end(), [&](int a, int b) {
-      for (int k = d - 1; k >= 0; k--)
-        if (oned[size_t(a) * d + k] != oned[size_t(b) * d + k])
-          return oned[size_t(a) * d + k] < oned[size_t(b) * d + k];
-      return a < b;
-    });
-  int *d_oned = nullptr, *d_cand = nullptr, *d_lut = nullptr;
-  int64_t *d_counts = nullptr;
-  int64_t scratch   = 0;
-  auto release = [&]() {
-    cudaFree(d_oned);
-    cudaFree(d_cand);
-    cudaFree(d_lut);
-    cudaFree(d_counts);
-  };
-  int rc = ASGK_OK;
-  if ((rc = dev_alloc(&d_oned, int64_t(oned.size()), scratch)) ||
-      (rc = dev_alloc(&d_cand, cells, scratch)) ||
-      (rc = dev_alloc(&d_lut, int64_t(lut.size()), scratch)) ||
-      (rc = dev_alloc(&d_counts, cells, scratch)))
-  {
+    std::vector<int64_t> counts(cells), row_ptr(size_t(cells) + 1, 0);
+    if (cudaMemcpy(d_oned, oned.data(), sizeof(int) * oned.size(), cudaMemcpyHostToDevice) ||
+        cudaMemcpy(d_cand, cand.data(), sizeof(int) * cand.size(), cudaMemcpyHostToDevice) ||
+        cudaMemcpy(d_lut, lut.data(), sizeof(int) * lut.size(), cudaMemcpyHostToDevice))
+      rc = ASGK_ERR_CUDA;
+    if (!rc)
+      rc = launch_count_pairs(d, cells, d_oned, d_cand, d_lut, R, d_counts, nullptr);
+    if (!rc && cudaMemcpy(counts.data(), d_counts, sizeof(int64_t) * cells,
+                          cudaMemcpyDeviceToHost) != cudaSuccess)
+      rc = ASGK_ERR_CUDA;
+    if (rc)
+    {
+      release();
+      return rc;
+    }
+    for (int r = 0; r < cells; r++)
+      row_ptr[r + 1] = row_ptr[r] + counts[r];
+    int64_t const nnz = row_ptr[cells];
+    std::unique_ptr<asgk_plan> pl(new (std::nothrow) asgk_plan());
+    if (!pl)
+    {
+      release();
+      return ASGK_ERR_ALLOC;
+    }
+    plan_data &p = pl->p;
+    // every pair carries its d connection indices (written by the fill)
+    if ((rc = alloc_plan(p, d, n, cells, cells, num_terms, nnz, index_mode::conn,
+                         vA_len, nnz * d)))
+    {
+      release();
+      return rc;
+    }
+    std::vector<int> order(cells);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int a, int b) { return counts[a] > counts[b]; });
+    if (cudaMemcpy(p.row_ptr, row_ptr.data(), sizeof(int64_t) * row_ptr.size(),
+                   cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(p.row_order, order.data(), sizeof(int) * order.size(),
+                   cudaMemcpyHostToDevice) != cudaSuccess)
+      rc = ASGK_ERR_CUDA;
+    if (!rc && nnz > 0)
+      rc = launch_fill_pairs(d, cells, d_oned, d_cand, d_lut, R, p.row_ptr, p.col,
+                             p.idx, nullptr);
+    if (!rc)
+      rc = upload_values(p, vA);
     release();
-    return rc;
+    if (rc)
+    {
+      free_plan(p);
+      return rc;
+    }
+    *plan = pl.release();
+    return ASGK_OK;
   }
-  std::vector<int64_t> counts(cells), row_ptr(size_t(cells) + 1, 0);
-  if (cudaMemcpy(d_oned, oned.data(), sizeof(int) * oned.size(), cudaMemcpyHostToDevice) ||
-      cudaMemcpy(d_cand, cand.data(), sizeof(int) * cand.size(), cudaMemcpyHostToDevice) ||
-      cudaMemcpy(d_lut, lut.data(), sizeof(int) * lut.size(), cudaMemcpyHostToDevice))
-    rc = ASGK_ERR_CUDA;
-  if (!rc)
-    rc = launch_count_pairs(d, cells, d_oned, d_cand, d_lut, R, d_counts, nullptr);
-  if (!rc && cudaMemcpy(counts.data(), d_counts, sizeof(int64_t) * cells,
-                        cudaMemcpyDeviceToHost) != cudaSuccess)
-    rc = ASGK_ERR_CUDA;
-  if (rc)
+  catch (std::bad_alloc const &)
   {
-    release();
-    return rc;
-  }
-  for (int r = 0; r < cells; r++)
-    row_ptr[r + 1] = row_ptr[r] + counts[r];
-  int64_t const nnz = row_ptr[cells];
-  std::unique_ptr<asgk_plan> pl(new (std::nothrow) asgk_plan());
-  if (!pl)
-  {
-    release();
     return ASGK_ERR_ALLOC;
   }
-  plan_data &p = pl->p;
-  // every pair carries its d connection indices (written by the fill)
-  if ((rc = alloc_plan(p, d, n, cells, cells, num_terms, nnz, index_mode::conn,
-                       vA_len, nnz * d)))
+  catch (...)
   {
-    release();
-    return rc;
+    return ASGK_ERR_INVALID;
   }
-  std::vector<int> order(cells);
-  std::iota(order.begin(), order.end(), 0);
-  std::stable_sort(order.begin(), order.end(),
-                   [&](int a, int b) { return counts[a] > counts[b]; });
-  if (cudaMemcpy(p.row_ptr, row_ptr.data(), sizeof(int64_t) * row_ptr.size(),
-                 cudaMemcpyHostToDevice) != cudaSuccess ||
-      cudaMemcpy(p.row_order, order.data(), sizeof(int) * order.size(),
-                 cudaMemcpyHostToDevice) != cudaSuccess)
-    rc = ASGK_ERR_CUDA;
-  if (!rc && nnz > 0)
-    rc = launch_fill_pairs(d, cells, d_oned, d_cand, d_lut, R, p.row_ptr, p.col,
-                           p.idx, nullptr);
-  if (!rc)
-    rc = upload_values(p, vA);
-  release();
-  if (rc)
-  {
-    free_plan(p);
-    return rc;
-  }
-  *plan = pl.release();
-  return ASGK_OK;
 }
 
 int asgk_plan_kind(const asgk_plan *plan)
@@ -1315,17 +1403,28 @@ int asgk_plan_kind(const asgk_plan *plan)
 int asgk_plan_update_terms(asgk_plan *plan, const double *const *terms,
                            int num_terms)
 {
-  if (!plan || !plan->p.dense || num_terms != plan->p.terms ||
-      (num_terms > 0 && terms == nullptr))
-    return ASGK_ERR_INVALID;
-  for (int t = 0; t < num_terms; t++)
-    if (terms[t] == nullptr)
+  try
+  {
+    if (!plan || !plan->p.dense || num_terms != plan->p.terms ||
+        (num_terms > 0 && terms == nullptr))
       return ASGK_ERR_INVALID;
-  auto &p = plan->p;
-  if (num_terms == 0)
-    return ASGK_OK;
-  std::vector<double> vA = dense_values(p.d, p.n, p.terms, p.dense_nb, terms);
-  return upload_values(p, vA.data());
+    for (int t = 0; t < num_terms; t++)
+      if (terms[t] == nullptr)
+        return ASGK_ERR_INVALID;
+    auto &p = plan->p;
+    if (num_terms == 0)
+      return ASGK_OK;
+    std::vector<double> vA = dense_values(p.d, p.n, p.terms, p.dense_nb, terms);
+    return upload_values(p, vA.data());
+  }
+  catch (std::bad_alloc const &)
+  {
+    return ASGK_ERR_ALLOC;
+  }
+  catch (...)
+  {
+    return ASGK_ERR_INVALID;
+  }
 }
 
 void asgk_plan_destroy(asgk_plan *plan)
@@ -1339,440 +1438,539 @@ void asgk_plan_destroy(asgk_plan *plan)
 
 int asgk_plan_update_values(asgk_plan *plan, const double *vA, int64_t vA_len)
 {
-  if (!plan || plan->p.dense || vA_len != plan->p.vA_len || (vA_len > 0 && !vA))
-    return ASGK_ERR_INVALID;
-  auto &p = plan->p;
-  if (p.global)
+  try
   {
-    std::vector<double> B;
-    int n_identity = 0;
-    std::vector<std::vector<int>> multi;
-    if (int rc = global_blocks(p.d, p.terms, p.g_conn_row, p.g_conn_col, vA, B,
-                               n_identity, multi))
-      return rc;
-    // the chains are built for the dimensions each term acts in
-    if (multi != p.g_multi)
+    if (!plan || plan->p.dense || vA_len != plan->p.vA_len || (vA_len > 0 && !vA))
       return ASGK_ERR_INVALID;
-    if (int rc = upload_global_blocks(p, B))
-      return rc;
-    p.g_identity = n_identity;
+    auto &p = plan->p;
+    if (p.global)
+    {
+      std::vector<double> B;
+      int n_identity = 0;
+      std::vector<std::vector<int>> multi;
+      if (int rc = global_blocks(p.d, p.terms, p.g_conn_row, p.g_conn_col, vA, B,
+                                 n_identity, multi))
+        return rc;
+      // the chains are built for the dimensions each term acts in
+      if (multi != p.g_multi)
+        return ASGK_ERR_INVALID;
+      if (int rc = upload_global_blocks(p, B))
+        return rc;
+      p.g_identity = n_identity;
+    }
+    return upload_values(p, vA);
   }
-  return upload_values(p, vA);
+  catch (std::bad_alloc const &)
+  {
+    return ASGK_ERR_ALLOC;
+  }
+  catch (...)
+  {
+    return ASGK_ERR_INVALID;
+  }
 }
 
 int asgk_plan_create_global(asgk_plan **plan, int d, int n, int level,
                             int num_cells, const int *table, int num_terms,
                             const double *vA, int64_t vA_len)
 {
-  if (plan == nullptr)
-    return ASGK_ERR_INVALID;
-  *plan = nullptr;
-  if (n != 3)
-    return ASGK_ERR_UNSUPPORTED;
-  if (num_terms < 1 || vA == nullptr || table == nullptr || num_cells < 1)
-    return ASGK_ERR_INVALID;
-  direction_pairs dp;
-  if (int rc = build_direction_pairs(d, level, num_cells, table, dp))
-    return rc;
-  if (vA_len != int64_t(dp.nconn) * d * num_terms * 9)
-    return ASGK_ERR_INVALID;
-  std::vector<double> B;
-  int n_identity = 0;
-  std::vector<std::vector<int>> multi;
-  if (int rc = global_blocks(d, num_terms, dp.conn_row, dp.conn_col, vA, B,
-                             n_identity, multi))
-    return rc;
-  // entries of dimensions some term acts in
-  std::vector<char> used(d, 0);
-  for (int64_t j = 0; j < dp.nconn; j++)
-    for (int k = 0; k < d; k++)
-      for (int e = 0; e < 9; e++)
-        if (B[(j * d + k) * 10 + e] != 0.0)
-          used[k] = 1;
-  std::vector<int64_t> gptr(num_cells + 1, 0);
-  std::vector<int> gcol, gkb;
-  for (int r = 0; r < num_cells; r++)
+  try
   {
-    for (int64_t e = dp.ptr[r]; e < dp.ptr[r + 1]; e++)
-      if (used[dp.dim[e]])
-      {
-        gcol.push_back(dp.col[e]);
-        gkb.push_back(dp.conn[e] * d + dp.dim[e]);
-      }
-    gptr[r + 1] = int64_t(gcol.size());
-  }
-  // the diagonal pairs (one per cell) for the Jacobi preconditioners
-  std::vector<int64_t> rp(num_cells + 1);
-  std::vector<int> col(num_cells), conn(size_t(num_cells) * d);
-  for (int r = 0; r <= num_cells; r++)
-    rp[r] = r;
-  for (int r = 0; r < num_cells; r++)
-  {
-    col[r] = r;
-    for (int k = 0; k < d; k++)
-      conn[size_t(r) * d + k] = dp.self_conn[size_t(r) * d + k];
-  }
-  if (int rc = build_plan(plan, d, n, num_cells, num_cells, num_terms, rp,
-                          col.data(), conn.data(), index_mode::conn, vA, vA_len))
-    return rc;
-  auto &p = (*plan)->p;
-  p.global     = true;
-  p.gnnz       = int64_t(gcol.size());
-  p.g_identity = n_identity;
-  p.g_conn_row = dp.conn_row;
-  p.g_conn_col = dp.conn_col;
-  int64_t &bytes = p.device_bytes;
-  int rc = ASGK_OK;
-  if ((rc = dev_alloc(&p.gptr, num_cells + 1, bytes)) ||
-      (rc = dev_alloc(&p.gcol, std::max<int64_t>(p.gnnz, 1), bytes)) ||
-      (rc = dev_alloc(&p.gkb, std::max<int64_t>(p.gnnz, 1), bytes)) ||
-      (rc = dev_alloc(&p.gB64, int64_t(B.size()), bytes)) ||
-      (rc = dev_alloc(&p.gB32, int64_t(B.size() / 10 * 12), bytes)))
-  {
-    asgk_plan_destroy(*plan);
+    if (plan == nullptr)
+      return ASGK_ERR_INVALID;
     *plan = nullptr;
-    return rc;
-  }
-  auto up = [&](void *dst, const void *src, size_t b) -> int {
-    if (b == 0)
-      return ASGK_OK;
-    ASGK_CUDA(cudaMemcpy(dst, src, b, cudaMemcpyHostToDevice));
-    return ASGK_OK;
-  };
-  // cells with the most single-direction neighbours first (coarse cells
-  // reach every cell of a dimension: up to 2^level per dimension), each
-  // cell's list cut into slices of at most global_slice(d) entries
-  std::vector<int> order(num_cells);
-  std::iota(order.begin(), order.end(), 0);
-  std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
-    return (gptr[a + 1] - gptr[a]) > (gptr[b + 1] - gptr[b]);
-  });
-  std::vector<int> srow, slen, rs0(num_cells), rns(num_cells);
-  std::vector<int64_t> sbeg;
-  for (int r : order)
-  {
-    int64_t const e = gptr[r + 1] - gptr[r];
-    int const sz    = global_slice(d);
-    int const ns    = int(std::max<int64_t>(1, (e + sz - 1) / sz));
-    rs0[r] = int(srow.size());
-    rns[r] = ns;
-    for (int q = 0; q < ns; q++)
+    if (n != 3)
+      return ASGK_ERR_UNSUPPORTED;
+    if (num_terms < 1 || vA == nullptr || table == nullptr || num_cells < 1)
+      return ASGK_ERR_INVALID;
+    direction_pairs dp;
+    if (int rc = build_direction_pairs(d, level, num_cells, table, dp))
+      return rc;
+    if (vA_len != int64_t(dp.nconn) * d * num_terms * 9)
+      return ASGK_ERR_INVALID;
+    std::vector<double> B;
+    int n_identity = 0;
+    std::vector<std::vector<int>> multi;
+    if (int rc = global_blocks(d, num_terms, dp.conn_row, dp.conn_col, vA, B,
+                               n_identity, multi))
+      return rc;
+    // entries of dimensions some term acts in
+    std::vector<char> used(d, 0);
+    for (int64_t j = 0; j < dp.nconn; j++)
+      for (int k = 0; k < d; k++)
+        for (int e = 0; e < 9; e++)
+          if (B[(j * d + k) * 10 + e] != 0.0)
+            used[k] = 1;
+    std::vector<int64_t> gptr(num_cells + 1, 0);
+    std::vector<int> gcol, gkb;
+    for (int r = 0; r < num_cells; r++)
     {
-      srow.push_back(r);
-      sbeg.push_back(gptr[r] + int64_t(q) * sz);
-      slen.push_back(int(std::min<int64_t>(sz, e - int64_t(q) * sz)));
-    }
-  }
-  p.gslices = int(srow.size());
-  if ((rc = dev_alloc(&p.slice_row, p.gslices, bytes)) ||
-      (rc = dev_alloc(&p.slice_len, p.gslices, bytes)) ||
-      (rc = dev_alloc(&p.slice_beg, p.gslices, bytes)) ||
-      (rc = dev_alloc(&p.row_slice0, num_cells, bytes)) ||
-      (rc = dev_alloc(&p.row_nslice, num_cells, bytes)) ||
-      (rc = dev_alloc(&p.gscratch, int64_t(p.gslices) * p.tensor, bytes)) ||
-      (rc = dev_alloc(&p.gtickets, num_cells, bytes)))
-  {
-    asgk_plan_destroy(*plan);
-    *plan = nullptr;
-    return rc;
-  }
-  // chains of the terms acting in several dimensions
-  p.g_multi = multi;
-  if (!multi.empty())
-  {
-    std::vector<std::vector<std::pair<int, int>>> chains;
-    std::vector<int> chain_term;
-    for (auto const &m : multi)
-      for (auto &c : term_chains(std::vector<int>(m.begin() + 1, m.end())))
-      {
-        chains.push_back(c);
-        chain_term.push_back(m[0]);
-      }
-    p.gchains = int(chains.size());
-    int stages = 0;
-    for (auto const &c : chains)
-      stages = std::max(stages, int(c.size()));
-    // per-dimension neighbour lists (every entry of the direction pairs)
-    std::vector<int64_t> dptr(size_t(d) * (num_cells + 1), 0);
-    std::vector<int> dcol, dconn;
-    std::vector<unsigned char> drel;
-    std::vector<int64_t> per_dim(d, 0);
-    for (int k = 0; k < d; k++)
-    {
-      for (int r = 0; r < num_cells; r++)
-      {
-        for (int64_t e = dp.ptr[r]; e < dp.ptr[r + 1]; e++)
-          if (dp.dim[e] == k)
-          {
-            int const j = dp.conn[e];
-            dcol.push_back(dp.col[e]);
-            dconn.push_back(j);
-            drel.push_back(dp.conn_col[j] < dp.conn_row[j] ? 0 : (dp.conn_col[j] == dp.conn_row[j] ? 1 : 2));
-          }
-        dptr[size_t(k) * (num_cells + 1) + r + 1] = int64_t(dcol.size());
-      }
-      per_dim[k] = int64_t(dcol.size()) - dptr[size_t(k) * (num_cells + 1)];
-      if (k + 1 < d)
-        dptr[size_t(k + 1) * (num_cells + 1)] = int64_t(dcol.size());
-    }
-    std::vector<int4> jobs;
-    for (int s = 0; s < stages; s++)
-    {
-      p.stage_job0.push_back(int(jobs.size()));
-      for (int c = 0; c < p.gchains; c++)
-        if (int(chains[c].size()) > s)
+      for (int64_t e = dp.ptr[r]; e < dp.ptr[r + 1]; e++)
+        if (used[dp.dim[e]])
         {
-          jobs.push_back(make_int4(c, chains[c][s].first, chains[c][s].second, chain_term[c]));
-          p.gchain_entries += per_dim[chains[c][s].first];
+          gcol.push_back(dp.col[e]);
+          gkb.push_back(dp.conn[e] * d + dp.dim[e]);
         }
-      p.stage_njobs.push_back(int(jobs.size()) - p.stage_job0.back());
+      gptr[r + 1] = int64_t(gcol.size());
     }
-    std::vector<int> last(p.gchains);
-    for (int c = 0; c < p.gchains; c++)
-      last[c] = (int(chains[c].size()) - 1) % 2;
-    int64_t const N = int64_t(num_cells) * p.tensor;
-    if ((rc = dev_alloc(&p.gjobs, int64_t(jobs.size()), bytes)) ||
-        (rc = dev_alloc(&p.gchain_last, p.gchains, bytes)) ||
-        (rc = dev_alloc(&p.gd_ptr, int64_t(dptr.size()), bytes)) ||
-        (rc = dev_alloc(&p.gd_col, std::max<int64_t>(int64_t(dcol.size()), 1), bytes)) ||
-        (rc = dev_alloc(&p.gd_conn, std::max<int64_t>(int64_t(dconn.size()), 1), bytes)) ||
-        (rc = dev_alloc(&p.gd_rel, std::max<int64_t>(int64_t(drel.size()), 1), bytes)) ||
-        (rc = dev_alloc(&p.gwork, 2 * int64_t(p.gchains) * N, bytes)) ||
-        (rc = up(p.gjobs, jobs.data(), sizeof(int4) * jobs.size())) ||
-        (rc = up(p.gchain_last, last.data(), sizeof(int) * last.size())) ||
-        (rc = up(p.gd_ptr, dptr.data(), sizeof(int64_t) * dptr.size())) ||
-        (rc = up(p.gd_col, dcol.data(), sizeof(int) * dcol.size())) ||
-        (rc = up(p.gd_conn, dconn.data(), sizeof(int) * dconn.size())) ||
-        (rc = up(p.gd_rel, drel.data(), drel.size())))
+    // the diagonal pairs (one per cell) for the Jacobi preconditioners
+    std::vector<int64_t> rp(num_cells + 1);
+    std::vector<int> col(num_cells), conn(size_t(num_cells) * d);
+    for (int r = 0; r <= num_cells; r++)
+      rp[r] = r;
+    for (int r = 0; r < num_cells; r++)
+    {
+      col[r] = r;
+      for (int k = 0; k < d; k++)
+        conn[size_t(r) * d + k] = dp.self_conn[size_t(r) * d + k];
+    }
+    if (int rc = build_plan(plan, d, n, num_cells, num_cells, num_terms, rp,
+                            col.data(), conn.data(), index_mode::conn, vA, vA_len))
+      return rc;
+    auto &p = (*plan)->p;
+    p.global     = true;
+    p.gnnz       = int64_t(gcol.size());
+    p.g_identity = n_identity;
+    p.g_conn_row = dp.conn_row;
+    p.g_conn_col = dp.conn_col;
+    int64_t &bytes = p.device_bytes;
+    int rc = ASGK_OK;
+    if ((rc = dev_alloc(&p.gptr, num_cells + 1, bytes)) ||
+        (rc = dev_alloc(&p.gcol, std::max<int64_t>(p.gnnz, 1), bytes)) ||
+        (rc = dev_alloc(&p.gkb, std::max<int64_t>(p.gnnz, 1), bytes)) ||
+        (rc = dev_alloc(&p.gB64, int64_t(B.size()), bytes)) ||
+        (rc = dev_alloc(&p.gB32, int64_t(B.size() / 10 * 12), bytes)))
     {
       asgk_plan_destroy(*plan);
       *plan = nullptr;
       return rc;
     }
+    auto up = [&](void *dst, const void *src, size_t b) -> int {
+      if (b == 0)
+        return ASGK_OK;
+      ASGK_CUDA(cudaMemcpy(dst, src, b, cudaMemcpyHostToDevice));
+      return ASGK_OK;
+    };
+    // cells with the most single-direction neighbours first (coarse cells
+    // reach every cell of a dimension: up to 2^level per dimension), each
+    // cell's list cut into slices of at most global_slice(d) entries
+    std::vector<int> order(num_cells);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+      return (gptr[a + 1] - gptr[a]) > (gptr[b + 1] - gptr[b]);
+    });
+    std::vector<int> srow, slen, rs0(num_cells), rns(num_cells);
+    std::vector<int64_t> sbeg;
+    for (int r : order)
+    {
+      int64_t const e = gptr[r + 1] - gptr[r];
+      int const sz    = global_slice(d);
+      int const ns    = int(std::max<int64_t>(1, (e + sz - 1) / sz));
+      rs0[r] = int(srow.size());
+      rns[r] = ns;
+      for (int q = 0; q < ns; q++)
+      {
+        srow.push_back(r);
+        sbeg.push_back(gptr[r] + int64_t(q) * sz);
+        slen.push_back(int(std::min<int64_t>(sz, e - int64_t(q) * sz)));
+      }
+    }
+    p.gslices = int(srow.size());
+    if ((rc = dev_alloc(&p.slice_row, p.gslices, bytes)) ||
+        (rc = dev_alloc(&p.slice_len, p.gslices, bytes)) ||
+        (rc = dev_alloc(&p.slice_beg, p.gslices, bytes)) ||
+        (rc = dev_alloc(&p.row_slice0, num_cells, bytes)) ||
+        (rc = dev_alloc(&p.row_nslice, num_cells, bytes)) ||
+        (rc = dev_alloc(&p.gscratch, int64_t(p.gslices) * p.tensor, bytes)) ||
+        (rc = dev_alloc(&p.gtickets, num_cells, bytes)))
+    {
+      asgk_plan_destroy(*plan);
+      *plan = nullptr;
+      return rc;
+    }
+    // chains of the terms acting in several dimensions
+    p.g_multi = multi;
+    if (!multi.empty())
+    {
+      std::vector<std::vector<std::pair<int, int>>> chains;
+      std::vector<int> chain_term;
+      for (auto const &m : multi)
+        for (auto &c : term_chains(std::vector<int>(m.begin() + 1, m.end())))
+        {
+          chains.push_back(c);
+          chain_term.push_back(m[0]);
+        }
+      p.gchains = int(chains.size());
+      int stages = 0;
+      for (auto const &c : chains)
+        stages = std::max(stages, int(c.size()));
+      // per-dimension neighbour lists (every entry of the direction pairs)
+      std::vector<int64_t> dptr(size_t(d) * (num_cells + 1), 0);
+      std::vector<int> dcol, dconn;
+      std::vector<unsigned char> drel;
+      std::vector<int64_t> per_dim(d, 0);
+      for (int k = 0; k < d; k++)
+      {
+        for (int r = 0; r < num_cells; r++)
+        {
+          for (int64_t e = dp.ptr[r]; e < dp.ptr[r + 1]; e++)
+            if (dp.dim[e] == k)
+            {
+              int const j = dp.conn[e];
+              dcol.push_back(dp.col[e]);
+              dconn.push_back(j);
+              drel.push_back(dp.conn_col[j] < dp.conn_row[j] ? 0 : (dp.conn_col[j] == dp.conn_row[j] ? 1 : 2));
+            }
+          dptr[size_t(k) * (num_cells + 1) + r + 1] = int64_t(dcol.size());
+        }
+        per_dim[k] = int64_t(dcol.size()) - dptr[size_t(k) * (num_cells + 1)];
+        if (k + 1 < d)
+          dptr[size_t(k + 1) * (num_cells + 1)] = int64_t(dcol.size());
+      }
+      std::vector<int4> jobs;
+      for (int s = 0; s < stages; s++)
+      {
+        p.stage_job0.push_back(int(jobs.size()));
+        for (int c = 0; c < p.gchains; c++)
+          if (int(chains[c].size()) > s)
+          {
+            jobs.push_back(make_int4(c, chains[c][s].first, chains[c][s].second, chain_term[c]));
+            p.gchain_entries += per_dim[chains[c][s].first];
+          }
+        p.stage_njobs.push_back(int(jobs.size()) - p.stage_job0.back());
+      }
+      std::vector<int> last(p.gchains);
+      for (int c = 0; c < p.gchains; c++)
+        last[c] = (int(chains[c].size()) - 1) % 2;
+      int64_t const N = int64_t(num_cells) * p.tensor;
+      if ((rc = dev_alloc(&p.gjobs, int64_t(jobs.size()), bytes)) ||
+          (rc = dev_alloc(&p.gchain_last, p.gchains, bytes)) ||
+          (rc = dev_alloc(&p.gd_ptr, int64_t(dptr.size()), bytes)) ||
+          (rc = dev_alloc(&p.gd_col, std::max<int64_t>(int64_t(dcol.size()), 1), bytes)) ||
+          (rc = dev_alloc(&p.gd_conn, std::max<int64_t>(int64_t(dconn.size()), 1), bytes)) ||
+          (rc = dev_alloc(&p.gd_rel, std::max<int64_t>(int64_t(drel.size()), 1), bytes)) ||
+          (rc = dev_alloc(&p.gwork, 2 * int64_t(p.gchains) * N, bytes)) ||
+          (rc = up(p.gjobs, jobs.data(), sizeof(int4) * jobs.size())) ||
+          (rc = up(p.gchain_last, last.data(), sizeof(int) * last.size())) ||
+          (rc = up(p.gd_ptr, dptr.data(), sizeof(int64_t) * dptr.size())) ||
+          (rc = up(p.gd_col, dcol.data(), sizeof(int) * dcol.size())) ||
+          (rc = up(p.gd_conn, dconn.data(), sizeof(int) * dconn.size())) ||
+          (rc = up(p.gd_rel, drel.data(), drel.size())))
+      {
+        asgk_plan_destroy(*plan);
+        *plan = nullptr;
+        return rc;
+      }
+    }
+    std::vector<unsigned> zeros(num_cells, 0u);
+    if ((rc = up(p.row_order, order.data(), sizeof(int) * order.size())) ||
+        (rc = up(p.slice_row, srow.data(), sizeof(int) * srow.size())) ||
+        (rc = up(p.slice_len, slen.data(), sizeof(int) * slen.size())) ||
+        (rc = up(p.slice_beg, sbeg.data(), sizeof(int64_t) * sbeg.size())) ||
+        (rc = up(p.row_slice0, rs0.data(), sizeof(int) * rs0.size())) ||
+        (rc = up(p.row_nslice, rns.data(), sizeof(int) * rns.size())) ||
+        (rc = up(p.gtickets, zeros.data(), sizeof(unsigned) * zeros.size())) ||
+        (rc = up(p.gptr, gptr.data(), sizeof(int64_t) * gptr.size())) ||
+        (rc = up(p.gcol, gcol.data(), sizeof(int) * gcol.size())) ||
+        (rc = up(p.gkb, gkb.data(), sizeof(int) * gkb.size())) ||
+        (rc = upload_global_blocks(p, B)))
+    {
+      asgk_plan_destroy(*plan);
+      *plan = nullptr;
+      return rc;
+    }
+    return ASGK_OK;
   }
-  std::vector<unsigned> zeros(num_cells, 0u);
-  if ((rc = up(p.row_order, order.data(), sizeof(int) * order.size())) ||
-      (rc = up(p.slice_row, srow.data(), sizeof(int) * srow.size())) ||
-      (rc = up(p.slice_len, slen.data(), sizeof(int) * slen.size())) ||
-      (rc = up(p.slice_beg, sbeg.data(), sizeof(int64_t) * sbeg.size())) ||
-      (rc = up(p.row_slice0, rs0.data(), sizeof(int) * rs0.size())) ||
-      (rc = up(p.row_nslice, rns.data(), sizeof(int) * rns.size())) ||
-      (rc = up(p.gtickets, zeros.data(), sizeof(unsigned) * zeros.size())) ||
-      (rc = up(p.gptr, gptr.data(), sizeof(int64_t) * gptr.size())) ||
-      (rc = up(p.gcol, gcol.data(), sizeof(int) * gcol.size())) ||
-      (rc = up(p.gkb, gkb.data(), sizeof(int) * gkb.size())) ||
-      (rc = upload_global_blocks(p, B)))
+  catch (std::bad_alloc const &)
   {
-    asgk_plan_destroy(*plan);
-    *plan = nullptr;
-    return rc;
+    return ASGK_ERR_ALLOC;
   }
-  return ASGK_OK;
+  catch (...)
+  {
+    return ASGK_ERR_INVALID;
+  }
 }
 
 int asgk_plan_info(const asgk_plan *plan, int64_t *num_batch,
                    int64_t *input_size, int64_t *output_size, int64_t *flops,
                    int64_t *device_bytes)
 {
-  if (!plan)
+  try
+  {
+    if (!plan)
+      return ASGK_ERR_INVALID;
+    auto const &p = plan->p;
+    if (num_batch)
+      *num_batch = p.global ? p.gnnz + p.gchain_entries : p.nnz;
+    if (input_size)
+      *input_size = int64_t(p.cols) * p.tensor;
+    if (output_size)
+      *output_size = int64_t(p.rows) * p.tensor;
+    // global mode: one contraction in one dimension per entry
+    if (flops)
+      *flops = p.global ? int64_t(p.tensor) * p.n * (p.gnnz + p.gchain_entries) * 2
+                        : int64_t(p.tensor) * p.n * p.d * p.terms * p.nnz * 2;
+    if (device_bytes)
+      *device_bytes = p.device_bytes;
+    return ASGK_OK;
+  }
+  catch (std::bad_alloc const &)
+  {
+    return ASGK_ERR_ALLOC;
+  }
+  catch (...)
+  {
     return ASGK_ERR_INVALID;
-  auto const &p = plan->p;
-  if (num_batch)
-    *num_batch = p.global ? p.gnnz + p.gchain_entries : p.nnz;
-  if (input_size)
-    *input_size = int64_t(p.cols) * p.tensor;
-  if (output_size)
-    *output_size = int64_t(p.rows) * p.tensor;
-  // global mode: one contraction in one dimension per entry
-  if (flops)
-    *flops = p.global ? int64_t(p.tensor) * p.n * (p.gnnz + p.gchain_entries) * 2
-                      : int64_t(p.tensor) * p.n * p.d * p.terms * p.nnz * 2;
-  if (device_bytes)
-    *device_bytes = p.device_bytes;
-  return ASGK_OK;
+  }
 }
 
 int asgk_apply(asgk_plan *plan, int precision, double alpha, const double *x,
                double beta, double *y, asgk_stream stream)
 {
-  if (!plan || !x || !y)
-    return ASGK_ERR_INVALID;
-  auto &p = plan->p;
-  cudaStream_t s = as_stream(stream);
-  if (p.terms == 0 || p.nnz == 0 || alpha == 0.0)
+  try
   {
-    // only the scaling of y remains (src/asgard_kronmult_matrix.hpp:344-349)
-    int64_t const ny = int64_t(p.rows) * p.tensor;
-    if (beta == 0.0)
-      return launch_fill(y, ny, 0.0, s);
-    if (beta != 1.0)
-      return launch_scale(y, ny, beta, s);
-    return ASGK_OK;
+    if (!plan || !x || !y)
+      return ASGK_ERR_INVALID;
+    auto &p = plan->p;
+    cudaStream_t s = as_stream(stream);
+    if (p.terms == 0 || p.nnz == 0 || alpha == 0.0)
+    {
+      // only the scaling of y remains (src/asgard_kronmult_matrix.hpp:344-349)
+      int64_t const ny = int64_t(p.rows) * p.tensor;
+      if (beta == 0.0)
+        return launch_fill(y, ny, 0.0, s);
+      if (beta != 1.0)
+        return launch_scale(y, ny, beta, s);
+      return ASGK_OK;
+    }
+    return launch_apply(p, precision, alpha, x, 0, beta, y, 0, 0.0, s);
   }
-  return launch_apply(p, precision, alpha, x, 0, beta, y, 0, 0.0, s);
+  catch (std::bad_alloc const &)
+  {
+    return ASGK_ERR_ALLOC;
+  }
+  catch (...)
+  {
+    return ASGK_ERR_INVALID;
+  }
 }
 
 int asgk_apply_f32(asgk_plan *plan, float alpha, const float *x, float beta,
                    float *y, asgk_stream stream)
 {
-  if (!plan || !x || !y)
+  try
+  {
+    if (!plan || !x || !y)
+      return ASGK_ERR_INVALID;
+    auto &p = plan->p;
+    if (p.terms == 0 || p.nnz == 0)
+      return ASGK_ERR_UNSUPPORTED;
+    return launch_apply(p, ASGK_FP32, alpha, x, 1, beta, y, 1, 0.0,
+                        as_stream(stream));
+  }
+  catch (std::bad_alloc const &)
+  {
+    return ASGK_ERR_ALLOC;
+  }
+  catch (...)
+  {
     return ASGK_ERR_INVALID;
-  auto &p = plan->p;
-  if (p.terms == 0 || p.nnz == 0)
-    return ASGK_ERR_UNSUPPORTED;
-  return launch_apply(p, ASGK_FP32, alpha, x, 1, beta, y, 1, 0.0,
-                      as_stream(stream));
+  }
 }
 
 int asgk_apply_host(asgk_plan *plan, double alpha, const double *x,
                     double beta, double *y, asgk_stream stream)
 {
-  if (!plan || !x || !y)
-    return ASGK_ERR_INVALID;
-  auto &p          = plan->p;
-  cudaStream_t s   = as_stream(stream);
-  int64_t const nx = int64_t(p.cols) * p.tensor;
-  int64_t const ny = int64_t(p.rows) * p.tensor;
-  if (p.xw == nullptr)
+  try
   {
-    int rc = ASGK_OK;
-    if ((rc = dev_alloc(&p.xw, std::max<int64_t>(nx, 1), p.device_bytes)) ||
-        (rc = dev_alloc(&p.yw, std::max<int64_t>(ny, 1), p.device_bytes)))
+    if (!plan || !x || !y)
+      return ASGK_ERR_INVALID;
+    auto &p          = plan->p;
+    cudaStream_t s   = as_stream(stream);
+    int64_t const nx = int64_t(p.cols) * p.tensor;
+    int64_t const ny = int64_t(p.rows) * p.tensor;
+    if (p.xw == nullptr)
     {
-      cudaFree(p.xw);
-      p.xw = nullptr;
-      return rc;
+      int rc = ASGK_OK;
+      if ((rc = dev_alloc(&p.xw, std::max<int64_t>(nx, 1), p.device_bytes)) ||
+          (rc = dev_alloc(&p.yw, std::max<int64_t>(ny, 1), p.device_bytes)))
+      {
+        cudaFree(p.xw);
+        p.xw = nullptr;
+        return rc;
+      }
+      p.ws_owned = true;
     }
-    p.ws_owned = true;
-  }
-  ASGK_CUDA(cudaMemcpyAsync(p.xw, x, sizeof(double) * nx,
-                            cudaMemcpyHostToDevice, s));
-  if (beta != 0.0)
-    ASGK_CUDA(cudaMemcpyAsync(p.yw, y, sizeof(double) * ny,
+    ASGK_CUDA(cudaMemcpyAsync(p.xw, x, sizeof(double) * nx,
                               cudaMemcpyHostToDevice, s));
-  if (int rc = asgk_apply(plan, ASGK_FP64, alpha, p.xw, beta, p.yw, stream))
-    return rc;
-  ASGK_CUDA(cudaMemcpyAsync(y, p.yw, sizeof(double) * ny,
-                            cudaMemcpyDeviceToHost, s));
-  ASGK_CUDA(cudaStreamSynchronize(s));
-  return ASGK_OK;
+    if (beta != 0.0)
+      ASGK_CUDA(cudaMemcpyAsync(p.yw, y, sizeof(double) * ny,
+                                cudaMemcpyHostToDevice, s));
+    if (int rc = asgk_apply(plan, ASGK_FP64, alpha, p.xw, beta, p.yw, stream))
+      return rc;
+    ASGK_CUDA(cudaMemcpyAsync(y, p.yw, sizeof(double) * ny,
+                              cudaMemcpyDeviceToHost, s));
+    ASGK_CUDA(cudaStreamSynchronize(s));
+    return ASGK_OK;
+  }
+  catch (std::bad_alloc const &)
+  {
+    return ASGK_ERR_ALLOC;
+  }
+  catch (...)
+  {
+    return ASGK_ERR_INVALID;
+  }
 }
 
 int asgk_apply_euler(asgk_plan *plan, int precision, double dt, double alpha,
                      const double *x, double beta, double *y,
                      asgk_stream stream)
 {
-  if (!plan || !x || !y)
-    return ASGK_ERR_INVALID;
-  auto &p = plan->p;
-  if (p.rows != p.cols)
-    return ASGK_ERR_INVALID;
-  cudaStream_t s = as_stream(stream);
-  if (p.terms == 0 || p.nnz == 0 || dt == 0.0)
+  try
   {
-    int64_t const ny = int64_t(p.rows) * p.tensor;
-    if (beta == 0.0)
+    if (!plan || !x || !y)
+      return ASGK_ERR_INVALID;
+    auto &p = plan->p;
+    if (p.rows != p.cols)
+      return ASGK_ERR_INVALID;
+    cudaStream_t s = as_stream(stream);
+    if (p.terms == 0 || p.nnz == 0 || dt == 0.0)
     {
-      if (int rc = launch_copy(y, x, ny, s))
+      int64_t const ny = int64_t(p.rows) * p.tensor;
+      if (beta == 0.0)
+      {
+        if (int rc = launch_copy(y, x, ny, s))
+          return rc;
+        return launch_scale(y, ny, alpha, s);
+      }
+      if (int rc = launch_scale(y, ny, beta, s))
         return rc;
-      return launch_scale(y, ny, alpha, s);
+      return launch_axpy(y, x, ny, alpha, s);
     }
-    if (int rc = launch_scale(y, ny, beta, s))
-      return rc;
-    return launch_axpy(y, x, ny, alpha, s);
+    return launch_apply(p, precision, -dt * alpha, x, 0, beta, y, 0, alpha, s);
   }
-  return launch_apply(p, precision, -dt * alpha, x, 0, beta, y, 0, alpha, s);
+  catch (std::bad_alloc const &)
+  {
+    return ASGK_ERR_ALLOC;
+  }
+  catch (...)
+  {
+    return ASGK_ERR_INVALID;
+  }
 }
 
 int asgk_gmres_dense(int n, const double *A, double *x, const double *b,
                      int restart, int max_outer, double tol,
                      asgk_gmres_info *info)
 {
-  if (n <= 0 || !A || !x || !b)
-    return ASGK_ERR_INVALID;
-  if (restart <= 0)
-    restart = asgk_default_gmres_restarts(n);
-  if (restart > n)
-    return ASGK_ERR_INVALID;
-  if (max_outer <= 0)
-    max_outer = n;
-  if (!(tol > 0))
-    tol = 1e-12;
-  double *dA = nullptr, *dx = nullptr, *db = nullptr;
-  int64_t bytes = 0;
-  int rc;
-  if ((rc = dev_alloc(&dA, int64_t(n) * n, bytes)) ||
-      (rc = dev_alloc(&dx, n, bytes)) || (rc = dev_alloc(&db, n, bytes)))
+  try
   {
+    if (n <= 0 || !A || !x || !b)
+      return ASGK_ERR_INVALID;
+    if (restart <= 0)
+      restart = asgk_default_gmres_restarts(n);
+    if (restart > n)
+      return ASGK_ERR_INVALID;
+    if (max_outer <= 0)
+      max_outer = n;
+    if (!(tol > 0))
+      tol = 1e-12;
+    double *dA = nullptr, *dx = nullptr, *db = nullptr;
+    int64_t bytes = 0;
+    int rc;
+    if ((rc = dev_alloc(&dA, int64_t(n) * n, bytes)) ||
+        (rc = dev_alloc(&dx, n, bytes)) || (rc = dev_alloc(&db, n, bytes)))
+    {
+      cudaFree(dA);
+      cudaFree(dx);
+      return rc;
+    }
+    cudaStream_t s = nullptr;
+    gmres_ws ws;
+    core_stats st;
+    auto mat = [&](double a, const double *xin, double bb, double *yout,
+                   cudaStream_t ss) -> int {
+      k_dense_gemv<<<(n + 3) / 4, 128, 0, ss>>>(n, dA, a, xin, bb, yout);
+      ASGK_LAUNCHED();
+      return ASGK_OK;
+    };
+    rc = ASGK_OK;
+    if (cudaMemcpy(dA, A, sizeof(double) * n * int64_t(n), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(dx, x, sizeof(double) * n, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(db, b, sizeof(double) * n, cudaMemcpyHostToDevice) != cudaSuccess)
+      rc = ASGK_ERR_CUDA;
+    if (rc == ASGK_OK)
+      rc = gmres_core(ws, n, mat, nullptr, dx, db, restart, max_outer, tol, st, s);
+    if (rc == ASGK_OK &&
+        cudaMemcpy(x, dx, sizeof(double) * n, cudaMemcpyDeviceToHost) != cudaSuccess)
+      rc = ASGK_ERR_CUDA;
     cudaFree(dA);
     cudaFree(dx);
+    cudaFree(db);
+    if (rc == ASGK_OK && info)
+    {
+      *info              = asgk_gmres_info{};
+      info->error        = st.err;
+      info->iterations   = st.total;
+      info->status       = st.status;
+      info->outer_steps  = st.restarts;
+      info->matvecs_fp64 = st.matvecs;
+    }
     return rc;
   }
-  cudaStream_t s = nullptr;
-  gmres_ws ws;
-  core_stats st;
-  auto mat = [&](double a, const double *xin, double bb, double *yout,
-                 cudaStream_t ss) -> int {
-    k_dense_gemv<<<(n + 3) / 4, 128, 0, ss>>>(n, dA, a, xin, bb, yout);
-    ASGK_LAUNCHED();
-    return ASGK_OK;
-  };
-  rc = ASGK_OK;
-  if (cudaMemcpy(dA, A, sizeof(double) * n * int64_t(n), cudaMemcpyHostToDevice) != cudaSuccess ||
-      cudaMemcpy(dx, x, sizeof(double) * n, cudaMemcpyHostToDevice) != cudaSuccess ||
-      cudaMemcpy(db, b, sizeof(double) * n, cudaMemcpyHostToDevice) != cudaSuccess)
-    rc = ASGK_ERR_CUDA;
-  if (rc == ASGK_OK)
-    rc = gmres_core(ws, n, mat, nullptr, dx, db, restart, max_outer, tol, st, s);
-  if (rc == ASGK_OK &&
-      cudaMemcpy(x, dx, sizeof(double) * n, cudaMemcpyDeviceToHost) != cudaSuccess)
-    rc = ASGK_ERR_CUDA;
-  cudaFree(dA);
-  cudaFree(dx);
-  cudaFree(db);
-  if (rc == ASGK_OK && info)
+  catch (std::bad_alloc const &)
   {
-    *info              = asgk_gmres_info{};
-    info->error        = st.err;
-    info->iterations   = st.total;
-    info->status       = st.status;
-    info->outer_steps  = st.restarts;
-    info->matvecs_fp64 = st.matvecs;
+    return ASGK_ERR_ALLOC;
   }
-  return rc;
+  catch (...)
+  {
+    return ASGK_ERR_INVALID;
+  }
 }
 
 int asgk_cgs_step(const double *V, int64_t ldv, int k, double *w, int64_t n,
                   double *h, double *norm, asgk_stream stream)
 {
-  if (!V || !w || !h || !norm || k < 1 || n < 1 || ldv < n)
+  try
+  {
+    if (!V || !w || !h || !norm || k < 1 || n < 1 || ldv < n)
+      return ASGK_ERR_INVALID;
+    cudaStream_t s   = as_stream(stream);
+    int const blocks = max_reduction_blocks();
+    double *part     = nullptr;
+    size_t const cnt = size_t(blocks) * (k + 1) + 1;
+    ASGK_CUDA(cudaMallocAsync(reinterpret_cast<void **>(&part),
+                              sizeof(double) * cnt, s));
+    double *nrm2 = part + size_t(blocks) * (k + 1);
+    int used     = 0;
+    int rc       = launch_multidot(V, ldv, k, w, n, part, &used, s);
+    if (!rc)
+      rc = launch_reduce_parts(part, used, k, h, s);
+    if (!rc)
+      rc = launch_update_norm(V, ldv, k, h, w, n, part, &used, s);
+    if (!rc)
+      rc = launch_reduce_parts(part, used, 1, nrm2, s);
+    double host = 0;
+    if (!rc && cudaMemcpyAsync(&host, nrm2, sizeof(double),
+                               cudaMemcpyDeviceToHost, s) != cudaSuccess)
+      rc = ASGK_ERR_CUDA;
+    if (cudaFreeAsync(part, s) != cudaSuccess && !rc)
+      rc = ASGK_ERR_CUDA;
+    if (!rc && cudaStreamSynchronize(s) != cudaSuccess)
+      rc = ASGK_ERR_CUDA;
+    if (!rc)
+      *norm = std::sqrt(host);
+    return rc;
+  }
+  catch (std::bad_alloc const &)
+  {
+    return ASGK_ERR_ALLOC;
+  }
+  catch (...)
+  {
     return ASGK_ERR_INVALID;
-  cudaStream_t s   = as_stream(stream);
-  int const blocks = max_reduction_blocks();
-  double *part     = nullptr;
-  size_t const cnt = size_t(blocks) * (k + 1) + 1;
-  ASGK_CUDA(cudaMallocAsync(reinterpret_cast<void **>(&part),
-                            sizeof(double) * cnt, s));
-  double *nrm2 = part + size_t(blocks) * (k + 1);
-  int used     = 0;
-  int rc       = launch_multidot(V, ldv, k, w, n, part, &used, s);
-  if (!rc)
-    rc = launch_reduce_parts(part, used, k, h, s);
-  if (!rc)
-    rc = launch_update_norm(V, ldv, k, h, w, n, part, &used, s);
-  if (!rc)
-    rc = launch_reduce_parts(part, used, 1, nrm2, s);
-  double host = 0;
-  if (!rc && cudaMemcpyAsync(&host, nrm2, sizeof(double),
-                             cudaMemcpyDeviceToHost, s) != cudaSuccess)
-    rc = ASGK_ERR_CUDA;
-  if (cudaFreeAsync(part, s) != cudaSuccess && !rc)
-    rc = ASGK_ERR_CUDA;
-  if (!rc && cudaStreamSynchronize(s) != cudaSuccess)
-    rc = ASGK_ERR_CUDA;
-  if (!rc)
-    *norm = std::sqrt(host);
-  return rc;
+  }
 }
 
 int asgk_default_gmres_restarts(int64_t n)
@@ -1982,20 +2180,31 @@ int asgk_gmres_euler(asgk_plan *plan, double dt, double *x, const double *b,
                      int precision, asgk_mlp *precond, asgk_gmres_info *info,
                      asgk_stream stream)
 {
-  if (precond == nullptr)
-    return gmres_euler_impl(plan, dt, x, b, restart, max_outer, tol, tol_mode,
-                            precision, nullptr, info, stream);
-  cudaStream_t s = as_stream(stream);
-  make_pc_t const mk = [&](bool low) -> precond_t {
-    return [=](double *v, double *z, const double *sc, cudaStream_t ss) -> int {
-      if (sc)
-        if (int rc = launch_scale_by(v, int64_t(plan->p.rows) * plan->p.tensor, sc, ss))
-          return rc;
-      return mlp_precondition(precond, plan, v, z, ss, low);
+  try
+  {
+    if (precond == nullptr)
+      return gmres_euler_impl(plan, dt, x, b, restart, max_outer, tol, tol_mode,
+                              precision, nullptr, info, stream);
+    cudaStream_t s = as_stream(stream);
+    make_pc_t const mk = [&](bool low) -> precond_t {
+      return [=](double *v, double *z, const double *sc, cudaStream_t ss) -> int {
+        if (sc)
+          if (int rc = launch_scale_by(v, int64_t(plan->p.rows) * plan->p.tensor, sc, ss))
+            return rc;
+        return mlp_precondition(precond, plan, v, z, ss, low);
+      };
     };
-  };
-  return gmres_euler_impl(plan, dt, x, b, restart, max_outer, tol, tol_mode,
-                          precision, &mk, info, stream);
+    return gmres_euler_impl(plan, dt, x, b, restart, max_outer, tol, tol_mode,
+                            precision, &mk, info, stream);
+  }
+  catch (std::bad_alloc const &)
+  {
+    return ASGK_ERR_ALLOC;
+  }
+  catch (...)
+  {
+    return ASGK_ERR_INVALID;
+  }
 }
 
 int asgk_gmres_euler_jacobi(asgk_plan *plan, double dt, double *x,
@@ -2004,17 +2213,28 @@ int asgk_gmres_euler_jacobi(asgk_plan *plan, double dt, double *x,
                             asgk_jacobi *precond, asgk_gmres_info *info,
                             asgk_stream stream)
 {
-  if (precond == nullptr)
-    return ASGK_ERR_INVALID;
-  cudaStream_t s = as_stream(stream);
-  make_pc_t const mk = [&](bool low) -> precond_t {
-    return [=](double *v, double *z, const double *sc, cudaStream_t ss) -> int {
-      return jacobi_apply_handle(precond, low, v, z, sc, ss);
+  try
+  {
+    if (precond == nullptr)
+      return ASGK_ERR_INVALID;
+    cudaStream_t s = as_stream(stream);
+    make_pc_t const mk = [&](bool low) -> precond_t {
+      return [=](double *v, double *z, const double *sc, cudaStream_t ss) -> int {
+        return jacobi_apply_handle(precond, low, v, z, sc, ss);
+      };
     };
-  };
-  return gmres_euler_impl(plan, dt, x, b, restart, max_outer, tol, tol_mode,
-                          precision, &mk, info, stream, jacobi_serial(precond),
-                          true);
+    return gmres_euler_impl(plan, dt, x, b, restart, max_outer, tol, tol_mode,
+                            precision, &mk, info, stream, jacobi_serial(precond),
+                            true);
+  }
+  catch (std::bad_alloc const &)
+  {
+    return ASGK_ERR_ALLOC;
+  }
+  catch (...)
+  {
+    return ASGK_ERR_INVALID;
+  }
 }
 
 int asgk_set_gmres_graphs(int enable)
@@ -2030,45 +2250,56 @@ int asgk_implicit_advance(asgk_plan *plan, double dt, double *x, int steps,
                           int precision, int pc_kind, void *precond,
                           asgk_gmres_info *info, asgk_stream stream)
 {
-  if (!plan || !x || steps < 0 || (steps > 0 && !info) || forcing_stride < 0 ||
-      pc_kind < 0 || pc_kind > 2 || (pc_kind != 0 && !precond))
-    return ASGK_ERR_INVALID;
-  auto &p = plan->p;
-  if (p.rows != p.cols)
-    return ASGK_ERR_INVALID;
-  int64_t const n = int64_t(p.rows) * p.tensor;
-  if (forcing && forcing_stride != 0 && forcing_stride < n)
-    return ASGK_ERR_INVALID;
-  cudaStream_t s = as_stream(stream);
-  double *b      = nullptr;
-  int64_t unused = 0;
-  if (int rc = dev_alloc(&b, std::max<int64_t>(n, 1), unused))
-    return rc;
-  int status = ASGK_OK;
-  for (int k = 0; k < steps && status == ASGK_OK; k++)
+  try
   {
-    // right-hand side x + dt * f(t + dt); the solve starts from it, as the
-    // reference starts from a copy of its right-hand side
-    if (forcing)
-      status = launch_axpy(x, forcing + k * forcing_stride, n, dt, s);
-    if (status == ASGK_OK)
-      status = launch_copy(b, x, n, s);
-    if (status != ASGK_OK)
-      break;
-    if (pc_kind == 1)
-      status = asgk_gmres_euler_jacobi(plan, dt, x, b, restart, max_outer, tol,
-                                       tol_mode, precision,
-                                       static_cast<asgk_jacobi *>(precond),
-                                       info + k, stream);
-    else
-      status = asgk_gmres_euler(plan, dt, x, b, restart, max_outer, tol,
-                                tol_mode, precision,
-                                static_cast<asgk_mlp *>(pc_kind == 2 ? precond : nullptr),
-                                info + k, stream);
+    if (!plan || !x || steps < 0 || (steps > 0 && !info) || forcing_stride < 0 ||
+        pc_kind < 0 || pc_kind > 2 || (pc_kind != 0 && !precond))
+      return ASGK_ERR_INVALID;
+    auto &p = plan->p;
+    if (p.rows != p.cols)
+      return ASGK_ERR_INVALID;
+    int64_t const n = int64_t(p.rows) * p.tensor;
+    if (forcing && forcing_stride != 0 && forcing_stride < n)
+      return ASGK_ERR_INVALID;
+    cudaStream_t s = as_stream(stream);
+    double *b      = nullptr;
+    int64_t unused = 0;
+    if (int rc = dev_alloc(&b, std::max<int64_t>(n, 1), unused))
+      return rc;
+    int status = ASGK_OK;
+    for (int k = 0; k < steps && status == ASGK_OK; k++)
+    {
+      // right-hand side x + dt * f(t + dt); the solve starts from it, as the
+      // reference starts from a copy of its right-hand side
+      if (forcing)
+        status = launch_axpy(x, forcing + k * forcing_stride, n, dt, s);
+      if (status == ASGK_OK)
+        status = launch_copy(b, x, n, s);
+      if (status != ASGK_OK)
+        break;
+      if (pc_kind == 1)
+        status = asgk_gmres_euler_jacobi(plan, dt, x, b, restart, max_outer, tol,
+                                         tol_mode, precision,
+                                         static_cast<asgk_jacobi *>(precond),
+                                         info + k, stream);
+      else
+        status = asgk_gmres_euler(plan, dt, x, b, restart, max_outer, tol,
+                                  tol_mode, precision,
+                                  static_cast<asgk_mlp *>(pc_kind == 2 ? precond : nullptr),
+                                  info + k, stream);
+    }
+    cudaStreamSynchronize(s);
+    cudaFree(b);
+    return status;
   }
-  cudaStreamSynchronize(s);
-  cudaFree(b);
-  return status;
+  catch (std::bad_alloc const &)
+  {
+    return ASGK_ERR_ALLOC;
+  }
+  catch (...)
+  {
+    return ASGK_ERR_INVALID;
+  }
 }
 
 } // extern "C"

@@ -24,6 +24,8 @@
 
 #include "internal.cuh"
 
+#include <new>
+
 #include <omp.h>
 
 namespace
@@ -189,16 +191,27 @@ extern "C"
 int asgk_connect_1d(int level, int *num_rows, int *num_conn, int *pntr,
                     int *indx)
 {
-  if (level < 0 || level > 12 || !num_rows || !num_conn)
+  try
+  {
+    if (level < 0 || level > 12 || !num_rows || !num_conn)
+      return ASGK_ERR_INVALID;
+    conn1d c(level);
+    *num_rows = c.rows;
+    *num_conn = int(c.indx.size());
+    if (pntr)
+      std::copy(c.pntr.begin(), c.pntr.end(), pntr);
+    if (indx)
+      std::copy(c.indx.begin(), c.indx.end(), indx);
+    return ASGK_OK;
+  }
+  catch (std::bad_alloc const &)
+  {
+    return ASGK_ERR_ALLOC;
+  }
+  catch (...)
+  {
     return ASGK_ERR_INVALID;
-  conn1d c(level);
-  *num_rows = c.rows;
-  *num_conn = int(c.indx.size());
-  if (pntr)
-    std::copy(c.pntr.begin(), c.pntr.end(), pntr);
-  if (indx)
-    std::copy(c.indx.begin(), c.indx.end(), indx);
-  return ASGK_OK;
+  }
 }
 
 int64_t asgk_sparse_grid(int d, int level, int *table)
@@ -266,94 +279,116 @@ int64_t asgk_sparse_grid(int d, int level, int *table)
 int asgk_build_pairs(int d, int level, int num_cells, const int *table,
                      int64_t *nnz, int64_t *row_ptr, int *col_indx, int *conn)
 {
-  if (d < 1 || d > 6 || level < 0 || level > 12 || num_cells < 0 || !table ||
-      !nnz)
-    return ASGK_ERR_INVALID;
-  conn1d const c(level);
-  int const R = c.rows;
-  // per cell: its 1D index in every dimension
-  std::vector<int> oned(size_t(num_cells) * d);
-  for (int i = 0; i < num_cells; i++)
-    for (int k = 0; k < d; k++)
-    {
-      int const L = table[int64_t(i) * 2 * d + k];
-      int const p = table[int64_t(i) * 2 * d + d + k];
-      if (L < 0 || L > level || p < 0 || (L > 1 && p >= (1 << (L - 1))) ||
-          (L <= 1 && p != 0))
-        return ASGK_ERR_INVALID;
-      oned[size_t(i) * d + k] = index_1d(L, p);
-    }
-  std::vector<int64_t> counts(num_cells, 0);
-#pragma omp parallel for schedule(dynamic, 16)
-  for (int r = 0; r < num_cells; r++)
+  try
   {
-    const int *ro = &oned[size_t(r) * d];
-    int64_t cnt   = 0;
-    for (int cc = 0; cc < num_cells; cc++)
-    {
-      const int *co = &oned[size_t(cc) * d];
-      bool ok       = true;
-      for (int k = 0; k < d && ok; k++)
-        ok = c.lut[size_t(ro[k]) * R + co[k]] >= 0;
-      cnt += ok;
-    }
-    counts[r] = cnt;
-  }
-  int64_t total = 0;
-  for (int r = 0; r < num_cells; r++)
-    total += counts[r];
-  *nnz = total;
-  if (!row_ptr || !col_indx)
-    return ASGK_OK;
-  row_ptr[0] = 0;
-  for (int r = 0; r < num_cells; r++)
-    row_ptr[r + 1] = row_ptr[r] + counts[r];
-#pragma omp parallel for schedule(dynamic, 16)
-  for (int r = 0; r < num_cells; r++)
-  {
-    const int *ro = &oned[size_t(r) * d];
-    int64_t pos   = row_ptr[r];
-    for (int cc = 0; cc < num_cells; cc++)
-    {
-      const int *co = &oned[size_t(cc) * d];
-      int off[6];
-      bool ok = true;
-      for (int k = 0; k < d && ok; k++)
+    if (d < 1 || d > 6 || level < 0 || level > 12 || num_cells < 0 || !table ||
+        !nnz)
+      return ASGK_ERR_INVALID;
+    conn1d const c(level);
+    int const R = c.rows;
+    // per cell: its 1D index in every dimension
+    std::vector<int> oned(size_t(num_cells) * d);
+    for (int i = 0; i < num_cells; i++)
+      for (int k = 0; k < d; k++)
       {
-        off[k] = c.lut[size_t(ro[k]) * R + co[k]];
-        ok     = off[k] >= 0;
+        int const L = table[int64_t(i) * 2 * d + k];
+        int const p = table[int64_t(i) * 2 * d + d + k];
+        if (L < 0 || L > level || p < 0 || (L > 1 && p >= (1 << (L - 1))) ||
+            (L <= 1 && p != 0))
+          return ASGK_ERR_INVALID;
+        oned[size_t(i) * d + k] = index_1d(L, p);
       }
-      if (!ok)
-        continue;
-      col_indx[pos] = cc;
-      if (conn)
-        for (int k = 0; k < d; k++)
-          conn[pos * d + k] = off[k];
-      ++pos;
+    std::vector<int64_t> counts(num_cells, 0);
+  #pragma omp parallel for schedule(dynamic, 16)
+    for (int r = 0; r < num_cells; r++)
+    {
+      const int *ro = &oned[size_t(r) * d];
+      int64_t cnt   = 0;
+      for (int cc = 0; cc < num_cells; cc++)
+      {
+        const int *co = &oned[size_t(cc) * d];
+        bool ok       = true;
+        for (int k = 0; k < d && ok; k++)
+          ok = c.lut[size_t(ro[k]) * R + co[k]] >= 0;
+        cnt += ok;
+      }
+      counts[r] = cnt;
     }
+    int64_t total = 0;
+    for (int r = 0; r < num_cells; r++)
+      total += counts[r];
+    *nnz = total;
+    if (!row_ptr || !col_indx)
+      return ASGK_OK;
+    row_ptr[0] = 0;
+    for (int r = 0; r < num_cells; r++)
+      row_ptr[r + 1] = row_ptr[r] + counts[r];
+  #pragma omp parallel for schedule(dynamic, 16)
+    for (int r = 0; r < num_cells; r++)
+    {
+      const int *ro = &oned[size_t(r) * d];
+      int64_t pos   = row_ptr[r];
+      for (int cc = 0; cc < num_cells; cc++)
+      {
+        const int *co = &oned[size_t(cc) * d];
+        int off[6];
+        bool ok = true;
+        for (int k = 0; k < d && ok; k++)
+        {
+          off[k] = c.lut[size_t(ro[k]) * R + co[k]];
+          ok     = off[k] >= 0;
+        }
+        if (!ok)
+          continue;
+        col_indx[pos] = cc;
+        if (conn)
+          for (int k = 0; k < d; k++)
+            conn[pos * d + k] = off[k];
+        ++pos;
+      }
+    }
+    return ASGK_OK;
   }
-  return ASGK_OK;
+  catch (std::bad_alloc const &)
+  {
+    return ASGK_ERR_ALLOC;
+  }
+  catch (...)
+  {
+    return ASGK_ERR_INVALID;
+  }
 }
 
 int asgk_direction_pairs(int d, int level, int num_cells, const int *table,
                          int64_t *nnz, int64_t *row_ptr, int *col_indx,
                          int *dim, int *conn)
 {
-  if (!nnz)
+  try
+  {
+    if (!nnz)
+      return ASGK_ERR_INVALID;
+    asgk::direction_pairs dp;
+    if (int rc = asgk::build_direction_pairs(d, level, num_cells, table, dp))
+      return rc;
+    *nnz = int64_t(dp.col.size());
+    if (row_ptr)
+      std::copy(dp.ptr.begin(), dp.ptr.end(), row_ptr);
+    if (col_indx)
+      std::copy(dp.col.begin(), dp.col.end(), col_indx);
+    if (dim)
+      std::copy(dp.dim.begin(), dp.dim.end(), dim);
+    if (conn)
+      std::copy(dp.conn.begin(), dp.conn.end(), conn);
+    return ASGK_OK;
+  }
+  catch (std::bad_alloc const &)
+  {
+    return ASGK_ERR_ALLOC;
+  }
+  catch (...)
+  {
     return ASGK_ERR_INVALID;
-  asgk::direction_pairs dp;
-  if (int rc = asgk::build_direction_pairs(d, level, num_cells, table, dp))
-    return rc;
-  *nnz = int64_t(dp.col.size());
-  if (row_ptr)
-    std::copy(dp.ptr.begin(), dp.ptr.end(), row_ptr);
-  if (col_indx)
-    std::copy(dp.col.begin(), dp.col.end(), col_indx);
-  if (dim)
-    std::copy(dp.dim.begin(), dp.dim.end(), dim);
-  if (conn)
-    std::copy(dp.conn.begin(), dp.conn.end(), conn);
-  return ASGK_OK;
+  }
 }
 
 } // extern "C"

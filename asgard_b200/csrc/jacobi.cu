@@ -418,16 +418,27 @@ struct asgk_jacobi
 
 int asgk_jacobi_create(asgk_jacobi **out, asgk_plan *plan, double dt, int kind)
 {
-  if (out == nullptr || plan == nullptr || !std::isfinite(dt))
-    return ASGK_ERR_INVALID;
-  *out = nullptr;
-  std::unique_ptr<asgk_jacobi> j(new (std::nothrow) asgk_jacobi());
-  if (!j)
+  try
+  {
+    if (out == nullptr || plan == nullptr || !std::isfinite(dt))
+      return ASGK_ERR_INVALID;
+    *out = nullptr;
+    std::unique_ptr<asgk_jacobi> j(new (std::nothrow) asgk_jacobi());
+    if (!j)
+      return ASGK_ERR_ALLOC;
+    if (int rc = asgk::jacobi_build(plan->p, dt, kind, j->jd))
+      return rc;
+    *out = j.release();
+    return ASGK_OK;
+  }
+  catch (std::bad_alloc const &)
+  {
     return ASGK_ERR_ALLOC;
-  if (int rc = asgk::jacobi_build(plan->p, dt, kind, j->jd))
-    return rc;
-  *out = j.release();
-  return ASGK_OK;
+  }
+  catch (...)
+  {
+    return ASGK_ERR_INVALID;
+  }
 }
 
 void asgk_jacobi_destroy(asgk_jacobi *pc) { delete pc; }
@@ -435,11 +446,22 @@ void asgk_jacobi_destroy(asgk_jacobi *pc) { delete pc; }
 int asgk_jacobi_apply(asgk_jacobi *pc, const double *v, double *z,
                       asgk_stream stream)
 {
-  if (pc == nullptr || v == nullptr || z == nullptr)
+  try
+  {
+    if (pc == nullptr || v == nullptr || z == nullptr)
+      return ASGK_ERR_INVALID;
+    // without a scale state v is only read
+    return asgk::jacobi_apply(pc->jd, false, const_cast<double *>(v), z, nullptr,
+                              static_cast<cudaStream_t>(stream));
+  }
+  catch (std::bad_alloc const &)
+  {
+    return ASGK_ERR_ALLOC;
+  }
+  catch (...)
+  {
     return ASGK_ERR_INVALID;
-  // without a scale state v is only read
-  return asgk::jacobi_apply(pc->jd, false, const_cast<double *>(v), z, nullptr,
-                            static_cast<cudaStream_t>(stream));
+  }
 }
 
 uint64_t asgk::jacobi_serial(const asgk_jacobi *pc) { return pc ? pc->jd.serial : 0; }
@@ -453,13 +475,24 @@ int asgk::jacobi_apply_handle(asgk_jacobi *pc, bool low, double *v, double *z,
 int asgk_jacobi_info(asgk_jacobi *pc, int *kind, double *dt,
                      int64_t *device_bytes)
 {
-  if (pc == nullptr)
+  try
+  {
+    if (pc == nullptr)
+      return ASGK_ERR_INVALID;
+    if (kind)
+      *kind = pc->jd.kind;
+    if (dt)
+      *dt = pc->jd.dt;
+    if (device_bytes)
+      *device_bytes = pc->jd.device_bytes;
+    return ASGK_OK;
+  }
+  catch (std::bad_alloc const &)
+  {
+    return ASGK_ERR_ALLOC;
+  }
+  catch (...)
+  {
     return ASGK_ERR_INVALID;
-  if (kind)
-    *kind = pc->jd.kind;
-  if (dt)
-    *dt = pc->jd.dt;
-  if (device_bytes)
-    *device_bytes = pc->jd.device_bytes;
-  return ASGK_OK;
+  }
 }

@@ -24,6 +24,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <new>
 #include <random>
 #include <vector>
 
@@ -655,123 +656,167 @@ int asgk_mlp_create(asgk_mlp **out, int d, int n, int num_cells,
                     const int *cell_levels, int max_level, int hidden,
                     uint64_t seed)
 {
-  if (!out || d < 1 || d > 6 || n < 1 || num_cells < 1 || !cell_levels ||
-      max_level < 1 || hidden < 16 || hidden > 4096)
-    return ASGK_ERR_INVALID;
-  *out   = nullptr;
-  auto *m = new (std::nothrow) mlp_state();
-  if (!m)
+  try
+  {
+    if (!out || d < 1 || d > 6 || n < 1 || num_cells < 1 || !cell_levels ||
+        max_level < 1 || hidden < 16 || hidden > 4096)
+      return ASGK_ERR_INVALID;
+    *out   = nullptr;
+    auto *m = new (std::nothrow) mlp_state();
+    if (!m)
+      return ASGK_ERR_ALLOC;
+    int ts = 1;
+    for (int i = 0; i < d; i++)
+      ts *= n;
+    m->d      = d;
+    m->ts     = ts;
+    m->hidden = hidden;
+    m->cells  = num_cells;
+    int64_t o = 0, ob = 0;
+    for (int l = 0; l < kLayers; l++)
+    {
+      m->off_W[l]  = o;
+      m->off_Wb[l] = ob;
+      int64_t const nw = int64_t(m->fan_in(l)) * m->fan_out(l);
+      o += nw;
+      ob += nw;
+    }
+    for (int l = 0; l < 3; l++)
+    {
+      m->off_P[l] = o;
+      o += int64_t(d) * hidden;
+      m->off_p[l] = o;
+      o += hidden;
+    }
+    m->nparams = o;
+    m->nWb     = ob;
+    int rc     = ASGK_OK;
+    if ((rc = m->alloc(&m->params, o)) || (rc = m->alloc(&m->grads, o)) ||
+        (rc = m->alloc(&m->m1, o)) || (rc = m->alloc(&m->m2, o)) ||
+        (rc = m->alloc(&m->Wb, ob)) || (rc = m->alloc(&m->lev, int64_t(num_cells) * d)))
+    {
+      delete m;
+      return rc;
+    }
+    // W_l uniform(-a, a), a = sqrt(6 / (fan_in + fan_out)), the last layer
+    // scaled by 0.1 (the untrained network is close to the identity map);
+    // gate weights P_l uniform(-1, 1), gate biases 1 (gates start near 0.84)
+    std::mt19937_64 rng(seed);
+    std::vector<float> h(o, 0.f);
+    for (int l = 0; l < kLayers; l++)
+    {
+      double const a = std::sqrt(6.0 / (m->fan_in(l) + m->fan_out(l))) *
+                       ((l == kLayers - 1) ? 0.1 : 1.0);
+      std::uniform_real_distribution<double> U(-a, a);
+      int64_t const nw = int64_t(m->fan_in(l)) * m->fan_out(l);
+      for (int64_t i = 0; i < nw; i++)
+        h[m->off_W[l] + i] = float(U(rng));
+    }
+    std::uniform_real_distribution<double> Ug(-1.0, 1.0);
+    for (int l = 0; l < 3; l++)
+    {
+      for (int64_t i = 0; i < int64_t(d) * hidden; i++)
+        h[m->off_P[l] + i] = float(Ug(rng));
+      for (int i = 0; i < hidden; i++)
+        h[m->off_p[l] + i] = 1.0f;
+    }
+    std::vector<float> lev(size_t(num_cells) * d);
+    for (size_t i = 0; i < lev.size(); i++)
+      lev[i] = float(cell_levels[i]) / float(max_level);
+    if (cudaMemcpy(m->params, h.data(), sizeof(float) * o, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemset(m->m1, 0, sizeof(float) * o) != cudaSuccess ||
+        cudaMemset(m->m2, 0, sizeof(float) * o) != cudaSuccess ||
+        cudaMemset(m->grads, 0, sizeof(float) * o) != cudaSuccess ||
+        cudaMemcpy(m->lev, lev.data(), sizeof(float) * lev.size(),
+                   cudaMemcpyHostToDevice) != cudaSuccess)
+      rc = ASGK_ERR_CUDA;
+    if (!rc)
+      rc = m->sync_bf16(nullptr);
+    if (!rc && cudaDeviceSynchronize() != cudaSuccess)
+      rc = ASGK_ERR_CUDA;
+    if (rc)
+    {
+      delete m;
+      return rc;
+    }
+    *out = reinterpret_cast<asgk_mlp *>(m);
+    return ASGK_OK;
+  }
+  catch (std::bad_alloc const &)
+  {
     return ASGK_ERR_ALLOC;
-  int ts = 1;
-  for (int i = 0; i < d; i++)
-    ts *= n;
-  m->d      = d;
-  m->ts     = ts;
-  m->hidden = hidden;
-  m->cells  = num_cells;
-  int64_t o = 0, ob = 0;
-  for (int l = 0; l < kLayers; l++)
-  {
-    m->off_W[l]  = o;
-    m->off_Wb[l] = ob;
-    int64_t const nw = int64_t(m->fan_in(l)) * m->fan_out(l);
-    o += nw;
-    ob += nw;
   }
-  for (int l = 0; l < 3; l++)
+  catch (...)
   {
-    m->off_P[l] = o;
-    o += int64_t(d) * hidden;
-    m->off_p[l] = o;
-    o += hidden;
+    return ASGK_ERR_INVALID;
   }
-  m->nparams = o;
-  m->nWb     = ob;
-  int rc     = ASGK_OK;
-  if ((rc = m->alloc(&m->params, o)) || (rc = m->alloc(&m->grads, o)) ||
-      (rc = m->alloc(&m->m1, o)) || (rc = m->alloc(&m->m2, o)) ||
-      (rc = m->alloc(&m->Wb, ob)) || (rc = m->alloc(&m->lev, int64_t(num_cells) * d)))
-  {
-    delete m;
-    return rc;
-  }
-  // W_l uniform(-a, a), a = sqrt(6 / (fan_in + fan_out)), the last layer
-  // scaled by 0.1 (the untrained network is close to the identity map);
-  // gate weights P_l uniform(-1, 1), gate biases 1 (gates start near 0.84)
-  std::mt19937_64 rng(seed);
-  std::vector<float> h(o, 0.f);
-  for (int l = 0; l < kLayers; l++)
-  {
-    double const a = std::sqrt(6.0 / (m->fan_in(l) + m->fan_out(l))) *
-                     ((l == kLayers - 1) ? 0.1 : 1.0);
-    std::uniform_real_distribution<double> U(-a, a);
-    int64_t const nw = int64_t(m->fan_in(l)) * m->fan_out(l);
-    for (int64_t i = 0; i < nw; i++)
-      h[m->off_W[l] + i] = float(U(rng));
-  }
-  std::uniform_real_distribution<double> Ug(-1.0, 1.0);
-  for (int l = 0; l < 3; l++)
-  {
-    for (int64_t i = 0; i < int64_t(d) * hidden; i++)
-      h[m->off_P[l] + i] = float(Ug(rng));
-    for (int i = 0; i < hidden; i++)
-      h[m->off_p[l] + i] = 1.0f;
-  }
-  std::vector<float> lev(size_t(num_cells) * d);
-  for (size_t i = 0; i < lev.size(); i++)
-    lev[i] = float(cell_levels[i]) / float(max_level);
-  if (cudaMemcpy(m->params, h.data(), sizeof(float) * o, cudaMemcpyHostToDevice) != cudaSuccess ||
-      cudaMemset(m->m1, 0, sizeof(float) * o) != cudaSuccess ||
-      cudaMemset(m->m2, 0, sizeof(float) * o) != cudaSuccess ||
-      cudaMemset(m->grads, 0, sizeof(float) * o) != cudaSuccess ||
-      cudaMemcpy(m->lev, lev.data(), sizeof(float) * lev.size(),
-                 cudaMemcpyHostToDevice) != cudaSuccess)
-    rc = ASGK_ERR_CUDA;
-  if (!rc)
-    rc = m->sync_bf16(nullptr);
-  if (!rc && cudaDeviceSynchronize() != cudaSuccess)
-    rc = ASGK_ERR_CUDA;
-  if (rc)
-  {
-    delete m;
-    return rc;
-  }
-  *out = reinterpret_cast<asgk_mlp *>(m);
-  return ASGK_OK;
 }
 
 void asgk_mlp_destroy(asgk_mlp *mlp) { delete reinterpret_cast<mlp_state *>(mlp); }
 
 int asgk_mlp_num_params(const asgk_mlp *mlp, int64_t *count)
 {
-  auto const *m = reinterpret_cast<const mlp_state *>(mlp);
-  if (!m || !count)
+  try
+  {
+    auto const *m = reinterpret_cast<const mlp_state *>(mlp);
+    if (!m || !count)
+      return ASGK_ERR_INVALID;
+    *count = m->nparams;
+    return ASGK_OK;
+  }
+  catch (std::bad_alloc const &)
+  {
+    return ASGK_ERR_ALLOC;
+  }
+  catch (...)
+  {
     return ASGK_ERR_INVALID;
-  *count = m->nparams;
-  return ASGK_OK;
+  }
 }
 
 int asgk_mlp_get_params(const asgk_mlp *mlp, float *params)
 {
-  auto const *m = reinterpret_cast<const mlp_state *>(mlp);
-  if (!m || !params)
+  try
+  {
+    auto const *m = reinterpret_cast<const mlp_state *>(mlp);
+    if (!m || !params)
+      return ASGK_ERR_INVALID;
+    ASGK_CUDA(cudaMemcpy(params, m->params, sizeof(float) * m->nparams,
+                         cudaMemcpyDeviceToHost));
+    return ASGK_OK;
+  }
+  catch (std::bad_alloc const &)
+  {
+    return ASGK_ERR_ALLOC;
+  }
+  catch (...)
+  {
     return ASGK_ERR_INVALID;
-  ASGK_CUDA(cudaMemcpy(params, m->params, sizeof(float) * m->nparams,
-                       cudaMemcpyDeviceToHost));
-  return ASGK_OK;
+  }
 }
 
 int asgk_mlp_set_params(asgk_mlp *mlp, const float *params)
 {
-  auto *m = reinterpret_cast<mlp_state *>(mlp);
-  if (!m || !params)
+  try
+  {
+    auto *m = reinterpret_cast<mlp_state *>(mlp);
+    if (!m || !params)
+      return ASGK_ERR_INVALID;
+    ASGK_CUDA(cudaMemcpy(m->params, params, sizeof(float) * m->nparams,
+                         cudaMemcpyHostToDevice));
+    if (int rc = m->sync_bf16(nullptr))
+      return rc;
+    ASGK_CUDA(cudaDeviceSynchronize());
+    return ASGK_OK;
+  }
+  catch (std::bad_alloc const &)
+  {
+    return ASGK_ERR_ALLOC;
+  }
+  catch (...)
+  {
     return ASGK_ERR_INVALID;
-  ASGK_CUDA(cudaMemcpy(m->params, params, sizeof(float) * m->nparams,
-                       cudaMemcpyHostToDevice));
-  if (int rc = m->sync_bf16(nullptr))
-    return rc;
-  ASGK_CUDA(cudaDeviceSynchronize());
-  return ASGK_OK;
+  }
 }
 
 // One forward + backward pass on host rows (X: rows x (n^d + d) = residual
@@ -781,37 +826,48 @@ int asgk_mlp_forward_backward(asgk_mlp *mlp, int rows, const float *X,
                               const float *T, float *Y, float *grads,
                               double *loss)
 {
-  auto *m = reinterpret_cast<mlp_state *>(mlp);
-  if (!m || rows < 1 || !X || !T)
-    return ASGK_ERR_INVALID;
-  if (int rc = m->ensure_rows(rows))
-    return rc;
-  int const in = m->ts + m->d;
-  std::vector<bf16> u(size_t(rows) * m->ts);
-  std::vector<float> lr(size_t(rows) * m->d);
-  for (int r = 0; r < rows; r++)
+  try
   {
-    for (int i = 0; i < m->ts; i++)
-      u[size_t(r) * m->ts + i] = __float2bfloat16(X[size_t(r) * in + i]);
-    for (int i = 0; i < m->d; i++)
-      lr[size_t(r) * m->d + i] = X[size_t(r) * in + m->ts + i];
+    auto *m = reinterpret_cast<mlp_state *>(mlp);
+    if (!m || rows < 1 || !X || !T)
+      return ASGK_ERR_INVALID;
+    if (int rc = m->ensure_rows(rows))
+      return rc;
+    int const in = m->ts + m->d;
+    std::vector<bf16> u(size_t(rows) * m->ts);
+    std::vector<float> lr(size_t(rows) * m->d);
+    for (int r = 0; r < rows; r++)
+    {
+      for (int i = 0; i < m->ts; i++)
+        u[size_t(r) * m->ts + i] = __float2bfloat16(X[size_t(r) * in + i]);
+      for (int i = 0; i < m->d; i++)
+        lr[size_t(r) * m->d + i] = X[size_t(r) * in + m->ts + i];
+    }
+    ASGK_CUDA(cudaMemcpy(m->U, u.data(), sizeof(bf16) * u.size(), cudaMemcpyHostToDevice));
+    ASGK_CUDA(cudaMemcpy(m->Lr, lr.data(), sizeof(float) * lr.size(), cudaMemcpyHostToDevice));
+    ASGK_CUDA(cudaMemcpy(m->T, T, sizeof(float) * size_t(rows) * m->ts, cudaMemcpyHostToDevice));
+    if (int rc = m->forward(rows, nullptr))
+      return rc;
+    double l = 0;
+    if (int rc = m->backward(rows, 1.0f, &l, nullptr))
+      return rc;
+    ASGK_CUDA(cudaDeviceSynchronize());
+    if (Y)
+      ASGK_CUDA(cudaMemcpy(Y, m->Y, sizeof(float) * size_t(rows) * m->ts, cudaMemcpyDeviceToHost));
+    if (grads)
+      ASGK_CUDA(cudaMemcpy(grads, m->grads, sizeof(float) * m->nparams, cudaMemcpyDeviceToHost));
+    if (loss)
+      *loss = 0.5 * l;
+    return ASGK_OK;
   }
-  ASGK_CUDA(cudaMemcpy(m->U, u.data(), sizeof(bf16) * u.size(), cudaMemcpyHostToDevice));
-  ASGK_CUDA(cudaMemcpy(m->Lr, lr.data(), sizeof(float) * lr.size(), cudaMemcpyHostToDevice));
-  ASGK_CUDA(cudaMemcpy(m->T, T, sizeof(float) * size_t(rows) * m->ts, cudaMemcpyHostToDevice));
-  if (int rc = m->forward(rows, nullptr))
-    return rc;
-  double l = 0;
-  if (int rc = m->backward(rows, 1.0f, &l, nullptr))
-    return rc;
-  ASGK_CUDA(cudaDeviceSynchronize());
-  if (Y)
-    ASGK_CUDA(cudaMemcpy(Y, m->Y, sizeof(float) * size_t(rows) * m->ts, cudaMemcpyDeviceToHost));
-  if (grads)
-    ASGK_CUDA(cudaMemcpy(grads, m->grads, sizeof(float) * m->nparams, cudaMemcpyDeviceToHost));
-  if (loss)
-    *loss = 0.5 * l;
-  return ASGK_OK;
+  catch (std::bad_alloc const &)
+  {
+    return ASGK_ERR_ALLOC;
+  }
+  catch (...)
+  {
+    return ASGK_ERR_INVALID;
+  }
 }
 
 // Trains on (v, e) pairs given as num_samples device vectors of cells*n^d
@@ -822,76 +878,87 @@ int asgk_mlp_train(asgk_mlp *mlp, const double *v, const double *e,
                    int num_samples, int epochs, int batch, float lr,
                    uint64_t seed, double *final_loss, asgk_stream stream)
 {
-  auto *m = reinterpret_cast<mlp_state *>(mlp);
-  if (!m || !v || !e || num_samples < 1 || epochs < 1 || batch < 1)
-    return ASGK_ERR_INVALID;
-  cudaStream_t s    = static_cast<cudaStream_t>(stream);
-  int64_t const all = int64_t(num_samples) * m->cells;
-  if (all > (int64_t(1) << 30))
-    return ASGK_ERR_UNSUPPORTED;
-  batch = int(std::min<int64_t>(batch, all));
-  if (int rc = m->ensure_rows(batch))
-    return rc;
-  int *cell_of = nullptr, *sample_of = nullptr;
-  if (cudaMalloc(&cell_of, sizeof(int) * batch) != cudaSuccess ||
-      cudaMalloc(&sample_of, sizeof(int) * batch) != cudaSuccess)
+  try
   {
+    auto *m = reinterpret_cast<mlp_state *>(mlp);
+    if (!m || !v || !e || num_samples < 1 || epochs < 1 || batch < 1)
+      return ASGK_ERR_INVALID;
+    cudaStream_t s    = static_cast<cudaStream_t>(stream);
+    int64_t const all = int64_t(num_samples) * m->cells;
+    if (all > (int64_t(1) << 30))
+      return ASGK_ERR_UNSUPPORTED;
+    batch = int(std::min<int64_t>(batch, all));
+    if (int rc = m->ensure_rows(batch))
+      return rc;
+    int *cell_of = nullptr, *sample_of = nullptr;
+    if (cudaMalloc(&cell_of, sizeof(int) * batch) != cudaSuccess ||
+        cudaMalloc(&sample_of, sizeof(int) * batch) != cudaSuccess)
+    {
+      cudaFree(cell_of);
+      return ASGK_ERR_ALLOC;
+    }
+    std::vector<int64_t> order(all);
+    for (int64_t i = 0; i < all; i++)
+      order[i] = i;
+    std::mt19937_64 rng(seed);
+    std::vector<int> hc(batch), hs(batch);
+    double epoch_loss = 0;
+    int rc            = ASGK_OK;
+    for (int ep = 0; ep < epochs && !rc; ep++)
+    {
+      std::shuffle(order.begin(), order.end(), rng);
+      epoch_loss   = 0;
+      int64_t seen = 0;
+      for (int64_t b0 = 0; b0 + batch <= all && !rc; b0 += batch)
+      {
+        for (int i = 0; i < batch; i++)
+        {
+          hs[i] = int(order[b0 + i] / m->cells);
+          hc[i] = int(order[b0 + i] % m->cells);
+        }
+        if (cudaMemcpyAsync(cell_of, hc.data(), sizeof(int) * batch,
+                            cudaMemcpyHostToDevice, s) != cudaSuccess ||
+            cudaMemcpyAsync(sample_of, hs.data(), sizeof(int) * batch,
+                            cudaMemcpyHostToDevice, s) != cudaSuccess)
+        {
+          rc = ASGK_ERR_CUDA;
+          break;
+        }
+        k_train_rows<<<batch, 128, 0, s>>>(v, e, cell_of, sample_of, batch,
+                                           m->ts, m->d, int64_t(m->cells) * m->ts,
+                                           m->lev, m->U, m->Lr, m->T);
+        if (cudaGetLastError() != cudaSuccess)
+        {
+          rc = ASGK_ERR_CUDA;
+          break;
+        }
+        count_launch();
+        double l = 0;
+        float const gscale = 1.0f / float(int64_t(batch) * m->ts);
+        if ((rc = m->forward(batch, s)) ||
+            (rc = m->backward(batch, gscale, &l, s)) || (rc = m->adam(lr, s)))
+          break;
+        epoch_loss += l;
+        seen += int64_t(batch) * m->ts;
+      }
+      if (seen > 0)
+        epoch_loss /= double(seen);
+    }
+    cudaStreamSynchronize(s);
     cudaFree(cell_of);
+    cudaFree(sample_of);
+    if (final_loss)
+      *final_loss = epoch_loss;
+    return rc;
+  }
+  catch (std::bad_alloc const &)
+  {
     return ASGK_ERR_ALLOC;
   }
-  std::vector<int64_t> order(all);
-  for (int64_t i = 0; i < all; i++)
-    order[i] = i;
-  std::mt19937_64 rng(seed);
-  std::vector<int> hc(batch), hs(batch);
-  double epoch_loss = 0;
-  int rc            = ASGK_OK;
-  for (int ep = 0; ep < epochs && !rc; ep++)
+  catch (...)
   {
-    std::shuffle(order.begin(), order.end(), rng);
-    epoch_loss   = 0;
-    int64_t seen = 0;
-    for (int64_t b0 = 0; b0 + batch <= all && !rc; b0 += batch)
-    {
-      for (int i = 0; i < batch; i++)
-      {
-        hs[i] = int(order[b0 + i] / m->cells);
-        hc[i] = int(order[b0 + i] % m->cells);
-      }
-      if (cudaMemcpyAsync(cell_of, hc.data(), sizeof(int) * batch,
-                          cudaMemcpyHostToDevice, s) != cudaSuccess ||
-          cudaMemcpyAsync(sample_of, hs.data(), sizeof(int) * batch,
-                          cudaMemcpyHostToDevice, s) != cudaSuccess)
-      {
-        rc = ASGK_ERR_CUDA;
-        break;
-      }
-      k_train_rows<<<batch, 128, 0, s>>>(v, e, cell_of, sample_of, batch,
-                                         m->ts, m->d, int64_t(m->cells) * m->ts,
-                                         m->lev, m->U, m->Lr, m->T);
-      if (cudaGetLastError() != cudaSuccess)
-      {
-        rc = ASGK_ERR_CUDA;
-        break;
-      }
-      count_launch();
-      double l = 0;
-      float const gscale = 1.0f / float(int64_t(batch) * m->ts);
-      if ((rc = m->forward(batch, s)) ||
-          (rc = m->backward(batch, gscale, &l, s)) || (rc = m->adam(lr, s)))
-        break;
-      epoch_loss += l;
-      seen += int64_t(batch) * m->ts;
-    }
-    if (seen > 0)
-      epoch_loss /= double(seen);
+    return ASGK_ERR_INVALID;
   }
-  cudaStreamSynchronize(s);
-  cudaFree(cell_of);
-  cudaFree(sample_of);
-  if (final_loss)
-    *final_loss = epoch_loss;
-  return rc;
 }
 
 // Residual-space training on (residual, GMRES-correction) pairs (r_k, e_k)
@@ -906,116 +973,149 @@ int asgk_mlp_train_residual(asgk_mlp *mlp, asgk_plan *plan, asgk_plan *plan_T,
                             int precision, uint64_t seed, double *final_loss,
                             asgk_stream stream)
 {
-  auto *m = reinterpret_cast<mlp_state *>(mlp);
-  if (!m || !plan || !plan_T || !r || !e || num_samples < 1 || epochs < 1)
-    return ASGK_ERR_INVALID;
-  if (plan->p.rows != m->cells || plan->p.tensor != m->ts ||
-      plan_T->p.rows != m->cells || plan_T->p.tensor != m->ts)
-    return ASGK_ERR_INVALID;
-  cudaStream_t s  = static_cast<cudaStream_t>(stream);
-  int64_t const N = int64_t(m->cells) * m->ts;
-  if (int rc = m->ensure_rows(m->cells))
-    return rc;
-  double *buf = nullptr, *part = nullptr;
-  if (cudaMalloc(&buf, sizeof(double) * 4 * N) != cudaSuccess ||
-      cudaMalloc(&part, sizeof(double) * 1024) != cudaSuccess)
+  try
   {
-    cudaGetLastError();
+    auto *m = reinterpret_cast<mlp_state *>(mlp);
+    if (!m || !plan || !plan_T || !r || !e || num_samples < 1 || epochs < 1)
+      return ASGK_ERR_INVALID;
+    if (plan->p.rows != m->cells || plan->p.tensor != m->ts ||
+        plan_T->p.rows != m->cells || plan_T->p.tensor != m->ts)
+      return ASGK_ERR_INVALID;
+    cudaStream_t s  = static_cast<cudaStream_t>(stream);
+    int64_t const N = int64_t(m->cells) * m->ts;
+    if (int rc = m->ensure_rows(m->cells))
+      return rc;
+    double *buf = nullptr, *part = nullptr;
+    if (cudaMalloc(&buf, sizeof(double) * 4 * N) != cudaSuccess ||
+        cudaMalloc(&part, sizeof(double) * 1024) != cudaSuccess)
+    {
+      cudaGetLastError();
+      cudaFree(buf);
+      return ASGK_ERR_ALLOC;
+    }
+    double *z = buf, *dv = buf + N, *q = buf + 2 * N, *g = buf + 3 * N;
+    int const gb = grid1(N);
+    std::vector<double> hp(gb);
+    auto sumsq = [&](const double *x, double &out) -> int {
+      k_sumsq<<<gb, 256, 0, s>>>(x, N, part);
+      ASGK_LAUNCHED();
+      ASGK_CUDA(cudaMemcpyAsync(hp.data(), part, sizeof(double) * gb,
+                                cudaMemcpyDeviceToHost, s));
+      ASGK_CUDA(cudaStreamSynchronize(s));
+      out = 0;
+      for (double v : hp)
+        out += v;
+      return ASGK_OK;
+    };
+    std::vector<int> order(num_samples);
+    for (int i = 0; i < num_samples; i++)
+      order[i] = i;
+    std::mt19937_64 rng(seed);
+    double epoch_loss = 0;
+    int rc            = ASGK_OK;
+    for (int ep = 0; ep < epochs && !rc; ep++)
+    {
+      std::shuffle(order.begin(), order.end(), rng);
+      epoch_loss = 0;
+      for (int it = 0; it < num_samples && !rc; it++)
+      {
+        const double *rk = r + int64_t(order[it]) * N;
+        const double *ek = e + int64_t(order[it]) * N;
+        double nr2 = 0, nq2 = 0;
+        if ((rc = sumsq(rk, nr2)))
+          break;
+        if (!(nr2 > 0))
+          continue;
+        k_pc_features<<<m->cells, 128, 0, s>>>(rk, m->cells, m->ts, m->d, m->lev,
+                                               m->U, m->Lr, m->scale);
+        if (cudaGetLastError() != cudaSuccess)
+        {
+          rc = ASGK_ERR_CUDA;
+          break;
+        }
+        count_launch();
+        if ((rc = m->forward(m->cells, s)))
+          break;
+        k_pc_output<<<gb, 256, 0, s>>>(m->Y, m->cells, m->ts, m->scale, rk, z, 0);
+        k_sub<<<gb, 256, 0, s>>>(z, ek, dv, N);
+        if (cudaGetLastError() != cudaSuccess)
+        {
+          rc = ASGK_ERR_CUDA;
+          break;
+        }
+        count_launch(2);
+        if ((rc = asgk_apply_euler(plan, precision, dt, 1.0, dv, 0.0, q, stream)) ||
+            (rc = sumsq(q, nq2)) ||
+            (rc = asgk_apply_euler(plan_T, precision, dt, 1.0, q, 0.0, g, stream)))
+          break;
+        epoch_loss += nq2 / nr2;
+        k_resid_grad<<<gb, 256, 0, s>>>(g, m->scale, m->cells, m->ts, 2.0 / nr2,
+                                        m->dY);
+        if (cudaGetLastError() != cudaSuccess)
+        {
+          rc = ASGK_ERR_CUDA;
+          break;
+        }
+        count_launch();
+        if ((rc = m->backward_from_dY(m->cells, s)) || (rc = m->adam(lr, s)))
+          break;
+      }
+      epoch_loss /= num_samples;
+    }
+    cudaStreamSynchronize(s);
     cudaFree(buf);
+    cudaFree(part);
+    if (final_loss)
+      *final_loss = epoch_loss;
+    return rc;
+  }
+  catch (std::bad_alloc const &)
+  {
     return ASGK_ERR_ALLOC;
   }
-  double *z = buf, *dv = buf + N, *q = buf + 2 * N, *g = buf + 3 * N;
-  int const gb = grid1(N);
-  std::vector<double> hp(gb);
-  auto sumsq = [&](const double *x, double &out) -> int {
-    k_sumsq<<<gb, 256, 0, s>>>(x, N, part);
-    ASGK_LAUNCHED();
-    ASGK_CUDA(cudaMemcpyAsync(hp.data(), part, sizeof(double) * gb,
-                              cudaMemcpyDeviceToHost, s));
-    ASGK_CUDA(cudaStreamSynchronize(s));
-    out = 0;
-    for (double v : hp)
-      out += v;
-    return ASGK_OK;
-  };
-  std::vector<int> order(num_samples);
-  for (int i = 0; i < num_samples; i++)
-    order[i] = i;
-  std::mt19937_64 rng(seed);
-  double epoch_loss = 0;
-  int rc            = ASGK_OK;
-  for (int ep = 0; ep < epochs && !rc; ep++)
+  catch (...)
   {
-    std::shuffle(order.begin(), order.end(), rng);
-    epoch_loss = 0;
-    for (int it = 0; it < num_samples && !rc; it++)
-    {
-      const double *rk = r + int64_t(order[it]) * N;
-      const double *ek = e + int64_t(order[it]) * N;
-      double nr2 = 0, nq2 = 0;
-      if ((rc = sumsq(rk, nr2)))
-        break;
-      if (!(nr2 > 0))
-        continue;
-      k_pc_features<<<m->cells, 128, 0, s>>>(rk, m->cells, m->ts, m->d, m->lev,
-                                             m->U, m->Lr, m->scale);
-      if (cudaGetLastError() != cudaSuccess)
-      {
-        rc = ASGK_ERR_CUDA;
-        break;
-      }
-      count_launch();
-      if ((rc = m->forward(m->cells, s)))
-        break;
-      k_pc_output<<<gb, 256, 0, s>>>(m->Y, m->cells, m->ts, m->scale, rk, z, 0);
-      k_sub<<<gb, 256, 0, s>>>(z, ek, dv, N);
-      if (cudaGetLastError() != cudaSuccess)
-      {
-        rc = ASGK_ERR_CUDA;
-        break;
-      }
-      count_launch(2);
-      if ((rc = asgk_apply_euler(plan, precision, dt, 1.0, dv, 0.0, q, stream)) ||
-          (rc = sumsq(q, nq2)) ||
-          (rc = asgk_apply_euler(plan_T, precision, dt, 1.0, q, 0.0, g, stream)))
-        break;
-      epoch_loss += nq2 / nr2;
-      k_resid_grad<<<gb, 256, 0, s>>>(g, m->scale, m->cells, m->ts, 2.0 / nr2,
-                                      m->dY);
-      if (cudaGetLastError() != cudaSuccess)
-      {
-        rc = ASGK_ERR_CUDA;
-        break;
-      }
-      count_launch();
-      if ((rc = m->backward_from_dY(m->cells, s)) || (rc = m->adam(lr, s)))
-        break;
-    }
-    epoch_loss /= num_samples;
+    return ASGK_ERR_INVALID;
   }
-  cudaStreamSynchronize(s);
-  cudaFree(buf);
-  cudaFree(part);
-  if (final_loss)
-    *final_loss = epoch_loss;
-  return rc;
 }
 
 int asgk_mlp_set_base(asgk_mlp *mlp, asgk_jacobi *base)
 {
-  auto *m = reinterpret_cast<mlp_state *>(mlp);
-  if (!m)
+  try
+  {
+    auto *m = reinterpret_cast<mlp_state *>(mlp);
+    if (!m)
+      return ASGK_ERR_INVALID;
+    m->base = base;
+    return ASGK_OK;
+  }
+  catch (std::bad_alloc const &)
+  {
+    return ASGK_ERR_ALLOC;
+  }
+  catch (...)
+  {
     return ASGK_ERR_INVALID;
-  m->base = base;
-  return ASGK_OK;
+  }
 }
 
 // z = M(v) for a full vector of cells*n^d values (device pointers).
 int asgk_mlp_apply(asgk_mlp *mlp, asgk_plan *plan, const double *v, double *z,
                    asgk_stream stream)
 {
-  return mlp_precondition(mlp, plan, v, z, static_cast<cudaStream_t>(stream),
-                          false);
+  try
+  {
+    return mlp_precondition(mlp, plan, v, z, static_cast<cudaStream_t>(stream),
+                            false);
+  }
+  catch (std::bad_alloc const &)
+  {
+    return ASGK_ERR_ALLOC;
+  }
+  catch (...)
+  {
+    return ASGK_ERR_INVALID;
+  }
 }
 
 } // extern "C"
