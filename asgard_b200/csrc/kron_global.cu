@@ -43,14 +43,17 @@ __device__ __forceinline__ int dim_stride(int k)
 }
 
 // One CTA per slice of at most kSlice entries of an output cell's
-// neighbour list (32 up to d = 4, 64 above).  The NW warps take the slice's
-// entries in turn (four in
-// flight per warp), each warp holding a partial output tensor (PER entries
-// per lane, with their base-3 digits packed two bits per dimension), summed
-// over the warps in shared memory.  A cell with one slice writes y at once;
-// the slices of a cell with several write partial tensors to scratch, and
-// the last of them to finish (an atomic ticket, no waiting) adds them in
-// slice order and writes y -- deterministic whichever slice ends last.
+// neighbour list (32 up to d = 4, 64 above).  A cell's entries come in
+// dimension order; for the entries along dimension k, lane f of a warp owns
+// fibre f of the 3^d tensor along k (the three entries that differ only in
+// their k-th index): it loads the neighbour's fibre and applies the 3x3 block
+// to it, accumulating in registers, and adds its three sums into the warp's
+// row of shared memory when the dimension changes.  The NW warps take the
+// slice's entries in turn (four in flight per warp); their rows are summed
+// at the end.  A cell with one slice writes y at once; the slices of a cell
+// with several write partial tensors to scratch, and the last of them to
+// finish (an atomic ticket, no waiting) adds them in slice order and writes
+// y -- deterministic whichever slice ends last.
 template<int D, typename TC, int NW, int kSlice>
 __global__ void __launch_bounds__(NW * 32)
     kron_global_rows(const int *__restrict__ slice_row,
@@ -65,11 +68,13 @@ __global__ void __launch_bounds__(NW * 32)
                      double *__restrict__ y, double ex)
 {
   constexpr int TS  = ipow3g(D);
-  constexpr int PER = (TS + 31) / 32; // outputs per lane
+  constexpr int NF  = TS / 3;           // fibres along one dimension
+  constexpr int FPL = (NF + 31) / 32;   // fibres per lane
   constexpr int PAD = padG<TC>::value;
   constexpr int NT  = NW * 32;
   __shared__ TC red[NW * TS];
   __shared__ int s_col[kSlice], s_kb[kSlice];
+  __shared__ int s_seg[D + 1];
   __shared__ unsigned s_ticket;
 
   int const warp   = threadIdx.x >> 5;
@@ -86,72 +91,80 @@ __global__ void __launch_bounds__(NW * 32)
     s_col[i] = __ldg(gcol + eb + i);
     s_kb[i]  = __ldg(gkb + eb + i);
   }
-  // base-3 digits of this lane's outputs, two bits per dimension
-  unsigned dig[PER];
-#pragma unroll
-  for (int o = 0; o < PER; o++)
+  for (int i = threadIdx.x; i < NW * TS; i += NT)
+    red[i] = TC(0);
+  __syncthreads();
+  if (threadIdx.x == 0)
   {
-    int v = lane + 32 * o;
-    unsigned pk = 0;
-#pragma unroll
-    for (int k = D - 1; k >= 0; k--)
+    // the slice's entries per dimension (they come in dimension order)
+    int e = 0;
+    for (int k = 0; k < D; k++)
     {
-      pk |= unsigned(v % 3) << (2 * k);
-      v /= 3;
+      s_seg[k] = e;
+      while (e < n && s_kb[e] % D == k)
+        ++e;
     }
-    dig[o] = pk;
+    s_seg[D] = e;
   }
-  TC acc[PER];
-#pragma unroll
-  for (int o = 0; o < PER; o++)
-    acc[o] = TC(0);
   __syncthreads();
 
-  auto entry = [&](int j) {
-    int const c      = s_col[j];
-    int const kb     = s_kb[j];
-    int const k      = kb % D;
+  TC *myred = red + warp * TS;
+  for (int k = 0; k < D; k++)
+  {
+    int const sa = s_seg[k], sb = s_seg[k + 1];
+    if (sa == sb)
+      continue;
     int const stride = dim_stride<D>(k);
-    const TC *b      = B + int64_t(kb) * PAD;
-    const double *xc = x + int64_t(c) * TS;
-    TC const b0 = __ldg(b), b1 = __ldg(b + 1), b2 = __ldg(b + 2);
-    TC const b3 = __ldg(b + 3), b4 = __ldg(b + 4), b5 = __ldg(b + 5);
-    TC const b6 = __ldg(b + 6), b7 = __ldg(b + 7), b8 = __ldg(b + 8);
+    int fb[FPL]; // first entry of each fibre this lane owns
+    TC acc[FPL][3];
 #pragma unroll
-    for (int o = 0; o < PER; o++)
+    for (int m = 0; m < FPL; m++)
     {
-      int const i = lane + 32 * o;
-      if (i < TS)
-      {
-        int const ik   = int((dig[o] >> (2 * k)) & 3u);
-        int const base = i - ik * stride;
-        TC const v0 = static_cast<TC>(__ldg(xc + base));
-        TC const v1 = static_cast<TC>(__ldg(xc + base + stride));
-        TC const v2 = static_cast<TC>(__ldg(xc + base + 2 * stride));
-        // row ik of the column-major block
-        TC const a0 = ik == 0 ? b0 : (ik == 1 ? b1 : b2);
-        TC const a1 = ik == 0 ? b3 : (ik == 1 ? b4 : b5);
-        TC const a2 = ik == 0 ? b6 : (ik == 1 ? b7 : b8);
-        acc[o] = fma(a2, v2, fma(a1, v1, fma(a0, v0, acc[o])));
-      }
+      int const f = lane + 32 * m;
+      fb[m]       = (f / stride) * 3 * stride + (f % stride);
+      acc[m][0] = acc[m][1] = acc[m][2] = TC(0);
     }
-  };
-  for (int j = warp; j < n; j += 4 * NW)
-  {
-    entry(j);
-    if (j + NW < n)
-      entry(j + NW);
-    if (j + 2 * NW < n)
-      entry(j + 2 * NW);
-    if (j + 3 * NW < n)
-      entry(j + 3 * NW);
-  }
+    auto entry = [&](int j) {
+      const TC *b      = B + int64_t(s_kb[j]) * PAD;
+      const double *xc = x + int64_t(s_col[j]) * TS;
+      TC const b0 = __ldg(b), b1 = __ldg(b + 1), b2 = __ldg(b + 2);
+      TC const b3 = __ldg(b + 3), b4 = __ldg(b + 4), b5 = __ldg(b + 5);
+      TC const b6 = __ldg(b + 6), b7 = __ldg(b + 7), b8 = __ldg(b + 8);
 #pragma unroll
-  for (int o = 0; o < PER; o++)
-  {
-    int const i = lane + 32 * o;
-    if (i < TS)
-      red[warp * TS + i] = acc[o];
+      for (int m = 0; m < FPL; m++)
+      {
+        if (lane + 32 * m < NF)
+        {
+          TC const v0 = static_cast<TC>(__ldg(xc + fb[m]));
+          TC const v1 = static_cast<TC>(__ldg(xc + fb[m] + stride));
+          TC const v2 = static_cast<TC>(__ldg(xc + fb[m] + 2 * stride));
+          // column-major block: out_q += sum_p A(q, p) v_p, A(q, p) = b[q + 3p]
+          acc[m][0] = fma(b6, v2, fma(b3, v1, fma(b0, v0, acc[m][0])));
+          acc[m][1] = fma(b7, v2, fma(b4, v1, fma(b1, v0, acc[m][1])));
+          acc[m][2] = fma(b8, v2, fma(b5, v1, fma(b2, v0, acc[m][2])));
+        }
+      }
+    };
+    for (int j = sa + warp; j < sb; j += 4 * NW)
+    {
+      entry(j);
+      if (j + NW < sb)
+        entry(j + NW);
+      if (j + 2 * NW < sb)
+        entry(j + 2 * NW);
+      if (j + 3 * NW < sb)
+        entry(j + 3 * NW);
+    }
+    // lanes own distinct fibres: their outputs along k do not overlap
+#pragma unroll
+    for (int m = 0; m < FPL; m++)
+      if (lane + 32 * m < NF)
+      {
+        myred[fb[m]] += acc[m][0];
+        myred[fb[m] + stride] += acc[m][1];
+        myred[fb[m] + 2 * stride] += acc[m][2];
+      }
+    __syncwarp(); // before the next dimension's fibres touch these entries
   }
   __syncthreads();
   int64_t const base = int64_t(row) * TS;
