@@ -367,10 +367,29 @@ __global__ void __launch_bounds__(kThreads)
     }
     else
     {
-      // two rows, four basis loads in flight (four partial sums per row)
+      // two rows, eight basis loads in flight (four partial sums per row)
       double x0 = 0.0, x1 = 0.0, x2 = 0.0, x3 = 0.0;
       double y0 = 0.0, y1 = 0.0, y2 = 0.0, y3 = 0.0;
       int j = 0;
+      for (; j + 8 <= k; j += 8)
+      {
+        T u[8];
+#pragma unroll
+        for (int q = 0; q < 8; q++)
+          u[q] = Vu[r + (j + q) * ldu];
+#pragma unroll
+        for (int q = 0; q < 8; q += 4)
+        {
+          x0 = fma(u[q].x, hs[j + q], x0);
+          y0 = fma(u[q].y, hs[j + q], y0);
+          x1 = fma(u[q + 1].x, hs[j + q + 1], x1);
+          y1 = fma(u[q + 1].y, hs[j + q + 1], y1);
+          x2 = fma(u[q + 2].x, hs[j + q + 2], x2);
+          y2 = fma(u[q + 2].y, hs[j + q + 2], y2);
+          x3 = fma(u[q + 3].x, hs[j + q + 3], x3);
+          y3 = fma(u[q + 3].y, hs[j + q + 3], y3);
+        }
+      }
       for (; j + 4 <= k; j += 4)
       {
         T const a = Vu[r + j * ldu], b = Vu[r + (j + 1) * ldu];
