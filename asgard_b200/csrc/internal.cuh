@@ -40,10 +40,11 @@ inline void count_launch(int k = 1) { g_launches.fetch_add(k, std::memory_order_
     ::asgk::count_launch();                                                    \
   } while (0)
 
-// Entries of a global-form neighbour list handled by one CTA: 32 for
-// tensors of up to 81 entries (4-warp CTAs), 64 above (8 warps).
+// Entries of a global-form neighbour list handled by one CTA (4 warps for
+// tensors of up to 81 entries, 8 above).  Measured at d=3/4, level 7: 64
+// beats 16, 32 and 128.
 constexpr int kGlobalSliceMax = 64;
-constexpr int global_slice(int d) { return d <= 4 ? 32 : 64; }
+constexpr int global_slice(int) { return 64; }
 
 // How the factor blocks of a pair are addressed.
 enum class index_mode : int

@@ -42,8 +42,8 @@ __device__ __forceinline__ int dim_stride(int k)
   return int((packed >> (8 * k)) & 0xff);
 }
 
-// One CTA per slice of at most kSlice entries of an output cell's
-// neighbour list (32 up to d = 4, 64 above).  A cell's entries come in
+// One CTA per slice of at most kSlice (64) entries of an output cell's
+// neighbour list.  A cell's entries come in
 // dimension order; for the entries along dimension k, lane f of a warp owns
 // fibre f of the 3^d tensor along k (the three entries that differ only in
 // their k-th index): it loads the neighbour's fibre and applies the 3x3 block
