@@ -496,7 +496,9 @@ int launch_multidot_h(const double *V, int64_t ldv, int k, const double *w,
                       cudaStream_t s)
 {
   int const groups = (k + kDotCols - 1) / kDotCols;
-  dim3 const grid(grid_for(n), groups);
+  // one block per SM and column group (measured: more row blocks lengthen
+  // the final sums more than they shorten the pass)
+  dim3 const grid(std::min(grid_for(n), sm_count()), groups);
   if (vec2_ok(V, ldv, w) && n % 2 == 0)
     k_multidot_h<2><<<grid, kThreads, 0, s>>>(V, ldv, k, w, n, part, tickets, h);
   else
@@ -509,7 +511,7 @@ int launch_update_norm_h(const double *V, int64_t ldv, int k, const double *h,
                          double *w, int64_t n, double *part, unsigned *ticket,
                          double *out, cudaStream_t s, givens_args const *ga)
 {
-  int const g        = grid_wide(n);
+  int const g        = grid_for(n); // two blocks per SM (measured best)
   givens_args const a = ga ? *ga : givens_args{};
   size_t const shm   = sizeof(double) *
                      (std::max(k, 1) + (ga ? 3 * int64_t(a.restart + 1) : 0));
