@@ -14,6 +14,8 @@
 namespace asgk
 {
 std::atomic<int64_t> g_launches{0};
+thread_local bool g_recording            = false;
+thread_local int64_t g_recorded_launches = 0;
 
 namespace
 {
@@ -652,7 +654,8 @@ int record_cycle(gmres_ws &ws, int64_t n, matvec_t const &mat,
   cudaGraph_t graph     = nullptr;
   if (cudaGraphCreate(&graph, 0) != cudaSuccess)
     return ASGK_ERR_CUDA;
-  int64_t const launches0 = g_launches.load();
+  g_recording         = true;
+  g_recorded_launches = 0;
   std::vector<cudaGraphConditionalHandle> hs(restart);
   int rc = ASGK_OK;
   for (int i = 0; i < restart && rc == ASGK_OK; i++)
@@ -682,7 +685,7 @@ int record_cycle(gmres_ws &ws, int64_t n, matvec_t const &mat,
       rc = ASGK_ERR_CUDA;
       break;
     }
-    int64_t const before = g_launches.load();
+    int64_t const before = g_recorded_launches;
     double *vi  = ws.V + int64_t(i) * n;
     double *w   = ws.V + int64_t(i + 1) * n;
     int const k = i + 1;
@@ -718,11 +721,11 @@ int record_cycle(gmres_ws &ws, int64_t n, matvec_t const &mat,
     if (cudaStreamEndCapture(cs, &captured) != cudaSuccess && rc == ASGK_OK)
       rc = ASGK_ERR_CUDA;
     if (i == 0)
-      kps = int(g_launches.load() - before);
+      kps = int(g_recorded_launches - before);
     prev = node;
   }
   // what was launched while recording runs later, counted per executed step
-  g_launches.store(launches0);
+  g_recording = false;
   cudaGraphExec_t exec = nullptr;
   if (rc == ASGK_OK && cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess)
     rc = ASGK_ERR_CUDA;

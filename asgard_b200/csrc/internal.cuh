@@ -11,9 +11,19 @@
 
 namespace asgk
 {
-// Launch counter (all kernels launched by this library).
+// Launch counter (all kernels launched by this library).  While a thread
+// records a GMRES cycle into a graph its launches run later, so they go to a
+// per-thread tally instead (the solver counts them per executed step).
 extern std::atomic<int64_t> g_launches;
-inline void count_launch(int k = 1) { g_launches.fetch_add(k, std::memory_order_relaxed); }
+extern thread_local bool g_recording;
+extern thread_local int64_t g_recorded_launches;
+inline void count_launch(int64_t k = 1)
+{
+  if (g_recording)
+    g_recorded_launches += k;
+  else
+    g_launches.fetch_add(k, std::memory_order_relaxed);
+}
 
 #define ASGK_CUDA(call)                                                        \
   do                                                                           \
