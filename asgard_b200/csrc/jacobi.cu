@@ -10,14 +10,24 @@
 //   factors, built and inverted on the device (Gauss-Jordan, partial
 //   pivoting, one CTA per cell) and applied as a batched block product.  A
 //   cell-local map that contains the point preconditioner as its diagonal.
+// kron: the same block inverse for global plans whose terms act in one
+//   dimension each, where a cell's diagonal block is the Kronecker sum
+//   (1 - dt n_identity) I - dt sum_k (I (x) B_k (x) I) of its 3x3 self
+//   blocks B_k: with B_k = V_k diag(lambda_k) V_k^-1 (eigendecompositions on
+//   the host, one per 1D cell and dimension) the inverse is
+//   (x)_k V_k diag(1 / mu) (x)_k V_k^-1, mu = (1 - dt n_identity)
+//   - dt sum_k lambda_k,i_k, applied in 2d complex contractions per cell
+//   from a few hundred bytes of tables instead of the n^d x n^d inverse.
 #include "internal.cuh"
 
 #include <cuda_fp16.h>
 
 #include <algorithm>
 #include <cmath>
+#include <complex>
 #include <memory>
 #include <new>
+#include <vector>
 
 namespace asgk
 {
@@ -304,6 +314,327 @@ __global__ void k_point_apply(int64_t n, const double *__restrict__ inv_diag,
   }
 }
 
+// ---- Kronecker-sum block inverse -------------------------------------------
+// Table entry of one (1D cell, dimension): V (3x3), W = V^-1 (3x3), column-
+// major, then the 3 eigenvalues; complex values as (re, im) pairs.
+constexpr int kKronTab = 42;
+
+constexpr int ipow3j(int k) { return k == 0 ? 1 : 3 * ipow3j(k - 1); }
+
+// One warp per cell: u = v (scaled by scale_state[1] in place first when
+// given), u <- (I (x) W_k (x) I) u for every k, u_i /= mu_i,
+// u <- (I (x) V_k (x) I) u for every k, z = Re u.  The cell's D tables are
+// staged in shared memory and the loops over dimensions unrolled; a stage
+// gives each lane whole fibres (three loads, nine complex multiply-adds,
+// three stores).  Shared memory per warp: 2 buffers x (re, im) x 3^D values,
+// then D tables.
+template<typename R, int D, int WPC>
+__global__ void __launch_bounds__(WPC * 32)
+    k_kron_apply(int rows, const int *__restrict__ kself,
+                 const R *__restrict__ tab, double shift, double dt,
+                 double *__restrict__ v, double *__restrict__ z,
+                 const double *__restrict__ scale_state)
+{
+  constexpr int TS  = ipow3j(D);
+  constexpr int PER = (TS + 31) / 32;
+  constexpr int WS  = 4 * TS + D * kKronTab; // per-warp shared values
+  // up to four entries per lane keep their digits in registers; more (d >= 5)
+  // divide by the compile-time strides instead
+  constexpr bool KEEP = PER <= 4;
+  constexpr int PD    = KEEP ? PER : 1;
+  extern __shared__ __align__(16) unsigned char kron_smem[];
+  int const warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int const c    = blockIdx.x * WPC + warp;
+  if (c >= rows)
+    return;
+  R *base = reinterpret_cast<R *>(kron_smem) + int64_t(warp) * WS;
+  R *bufr[2] = {base, base + 2 * TS};
+  R *bufi[2] = {base + TS, base + 3 * TS};
+  R *tabs    = base + 4 * TS; // [D][kKronTab]
+  for (int e = lane; e < D * kKronTab; e += 32)
+  {
+    int const k = e / kKronTab;
+    tabs[e]     = tab[(int64_t(kself[int64_t(c) * D + k]) * D + k) * kKronTab +
+                  (e - k * kKronTab)];
+  }
+  double const f = scale_state ? scale_state[1] : 1.0;
+  unsigned dig[PD]; // base-3 digits, two bits per dimension, dim 0 highest
+  auto digit = [&](int o, int i, int k) -> int {
+    if constexpr (KEEP)
+      return int((dig[o] >> (2 * k)) & 3u);
+    else
+      return (i / ipow3j(D - 1 - k)) % 3;
+  };
+#pragma unroll
+  for (int o = 0; o < PD; o++)
+  {
+    int t       = lane + 32 * o;
+    unsigned pk = 0;
+#pragma unroll
+    for (int k = D - 1; k >= 0; k--)
+    {
+      pk |= unsigned(t % 3) << (2 * k);
+      t /= 3;
+    }
+    dig[o] = pk;
+  }
+#pragma unroll(KEEP ? PER : 1)
+  for (int o = 0; o < PER; o++)
+  {
+    int const i = lane + 32 * o;
+    if (i < TS)
+    {
+      double vv = v[int64_t(c) * TS + i];
+      if (scale_state)
+      {
+        vv                     = vv * f;
+        v[int64_t(c) * TS + i] = vv;
+      }
+      bufr[0][i] = R(vv);
+      bufi[0][i] = R(0);
+    }
+  }
+  __syncwarp();
+  int cur = 0;
+  // out = (I (x) M (x) I) in along dimension k, M column-major complex: lane
+  // f takes fibre f along k (the three entries that differ only in their
+  // k-th index), so every input is read once and M sits in registers
+  auto stage = [&](int k, int st, int moff) {
+    constexpr int NF = TS / 3;
+    const R *mp      = tabs + k * kKronTab + moff;
+    R mr[9], mi[9];
+#pragma unroll
+    for (int e = 0; e < 9; e++)
+    {
+      mr[e] = mp[2 * e];
+      mi[e] = mp[2 * e + 1];
+    }
+    const R *ir = bufr[cur], *ii = bufi[cur];
+    R *orr = bufr[cur ^ 1], *oi = bufi[cur ^ 1];
+#pragma unroll(NF <= 32 ? 1 : 2)
+    for (int fb = lane; fb < NF; fb += 32)
+    {
+      int const b0 = (fb / st) * 3 * st + (fb % st);
+      R xr[3], xi[3];
+#pragma unroll
+      for (int pp = 0; pp < 3; pp++)
+      {
+        xr[pp] = ir[b0 + pp * st];
+        xi[pp] = ii[b0 + pp * st];
+      }
+#pragma unroll
+      for (int q = 0; q < 3; q++)
+      {
+        R yr = R(0), yi = R(0);
+#pragma unroll
+        for (int pp = 0; pp < 3; pp++)
+        {
+          yr += mr[q + 3 * pp] * xr[pp] - mi[q + 3 * pp] * xi[pp];
+          yi += mr[q + 3 * pp] * xi[pp] + mi[q + 3 * pp] * xr[pp];
+        }
+        orr[b0 + q * st] = yr;
+        oi[b0 + q * st]  = yi;
+      }
+    }
+    cur ^= 1;
+    __syncwarp();
+  };
+#pragma unroll
+  for (int k = 0; k < D; k++)
+    stage(k, ipow3j(D - 1 - k), 18); // W_k
+  {
+    R const sh = R(shift), mdt = R(-dt);
+    R *ur = bufr[cur], *ui = bufi[cur];
+#pragma unroll(KEEP ? PER : 1)
+    for (int o = 0; o < PER; o++)
+    {
+      int const i = lane + 32 * o;
+      if (i < TS)
+      {
+        R mr = sh, mi = R(0);
+#pragma unroll
+        for (int k = 0; k < D; k++)
+        {
+          int const q = digit(o, i, k);
+          mr += mdt * tabs[k * kKronTab + 36 + 2 * q];
+          mi += mdt * tabs[k * kKronTab + 37 + 2 * q];
+        }
+        R const den = mr * mr + mi * mi;
+        R const xr = ur[i], xi = ui[i];
+        ur[i] = (xr * mr + xi * mi) / den;
+        ui[i] = (xi * mr - xr * mi) / den;
+      }
+    }
+    __syncwarp();
+  }
+#pragma unroll
+  for (int k = 0; k < D; k++)
+    stage(k, ipow3j(D - 1 - k), 0); // V_k
+  for (int o = 0; o < PER; o++)
+  {
+    int const i = lane + 32 * o;
+    if (i < TS)
+      z[int64_t(c) * TS + i] = double(bufr[cur][i]);
+  }
+}
+
+template<typename R, int D>
+int launch_kron_apply(int rows, const int *kself, const R *tab, double shift,
+                      double dt, double *v, double *z, const double *sc,
+                      cudaStream_t s)
+{
+  constexpr int TS  = ipow3j(D);
+  constexpr int WPC = TS <= 81 ? 4 : 2;
+  size_t const shm  = size_t(WPC) * (4 * TS + D * kKronTab) * sizeof(R);
+  auto kern         = k_kron_apply<R, D, WPC>;
+  if (shm > 48 * 1024)
+    ASGK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   int(shm)));
+  kern<<<(rows + WPC - 1) / WPC, WPC * 32, shm, s>>>(rows, kself, tab, shift, dt,
+                                                   v, z, sc);
+  ASGK_LAUNCHED();
+  return ASGK_OK;
+}
+
+template<typename R>
+int kron_apply_r(int d, int rows, const int *kself, const R *tab, double shift,
+                 double dt, double *v, double *z, const double *sc,
+                 cudaStream_t s)
+{
+  switch (d)
+  {
+  case 1: return launch_kron_apply<R, 1>(rows, kself, tab, shift, dt, v, z, sc, s);
+  case 2: return launch_kron_apply<R, 2>(rows, kself, tab, shift, dt, v, z, sc, s);
+  case 3: return launch_kron_apply<R, 3>(rows, kself, tab, shift, dt, v, z, sc, s);
+  case 4: return launch_kron_apply<R, 4>(rows, kself, tab, shift, dt, v, z, sc, s);
+  case 5: return launch_kron_apply<R, 5>(rows, kself, tab, shift, dt, v, z, sc, s);
+  case 6: return launch_kron_apply<R, 6>(rows, kself, tab, shift, dt, v, z, sc, s);
+  default: return ASGK_ERR_UNSUPPORTED;
+  }
+}
+
+using cd = std::complex<double>;
+
+// B V = V diag(lam), W = V^-1, for a real 3x3 b (column-major).  A multiple
+// of the identity (a dimension no term acts in) gives V = W = I.  False when
+// the eigenvalues are not distinct or a check fails (residual, inverse).
+bool eig3(const double *b, cd lam[3], cd V[9], cd W[9])
+{
+  auto A = [&](int i, int j) { return b[i + 3 * j]; };
+  double nb = 0;
+  for (int e = 0; e < 9; e++)
+    nb = std::max(nb, std::fabs(b[e]));
+  bool const scalar = A(1, 0) == 0 && A(2, 0) == 0 && A(0, 1) == 0 &&
+                      A(2, 1) == 0 && A(0, 2) == 0 && A(1, 2) == 0 &&
+                      A(0, 0) == A(1, 1) && A(1, 1) == A(2, 2);
+  if (scalar)
+  {
+    for (int e = 0; e < 9; e++)
+      V[e] = W[e] = cd((e % 4 == 0) ? 1.0 : 0.0);
+    lam[0] = lam[1] = lam[2] = cd(A(0, 0));
+    return true;
+  }
+  // characteristic polynomial x^3 + c2 x^2 + c1 x + c0
+  double const tr = A(0, 0) + A(1, 1) + A(2, 2);
+  double const m  = A(0, 0) * A(1, 1) - A(0, 1) * A(1, 0) + A(0, 0) * A(2, 2) -
+                   A(0, 2) * A(2, 0) + A(1, 1) * A(2, 2) - A(1, 2) * A(2, 1);
+  double const det = A(0, 0) * (A(1, 1) * A(2, 2) - A(1, 2) * A(2, 1)) -
+                     A(0, 1) * (A(1, 0) * A(2, 2) - A(1, 2) * A(2, 0)) +
+                     A(0, 2) * (A(1, 0) * A(2, 1) - A(1, 1) * A(2, 0));
+  double const c2 = -tr, c1 = m, c0 = -det;
+  auto poly = [&](cd x) { return ((x + c2) * x + c1) * x + c0; };
+  auto dpoly = [&](cd x) { return (3.0 * x + 2.0 * c2) * x + c1; };
+  // a real root by bisection on the Cauchy bound, then the quadratic
+  double lo = -(1 + std::max({std::fabs(c2), std::fabs(c1), std::fabs(c0)}));
+  double hi = -lo;
+  for (int it = 0; it < 200; it++)
+  {
+    double const mid = 0.5 * (lo + hi);
+    if (poly(cd(mid)).real() > 0)
+      hi = mid;
+    else
+      lo = mid;
+  }
+  double const r  = 0.5 * (lo + hi);
+  double const q1 = c2 + r, q0 = c1 + r * q1;
+  cd const sq     = std::sqrt(cd(q1 * q1 - 4 * q0));
+  lam[0]          = cd(r);
+  lam[1]          = (-q1 + sq) * 0.5;
+  lam[2]          = (-q1 - sq) * 0.5;
+  for (int e = 0; e < 3; e++) // polish on the cubic
+    for (int it = 0; it < 3; it++)
+    {
+      cd const dp = dpoly(lam[e]);
+      if (std::abs(dp) > 0)
+        lam[e] -= poly(lam[e]) / dp;
+    }
+  double const tiny = 1e-300;
+  for (int e = 0; e < 3; e++)
+    for (int f = e + 1; f < 3; f++)
+      if (std::abs(lam[e] - lam[f]) <= 1e-8 * (nb + tiny))
+        return false;
+  // eigenvectors: the largest cross product of two rows of (A - lam I)
+  for (int e = 0; e < 3; e++)
+  {
+    cd M[3][3];
+    for (int i = 0; i < 3; i++)
+      for (int j = 0; j < 3; j++)
+        M[i][j] = cd(A(i, j)) - ((i == j) ? lam[e] : cd(0));
+    auto cross = [&](int a, int c, cd out[3]) {
+      out[0] = M[a][1] * M[c][2] - M[a][2] * M[c][1];
+      out[1] = M[a][2] * M[c][0] - M[a][0] * M[c][2];
+      out[2] = M[a][0] * M[c][1] - M[a][1] * M[c][0];
+    };
+    cd best[3], cur[3];
+    double bn = -1;
+    int const pr[3][2] = {{0, 1}, {0, 2}, {1, 2}};
+    for (auto const &pq : pr)
+    {
+      cross(pq[0], pq[1], cur);
+      double const nn = std::abs(cur[0]) + std::abs(cur[1]) + std::abs(cur[2]);
+      if (nn > bn)
+      {
+        bn = nn;
+        std::copy(cur, cur + 3, best);
+      }
+    }
+    double const scale = std::sqrt(std::norm(best[0]) + std::norm(best[1]) + std::norm(best[2]));
+    if (!(scale > 1e-12 * (nb * nb + tiny)))
+      return false;
+    for (int i = 0; i < 3; i++)
+      V[i + 3 * e] = best[i] / scale;
+  }
+  // W = V^-1 by the adjugate
+  auto v = [&](int i, int j) { return V[i + 3 * j]; };
+  cd const dv = v(0, 0) * (v(1, 1) * v(2, 2) - v(1, 2) * v(2, 1)) -
+                v(0, 1) * (v(1, 0) * v(2, 2) - v(1, 2) * v(2, 0)) +
+                v(0, 2) * (v(1, 0) * v(2, 1) - v(1, 1) * v(2, 0));
+  if (!(std::abs(dv) > 1e-6)) // unit columns: |det| is a conditioning measure
+    return false;
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++)
+    {
+      int const i1 = (i + 1) % 3, i2 = (i + 2) % 3, j1 = (j + 1) % 3, j2 = (j + 2) % 3;
+      // (V^-1)(j, i) = cofactor(i, j) / det
+      W[j + 3 * i] = (v(i1, j1) * v(i2, j2) - v(i1, j2) * v(i2, j1)) / dv;
+    }
+  // checks: A V = V diag(lam) and W V = I
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++)
+    {
+      cd av = 0, wv = 0;
+      for (int q = 0; q < 3; q++)
+      {
+        av += A(i, q) * v(q, j);
+        wv += W[i + 3 * q] * v(q, j);
+      }
+      if (std::abs(av - v(i, j) * lam[j]) > 1e-10 * (nb + tiny) ||
+          std::abs(wv - cd(i == j ? 1.0 : 0.0)) > 1e-10)
+        return false;
+    }
+  return true;
+}
+
 } // namespace
 
 struct jacobi_data
@@ -317,12 +648,21 @@ struct jacobi_data
   double *M64      = nullptr; // block: rows*ts*ts, column-major per cell
   __half *M16      = nullptr; // applied inside the FP32 solves, ps16 per cell
   int ps16         = 0;       // ts*ts rounded up to a multiple of 8
+  // kron: per (1D cell, dimension) tables, each cell's self connections
+  int d            = 0;
+  double kshift    = 0;       // 1 - dt * (number of identity terms)
+  double *kt64     = nullptr; // [nconn * d][kKronTab]
+  float *kt32      = nullptr;
+  int *kself       = nullptr; // [rows * d]
   int64_t device_bytes = 0;
   ~jacobi_data()
   {
     cudaFree(inv_diag);
     cudaFree(M64);
     cudaFree(M16);
+    cudaFree(kt64);
+    cudaFree(kt32);
+    cudaFree(kself);
   }
 };
 
@@ -330,11 +670,16 @@ int jacobi_build(plan_data const &p, double dt, int kind, jacobi_data &jd)
 {
   if (p.rows != p.cols)
     return ASGK_ERR_INVALID;
-  if (kind != ASGK_JACOBI_POINT && kind != ASGK_JACOBI_BLOCK)
+  if (kind != ASGK_JACOBI_POINT && kind != ASGK_JACOBI_BLOCK &&
+      kind != ASGK_JACOBI_KRON)
     return ASGK_ERR_INVALID;
   int const ts = p.tensor;
   if (kind == ASGK_JACOBI_BLOCK && ts > 81)
     return ASGK_ERR_UNSUPPORTED; // the shared-memory inverse holds ts x 2ts
+  // the Kronecker-sum form needs the global form's per-dimension blocks and
+  // no term acting in several dimensions
+  if (kind == ASGK_JACOBI_KRON && (!p.global || p.gchains > 0 || p.n != 3))
+    return ASGK_ERR_UNSUPPORTED;
   static std::atomic<uint64_t> next_serial{1};
   jd.serial = next_serial.fetch_add(1);
   jd.kind = kind;
@@ -347,6 +692,57 @@ int jacobi_build(plan_data const &p, double dt, int kind, jacobi_data &jd)
   ASGK_CUDA(cudaMemset(err, 0, sizeof(int)));
   // the plan's FP64 factors in the layout its indices address
   const double *vA = p.vA64;
+  if (kind == ASGK_JACOBI_KRON)
+  {
+    // eigendecompositions of every self block (one per 1D cell and
+    // dimension), from the plan's pre-summed per-dimension blocks
+    int const d         = p.d;
+    int64_t const nconn = int64_t(p.g_conn_row.size());
+    std::vector<double> B(size_t(nconn) * d * 10);
+    ASGK_CUDA(cudaMemcpy(B.data(), p.gB64, sizeof(double) * B.size(),
+                         cudaMemcpyDeviceToHost));
+    std::vector<double> t64(size_t(nconn) * d * kKronTab, 0.0);
+    for (int64_t j = 0; j < nconn; j++)
+    {
+      if (p.g_conn_row[j] != p.g_conn_col[j])
+        continue;
+      for (int k = 0; k < d; k++)
+      {
+        cd lam[3], V[9], W[9];
+        if (!eig3(&B[size_t(j * d + k) * 10], lam, V, W))
+          return ASGK_ERR_UNSUPPORTED;
+        double *t = &t64[size_t(j * d + k) * kKronTab];
+        for (int e = 0; e < 9; e++)
+        {
+          t[2 * e]          = V[e].real();
+          t[2 * e + 1]      = V[e].imag();
+          t[18 + 2 * e]     = W[e].real();
+          t[18 + 2 * e + 1] = W[e].imag();
+        }
+        for (int e = 0; e < 3; e++)
+        {
+          t[36 + 2 * e]     = lam[e].real();
+          t[36 + 2 * e + 1] = lam[e].imag();
+        }
+      }
+    }
+    std::vector<float> t32(t64.begin(), t64.end());
+    jd.d      = d;
+    jd.kshift = 1.0 - dt * p.g_identity;
+    ASGK_CUDA(cudaMalloc(&jd.kt64, sizeof(double) * t64.size()));
+    ASGK_CUDA(cudaMalloc(&jd.kt32, sizeof(float) * t32.size()));
+    ASGK_CUDA(cudaMalloc(&jd.kself, sizeof(int) * size_t(p.rows) * d));
+    ASGK_CUDA(cudaMemcpy(jd.kt64, t64.data(), sizeof(double) * t64.size(),
+                         cudaMemcpyHostToDevice));
+    ASGK_CUDA(cudaMemcpy(jd.kt32, t32.data(), sizeof(float) * t32.size(),
+                         cudaMemcpyHostToDevice));
+    // the global plan's pair list holds each cell's own pair, with its self
+    // connection in every dimension
+    ASGK_CUDA(cudaMemcpy(jd.kself, p.idx, sizeof(int) * size_t(p.rows) * d,
+                         cudaMemcpyDeviceToDevice));
+    jd.device_bytes = int64_t(t64.size() * 12 + size_t(p.rows) * d * 4);
+    return ASGK_OK;
+  }
   if (kind == ASGK_JACOBI_POINT)
   {
     size_t const b = sizeof(double) * size_t(p.rows) * ts;
@@ -383,6 +779,14 @@ int jacobi_apply(jacobi_data const &jd, bool low, double *v, double *z,
                  const double *scale_state, cudaStream_t s)
 {
   int64_t const n = int64_t(jd.rows) * jd.ts;
+  if (jd.kind == ASGK_JACOBI_KRON)
+  {
+    if (low)
+      return kron_apply_r<float>(jd.d, jd.rows, jd.kself, jd.kt32, jd.kshift,
+                                 jd.dt, v, z, scale_state, s);
+    return kron_apply_r<double>(jd.d, jd.rows, jd.kself, jd.kt64, jd.kshift,
+                                jd.dt, v, z, scale_state, s);
+  }
   if (jd.kind == ASGK_JACOBI_POINT)
   {
     int const blocks = int(std::min<int64_t>((n + 255) / 256, 4096));

@@ -33,12 +33,15 @@ from ._lib import check, lib
 
 _MAGIC = b"ASGKMLP1"
 
-JACOBI_KINDS = {"point": 0, "block": 1}
+JACOBI_KINDS = {"point": 0, "block": 1, "kron": 2}
 
 
 class JacobiPreconditioner:
     """Point or cell-block Jacobi preconditioner of I - dt*K for a square
-    kronmult_matrix (see asgk_jacobi_create in include/asgard_b200.h)."""
+    kronmult_matrix (see asgk_jacobi_create in include/asgard_b200.h).
+    kind "kron": the cell-block inverse through the eigendecompositions of
+    its one-dimensional factors (global plans whose terms act in one
+    dimension each; raises AsgkError otherwise)."""
 
     def __init__(self, mat, dt, kind="block"):
         if kind not in JACOBI_KINDS:

@@ -280,7 +280,10 @@ int asgk_default_gmres_restarts(int64_t n);
 typedef enum asgk_jacobi_kind
 {
   ASGK_JACOBI_POINT = 0, /* the reference's diagonal preconditioner */
-  ASGK_JACOBI_BLOCK = 1  /* inverse of each cell's n^d x n^d diagonal block */
+  ASGK_JACOBI_BLOCK = 1, /* inverse of each cell's n^d x n^d diagonal block */
+  ASGK_JACOBI_KRON  = 2  /* the same inverse through the eigendecompositions of
+                            the block's 1D factors (global plans whose terms act
+                            in one dimension each; any d <= 6) */
 } asgk_jacobi_kind;
 
 /* Builds a Jacobi preconditioner of I - dt*K for a square plan, on the
@@ -291,7 +294,13 @@ typedef enum asgk_jacobi_kind
  * the reference has it in its global-kron mode only).  ASGK_JACOBI_BLOCK
  * inverts the whole diagonal block (I - dt*sum_t (x)_k A_{t,k}) of every
  * cell (Gauss-Jordan with partial pivoting; n^d <= 81, else
- * ASGK_ERR_UNSUPPORTED); ASGK_ERR_BREAKDOWN if a block is singular.  The
+ * ASGK_ERR_UNSUPPORTED); ASGK_ERR_BREAKDOWN if a block is singular.
+ * ASGK_JACOBI_KRON applies the block inverse of a global plan whose terms
+ * act in one dimension each (there the block is a Kronecker sum of the
+ * cell's 3x3 self blocks): each 3x3 factor is diagonalised on the host and
+ * the inverse applied as 2d complex contractions per cell, O(d n^(d+1))
+ * work and a few hundred bytes of tables per cell; ASGK_ERR_UNSUPPORTED for
+ * other plans or a factor that is defective or badly conditioned.  The
  * preconditioner keeps no reference to the plan. */
 int asgk_jacobi_create(asgk_jacobi **pc, asgk_plan *plan, double dt, int kind);
 void asgk_jacobi_destroy(asgk_jacobi *pc);
