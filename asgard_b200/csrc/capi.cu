@@ -463,7 +463,8 @@ inline void rot(double &x, double &y, double c, double s)
 inline int pos_from_indices(int i, int j) { return i + j * (j + 1) / 2; }
 
 // What a recorded GMRES cycle depends on besides the workspace buffers: the
-// operator (plan, dt, arithmetic), the preconditioner, the restart length.
+// operator (plan, dt, arithmetic), the preconditioner, the restart length,
+// the basis precision of the Gram-Schmidt passes.
 struct graph_key
 {
   const void *plan = nullptr; // the workspace dies with its plan
@@ -471,14 +472,16 @@ struct graph_key
   int precision    = 0;
   uint64_t pc      = 0;       // preconditioner serial (never reused), 0: none
   int restart      = 0;
+  bool low_basis   = false;
   bool operator==(graph_key const &o) const
   {
     return plan == o.plan && dt == o.dt && precision == o.precision &&
-           pc == o.pc && restart == o.restart;
+           pc == o.pc && restart == o.restart && low_basis == o.low_basis;
   }
 };
 
-bool g_gmres_graphs = true; // asgk_set_gmres_graphs
+bool g_gmres_graphs     = true; // asgk_set_gmres_graphs
+bool g_gmres_low_basis  = true; // asgk_set_gmres_basis
 
 // Device workspace of a GMRES solve, kept on the plan between solves.
 struct gmres_ws
@@ -489,6 +492,9 @@ struct gmres_ws
   double *V = nullptr, *Z = nullptr, *part = nullptr, *h = nullptr,
          *y = nullptr, *r = nullptr, *e = nullptr;
   double *hh = nullptr; // pinned host mirror of h
+  // FP32 copy of the basis for the Gram-Schmidt passes of FP32 inner solves
+  // (allocated on first use, n * (m + 1))
+  float *Vf = nullptr;
   // reduction tickets: [0] update-norm, [1] norm, [2..] multi-dot groups
   unsigned *tickets = nullptr;
   int nblocks = 0;
@@ -529,6 +535,8 @@ struct gmres_ws
       cudaFreeHost(hstate);
     hstate = nullptr;
     cudaFree(V);
+    cudaFree(Vf);
+    Vf = nullptr;
     cudaFree(Z);
     cudaFree(part);
     cudaFree(h);
@@ -543,16 +551,22 @@ struct gmres_ws
     N = 0;
     m = 0;
   }
-  int ensure(int64_t n, int restart, bool flex)
+  int ensure(int64_t n, int restart, bool flex, bool low = false)
   {
     if (n == N && restart <= m && (!flex || Z != nullptr))
-      return ASGK_OK;
+    {
+      if (!low || Vf != nullptr)
+        return ASGK_OK;
+      int64_t bytes = 0;
+      return dev_alloc(&Vf, n * (m + 1), bytes);
+    }
     release();
     int64_t bytes = 0;
     nblocks       = max_reduction_blocks_wide();
     int rc;
     if ((rc = dev_alloc(&V, n * (restart + 1), bytes)) ||
         (flex && (rc = dev_alloc(&Z, n * restart, bytes))) ||
+        (low && (rc = dev_alloc(&Vf, n * (restart + 1), bytes))) ||
         (rc = dev_alloc(&part, int64_t(nblocks) * (restart + 2), bytes)) ||
         (rc = dev_alloc(&h, restart + 2, bytes)) ||
         (rc = dev_alloc(&y, restart + 1, bytes)) ||
@@ -595,9 +609,11 @@ struct gmres_ws
 using matvec_t  = std::function<int(double alpha, const double *x, double beta,
                                     double *y, cudaStream_t s)>;
 // (with scale_state, v *= scale_state[1] in place first: a recorded step's
-// normalisation of its basis vector, fused into the preconditioner)
+// normalisation of its basis vector, fused into the preconditioner; with
+// vcopy, also vcopy = FP32(v): the basis copy of an FP32 inner solve)
 using precond_t = std::function<int(double *v, double *z,
-                                    const double *scale_state, cudaStream_t s)>;
+                                    const double *scale_state, float *vcopy,
+                                    cudaStream_t s)>;
 
 struct core_stats
 {
@@ -640,10 +656,12 @@ int norm2(gmres_ws &ws, const double *v, int64_t n, double &out,
 // Records one restart cycle: a chain of `restart` conditional nodes, Arnoldi
 // step i in the body of node i with its basis columns fixed at record time
 // (preconditioner, operator, the two Gram-Schmidt passes, the second ending
-// in the Givens step, and the scaling of the new basis vector, folded into
-// the next step's preconditioner when there is one).  Node 0 always runs; step i's Givens
-// kernel opens node i + 1 only while the cycle goes on, so a cycle runs with
-// no host round trip and stops where the host-driven loop would.
+// in the Givens step, and the scaling of the new basis vector: folded into
+// the next step's preconditioner when there is one, or with an FP32 basis
+// copy (low) a kernel that scales and writes the copy).  Node 0 always runs;
+// step i's Givens kernel opens node i + 1 only while the cycle goes on, so a
+// cycle runs with no host round trip and stops where the host-driven loop
+// would.
 int record_cycle(gmres_ws &ws, int64_t n, matvec_t const &mat,
                  precond_t const *pc, int restart, gmres_ws::cycle_graph &out)
 {
@@ -651,6 +669,7 @@ int record_cycle(gmres_ws &ws, int64_t n, matvec_t const &mat,
       cudaStreamCreateWithFlags(&ws.capture, cudaStreamNonBlocking) != cudaSuccess)
     return ASGK_ERR_CUDA;
   cudaStream_t const cs = ws.capture;
+  bool const low        = out.key.low_basis;
   cudaGraph_t graph     = nullptr;
   if (cudaGraphCreate(&graph, 0) != cudaSuccess)
     return ASGK_ERR_CUDA;
@@ -692,16 +711,18 @@ int record_cycle(gmres_ws &ws, int64_t n, matvec_t const &mat,
     if (pc)
     {
       // the preconditioner also normalises v_i (step i-1 left 1/||w|| in the
-      // state; v_0 was normalised before the cycle)
+      // state; v_0 was normalised before the cycle) and writes its FP32 copy
       double *zi = ws.Z + int64_t(i) * n;
-      rc         = (*pc)(vi, zi, i > 0 ? ws.dstate : nullptr, cs);
+      rc         = (*pc)(vi, zi, i > 0 ? ws.dstate : nullptr,
+                         (i > 0 && low) ? ws.Vf + int64_t(i) * n : nullptr, cs);
       if (rc == ASGK_OK)
         rc = mat(1.0, zi, 0.0, w, cs);
     }
     else
       rc = mat(1.0, vi, 0.0, w, cs);
     if (rc == ASGK_OK)
-      rc = launch_multidot_h(ws.V, n, k, w, n, ws.part, ws.tickets + 2, ws.h, cs);
+      rc = low ? launch_multidot_hf(ws.Vf, n, k, w, n, ws.part, ws.tickets + 2, ws.h, cs)
+               : launch_multidot_h(ws.V, n, k, w, n, ws.part, ws.tickets + 2, ws.h, cs);
     if (rc == ASGK_OK)
     {
       givens_args ga;
@@ -710,13 +731,17 @@ int record_cycle(gmres_ws &ws, int64_t n, matvec_t const &mat,
       ga.restart  = restart;
       ga.has_next = (i + 1 < restart) ? 1 : 0;
       ga.next     = ga.has_next ? hs[i + 1] : hs[i];
-      rc = launch_update_norm_h(ws.V, n, k, ws.h, w, n, ws.part, ws.tickets,
-                                ws.h + k, cs, &ga);
+      rc = low ? launch_update_norm_hf(ws.Vf, n, k, ws.h, w, n, ws.part, ws.tickets,
+                                       ws.h + k, cs, &ga)
+               : launch_update_norm_h(ws.V, n, k, ws.h, w, n, ws.part, ws.tickets,
+                                      ws.h + k, cs, &ga);
     }
-    // without a preconditioner to fold it into, w is normalised here (the
-    // last step's w is never read: the solution update uses v_0..v_{k-1})
+    // without a preconditioner to fold it into, w is normalised here, with
+    // its FP32 copy when there is one (the last step's w is never read: the
+    // solution update uses v_0..v_{k-1})
     if (rc == ASGK_OK && !pc)
-      rc = launch_scale_by(w, n, ws.dstate, cs);
+      rc = low ? launch_store_basis(w, ws.Vf + int64_t(i + 1) * n, n, ws.dstate, 0.0, cs)
+               : launch_scale_by(w, n, ws.dstate, cs);
     cudaGraph_t captured = nullptr;
     if (cudaStreamEndCapture(cs, &captured) != cudaSuccess && rc == ASGK_OK)
       rc = ASGK_ERR_CUDA;
@@ -786,10 +811,12 @@ gmres_ws::cycle_graph const *cycle_graph_for(gmres_ws &ws, int64_t n,
 int gmres_core(gmres_ws &ws, int64_t n, matvec_t const &mat,
                precond_t const *pc, double *x, const double *b, int restart,
                int max_outer, double tol, core_stats &st, cudaStream_t s,
-               bool verify = false, graph_key const *gk = nullptr)
+               bool verify = false, graph_key const *gk = nullptr,
+               bool low_basis = false)
 {
   bool const flex = (pc != nullptr);
-  if (int rc = ws.ensure(n, restart, flex))
+  bool const low  = (gk != nullptr) ? gk->low_basis : low_basis;
+  if (int rc = ws.ensure(n, restart, flex, low))
     return rc;
   std::vector<double> proj(size_t(restart) * (restart + 1) / 2, 0.0);
   std::vector<double> sines(restart + 1, 0.0), cosines(restart + 1, 0.0),
@@ -827,7 +854,8 @@ int gmres_core(gmres_ws &ws, int64_t n, matvec_t const &mat,
       break;
     }
     cycle_start = inner_res;
-    if (int rc = launch_scale(r0, n, 1.0 / inner_res, s))
+    if (int rc = low ? launch_store_basis(r0, ws.Vf, n, nullptr, 1.0 / inner_res, s)
+                     : launch_scale(r0, n, 1.0 / inner_res, s))
       return rc;
     ksol[0] = inner_res;
     int inner = 0;
@@ -871,7 +899,7 @@ int gmres_core(gmres_ws &ws, int64_t n, matvec_t const &mat,
       if (flex)
       {
         double *zi = ws.Z + int64_t(inner) * n;
-        if (int rc = (*pc)(vi, zi, nullptr, s))
+        if (int rc = (*pc)(vi, zi, nullptr, nullptr, s))
           return rc;
         ++st.pcalls;
         if (int rc = mat(1.0, zi, 0.0, w, s))
@@ -882,11 +910,15 @@ int gmres_core(gmres_ws &ws, int64_t n, matvec_t const &mat,
       ++st.total;
       ++st.matvecs;
       int const k = inner + 1;
-      if (int rc = launch_multidot_h(ws.V, n, k, w, n, ws.part, ws.tickets + 2,
-                                     ws.h, s))
+      if (int rc = low ? launch_multidot_hf(ws.Vf, n, k, w, n, ws.part,
+                                            ws.tickets + 2, ws.h, s)
+                       : launch_multidot_h(ws.V, n, k, w, n, ws.part,
+                                           ws.tickets + 2, ws.h, s))
         return rc;
-      if (int rc = launch_update_norm_h(ws.V, n, k, ws.h, w, n, ws.part,
-                                        ws.tickets, ws.h + k, s))
+      if (int rc = low ? launch_update_norm_hf(ws.Vf, n, k, ws.h, w, n, ws.part,
+                                               ws.tickets, ws.h + k, s)
+                       : launch_update_norm_h(ws.V, n, k, ws.h, w, n, ws.part,
+                                              ws.tickets, ws.h + k, s))
         return rc;
       ASGK_CUDA(cudaMemcpyAsync(ws.hh, ws.h, sizeof(double) * (k + 1),
                                 cudaMemcpyDeviceToHost, s));
@@ -899,7 +931,9 @@ int gmres_core(gmres_ws &ws, int64_t n, matvec_t const &mat,
         return ASGK_OK;
       }
       if (nrm > 0)
-        if (int rc = launch_scale(w, n, 1.0 / nrm, s))
+        if (int rc = low ? launch_store_basis(w, ws.Vf + int64_t(inner + 1) * n, n,
+                                              nullptr, 1.0 / nrm, s)
+                         : launch_scale(w, n, 1.0 / nrm, s))
           return rc;
       double *coeffs = proj.data() + pos_from_indices(0, inner);
       for (int j = 0; j < k; j++)
@@ -2109,11 +2143,14 @@ int gmres_euler_impl(asgk_plan *plan, double dt, double *x, const double *b,
       core_stats ist;
       double const itol = std::max(inner_rtol * rnorm, 0.5 * tol_abs);
       int const inner_outer = std::max(1, max_outer);
-      graph_key const gk{plan, dt, precision, use_pc ? pc_serial : 0, restart};
+      // FP32 inner solves: Gram-Schmidt over an FP32 copy of the basis
+      bool const low_basis = (precision != ASGK_FP64) && g_gmres_low_basis;
+      graph_key const gk{plan, dt, precision, use_pc ? pc_serial : 0, restart,
+                         low_basis};
       bool const recordable = (use_pc == nullptr || pc_graph_ok);
       if (int rc = gmres_core(ws, n, (precision == ASGK_FP64) ? matvec_t(op64) : matvec_t(oplow),
                               use_pc, ws.e, ws.r, restart, inner_outer, itol, ist, s,
-                              false, recordable ? &gk : nullptr))
+                              false, recordable ? &gk : nullptr, low_basis))
         return rc;
       total += ist.total;
       if (precision == ASGK_FP64)
@@ -2190,9 +2227,16 @@ int asgk_gmres_euler(asgk_plan *plan, double dt, double *x, const double *b,
                               precision, nullptr, info, stream);
     cudaStream_t s = as_stream(stream);
     make_pc_t const mk = [&](bool low) -> precond_t {
-      return [=](double *v, double *z, const double *sc, cudaStream_t ss) -> int {
-        if (sc)
-          if (int rc = launch_scale_by(v, int64_t(plan->p.rows) * plan->p.tensor, sc, ss))
+      return [=](double *v, double *z, const double *sc, float *vc,
+                 cudaStream_t ss) -> int {
+        int64_t const nn = int64_t(plan->p.rows) * plan->p.tensor;
+        if (vc)
+        {
+          if (int rc = launch_store_basis(v, vc, nn, sc, 1.0, ss))
+            return rc;
+        }
+        else if (sc)
+          if (int rc = launch_scale_by(v, nn, sc, ss))
             return rc;
         return mlp_precondition(precond, plan, v, z, ss, low);
       };
@@ -2222,8 +2266,9 @@ int asgk_gmres_euler_jacobi(asgk_plan *plan, double dt, double *x,
       return ASGK_ERR_INVALID;
     cudaStream_t s = as_stream(stream);
     make_pc_t const mk = [&](bool low) -> precond_t {
-      return [=](double *v, double *z, const double *sc, cudaStream_t ss) -> int {
-        return jacobi_apply_handle(precond, low, v, z, sc, ss);
+      return [=](double *v, double *z, const double *sc, float *vc,
+                 cudaStream_t ss) -> int {
+        return jacobi_apply_handle(precond, low, v, z, sc, vc, ss);
       };
     };
     return gmres_euler_impl(plan, dt, x, b, restart, max_outer, tol, tol_mode,
@@ -2244,6 +2289,13 @@ int asgk_set_gmres_graphs(int enable)
 {
   int const old  = g_gmres_graphs ? 1 : 0;
   g_gmres_graphs = (enable != 0);
+  return old;
+}
+
+int asgk_set_gmres_basis(int fp32)
+{
+  int const old     = g_gmres_low_basis ? 1 : 0;
+  g_gmres_low_basis = (fp32 != 0);
   return old;
 }
 

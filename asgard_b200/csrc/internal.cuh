@@ -177,11 +177,13 @@ int launch_fill_pairs(int d, int cells, const int *oned, const int *cand,
 // jacobi.cu
 struct jacobi_data;
 // z = M v; with scale_state, v *= scale_state[1] in place first (the
-// normalisation of a recorded GMRES step's new basis vector, fused)
+// normalisation of a recorded GMRES step's new basis vector, fused), and
+// with vcopy also vcopy = FP32(v) (the basis copy of FP32 inner solves)
 int jacobi_apply(jacobi_data const &jd, bool low, double *v, double *z,
-                 const double *scale_state, cudaStream_t s);
+                 const double *scale_state, float *vcopy, cudaStream_t s);
 int jacobi_apply_handle(asgk_jacobi *pc, bool low, double *v, double *z,
-                        const double *scale_state, cudaStream_t s);
+                        const double *scale_state, float *vcopy,
+                        cudaStream_t s);
 // never reused within a process: identifies a preconditioner in caches
 uint64_t jacobi_serial(const asgk_jacobi *pc);
 
@@ -219,6 +221,17 @@ int launch_update_norm_h(const double *V, int64_t ldv, int k, const double *h,
                          givens_args const *ga = nullptr);
 int launch_norm2_h(const double *v, int64_t n, double *part, unsigned *ticket,
                    double *out, cudaStream_t s);
+// the same two passes over an FP32 copy of the basis (w, h, sums FP64)
+int launch_multidot_hf(const float *V, int64_t ldv, int k, const double *w,
+                       int64_t n, double *part, unsigned *tickets, double *h,
+                       cudaStream_t s);
+int launch_update_norm_hf(const float *V, int64_t ldv, int k, const double *h,
+                          double *w, int64_t n, double *part, unsigned *ticket,
+                          double *out, cudaStream_t s,
+                          givens_args const *ga = nullptr);
+// w *= f, vf = FP32(w); f = state[1] when state is set, else scale
+int launch_store_basis(double *w, float *vf, int64_t n, const double *state,
+                       double scale, cudaStream_t s);
 // v *= state[1], the scale a recorded GMRES step computed on the device
 int launch_scale_by(double *v, int64_t n, const double *state, cudaStream_t s);
 int launch_xpby(double *y, const double *x, int64_t n, double beta,

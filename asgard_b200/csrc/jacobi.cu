@@ -202,7 +202,8 @@ template<typename TM>
 __global__ void k_block_apply(int rows, int ts, const TM *__restrict__ M,
                               double *__restrict__ v,
                               double *__restrict__ z,
-                              const double *__restrict__ scale_state)
+                              const double *__restrict__ scale_state,
+                              float *__restrict__ vcopy)
 {
   extern __shared__ double vs[];
   int const row = blockIdx.x;
@@ -214,6 +215,8 @@ __global__ void k_block_apply(int rows, int ts, const TM *__restrict__ M,
       double const vv          = v[int64_t(row) * ts + i] * f;
       v[int64_t(row) * ts + i] = vv;
       vs[i]                    = vv;
+      if (vcopy)
+        vcopy[int64_t(row) * ts + i] = float(vv);
     }
   }
   else
@@ -242,7 +245,8 @@ constexpr int kApply16Loads   = 8; // 16-byte loads per thread: ps <= 8192
 __global__ void __launch_bounds__(kApply16Threads)
     k_block_apply16(int ts, int ps, const __half *__restrict__ M,
                     double *__restrict__ v, double *__restrict__ z,
-                    const double *__restrict__ scale_state)
+                    const double *__restrict__ scale_state,
+                    float *__restrict__ vcopy)
 {
   extern __shared__ __align__(16) unsigned char smem16[];
   __half *Ms = reinterpret_cast<__half *>(smem16);
@@ -266,6 +270,8 @@ __global__ void __launch_bounds__(kApply16Threads)
       double const vv          = v[int64_t(row) * ts + i] * f;
       v[int64_t(row) * ts + i] = vv;
       vs[i]                    = static_cast<float>(vv);
+      if (vcopy)
+        vcopy[int64_t(row) * ts + i] = static_cast<float>(vv);
     }
   }
   else
@@ -298,7 +304,8 @@ __global__ void __launch_bounds__(kApply16Threads)
 __global__ void k_point_apply(int64_t n, const double *__restrict__ inv_diag,
                               double *__restrict__ v,
                               double *__restrict__ z,
-                              const double *__restrict__ scale_state)
+                              const double *__restrict__ scale_state,
+                              float *__restrict__ vcopy)
 {
   double const f = scale_state ? scale_state[1] : 1.0;
   for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n;
@@ -309,6 +316,8 @@ __global__ void k_point_apply(int64_t n, const double *__restrict__ inv_diag,
     {
       vv   = vv * f;
       v[i] = vv;
+      if (vcopy)
+        vcopy[i] = float(vv);
     }
     z[i] = vv * inv_diag[i];
   }
@@ -322,7 +331,7 @@ constexpr int kKronTab = 42;
 constexpr int ipow3j(int k) { return k == 0 ? 1 : 3 * ipow3j(k - 1); }
 
 // One warp per cell: u = v (scaled by scale_state[1] in place first when
-// given), u <- (I (x) W_k (x) I) u for every k, u_i /= mu_i,
+// given, and then also written rounded to FP32 into vcopy when given), u <- (I (x) W_k (x) I) u for every k, u_i /= mu_i,
 // u <- (I (x) V_k (x) I) u for every k, z = Re u.  The cell's D tables are
 // staged in shared memory and the loops over dimensions unrolled; a stage
 // gives each lane whole fibres (three loads, nine complex multiply-adds,
@@ -333,7 +342,8 @@ __global__ void __launch_bounds__(WPC * 32)
     k_kron_apply(int rows, const int *__restrict__ kself,
                  const R *__restrict__ tab, double shift, double dt,
                  double *__restrict__ v, double *__restrict__ z,
-                 const double *__restrict__ scale_state)
+                 const double *__restrict__ scale_state,
+                 float *__restrict__ vcopy)
 {
   constexpr int TS  = ipow3j(D);
   constexpr int PER = (TS + 31) / 32;
@@ -389,6 +399,8 @@ __global__ void __launch_bounds__(WPC * 32)
       {
         vv                     = vv * f;
         v[int64_t(c) * TS + i] = vv;
+        if (vcopy)
+          vcopy[int64_t(c) * TS + i] = float(vv);
       }
       bufr[0][i] = R(vv);
       bufi[0][i] = R(0);
@@ -481,7 +493,7 @@ __global__ void __launch_bounds__(WPC * 32)
 template<typename R, int D>
 int launch_kron_apply(int rows, const int *kself, const R *tab, double shift,
                       double dt, double *v, double *z, const double *sc,
-                      cudaStream_t s)
+                      float *vc, cudaStream_t s)
 {
   constexpr int TS  = ipow3j(D);
   constexpr int WPC = TS <= 81 ? 4 : 2;
@@ -491,7 +503,7 @@ int launch_kron_apply(int rows, const int *kself, const R *tab, double shift,
     ASGK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    int(shm)));
   kern<<<(rows + WPC - 1) / WPC, WPC * 32, shm, s>>>(rows, kself, tab, shift, dt,
-                                                   v, z, sc);
+                                                   v, z, sc, vc);
   ASGK_LAUNCHED();
   return ASGK_OK;
 }
@@ -499,16 +511,16 @@ int launch_kron_apply(int rows, const int *kself, const R *tab, double shift,
 template<typename R>
 int kron_apply_r(int d, int rows, const int *kself, const R *tab, double shift,
                  double dt, double *v, double *z, const double *sc,
-                 cudaStream_t s)
+                 float *vc, cudaStream_t s)
 {
   switch (d)
   {
-  case 1: return launch_kron_apply<R, 1>(rows, kself, tab, shift, dt, v, z, sc, s);
-  case 2: return launch_kron_apply<R, 2>(rows, kself, tab, shift, dt, v, z, sc, s);
-  case 3: return launch_kron_apply<R, 3>(rows, kself, tab, shift, dt, v, z, sc, s);
-  case 4: return launch_kron_apply<R, 4>(rows, kself, tab, shift, dt, v, z, sc, s);
-  case 5: return launch_kron_apply<R, 5>(rows, kself, tab, shift, dt, v, z, sc, s);
-  case 6: return launch_kron_apply<R, 6>(rows, kself, tab, shift, dt, v, z, sc, s);
+  case 1: return launch_kron_apply<R, 1>(rows, kself, tab, shift, dt, v, z, sc, vc, s);
+  case 2: return launch_kron_apply<R, 2>(rows, kself, tab, shift, dt, v, z, sc, vc, s);
+  case 3: return launch_kron_apply<R, 3>(rows, kself, tab, shift, dt, v, z, sc, vc, s);
+  case 4: return launch_kron_apply<R, 4>(rows, kself, tab, shift, dt, v, z, sc, vc, s);
+  case 5: return launch_kron_apply<R, 5>(rows, kself, tab, shift, dt, v, z, sc, vc, s);
+  case 6: return launch_kron_apply<R, 6>(rows, kself, tab, shift, dt, v, z, sc, vc, s);
   default: return ASGK_ERR_UNSUPPORTED;
   }
 }
@@ -776,21 +788,21 @@ int jacobi_build(plan_data const &p, double dt, int kind, jacobi_data &jd)
 }
 
 int jacobi_apply(jacobi_data const &jd, bool low, double *v, double *z,
-                 const double *scale_state, cudaStream_t s)
+                 const double *scale_state, float *vcopy, cudaStream_t s)
 {
   int64_t const n = int64_t(jd.rows) * jd.ts;
   if (jd.kind == ASGK_JACOBI_KRON)
   {
     if (low)
       return kron_apply_r<float>(jd.d, jd.rows, jd.kself, jd.kt32, jd.kshift,
-                                 jd.dt, v, z, scale_state, s);
+                                 jd.dt, v, z, scale_state, vcopy, s);
     return kron_apply_r<double>(jd.d, jd.rows, jd.kself, jd.kt64, jd.kshift,
-                                jd.dt, v, z, scale_state, s);
+                                jd.dt, v, z, scale_state, vcopy, s);
   }
   if (jd.kind == ASGK_JACOBI_POINT)
   {
     int const blocks = int(std::min<int64_t>((n + 255) / 256, 4096));
-    k_point_apply<<<blocks, 256, 0, s>>>(n, jd.inv_diag, v, z, scale_state);
+    k_point_apply<<<blocks, 256, 0, s>>>(n, jd.inv_diag, v, z, scale_state, vcopy);
     ASGK_LAUNCHED();
     return ASGK_OK;
   }
@@ -800,14 +812,14 @@ int jacobi_apply(jacobi_data const &jd, bool low, double *v, double *z,
       return ASGK_ERR_UNSUPPORTED;
     size_t const shm = sizeof(__half) * jd.ps16 + sizeof(float) * jd.ts;
     k_block_apply16<<<jd.rows, kApply16Threads, shm, s>>>(jd.ts, jd.ps16, jd.M16, v, z,
-                                                          scale_state);
+                                                          scale_state, vcopy);
   }
   else
   {
     int const threads = jd.ts <= 32 ? 32 : (jd.ts <= 64 ? 64 : 128);
     size_t const shm  = sizeof(double) * jd.ts;
     k_block_apply<double><<<jd.rows, threads, shm, s>>>(jd.rows, jd.ts, jd.M64, v, z,
-                                                        scale_state);
+                                                        scale_state, vcopy);
   }
   ASGK_LAUNCHED();
   return ASGK_OK;
@@ -856,7 +868,7 @@ int asgk_jacobi_apply(asgk_jacobi *pc, const double *v, double *z,
       return ASGK_ERR_INVALID;
     // without a scale state v is only read
     return asgk::jacobi_apply(pc->jd, false, const_cast<double *>(v), z, nullptr,
-                              static_cast<cudaStream_t>(stream));
+                              nullptr, static_cast<cudaStream_t>(stream));
   }
   catch (std::bad_alloc const &)
   {
@@ -871,9 +883,10 @@ int asgk_jacobi_apply(asgk_jacobi *pc, const double *v, double *z,
 uint64_t asgk::jacobi_serial(const asgk_jacobi *pc) { return pc ? pc->jd.serial : 0; }
 
 int asgk::jacobi_apply_handle(asgk_jacobi *pc, bool low, double *v, double *z,
-                              const double *scale_state, cudaStream_t s)
+                              const double *scale_state, float *vcopy,
+                              cudaStream_t s)
 {
-  return asgk::jacobi_apply(pc->jd, low, v, z, scale_state, s);
+  return asgk::jacobi_apply(pc->jd, low, v, z, scale_state, vcopy, s);
 }
 
 int asgk_jacobi_info(asgk_jacobi *pc, int *kind, double *dt,

@@ -274,6 +274,36 @@ __device__ __forceinline__ bool last_block(unsigned *ticket, unsigned nblocks)
   return s_last != 0;
 }
 
+// The end of an update pass: this block's partial of ||w||^2, the ordered
+// total from the last block, then (ga.state set: a recorded GMRES step) the
+// step's Givens update: earlier rotations staged in shared memory after the
+// k coefficients, then one thread (the serial part touches shared memory
+// only).
+__device__ __forceinline__ void finish_update(double (&v)[1], double *sh,
+                                              double *hs, int k, double *part,
+                                              unsigned *ticket, double *out,
+                                              givens_args const &ga)
+{
+  block_sum<1>(v, sh);
+  if (threadIdx.x == 0)
+    part[blockIdx.x] = v[0];
+  if (!last_block(ticket, gridDim.x))
+    return;
+  ordered_column_sums(part, gridDim.x, 1, 0, 1, out);
+  if (threadIdx.x == 0)
+    *ticket = 0u;
+  if (ga.state == nullptr)
+    return;
+  double *csn    = hs + k;                     // cosines, sines: 2*(restart+1)
+  double *coeffs = csn + 2 * (ga.restart + 1); // k
+  const double *cs_g = ga.state + kStateHead + ga.restart + 1;
+  for (int j = threadIdx.x; j < 2 * (ga.restart + 1); j += blockDim.x)
+    csn[j] = (j % (ga.restart + 1) < ga.step) ? cs_g[j] : 0.0;
+  __syncthreads();
+  if (threadIdx.x == 0)
+    givens_step(ga, hs, *out, coeffs, csn);
+}
+
 template<int VEC> struct vload;
 template<> struct vload<1>
 {
@@ -416,26 +446,199 @@ __global__ void __launch_bounds__(kThreads)
       v[0] += wr.x * wr.x + wr.y * wr.y;
     }
   }
-  block_sum<1>(v, sh);
+  finish_update(v, sh, hs, k, part, ticket, out, ga);
+}
+
+// ---- the same two passes over an FP32 copy of the basis -----------------
+//
+// In the FP32 inner solves of iterative refinement the basis columns used
+// by Gram-Schmidt are stored in FP32 beside the FP64 ones (which the
+// operator and the solution update keep reading): the two passes move half
+// the bytes, and a 50-column basis of the benchmark sizes stays in L2.  w,
+// h and all sums stay FP64.  VEC = 4 reads four rows per 16-byte load (n
+// and the leading dimension multiples of 4, 16-byte aligned vectors).
+
+template<int VEC> struct fload;
+template<> struct fload<1>
+{
+  using T = float;
+};
+template<> struct fload<4>
+{
+  using T = float4;
+};
+__device__ __forceinline__ double fcomp(float a, int) { return double(a); }
+__device__ __forceinline__ double fcomp(float4 const &a, int e)
+{
+  return double(e == 0 ? a.x : e == 1 ? a.y : e == 2 ? a.z : a.w);
+}
+
+// rows VEC*r .. VEC*r + VEC - 1 of w
+template<int VEC>
+__device__ __forceinline__ void load_rows(const double *w, int64_t r, double (&o)[VEC])
+{
+  if constexpr (VEC == 1)
+    o[0] = w[r];
+  else
+  {
+    const double2 *p = reinterpret_cast<const double2 *>(w) + r * (VEC / 2);
+#pragma unroll
+    for (int q = 0; q < VEC / 2; q++)
+    {
+      double2 const t = p[q];
+      o[2 * q]        = t.x;
+      o[2 * q + 1]    = t.y;
+    }
+  }
+}
+template<int VEC>
+__device__ __forceinline__ void store_rows(double *w, int64_t r, double const (&o)[VEC])
+{
+  if constexpr (VEC == 1)
+    w[r] = o[0];
+  else
+  {
+    double2 *p = reinterpret_cast<double2 *>(w) + r * (VEC / 2);
+#pragma unroll
+    for (int q = 0; q < VEC / 2; q++)
+      p[q] = make_double2(o[2 * q], o[2 * q + 1]);
+  }
+}
+
+// h[j] = V[:, j] . w for j < k (V FP32); grid (row chunks, column groups)
+template<int VEC>
+__global__ void __launch_bounds__(kThreads)
+    k_multidot_f(const float *__restrict__ V, int64_t ldv, int k,
+                 const double *__restrict__ w, int64_t n,
+                 double *__restrict__ part, unsigned *__restrict__ tickets,
+                 double *__restrict__ h)
+{
+  using T = typename fload<VEC>::T;
+  __shared__ double sh[kDotCols * 32];
+  int64_t const nu    = n / VEC;
+  int64_t const chunk = (nu + gridDim.x - 1) / gridDim.x;
+  int64_t const beg   = blockIdx.x * chunk;
+  int64_t const end   = min(nu, beg + chunk);
+  int const j0        = blockIdx.y * kDotCols;
+  int const nj        = min(kDotCols, k - j0);
+  int64_t const ldu   = ldv / VEC;
+  double a[kDotCols];
+#pragma unroll
+  for (int j = 0; j < kDotCols; j++)
+    a[j] = 0.0;
+  const T *Vj = reinterpret_cast<const T *>(V + int64_t(j0) * ldv);
+  for (int64_t r = beg + threadIdx.x; r < end; r += blockDim.x)
+  {
+    double wr[VEC];
+    load_rows<VEC>(w, r, wr);
+#pragma unroll
+    for (int j = 0; j < kDotCols; j++)
+      if (j < nj)
+      {
+        T const v = Vj[r + j * ldu];
+#pragma unroll
+        for (int e = 0; e < VEC; e++)
+          a[j] = fma(fcomp(v, e), wr[e], a[j]);
+      }
+  }
+  block_sum<kDotCols>(a, sh);
   if (threadIdx.x == 0)
-    part[blockIdx.x] = v[0];
-  if (!last_block(ticket, gridDim.x))
+    for (int j = 0; j < nj; j++)
+      part[int64_t(blockIdx.x) * k + j0 + j] = a[j];
+  if (!last_block(tickets + blockIdx.y, gridDim.x))
     return;
-  ordered_column_sums(part, gridDim.x, 1, 0, 1, out);
+  ordered_column_sums(part, gridDim.x, k, j0, nj, h);
   if (threadIdx.x == 0)
-    *ticket = 0u;
-  if (ga.state == nullptr)
-    return;
-  // the Givens update: earlier rotations staged in shared memory, then one
-  // thread (the serial part touches shared memory only)
-  double *csn    = hs + k;                   // cosines, sines: 2*(restart+1)
-  double *coeffs = csn + 2 * (ga.restart + 1); // k
-  const double *cs_g = ga.state + kStateHead + ga.restart + 1;
-  for (int j = threadIdx.x; j < 2 * (ga.restart + 1); j += blockDim.x)
-    csn[j] = (j % (ga.restart + 1) < ga.step) ? cs_g[j] : 0.0;
+    tickets[blockIdx.y] = 0u;
+}
+
+// w -= V[:, :k] h (V FP32); *out = ||w||^2; the Givens update of a recorded
+// step as in k_update_norm_h
+template<int VEC>
+__global__ void __launch_bounds__(kThreads)
+    k_update_norm_f(const float *__restrict__ V, int64_t ldv, int k,
+                    const double *__restrict__ h, double *__restrict__ w,
+                    int64_t n, double *__restrict__ part,
+                    unsigned *__restrict__ ticket, double *__restrict__ out,
+                    givens_args ga)
+{
+  using T = typename fload<VEC>::T;
+  extern __shared__ double hs[];
+  __shared__ double sh[32];
+  for (int j = threadIdx.x; j < k; j += blockDim.x)
+    hs[j] = h[j];
   __syncthreads();
-  if (threadIdx.x == 0)
-    givens_step(ga, hs, *out, coeffs, csn);
+  int64_t const nu    = n / VEC;
+  int64_t const chunk = (nu + gridDim.x - 1) / gridDim.x;
+  int64_t const beg   = blockIdx.x * chunk;
+  int64_t const end   = min(nu, beg + chunk);
+  int64_t const ldu   = ldv / VEC;
+  const T *Vu         = reinterpret_cast<const T *>(V);
+  double v[1]         = {0.0};
+  for (int64_t r = beg + threadIdx.x; r < end; r += blockDim.x)
+  {
+    // eight basis loads in flight, four partial sums per row
+    double acc[4][VEC];
+#pragma unroll
+    for (int q = 0; q < 4; q++)
+#pragma unroll
+      for (int e = 0; e < VEC; e++)
+        acc[q][e] = 0.0;
+    int j = 0;
+    for (; j + 8 <= k; j += 8)
+    {
+      T u[8];
+#pragma unroll
+      for (int q = 0; q < 8; q++)
+        u[q] = Vu[r + (j + q) * ldu];
+#pragma unroll
+      for (int q = 0; q < 8; q++)
+#pragma unroll
+        for (int e = 0; e < VEC; e++)
+          acc[q & 3][e] = fma(fcomp(u[q], e), hs[j + q], acc[q & 3][e]);
+    }
+    for (; j < k; j++)
+    {
+      T const u = Vu[r + j * ldu];
+#pragma unroll
+      for (int e = 0; e < VEC; e++)
+        acc[0][e] = fma(fcomp(u, e), hs[j], acc[0][e]);
+    }
+    double wr[VEC];
+    load_rows<VEC>(w, r, wr);
+#pragma unroll
+    for (int e = 0; e < VEC; e++)
+    {
+      wr[e] -= (acc[0][e] + acc[1][e]) + (acc[2][e] + acc[3][e]);
+      v[0] += wr[e] * wr[e];
+    }
+    store_rows<VEC>(w, r, wr);
+  }
+  finish_update(v, sh, hs, k, part, ticket, out, ga);
+}
+
+// w *= f and vf = FP32(w), f = state[1] (the 1/||w|| of a recorded step) or
+// scale: a new basis vector normalised, with its FP32 copy
+template<int VEC>
+__global__ void k_store_basis(double *__restrict__ w, float *__restrict__ vf,
+                              int64_t n, const double *__restrict__ state,
+                              double scale)
+{
+  double const f = state ? state[1] : scale;
+  for (int64_t r = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; r < n / VEC;
+       r += int64_t(gridDim.x) * blockDim.x)
+  {
+    double x[VEC];
+    load_rows<VEC>(w, r, x);
+#pragma unroll
+    for (int e = 0; e < VEC; e++)
+      x[e] *= f;
+    store_rows<VEC>(w, r, x);
+    if constexpr (VEC == 1)
+      vf[r] = float(x[0]);
+    else
+      reinterpret_cast<float2 *>(vf)[r] = make_float2(float(x[0]), float(x[1]));
+  }
 }
 
 // *out = ||x||^2
@@ -486,6 +689,12 @@ bool vec2_ok(const double *a, int64_t ld, const double *b)
          (reinterpret_cast<uintptr_t>(b) % 16 == 0);
 }
 
+bool vec4_ok(const float *a, int64_t ld, const double *b, int64_t n)
+{
+  return (n % 4 == 0) && (ld % 4 == 0) && (reinterpret_cast<uintptr_t>(a) % 16 == 0) &&
+         (reinterpret_cast<uintptr_t>(b) % 16 == 0);
+}
+
 } // namespace
 
 int max_reduction_blocks() { return 2 * sm_count(); }
@@ -519,6 +728,49 @@ int launch_update_norm_h(const double *V, int64_t ldv, int k, const double *h,
     k_update_norm_h<2><<<g, kThreads, shm, s>>>(V, ldv, k, h, w, n, part, ticket, out, a);
   else
     k_update_norm_h<1><<<g, kThreads, shm, s>>>(V, ldv, k, h, w, n, part, ticket, out, a);
+  ASGK_LAUNCHED();
+  return ASGK_OK;
+}
+
+int launch_multidot_hf(const float *V, int64_t ldv, int k, const double *w,
+                       int64_t n, double *part, unsigned *tickets, double *h,
+                       cudaStream_t s)
+{
+  int const groups = (k + kDotCols - 1) / kDotCols;
+  dim3 const grid(std::min(grid_for(n), sm_count()), groups);
+  if (vec4_ok(V, ldv, w, n))
+    k_multidot_f<4><<<grid, kThreads, 0, s>>>(V, ldv, k, w, n, part, tickets, h);
+  else
+    k_multidot_f<1><<<grid, kThreads, 0, s>>>(V, ldv, k, w, n, part, tickets, h);
+  ASGK_LAUNCHED();
+  return ASGK_OK;
+}
+
+int launch_update_norm_hf(const float *V, int64_t ldv, int k, const double *h,
+                          double *w, int64_t n, double *part, unsigned *ticket,
+                          double *out, cudaStream_t s, givens_args const *ga)
+{
+  int const g        = grid_for(n);
+  givens_args const a = ga ? *ga : givens_args{};
+  size_t const shm   = sizeof(double) *
+                     (std::max(k, 1) + (ga ? 3 * int64_t(a.restart + 1) : 0));
+  if (vec4_ok(V, ldv, w, n))
+    k_update_norm_f<4><<<g, kThreads, shm, s>>>(V, ldv, k, h, w, n, part, ticket, out, a);
+  else
+    k_update_norm_f<1><<<g, kThreads, shm, s>>>(V, ldv, k, h, w, n, part, ticket, out, a);
+  ASGK_LAUNCHED();
+  return ASGK_OK;
+}
+
+int launch_store_basis(double *w, float *vf, int64_t n, const double *state,
+                       double scale, cudaStream_t s)
+{
+  bool const v2 = (n % 2 == 0) && (reinterpret_cast<uintptr_t>(w) % 16 == 0) &&
+                  (reinterpret_cast<uintptr_t>(vf) % 8 == 0);
+  if (v2)
+    k_store_basis<2><<<grid_for(n / 2), kThreads, 0, s>>>(w, vf, n, state, scale);
+  else
+    k_store_basis<1><<<grid_for(n), kThreads, 0, s>>>(w, vf, n, state, scale);
   ASGK_LAUNCHED();
   return ASGK_OK;
 }

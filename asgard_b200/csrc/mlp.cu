@@ -632,7 +632,7 @@ int mlp_precondition(asgk_mlp *mlp, asgk_plan *plan, const double *v,
     return rc;
   if (m->base)
     if (int rc = jacobi_apply_handle(m->base, low, const_cast<double *>(v), z,
-                                     nullptr, s)) // v only read
+                                     nullptr, nullptr, s)) // v only read
       return rc;
   k_pc_features<<<m->cells, 128, 0, s>>>(v, m->cells, m->ts, m->d, m->lev,
                                          m->U, m->Lr, m->scale);

@@ -39,6 +39,9 @@ def main():
     ap.add_argument("--no-graphs", action="store_true",
                     help="drive every GMRES cycle from the host (no recorded "
                          "cycles; the same kernels, for per-kernel captures)")
+    ap.add_argument("--basis", default="fp32", choices=["fp32", "fp64"],
+                    help="Krylov basis read by the Gram-Schmidt passes of FP32 "
+                         "inner solves")
     ap.add_argument("--trace", action="store_true",
                     help="also run one solve under torch.profiler (CUPTI) and "
                          "print its kernels: launches, device time, share, and "
@@ -55,6 +58,7 @@ def main():
 
     if args.no_graphs:
         ab.lib.asgk_set_gmres_graphs(0)
+    ab.lib.asgk_set_gmres_basis(1 if args.basis == "fp32" else 0)
     t0 = time.perf_counter()
     if args.device_build:
         from asgard_b200.operators import factor_values
@@ -97,7 +101,7 @@ def main():
         torch.cuda.synchronize()
         s = e0.elapsed_time(e1) / 1e3 / args.advance
         print(json.dumps({"d": args.d, "level": args.level, "terms": args.terms,
-                          "mode": args.mode, "precond": args.precond,
+                          "mode": args.mode, "precond": args.precond, "basis": args.basis,
                           "precision": args.precision, "dofs": op.N,
                           "steps": args.advance, "s_per_step": s,
                           "steps_per_s": 1.0 / s,
@@ -120,7 +124,7 @@ def main():
     torch.cuda.synchronize()
     s = e0.elapsed_time(e1) / 1e3 / args.solves
     print(json.dumps({"d": args.d, "level": args.level, "terms": args.terms,
-                      "mode": args.mode, "precond": args.precond,
+                      "mode": args.mode, "precond": args.precond, "basis": args.basis,
                       "precision": args.precision, "dofs": op.N,
                       "s_per_solve": s, "solves_per_s": 1.0 / s,
                       "iterations": [i.iterations for i in infos],

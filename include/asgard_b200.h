@@ -327,6 +327,17 @@ int asgk_gmres_euler_jacobi(asgk_plan *plan, double dt, double *x,
  * returns the previous setting.  No counterpart in the reference. */
 int asgk_set_gmres_graphs(int enable);
 
+/* The FP32 inner solves of iterative refinement (precision ASGK_FP32) run
+ * their Gram-Schmidt passes over an FP32 copy of the Krylov basis (fp32 = 1,
+ * the default): each new basis vector is normalised in FP64 and also stored
+ * rounded to FP32, and the projections h = V^T w and the update w -= V h
+ * read that copy, with w, h and every sum in FP64.  The operator, the
+ * preconditioner and the solution update keep the FP64 vectors, and the
+ * outer FP64 residual decides convergence as before.  fp32 = 0 reads the
+ * FP64 basis.  Process-wide; returns the previous setting.  No counterpart
+ * in the reference. */
+int asgk_set_gmres_basis(int fp32);
+
 /* ------------------------------------------------ implicit time loop */
 
 typedef enum asgk_pc_kind

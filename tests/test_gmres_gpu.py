@@ -134,7 +134,8 @@ def test_cgs_step_against_fp64_reference(cuda, n, k):
 
 @pytest.mark.parametrize("mode,precond,precision", [
     ("pairs", None, "fp64"), ("pairs", "point", "fp64"),
-    ("global", "block", "fp32"), ("global", None, "fp32"), ("dense", "block", "fp64")])
+    ("global", "block", "fp32"), ("global", None, "fp32"), ("global", "kron", "fp32"),
+    ("dense", "block", "fp64")])
 def test_recorded_cycles_match_host_driven_cycles(cuda, mode, precond, precision):
     """Restart cycles run as recorded CUDA graphs (device-side Givens steps,
     one launch per cycle) give the host-driven loop's iterates bit for bit:
@@ -171,3 +172,33 @@ def test_recorded_cycles_match_host_driven_cycles(cuda, mode, precond, precision
         # every executed step's kernels are counted (operator, two
         # Gram-Schmidt passes, preconditioner or scaling: at least three)
         assert lg >= 3 * ig.iterations and lh >= 3 * ih.iterations
+
+
+@pytest.mark.parametrize("precond", [None, "kron"])
+def test_fp32_basis_gram_schmidt(cuda, precond):
+    """FP32 inner solves orthogonalise against an FP32 copy of the basis
+    (the default) or the FP64 basis: both reach the 1e-10 FP64 relative
+    residual with nearly the same iteration counts, and the solutions agree
+    to the accuracy the residual allows."""
+    import asgard_b200 as ab
+    import torch
+    op = ab.SparseGridOperator(3, 5, 3, kind="advdiff", nu=0.1)
+    mat = op.kronmult_matrix(mode="global")
+    dt = 1e-3
+    pc = ab.JacobiPreconditioner(mat, dt, kind=precond) if precond else None
+    b = to_dev(np.random.default_rng(12).uniform(-1, 1, op.N))
+    res = {}
+    try:
+        for basis in (0, 1):
+            ab.lib.asgk_set_gmres_basis(basis)
+            x = torch.zeros_like(b)
+            info = ab.simple_gmres_euler(dt, mat, x, b, 50, 200, 1e-10, tol_mode="rel",
+                                         precision="fp32", precond=pc)
+            assert info.status == 0 and info.true_relres <= 1e-10
+            res[basis] = (x.cpu().numpy(), info)
+    finally:
+        ab.lib.asgk_set_gmres_basis(1)
+    (x64, i64), (x32, i32) = res[0], res[1]
+    assert abs(i32.iterations - i64.iterations) <= 2 + i64.iterations // 10, \
+        (i32.iterations, i64.iterations)
+    assert rel_err(x32, x64) < 1e-7
