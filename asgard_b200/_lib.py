@@ -29,7 +29,7 @@ EXPORTS = [
     "asgk_mlp_train_residual", "asgk_jacobi_create", "asgk_jacobi_destroy",
     "asgk_jacobi_apply", "asgk_jacobi_info", "asgk_gmres_euler_jacobi",
     "asgk_mlp_set_base", "asgk_implicit_advance", "asgk_set_gmres_graphs",
-    "asgk_set_gmres_basis",
+    "asgk_set_gmres_basis", "asgk_set_gmres_node_steps",
 ]
 
 
@@ -103,6 +103,7 @@ def _load():
         "asgk_gmres_euler_jacobi": ([_vp, _d, _vp, _vp, _i, _i, _d, _i, _i, _vp, C.POINTER(GmresInfo), _vp], _i),
         "asgk_set_gmres_graphs": ([_i], _i),
         "asgk_set_gmres_basis": ([_i], _i),
+        "asgk_set_gmres_node_steps": ([_i], _i),
         "asgk_implicit_advance": ([_vp, _d, _vp, _i, _vp, _i64, _i, _i, _d, _i, _i, _i, _vp, C.POINTER(GmresInfo), _vp], _i),
         "asgk_mlp_train_residual": ([_vp, _vp, _vp, _d, _vp, _vp, _i, _i, C.c_float, _i, C.c_uint64, C.POINTER(_d), _vp], _i),
     }

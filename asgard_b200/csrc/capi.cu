@@ -16,6 +16,7 @@ namespace asgk
 std::atomic<int64_t> g_launches{0};
 thread_local bool g_recording            = false;
 thread_local int64_t g_recorded_launches = 0;
+thread_local const double *g_gate        = nullptr;
 
 namespace
 {
@@ -464,7 +465,8 @@ inline int pos_from_indices(int i, int j) { return i + j * (j + 1) / 2; }
 
 // What a recorded GMRES cycle depends on besides the workspace buffers: the
 // operator (plan, dt, arithmetic), the preconditioner, the restart length,
-// the basis precision of the Gram-Schmidt passes.
+// the basis precision of the Gram-Schmidt passes, the Arnoldi steps per
+// graph node.
 struct graph_key
 {
   const void *plan = nullptr; // the workspace dies with its plan
@@ -473,15 +475,21 @@ struct graph_key
   uint64_t pc      = 0;       // preconditioner serial (never reused), 0: none
   int restart      = 0;
   bool low_basis   = false;
+  int node_steps   = 1;
   bool operator==(graph_key const &o) const
   {
     return plan == o.plan && dt == o.dt && precision == o.precision &&
-           pc == o.pc && restart == o.restart && low_basis == o.low_basis;
+           pc == o.pc && restart == o.restart && low_basis == o.low_basis &&
+           node_steps == o.node_steps;
   }
 };
 
 bool g_gmres_graphs     = true; // asgk_set_gmres_graphs
 bool g_gmres_low_basis  = true; // asgk_set_gmres_basis
+// steps per node of a recorded cycle (asgk_set_gmres_node_steps): at d=4
+// level 7 a 138-iteration solve took 9.85 / 8.49 / 8.33 / 8.23 ms with 1 / 4
+// / 8 / 16 (node boundaries cost ~10 us, a skipped launch ~1 us)
+int g_gmres_node_steps  = 16;
 
 // Device workspace of a GMRES solve, kept on the plan between solves.
 struct gmres_ws
@@ -638,6 +646,7 @@ __global__ void k_cycle_start(double *st, double inner_res, double tol)
     st[3]          = 0.0;
     st[4]          = ASGK_OK;
     st[5]          = tol;
+    st[kGoSlot]    = 1.0;
     st[kStateHead] = inner_res;
   }
 }
@@ -653,15 +662,18 @@ int norm2(gmres_ws &ws, const double *v, int64_t n, double &out,
   return ASGK_OK;
 }
 
-// Records one restart cycle: a chain of `restart` conditional nodes, Arnoldi
-// step i in the body of node i with its basis columns fixed at record time
-// (preconditioner, operator, the two Gram-Schmidt passes, the second ending
-// in the Givens step, and the scaling of the new basis vector: folded into
-// the next step's preconditioner when there is one, or with an FP32 basis
-// copy (low) a kernel that scales and writes the copy).  Node 0 always runs;
-// step i's Givens kernel opens node i + 1 only while the cycle goes on, so a
-// cycle runs with no host round trip and stops where the host-driven loop
-// would.
+// Records one restart cycle: a chain of conditional nodes of S =
+// key.node_steps Arnoldi steps each, the basis columns of every step fixed at
+// record time (preconditioner, operator, the two Gram-Schmidt passes, the
+// second ending in the Givens step, and the scaling of the new basis vector:
+// folded into the next step's preconditioner when there is one, or with an
+// FP32 basis copy (low) a kernel that scales and writes the copy).  Node 0
+// always runs; the Givens step that ends node b opens node b + 1 only while
+// the cycle goes on, so a cycle runs with no host round trip and stops where
+// the host-driven loop would.  With S > 1 the kernels of each step read the
+// go flag the previous step's Givens update left and return at once when the
+// cycle has stopped inside the node: a node boundary costs far more than an
+// empty launch.
 int record_cycle(gmres_ws &ws, int64_t n, matvec_t const &mat,
                  precond_t const *pc, int restart, gmres_ws::cycle_graph &out)
 {
@@ -670,24 +682,27 @@ int record_cycle(gmres_ws &ws, int64_t n, matvec_t const &mat,
     return ASGK_ERR_CUDA;
   cudaStream_t const cs = ws.capture;
   bool const low        = out.key.low_basis;
+  int const S           = std::max(1, std::min(out.key.node_steps, restart));
+  int const nodes       = (restart + S - 1) / S;
   cudaGraph_t graph     = nullptr;
   if (cudaGraphCreate(&graph, 0) != cudaSuccess)
     return ASGK_ERR_CUDA;
   g_recording         = true;
   g_recorded_launches = 0;
-  std::vector<cudaGraphConditionalHandle> hs(restart);
+  g_gate              = nullptr;
+  std::vector<cudaGraphConditionalHandle> hs(nodes);
   int rc = ASGK_OK;
-  for (int i = 0; i < restart && rc == ASGK_OK; i++)
-    if (cudaGraphConditionalHandleCreate(&hs[i], graph, i == 0 ? 1u : 0u,
+  for (int b = 0; b < nodes && rc == ASGK_OK; b++)
+    if (cudaGraphConditionalHandleCreate(&hs[b], graph, b == 0 ? 1u : 0u,
                                          cudaGraphCondAssignDefault) != cudaSuccess)
       rc = ASGK_ERR_CUDA;
   cudaGraphNode_t prev = nullptr;
   int kps              = 0;
-  for (int i = 0; i < restart && rc == ASGK_OK; i++)
+  for (int b = 0; b < nodes && rc == ASGK_OK; b++)
   {
     cudaGraphNodeParams np{};
     np.type                = cudaGraphNodeTypeConditional;
-    np.conditional.handle  = hs[i];
+    np.conditional.handle  = hs[b];
     np.conditional.type    = cudaGraphCondTypeIf;
     np.conditional.size    = 1;
     cudaGraphNode_t node   = nullptr;
@@ -704,53 +719,66 @@ int record_cycle(gmres_ws &ws, int64_t n, matvec_t const &mat,
       rc = ASGK_ERR_CUDA;
       break;
     }
-    int64_t const before = g_recorded_launches;
-    double *vi  = ws.V + int64_t(i) * n;
-    double *w   = ws.V + int64_t(i + 1) * n;
-    int const k = i + 1;
-    if (pc)
+    int const i_end = std::min(restart, (b + 1) * S);
+    for (int i = b * S; i < i_end && rc == ASGK_OK; i++)
     {
-      // the preconditioner also normalises v_i (step i-1 left 1/||w|| in the
-      // state; v_0 was normalised before the cycle) and writes its FP32 copy
-      double *zi = ws.Z + int64_t(i) * n;
-      rc         = (*pc)(vi, zi, i > 0 ? ws.dstate : nullptr,
-                         (i > 0 && low) ? ws.Vf + int64_t(i) * n : nullptr, cs);
+      // the first step of a node runs whenever the node does
+      g_gate               = (S > 1 && i > b * S) ? ws.dstate + kGoSlot : nullptr;
+      int64_t const before = g_recorded_launches;
+      double *vi  = ws.V + int64_t(i) * n;
+      double *w   = ws.V + int64_t(i + 1) * n;
+      int const k = i + 1;
+      if (pc)
+      {
+        // the preconditioner also normalises v_i (step i-1 left 1/||w|| in
+        // the state; v_0 was normalised before the cycle) and writes its FP32
+        // copy
+        double *zi = ws.Z + int64_t(i) * n;
+        rc         = (*pc)(vi, zi, i > 0 ? ws.dstate : nullptr,
+                           (i > 0 && low) ? ws.Vf + int64_t(i) * n : nullptr, cs);
+        if (rc == ASGK_OK)
+          rc = mat(1.0, zi, 0.0, w, cs);
+      }
+      else
+        rc = mat(1.0, vi, 0.0, w, cs);
       if (rc == ASGK_OK)
-        rc = mat(1.0, zi, 0.0, w, cs);
+        rc = low ? launch_multidot_hf(ws.Vf, n, k, w, n, ws.part, ws.tickets + 2, ws.h, cs)
+                 : launch_multidot_h(ws.V, n, k, w, n, ws.part, ws.tickets + 2, ws.h, cs);
+      if (rc == ASGK_OK)
+      {
+        givens_args ga;
+        ga.state    = ws.dstate;
+        ga.step     = i;
+        ga.restart  = restart;
+        ga.has_next = (i + 1 == i_end && b + 1 < nodes) ? 1 : 0;
+        ga.next     = ga.has_next ? hs[b + 1] : hs[b];
+        rc = low ? launch_update_norm_hf(ws.Vf, n, k, ws.h, w, n, ws.part, ws.tickets,
+                                         ws.h + k, cs, &ga)
+                 : launch_update_norm_h(ws.V, n, k, ws.h, w, n, ws.part, ws.tickets,
+                                        ws.h + k, cs, &ga);
+      }
+      // without a preconditioner to fold it into, w is normalised here, with
+      // its FP32 copy when there is one.  The last step's w is never read
+      // (the solution update uses v_0..v_{k-1}), so with S > 1 this kernel
+      // reads the go flag this step's Givens update just wrote.
+      if (rc == ASGK_OK && !pc)
+      {
+        g_gate = (S > 1) ? ws.dstate + kGoSlot : nullptr;
+        rc = low ? launch_store_basis(w, ws.Vf + int64_t(i + 1) * n, n, ws.dstate, 0.0, cs)
+                 : launch_scale_by(w, n, ws.dstate, cs);
+      }
+      if (i == 0)
+        kps = int(g_recorded_launches - before);
     }
-    else
-      rc = mat(1.0, vi, 0.0, w, cs);
-    if (rc == ASGK_OK)
-      rc = low ? launch_multidot_hf(ws.Vf, n, k, w, n, ws.part, ws.tickets + 2, ws.h, cs)
-               : launch_multidot_h(ws.V, n, k, w, n, ws.part, ws.tickets + 2, ws.h, cs);
-    if (rc == ASGK_OK)
-    {
-      givens_args ga;
-      ga.state    = ws.dstate;
-      ga.step     = i;
-      ga.restart  = restart;
-      ga.has_next = (i + 1 < restart) ? 1 : 0;
-      ga.next     = ga.has_next ? hs[i + 1] : hs[i];
-      rc = low ? launch_update_norm_hf(ws.Vf, n, k, ws.h, w, n, ws.part, ws.tickets,
-                                       ws.h + k, cs, &ga)
-               : launch_update_norm_h(ws.V, n, k, ws.h, w, n, ws.part, ws.tickets,
-                                      ws.h + k, cs, &ga);
-    }
-    // without a preconditioner to fold it into, w is normalised here, with
-    // its FP32 copy when there is one (the last step's w is never read: the
-    // solution update uses v_0..v_{k-1})
-    if (rc == ASGK_OK && !pc)
-      rc = low ? launch_store_basis(w, ws.Vf + int64_t(i + 1) * n, n, ws.dstate, 0.0, cs)
-               : launch_scale_by(w, n, ws.dstate, cs);
+    g_gate = nullptr;
     cudaGraph_t captured = nullptr;
     if (cudaStreamEndCapture(cs, &captured) != cudaSuccess && rc == ASGK_OK)
       rc = ASGK_ERR_CUDA;
-    if (i == 0)
-      kps = int(g_recorded_launches - before);
     prev = node;
   }
   // what was launched while recording runs later, counted per executed step
   g_recording = false;
+  g_gate      = nullptr;
   cudaGraphExec_t exec = nullptr;
   if (rc == ASGK_OK && cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess)
     rc = ASGK_ERR_CUDA;
@@ -2081,12 +2109,20 @@ int gmres_euler_impl(asgk_plan *plan, double dt, double *x, const double *b,
     return rc;
   double const tol_abs = (tol_mode == ASGK_TOL_REL) ? tol * bnorm : tol;
 
+  // recorded cycles take several Arnoldi steps per graph node when every
+  // kernel of a step reads the gate: the global operator without chains
+  // (one kernel), a Jacobi preconditioner or none, the Krylov kernels
+  int const node_steps =
+      (p.global && p.gchains == 0 && p.terms > 0 && p.nnz > 0 && dt != 0.0)
+          ? g_gmres_node_steps
+          : 1;
+
   core_stats st;
   int status = ASGK_OK;
   double true_res = -1; // FP64 residual of the final x when already known
   if (precision == ASGK_FP64 && !precond)
   {
-    graph_key const gk{plan, dt, ASGK_FP64, 0, restart};
+    graph_key const gk{plan, dt, ASGK_FP64, 0, restart, false, node_steps};
     if (int rc = gmres_core(ws, n, op64, nullptr, x, b, restart, max_outer,
                             tol_abs, st, s, tol_mode == ASGK_TOL_REL, &gk))
       return rc;
@@ -2146,7 +2182,7 @@ int gmres_euler_impl(asgk_plan *plan, double dt, double *x, const double *b,
       // FP32 inner solves: Gram-Schmidt over an FP32 copy of the basis
       bool const low_basis = (precision != ASGK_FP64) && g_gmres_low_basis;
       graph_key const gk{plan, dt, precision, use_pc ? pc_serial : 0, restart,
-                         low_basis};
+                         low_basis, node_steps};
       bool const recordable = (use_pc == nullptr || pc_graph_ok);
       if (int rc = gmres_core(ws, n, (precision == ASGK_FP64) ? matvec_t(op64) : matvec_t(oplow),
                               use_pc, ws.e, ws.r, restart, inner_outer, itol, ist, s,
@@ -2289,6 +2325,14 @@ int asgk_set_gmres_graphs(int enable)
 {
   int const old  = g_gmres_graphs ? 1 : 0;
   g_gmres_graphs = (enable != 0);
+  return old;
+}
+
+int asgk_set_gmres_node_steps(int steps)
+{
+  int const old = g_gmres_node_steps;
+  if (steps >= 1)
+    g_gmres_node_steps = steps;
   return old;
 }
 

@@ -8,23 +8,26 @@
 namespace asgk
 {
 // Device state of a recorded cycle (doubles): the estimated residual, 1/||w||
-// for the new basis vector, ||w||, steps done, status, tolerance; then g, the
+// for the new basis vector, ||w||, steps done, status, tolerance, go (1 while
+// the cycle continues: the gate of the kernels of later steps); then g, the
 // cosines, the sines (restart + 1 each) and the packed Hessenberg columns
 // (restart*(restart+1)/2).
-constexpr int kStateHead = 6;
+constexpr int kGoSlot    = 6;
+constexpr int kStateHead = 7;
 inline int64_t state_len(int restart)
 {
   return kStateHead + 3 * int64_t(restart + 1) + int64_t(restart) * (restart + 1) / 2;
 }
 
 // Where step i of a recorded cycle reports (the Givens part of the
-// update-and-norm pass): null for a host-driven step.
+// update-and-norm pass): null for a host-driven step.  has_next: the step
+// ends its graph node and sets the condition of the next node.
 struct givens_args
 {
   double *state = nullptr;
   int step      = 0;
   int restart   = 0;
-  cudaGraphConditionalHandle next = 0; // condition of step + 1
+  cudaGraphConditionalHandle next = 0; // condition of the next node
   int has_next  = 0;
 };
 
@@ -72,9 +75,10 @@ __device__ __forceinline__ void rotg_d(double &a, double &b, double &c, double &
 // Step ga.step's Givens update (one thread): hk = the projections h[0..k)
 // (k = step + 1), nrm2 = ||w||^2; csn holds the cosines then the sines of the
 // earlier steps (restart + 1 each, a copy in shared memory).  Writes the new
-// Hessenberg column, rotation, g entries, residual estimate, 1/||w|| and the
-// condition of the next step (go on while the estimate is above the
-// tolerance, the cycle is not full and w is not zero).
+// Hessenberg column, rotation, g entries, residual estimate, 1/||w||, the go
+// flag and, at the end of a node, the condition of the next node (go on
+// while the estimate is above the tolerance, the cycle is not full and w is
+// not zero).
 __device__ __forceinline__ void givens_step(givens_args const &ga,
                                             const double *hk, double nrm2,
                                             double *coeffs, const double *csn)
@@ -121,6 +125,7 @@ __device__ __forceinline__ void givens_step(givens_args const &ga,
     }
     go = (res > tol && k < ga.restart && nrm != 0.0) ? 1u : 0u;
   }
+  st[kGoSlot] = go ? 1.0 : 0.0;
   if (ga.has_next)
     cudaGraphSetConditional(ga.next, go);
 }

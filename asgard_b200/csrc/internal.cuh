@@ -25,6 +25,19 @@ inline void count_launch(int64_t k = 1)
     g_launches.fetch_add(k, std::memory_order_relaxed);
 }
 
+// While a GMRES cycle is recorded with several Arnoldi steps per graph node,
+// every kernel of a step is handed the cycle's "go" flag and returns at once
+// when it is 0 (the cycle stopped at an earlier step of the node): the
+// recorder sets g_gate around those launches and the launchers pass it on
+// (null otherwise: no check).
+extern thread_local const double *g_gate;
+#ifdef __CUDACC__
+__device__ __forceinline__ bool gate_closed(const double *gate)
+{
+  return gate != nullptr && *gate == 0.0;
+}
+#endif
+
 #define ASGK_CUDA(call)                                                        \
   do                                                                           \
   {                                                                            \

@@ -203,8 +203,11 @@ __global__ void k_block_apply(int rows, int ts, const TM *__restrict__ M,
                               double *__restrict__ v,
                               double *__restrict__ z,
                               const double *__restrict__ scale_state,
-                              float *__restrict__ vcopy)
+                              float *__restrict__ vcopy,
+                              const double *__restrict__ gate)
 {
+  if (gate_closed(gate))
+    return;
   extern __shared__ double vs[];
   int const row = blockIdx.x;
   if (scale_state)
@@ -246,8 +249,10 @@ __global__ void __launch_bounds__(kApply16Threads)
     k_block_apply16(int ts, int ps, const __half *__restrict__ M,
                     double *__restrict__ v, double *__restrict__ z,
                     const double *__restrict__ scale_state,
-                    float *__restrict__ vcopy)
+                    float *__restrict__ vcopy, const double *__restrict__ gate)
 {
+  if (gate_closed(gate))
+    return;
   extern __shared__ __align__(16) unsigned char smem16[];
   __half *Ms = reinterpret_cast<__half *>(smem16);
   float *vs  = reinterpret_cast<float *>(smem16 + sizeof(__half) * ps);
@@ -305,8 +310,11 @@ __global__ void k_point_apply(int64_t n, const double *__restrict__ inv_diag,
                               double *__restrict__ v,
                               double *__restrict__ z,
                               const double *__restrict__ scale_state,
-                              float *__restrict__ vcopy)
+                              float *__restrict__ vcopy,
+                              const double *__restrict__ gate)
 {
+  if (gate_closed(gate))
+    return;
   double const f = scale_state ? scale_state[1] : 1.0;
   for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n;
        i += int64_t(gridDim.x) * blockDim.x)
@@ -343,8 +351,10 @@ __global__ void __launch_bounds__(WPC * 32)
                  const R *__restrict__ tab, double shift, double dt,
                  double *__restrict__ v, double *__restrict__ z,
                  const double *__restrict__ scale_state,
-                 float *__restrict__ vcopy)
+                 float *__restrict__ vcopy, const double *__restrict__ gate)
 {
+  if (gate_closed(gate))
+    return;
   constexpr int TS  = ipow3j(D);
   constexpr int PER = (TS + 31) / 32;
   constexpr int WS  = 4 * TS + D * kKronTab; // per-warp shared values
@@ -503,7 +513,7 @@ int launch_kron_apply(int rows, const int *kself, const R *tab, double shift,
     ASGK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    int(shm)));
   kern<<<(rows + WPC - 1) / WPC, WPC * 32, shm, s>>>(rows, kself, tab, shift, dt,
-                                                   v, z, sc, vc);
+                                                   v, z, sc, vc, g_gate);
   ASGK_LAUNCHED();
   return ASGK_OK;
 }
@@ -802,7 +812,8 @@ int jacobi_apply(jacobi_data const &jd, bool low, double *v, double *z,
   if (jd.kind == ASGK_JACOBI_POINT)
   {
     int const blocks = int(std::min<int64_t>((n + 255) / 256, 4096));
-    k_point_apply<<<blocks, 256, 0, s>>>(n, jd.inv_diag, v, z, scale_state, vcopy);
+    k_point_apply<<<blocks, 256, 0, s>>>(n, jd.inv_diag, v, z, scale_state, vcopy,
+                                         g_gate);
     ASGK_LAUNCHED();
     return ASGK_OK;
   }
@@ -812,14 +823,14 @@ int jacobi_apply(jacobi_data const &jd, bool low, double *v, double *z,
       return ASGK_ERR_UNSUPPORTED;
     size_t const shm = sizeof(__half) * jd.ps16 + sizeof(float) * jd.ts;
     k_block_apply16<<<jd.rows, kApply16Threads, shm, s>>>(jd.ts, jd.ps16, jd.M16, v, z,
-                                                          scale_state, vcopy);
+                                                          scale_state, vcopy, g_gate);
   }
   else
   {
     int const threads = jd.ts <= 32 ? 32 : (jd.ts <= 64 ? 64 : 128);
     size_t const shm  = sizeof(double) * jd.ts;
     k_block_apply<double><<<jd.rows, threads, shm, s>>>(jd.rows, jd.ts, jd.M64, v, z,
-                                                        scale_state, vcopy);
+                                                        scale_state, vcopy, g_gate);
   }
   ASGK_LAUNCHED();
   return ASGK_OK;

@@ -65,8 +65,11 @@ __global__ void __launch_bounds__(NW * 32)
                      const TC *__restrict__ B, double *__restrict__ scratch,
                      unsigned *__restrict__ tickets, double alpha,
                      const double *__restrict__ x, double beta,
-                     double *__restrict__ y, double ex)
+                     double *__restrict__ y, double ex,
+                     const double *__restrict__ gate)
 {
+  if (gate_closed(gate))
+    return;
   constexpr int TS  = ipow3g(D);
   constexpr int NF  = TS / 3;           // fibres along one dimension
   constexpr int FPL = (NF + 31) / 32;   // fibres per lane
@@ -345,7 +348,7 @@ int launch_global_d(plan_data const &p, double alpha, const double *x,
     B = p.gB32;
   kron_global_rows<D, TC, NW, SLICE><<<p.gslices, NW * 32, 0, s>>>(
       p.slice_row, p.slice_beg, p.slice_len, p.row_slice0, p.row_nslice, p.gcol, p.gkb, B,
-      p.gscratch, p.gtickets, alpha, x, beta, y, ex);
+      p.gscratch, p.gtickets, alpha, x, beta, y, ex, g_gate);
   ASGK_LAUNCHED();
   if (p.gchains > 0)
     return launch_chains<D, TC>(p, alpha, x, y, s);
@@ -374,8 +377,8 @@ int launch_global(plan_data const &p, int precision, double alpha,
                   const double *x, double beta, double *y, double ex,
                   cudaStream_t s)
 {
-  if (p.n != 3)
-    return ASGK_ERR_UNSUPPORTED;
+  if (p.n != 3 || (g_gate != nullptr && p.gchains > 0))
+    return ASGK_ERR_UNSUPPORTED; // the chain kernels take no gate
   // terms that are the identity in every dimension add n_identity * x
   double const ex_eff = ex + alpha * p.g_identity;
   if (precision == ASGK_FP64)

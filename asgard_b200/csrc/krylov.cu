@@ -320,8 +320,10 @@ __global__ void __launch_bounds__(kThreads)
     k_multidot_h(const double *__restrict__ V, int64_t ldv, int k,
                  const double *__restrict__ w, int64_t n,
                  double *__restrict__ part, unsigned *__restrict__ tickets,
-                 double *__restrict__ h)
+                 double *__restrict__ h, const double *__restrict__ gate)
 {
+  if (gate_closed(gate))
+    return;
   using T = typename vload<VEC>::T;
   __shared__ double sh[kDotCols * 32];
   int64_t const nu    = n / VEC;
@@ -371,8 +373,10 @@ __global__ void __launch_bounds__(kThreads)
                     const double *__restrict__ h, double *__restrict__ w,
                     int64_t n, double *__restrict__ part,
                     unsigned *__restrict__ ticket, double *__restrict__ out,
-                    givens_args ga)
+                    givens_args ga, const double *__restrict__ gate)
 {
+  if (gate_closed(gate))
+    return;
   using T = typename vload<VEC>::T;
   extern __shared__ double hs[];
   __shared__ double sh[32];
@@ -511,8 +515,10 @@ __global__ void __launch_bounds__(kThreads)
     k_multidot_f(const float *__restrict__ V, int64_t ldv, int k,
                  const double *__restrict__ w, int64_t n,
                  double *__restrict__ part, unsigned *__restrict__ tickets,
-                 double *__restrict__ h)
+                 double *__restrict__ h, const double *__restrict__ gate)
 {
+  if (gate_closed(gate))
+    return;
   using T = typename fload<VEC>::T;
   __shared__ double sh[kDotCols * 32];
   int64_t const nu    = n / VEC;
@@ -560,8 +566,10 @@ __global__ void __launch_bounds__(kThreads)
                     const double *__restrict__ h, double *__restrict__ w,
                     int64_t n, double *__restrict__ part,
                     unsigned *__restrict__ ticket, double *__restrict__ out,
-                    givens_args ga)
+                    givens_args ga, const double *__restrict__ gate)
 {
+  if (gate_closed(gate))
+    return;
   using T = typename fload<VEC>::T;
   extern __shared__ double hs[];
   __shared__ double sh[32];
@@ -622,8 +630,10 @@ __global__ void __launch_bounds__(kThreads)
 template<int VEC>
 __global__ void k_store_basis(double *__restrict__ w, float *__restrict__ vf,
                               int64_t n, const double *__restrict__ state,
-                              double scale)
+                              double scale, const double *__restrict__ gate)
 {
+  if (gate_closed(gate))
+    return;
   double const f = state ? state[1] : scale;
   for (int64_t r = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; r < n / VEC;
        r += int64_t(gridDim.x) * blockDim.x)
@@ -675,8 +685,11 @@ int grid_wide(int64_t n, int groups = 1)
 }
 
 // v *= a[1] (the 1/||w|| a recorded GMRES step leaves in its device state)
-__global__ void k_scale_by(double *v, int64_t n, const double *__restrict__ a)
+__global__ void k_scale_by(double *v, int64_t n, const double *__restrict__ a,
+                           const double *__restrict__ gate)
 {
+  if (gate_closed(gate))
+    return;
   double const f = a[1];
   for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n;
        i += int64_t(gridDim.x) * blockDim.x)
@@ -709,9 +722,9 @@ int launch_multidot_h(const double *V, int64_t ldv, int k, const double *w,
   // the final sums more than they shorten the pass)
   dim3 const grid(std::min(grid_for(n), sm_count()), groups);
   if (vec2_ok(V, ldv, w) && n % 2 == 0)
-    k_multidot_h<2><<<grid, kThreads, 0, s>>>(V, ldv, k, w, n, part, tickets, h);
+    k_multidot_h<2><<<grid, kThreads, 0, s>>>(V, ldv, k, w, n, part, tickets, h, g_gate);
   else
-    k_multidot_h<1><<<grid, kThreads, 0, s>>>(V, ldv, k, w, n, part, tickets, h);
+    k_multidot_h<1><<<grid, kThreads, 0, s>>>(V, ldv, k, w, n, part, tickets, h, g_gate);
   ASGK_LAUNCHED();
   return ASGK_OK;
 }
@@ -725,9 +738,11 @@ int launch_update_norm_h(const double *V, int64_t ldv, int k, const double *h,
   size_t const shm   = sizeof(double) *
                      (std::max(k, 1) + (ga ? 3 * int64_t(a.restart + 1) : 0));
   if (vec2_ok(V, ldv, w) && n % 2 == 0)
-    k_update_norm_h<2><<<g, kThreads, shm, s>>>(V, ldv, k, h, w, n, part, ticket, out, a);
+    k_update_norm_h<2><<<g, kThreads, shm, s>>>(V, ldv, k, h, w, n, part, ticket, out, a,
+                                                g_gate);
   else
-    k_update_norm_h<1><<<g, kThreads, shm, s>>>(V, ldv, k, h, w, n, part, ticket, out, a);
+    k_update_norm_h<1><<<g, kThreads, shm, s>>>(V, ldv, k, h, w, n, part, ticket, out, a,
+                                                g_gate);
   ASGK_LAUNCHED();
   return ASGK_OK;
 }
@@ -739,9 +754,9 @@ int launch_multidot_hf(const float *V, int64_t ldv, int k, const double *w,
   int const groups = (k + kDotCols - 1) / kDotCols;
   dim3 const grid(std::min(grid_for(n), sm_count()), groups);
   if (vec4_ok(V, ldv, w, n))
-    k_multidot_f<4><<<grid, kThreads, 0, s>>>(V, ldv, k, w, n, part, tickets, h);
+    k_multidot_f<4><<<grid, kThreads, 0, s>>>(V, ldv, k, w, n, part, tickets, h, g_gate);
   else
-    k_multidot_f<1><<<grid, kThreads, 0, s>>>(V, ldv, k, w, n, part, tickets, h);
+    k_multidot_f<1><<<grid, kThreads, 0, s>>>(V, ldv, k, w, n, part, tickets, h, g_gate);
   ASGK_LAUNCHED();
   return ASGK_OK;
 }
@@ -755,9 +770,11 @@ int launch_update_norm_hf(const float *V, int64_t ldv, int k, const double *h,
   size_t const shm   = sizeof(double) *
                      (std::max(k, 1) + (ga ? 3 * int64_t(a.restart + 1) : 0));
   if (vec4_ok(V, ldv, w, n))
-    k_update_norm_f<4><<<g, kThreads, shm, s>>>(V, ldv, k, h, w, n, part, ticket, out, a);
+    k_update_norm_f<4><<<g, kThreads, shm, s>>>(V, ldv, k, h, w, n, part, ticket, out, a,
+                                                g_gate);
   else
-    k_update_norm_f<1><<<g, kThreads, shm, s>>>(V, ldv, k, h, w, n, part, ticket, out, a);
+    k_update_norm_f<1><<<g, kThreads, shm, s>>>(V, ldv, k, h, w, n, part, ticket, out, a,
+                                                g_gate);
   ASGK_LAUNCHED();
   return ASGK_OK;
 }
@@ -768,16 +785,16 @@ int launch_store_basis(double *w, float *vf, int64_t n, const double *state,
   bool const v2 = (n % 2 == 0) && (reinterpret_cast<uintptr_t>(w) % 16 == 0) &&
                   (reinterpret_cast<uintptr_t>(vf) % 8 == 0);
   if (v2)
-    k_store_basis<2><<<grid_for(n / 2), kThreads, 0, s>>>(w, vf, n, state, scale);
+    k_store_basis<2><<<grid_for(n / 2), kThreads, 0, s>>>(w, vf, n, state, scale, g_gate);
   else
-    k_store_basis<1><<<grid_for(n), kThreads, 0, s>>>(w, vf, n, state, scale);
+    k_store_basis<1><<<grid_for(n), kThreads, 0, s>>>(w, vf, n, state, scale, g_gate);
   ASGK_LAUNCHED();
   return ASGK_OK;
 }
 
 int launch_scale_by(double *v, int64_t n, const double *state, cudaStream_t s)
 {
-  k_scale_by<<<grid_for(n), kThreads, 0, s>>>(v, n, state);
+  k_scale_by<<<grid_for(n), kThreads, 0, s>>>(v, n, state, g_gate);
   ASGK_LAUNCHED();
   return ASGK_OK;
 }

@@ -42,6 +42,9 @@ def main():
     ap.add_argument("--basis", default="fp32", choices=["fp32", "fp64"],
                     help="Krylov basis read by the Gram-Schmidt passes of FP32 "
                          "inner solves")
+    ap.add_argument("--node-steps", type=int, default=0,
+                    help="Arnoldi steps per node of a recorded cycle (0: the "
+                         "library default)")
     ap.add_argument("--trace", action="store_true",
                     help="also run one solve under torch.profiler (CUPTI) and "
                          "print its kernels: launches, device time, share, and "
@@ -59,6 +62,8 @@ def main():
     if args.no_graphs:
         ab.lib.asgk_set_gmres_graphs(0)
     ab.lib.asgk_set_gmres_basis(1 if args.basis == "fp32" else 0)
+    if args.node_steps > 0:
+        ab.lib.asgk_set_gmres_node_steps(args.node_steps)
     t0 = time.perf_counter()
     if args.device_build:
         from asgard_b200.operators import factor_values
@@ -102,6 +107,7 @@ def main():
         s = e0.elapsed_time(e1) / 1e3 / args.advance
         print(json.dumps({"d": args.d, "level": args.level, "terms": args.terms,
                           "mode": args.mode, "precond": args.precond, "basis": args.basis,
+                      "node_steps": ab.lib.asgk_set_gmres_node_steps(0),
                           "precision": args.precision, "dofs": op.N,
                           "steps": args.advance, "s_per_step": s,
                           "steps_per_s": 1.0 / s,
@@ -125,6 +131,7 @@ def main():
     s = e0.elapsed_time(e1) / 1e3 / args.solves
     print(json.dumps({"d": args.d, "level": args.level, "terms": args.terms,
                       "mode": args.mode, "precond": args.precond, "basis": args.basis,
+                      "node_steps": ab.lib.asgk_set_gmres_node_steps(0),
                       "precision": args.precision, "dofs": op.N,
                       "s_per_solve": s, "solves_per_s": 1.0 / s,
                       "iterations": [i.iterations for i in infos],
@@ -135,7 +142,8 @@ def main():
 
 def trace(solve, b):
     """One solve under torch.profiler: per-kernel launches and device time,
-    device-busy time against the solve's wall time."""
+    device-busy time against the solve's wall time, and the idle time between
+    consecutive device activities grouped by (previous, next) kernel."""
     import re
     import torch
     from torch.profiler import ProfilerActivity, profile
@@ -151,20 +159,35 @@ def trace(solve, b):
     evs = [e for e in prof.events() if e.device_type.name == "CUDA"]
     spans = sorted((e.time_range.start, e.time_range.end) for e in evs)
     busy = sum(e - s for s, e in spans)
+
+    def short(e):
+        name = e.name.replace("(anonymous namespace)::", "").replace("asgk::", "")
+        return re.sub(r"\(.*", "", name)
+
     per = {}
     for e in evs:
-        name = e.name.replace("(anonymous namespace)::", "").replace("asgk::", "")
-        name = re.sub(r"\(.*", "", name)
-        c = per.setdefault(name, [0, 0.0])
+        c = per.setdefault(short(e), [0, 0.0])
         c[0] += 1
         c[1] += e.time_range.end - e.time_range.start
+    # idle time between consecutive device activities, by transition
+    order = sorted(evs, key=lambda e: e.time_range.start)
+    gaps = {}
+    for a, b in zip(order, order[1:]):
+        g = max(0.0, b.time_range.start - a.time_range.end)
+        key = short(a).split("<")[0].replace("void ", "") + " -> " + \
+            short(b).split("<")[0].replace("void ", "")
+        c = gaps.setdefault(key, [0, 0.0])
+        c[0] += 1
+        c[1] += g
     print(json.dumps({"trace": {
         "iterations": info.iterations, "wall_ms": wall * 1e3,
         "device_busy_ms": busy / 1e3,
         "first_to_last_ms": (spans[-1][1] - spans[0][0]) / 1e3,
         "kernels": [{"name": k, "launches": c, "ms": t / 1e3,
                      "us_per_launch": t / c, "share": t / busy}
-                    for k, (c, t) in sorted(per.items(), key=lambda kv: -kv[1][1])]}}))
+                    for k, (c, t) in sorted(per.items(), key=lambda kv: -kv[1][1])],
+        "gaps": [{"between": k, "count": c, "ms": t / 1e3, "us_each": t / c}
+                 for k, (c, t) in sorted(gaps.items(), key=lambda kv: -kv[1][1])[:12]]}}))
 
 
 if __name__ == "__main__":

@@ -327,6 +327,14 @@ int asgk_gmres_euler_jacobi(asgk_plan *plan, double dt, double *x,
  * returns the previous setting.  No counterpart in the reference. */
 int asgk_set_gmres_graphs(int enable);
 
+/* Arnoldi steps per conditional node of a recorded cycle (default 16) for
+ * plans whose step kernels can skip themselves (global plans whose terms act
+ * in one dimension each, with a Jacobi preconditioner or none; one step per
+ * node otherwise).  Inside a node, the kernels of the steps after the cycle
+ * stopped return at once; iterates are the same for every value.  steps < 1
+ * only reads the setting.  Process-wide; returns the previous setting. */
+int asgk_set_gmres_node_steps(int steps);
+
 /* The FP32 inner solves of iterative refinement (precision ASGK_FP32) run
  * their Gram-Schmidt passes over an FP32 copy of the Krylov basis (fp32 = 1,
  * the default): each new basis vector is normalised in FP64 and also stored

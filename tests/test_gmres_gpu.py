@@ -202,3 +202,41 @@ def test_fp32_basis_gram_schmidt(cuda, precond):
     assert abs(i32.iterations - i64.iterations) <= 2 + i64.iterations // 10, \
         (i32.iterations, i64.iterations)
     assert rel_err(x32, x64) < 1e-7
+
+
+@pytest.mark.parametrize("precond,precision", [(None, "fp32"), ("kron", "fp32"),
+                                               ("block", "fp64")])
+def test_node_steps_give_the_same_iterates(cuda, precond, precision):
+    """Recorded cycles with several Arnoldi steps per graph node (the kernels
+    of steps after the cycle stopped skip themselves) give the iterates of
+    one step per node bit for bit, whatever the node size and wherever the
+    cycles stop inside a node."""
+    import asgard_b200 as ab
+    import torch
+    op = ab.SparseGridOperator(3, 5, 3, kind="advdiff")
+    mat = op.kronmult_matrix(mode="global")
+    dt = 4e-3
+    pc = ab.JacobiPreconditioner(mat, dt, kind=precond) if precond else None
+    b = torch.from_numpy(np.random.default_rng(21).uniform(-1, 1, op.N)).cuda()
+    out = {}
+    old = ab.lib.asgk_set_gmres_node_steps(0)
+    try:
+        for steps in (1, 3, 8, 30):
+            ab.lib.asgk_set_gmres_node_steps(steps)
+            x = torch.zeros_like(b)
+            l0 = ab.launch_count()
+            info = ab.simple_gmres_euler(dt, mat, x, b, 30, 200, 1e-10,
+                                         tol_mode="rel", precision=precision,
+                                         precond=pc)
+            torch.cuda.synchronize()
+            assert info.status == 0 and info.true_relres <= 1e-10
+            out[steps] = (x.cpu().numpy(), info, ab.launch_count() - l0)
+    finally:
+        ab.lib.asgk_set_gmres_node_steps(old)
+    x1, i1, l1 = out[1]
+    for steps in (3, 8, 30):
+        xs, i_s, ls = out[steps]
+        assert i_s.iterations == i1.iterations and i_s.outer_steps == i1.outer_steps
+        assert np.array_equal(xs, x1)
+        assert i_s.error == i1.error and i_s.true_relres == i1.true_relres
+        assert ls == l1  # skipped launches are not counted as work
