@@ -390,6 +390,29 @@ def launch_count() -> int:
     return lib.asgk_launch_count()
 
 
+def gmres_settings(graphs=None, node_steps=None, fp32_basis=None) -> dict:
+    """Process-wide settings of the device GMRES (asgk_set_gmres_graphs,
+    asgk_set_gmres_node_steps, asgk_set_gmres_basis): restart cycles recorded
+    as CUDA graphs, Arnoldi steps per recorded graph node, and whether the
+    FP32 inner solves orthogonalise against an FP32 copy of the basis.  The
+    arguments given are set; returns the settings in force before the call
+    (pass the dict back as keyword arguments to restore them).  None of them
+    changes iterates except fp32_basis."""
+    old_steps = lib.asgk_set_gmres_node_steps(node_steps if node_steps is not None else 0)
+    if graphs is None:
+        old_graphs = lib.asgk_set_gmres_graphs(1)
+        lib.asgk_set_gmres_graphs(old_graphs)
+    else:
+        old_graphs = lib.asgk_set_gmres_graphs(1 if graphs else 0)
+    if fp32_basis is None:
+        old_basis = lib.asgk_set_gmres_basis(1)
+        lib.asgk_set_gmres_basis(old_basis)
+    else:
+        old_basis = lib.asgk_set_gmres_basis(1 if fp32_basis else 0)
+    return {"graphs": bool(old_graphs), "node_steps": old_steps,
+            "fp32_basis": bool(old_basis)}
+
+
 __all__ = ["kronmult_matrix", "simple_gmres_euler", "simple_gmres", "cgs_step",
-           "implicit_advance",
+           "implicit_advance", "gmres_settings",
            "gmres_info", "default_gmres_restarts", "launch_count", "AsgkError"]

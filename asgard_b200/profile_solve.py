@@ -59,11 +59,8 @@ def main():
     import torch
     import asgard_b200 as ab
 
-    if args.no_graphs:
-        ab.lib.asgk_set_gmres_graphs(0)
-    ab.lib.asgk_set_gmres_basis(1 if args.basis == "fp32" else 0)
-    if args.node_steps > 0:
-        ab.lib.asgk_set_gmres_node_steps(args.node_steps)
+    ab.gmres_settings(graphs=not args.no_graphs, fp32_basis=args.basis == "fp32",
+                      node_steps=args.node_steps if args.node_steps > 0 else None)
     t0 = time.perf_counter()
     if args.device_build:
         from asgard_b200.operators import factor_values
@@ -107,7 +104,7 @@ def main():
         s = e0.elapsed_time(e1) / 1e3 / args.advance
         print(json.dumps({"d": args.d, "level": args.level, "terms": args.terms,
                           "mode": args.mode, "precond": args.precond, "basis": args.basis,
-                      "node_steps": ab.lib.asgk_set_gmres_node_steps(0),
+                      "node_steps": ab.gmres_settings()["node_steps"],
                           "precision": args.precision, "dofs": op.N,
                           "steps": args.advance, "s_per_step": s,
                           "steps_per_s": 1.0 / s,
@@ -131,7 +128,7 @@ def main():
     s = e0.elapsed_time(e1) / 1e3 / args.solves
     print(json.dumps({"d": args.d, "level": args.level, "terms": args.terms,
                       "mode": args.mode, "precond": args.precond, "basis": args.basis,
-                      "node_steps": ab.lib.asgk_set_gmres_node_steps(0),
+                      "node_steps": ab.gmres_settings()["node_steps"],
                       "precision": args.precision, "dofs": op.N,
                       "s_per_solve": s, "solves_per_s": 1.0 / s,
                       "iterations": [i.iterations for i in infos],

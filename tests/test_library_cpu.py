@@ -25,6 +25,23 @@ def test_library_exports_every_declared_symbol():
     assert not missing, missing
 
 
+def test_gmres_settings_set_and_restore():
+    """The process-wide GMRES settings (no device work): defaults, a change
+    reported back, and the restore from the returned dict."""
+    import asgard_b200 as ab
+    old = ab.gmres_settings()
+    assert old == {"graphs": True, "node_steps": 16, "fp32_basis": True}
+    try:
+        assert ab.gmres_settings(graphs=False, node_steps=3, fp32_basis=False) == old
+        assert ab.gmres_settings() == {"graphs": False, "node_steps": 3,
+                                       "fp32_basis": False}
+        ab.gmres_settings(node_steps=0)  # below 1: only read
+        assert ab.gmres_settings()["node_steps"] == 3
+    finally:
+        ab.gmres_settings(**old)
+    assert ab.gmres_settings() == old
+
+
 @pytest.mark.parametrize("name", ["continuity_2_L4", "continuity_3_L3",
                                   "continuity_6_L2", "diffusion_2_L3"])
 def test_builder_matches_reference_builder(name):
