@@ -29,7 +29,7 @@ EXPORTS = [
     "asgk_mlp_train_residual", "asgk_jacobi_create", "asgk_jacobi_destroy",
     "asgk_jacobi_apply", "asgk_jacobi_info", "asgk_gmres_euler_jacobi",
     "asgk_mlp_set_base", "asgk_implicit_advance", "asgk_set_gmres_graphs",
-    "asgk_set_gmres_basis", "asgk_set_gmres_node_steps",
+    "asgk_set_gmres_basis", "asgk_set_gmres_node_steps", "asgk_imex_advance",
 ]
 
 
@@ -46,6 +46,9 @@ class GmresInfo(C.Structure):
 
 _vp = C.c_void_p
 _i = C.c_int
+# asgk_imex_hook: (ctx, step, stage, event, const double *f, stream) -> status
+IMEX_HOOK = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p,
+                        C.c_void_p)
 _i64 = C.c_int64
 _d = C.c_double
 
@@ -105,6 +108,8 @@ def _load():
         "asgk_set_gmres_basis": ([_i], _i),
         "asgk_set_gmres_node_steps": ([_i], _i),
         "asgk_implicit_advance": ([_vp, _d, _vp, _i, _vp, _i64, _i, _i, _d, _i, _i, _i, _vp, C.POINTER(GmresInfo), _vp], _i),
+        "asgk_imex_advance": ([_vp, _vp, _d, _vp, _i, _i, _i, _d, _i, _i, _vp, _vp, _vp, _vp,
+                               _vp, C.POINTER(GmresInfo), _vp], _i),
         "asgk_mlp_train_residual": ([_vp, _vp, _vp, _d, _vp, _vp, _i, _i, C.c_float, _i, C.c_uint64, C.POINTER(_d), _vp], _i),
     }
     for name, (args, res) in sig.items():

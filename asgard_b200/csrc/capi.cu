@@ -1521,6 +1521,11 @@ int asgk_plan_update_values(asgk_plan *plan, const double *vA, int64_t vA_len)
         return ASGK_ERR_INVALID;
       if (int rc = upload_global_blocks(p, B))
         return rc;
+      // the identity terms enter the launches as a scalar, which recorded
+      // GMRES cycles hold: a change of their count drops the recordings
+      if (p.g_identity != n_identity)
+        if (auto *ex = extras_of(plan, false))
+          ex->ws.drop_graphs();
       p.g_identity = n_identity;
     }
     return upload_values(p, vA);
@@ -2389,6 +2394,98 @@ int asgk_implicit_advance(asgk_plan *plan, double dt, double *x, int steps,
     }
     cudaStreamSynchronize(s);
     cudaFree(b);
+    return status;
+  }
+  catch (std::bad_alloc const &)
+  {
+    return ASGK_ERR_ALLOC;
+  }
+  catch (...)
+  {
+    return ASGK_ERR_INVALID;
+  }
+}
+
+int asgk_imex_advance(asgk_plan *explicit_plan, asgk_plan *implicit_plan,
+                      double dt, double *x, int steps, int restart,
+                      int max_outer, double tol, int tol_mode, int precision,
+                      asgk_jacobi *pc_stage1, asgk_jacobi *pc_stage2,
+                      asgk_imex_hook hook, void *hook_ctx, double *work,
+                      asgk_gmres_info *info, asgk_stream stream)
+{
+  try
+  {
+    if (!explicit_plan || !x || steps < 0 || (steps > 0 && !info))
+      return ASGK_ERR_INVALID;
+    auto const &pe = explicit_plan->p;
+    if (pe.rows != pe.cols)
+      return ASGK_ERR_INVALID;
+    int64_t const n = int64_t(pe.rows) * pe.tensor;
+    if (implicit_plan &&
+        int64_t(implicit_plan->p.rows) * implicit_plan->p.tensor != n)
+      return ASGK_ERR_INVALID;
+    cudaStream_t s = as_stream(stream);
+    // f_0, the explicit product, f_1 (then f_1 + dt E f_1), the stage-1
+    // solution (then the stage-2 solve's iterate)
+    double *owned = nullptr;
+    int64_t unused = 0;
+    int status     = ASGK_OK;
+    if (!work)
+    {
+      if ((status = dev_alloc(&owned, std::max<int64_t>(4 * n, 1), unused)))
+        return status;
+      work = owned;
+    }
+    double *const f0 = work, *const fx = work + n, *const f1 = work + 2 * n,
+                  *const f1s = work + 3 * n;
+    auto call_hook = [&](int k, int stage, int event, const double *f) -> int {
+      return hook ? hook(hook_ctx, k, stage, event, f, stream) : ASGK_OK;
+    };
+    auto solve = [&](double h, asgk_jacobi *pc, double *xs, const double *b,
+                     asgk_gmres_info *out) -> int {
+      if (pc)
+        return asgk_gmres_euler_jacobi(implicit_plan, h, xs, b, restart, max_outer,
+                                       tol, tol_mode, precision, pc, out, stream);
+      return asgk_gmres_euler(implicit_plan, h, xs, b, restart, max_outer, tol,
+                              tol_mode, precision, nullptr, out, stream);
+    };
+    for (int k = 0; k < steps && status == ASGK_OK; k++)
+    {
+      asgk_gmres_info *i1 = info + 2 * k, *i2 = info + 2 * k + 1;
+      *i1 = asgk_gmres_info{};
+      *i2 = asgk_gmres_info{};
+      // stage 1: f_1s = f_0 + dt E f_0 (in x), f_1 from it
+      if ((status = launch_copy(f0, x, n, s)) ||
+          (status = call_hook(k, 0, ASGK_IMEX_BEFORE_EXPLICIT, x)) ||
+          (status = asgk_apply(explicit_plan, ASGK_FP64, 1.0, x, 0.0, fx, stream)) ||
+          (status = launch_axpy(x, fx, n, dt, s)) ||
+          (status = call_hook(k, 0, ASGK_IMEX_BEFORE_IMPLICIT, x)) ||
+          (status = launch_copy(f1, x, n, s)))
+        break;
+      if (implicit_plan)
+      {
+        if ((status = solve(dt, pc_stage1, f1, x, i1)) ||
+            (status = launch_copy(f1s, f1, n, s)))
+          break;
+      }
+      // stage 2: f_2s = (f_0 + f_1 + dt E f_1) / 2 (in x), f_2 from it
+      if ((status = launch_copy(x, f0, n, s)) ||
+          (status = call_hook(k, 1, ASGK_IMEX_BEFORE_EXPLICIT, f1)) ||
+          (status = asgk_apply(explicit_plan, ASGK_FP64, 1.0, f1, 0.0, fx, stream)) ||
+          (status = launch_axpy(f1, fx, n, dt, s)) ||
+          (status = launch_axpy(x, f1, n, 1.0, s)) ||
+          (status = launch_scale(x, n, 0.5, s)) ||
+          (status = call_hook(k, 1, ASGK_IMEX_BEFORE_IMPLICIT, x)))
+        break;
+      if (implicit_plan)
+      {
+        if ((status = solve(0.5 * dt, pc_stage2, f1s, x, i2)) ||
+            (status = launch_copy(x, f1s, n, s)))
+          break;
+      }
+    }
+    cudaStreamSynchronize(s);
+    cudaFree(owned);
     return status;
   }
   catch (std::bad_alloc const &)

@@ -15,7 +15,7 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from ._lib import AsgkError, GmresInfo, check, lib
+from ._lib import IMEX_HOOK, AsgkError, GmresInfo, check, lib
 
 FP64, FP32, BF16 = 0, 1, 2
 TOL_ABS, TOL_REL = 0, 1
@@ -349,6 +349,62 @@ def implicit_advance(dt, mat: kronmult_matrix, x, steps, forcing=None,
     return [gmres_info(**infos[k].as_dict()) for k in range(steps)]
 
 
+IMEX_BEFORE_EXPLICIT, IMEX_BEFORE_IMPLICIT = 0, 1
+
+
+def imex_advance(dt, explicit: kronmult_matrix, implicit, x, steps, restart=-1,
+                 max_iter=-1, tol=-1.0, tol_mode="abs", precision="fp64",
+                 precond=(None, None), hook=None, stream=None):
+    """`steps` steps of the reference's two-stage IMEX scheme (imex_advance,
+    src/time_advance.cpp:477-990) with x resident on the device:
+    f_1s = f_0 + dt E f_0, f_1 = (I - dt I)^-1 f_1s; f_2s = (f_0 + f_1 +
+    dt E f_1) / 2, f_2 = (I - dt/2 I)^-1 f_2s, E = explicit, I = implicit
+    (None: no implicit part, f_1 = f_1s and the step ends with f_2s).
+    precond: Jacobi preconditioners of `implicit` for dt and dt/2 (or None).
+    hook(step, stage, event, f) is called with f a device tensor (read-only)
+    at IMEX_BEFORE_EXPLICIT (the state the stage's explicit apply reads: the
+    reference's Poisson update) and IMEX_BEFORE_IMPLICIT (the stage's explicit
+    result: moments and coefficient regeneration; the hook may call
+    update_stored_coefficients on the plans); a non-zero return or an
+    exception stops the loop.  Returns per step the (stage 1, stage 2)
+    gmres_info pair."""
+    import torch
+    n = explicit.output_size()
+    if implicit is not None and restart is not None and restart > n:
+        raise ValueError(f"Number of inner iterations {restart} must be less than {n}!")
+    work = torch.empty((4, max(n, 1)), dtype=torch.float64, device=x.device)
+    views = {x.data_ptr(): x}
+    views.update({work[i].data_ptr(): work[i] for i in range(4)})
+    errors = []
+
+    def _call(ctx, step, stage, event, f, strm):
+        try:
+            r = hook(step, stage, event, views[f])
+            return 0 if r is None else int(r)
+        except Exception as e:  # reported after the call returns
+            errors.append(e)
+            return 1
+    cb = IMEX_HOOK(_call) if hook is not None else None
+    infos = (GmresInfo * max(2 * steps, 1))()
+    pc1, pc2 = precond if precond is not None else (None, None)
+    rc = lib.asgk_imex_advance(explicit.handle,
+                               implicit.handle if implicit is not None else None,
+                               dt, _ptr(x), steps,
+                               -1 if restart is None else restart,
+                               -1 if max_iter is None else max_iter, tol,
+                               TOL_REL if tol_mode == "rel" else TOL_ABS,
+                               _precision(precision),
+                               pc1.handle if pc1 is not None else None,
+                               pc2.handle if pc2 is not None else None,
+                               C.cast(cb, C.c_void_p) if cb is not None else None,
+                               None, work.data_ptr(), infos, _stream(stream))
+    if errors:
+        raise errors[0]
+    check(rc, "imex_advance")
+    return [(gmres_info(**infos[2 * k].as_dict()), gmres_info(**infos[2 * k + 1].as_dict()))
+            for k in range(steps)]
+
+
 def simple_gmres(A, x, b, M=None, restart=-1, max_iter=-1, tol=-1.0):
     """Dense test path of solver::simple_gmres (host arrays, solved on the GPU)."""
     if M is not None and np.size(M) > 0:
@@ -414,5 +470,5 @@ def gmres_settings(graphs=None, node_steps=None, fp32_basis=None) -> dict:
 
 
 __all__ = ["kronmult_matrix", "simple_gmres_euler", "simple_gmres", "cgs_step",
-           "implicit_advance", "gmres_settings",
+           "implicit_advance", "imex_advance", "gmres_settings",
            "gmres_info", "default_gmres_restarts", "launch_count", "AsgkError"]

@@ -373,6 +373,56 @@ int asgk_implicit_advance(asgk_plan *plan, double dt, double *x, int steps,
                           int precision, int pc_kind, void *precond,
                           asgk_gmres_info *info, asgk_stream stream);
 
+/* ------------------------------------------------ IMEX time loop */
+
+/* Events of the IMEX hook: the points where the reference's imex_advance
+ * updates PDE-specific state. */
+typedef enum asgk_imex_event
+{
+  ASGK_IMEX_BEFORE_EXPLICIT = 0, /* f: the state the stage's explicit apply
+                                    reads (f_0, then f_1): the reference's
+                                    Poisson update */
+  ASGK_IMEX_BEFORE_IMPLICIT = 1  /* f: the stage's explicit result (f_1s, then
+                                    f_2s): the reference's moments and
+                                    coefficient regeneration */
+} asgk_imex_event;
+
+/* Called by asgk_imex_advance at each event of each stage (stage 0, 1) of
+ * each step.  f is a device vector of the plans' size, valid during the call
+ * (work on `stream`, or synchronise it first).  The hook may change the
+ * plans' coefficients (asgk_plan_update_values / asgk_plan_update_terms),
+ * as generate_all_coefficients does in the reference; a Jacobi
+ * preconditioner built earlier is then kept as it is (a preconditioner, not
+ * the inverse of the updated operator).  Return 0 to go on; any other value
+ * stops the loop and is returned by asgk_imex_advance. */
+typedef int (*asgk_imex_hook)(void *ctx, int step, int stage, int event,
+                              const double *f, asgk_stream stream);
+
+/* `steps` steps of the reference's two-stage IMEX scheme (imex_advance,
+ * src/time_advance.cpp:477-990) with x resident on the device:
+ *   f_1s = f_0 + dt E f_0;           f_1 solves (I - dt I_op) f_1 = f_1s
+ *   f_2s = (f_0 + f_1 + dt E f_1)/2; f_2 solves (I - dt/2 I_op) f_2 = f_2s
+ * E = explicit_plan (applied in FP64), I_op = implicit_plan.  The stage-1
+ * solve starts from f_1s, the stage-2 solve from f_1, as the reference does
+ * without a previous refined solution.  implicit_plan null: no implicit
+ * part (the reference without a collision operator): f_1 = f_1s and the
+ * step ends with f_2s.  The solves take restart, max_outer, tol, tol_mode
+ * and precision as asgk_gmres_euler; pc_stage1 / pc_stage2 (or null) are
+ * Jacobi preconditioners of the implicit plan for dt and dt/2.  hook (or
+ * null) with hook_ctx: see asgk_imex_hook.  info receives 2 entries per
+ * step (stage 1, stage 2; zeros without an implicit plan), including
+ * solves that stopped short of the tolerance (the loop goes on, as the
+ * reference's does).  x is f_0 on entry and the last step's result on exit.
+ * work: 4 vectors of the plans' size (device, contiguous: f_0, the explicit
+ * product, f_1, the stage-1 solution), or null to have them allocated for
+ * the call; every f a hook receives is x or one of them. */
+int asgk_imex_advance(asgk_plan *explicit_plan, asgk_plan *implicit_plan,
+                      double dt, double *x, int steps, int restart,
+                      int max_outer, double tol, int tol_mode, int precision,
+                      asgk_jacobi *pc_stage1, asgk_jacobi *pc_stage2,
+                      asgk_imex_hook hook, void *hook_ctx, double *work,
+                      asgk_gmres_info *info, asgk_stream stream);
+
 /* ------------------------------------------------ learned preconditioner */
 
 /* A per-cell learned preconditioner (no counterpart in the reference, which

@@ -295,6 +295,56 @@ def gmres_euler(d, n, pntr, indx, terms, iA, vA, dt, x, b, restart, max_outer,
     return err.value, it.value
 
 
+def imex_advance(d, n, explicit, implicit, dt, x, steps, restart, max_outer,
+                 tol, hook=None):
+    """The reference's two-stage IMEX step (imex_advance,
+    src/time_advance.cpp:477-990) restated over the oracle's kronmult and
+    GMRES, x (FP64 numpy) updated in place.  explicit / implicit: operators
+    as (pntr, indx, terms, iA, vA) tuples; implicit None is the reference
+    without a collision operator (f_1 = f_1s, the step ends with f_2s).
+    hook(step, stage, event, f) runs where the reference updates PDE state:
+    event 0 before each explicit apply (f: its input, the Poisson update at
+    :572-640, called at :792 and :891), event 1 before each implicit solve
+    (f: the stage's explicit result, calculate_moments +
+    generate_all_coefficients at :829-840 and :930-938); it may change the vA
+    arrays in place.  Returns
+    the per-step (stage 1, stage 2) GMRES iteration counts."""
+    def apply(op, v):
+        pntr, indx, terms, iA, vA = op
+        y = np.zeros_like(v)
+        return kronmult(d, n, pntr, indx, terms, iA, vA, 1.0, v, 0.0, y)
+
+    def solve(h, x0, b):
+        pntr, indx, terms, iA, vA = implicit
+        _, it = gmres_euler(d, n, pntr, indx, terms, iA, vA, h, x0, b, restart,
+                            max_outer, tol)
+        return it
+
+    call = hook if hook is not None else (lambda *a: None)
+    its = []
+    for k in range(steps):
+        f0 = x.copy()                         # f_orig (:524-529)
+        call(k, 0, 0, x)
+        x += dt * apply(explicit, x)          # f_1s = f_0 + dt A f_0 (:800-822)
+        call(k, 0, 1, x)
+        f1 = x.copy()                         # initial guess f_1s (:849)
+        it1 = solve(dt, f1, x.copy()) if implicit is not None else 0
+        f1_out = f1.copy()                    # f_1_output (:873)
+        x[:] = f0                             # (:887)
+        call(k, 1, 0, f1)
+        f1 += dt * apply(explicit, f1)        # f_2 = f_1 + dt T(f_1) (:897-918)
+        x += f1
+        x *= 0.5                              # f_2s (:921-922)
+        call(k, 1, 1, x)
+        if implicit is not None:
+            it2 = solve(0.5 * dt, f1_out, x.copy())   # from f_1_output (:945-970)
+            x[:] = f1_out
+        else:
+            it2 = 0
+        its.append((it1, it2))
+    return its
+
+
 def gmres_dense(A, x, b, restart, max_outer, tol, lib=None):
     n = len(b)
     At = np.asfortranarray(A).ravel(order="F").copy()

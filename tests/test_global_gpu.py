@@ -193,3 +193,40 @@ def test_global_matches_reference_global_kron(cuda, d, L, T, kind):
     y_ref, _ = oracle.ref_global_apply(d, 3, L, op.table, T, op.vA, x)
     g = op.kronmult_matrix(mode="global")
     assert rel_err(_apply(g, 1.0, x, 0.0, np.zeros(op.N)), y_ref) < 1e-13
+
+
+def test_value_update_changing_identity_terms_drops_recorded_cycles(cuda):
+    """A term that is the identity in every dimension enters the global
+    form's launches as a scalar that recorded GMRES cycles hold; an update
+    that makes it a real term must not replay those recordings: the solve
+    after the update equals a solve on a plan built from the new values."""
+    import asgard_b200 as ab
+    import torch
+    from asgard_b200.operators import connect_1d, factor_values, sparse_grid
+    d, L, T = 3, 5, 3
+    pntr, indx = connect_1d(L)
+    rows = np.repeat(np.arange(len(pntr) - 1), np.diff(pntr))
+    eye = np.where((rows == indx)[:, None], np.eye(3).ravel(order="F")[None, :], 0.0)
+    vA = factor_values(d, L, T).reshape(len(indx), T, d, 9)
+    vA[:, 2] = eye[:, None, :]                 # term 2: identity everywhere
+    v0 = np.ascontiguousarray(vA.reshape(-1))
+    v1 = vA.copy()
+    v1[:, 2, 0] *= 1.5                         # term 2 now scales dimension 0
+    v1 = np.ascontiguousarray(v1.reshape(-1))
+    table = sparse_grid(d, L)
+    b = torch.from_numpy(np.random.default_rng(2).uniform(-1, 1, table.shape[0] * 27)).cuda()
+    dt = 2e-3
+
+    def solve(mat):
+        x = torch.zeros_like(b)
+        info = ab.simple_gmres_euler(dt, mat, x, b, 30, 100, 1e-11, tol_mode="rel")
+        assert info.status == 0
+        return x.cpu().numpy(), info.iterations
+
+    mat = ab.kronmult_matrix.from_global(d, 3, L, table, T, v0)
+    solve(mat)                                 # records the cycles
+    mat.update_stored_coefficients(v1)
+    x_upd, it_upd = solve(mat)
+    x_new, it_new = solve(ab.kronmult_matrix.from_global(d, 3, L, table, T, v1))
+    assert it_upd == it_new
+    assert np.array_equal(x_upd, x_new)
