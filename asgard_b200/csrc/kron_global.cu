@@ -89,26 +89,26 @@ __global__ void __launch_bounds__(NW * 32)
   int64_t const eb = slice_beg[sl];
   int const n      = slice_len[sl];
 
+  // the slice's entries come in dimension order: s_seg[k] is the first
+  // entry along dimension k or after (s_seg[D] = n), written by the entry
+  // that opens the segment
   for (int i = threadIdx.x; i < n; i += NT)
   {
-    s_col[i] = __ldg(gcol + eb + i);
-    s_kb[i]  = __ldg(gkb + eb + i);
+    int const kb = __ldg(gkb + eb + i);
+    s_col[i]     = __ldg(gcol + eb + i);
+    s_kb[i]      = kb;
+    int const dk = kb % D;
+    int const dp = (i > 0) ? __ldg(gkb + eb + i - 1) % D : -1;
+    for (int k = dp + 1; k <= dk; k++)
+      s_seg[k] = i;
+    if (i == n - 1)
+      for (int k = dk + 1; k <= D; k++)
+        s_seg[k] = n;
   }
+  if (n == 0 && threadIdx.x <= D)
+    s_seg[threadIdx.x] = 0;
   for (int i = threadIdx.x; i < NW * TS; i += NT)
     red[i] = TC(0);
-  __syncthreads();
-  if (threadIdx.x == 0)
-  {
-    // the slice's entries per dimension (they come in dimension order)
-    int e = 0;
-    for (int k = 0; k < D; k++)
-    {
-      s_seg[k] = e;
-      while (e < n && s_kb[e] % D == k)
-        ++e;
-    }
-    s_seg[D] = e;
-  }
   __syncthreads();
 
   TC *myred = red + warp * TS;
@@ -130,9 +130,24 @@ __global__ void __launch_bounds__(NW * 32)
     auto entry = [&](int j) {
       const TC *b      = B + int64_t(s_kb[j]) * PAD;
       const double *xc = x + int64_t(s_col[j]) * TS;
-      TC const b0 = __ldg(b), b1 = __ldg(b + 1), b2 = __ldg(b + 2);
-      TC const b3 = __ldg(b + 3), b4 = __ldg(b + 4), b5 = __ldg(b + 5);
-      TC const b6 = __ldg(b + 6), b7 = __ldg(b + 7), b8 = __ldg(b + 8);
+      // the padded block (12 floats / 10 doubles) in 16-byte loads
+      TC b0, b1, b2, b3, b4, b5, b6, b7, b8;
+      if constexpr (sizeof(TC) == 4)
+      {
+        const float4 *q = reinterpret_cast<const float4 *>(b);
+        float4 const q0 = __ldg(q), q1 = __ldg(q + 1), q2 = __ldg(q + 2);
+        b0 = q0.x, b1 = q0.y, b2 = q0.z, b3 = q0.w;
+        b4 = q1.x, b5 = q1.y, b6 = q1.z, b7 = q1.w;
+        b8 = q2.x;
+      }
+      else
+      {
+        const double2 *q = reinterpret_cast<const double2 *>(b);
+        double2 const q0 = __ldg(q), q1 = __ldg(q + 1), q2 = __ldg(q + 2);
+        double2 const q3 = __ldg(q + 3), q4 = __ldg(q + 4);
+        b0 = q0.x, b1 = q0.y, b2 = q1.x, b3 = q1.y, b4 = q2.x;
+        b5 = q2.y, b6 = q3.x, b7 = q3.y, b8 = q4.x;
+      }
 #pragma unroll
       for (int m = 0; m < FPL; m++)
       {
