@@ -371,6 +371,18 @@ __global__ void __launch_bounds__(WPC * 32)
   R *bufr[2] = {base, base + 2 * TS};
   R *bufi[2] = {base + TS, base + 3 * TS};
   R *tabs    = base + 4 * TS; // [D][kKronTab]
+  // with up to four entries per lane, v's loads are issued first so they
+  // overlap the dependent table loads (cell -> table index -> table)
+  double vpre[KEEP ? PER : 1];
+  if constexpr (KEEP)
+  {
+#pragma unroll
+    for (int o = 0; o < PER; o++)
+    {
+      int const i = lane + 32 * o;
+      vpre[o]     = (i < TS) ? v[int64_t(c) * TS + i] : 0.0;
+    }
+  }
   for (int e = lane; e < D * kKronTab; e += 32)
   {
     int const k = e / kKronTab;
@@ -404,7 +416,11 @@ __global__ void __launch_bounds__(WPC * 32)
     int const i = lane + 32 * o;
     if (i < TS)
     {
-      double vv = v[int64_t(c) * TS + i];
+      double vv;
+      if constexpr (KEEP)
+        vv = vpre[o];
+      else
+        vv = v[int64_t(c) * TS + i];
       if (scale_state)
       {
         vv                     = vv * f;

@@ -53,7 +53,7 @@ TOL = 1e-10
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
     ap.add_argument("--workload", default="d4", choices=sorted(WORKLOADS))
@@ -73,7 +73,7 @@ def parse():
 
 class ClockSampler:
     """SM clock and throttle reasons during the timed region: NVML read every
-    10 ms from a thread (the timed region of a short run lasts well under a
+    2 ms from a thread (the timed region of a short run lasts well under a
     second); `nvidia-smi -lms 200` when NVML is unavailable.  Read-only."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
@@ -118,7 +118,7 @@ class ClockSampler:
                         self.samples.append((float(sm), int(get_reasons(self.h))))
                     except Exception:
                         pass
-                    time.sleep(0.01)
+                    time.sleep(0.002)
             self.t = threading.Thread(target=poll, daemon=True)
             self.t.start()
             return
@@ -147,7 +147,7 @@ class ClockSampler:
                               for nm, bit in self.BITS.items() if r & bit})
             return {"sm_mhz": sm[len(sm) // 2] if sm else None,
                     "sm_max_mhz": self.max_mhz, "reasons": reasons,
-                    "samples": len(sm), "source": "NVML every 10 ms"}
+                    "samples": len(sm), "source": "NVML every 2 ms"}
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.proc.terminate()
