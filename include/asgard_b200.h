@@ -320,11 +320,12 @@ int asgk_gmres_euler_jacobi(asgk_plan *plan, double dt, double *x,
                             asgk_stream stream);
 
 /* Restart cycles of the device GMRES run as recorded CUDA graphs (one
- * launch per cycle: each Arnoldi step's Givens update runs on the device and
- * opens the next step, so no host round trip per iteration) whenever the
- * preconditioner is none or Jacobi; the host-driven loop otherwise, or with
- * enable = 0.  Both give the same iterates bit for bit.  Process-wide;
- * returns the previous setting.  No counterpart in the reference. */
+ * launch per cycle: each Arnoldi step's Givens update runs on the device,
+ * writes the cycle's go flag and, at the end of a graph node, opens the next
+ * node, so no host round trip per iteration) whenever the preconditioner is
+ * none or Jacobi; the host-driven loop otherwise, or with enable = 0.  Both
+ * give the same iterates bit for bit.  Process-wide; returns the previous
+ * setting.  No counterpart in the reference. */
 int asgk_set_gmres_graphs(int enable);
 
 /* Arnoldi steps per conditional node of a recorded cycle (default 16) for
