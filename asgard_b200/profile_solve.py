@@ -123,7 +123,10 @@ def main():
         # part, the same operator scaled by 1e-3 as the (non-stiff) explicit
         # part; preconditioners for dt and dt/2
         mat_e = op.kronmult_matrix(mode=args.mode)
-        mat_e.update_stored_coefficients(op.vA * 1e-3)
+        ve = op.vA.reshape(-1, op.terms, op.d, op.n * op.n).copy()
+        for t in range(op.terms):      # term t acts in dimension t mod d
+            ve[:, t, t % op.d] *= 1e-3
+        mat_e.update_stored_coefficients(ve.reshape(-1))
         pcs = (None, None) if pc is None else (
             pc, ab.JacobiPreconditioner(mat, 0.5 * args.dt, kind=args.precond))
         x = bs[0].clone()
