@@ -25,6 +25,16 @@ def test_library_exports_every_declared_symbol():
     assert not missing, missing
 
 
+def test_cpp_dropin_compiles_and_links(tmp_path):
+    """The C++ drop-in program (the reference-side usage of the header-only
+    mirror over the C ABI) compiles and links against the in-tree library
+    with g++ alone; the GPU test runs it."""
+    from test_cpp_dropin_gpu import compile_dropin
+    r = compile_dropin(tmp_path / "dropin")
+    assert r.returncode == 0, r.stderr
+    assert (tmp_path / "dropin").exists()
+
+
 def test_gmres_settings_set_and_restore():
     """The process-wide GMRES settings (no device work): defaults, a change
     reported back, and the restore from the returned dict."""
