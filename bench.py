@@ -13,8 +13,8 @@ block-Jacobi right preconditioning (each cell's diagonal block inverted
 through the eigendecompositions of its 3x3 1D factors; the learned correction
 on top of it is trained and kept only if its validation solve gains), FP32
 operator inside
-FP64 iterative refinement.  Timed beside it: the north star's plain
-baseline -- FP64 GMRES with the connected-pair FP64 kronmult -- and the same
+FP64 iterative refinement.  Timed beside it: the plain baseline -- FP64
+GMRES with the connected-pair FP64 kronmult -- and the same
 method on the connected-pair operator.  Inputs are resident in HBM when the
 timed region starts; the plain baseline's operator (pair list + factor
 indices, ~245 MB) is larger than L2; no extra L2 flush is done between
@@ -23,8 +23,8 @@ steps (the method's working set is L2-sized by design).
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
 For N > 1 (torchrun, one rank per GPU) every rank solves its own right-hand
-sides on its own copy of the operator (replicas: the north star forbids
-sharding the solve); value = solves of all ranks / max-over-ranks time.
+sides on its own copy of the operator (replicas: the solve is not
+sharded); value = solves of all ranks / max-over-ranks time.
 """
 from __future__ import annotations
 
