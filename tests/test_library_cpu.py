@@ -35,6 +35,23 @@ def test_cpp_dropin_compiles_and_links(tmp_path):
     assert (tmp_path / "dropin").exists()
 
 
+def test_imex_rejects_invalid_arguments_without_device_work():
+    """asgk_imex_advance checks its arguments before any CUDA call: no
+    explicit plan, no state vector, or no info array for a positive step
+    count are ASGK_ERR_INVALID; zero steps need no info."""
+    import ctypes as C
+    import asgard_b200 as ab
+    inv = 1  # ASGK_ERR_INVALID
+    call = lambda plan, x, steps, info: ab.lib.asgk_imex_advance(
+        plan, None, 1e-3, x, steps, 10, 10, 1e-10, 0, 0, None, None, None, None,
+        None, info, None)
+    dummy = C.c_double(0.0)
+    assert call(None, C.addressof(dummy), 1, None) == inv
+    assert call(C.addressof(dummy), None, 1, None) == inv
+    assert call(C.addressof(dummy), C.addressof(dummy), 1, None) == inv
+    assert call(C.addressof(dummy), C.addressof(dummy), -1, None) == inv
+
+
 def test_gmres_settings_set_and_restore():
     """The process-wide GMRES settings (no device work): defaults, a change
     reported back, and the restore from the returned dict."""
