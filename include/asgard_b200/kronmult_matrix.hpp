@@ -317,6 +317,68 @@ simple_gmres_euler(double dt, kronmult_matrix<double> const &mat, double *x,
   return gmres_info<double>{info.error, info.iterations};
 }
 
+//! A Jacobi preconditioner of I - dt*K built on the device and owned here:
+//! ASGK_JACOBI_POINT is the reference's diagonal preconditioner
+//! (build_preconditioner, src/asgard_kronmult_matrix.cpp:1015-1067);
+//! ASGK_JACOBI_BLOCK and ASGK_JACOBI_KRON invert each cell's diagonal block
+//! (KRON: global plans whose terms act in one dimension each, any d).
+class jacobi_preconditioner
+{
+public:
+  jacobi_preconditioner(kronmult_matrix<double> const &mat, double dt,
+                        int kind = ASGK_JACOBI_POINT)
+      : dt_(dt)
+  {
+    check(asgk_jacobi_create(&pc_, mat.plan(), dt, kind), "jacobi_preconditioner");
+  }
+  ~jacobi_preconditioner()
+  {
+    if (pc_)
+      asgk_jacobi_destroy(pc_);
+  }
+  jacobi_preconditioner(jacobi_preconditioner const &)            = delete;
+  jacobi_preconditioner &operator=(jacobi_preconditioner const &) = delete;
+  jacobi_preconditioner(jacobi_preconditioner &&o) noexcept
+      : pc_(std::exchange(o.pc_, nullptr)), dt_(o.dt_)
+  {}
+  jacobi_preconditioner &operator=(jacobi_preconditioner &&o) noexcept
+  {
+    std::swap(pc_, o.pc_);
+    std::swap(dt_, o.dt_);
+    return *this;
+  }
+  asgk_jacobi *handle() const { return pc_; }
+  double dt() const { return dt_; }
+
+private:
+  asgk_jacobi *pc_ = nullptr;
+  double dt_       = 0;
+};
+
+//! The reference's global-kron simple_gmres_euler, which preconditions
+//! with its diagonal preconditioner (src/solver.cpp:93-117): here the
+//! caller's Jacobi preconditioner of (mat, dt), applied on the right
+//! through flexible GMRES; same criterion and result as the overload above.
+inline gmres_info<double>
+simple_gmres_euler(double dt, kronmult_matrix<double> const &mat, double *x,
+                   double const *b, int restart, int max_iter, double tol,
+                   jacobi_preconditioner const &pc)
+{
+  int64_t const n = mat.output_size();
+  if (restart > n)
+    throw std::invalid_argument("Number of inner iterations " +
+                                std::to_string(restart) + " must be less than " +
+                                std::to_string(n) + "!");
+  asgk_gmres_info info{};
+  check(asgk_gmres_euler_jacobi(mat.plan(), dt, x, b, restart, max_iter, tol,
+                                ASGK_TOL_ABS, ASGK_FP64, pc.handle(), &info,
+                                nullptr),
+        "simple_gmres_euler");
+  if (info.status == ASGK_ERR_NONFINITE)
+    throw std::runtime_error("simple_gmres_euler: non-finite residual");
+  return gmres_info<double>{info.error, info.iterations};
+}
+
 //! solver::simple_gmres on a dense column-major host matrix (no
 //! preconditioner) -- src/solver.cpp:55-74.
 inline gmres_info<double> simple_gmres(std::vector<double> const &A,

@@ -87,6 +87,26 @@ int main(int argc, char **argv)
   std::vector<double> sol(N);
   cudaMemcpy(sol.data(), dx, sizeof(double) * N, cudaMemcpyDeviceToHost);
 
+  // the same step through the overload of the reference's global-kron
+  // simple_gmres_euler, with a diagonal (point Jacobi) preconditioner
+  double pc_rel = 1.0, pc_its = 0.0, pc_err = 1.0;
+  {
+    solver::jacobi_preconditioner pc(mat, 1e-2, ASGK_JACOBI_POINT);
+    cudaMemset(dx, 0, sizeof(double) * N);
+    auto ip = solver::simple_gmres_euler(1e-2, mat, dx, db, 20, 50, 1e-12, pc);
+    std::vector<double> sp(N);
+    cudaMemcpy(sp.data(), dx, sizeof(double) * N, cudaMemcpyDeviceToHost);
+    double nu = 0, de = 0;
+    for (int64_t i = 0; i < N; i++)
+    {
+      nu += (sp[i] - sol[i]) * (sp[i] - sol[i]);
+      de += sol[i] * sol[i];
+    }
+    pc_rel = std::sqrt(nu / de);
+    pc_its = ip.iterations;
+    pc_err = ip.error;
+  }
+
   // the same operator in the global Kronecker form (every term here acts in
   // all dimensions: chains of masked 1D passes), then a single-direction
   // operator
@@ -266,7 +286,7 @@ int main(int argc, char **argv)
                               double(dmat.is_dense()), double(dmat.num_batch()),
                               double(dmat.flops()), dense_rel, dense_update_rel,
                               chunk_rel, pairs_rel, double(chunked.num_pairs()),
-                              ws_rel, ws_used};
+                              ws_rel, ws_used, pc_rel, pc_its, pc_err};
   put(o, meta);
   cudaFree(dx);
   cudaFree(dy);

@@ -78,3 +78,6 @@ def test_cpp_dropin_header(cuda, tmp_path):
     assert meta[22] == len(col)
     # set_workspace: host applies stage x in the caller's device buffer
     assert meta[23] < 1e-13 and meta[24] == 1.0
+    # the preconditioned overload (point Jacobi, right-preconditioned): the
+    # same solution to the tolerance the criterion allows
+    assert meta[25] < 1e-8 and meta[26] >= 1 and meta[27] <= 1e-12
