@@ -1,10 +1,12 @@
 """Benchmark: implicit backward-Euler solves per second on one B200.
 
-Workload (default ``d4``): d=4, n=3 (81 dofs per cell), level-7 sparse grid
-(4048 cells, 327,888 dofs, 12,258,592 connected cell pairs), 4 terms of
-advection/diffusion factors, solve (I - dt*K) x = b with dt = 1e-3,
-b uniform in [-1, 1] (seeded, a new b every step), GMRES restart 50, until the
-FP64 relative residual ||b - (I - dt K) x|| / ||b|| <= 1e-10.
+Workload (default ``d6``): d=6, n=3 (729 dofs per cell), level-7 sparse grid
+(16,172 cells, 11,789,388 dofs, 226,043,944 connected cell pairs), 6 terms
+of advection/diffusion factors (term t acts in dimension t, even terms DG
+advection, odd terms 0.1 x LDG diffusion), solve (I - dt*K) x = b with
+dt = 5e-4, b uniform in [-1, 1] (seeded, a new b every step), GMRES restart
+50, until the FP64 relative residual ||b - (I - dt K) x|| / ||b|| <= 1e-10.
+``--workload d4`` is the d=4 level-7 configuration (4 terms, dt = 1e-3).
 
 A step is one solve by the framework's method: the operator in its global
 Kronecker form (the reference's global_kron_matrix; the same operator as
@@ -12,19 +14,24 @@ the connected-pair kronmult, its terms acting in one dimension each),
 block-Jacobi right preconditioning (each cell's diagonal block inverted
 through the eigendecompositions of its 3x3 1D factors; the learned correction
 on top of it is trained and kept only if its validation solve gains), FP32
-operator inside
-FP64 iterative refinement.  Timed beside it: the plain baseline -- FP64
-GMRES with the connected-pair FP64 kronmult -- and the same
-method on the connected-pair operator.  Inputs are resident in HBM when the
-timed region starts; the plain baseline's operator (pair list + factor
-indices, ~245 MB) is larger than L2; no extra L2 flush is done between
-steps (the method's working set is L2-sized by design).
+operator inside FP64 iterative refinement.  Timed beside it: the plain
+baseline -- FP64 GMRES with the connected-pair FP64 kronmult (one solve by
+default: about four minutes at d=6) -- and, at d <= 4, the same method on the
+connected-pair operator.  Inputs are resident in HBM when the timed region
+starts; at d=6 every vector (94 MB) and the plain baseline's pair list
+(6.3 GB) are larger than L2, at d=4 the method's working set is L2-sized by
+design; no extra L2 flush is done between steps.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
 For N > 1 (torchrun, one rank per GPU) every rank solves its own right-hand
 sides on its own copy of the operator (replicas: the solve is not
 sharded); value = solves of all ranks / max-over-ranks time.
+
+``--impl reference`` runs the reference's own CPU path on the host cores:
+its sparse grid, global Kronecker matrix, diagonal preconditioner and
+solver::simple_gmres_euler, compiled from the reference sources into
+oracle/_ref/libasgard_ref_gsolve.so; it imports nothing of this framework.
 """
 from __future__ import annotations
 
@@ -41,13 +48,21 @@ sys.path.insert(0, ROOT)
 
 METRIC = "implicit-step solves/s at 1e-10 residual, learned+mixed vs plain FP64 (1 B200)"
 WORKLOADS = {
-    "d4": dict(d=4, level=7, terms=4, dt=1e-3, nu=0.1, kind="advdiff"),
-    "d5": dict(d=5, level=7, terms=4, dt=1e-3, nu=0.1, kind="advdiff"),
     "d6": dict(d=6, level=7, terms=6, dt=5e-4, nu=0.1, kind="advdiff"),
+    "d5": dict(d=5, level=7, terms=4, dt=1e-3, nu=0.1, kind="advdiff"),
+    "d4": dict(d=4, level=7, terms=4, dt=1e-3, nu=0.1, kind="advdiff"),
     "d3": dict(d=3, level=7, terms=3, dt=1e-3, nu=0.1, kind="advdiff"),
 }
 RESTART = 50
 TOL = 1e-10
+
+# DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of
+# each workload's operator kernels, from one ncu capture of that kernel on
+# that workload; None where no capture was taken.
+KERNEL_TRAFFIC = {
+    ("pairs", "d4"): 254_243_328 + 4_232_704,
+    ("global", "d4"): 3_930_368,
+}
 
 
 def parse():
@@ -56,10 +71,17 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
-    ap.add_argument("--workload", default="d4", choices=sorted(WORKLOADS))
-    ap.add_argument("--plain-steps", type=int, default=2)
-    ap.add_argument("--e2e-steps", type=int, default=2)
-    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="d6", choices=sorted(WORKLOADS))
+    ap.add_argument("--plain-steps", type=int, default=1,
+                    help="timed plain FP64 solves (about 250 s each at d=6)")
+    ap.add_argument("--pair-method-steps", type=int, default=None,
+                    help="timed solves of the method on the connected-pair "
+                         "operator (default 2 at d <= 4, 0 above)")
+    ap.add_argument("--e2e-steps", type=int, default=None,
+                    help="solves through host buffers (default: --steps)")
+    ap.add_argument("--cpu-baseline", default="solve", choices=["solve", "none"],
+                    help="solve: one full solve by the reference's CPU path "
+                         "(rank 0, one GPU); none: skip")
     ap.add_argument("--method", default="learned-block-fp32",
                     choices=["learned-block-fp32", "learned-block-fp64",
                              "block-fp32", "block-fp64", "learned-fp32",
@@ -73,9 +95,9 @@ def parse():
 
 class ClockSampler:
     """SM clock and throttle reasons during the timed region: NVML read every
-    10 ms from a thread (the default 20 steps last ~0.16 s; reading every 2 ms
-    slowed the host-driven parts of the solves by ~5 %); `nvidia-smi -lms
-    200` when NVML is unavailable.  Read-only."""
+    10 ms from a thread (reading every 2 ms slowed the host-driven parts of
+    the solves by ~5 %); `nvidia-smi -lms 200` when NVML is unavailable.
+    Read-only."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -176,168 +198,161 @@ class ClockSampler:
                 "samples": len(sm), "source": "nvidia-smi every 200 ms"}
 
 
-def peaks():
-    try:
-        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
-            return json.load(f)
-    except OSError:
-        return {}
-
-
-# ---------------------------------------------------------------- reference arm
-
-def reference_arm(args):
-    """The reference's own CPU paths (compiled from source into oracle/_ref),
-    all host threads: kronmult_matrix<double>::apply on the CPU sparse format
-    (local-kron mode) and, where its terms allow and the operator is small
-    enough to set up, the global Kronecker product (global-kron mode,
-    kronmult::global_cpu).  Each step times one full-operator product of
-    each and converts it to solves/s with the iteration count of the
-    reference GMRES algorithm on this workload; the line's value is the
-    faster of the two (the reference's strongest CPU path)."""
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    if rank != 0:
-        return
-    import numpy as np
-    import oracle
-    if not oracle.ref_available():
-        print(json.dumps({"impl": "reference", "unavailable":
-                          "reference library oracle/_ref/libasgard_ref.so was not built"}))
-        return
-    R = oracle.ref()
-    cfg = WORKLOADS[args.workload]
-    from asgard_b200 import operators as ops
-    d, L, T = cfg["d"], cfg["level"], cfg["terms"]
-    table = ops.sparse_grid(d, L)
-    row_ptr, col, conn = ops.build_pairs(d, L, table)
-    vA = ops.factor_values(d, L, T, cfg["kind"], cfg["nu"])
-    iA = ops.expand_iA(conn, d, 3, T)
-    pntr = row_ptr.astype(np.int32)
-    rows = len(pntr) - 1
-    N = rows * 3 ** d
-    x = np.random.default_rng(0).uniform(-1, 1, N)
-    y = np.zeros(N)
-    iters = _plain_iterations(args.workload)
-    times = []
-    for s in range(args.warmup + args.steps):
-        t0 = time.perf_counter()
-        oracle.kronmult(d, 3, pntr, col, T, iA, vA, -cfg["dt"], x, 0.0, y, lib=R)
-        dt = time.perf_counter() - t0
-        if s >= args.warmup:
-            times.append(dt)
-    t_sparse = sorted(times)[len(times) // 2]
-    cores = R.ref_num_threads()
-    paths = {"cpu_sparse": {"apply_s": t_sparse, "value": 1.0 / (t_sparse * iters)}}
-    g = _ref_global(d, L, T, table, vA, N)
-    if g is not None:
-        gtimes = [g.apply(x)[1] for _ in range(args.warmup + args.steps)][args.warmup:]
-        t_global = sorted(gtimes)[len(gtimes) // 2]
-        paths["global_cpu"] = {"apply_s": t_global, "value": 1.0 / (t_global * iters)}
-    best = max(paths, key=lambda k: paths[k]["value"])
-    value, t_apply = paths[best]["value"], paths[best]["apply_s"]
-    line = {
-        "impl": "reference", "metric": METRIC, "value": value,
-        "unit": "solves/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": t_apply * iters * 1e3,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64", "data": "synthetic",
-        "config": _config(args.workload),
-        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": cores,
-                         "kind": "reference",
-                         "sample": f"{args.steps} full-operator products of the reference's "
-                                   f"{best} (OpenMP {cores} threads); solves/s = "
-                                   f"1/(median product time x {iters} GMRES iterations)"},
-        "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0,
-                "d2h_bytes_per_step": 0},
-        "apply_s": t_apply, "gmres_iterations": iters, "paths": paths,
-    }
-    print(json.dumps(line))
-
-
-def _ref_global(d, L, T, table, vA, N):
-    """The reference's global product when built and affordable to set up
-    (its pattern build is single-threaded host code: up to ~4 M unknowns)."""
-    import oracle
-    if not oracle.ref_global_available() or N > 4_000_000:
-        return None
-    try:
-        return oracle.RefGlobal(d, 3, L, table, T, vA)
-    except (OSError, ValueError):
-        return None
-
-
-# Iterations of the reference GMRES algorithm (restart 50, FP64, relative
-# tolerance 1e-10, b uniform) on each workload, as this framework's plain
-# FP64 GMRES measured them (same algorithm; bench line "plain_fp64"); the
-# reference arm turns its CPU apply time into solves/s with them.
-PLAIN_ITERATIONS = {"d4": 230}
-
-# DRAM bytes per launch of the dominant kernel from one ncu capture
-# (profiles/kron3_staged_d4_L7_fp64.md); None where none was taken.
-KERNEL_TRAFFIC = {"d4": 254_243_328 + 4_232_704}
-# the same for the global form's kernel (profiles/kron_global_rows_d4_L7.md)
-GLOBAL_TRAFFIC = {"d4": 3_930_368 + 0}
-
-
 def _measured_hbm_gbs():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
-            return float(json.load(f)["hbm_gbs"])
+            return float(json.load(f)["hbm_gbs"]), "MEASURED_PEAKS.json hbm_gbs"
     except (OSError, KeyError, ValueError):
-        return 6650.0
-
-
-def _plain_iterations(workload):
-    # other workloads reuse the d4 count (not measured on them)
-    return PLAIN_ITERATIONS.get(workload, PLAIN_ITERATIONS["d4"])
+        return 6650.0, "fallback 6.65 TB/s"
 
 
 def _config(workload):
     cfg = WORKLOADS[workload]
     return {"workload": f"d={cfg['d']} n=3 level {cfg['level']} sparse grid, "
-                        f"{cfg['terms']} advection/diffusion terms (nu={cfg['nu']}), "
-                        f"dt={cfg['dt']}, GMRES restart {RESTART}, rel tol {TOL}",
+                        f"{cfg['terms']} advection/diffusion terms (diffusion "
+                        f"scaled by nu={cfg['nu']}), dt={cfg['dt']}, GMRES "
+                        f"restart {RESTART}, rel tol {TOL}",
             "d": cfg["d"], "n": 3, "level": cfg["level"], "terms": cfg["terms"],
-            "dt": cfg["dt"], "restart": RESTART, "tol": TOL,
-            "l2": "operator data (pair list + indices) larger than L2; no flush"}
+            "dt": cfg["dt"], "nu": cfg["nu"], "restart": RESTART, "tol": TOL,
+            "l2": ("vectors (94 MB) and the plain baseline's pair list larger "
+                   "than L2; no flush" if cfg["d"] >= 6 else
+                   "plain baseline's pair list larger than L2; the method's "
+                   "working set L2-sized; no flush")}
+
+
+# ---------------------------------------------------------------- reference arm
+
+class ReferenceSolves:
+    """The reference's implicit solve on the host cores, driven one GMRES
+    restart cycle at a time: each call of its solver::simple_gmres_euler with
+    max_iter = 1 runs one cycle (the residual b - (I - dt K) x, its diagonal
+    preconditioner, up to 50 Arnoldi steps, the update of x) from the
+    current x, which is what its own outer loop does between cycles; when a
+    cycle meets the tolerance the solve is complete and the next starts from
+    x = 0 with a new b.  The tolerance is the reference's (absolute, on its
+    estimated left-preconditioned residual), set to TOL * ||b|| / max_i
+    |1 - dt pc_i| so that the true relative residual ||b - (I - dt K) x|| /
+    ||b|| is at most TOL (r = M r_prec with M = diag(1 - dt pc)); every
+    completed solve's true residual is recomputed by the reference's apply."""
+
+    def __init__(self, workload, seed=0):
+        import numpy as np
+        import oracle
+        cfg = WORKLOADS[workload]
+        self.np = np
+        self.dt = cfg["dt"]
+        t0 = time.perf_counter()
+        self.R = oracle.RefGlobalSolver.synthetic(cfg["d"], cfg["level"],
+                                                  cfg["terms"], cfg["nu"])
+        self.setup_s = time.perf_counter() - t0
+        pc = self.R.precond()
+        self.mmax = float(np.abs(1.0 - self.dt * pc).max())
+        self.rng = np.random.default_rng(seed)
+        self.cores = oracle._gsolve_lib().ref_gsolve_num_threads()
+        self.solves = []          # completed: iterations, seconds, true relres
+        self._new_solve()
+
+    def _new_solve(self):
+        np = self.np
+        self.b = self.rng.uniform(-1.0, 1.0, self.R.N)
+        self.x = np.zeros(self.R.N)
+        self.tol = TOL * float(np.linalg.norm(self.b)) / self.mmax
+        self.its = 0
+        self.sec = 0.0
+
+    def cycle(self):
+        """One restart cycle; returns (iterations, seconds)."""
+        t0 = time.perf_counter()
+        err, its, _ = self.R.gmres_euler(self.dt, self.x, self.b, RESTART, 1,
+                                         self.tol)
+        sec = time.perf_counter() - t0
+        self.its += its
+        self.sec += sec
+        if err <= self.tol:
+            np = self.np
+            Kx, _ = self.R.apply(1.0, self.x)
+            r = self.b - (self.x - self.dt * Kx)
+            self.solves.append({"iterations": self.its, "seconds": self.sec,
+                                "error": err, "true_relres":
+                                float(np.linalg.norm(r) / np.linalg.norm(self.b))})
+            self._new_solve()
+        return its, sec
+
+    def full_solve(self):
+        """Cycles until the current solve completes; returns its record."""
+        n = len(self.solves)
+        while len(self.solves) == n:
+            self.cycle()
+        return self.solves[-1]
+
+
+def reference_arm(args):
+    """The reference's own CPU path (see ReferenceSolves), all host threads.
+    A step is one GMRES restart cycle of the reference solver (a bounded
+    sample: a full d=6 solve takes minutes on the host); the steps run
+    consecutive real solves.  value = iterations per second over the timed
+    steps / mean iterations of the solves completed in the run."""
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import oracle
+    if not oracle.ref_gsolve_available():
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "reference library oracle/_ref/libasgard_ref_gsolve.so "
+                          "was not built"}))
+        return
+    ref = ReferenceSolves(args.workload)
+    for _ in range(args.warmup):
+        ref.cycle()
+    timed_its, timed_s, times = 0, 0.0, []
+    for _ in range(args.steps):
+        its, sec = ref.cycle()
+        timed_its += its
+        timed_s += sec
+        times.append(sec)
+    if not ref.solves:          # too few cycles in the run for one solve
+        ref.full_solve()
+    its_per_solve = sum(s["iterations"] for s in ref.solves) / len(ref.solves)
+    value = (timed_its / timed_s) / its_per_solve
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value,
+        "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": timed_s / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic",
+        "config": _config(args.workload),
+        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": ref.cores,
+                         "kind": "reference",
+                         "sample": f"{args.steps} GMRES restart cycles of the reference's "
+                                   f"solver::simple_gmres_euler over its global_kron_matrix "
+                                   f"(OpenMP {ref.cores} threads), consecutive real solves; "
+                                   f"solves/s = timed iterations/s / {its_per_solve:.1f} "
+                                   f"iterations per completed solve"},
+        "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+        "step": "one GMRES restart cycle (up to 51 iterations in the reference's count)",
+        "iterations_timed": timed_its, "seconds_timed": timed_s,
+        "cycle_s": {"min": min(times), "max": max(times)},
+        "solves": ref.solves, "setup_s": ref.setup_s,
+        "solver": "reference solver::simple_gmres_euler(dt, matrix_entry::regular, "
+                  "global_kron_matrix, ...), left diagonal preconditioner, "
+                  f"absolute tol TOL*||b||/max|1-dt pc| (max |1-dt pc| = {ref.mmax:.4g})",
+    }
+    print(json.dumps(line))
 
 
 # ---------------------------------------------------------------- our arm
 
-def main():
-    args = parse()
-    if args.impl == "reference":
-        return reference_arm(args)
-    import numpy as np
+def build_method(args, ab, op, mat, gmat, mmat, dt, rank):
+    """Setup of the method, not timed (as the reference's matrix setup is
+    not part of solves/s): block-Jacobi inverse -- through the
+    eigendecompositions of each cell's 1D factors on the global form (any
+    d), else the dense per-cell inverses (n^d <= 81) -- and the learned
+    network's training.  Returns (method dict, training info)."""
     import torch
-    import asgard_b200 as ab
-
-    from asgard_b200 import replicas
-    world, rank, local = replicas.init("nccl")
-    cfg = WORKLOADS[args.workload]
-    d, L, T, dt = cfg["d"], cfg["level"], cfg["terms"], cfg["dt"]
-    op = ab.SparseGridOperator(d, L, T, kind=cfg["kind"], nu=cfg["nu"])
-    mat = op.kronmult_matrix()          # connected pairs: the plain baseline
-    N = op.N
-    # the method's operator: the global Kronecker form of the same operator
-    # (terms acting in one dimension each) unless --operator pairs
-    gmat = None
-    if args.operator == "global":
-        try:
-            gmat = op.kronmult_matrix(mode="global")
-        except ab.AsgkError:
-            gmat = None
-    mmat = gmat if gmat is not None else mat
-    gen = torch.Generator(device="cuda").manual_seed(replicas.rhs_seed(rank))
-    nb = args.warmup + args.steps
-    B = [torch.rand(N, dtype=torch.float64, device="cuda", generator=gen) * 2 - 1
-         for _ in range(max(nb, args.plain_steps + 1))]
+    d = op.d
     precision = "fp64" if args.method.endswith("fp64") else "fp32"
-    # setup, not timed (like building the operator): the block-Jacobi
-    # inverse -- through the eigendecompositions of each cell's 1D factors
-    # on the global form (any d), else the dense per-cell inverses (n^d <= 81)
-    # -- and the learned network's training
     base, base_form = None, None
     if "block" in args.method:
         if gmat is not None:
@@ -361,7 +376,8 @@ def main():
         if gmat is not None:
             from asgard_b200.operators import transpose_factor_values
             mat_T = ab.kronmult_matrix.from_global(
-                d, 3, L, op.table, T, transpose_factor_values(op.vA, d, L, T))
+                d, 3, op.level, op.table, op.terms,
+                transpose_factor_values(op.vA, d, op.level, op.terms))
         else:
             mat_T = op.kronmult_matrix_transposed()
         train_info = net.train(mmat, dt, num_solves=args.train_solves,
@@ -386,7 +402,40 @@ def main():
     parts.append("FP32 operator, FP64 refinement" if precision == "fp32" else "FP64")
     parts.insert(0, "global Kronecker operator" if gmat is not None
                  else "connected-pair operator")
-    method = dict(precision=precision, precond=pc, name=", ".join(parts))
+    return dict(precision=precision, precond=pc, name=", ".join(parts)), train_info
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return reference_arm(args)
+    import torch
+    import asgard_b200 as ab
+
+    from asgard_b200 import replicas
+    world, rank, local = replicas.init("nccl")
+    cfg = WORKLOADS[args.workload]
+    d, L, T, dt = cfg["d"], cfg["level"], cfg["terms"], cfg["dt"]
+    pair_steps = (args.pair_method_steps if args.pair_method_steps is not None
+                  else (2 if d <= 4 else 0))
+    e2e_steps = args.e2e_steps if args.e2e_steps is not None else args.steps
+    op = ab.SparseGridOperator(d, L, T, kind=cfg["kind"], nu=cfg["nu"])
+    mat = op.kronmult_matrix()          # connected pairs: the plain baseline
+    N = op.N
+    # the method's operator: the global Kronecker form of the same operator
+    # (terms acting in one dimension each) unless --operator pairs
+    gmat = None
+    if args.operator == "global":
+        try:
+            gmat = op.kronmult_matrix(mode="global")
+        except ab.AsgkError:
+            gmat = None
+    mmat = gmat if gmat is not None else mat
+    gen = torch.Generator(device="cuda").manual_seed(replicas.rhs_seed(rank))
+    nb = args.warmup + args.steps
+    B = [torch.rand(N, dtype=torch.float64, device="cuda", generator=gen) * 2 - 1
+         for _ in range(max(nb, args.plain_steps, pair_steps))]
+    method, train_info = build_method(args, ab, op, mat, gmat, mmat, dt, rank)
 
     def solve(b, precision, precond=None, m=None):
         x = torch.zeros(N, dtype=torch.float64, device="cuda")
@@ -396,12 +445,12 @@ def main():
                                      precond=precond)
         return x, info
 
-    # warm-up (method and plain)
-    infos = []
+    # warm-up: the method's solves; one FP64 apply of the plain operator
     for i in range(args.warmup):
-        _, info = solve(B[i], method["precision"], method["precond"])
-        infos.append(info)
-    _, pinfo = solve(B[0], "fp64", None, mat)
+        solve(B[i], method["precision"], method["precond"])
+    ytmp = torch.empty_like(B[0])
+    mat.apply_euler(dt, 1.0, B[0], 0.0, ytmp, precision="fp64")
+    torch.cuda.synchronize()
 
     # ---- timed: the method
     launches0 = ab.launch_count()
@@ -423,7 +472,25 @@ def main():
     t_method = replicas.max_over_ranks(t_local)
     value = replicas.throughput(args.steps, t_local)
 
-    # ---- timed: plain FP64 GMRES with the FP64 kronmult
+    # ---- e2e through the public API with host buffers: every step copies
+    # its own b from pinned host memory and reads x back
+    hb = [torch.empty(N, dtype=torch.float64, pin_memory=True) for _ in range(e2e_steps)]
+    for i, h in enumerate(hb):
+        h.copy_(B[(args.warmup + i) % len(B)].cpu())
+    hx = torch.empty(N, dtype=torch.float64, pin_memory=True)
+    replicas.barrier()
+    e0.record()
+    for i in range(e2e_steps):
+        bd = hb[i].to("cuda", non_blocking=True)
+        x, _ = solve(bd, method["precision"], method["precond"])
+        hx.copy_(x, non_blocking=True)
+    e1.record()
+    replicas.barrier()
+    t_local = e0.elapsed_time(e1) / 1e3
+    e2e_value = replicas.throughput(e2e_steps, t_local)
+    del hb
+
+    # ---- timed: plain FP64 GMRES with the FP64 connected-pair kronmult
     replicas.barrier()
     e0.record()
     pinfos = []
@@ -434,34 +501,82 @@ def main():
     replicas.barrier()
     t_local = e0.elapsed_time(e1) / 1e3
     t_plain = replicas.max_over_ranks(t_local)
-    plain_value = replicas.throughput(args.plain_steps, t_local)
+    plain_value = replicas.throughput(max(args.plain_steps, 0), t_local) \
+        if args.plain_steps > 0 else None
 
     # ---- timed: the same method on the connected-pair operator
     pair_method = None
-    if gmat is not None:
+    if gmat is not None and pair_steps > 0:
         replicas.barrier()
         e0.record()
         qinfos = []
-        for i in range(args.plain_steps):
+        for i in range(pair_steps):
             _, info = solve(B[i], method["precision"], method["precond"], mat)
             qinfos.append(info)
         e1.record()
         replicas.barrier()
         t_local = e0.elapsed_time(e1) / 1e3
-        pair_method = {"value": replicas.throughput(args.plain_steps, t_local),
+        pair_method = {"value": replicas.throughput(pair_steps, t_local),
                        "unit": "solves/s",
                        "iterations": [i.iterations for i in qinfos],
                        "true_relres": max(i.true_relres for i in qinfos)}
 
-    # ---- rooflines by CUDA events (average launch duration): the
-    # connected-pair kronmult (FP64, the plain baseline's kernel, and FP32)
-    # and the method's operator kernel
-    xs = B[0]
+    roofline = rooflines(ab, op, mat, gmat, method, dt, args.workload, B[0])
+
+    # ---- CPU baseline (rank 0, N = 1): the reference's own solve
+    cpu = None
+    if rank == 0 and world == 1 and args.cpu_baseline == "solve":
+        cpu = cpu_baseline(args.workload)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "solves/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": t_method / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic",
+            "config": dict(_config(args.workload), method=args.method,
+                           parallelism=f"replicas x{world}"),
+            "plain_fp64": ({"value": plain_value, "unit": "solves/s",
+                            "iterations": [i.iterations for i in pinfos],
+                            "true_relres": max(i.true_relres for i in pinfos),
+                            "ms_per_solve": t_plain / args.plain_steps * 1e3}
+                           if pinfos else None),
+            "method": {"name": method["name"],
+                       "iterations": [i.iterations for i in minfos],
+                       "true_relres": max(i.true_relres for i in minfos),
+                       "outer_steps": minfos[0].outer_steps,
+                       "matvecs_low": minfos[0].matvecs_low,
+                       "matvecs_fp64": minfos[0].matvecs_fp64,
+                       "precond_calls": minfos[0].precond_calls,
+                       "fallback": max(i.fallback for i in minfos),
+                       "training": train_info,
+                       "speedup_vs_plain": (value / plain_value
+                                            if plain_value else None)},
+            "clocks": clk,
+            "e2e": {"value": e2e_value, "unit": "solves/s",
+                    "h2d_bytes_per_step": N * 8, "d2h_bytes_per_step": N * 8,
+                    "steps": e2e_steps},
+            "gpu_launches": launches,
+            "pair_operator_method": pair_method,
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line))
+    replicas.shutdown()
+
+
+def rooflines(ab, op, mat, gmat, method, dt, workload, xs):
+    """Average launch durations by CUDA events on the launching stream: the
+    method's operator kernel (global form, algorithmic bytes against the
+    measured HBM bandwidth) and the plain baseline's connected-pair kernel
+    (algorithmic flops against the live-measured FP64 FMA peak)."""
+    import torch
+    d, N = op.d, op.N
     ys = torch.zeros_like(xs)
     flops = op.flops()
-    reps = 5
 
-    def time_apply(m, precision):
+    def time_apply(m, precision, reps):
         m.apply_euler(dt, 1.0, xs, 0.0, ys, precision=precision)
         torch.cuda.synchronize()
         a0 = torch.cuda.Event(enable_timing=True)
@@ -473,8 +588,9 @@ def main():
         torch.cuda.synchronize()
         return a0.elapsed_time(a1) / 1e3 / reps
 
-    t64 = time_apply(mat, "fp64")
-    t32 = time_apply(mat, "fp32")
+    preps = 5 if d <= 4 else 2
+    t64 = time_apply(mat, "fp64", preps)
+    t32 = time_apply(mat, "fp32", preps)
     fp64_peak = ab._lib.C.c_double()
     ab.lib.asgk_measure_fma_peak(0, ab._lib.C.byref(fp64_peak))
     fp32_peak = ab._lib.C.c_double()
@@ -485,124 +601,48 @@ def main():
                  "achieved": flops / t64 / 1e12, "peak": fp64_peak.value,
                  "peak_source": "measured live (FMA chain kernel)",
                  "unit": "TFLOP/s", "frac": flops / t64 / 1e12 / fp64_peak.value,
-                 "traffic": KERNEL_TRAFFIC.get(args.workload),
+                 "traffic": KERNEL_TRAFFIC.get(("pairs", workload)),
                  "traffic_source": "ncu dram__bytes_read+write, one launch",
                  "ms_per_launch": t64 * 1e3, "flops_per_launch": flops,
                  "fp32_kernel": {"ms_per_launch": t32 * 1e3,
                                  "achieved": flops / t32 / 1e12,
                                  "peak": fp32_peak.value,
                                  "frac": flops / t32 / 1e12 / fp32_peak.value}}
-    if gmat is not None:
-        # the method's operator kernel: algorithmic bytes per launch are x
-        # read once, y written, the neighbour lists and the pre-summed blocks
-        tg = time_apply(gmat, method["precision"])
-        nbytes = (16 * N + 8 * gmat.num_pairs() + 8 * (op.rows + 1)
-                  + 48 * len(op.vA) // (9 * T))
-        hbm = _measured_hbm_gbs()
-        roofline = {"bound": "hbm",
-                    "kernel": f"kron_global_rows<d={d}, {method['precision']}>",
-                    "achieved": nbytes / tg / 1e9, "peak": hbm,
-                    "peak_source": "MEASURED_PEAKS.json hbm_gbs" if hbm != 6650.0
-                                   else "fallback 6.65 TB/s",
-                    "unit": "GB/s", "frac": nbytes / tg / 1e9 / hbm,
-                    "traffic": GLOBAL_TRAFFIC.get(args.workload),
-                    "traffic_source": "ncu dram__bytes_read+write, one launch",
-                    "bytes_per_launch": nbytes, "ms_per_launch": tg * 1e3,
-                    "note": "working set L2-resident; launch/latency bound",
-                    "pair_kernel": pair_roof}
-    else:
-        roofline = pair_roof
-
-    # ---- e2e through the public API with host buffers
-    e2e_value = None
-    hb = torch.empty(N, dtype=torch.float64, pin_memory=True)
-    hx = torch.empty(N, dtype=torch.float64, pin_memory=True)
-    hb.copy_(B[0].cpu())
-    replicas.barrier()
-    e0.record()
-    for i in range(args.e2e_steps):
-        bd = hb.to("cuda", non_blocking=True)
-        x, _ = solve(bd, method["precision"], method["precond"])
-        hx.copy_(x, non_blocking=True)
-    e1.record()
-    replicas.barrier()
-    t_local = e0.elapsed_time(e1) / 1e3
-    e2e_value = replicas.throughput(args.e2e_steps, t_local)
-
-    # ---- CPU baseline (rank 0, N = 1): the reference compiled from source
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(op, cfg, pinfo.iterations)
-
-    if rank == 0:
-        line = {
-            "metric": METRIC, "value": value, "unit": "solves/s",
-            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": t_method / args.steps * 1e3,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64", "data": "synthetic",
-            "config": dict(_config(args.workload), method=args.method,
-                           parallelism=f"replicas x{world}"),
-            "plain_fp64": {"value": plain_value, "unit": "solves/s",
-                           "iterations": pinfo.iterations,
-                           "true_relres": max(i.true_relres for i in pinfos),
-                           "ms_per_solve": t_plain / args.plain_steps * 1e3},
-            "method": {"name": method["name"],
-                       "iterations": [i.iterations for i in minfos],
-                       "true_relres": max(i.true_relres for i in minfos),
-                       "outer_steps": minfos[0].outer_steps,
-                       "matvecs_low": minfos[0].matvecs_low,
-                       "matvecs_fp64": minfos[0].matvecs_fp64,
-                       "precond_calls": minfos[0].precond_calls,
-                       "fallback": max(i.fallback for i in minfos),
-                       "training": train_info,
-                       "speedup_vs_plain": value / plain_value},
-            "clocks": clk,
-            "e2e": {"value": e2e_value, "unit": "solves/s",
-                    "h2d_bytes_per_step": N * 8, "d2h_bytes_per_step": N * 8},
-            "gpu_launches": launches,
-            "pair_operator_method": pair_method,
-            "roofline": roofline,
-            "cpu_baseline": cpu,
-        }
-        print(json.dumps(line))
-    replicas.shutdown()
+    if gmat is None:
+        return pair_roof
+    # the method's operator kernel: algorithmic bytes per launch are x read
+    # once, y written, the neighbour lists and the pre-summed blocks
+    tg = time_apply(gmat, method["precision"], 10)
+    nbytes = (16 * N + 8 * gmat.num_pairs() + 8 * (op.rows + 1)
+              + 48 * len(op.vA) // (9 * op.terms))
+    hbm, src = _measured_hbm_gbs()
+    return {"bound": "hbm",
+            "kernel": f"kron_global_rows<d={d}, {method['precision']}>",
+            "achieved": nbytes / tg / 1e9, "peak": hbm, "peak_source": src,
+            "unit": "GB/s", "frac": nbytes / tg / 1e9 / hbm,
+            "traffic": KERNEL_TRAFFIC.get(("global", workload)),
+            "traffic_source": "ncu dram__bytes_read+write, one launch",
+            "bytes_per_launch": nbytes, "ms_per_launch": tg * 1e3,
+            "pair_kernel": pair_roof}
 
 
-def cpu_baseline(op, cfg, iters):
-    """The reference's CPU paths on the host cores (bounded sample: one
-    full-operator product each, converted with the plain iteration count):
-    cpu_sparse (local-kron kronmult_matrix::apply) and, where available, the
-    global Kronecker product; value = the faster."""
-    import numpy as np
+def cpu_baseline(workload):
+    """One full solve by the reference's own CPU path (ReferenceSolves) on
+    the host cores; value = 1 / its wall time.  Setup (the reference's
+    global matrix and preconditioner) is not timed."""
     import oracle
-    if not oracle.ref_available():
+    if not oracle.ref_gsolve_available():
         return {"value": None, "unit": "solves/s", "cores": 0, "kind": "reference",
                 "sample": "reference library not built"}
-    R = oracle.ref()
-    iA = op.iA()
-    pntr = op.row_ptr.astype(np.int32)
-    x = np.random.default_rng(0).uniform(-1, 1, op.N)
-    y = np.zeros(op.N)
-    t0 = time.perf_counter()
-    oracle.kronmult(op.d, 3, pntr, op.col, op.terms, iA, op.vA, -cfg["dt"], x,
-                    0.0, y, lib=R)
-    t_sparse = time.perf_counter() - t0
-    cores = R.ref_num_threads()
-    out = {"value": 1.0 / (t_sparse * iters), "unit": "solves/s",
-           "cores": cores, "kind": "reference",
-           "sample": f"1 full-operator product of the reference cpu_sparse kronmult "
-                     f"({t_sparse:.3f} s, {cores} OpenMP threads) x {iters} GMRES iterations",
-           "apply_s": t_sparse, "cpu_sparse_value": 1.0 / (t_sparse * iters)}
-    g = _ref_global(op.d, op.level, op.terms, op.table, op.vA, op.N)
-    if g is not None:
-        _, t_global = g.apply(x, reps=3)
-        out.update(value=1.0 / (t_global * iters), apply_s=t_global,
-                   global_cpu_value=1.0 / (t_global * iters),
-                   sample=f"best of 3 full-operator products of the reference's global "
-                          f"Kronecker product ({t_global * 1e3:.1f} ms, {cores} OpenMP "
-                          f"threads; cpu_sparse {t_sparse:.2f} s) x {iters} GMRES iterations")
-    return out
+    ref = ReferenceSolves(workload, seed=1)
+    s = ref.full_solve()
+    return {"value": 1.0 / s["seconds"], "unit": "solves/s", "cores": ref.cores,
+            "kind": "reference",
+            "sample": f"one full solve by the reference's solver::simple_gmres_euler "
+                      f"over its global_kron_matrix ({s['iterations']} iterations, "
+                      f"{s['seconds']:.1f} s, true relres {s['true_relres']:.2e}, "
+                      f"OpenMP {ref.cores} threads)",
+            "solve": s, "setup_s": ref.setup_s}
 
 
 if __name__ == "__main__":

@@ -157,6 +157,137 @@ def ref_global_apply(d, n, level, table, terms, vA, x, reps=1):
     return RefGlobal(d, n, level, table, terms, vA).apply(x, reps)
 
 
+REF_GSOLVE_SO = os.path.join(HERE, "_ref", "libasgard_ref_gsolve.so")
+_ref_gsolve = None
+
+
+def ref_gsolve_available() -> bool:
+    return os.path.exists(REF_GSOLVE_SO)
+
+
+def _gsolve_lib():
+    global _ref_gsolve
+    if _ref_gsolve is None:
+        if not ref_gsolve_available():
+            raise FileNotFoundError(REF_GSOLVE_SO)
+        _load_blas_deps()
+        lib = C.CDLL(REF_GSOLVE_SO)
+        lib.ref_gsolve_create_synthetic.argtypes = [
+            C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, _i32p, _i32p,
+            _f64p, _f64p]
+        lib.ref_gsolve_create_synthetic.restype = C.c_void_p
+        lib.ref_gsolve_create_builtin.argtypes = [C.c_char_p, C.c_int, C.c_int,
+                                                  C.c_int]
+        lib.ref_gsolve_create_builtin.restype = C.c_void_p
+        lib.ref_gsolve_destroy.argtypes = [C.c_void_p]
+        lib.ref_gsolve_destroy.restype = None
+        lib.ref_gsolve_info.argtypes = [C.c_void_p, C.POINTER(C.c_int),
+                                        C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                        C.POINTER(C.c_int64)]
+        lib.ref_gsolve_table.argtypes = [C.c_void_p, _i32p]
+        lib.ref_gsolve_precond.argtypes = [C.c_void_p, _f64p]
+        lib.ref_gsolve_apply.argtypes = [C.c_void_p, C.c_double, _f64p,
+                                         C.c_double, _f64p,
+                                         C.POINTER(C.c_double)]
+        lib.ref_gsolve_gmres_euler.argtypes = [
+            C.c_void_p, C.c_double, _f64p, _f64p, C.c_int, C.c_int,
+            C.c_double, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_int),
+            C.POINTER(C.c_double)]
+        _ref_gsolve = lib
+    return _ref_gsolve
+
+
+def load_ops1d(path=None):
+    """The level-7 1D blocks the synthetic advection/diffusion operators are
+    made of (generated from the reference by tests/golden/make_golden.py):
+    pntr/indx (level-7 1D connectivity), adv, dif (one column-major 3x3 block
+    per connection)."""
+    if path is None:
+        path = os.path.join(os.path.dirname(HERE), "asgard_b200", "data",
+                            "ops1d_L7.npz")
+    z = np.load(path)
+    return {k: np.ascontiguousarray(z[k]) for k in z.files}
+
+
+class RefGlobalSolver:
+    """The reference's implicit global-Kronecker path end to end
+    (``oracle/ref_gsolve_shim.cpp``): its sparse grid, make_global_kron_matrix,
+    set_specific_mode (values + diagonal preconditioner), the operator's CPU
+    apply and solver::simple_gmres_euler (src/solver.cpp:93-117, left diagonal
+    preconditioning, absolute tolerance on the estimated preconditioned
+    residual), OpenMP on all host threads.
+
+    ``RefGlobalSolver.synthetic(d, level, terms, nu)`` builds the benchmark's
+    advection/diffusion operator; ``RefGlobalSolver.builtin(name, d, level,
+    n)`` a built-in reference PDE."""
+
+    def __init__(self, handle):
+        self._lib = _gsolve_lib()
+        if not handle:
+            raise ValueError("the reference rejected the operator")
+        self._h = handle
+        d, n, cells, N = C.c_int(), C.c_int(), C.c_int(), C.c_int64()
+        self._lib.ref_gsolve_info(self._h, C.byref(d), C.byref(n),
+                                  C.byref(cells), C.byref(N))
+        self.d, self.n, self.cells, self.N = d.value, n.value, cells.value, N.value
+
+    @classmethod
+    def synthetic(cls, d, level, terms, nu, ops=None):
+        ops = ops if ops is not None else load_ops1d()
+        lib = _gsolve_lib()
+        h = lib.ref_gsolve_create_synthetic(
+            d, level, terms, 3, nu, ops["pntr"].astype(np.int32),
+            ops["indx"].astype(np.int32),
+            ops["adv"].astype(np.float64).reshape(-1),
+            ops["dif"].astype(np.float64).reshape(-1))
+        return cls(h)
+
+    @classmethod
+    def builtin(cls, name, d, level, n):
+        lib = _gsolve_lib()
+        return cls(lib.ref_gsolve_create_builtin(name.encode(), d, level, n))
+
+    def table(self):
+        t = np.zeros((self.cells, 2 * self.d), np.int32)
+        self._lib.ref_gsolve_table(self._h, t)
+        return t
+
+    def precond(self):
+        """The reference's diagonal preconditioner values pc (its solve
+        divides by 1 - dt*pc)."""
+        pc = np.zeros(self.N)
+        if self._lib.ref_gsolve_precond(self._h, pc) != 0:
+            raise ValueError("no preconditioner built")
+        return pc
+
+    def apply(self, alpha, x, beta=0.0, y=None):
+        """y <- beta*y + alpha*K*x; returns (y, seconds)."""
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.zeros(self.N) if y is None else y
+        sec = C.c_double()
+        if self._lib.ref_gsolve_apply(self._h, alpha, x, beta, y,
+                                      C.byref(sec)) != 0:
+            raise ValueError("apply failed")
+        return y, sec.value
+
+    def gmres_euler(self, dt, x, b, restart, max_iter, tol, quiet=True):
+        """solver::simple_gmres_euler in place on x; returns (error,
+        iterations, seconds)."""
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        err, its, sec = C.c_double(), C.c_int(), C.c_double()
+        rc = self._lib.ref_gsolve_gmres_euler(
+            self._h, dt, x, b, restart, max_iter, tol, int(quiet),
+            C.byref(err), C.byref(its), C.byref(sec))
+        if rc != 0:
+            raise ValueError("simple_gmres_euler failed")
+        return err.value, its.value, sec.value
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            self._lib.ref_gsolve_destroy(self._h)
+            self._h = None
+
+
 def ref():
     """The reference compiled from source; raises if it was not built."""
     global _ref
