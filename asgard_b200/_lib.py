@@ -17,7 +17,8 @@ EXPORTS = [
     "asgk_plan_update_terms", "asgk_plan_set_workspace", "asgk_plan_create_grid",
     "asgk_plan_destroy", "asgk_plan_update_values", "asgk_plan_info",
     "asgk_apply", "asgk_apply_f32", "asgk_apply_host", "asgk_apply_euler",
-    "asgk_gmres_euler", "asgk_gmres_dense", "asgk_default_gmres_restarts",
+    "asgk_gmres_euler", "asgk_gmres_dense", "asgk_gmres_dense_precond",
+    "asgk_default_gmres_restarts",
     "asgk_cgs_step", "asgk_cgs_step_noalloc",
     "asgk_sparse_grid", "asgk_connect_1d", "asgk_build_pairs",
     "asgk_direction_pairs",
@@ -78,6 +79,8 @@ def _load():
         "asgk_apply_euler": ([_vp, _i, _d, _d, _vp, _d, _vp, _vp], _i),
         "asgk_gmres_euler": ([_vp, _d, _vp, _vp, _i, _i, _d, _i, _i, _vp, C.POINTER(GmresInfo), _vp], _i),
         "asgk_gmres_dense": ([_i, _vp, _vp, _vp, _i, _i, _d, C.POINTER(GmresInfo)], _i),
+        "asgk_gmres_dense_precond": ([_i, _vp, _vp, _vp, _vp, _i, _i, _d,
+                                      C.POINTER(GmresInfo)], _i),
         "asgk_default_gmres_restarts": ([_i64], _i),
         "asgk_cgs_step": ([_vp, _i64, _i, _vp, _i64, _vp, C.POINTER(_d), _vp], _i),
         "asgk_cgs_step_noalloc": ([_vp, _i64, _i, _vp, _i64, _vp, C.POINTER(_d), _vp], _i),

@@ -421,6 +421,23 @@ __global__ void k_dense_gemv(int n, const double *__restrict__ A, double alpha,
     y[row] = (beta == 0.0 ? 0.0 : beta * y[row]) + alpha * s;
 }
 
+// FP32 vectors of kronmult_matrix<float> solves to and from the FP64 copies
+// the solver works on
+__global__ void k_widen(int64_t n, const float *__restrict__ in,
+                        double *__restrict__ out)
+{
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n;
+       i += int64_t(gridDim.x) * blockDim.x)
+    out[i] = double(in[i]);
+}
+__global__ void k_narrow(int64_t n, const double *__restrict__ in,
+                         float *__restrict__ out)
+{
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n;
+       i += int64_t(gridDim.x) * blockDim.x)
+    out[i] = float(in[i]);
+}
+
 // ------------------------------------------------------------------ GMRES
 
 // Reference BLAS Givens generation (drotg), as reached by lib_dispatch::rotg.
@@ -1934,6 +1951,14 @@ int asgk_gmres_dense(int n, const double *A, double *x, const double *b,
                      int restart, int max_outer, double tol,
                      asgk_gmres_info *info)
 {
+  return asgk_gmres_dense_precond(n, A, x, b, nullptr, restart, max_outer, tol,
+                                  info);
+}
+
+int asgk_gmres_dense_precond(int n, const double *A, double *x, const double *b,
+                             const double *M, int restart, int max_outer,
+                             double tol, asgk_gmres_info *info)
+{
   try
   {
     if (n <= 0 || !A || !x || !b)
@@ -1946,14 +1971,76 @@ int asgk_gmres_dense(int n, const double *A, double *x, const double *b,
       max_outer = n;
     if (!(tol > 0))
       tol = 1e-12;
-    double *dA = nullptr, *dx = nullptr, *db = nullptr;
+    // the reference's dense_preconditioner (src/solver.cpp:11-38) factors M
+    // and applies M^-1 on the left to every residual and new basis vector,
+    // which is GMRES on (M^-1 A) x = M^-1 b: M^-1 is formed once here (LU
+    // with partial pivoting on the host) and applied after A on the device
+    std::vector<double> Minv, bp;
+    if (M != nullptr)
+    {
+      std::vector<double> lu(M, M + int64_t(n) * n);
+      std::vector<int> piv(n);
+      for (int c = 0; c < n; c++)
+      {
+        int p = c;
+        for (int r = c + 1; r < n; r++)
+          if (std::abs(lu[r + int64_t(c) * n]) > std::abs(lu[p + int64_t(c) * n]))
+            p = r;
+        if (lu[p + int64_t(c) * n] == 0.0 || !std::isfinite(lu[p + int64_t(c) * n]))
+          return ASGK_ERR_BREAKDOWN;
+        piv[c] = p;
+        if (p != c)
+          for (int j = 0; j < n; j++)
+            std::swap(lu[c + int64_t(j) * n], lu[p + int64_t(j) * n]);
+        double const inv = 1.0 / lu[c + int64_t(c) * n];
+        for (int r = c + 1; r < n; r++)
+          lu[r + int64_t(c) * n] *= inv;
+        for (int j = c + 1; j < n; j++)
+        {
+          double const u = lu[c + int64_t(j) * n];
+          if (u != 0.0)
+            for (int r = c + 1; r < n; r++)
+              lu[r + int64_t(j) * n] -= lu[r + int64_t(c) * n] * u;
+        }
+      }
+      auto solve = [&](double *v) {
+        for (int c = 0; c < n; c++)
+          if (piv[c] != c)
+            std::swap(v[c], v[piv[c]]);
+        for (int c = 0; c < n; c++)
+          for (int r = c + 1; r < n; r++)
+            v[r] -= lu[r + int64_t(c) * n] * v[c];
+        for (int c = n - 1; c >= 0; c--)
+        {
+          v[c] /= lu[c + int64_t(c) * n];
+          for (int r = 0; r < c; r++)
+            v[r] -= lu[r + int64_t(c) * n] * v[c];
+        }
+      };
+      Minv.assign(int64_t(n) * n, 0.0);
+      for (int j = 0; j < n; j++)
+      {
+        double *col = Minv.data() + int64_t(j) * n;
+        col[j]      = 1.0;
+        solve(col);
+      }
+      bp.assign(b, b + n);
+      solve(bp.data());
+      b = bp.data();
+    }
+    double *dA = nullptr, *dx = nullptr, *db = nullptr, *dM = nullptr,
+           *dt = nullptr;
     int64_t bytes = 0;
     int rc;
     if ((rc = dev_alloc(&dA, int64_t(n) * n, bytes)) ||
-        (rc = dev_alloc(&dx, n, bytes)) || (rc = dev_alloc(&db, n, bytes)))
+        (rc = dev_alloc(&dx, n, bytes)) || (rc = dev_alloc(&db, n, bytes)) ||
+        (M != nullptr && ((rc = dev_alloc(&dM, int64_t(n) * n, bytes)) ||
+                          (rc = dev_alloc(&dt, n, bytes)))))
     {
       cudaFree(dA);
       cudaFree(dx);
+      cudaFree(db);
+      cudaFree(dM);
       return rc;
     }
     cudaStream_t s = nullptr;
@@ -1961,14 +2048,25 @@ int asgk_gmres_dense(int n, const double *A, double *x, const double *b,
     core_stats st;
     auto mat = [&](double a, const double *xin, double bb, double *yout,
                    cudaStream_t ss) -> int {
-      k_dense_gemv<<<(n + 3) / 4, 128, 0, ss>>>(n, dA, a, xin, bb, yout);
+      if (dM == nullptr)
+      {
+        k_dense_gemv<<<(n + 3) / 4, 128, 0, ss>>>(n, dA, a, xin, bb, yout);
+        ASGK_LAUNCHED();
+        return ASGK_OK;
+      }
+      k_dense_gemv<<<(n + 3) / 4, 128, 0, ss>>>(n, dA, 1.0, xin, 0.0, dt);
+      ASGK_LAUNCHED();
+      k_dense_gemv<<<(n + 3) / 4, 128, 0, ss>>>(n, dM, a, dt, bb, yout);
       ASGK_LAUNCHED();
       return ASGK_OK;
     };
     rc = ASGK_OK;
     if (cudaMemcpy(dA, A, sizeof(double) * n * int64_t(n), cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMemcpy(dx, x, sizeof(double) * n, cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemcpy(db, b, sizeof(double) * n, cudaMemcpyHostToDevice) != cudaSuccess)
+        cudaMemcpy(db, b, sizeof(double) * n, cudaMemcpyHostToDevice) != cudaSuccess ||
+        (dM != nullptr &&
+         cudaMemcpy(dM, Minv.data(), sizeof(double) * n * int64_t(n),
+                    cudaMemcpyHostToDevice) != cudaSuccess))
       rc = ASGK_ERR_CUDA;
     if (rc == ASGK_OK)
       rc = gmres_core(ws, n, mat, nullptr, dx, db, restart, max_outer, tol, st, s);
@@ -1978,6 +2076,8 @@ int asgk_gmres_dense(int n, const double *A, double *x, const double *b,
     cudaFree(dA);
     cudaFree(dx);
     cudaFree(db);
+    cudaFree(dM);
+    cudaFree(dt);
     if (rc == ASGK_OK && info)
     {
       *info              = asgk_gmres_info{};
@@ -2303,8 +2403,11 @@ int asgk_gmres_euler_jacobi(asgk_plan *plan, double dt, double *x,
 {
   try
   {
-    if (precond == nullptr)
+    if (precond == nullptr || plan == nullptr)
       return ASGK_ERR_INVALID;
+    // a preconditioner of another shape would index past v and z
+    if (int rc = jacobi_check_shape(precond, plan->p.rows, plan->p.tensor))
+      return rc;
     cudaStream_t s = as_stream(stream);
     make_pc_t const mk = [&](bool low) -> precond_t {
       return [=](double *v, double *z, const double *sc, float *vc,
@@ -2315,6 +2418,53 @@ int asgk_gmres_euler_jacobi(asgk_plan *plan, double dt, double *x,
     return gmres_euler_impl(plan, dt, x, b, restart, max_outer, tol, tol_mode,
                             precision, &mk, info, stream, jacobi_serial(precond),
                             true);
+  }
+  catch (std::bad_alloc const &)
+  {
+    return ASGK_ERR_ALLOC;
+  }
+  catch (...)
+  {
+    return ASGK_ERR_INVALID;
+  }
+}
+
+int asgk_gmres_euler_f32(asgk_plan *plan, float dt, float *x, const float *b,
+                         int restart, int max_outer, float tol,
+                         asgk_gmres_info *info, asgk_stream stream)
+{
+  try
+  {
+    if (!plan || !x || !b)
+      return ASGK_ERR_INVALID;
+    int64_t const n = int64_t(plan->p.rows) * plan->p.tensor;
+    if (plan->p.rows != plan->p.cols)
+      return ASGK_ERR_INVALID;
+    cudaStream_t s = as_stream(stream);
+    double *w      = nullptr;
+    int64_t unused = 0;
+    if (int rc = dev_alloc(&w, std::max<int64_t>(2 * n, 1), unused))
+      return rc;
+    double *xd = w, *bd = w + n;
+    int const blocks = int(std::min<int64_t>((n + 255) / 256, 65535));
+    k_widen<<<blocks, 256, 0, s>>>(n, x, xd);
+    k_widen<<<blocks, 256, 0, s>>>(n, b, bd);
+    int rc = cudaGetLastError() == cudaSuccess ? ASGK_OK : ASGK_ERR_CUDA;
+    count_launch(2);
+    if (rc == ASGK_OK)
+      rc = gmres_euler_impl(plan, double(dt), xd, bd, restart, max_outer,
+                            tol > 0 ? double(tol) : 1e-6, ASGK_TOL_ABS,
+                            ASGK_FP32, nullptr, info, stream);
+    if (rc == ASGK_OK)
+    {
+      k_narrow<<<blocks, 256, 0, s>>>(n, xd, x);
+      rc = cudaGetLastError() == cudaSuccess ? ASGK_OK : ASGK_ERR_CUDA;
+      count_launch(1);
+    }
+    if (cudaStreamSynchronize(s) != cudaSuccess && rc == ASGK_OK)
+      rc = ASGK_ERR_CUDA;
+    cudaFree(w);
+    return rc;
   }
   catch (std::bad_alloc const &)
   {
@@ -2364,6 +2514,12 @@ int asgk_implicit_advance(asgk_plan *plan, double dt, double *x, int steps,
       return ASGK_ERR_INVALID;
     int64_t const n = int64_t(p.rows) * p.tensor;
     if (forcing && forcing_stride != 0 && forcing_stride < n)
+      return ASGK_ERR_INVALID;
+    // a preconditioner of another shape is refused before any launch
+    if ((pc_kind == 1 &&
+         jacobi_check_shape(static_cast<asgk_jacobi *>(precond), p.rows, p.tensor)) ||
+        (pc_kind == 2 &&
+         mlp_check_shape(static_cast<asgk_mlp *>(precond), p.rows, p.tensor)))
       return ASGK_ERR_INVALID;
     cudaStream_t s = as_stream(stream);
     double *b      = nullptr;
@@ -2424,6 +2580,18 @@ int asgk_imex_advance(asgk_plan *explicit_plan, asgk_plan *implicit_plan,
     if (implicit_plan &&
         int64_t(implicit_plan->p.rows) * implicit_plan->p.tensor != n)
       return ASGK_ERR_INVALID;
+    // each stage's preconditioner must fit the implicit plan and invert
+    // I - dt*K for that stage's step: dt (stage 1) and dt/2 (stage 2)
+    for (int st = 0; st < 2; st++)
+    {
+      asgk_jacobi *pc = st == 0 ? pc_stage1 : pc_stage2;
+      if (pc == nullptr)
+        continue;
+      if (!implicit_plan ||
+          jacobi_check_shape(pc, implicit_plan->p.rows, implicit_plan->p.tensor) ||
+          jacobi_dt(pc) != (st == 0 ? dt : 0.5 * dt))
+        return ASGK_ERR_INVALID;
+    }
     cudaStream_t s = as_stream(stream);
     // f_0, the explicit product, f_1 (then f_1 + dt E f_1), the stage-1
     // solution (then the stage-2 solve's iterate)

@@ -14,7 +14,7 @@
 //   * k <= kMaxK (256) columns, and at most kMaxBlocks (512)
 //     reduction blocks (2 per SM, so GPUs with up to 256 SMs); larger requests
 //     return ASGK_ERR_NOALLOC_LIMIT without touching any argument;
-//   * the array (kScratch doubles, about 1 MiB) exists on every GPU that loads
+//   * the array (kScratch doubles, 1 MiB) exists on every GPU that loads
 //     the library and is held until the process exits;
 //   * every call writes the partial sums it later reads, so nothing has to
 //     start at zero, but all calls on a device share the one array: calls that
@@ -32,7 +32,10 @@ namespace
 {
 constexpr int kMaxK      = 256;
 constexpr int kMaxBlocks = 512;
-constexpr size_t kNormSlot = size_t(kMaxBlocks) * (kMaxK + 1);
+// the multi-dot pass writes one partial sum per (block, column), at most
+// kMaxBlocks * kMaxK; the norm pass then reuses the start of that region for
+// its kMaxBlocks partials, and their sum goes to the slot after it
+constexpr size_t kNormSlot = size_t(kMaxBlocks) * kMaxK;
 constexpr size_t kScratch  = kNormSlot + 1;
 } // namespace
 
@@ -73,9 +76,10 @@ int scratch_address(double **out)
 }
 } // namespace
 
-extern "C" int asgk_cgs_step_noalloc(const double *V, int64_t ldv, int k,
-                                     double *w, int64_t n, double *h,
-                                     double *norm, asgk_stream stream)
+namespace
+{
+int cgs_step_noalloc(const double *V, int64_t ldv, int k, double *w, int64_t n,
+                     double *h, double *norm, asgk_stream stream)
 {
   using namespace asgk;
   if (!V || !w || !h || !norm || k < 1 || n < 1 || ldv < n)
@@ -116,4 +120,25 @@ extern "C" int asgk_cgs_step_noalloc(const double *V, int64_t ldv, int k,
   ASGK_CUDA(cudaStreamSynchronize(s));
   *norm = std::sqrt(host);
   return ASGK_OK;
+}
+} // namespace
+
+// As every status-returning entry of the C ABI, no host exception crosses
+// the boundary (the mutex of the address cache can throw std::system_error).
+extern "C" int asgk_cgs_step_noalloc(const double *V, int64_t ldv, int k,
+                                     double *w, int64_t n, double *h,
+                                     double *norm, asgk_stream stream)
+{
+  try
+  {
+    return cgs_step_noalloc(V, ldv, k, w, n, h, norm, stream);
+  }
+  catch (std::bad_alloc const &)
+  {
+    return ASGK_ERR_ALLOC;
+  }
+  catch (...)
+  {
+    return ASGK_ERR_INVALID;
+  }
 }

@@ -199,6 +199,13 @@ int jacobi_apply_handle(asgk_jacobi *pc, bool low, double *v, double *z,
                         cudaStream_t s);
 // never reused within a process: identifies a preconditioner in caches
 uint64_t jacobi_serial(const asgk_jacobi *pc);
+// ASGK_OK when the preconditioner applies to vectors of rows * tensor
+// values (the shape of the plan it was built on), else ASGK_ERR_INVALID:
+// its kernels index their own tables by the cells of that plan and read and
+// write rows * tensor values of v and z
+int jacobi_check_shape(const asgk_jacobi *pc, int rows, int tensor);
+// the step size the preconditioner inverts I - dt*K for
+double jacobi_dt(const asgk_jacobi *pc);
 
 // kron_global.cu: global-mode apply
 int launch_global(plan_data const &p, int precision, double alpha,

@@ -909,6 +909,15 @@ int asgk_jacobi_apply(asgk_jacobi *pc, const double *v, double *z,
 
 uint64_t asgk::jacobi_serial(const asgk_jacobi *pc) { return pc ? pc->jd.serial : 0; }
 
+int asgk::jacobi_check_shape(const asgk_jacobi *pc, int rows, int tensor)
+{
+  if (pc == nullptr || pc->jd.rows != rows || pc->jd.ts != tensor)
+    return ASGK_ERR_INVALID;
+  return ASGK_OK;
+}
+
+double asgk::jacobi_dt(const asgk_jacobi *pc) { return pc ? pc->jd.dt : 0.0; }
+
 int asgk::jacobi_apply_handle(asgk_jacobi *pc, bool low, double *v, double *z,
                               const double *scale_state, float *vcopy,
                               cudaStream_t s)

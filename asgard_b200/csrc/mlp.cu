@@ -622,6 +622,12 @@ struct mlp_state
   }
 };
 
+int mlp_check_shape(const asgk_mlp *mlp, int rows, int tensor)
+{
+  auto const *m = reinterpret_cast<const mlp_state *>(mlp);
+  return (m && m->cells == rows && m->ts == tensor) ? ASGK_OK : ASGK_ERR_INVALID;
+}
+
 int mlp_precondition(asgk_mlp *mlp, asgk_plan *plan, const double *v,
                      double *z, cudaStream_t s, bool low)
 {
@@ -1085,6 +1091,9 @@ int asgk_mlp_set_base(asgk_mlp *mlp, asgk_jacobi *base)
   {
     auto *m = reinterpret_cast<mlp_state *>(mlp);
     if (!m)
+      return ASGK_ERR_INVALID;
+    // the base is applied to the network's full vectors (cells * n^d)
+    if (base != nullptr && jacobi_check_shape(base, m->cells, m->ts))
       return ASGK_ERR_INVALID;
     m->base = base;
     return ASGK_OK;

@@ -9,4 +9,6 @@ namespace asgk
 // (plus its base preconditioner, from its FP32 copy when low is set).
 int mlp_precondition(asgk_mlp *mlp, asgk_plan *plan, const double *v,
                      double *z, cudaStream_t s, bool low);
+// ASGK_OK when the network applies to rows cells of tensor values each
+int mlp_check_shape(const asgk_mlp *mlp, int rows, int tensor);
 } // namespace asgk

@@ -406,9 +406,9 @@ def imex_advance(dt, explicit: kronmult_matrix, implicit, x, steps, restart=-1,
 
 
 def simple_gmres(A, x, b, M=None, restart=-1, max_iter=-1, tol=-1.0):
-    """Dense test path of solver::simple_gmres (host arrays, solved on the GPU)."""
-    if M is not None and np.size(M) > 0:
-        raise NotImplementedError("dense LU preconditioner is not provided")
+    """Dense test path of solver::simple_gmres (host arrays, solved on the
+    GPU).  M: the reference's dense preconditioner (src/solver.cpp:11-38),
+    LU-factored and applied on the left; None or an empty matrix for none."""
     A = np.asfortranarray(A, dtype=np.float64)
     n = A.shape[0]
     if restart is not None and restart > n:
@@ -416,9 +416,16 @@ def simple_gmres(A, x, b, M=None, restart=-1, max_iter=-1, tol=-1.0):
     bb = _host(b, np.float64)
     if not (x.flags["C_CONTIGUOUS"] and x.dtype == np.float64):
         raise ValueError("x must be a contiguous float64 array")
+    Mp = None
+    if M is not None and np.size(M) > 0:
+        Mf = np.asfortranarray(M, dtype=np.float64)
+        if Mf.shape != (n, n):
+            raise ValueError("M must be n x n")
+        Mp = Mf.ctypes.data
     info = GmresInfo()
-    check(lib.asgk_gmres_dense(n, A.ctypes.data, x.ctypes.data, bb.ctypes.data,
-                               restart, max_iter, tol, C.byref(info)),
+    check(lib.asgk_gmres_dense_precond(n, A.ctypes.data, x.ctypes.data,
+                                       bb.ctypes.data, Mp, restart, max_iter,
+                                       tol, C.byref(info)),
           "simple_gmres")
     return gmres_info(**info.as_dict())
 

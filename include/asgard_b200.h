@@ -245,10 +245,32 @@ int asgk_gmres_euler(asgk_plan *plan, double dt, double *x, const double *b,
                      asgk_stream stream);
 
 /* solver::simple_gmres on a dense column-major n x n host matrix (the test
- * path of src/solver.cpp:55-74, without the LU preconditioner). */
+ * path of src/solver.cpp:55-74) with an empty M: no preconditioner; the same
+ * as asgk_gmres_dense_precond with M = NULL. */
 int asgk_gmres_dense(int n, const double *A, double *x, const double *b,
                      int restart, int max_outer, double tol,
                      asgk_gmres_info *info);
+/* simple_gmres_euler of kronmult_matrix<float> (the reference's FP32
+ * instantiation, src/solver.cpp:119-135 with P = float,
+ * src/asgard_kronmult_matrix.cpp:1633): x (initial guess and result) and b
+ * are FP32 device vectors.  The solve runs on FP64 copies of them (allocated
+ * for the call) with the FP32 operator inside FP64 iterative refinement,
+ * stopping when the FP64 residual ||b - (I - dt K) x|| is at most tol (the
+ * reference's absolute criterion; tol <= 0 selects its FP32 default 1e-6),
+ * and x is rounded back to FP32.  Synchronises the stream. */
+int asgk_gmres_euler_f32(asgk_plan *plan, float dt, float *x, const float *b,
+                         int restart, int max_outer, float tol,
+                         asgk_gmres_info *info, asgk_stream stream);
+
+/* simple_gmres(A, x, b, M, restart, max_iter, tol) with the reference's
+ * dense preconditioner M (src/solver.cpp:11-38, 55-74): M (column-major
+ * host n x n, or NULL for none) is LU-factored with partial pivoting and
+ * applied on the left to the residual and to every new basis vector, so the
+ * tolerance is on the estimated preconditioned residual, as in the
+ * reference.  A singular M: ASGK_ERR_BREAKDOWN before any device work. */
+int asgk_gmres_dense_precond(int n, const double *A, double *x,
+                             const double *b, const double *M, int restart,
+                             int max_outer, double tol, asgk_gmres_info *info);
 
 /* One classical Gram-Schmidt step of the device GMRES, the two GEMVs and the
  * norm of src/solver.cpp:233-245:
@@ -263,7 +285,7 @@ int asgk_cgs_step(const double *V, int64_t ldv, int k, double *w, int64_t n,
  * allocate once their solve runs (all device memory handed to their own pool
  * at start-up, or no device-wide synchronisation allowed).  No counterpart in
  * the reference.  Same arguments and result as asgk_cgs_step; the partial
- * sums use a fixed array of about 1 MiB inside the library (held on every
+ * sums use a fixed array of 1 MiB inside the library (held on every
  * GPU that loads it until exit).  k <= 256 columns and at most 512 reduction
  * blocks (GPUs up to 256 SMs), else ASGK_ERR_NOALLOC_LIMIT.  All calls share
  * the array: calls that overlap on the GPU race.  The first call on a device
@@ -312,7 +334,9 @@ int asgk_jacobi_info(asgk_jacobi *pc, int *kind, double *dt,
 /* asgk_gmres_euler with a Jacobi preconditioner applied on the right
  * (flexible GMRES; the reference applies its diagonal one to the residual).
  * With ASGK_FP32 the block inverses are applied from an FP16 copy (FP64
- * accumulation): an inexact preconditioner, which flexible GMRES allows. */
+ * accumulation): an inexact preconditioner, which flexible GMRES allows.
+ * A preconditioner built on a plan of another shape (cells or n^d) is
+ * refused with ASGK_ERR_INVALID before any launch. */
 int asgk_gmres_euler_jacobi(asgk_plan *plan, double dt, double *x,
                             const double *b, int restart, int max_outer,
                             double tol, int tol_mode, int precision,
@@ -409,7 +433,8 @@ typedef int (*asgk_imex_hook)(void *ctx, int step, int stage, int event,
  * part (the reference without a collision operator): f_1 = f_1s and the
  * step ends with f_2s.  The solves take restart, max_outer, tol, tol_mode
  * and precision as asgk_gmres_euler; pc_stage1 / pc_stage2 (or null) are
- * Jacobi preconditioners of the implicit plan for dt and dt/2.  hook (or
+ * Jacobi preconditioners of the implicit plan for dt and dt/2 (one of
+ * another shape or step size: ASGK_ERR_INVALID before any work).  hook (or
  * null) with hook_ctx: see asgk_imex_hook.  info receives 2 entries per
  * step (stage 1, stage 2; zeros without an implicit plan), including
  * solves that stopped short of the tolerance (the loop goes on, as the

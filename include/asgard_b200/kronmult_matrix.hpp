@@ -3,8 +3,12 @@
 // ABI of asgard_b200.h.  Header-only; link libasgard_b200.so.
 //
 // Differences from the reference types: vectors are std::vector (host) or raw
-// device pointers instead of fk::vector, and only P = double is provided (the
-// FP32 operator is reached through precision arguments).  Errors raise the
+// device pointers instead of fk::vector.  P = double and P = float are
+// provided, as the reference instantiates them (ASGARD_ENABLE_DOUBLE /
+// ASGARD_ENABLE_FLOAT, src/asgard_kronmult_matrix.cpp:1620-1640); a float
+// matrix keeps its factors as given (the plan also holds them widened to
+// FP64), applies device vectors in FP32 and host vectors through the FP64
+// host path.  Errors raise the
 // reference's exception types: std::runtime_error, and std::invalid_argument
 // for a restart larger than the system (src/solver.cpp:175-181).
 #pragma once
@@ -14,6 +18,7 @@
 #include <cstdint>
 #include <stdexcept>
 #include <string>
+#include <type_traits>
 #include <utility>
 #include <vector>
 
@@ -39,12 +44,23 @@ inline void check(int status, char const *what)
     throw std::runtime_error(std::string(what) + ": " + asgk_status_string(status));
 }
 
-template<typename P>
-class kronmult_matrix;
-
-template<>
-class kronmult_matrix<double>
+namespace detail
 {
+//! factors and vectors handed to the C ABI, which takes FP64 host arrays
+template<typename P>
+std::vector<double> widen(std::vector<P> const &v)
+{
+  return std::vector<double>(v.begin(), v.end());
+}
+inline std::vector<double> const &widen(std::vector<double> const &v) { return v; }
+} // namespace detail
+
+template<typename P>
+class kronmult_matrix
+{
+  static_assert(std::is_same_v<P, double> || std::is_same_v<P, float>,
+                "kronmult_matrix<P>: P is double or float");
+
 public:
   kronmult_matrix() = default;
 
@@ -53,16 +69,17 @@ public:
   kronmult_matrix(int num_dimensions, int kron_size, int num_rows,
                   int num_cols, int num_terms, std::vector<int> const &pntr,
                   std::vector<int> const &indx, std::vector<int> const &iA,
-                  std::vector<double> const &vA)
+                  std::vector<P> const &vA)
       : d_(num_dimensions), n_(kron_size), rows_(num_rows), cols_(num_cols),
         terms_(num_terms)
   {
     if (pntr.size() != size_t(num_rows) + 1)
       throw std::runtime_error("kronmult_matrix: pntr must have num_rows + 1 entries");
     std::vector<int64_t> rp(pntr.begin(), pntr.end());
+    auto const &wv = detail::widen(vA);
     check(asgk_plan_create(&plan_, d_, n_, rows_, cols_, terms_, rp.data(),
-                           indx.data(), iA.data(), vA.data(),
-                           int64_t(vA.size())),
+                           indx.data(), iA.data(), wv.data(),
+                           int64_t(wv.size())),
           "kronmult_matrix");
   }
 
@@ -76,7 +93,7 @@ public:
                   std::vector<std::vector<int>> const &list_pntr,
                   std::vector<std::vector<int>> const &list_indx,
                   std::vector<std::vector<int>> const &list_iA,
-                  std::vector<double> const &vA)
+                  std::vector<P> const &vA)
       : d_(num_dimensions), n_(kron_size), rows_(num_rows), cols_(num_cols),
         terms_(num_terms)
   {
@@ -97,9 +114,10 @@ public:
     }
     if (rp.size() != size_t(num_rows) + 1)
       throw std::runtime_error("kronmult_matrix: chunks must cover num_rows rows");
+    auto const &wv = detail::widen(vA);
     check(asgk_plan_create(&plan_, d_, n_, rows_, cols_, terms_, rp.data(),
-                           indx.data(), iA.data(), vA.data(),
-                           int64_t(vA.size())),
+                           indx.data(), iA.data(), wv.data(),
+                           int64_t(wv.size())),
           "kronmult_matrix");
   }
 
@@ -111,7 +129,7 @@ public:
                                          std::vector<std::vector<int>> const &list_row_indx,
                                          std::vector<std::vector<int>> const &list_col_indx,
                                          std::vector<std::vector<int>> const &list_iA,
-                                         std::vector<double> const &vA)
+                                         std::vector<P> const &vA)
   {
     if (list_row_indx.size() != list_col_indx.size() ||
         list_row_indx.size() != list_iA.size())
@@ -134,7 +152,7 @@ public:
                                     std::vector<int> const &row_indx,
                                     std::vector<int> const &col_indx,
                                     std::vector<int> const &iA,
-                                    std::vector<double> const &vA)
+                                    std::vector<P> const &vA)
   {
     kronmult_matrix m;
     m.d_     = num_dimensions;
@@ -147,7 +165,7 @@ public:
     check(asgk_plan_create_pairs(&m.plan_, m.d_, m.n_, m.rows_, m.cols_,
                                  m.terms_, int64_t(row_indx.size()),
                                  row_indx.data(), col_indx.data(), iA.data(),
-                                 vA.data(), int64_t(vA.size())),
+                                 detail::widen(vA).data(), int64_t(vA.size())),
           "kronmult_matrix");
     return m;
   }
@@ -159,7 +177,7 @@ public:
   //! cell; rows start at elem entry row_offset, columns at col_offset.
   kronmult_matrix(int num_dimensions, int kron_size, int num_rows,
                   int num_cols, int num_terms,
-                  std::vector<std::vector<double>> const &terms,
+                  std::vector<std::vector<P>> const &terms,
                   std::vector<int> const &elem, int row_offset, int col_offset,
                   int num_1d_blocks)
       : d_(num_dimensions), n_(kron_size), rows_(num_rows), cols_(num_cols),
@@ -167,9 +185,13 @@ public:
   {
     if (terms.size() != size_t(num_terms))
       throw std::runtime_error("kronmult_matrix: terms must hold num_terms arrays");
+    std::vector<std::vector<double>> wide;
     std::vector<double const *> tp;
     for (auto const &t : terms)
-      tp.push_back(t.data());
+    {
+      wide.push_back(detail::widen(t));
+      tp.push_back(wide.back().data());
+    }
     check(asgk_plan_create_dense(&plan_, d_, n_, rows_, cols_, terms_,
                                  tp.data(), elem.data(), int64_t(elem.size()),
                                  row_offset, col_offset, num_1d_blocks),
@@ -185,7 +207,7 @@ public:
   static kronmult_matrix global_form(int num_dimensions, int kron_size,
                                      int level, std::vector<int> const &table,
                                      int num_terms,
-                                     std::vector<double> const &vA)
+                                     std::vector<P> const &vA)
   {
     kronmult_matrix m;
     int const cells = int(table.size() / (2 * size_t(num_dimensions)));
@@ -195,8 +217,8 @@ public:
     m.cols_  = cells;
     m.terms_ = num_terms;
     check(asgk_plan_create_global(&m.plan_, num_dimensions, kron_size, level,
-                                  cells, table.data(), num_terms, vA.data(),
-                                  int64_t(vA.size())),
+                                  cells, table.data(), num_terms,
+                                  detail::widen(vA).data(), int64_t(vA.size())),
           "kronmult_matrix");
     return m;
   }
@@ -214,12 +236,25 @@ public:
   //! y = beta*y + alpha*K*x; rec says where x and y live
   //! (src/asgard_kronmult_matrix.hpp:340-478).  Not thread-safe, as there.
   template<resource rec = resource::host>
-  void apply(double alpha, double const x[], double beta, double y[]) const
+  void apply(P alpha, P const x[], P beta, P y[]) const
   {
-    if constexpr (rec == resource::host)
-      check(asgk_apply_host(plan_, alpha, x, beta, y, nullptr), "apply");
+    if constexpr (std::is_same_v<P, double>)
+    {
+      if constexpr (rec == resource::host)
+        check(asgk_apply_host(plan_, alpha, x, beta, y, nullptr), "apply");
+      else
+        check(asgk_apply(plan_, ASGK_FP64, alpha, x, beta, y, nullptr), "apply");
+    }
+    else if constexpr (rec == resource::device)
+      check(asgk_apply_f32(plan_, alpha, x, beta, y, nullptr), "apply");
     else
-      check(asgk_apply(plan_, ASGK_FP64, alpha, x, beta, y, nullptr), "apply");
+    {
+      std::vector<double> xd(x, x + input_size()), yd(y, y + output_size());
+      check(asgk_apply_host(plan_, alpha, xd.data(), beta, yd.data(), nullptr),
+            "apply");
+      for (size_t i = 0; i < yd.size(); i++)
+        y[i] = P(yd[i]);
+    }
   }
 
   //! num_rows * num_cols, as the reference returns for every matrix
@@ -256,17 +291,21 @@ public:
            kron_size * num_dimensions * num_terms * num_batch * 2;
   }
 
-  void update_stored_coefficients(std::vector<double> const &vA)
+  void update_stored_coefficients(std::vector<P> const &vA)
   {
-    check(asgk_plan_update_values(plan_, vA.data(), int64_t(vA.size())),
+    check(asgk_plan_update_values(plan_, detail::widen(vA).data(), int64_t(vA.size())),
           "update_stored_coefficients");
   }
   //! dense matrices: new per-term arrays (src/asgard_kronmult_matrix.hpp:538-561)
-  void update_stored_coefficients(std::vector<std::vector<double>> const &terms)
+  void update_stored_coefficients(std::vector<std::vector<P>> const &terms)
   {
+    std::vector<std::vector<double>> wide;
     std::vector<double const *> tp;
     for (auto const &t : terms)
-      tp.push_back(t.data());
+    {
+      wide.push_back(detail::widen(t));
+      tp.push_back(wide.back().data());
+    }
     check(asgk_plan_update_terms(plan_, tp.data(), int(terms.size())),
           "update_stored_coefficients");
   }
@@ -317,6 +356,28 @@ simple_gmres_euler(double dt, kronmult_matrix<double> const &mat, double *x,
   return gmres_info<double>{info.error, info.iterations};
 }
 
+//! The same for kronmult_matrix<float> on FP32 device vectors (the
+//! reference's FP32 instantiation): solved with the FP32 operator inside
+//! FP64 iterative refinement on FP64 copies (asgk_gmres_euler_f32), the
+//! reference's absolute criterion applied to the FP64 residual.
+inline gmres_info<float>
+simple_gmres_euler(float dt, kronmult_matrix<float> const &mat, float *x,
+                   float const *b, int restart, int max_iter, float tol)
+{
+  int64_t const n = mat.output_size();
+  if (restart > n)
+    throw std::invalid_argument("Number of inner iterations " +
+                                std::to_string(restart) + " must be less than " +
+                                std::to_string(n) + "!");
+  asgk_gmres_info info{};
+  check(asgk_gmres_euler_f32(mat.plan(), dt, x, b, restart, max_iter, tol, &info,
+                             nullptr),
+        "simple_gmres_euler");
+  if (info.status == ASGK_ERR_NONFINITE)
+    throw std::runtime_error("simple_gmres_euler: non-finite residual");
+  return gmres_info<float>{float(info.error), info.iterations};
+}
+
 //! A Jacobi preconditioner of I - dt*K built on the device and owned here:
 //! ASGK_JACOBI_POINT is the reference's diagonal preconditioner
 //! (build_preconditioner, src/asgard_kronmult_matrix.cpp:1015-1067);
@@ -355,15 +416,23 @@ private:
   double dt_       = 0;
 };
 
-//! The reference's global-kron simple_gmres_euler, which preconditions
-//! with its diagonal preconditioner (src/solver.cpp:93-117): here the
-//! caller's Jacobi preconditioner of (mat, dt), applied on the right
-//! through flexible GMRES; same criterion and result as the overload above.
+//! The counterpart of the reference's global-kron simple_gmres_euler, which
+//! preconditions with its diagonal preconditioner (src/solver.cpp:93-117):
+//! here the caller's Jacobi preconditioner of (mat, dt) is applied on the
+//! right through flexible GMRES, so the solve stops on the estimate of the
+//! unpreconditioned residual (absolute tolerance), whereas the reference
+//! applies its preconditioner on the left and stops on the preconditioned
+//! residual; iteration counts and the returned error therefore differ from
+//! the reference's.  A preconditioner built for another step size than dt
+//! is refused (std::invalid_argument).
 inline gmres_info<double>
 simple_gmres_euler(double dt, kronmult_matrix<double> const &mat, double *x,
                    double const *b, int restart, int max_iter, double tol,
                    jacobi_preconditioner const &pc)
 {
+  if (pc.dt() != dt)
+    throw std::invalid_argument("simple_gmres_euler: the preconditioner was built for dt = " +
+                                std::to_string(pc.dt()) + ", not " + std::to_string(dt));
   int64_t const n = mat.output_size();
   if (restart > n)
     throw std::invalid_argument("Number of inner iterations " +
@@ -379,21 +448,39 @@ simple_gmres_euler(double dt, kronmult_matrix<double> const &mat, double *x,
   return gmres_info<double>{info.error, info.iterations};
 }
 
-//! solver::simple_gmres on a dense column-major host matrix (no
-//! preconditioner) -- src/solver.cpp:55-74.
+//! solver::simple_gmres on a dense column-major host matrix with the
+//! reference's dense preconditioner M (src/solver.cpp:11-38, 55-74): M
+//! (column-major n x n) is LU-factored and applied on the left; an empty M
+//! means none, as an empty fk::matrix does there.
+inline gmres_info<double> simple_gmres(std::vector<double> const &A,
+                                       std::vector<double> &x,
+                                       std::vector<double> const &b,
+                                       std::vector<double> const &M,
+                                       int restart, int max_iter, double tol)
+{
+  int const n = int(b.size());
+  if (restart > n)
+    throw std::invalid_argument("Number of inner iterations " +
+                                std::to_string(restart) + " must be less than " +
+                                std::to_string(n) + "!");
+  if (A.size() != size_t(n) * n || x.size() != size_t(n) ||
+      (!M.empty() && M.size() != size_t(n) * n))
+    throw std::runtime_error("simple_gmres: A, x, b and M sizes differ");
+  asgk_gmres_info info{};
+  check(asgk_gmres_dense_precond(n, A.data(), x.data(), b.data(),
+                                 M.empty() ? nullptr : M.data(), restart,
+                                 max_iter, tol, &info),
+        "simple_gmres");
+  return gmres_info<double>{info.error, info.iterations};
+}
+
+//! The same without a preconditioner.
 inline gmres_info<double> simple_gmres(std::vector<double> const &A,
                                        std::vector<double> &x,
                                        std::vector<double> const &b,
                                        int restart, int max_iter, double tol)
 {
-  int const n = int(b.size());
-  if (restart > n)
-    throw std::invalid_argument("restart larger than the system");
-  asgk_gmres_info info{};
-  check(asgk_gmres_dense(n, A.data(), x.data(), b.data(), restart, max_iter,
-                         tol, &info),
-        "simple_gmres");
-  return gmres_info<double>{info.error, info.iterations};
+  return simple_gmres(A, x, b, std::vector<double>(), restart, max_iter, tol);
 }
 } // namespace solver
 } // namespace asgard_b200

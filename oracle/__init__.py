@@ -476,16 +476,25 @@ def imex_advance(d, n, explicit, implicit, dt, x, steps, restart, max_outer,
     return its
 
 
-def gmres_dense(A, x, b, restart, max_outer, tol, lib=None):
+def gmres_dense(A, x, b, restart, max_outer, tol, lib=None, M=None):
+    """solver::simple_gmres on a dense A (oracle restatement, or the compiled
+    reference with lib=ref()); M: the reference's dense preconditioner
+    (LU-factored and applied on the left, src/solver.cpp:11-38, 55-74),
+    reference only."""
     n = len(b)
     At = np.asfortranarray(A).ravel(order="F").copy()
     err, it = C.c_double(), C.c_int()
     if lib is None:
+        if M is not None:
+            raise ValueError("the oracle restatement takes no preconditioner")
         rc = oracle().orc_gmres_dense(n, At, x, b, restart, max_outer, tol,
                                       C.byref(err), C.byref(it))
     else:
-        rc = lib.ref_gmres_dense_f64(n, At, x, b, None, restart, max_outer,
-                                     tol, 1, C.byref(err), C.byref(it))
+        Mt = None if M is None else np.asfortranarray(M).ravel(order="F").copy()
+        rc = lib.ref_gmres_dense_f64(n, At, x, b,
+                                     None if Mt is None else Mt.ctypes.data,
+                                     restart, max_outer, tol, 1, C.byref(err),
+                                     C.byref(it))
     if rc != 0:
         raise RuntimeError(f"gmres checker returned {rc}")
     return err.value, it.value

@@ -2,9 +2,9 @@
 // way reference code would: builds a sparse-grid operator (d = 3, level 4,
 // 2 terms, seeded random factors) in the reference's CPU CSR format, its
 // multi-call chunk forms and its dense form, applies it on host and device
-// vectors, solves one
-// backward-Euler step with
-// simple_gmres_euler and one dense system with simple_gmres, and writes
+// vectors, solves one backward-Euler step with simple_gmres_euler, repeats
+// apply and solve through kronmult_matrix<float>, solves one dense system
+// with simple_gmres (with and without the dense preconditioner), and writes
 // inputs and results to a binary file for tests/test_cpp_dropin_gpu.py.
 #include "asgard_b200/kronmult_matrix.hpp"
 
@@ -263,6 +263,67 @@ int main(int argc, char **argv)
   std::vector<double> b3 = {2.084406360034887e-01, 6.444769305362776e-01, 3.687335330031937e-01};
   std::vector<double> x3(3, 0.0);
   auto info3 = solver::simple_gmres(A, x3, b3, 3, 3, 2.220446049250313e-16);
+  // the same with the reference's point-Jacobi dense preconditioner M
+  std::vector<double> M3 = {3.383861628748717e+00, 0.0, 0.0,
+                            0.0, 3.412141162288144e+00, 0.0,
+                            0.0, 0.0, 4.450671104482062e+00};
+  std::vector<double> x3p(3, 0.0);
+  auto info3p = solver::simple_gmres(A, x3p, b3, M3, 3, 3, 2.220446049250313e-16);
+
+  // a preconditioner built for another step size is refused
+  int dt_threw = 0;
+  {
+    solver::jacobi_preconditioner pc(mat, 2e-2, ASGK_JACOBI_POINT);
+    try
+    {
+      solver::simple_gmres_euler(1e-2, mat, dx, db, 20, 50, 1e-12, pc);
+    }
+    catch (std::invalid_argument const &)
+    {
+      dt_threw = 1;
+    }
+  }
+
+  // kronmult_matrix<float>: the same operator from FP32 factors, applied
+  // on host and device FP32 vectors, and one FP32 implicit step
+  double f_host_rel = 1.0, f_dev_rel = 1.0, f_sol_rel = 1.0, f_its = 0.0;
+  {
+    std::vector<float> vf(vA.begin(), vA.end()), xf(x.begin(), x.end()),
+        y0f(y0.begin(), y0.end()), bf(b.begin(), b.end());
+    kronmult_matrix<float> fm(d, n, int(cells), int(cells), T, pntr, col, iA, vf);
+    std::vector<float> yh = y0f;
+    fm.apply<resource::host>(0.5f, xf.data(), -2.0f, yh.data());
+    float *fx = nullptr, *fy = nullptr, *fb = nullptr;
+    cudaMalloc(&fx, sizeof(float) * N);
+    cudaMalloc(&fy, sizeof(float) * N);
+    cudaMalloc(&fb, sizeof(float) * N);
+    cudaMemcpy(fx, xf.data(), sizeof(float) * N, cudaMemcpyHostToDevice);
+    cudaMemcpy(fy, y0f.data(), sizeof(float) * N, cudaMemcpyHostToDevice);
+    fm.apply<resource::device>(0.5f, fx, -2.0f, fy);
+    std::vector<float> yd(N);
+    cudaMemcpy(yd.data(), fy, sizeof(float) * N, cudaMemcpyDeviceToHost);
+    cudaMemcpy(fb, bf.data(), sizeof(float) * N, cudaMemcpyHostToDevice);
+    cudaMemset(fx, 0, sizeof(float) * N);
+    auto fi = solver::simple_gmres_euler(1e-2f, fm, fx, fb, 20, 50, 1e-5f);
+    std::vector<float> fs(N);
+    cudaMemcpy(fs.data(), fx, sizeof(float) * N, cudaMemcpyDeviceToHost);
+    auto relf = [&](std::vector<float> const &a, std::vector<double> const &e) {
+      double nu = 0, de = 0;
+      for (int64_t i = 0; i < N; i++)
+      {
+        nu += (double(a[i]) - e[i]) * (double(a[i]) - e[i]);
+        de += e[i] * e[i];
+      }
+      return std::sqrt(nu / de);
+    };
+    f_host_rel = relf(yh, y_host);
+    f_dev_rel  = relf(yd, y_host);
+    f_sol_rel  = relf(fs, sol);
+    f_its      = fi.iterations;
+    cudaFree(fx);
+    cudaFree(fy);
+    cudaFree(fb);
+  }
 
   std::ofstream o(argv[1], std::ios::binary);
   put(o, pntr);
@@ -276,6 +337,7 @@ int main(int argc, char **argv)
   put(o, b);
   put(o, sol);
   put(o, x3);
+  put(o, x3p);
   std::vector<double> meta = {double(d), double(n), double(T), double(cells),
                               info.error, double(info.iterations), double(threw),
                               info3.error, double(mat.num_pairs()),
@@ -286,7 +348,10 @@ int main(int argc, char **argv)
                               double(dmat.is_dense()), double(dmat.num_batch()),
                               double(dmat.flops()), dense_rel, dense_update_rel,
                               chunk_rel, pairs_rel, double(chunked.num_pairs()),
-                              ws_rel, ws_used, pc_rel, pc_its, pc_err};
+                              ws_rel, ws_used, pc_rel, pc_its, pc_err,
+                              info3p.error, double(info3p.iterations),
+                              double(dt_threw), f_host_rel, f_dev_rel,
+                              f_sol_rel, f_its};
   put(o, meta);
   cudaFree(dx);
   cudaFree(dy);

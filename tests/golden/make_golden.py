@@ -184,15 +184,20 @@ def gmres_3x3():
         x1=[4.715561567725287e-02, 1.257695999382253e-01, 1.625351700791827e-02],
         b2=[9.789303188021963e-01, 8.085725142873675e-01, 7.370498473207234e-01],
         x2=[1.812300946484165e-01, -7.824949213916167e-02, 1.254969087137521e-01])
+    # the point-Jacobi preconditioner of the preconditioned cases (:149-151)
+    case["M"] = [[3.383861628748717e+00, 0.0, 0.0],
+                 [0.0, 3.412141162288144e+00, 0.0],
+                 [0.0, 0.0, 4.450671104482062e+00]]
     A = np.array(case["A"])
     R = oracle.ref()
     for k in ("1", "2"):
-        x = np.zeros(3)
-        err, its = oracle.gmres_dense(A, x, np.array(case["b" + k]), 3, 3,
-                                      np.finfo(np.float64).eps, lib=R)
-        case["ref_x" + k] = x.tolist()
-        case["ref_err" + k] = err
-        case["ref_iters" + k] = its
+        for tag, M in (("", None), ("pre_", np.array(case["M"]))):
+            x = np.zeros(3)
+            err, its = oracle.gmres_dense(A, x, np.array(case["b" + k]), 3, 3,
+                                          np.finfo(np.float64).eps, lib=R, M=M)
+            case[f"ref_{tag}x" + k] = x.tolist()
+            case[f"ref_{tag}err" + k] = err
+            case[f"ref_{tag}iters" + k] = its
     with open(os.path.join(OUT, "gmres_3x3.json"), "w") as f:
         json.dump(case, f, indent=1)
 

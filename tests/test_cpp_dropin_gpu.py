@@ -28,7 +28,7 @@ def _read(path):
     with open(path, "rb") as f:
         data = f.read()
     o = 0
-    for dt in [np.int32] * 3 + [np.float64] * 9:
+    for dt in [np.int32] * 3 + [np.float64] * 10:
         n = int(np.frombuffer(data, np.int64, 1, o)[0])
         o += 8
         out.append(np.frombuffer(data, dt, n, o).copy())
@@ -42,7 +42,7 @@ def test_cpp_dropin_header(cuda, tmp_path):
     assert r.returncode == 0, r.stderr
     out = tmp_path / "out.bin"
     subprocess.run([str(exe), str(out)], check=True)
-    pntr, col, iA, vA, x, y0, y_host, y_dev, b, sol, x3, meta = _read(out)
+    pntr, col, iA, vA, x, y0, y_host, y_dev, b, sol, x3, x3p, meta = _read(out)
     d, n, T = int(meta[0]), int(meta[1]), int(meta[2])
     expect = oracle.kronmult(d, n, pntr, col, T, iA, vA, 0.5, x, -2.0, y0.copy())
     assert rel_err(y_host, expect) < 1e-13
@@ -81,3 +81,13 @@ def test_cpp_dropin_header(cuda, tmp_path):
     # the preconditioned overload (point Jacobi, right-preconditioned): the
     # same solution to the tolerance the criterion allows
     assert meta[25] < 1e-8 and meta[26] >= 1 and meta[27] <= 1e-12
+    # simple_gmres with the reference's dense preconditioner: the preconditioned
+    # 3x3 known answer, the reference's iteration count (4)
+    eps = np.finfo(np.float64).eps
+    assert rmse_close(x3p, gold, 10 * eps) and meta[28] < eps and meta[29] == 4
+    # a Jacobi preconditioner built for another dt: std::invalid_argument
+    assert meta[30] == 1.0
+    # kronmult_matrix<float>: FP32 applies on host and device vectors and
+    # the FP32 implicit step agree with the FP64 results to FP32 accuracy
+    assert meta[31] < 1e-6 and meta[32] < 1e-6
+    assert meta[33] < 1e-5 and meta[34] >= 1

@@ -31,6 +31,28 @@ def test_gmres_known_answers(cuda):
         assert rmse_close(x, case["x" + k], 10 * eps)
 
 
+def test_gmres_known_answers_preconditioned(cuda):
+    """The point-Jacobi preconditioned 3x3 cases of src/solver_tests.cpp:
+    175-213 through the reference's dense preconditioner (LU of M applied on
+    the left): error below machine epsilon, the reference's iteration count
+    (reference-made fixture), x equal to the gold answer."""
+    import asgard_b200 as ab
+    case = json.load(open(golden("gmres_3x3.json")))
+    A, M = np.array(case["A"]), np.array(case["M"])
+    eps = np.finfo(np.float64).eps
+    for k in ("1", "2"):
+        x = np.zeros(3)
+        info = ab.simple_gmres(A, x, np.array(case["b" + k]), M, 3, 3, eps)
+        assert info.status == 0
+        assert info.error < eps
+        assert info.iterations == case["ref_pre_iters" + k]
+        assert rmse_close(x, case["x" + k], 10 * eps)
+        assert rmse_close(x, case["ref_pre_x" + k], 10 * eps)
+    # a singular M is refused before any device work
+    with pytest.raises(ab.AsgkError):
+        ab.simple_gmres(A, np.zeros(3), np.array(case["b1"]), np.zeros((3, 3)), 3, 3, eps)
+
+
 @pytest.mark.parametrize("name", ["continuity_2_L4", "continuity_3_L3", "diffusion_2_L3"])
 def test_gmres_euler_reference_pdes(cuda, name):
     """simple_gmres_euler on reference-built operators: the reference's answer

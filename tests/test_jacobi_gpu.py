@@ -98,6 +98,46 @@ def test_jacobi_errors(cuda):
         ab.JacobiPreconditioner(rect, 1e-3, kind="point")
 
 
+def test_preconditioner_of_another_plan_is_refused(cuda):
+    """A Jacobi preconditioner built on a smaller plan would index past the
+    solve's vectors: the solve, the implicit loop and the IMEX loop refuse it
+    before any kernel launches; the IMEX loop also refuses stage
+    preconditioners built for other step sizes."""
+    import torch
+    import asgard_b200 as ab
+    small = ab.SparseGridOperator(3, 3, 3, kind="advdiff")
+    big = ab.SparseGridOperator(3, 4, 3, kind="advdiff")
+    ms, mb = small.kronmult_matrix(), big.kronmult_matrix()
+    dt = 1e-3
+    pcs = {k: ab.JacobiPreconditioner(ms, dt, kind=k) for k in ("point", "block")}
+    b = torch.ones(big.N, dtype=torch.float64, device="cuda")
+    x = torch.zeros_like(b)
+    torch.cuda.synchronize()
+    for kind, pc in pcs.items():
+        before = ab.launch_count()
+        with pytest.raises(ab.AsgkError):
+            ab.simple_gmres_euler(dt, mb, x, b, 10, 2, 1e-10, precond=pc)
+        with pytest.raises(ab.AsgkError):
+            ab.implicit_advance(dt, mb, x, 1, restart=10, max_iter=2, tol=1e-10,
+                                precond=pc)
+        with pytest.raises(ab.AsgkError):
+            ab.imex_advance(dt, mb, mb, x, 1, restart=10, max_iter=2, tol=1e-10,
+                            precond=(pc, None))
+        assert ab.launch_count() == before, kind
+    # right shape, wrong step: stage 1 inverts I - dt K, stage 2 I - dt/2 K
+    p1 = ab.JacobiPreconditioner(mb, dt, kind="point")
+    p2 = ab.JacobiPreconditioner(mb, dt / 2, kind="point")
+    with pytest.raises(ab.AsgkError):
+        ab.imex_advance(dt, mb, mb, x, 1, restart=10, max_iter=2, tol=1e-10,
+                        precond=(p2, p1))
+    ab.imex_advance(dt, mb, mb, x, 1, restart=10, max_iter=2, tol=1e-10,
+                    precond=(p1, p2))
+    # the learned preconditioner's base must fit the network's cells
+    net = ab.LearnedPreconditioner(big)
+    with pytest.raises(ab.AsgkError):
+        net.set_base(pcs["point"])
+
+
 @pytest.mark.parametrize("d,L,T", [(2, 6, 2), (3, 5, 3), (4, 4, 4), (4, 7, 4)])
 def test_kron_block_jacobi_equals_dense_block(cuda, d, L, T):
     """The Kronecker-sum form of the cell-block inverse (eigendecompositions
