@@ -207,6 +207,15 @@ int jacobi_check_shape(const asgk_jacobi *pc, int rows, int tensor);
 // the step size the preconditioner inverts I - dt*K for
 double jacobi_dt(const asgk_jacobi *pc);
 
+// jacobi_line.cu: the line preconditioner (ASGK_JACOBI_LINE)
+struct line_data;
+int line_build(plan_data const &p, double dt, line_data **out, int64_t &bytes);
+void line_free(line_data *ld);
+int line_apply(line_data const &ld, bool low, double *v, double *z,
+               const double *scale_state, float *vcopy, cudaStream_t s);
+// the line dimensions (up to 3) into dims; returns how many
+int line_info(line_data const &ld, int *dims);
+
 // kron_global.cu: global-mode apply
 int launch_global(plan_data const &p, int precision, double alpha,
                   const double *x, double beta, double *y, double ex,

@@ -692,9 +692,12 @@ struct jacobi_data
   double *kt64     = nullptr; // [nconn * d][kKronTab]
   float *kt32      = nullptr;
   int *kself       = nullptr; // [rows * d]
+  // line: pencil tables and intermediates (jacobi_line.cu)
+  line_data *line  = nullptr;
   int64_t device_bytes = 0;
   ~jacobi_data()
   {
+    line_free(line);
     cudaFree(inv_diag);
     cudaFree(M64);
     cudaFree(M16);
@@ -709,7 +712,7 @@ int jacobi_build(plan_data const &p, double dt, int kind, jacobi_data &jd)
   if (p.rows != p.cols)
     return ASGK_ERR_INVALID;
   if (kind != ASGK_JACOBI_POINT && kind != ASGK_JACOBI_BLOCK &&
-      kind != ASGK_JACOBI_KRON)
+      kind != ASGK_JACOBI_KRON && kind != ASGK_JACOBI_LINE)
     return ASGK_ERR_INVALID;
   int const ts = p.tensor;
   if (kind == ASGK_JACOBI_BLOCK && ts > 81)
@@ -728,6 +731,11 @@ int jacobi_build(plan_data const &p, double dt, int kind, jacobi_data &jd)
   ASGK_CUDA(cudaMalloc(&err, sizeof(int)));
   std::unique_ptr<int, decltype(&cudaFree)> err_guard(err, &cudaFree);
   ASGK_CUDA(cudaMemset(err, 0, sizeof(int)));
+  if (kind == ASGK_JACOBI_LINE)
+  {
+    jd.d = p.d;
+    return line_build(p, dt, &jd.line, jd.device_bytes);
+  }
   // the plan's FP64 factors in the layout its indices address
   const double *vA = p.vA64;
   if (kind == ASGK_JACOBI_KRON)
@@ -817,6 +825,8 @@ int jacobi_apply(jacobi_data const &jd, bool low, double *v, double *z,
                  const double *scale_state, float *vcopy, cudaStream_t s)
 {
   int64_t const n = int64_t(jd.rows) * jd.ts;
+  if (jd.kind == ASGK_JACOBI_LINE)
+    return line_apply(*jd.line, low, v, z, scale_state, vcopy, s);
   if (jd.kind == ASGK_JACOBI_KRON)
   {
     if (low)

@@ -1,0 +1,823 @@
+// Line preconditioner (ASGK_JACOBI_LINE) of the backward-Euler operator
+// I - dt*K for global plans whose terms act in one dimension each.  No
+// counterpart in the reference, whose only preconditioner is the diagonal
+// one (src/solver.cpp:76-91).
+//
+// K = sum_k K_k, K_k the terms acting in dimension k.  K_k couples only
+// cells that agree outside dimension k (a "pencil" along k), and on a
+// pencil it is A_k restricted to the pencil's 1D cells (x) I on the other
+// dimensions.  On a standard sparse grid a pencil holds every 1D cell of
+// level <= L' along k, so its matrix is a leading principal submatrix of the
+// 1D operator A_k: one per pencil level.  For the "line" dimensions -- those
+// whose 1D operator is symmetric (the stiff diffusion terms) -- the solve
+//   M_k = s I - dt (K_k + sum_{j line, j != k} D_j),  D_j: cell-diagonal part of K_j,
+// s = 1 - dt * (identity terms), is exact per pencil: with A_P = Q diag(theta)
+// Q^T (A_P the pencil's submatrix) and the 3x3 self blocks of the other line
+// dimensions S_j = P_j diag(lambda_j) P_j^T (constant over the pencil: its
+// cells share their 1D cells outside k), all orthogonal,
+//   M_k^-1 = (Q (x) (x)_j P_j) diag(1 / (s - dt (theta + sum_j lambda_j))) (Q^T (x) (x)_j P_j^T)
+// on each group of values with fixed polynomial indices in the non-line
+// dimensions.  The preconditioner chains the line dimensions k_1 < ... < k_m:
+//   z = M_{k_m}^-1 B ... B M_{k_2}^-1 B M_{k_1}^-1 v,   B = s I - dt sum_{j line} D_j,
+// an alternating-direction product whose factors each invert one diffusion
+// direction exactly; dimensions with non-symmetric operators (advection)
+// are left to GMRES.  Each factor is one kernel launch over (pencil, group
+// range) units: gather the unit's values, apply B (factors after the first),
+// transform the columns by the P_j^T and the rows by Q^T (a dense product,
+// the pencil matrix read through L2), divide, transform back, scatter.  The
+// first factor also normalises v and writes its FP32 copy inside recorded
+// GMRES cycles; intermediates live in two vectors held by the
+// preconditioner; no atomics (each value belongs to exactly one unit).
+#include "internal.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <map>
+#include <memory>
+#include <new>
+#include <numeric>
+#include <vector>
+
+namespace asgk
+{
+namespace
+{
+constexpr int kLineThreads = 128;
+constexpr int kSelfEntry   = 21; // P (3x3 col-major), lambda (3), S (3x3 col-major)
+
+constexpr int ipow3l(int k) { return k <= 0 ? 1 : 3 * ipow3l(k - 1); }
+
+// Symmetric eigendecomposition by cyclic Jacobi rotations: A (n x n,
+// row-major, symmetric) = V diag(w) V^T with V orthogonal (eigenvectors in
+// its columns, row-major storage).  Each rotation zeroes one off-diagonal
+// entry a_pq: tau = (a_qq - a_pp) / (2 a_pq), t = sign(tau) / (|tau| +
+// sqrt(1 + tau^2)), c = 1/sqrt(1 + t^2), s = t c.
+bool sym_eig(int n, std::vector<double> A, std::vector<double> &V,
+             std::vector<double> &w)
+{
+  V.assign(size_t(n) * n, 0.0);
+  for (int i = 0; i < n; i++)
+    V[size_t(i) * n + i] = 1.0;
+  double norm = 0;
+  for (double a : A)
+    norm += a * a;
+  norm = std::sqrt(norm);
+  for (int sweep = 0; sweep < 60; sweep++)
+  {
+    double off = 0;
+    for (int p = 0; p < n; p++)
+      for (int q = p + 1; q < n; q++)
+        off += A[size_t(p) * n + q] * A[size_t(p) * n + q];
+    if (std::sqrt(2 * off) <= 1e-15 * norm || norm == 0.0)
+    {
+      w.resize(n);
+      for (int i = 0; i < n; i++)
+        w[i] = A[size_t(i) * n + i];
+      return true;
+    }
+    for (int p = 0; p < n; p++)
+      for (int q = p + 1; q < n; q++)
+      {
+        double const apq = A[size_t(p) * n + q];
+        if (std::abs(apq) <= 1e-300 ||
+            std::abs(apq) <= 1e-18 * (std::abs(A[size_t(p) * n + p]) +
+                                      std::abs(A[size_t(q) * n + q])))
+          continue;
+        double const tau = (A[size_t(q) * n + q] - A[size_t(p) * n + p]) / (2 * apq);
+        double const t   = (tau >= 0 ? 1.0 : -1.0) / (std::abs(tau) + std::sqrt(1 + tau * tau));
+        double const c   = 1 / std::sqrt(1 + t * t), s = t * c;
+        for (int k = 0; k < n; k++)
+        {
+          double const akp = A[size_t(k) * n + p], akq = A[size_t(k) * n + q];
+          A[size_t(k) * n + p] = c * akp - s * akq;
+          A[size_t(k) * n + q] = s * akp + c * akq;
+        }
+        for (int k = 0; k < n; k++)
+        {
+          double const apk = A[size_t(p) * n + k], aqk = A[size_t(q) * n + k];
+          A[size_t(p) * n + k] = c * apk - s * aqk;
+          A[size_t(q) * n + k] = s * apk + c * aqk;
+        }
+        for (int k = 0; k < n; k++)
+        {
+          double const vkp = V[size_t(k) * n + p], vkq = V[size_t(k) * n + q];
+          V[size_t(k) * n + p] = c * vkp - s * vkq;
+          V[size_t(k) * n + q] = s * vkp + c * vkq;
+        }
+      }
+  }
+  return false;
+}
+
+// Everything a factor launch reads (device pointers; the tables typed by R).
+template<typename R>
+struct line_args
+{
+  const int4 *units;  // (pencil, first group, groups, 0)
+  const int *pen_off; // into pen_cells
+  const int *pen_m;   // members
+  const int *pen_tab; // pencil matrix table
+  const int *pen_cells;
+  const int *c1;      // [cells][D] 1D cell of every cell in every dimension
+  const int *tab_off; // into Q / QT (each Rr x Rp)
+  const int *tab_th;  // into theta
+  const int *tab_rp;
+  const R *Q, *QT, *theta;
+  const R *self;      // [line index][1D cells][kSelfEntry]
+  int r1;             // number of 1D cells
+  int k, kidx;        // this factor's dimension and its index among the line dims
+  int line[3];        // line dimensions (increasing)
+  int nonline[6];     // the other dimensions (increasing)
+  R shift, dt;
+};
+
+template<typename R> struct vec4_of;
+template<> struct vec4_of<float>
+{
+  static __device__ __forceinline__ void load(const float *p, float q[4])
+  {
+    float4 const v = __ldg(reinterpret_cast<const float4 *>(p));
+    q[0] = v.x, q[1] = v.y, q[2] = v.z, q[3] = v.w;
+  }
+};
+template<> struct vec4_of<double>
+{
+  static __device__ __forceinline__ void load(const double *p, double q[4])
+  {
+    double2 const a = __ldg(reinterpret_cast<const double2 *>(p));
+    double2 const b = __ldg(reinterpret_cast<const double2 *>(p) + 1);
+    q[0] = a.x, q[1] = a.y, q[2] = b.x, q[3] = b.y;
+  }
+};
+
+// out[r][g][c] = sum_{t < Rr} Mt[t][r] in[t][g][c] for r < Rr (Mt rows of
+// Rp entries, zero beyond Rr), divided by den(r, c) when theta is given.
+template<typename R, int NC, int NCP>
+__device__ void dense_rows(const R *__restrict__ Mt, int Rr, int Rp, int G,
+                           const R *__restrict__ in, R *__restrict__ out,
+                           const R *__restrict__ theta, const R *lamc, R shift,
+                           R dt)
+{
+  int const rb_n  = Rp / 4;
+  int const items = rb_n * G;
+  for (int it = threadIdx.x; it < items; it += blockDim.x)
+  {
+    int const rb = it % rb_n, g = it / rb_n;
+    R acc[4][NC];
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+      for (int c = 0; c < NC; c++)
+        acc[i][c] = R(0);
+    const R *xr = in + g * NCP;
+    const R *mr = Mt + 4 * rb;
+    for (int t = 0; t < Rr; t++)
+    {
+      R q[4];
+      vec4_of<R>::load(mr + int64_t(t) * Rp, q);
+      R x[NC];
+#pragma unroll
+      for (int c = 0; c < NC; c++)
+        x[c] = xr[int64_t(t) * G * NCP + c];
+#pragma unroll
+      for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int c = 0; c < NC; c++)
+          acc[i][c] = fma(q[i], x[c], acc[i][c]);
+    }
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+    {
+      int const r = 4 * rb + i;
+      if (r >= Rr)
+        break;
+      R th = R(0);
+      if (theta)
+        th = __ldg(theta + r);
+#pragma unroll
+      for (int c = 0; c < NC; c++)
+      {
+        R v = acc[i][c];
+        if (theta)
+          v = v / (shift - dt * (th + lamc[c]));
+        out[(int64_t(r) * G + g) * NCP + c] = v;
+      }
+    }
+  }
+}
+
+// One factor M_k^-1 (after B when bj) on the (pencil, group range) units.
+// D dimensions, M line dimensions; NC = 3^(M-1) columns per group (the other
+// line dimensions' polynomials), groups: the 3^(D-M) polynomial indices of
+// the non-line dimensions.
+template<typename R, int D, int M>
+__global__ void __launch_bounds__(kLineThreads)
+    k_line_factor(line_args<R> a, const double *in64,
+                  const R *__restrict__ inR, double *__restrict__ out64,
+                  R *__restrict__ outR, int bj, const double *scale_state,
+                  double *vscale, float *vcopy, const double *gate)
+{
+  if (gate_closed(gate))
+    return;
+  constexpr int TS  = ipow3l(D);
+  constexpr int NC  = ipow3l(M - 1);
+  constexpr int NCP = NC == 1 ? 1 : (NC == 3 ? 4 : 12);
+  constexpr int NNL = D - M; // non-line dimensions
+  extern __shared__ __align__(16) unsigned char line_smem[];
+  int4 const u   = a.units[blockIdx.x];
+  int const pen  = u.x, g0 = u.y, G = u.z;
+  int const m    = a.pen_m[pen];
+  int const tab  = a.pen_tab[pen];
+  int const Rr   = 3 * m;
+  int const Rp   = a.tab_rp[tab];
+  const int *cells = a.pen_cells + a.pen_off[pen];
+  R *X = reinterpret_cast<R *>(line_smem);
+  R *Y = X + int64_t(Rp) * G * NCP;
+  __shared__ int s_offg[27];
+  __shared__ int s_offc[NC];
+  __shared__ R s_lamc[NC];
+  __shared__ R s_P[3][9]; // other line dimensions' eigenvectors (P_j, col-major)
+  __shared__ R s_S[3][9]; // their self blocks (B, all line dimensions)
+  int const cell0 = cells[0];
+  // offsets of the group and column digits in a cell's tensor (dimension 0
+  // slowest); the other line dimensions' eigen data, constant over the pencil
+  if (threadIdx.x < G)
+  {
+    int g = g0 + threadIdx.x, off = 0;
+    for (int q = NNL - 1; q >= 0; q--)
+    {
+      off += (g % 3) * ipow3l(D - 1 - a.nonline[q]);
+      g /= 3;
+    }
+    s_offg[threadIdx.x] = off;
+  }
+  if (threadIdx.x < NC)
+  {
+    int c = threadIdx.x, off = 0;
+    R lam = R(0);
+    for (int q = M - 1; q >= 0; q--)
+    {
+      if (q == a.kidx)
+        continue;
+      int const j  = a.line[q];
+      int const dg = c % 3;
+      c /= 3;
+      off += dg * ipow3l(D - 1 - j);
+      lam += a.self[(int64_t(q) * a.r1 + a.c1[int64_t(cell0) * D + j]) * kSelfEntry + 9 + dg];
+    }
+    s_offc[threadIdx.x] = off;
+    s_lamc[threadIdx.x] = lam;
+  }
+  if (threadIdx.x < 9 * M)
+  {
+    int const q = threadIdx.x / 9, e = threadIdx.x % 9;
+    int const j = a.line[q];
+    const R *sf = a.self + (int64_t(q) * a.r1 + a.c1[int64_t(cell0) * D + j]) * kSelfEntry;
+    s_P[q][e] = sf[e];
+    s_S[q][e] = sf[12 + e];
+  }
+  __syncthreads();
+  int const stk = ipow3l(D - 1 - a.k);
+  double const f = scale_state ? scale_state[1] : 1.0;
+  // gather (row = member * 3 + k polynomial, group, column)
+  int const nload = m * G * 3 * NC;
+  for (int e = threadIdx.x; e < nload; e += blockDim.x)
+  {
+    int const c  = e % NC;
+    int const pk = (e / NC) % 3;
+    int const g  = (e / (3 * NC)) % G;
+    int const i  = e / (3 * NC * G);
+    int64_t const gi = int64_t(cells[i]) * TS + s_offg[g] + s_offc[c] + pk * stk;
+    R val;
+    if (in64)
+    {
+      double vv = in64[gi];
+      if (scale_state)
+      {
+        vv *= f;
+        vscale[gi] = vv;
+        if (vcopy)
+          vcopy[gi] = float(vv);
+      }
+      val = R(vv);
+    }
+    else
+      val = inR[gi];
+    X[((int64_t(i) * 3 + pk) * G + g) * NCP + c] = val;
+  }
+  __syncthreads();
+  // B = s - dt sum_{line j} S_j along j, on each (member, group): its 3 x NC
+  // values are the cell's line-dimension polynomials
+  if (bj)
+  {
+    for (int it = threadIdx.x; it < m * G; it += blockDim.x)
+    {
+      int const i = it / G, g = it % G;
+      R v[3][NC], o[3][NC];
+#pragma unroll
+      for (int pk = 0; pk < 3; pk++)
+#pragma unroll
+        for (int c = 0; c < NC; c++)
+          v[pk][c] = X[((int64_t(i) * 3 + pk) * G + g) * NCP + c];
+      // this member's own self block along k
+      R Sk[9];
+      const R *sf = a.self + (int64_t(a.kidx) * a.r1 +
+                              a.c1[int64_t(cells[i]) * D + a.k]) * kSelfEntry + 12;
+#pragma unroll
+      for (int e = 0; e < 9; e++)
+        Sk[e] = sf[e];
+#pragma unroll
+      for (int pk = 0; pk < 3; pk++)
+#pragma unroll
+        for (int c = 0; c < NC; c++)
+        {
+          R acc = a.shift * v[pk][c];
+          // along k: sum_p S_k(pk, p) v[p][c]
+          acc -= a.dt * (Sk[pk] * v[0][c] + Sk[pk + 3] * v[1][c] + Sk[pk + 6] * v[2][c]);
+          // along the other line dimensions: the column digits
+          int stride = 1;
+#pragma unroll
+          for (int q = M - 1; q >= 0; q--)
+          {
+            if (q == a.kidx)
+              continue;
+            int const dg = (c / stride) % 3;
+            int const cb = c - dg * stride;
+            R s = R(0);
+#pragma unroll
+            for (int p = 0; p < 3; p++)
+              s += s_S[q][dg + 3 * p] * v[pk][cb + p * stride];
+            acc -= a.dt * s;
+            stride *= 3;
+          }
+          o[pk][c] = acc;
+        }
+#pragma unroll
+      for (int pk = 0; pk < 3; pk++)
+#pragma unroll
+        for (int c = 0; c < NC; c++)
+          X[((int64_t(i) * 3 + pk) * G + g) * NCP + c] = o[pk][c];
+    }
+    __syncthreads();
+  }
+  // columns: u <- P_j^T u along every other line dimension, per (row, group)
+  auto columns = [&](R *buf, bool forward) {
+    if constexpr (NC > 1)
+    {
+      for (int it = threadIdx.x; it < Rr * G; it += blockDim.x)
+      {
+        R *row = buf + int64_t(it) * NCP;
+        R v[NC];
+#pragma unroll
+        for (int c = 0; c < NC; c++)
+          v[c] = row[c];
+        int stride = 1;
+#pragma unroll
+        for (int q = M - 1; q >= 0; q--)
+        {
+          if (q == a.kidx)
+            continue;
+          R w[NC];
+#pragma unroll
+          for (int c = 0; c < NC; c++)
+          {
+            int const dg = (c / stride) % 3;
+            int const cb = c - dg * stride;
+            R s = R(0);
+#pragma unroll
+            for (int p = 0; p < 3; p++)
+              // forward: (P^T u)_dg = sum_p P(p, dg) u_p; back: (P u)_dg = sum_p P(dg, p) u_p
+              s += (forward ? s_P[q][p + 3 * dg] : s_P[q][dg + 3 * p]) * v[cb + p * stride];
+            w[c] = s;
+          }
+#pragma unroll
+          for (int c = 0; c < NC; c++)
+            v[c] = w[c];
+          stride *= 3;
+        }
+#pragma unroll
+        for (int c = 0; c < NC; c++)
+          row[c] = v[c];
+      }
+      __syncthreads();
+    }
+  };
+  columns(X, true);
+  int64_t const to = a.tab_off[tab];
+  // rows: Y = Q^T X, divided; then X = Q Y
+  dense_rows<R, NC, NCP>(a.Q + to, Rr, Rp, G, X, Y, a.theta + a.tab_th[tab], s_lamc,
+                         a.shift, a.dt);
+  __syncthreads();
+  dense_rows<R, NC, NCP>(a.QT + to, Rr, Rp, G, Y, X, nullptr, s_lamc, a.shift,
+                         a.dt);
+  __syncthreads();
+  columns(X, false);
+  // scatter
+  for (int e = threadIdx.x; e < nload; e += blockDim.x)
+  {
+    int const c  = e % NC;
+    int const pk = (e / NC) % 3;
+    int const g  = (e / (3 * NC)) % G;
+    int const i  = e / (3 * NC * G);
+    int64_t const gi = int64_t(cells[i]) * TS + s_offg[g] + s_offc[c] + pk * stk;
+    R const val = X[((int64_t(i) * 3 + pk) * G + g) * NCP + c];
+    if (out64)
+      out64[gi] = double(val);
+    else
+      outR[gi] = val;
+  }
+}
+
+template<typename R>
+struct line_tables
+{
+  R *Q = nullptr, *QT = nullptr, *theta = nullptr, *self = nullptr;
+  ~line_tables()
+  {
+    cudaFree(Q);
+    cudaFree(QT);
+    cudaFree(theta);
+    cudaFree(self);
+  }
+};
+
+struct line_factor
+{
+  int k = 0;
+  int nunits = 0;
+  int max_rows = 0; // largest Rp * G of its units (shared memory)
+  int4 *units = nullptr;
+  int *pen_off = nullptr, *pen_m = nullptr, *pen_tab = nullptr, *pen_cells = nullptr;
+  ~line_factor()
+  {
+    cudaFree(units);
+    cudaFree(pen_off);
+    cudaFree(pen_m);
+    cudaFree(pen_tab);
+    cudaFree(pen_cells);
+  }
+};
+
+template<typename T>
+int upload(T **dst, std::vector<T> const &src, int64_t &bytes)
+{
+  size_t const b = sizeof(T) * std::max<size_t>(src.size(), 1);
+  ASGK_CUDA(cudaMalloc(dst, b));
+  if (!src.empty())
+    ASGK_CUDA(cudaMemcpy(*dst, src.data(), sizeof(T) * src.size(),
+                         cudaMemcpyHostToDevice));
+  bytes += int64_t(b);
+  return ASGK_OK;
+}
+} // namespace
+
+struct line_data
+{
+  int d = 0, rows = 0, ts = 0, r1 = 0, m = 0;
+  int line[3] = {0, 0, 0};
+  int nonline[6] = {0, 0, 0, 0, 0, 0};
+  double shift = 1, dt = 0;
+  int *c1 = nullptr, *tab_off = nullptr, *tab_th = nullptr, *tab_rp = nullptr;
+  line_tables<double> t64;
+  line_tables<float> t32;
+  std::vector<std::unique_ptr<line_factor>> factors;
+  double *work = nullptr; // two intermediate vectors (rows * ts doubles each)
+  ~line_data()
+  {
+    cudaFree(c1);
+    cudaFree(tab_off);
+    cudaFree(tab_th);
+    cudaFree(tab_rp);
+    cudaFree(work);
+  }
+};
+
+void line_free(line_data *ld) { delete ld; }
+
+int line_build(plan_data const &p, double dt, line_data **out, int64_t &bytes)
+{
+  *out = nullptr;
+  if (!p.global || p.gchains > 0 || p.n != 3 || p.rows != p.cols)
+    return ASGK_ERR_UNSUPPORTED;
+  int const d         = p.d;
+  int64_t const nconn = int64_t(p.g_conn_row.size());
+  int r1              = 0;
+  for (int64_t j = 0; j < nconn; j++)
+    r1 = std::max(r1, std::max(p.g_conn_row[j], p.g_conn_col[j]) + 1);
+  std::vector<double> B(size_t(nconn) * d * 10);
+  ASGK_CUDA(cudaMemcpy(B.data(), p.gB64, sizeof(double) * B.size(),
+                       cudaMemcpyDeviceToHost));
+  // the full 1D operator of every dimension (3 r1 square, row-major)
+  int const nf = 3 * r1;
+  std::vector<std::vector<double>> F(d, std::vector<double>(size_t(nf) * nf, 0.0));
+  for (int64_t j = 0; j < nconn; j++)
+    for (int k = 0; k < d; k++)
+    {
+      const double *b = &B[size_t(j * d + k) * 10];
+      int const r = p.g_conn_row[j], c = p.g_conn_col[j];
+      for (int jj = 0; jj < 3; jj++)
+        for (int i = 0; i < 3; i++)
+          F[k][size_t(3 * r + i) * nf + 3 * c + jj] = b[i + 3 * jj];
+    }
+  // line dimensions: nonzero symmetric operators
+  std::vector<int> line, nonline;
+  for (int k = 0; k < d; k++)
+  {
+    double mx = 0, asym = 0;
+    for (int r = 0; r < nf; r++)
+      for (int c = 0; c < nf; c++)
+      {
+        mx   = std::max(mx, std::abs(F[k][size_t(r) * nf + c]));
+        asym = std::max(asym, std::abs(F[k][size_t(r) * nf + c] - F[k][size_t(c) * nf + r]));
+      }
+    if (mx > 0 && asym <= 1e-12 * mx)
+      line.push_back(k);
+    else
+      nonline.push_back(k);
+  }
+  if (line.empty() || line.size() > 3)
+    return ASGK_ERR_UNSUPPORTED;
+  int const M = int(line.size());
+  auto ld     = std::make_unique<line_data>();
+  ld->d = d, ld->rows = p.rows, ld->ts = p.tensor, ld->r1 = r1, ld->m = M, ld->dt = dt;
+  ld->shift = 1.0 - dt * p.g_identity;
+  for (int q = 0; q < M; q++)
+    ld->line[q] = line[q];
+  for (size_t q = 0; q < nonline.size(); q++)
+    ld->nonline[q] = nonline[q];
+  // every cell's 1D cells (its self connections in the global plan's
+  // diagonal pair list)
+  std::vector<int> selfc(size_t(p.rows) * d), c1(size_t(p.rows) * d);
+  ASGK_CUDA(cudaMemcpy(selfc.data(), p.idx, sizeof(int) * selfc.size(),
+                       cudaMemcpyDeviceToHost));
+  for (size_t e = 0; e < selfc.size(); e++)
+    c1[e] = p.g_conn_row[selfc[e]];
+  // self blocks of the line dimensions and their eigendecompositions
+  std::vector<double> self(size_t(M) * r1 * kSelfEntry, 0.0);
+  for (int q = 0; q < M; q++)
+    for (int c = 0; c < r1; c++)
+    {
+      std::vector<double> S(9), V, w;
+      for (int i = 0; i < 3; i++)
+        for (int jj = 0; jj < 3; jj++)
+          S[size_t(i) * 3 + jj] = F[line[q]][size_t(3 * c + i) * nf + 3 * c + jj];
+      if (!sym_eig(3, S, V, w))
+        return ASGK_ERR_UNSUPPORTED;
+      double *e = &self[(size_t(q) * r1 + c) * kSelfEntry];
+      for (int i = 0; i < 3; i++)
+        for (int jj = 0; jj < 3; jj++)
+        {
+          e[i + 3 * jj]      = V[size_t(i) * 3 + jj]; // P(i, jj), column jj eigenvector
+          e[12 + i + 3 * jj] = S[size_t(i) * 3 + jj];
+        }
+      for (int i = 0; i < 3; i++)
+        e[9 + i] = w[i];
+    }
+  // pencils of every line dimension, their matrices by (operator, 1D set)
+  int bits = 1;
+  while ((1 << bits) < r1)
+    ++bits;
+  if (bits * (d - 1) > 63)
+    return ASGK_ERR_UNSUPPORTED;
+  std::vector<int> opid(M);
+  for (int q = 0; q < M; q++)
+  {
+    opid[q] = q;
+    for (int q2 = 0; q2 < q; q2++)
+      if (F[line[q2]] == F[line[q]])
+      {
+        opid[q] = opid[q2];
+        break;
+      }
+  }
+  std::map<std::pair<int, std::vector<int>>, int> tabs;
+  std::vector<double> Qh, QTh, thh;
+  std::vector<int> toff, tth, trp;
+  int const ng = ipow3l(d - M);
+  for (int q = 0; q < M; q++)
+  {
+    int const k = line[q];
+    std::vector<std::pair<uint64_t, int>> keyed(p.rows);
+    for (int c = 0; c < p.rows; c++)
+    {
+      uint64_t key = 0;
+      for (int j = 0; j < d; j++)
+        if (j != k)
+          key = (key << bits) | uint64_t(c1[size_t(c) * d + j]);
+      keyed[c] = {key, c};
+    }
+    std::sort(keyed.begin(), keyed.end(), [&](auto const &x, auto const &y) {
+      if (x.first != y.first)
+        return x.first < y.first;
+      return c1[size_t(x.second) * d + k] < c1[size_t(y.second) * d + k];
+    });
+    std::vector<int> pen_off, pen_m, pen_tab, pen_cells;
+    for (size_t s = 0; s < keyed.size();)
+    {
+      size_t e = s;
+      while (e < keyed.size() && keyed[e].first == keyed[s].first)
+        ++e;
+      std::vector<int> set;
+      pen_off.push_back(int(pen_cells.size()));
+      for (size_t i = s; i < e; i++)
+      {
+        pen_cells.push_back(keyed[i].second);
+        set.push_back(c1[size_t(keyed[i].second) * d + k]);
+      }
+      pen_m.push_back(int(e - s));
+      auto const tk = std::make_pair(opid[q], set);
+      auto it       = tabs.find(tk);
+      if (it == tabs.end())
+      {
+        int const Rr = 3 * int(set.size());
+        int const Rp = (Rr + 3) / 4 * 4;
+        std::vector<double> A(size_t(Rr) * Rr);
+        for (int a2 = 0; a2 < Rr; a2++)
+          for (int b2 = 0; b2 < Rr; b2++)
+            A[size_t(a2) * Rr + b2] =
+                F[k][size_t(3 * set[a2 / 3] + a2 % 3) * nf + 3 * set[b2 / 3] + b2 % 3];
+        std::vector<double> V, w;
+        if (!sym_eig(Rr, A, V, w))
+          return ASGK_ERR_UNSUPPORTED;
+        int const id = int(toff.size());
+        toff.push_back(int(Qh.size()));
+        trp.push_back(Rp);
+        // Q [t][r] = eigenvector r's entry t; QT [r][t] = the same; theta
+        // padded to Rp entries
+        Qh.resize(Qh.size() + size_t(Rr) * Rp, 0.0);
+        QTh.resize(QTh.size() + size_t(Rr) * Rp, 0.0);
+        double *Qt = &Qh[toff.back()], *QTt = &QTh[toff.back()];
+        for (int t = 0; t < Rr; t++)
+          for (int r = 0; r < Rr; r++)
+          {
+            Qt[size_t(t) * Rp + r]  = V[size_t(t) * Rr + r];
+            QTt[size_t(r) * Rp + t] = V[size_t(t) * Rr + r];
+          }
+        tth.push_back(int(thh.size()));
+        thh.resize(thh.size() + Rp, 0.0);
+        for (int r = 0; r < Rr; r++)
+          thh[tth.back() + r] = w[r];
+        it = tabs.emplace(tk, id).first;
+      }
+      pen_tab.push_back(it->second);
+      s = e;
+    }
+    // units: pencils cut into group ranges, larger pencils first
+    int rpmax = 0;
+    for (int t : pen_tab)
+      rpmax = std::max(rpmax, trp[t]);
+    int const budget = std::max(256, rpmax);
+    std::vector<int> order(pen_m.size());
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int x, int y) { return pen_m[x] > pen_m[y]; });
+    std::vector<int4> units;
+    int max_rows = 0;
+    for (int pe : order)
+    {
+      int const Rp = trp[pen_tab[pe]];
+      int const G  = std::max(1, std::min(std::min(ng, 27), budget / Rp));
+      for (int g0 = 0; g0 < ng; g0 += G)
+      {
+        int const gc = std::min(G, ng - g0);
+        units.push_back(make_int4(pe, g0, gc, 0));
+        max_rows = std::max(max_rows, Rp * gc);
+      }
+    }
+    auto fac      = std::make_unique<line_factor>();
+    fac->k        = k;
+    fac->nunits   = int(units.size());
+    fac->max_rows = max_rows;
+    int rc;
+    if ((rc = upload(&fac->units, units, bytes)) || (rc = upload(&fac->pen_off, pen_off, bytes)) ||
+        (rc = upload(&fac->pen_m, pen_m, bytes)) || (rc = upload(&fac->pen_tab, pen_tab, bytes)) ||
+        (rc = upload(&fac->pen_cells, pen_cells, bytes)))
+      return rc;
+    ld->factors.push_back(std::move(fac));
+  }
+  std::vector<float> Q32(Qh.begin(), Qh.end()), QT32(QTh.begin(), QTh.end()),
+      th32(thh.begin(), thh.end()), self32(self.begin(), self.end());
+  int rc;
+  if ((rc = upload(&ld->c1, c1, bytes)) || (rc = upload(&ld->tab_off, toff, bytes)) ||
+      (rc = upload(&ld->tab_th, tth, bytes)) || (rc = upload(&ld->tab_rp, trp, bytes)) || (rc = upload(&ld->t64.Q, Qh, bytes)) ||
+      (rc = upload(&ld->t64.QT, QTh, bytes)) || (rc = upload(&ld->t64.theta, thh, bytes)) ||
+      (rc = upload(&ld->t64.self, self, bytes)) || (rc = upload(&ld->t32.Q, Q32, bytes)) ||
+      (rc = upload(&ld->t32.QT, QT32, bytes)) || (rc = upload(&ld->t32.theta, th32, bytes)) ||
+      (rc = upload(&ld->t32.self, self32, bytes)))
+    return rc;
+  size_t const wb = sizeof(double) * 2 * size_t(p.rows) * p.tensor;
+  ASGK_CUDA(cudaMalloc(&ld->work, wb));
+  bytes += int64_t(wb);
+  *out = ld.release();
+  return ASGK_OK;
+}
+
+namespace
+{
+template<typename R, int D, int M>
+int launch_factor(line_data const &ld, line_factor const &f, int q,
+                  const double *in64, const R *inR, double *out64, R *outR,
+                  bool bj, const double *sc, double *vscale, float *vc,
+                  cudaStream_t s)
+{
+  constexpr int NC  = ipow3l(M - 1);
+  constexpr int NCP = NC == 1 ? 1 : (NC == 3 ? 4 : 12);
+  line_tables<R> const &t = [&]() -> line_tables<R> const & {
+    if constexpr (sizeof(R) == 8)
+      return ld.t64;
+    else
+      return ld.t32;
+  }();
+  line_args<R> a{};
+  a.units = f.units, a.pen_off = f.pen_off, a.pen_m = f.pen_m, a.pen_tab = f.pen_tab;
+  a.pen_cells = f.pen_cells, a.c1 = ld.c1, a.tab_off = ld.tab_off, a.tab_th = ld.tab_th;
+  a.tab_rp = ld.tab_rp;
+  a.Q = t.Q, a.QT = t.QT, a.theta = t.theta, a.self = t.self, a.r1 = ld.r1;
+  a.k = f.k, a.kidx = q;
+  for (int i = 0; i < 3; i++)
+    a.line[i] = ld.line[i];
+  for (int i = 0; i < 6; i++)
+    a.nonline[i] = ld.nonline[i];
+  a.shift = R(ld.shift), a.dt = R(ld.dt);
+  size_t const shm = 2 * sizeof(R) * size_t(f.max_rows) * NCP;
+  auto kern        = k_line_factor<R, D, M>;
+  if (shm > 48 * 1024)
+    ASGK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   int(shm)));
+  kern<<<f.nunits, kLineThreads, shm, s>>>(a, in64, inR, out64, outR, bj ? 1 : 0,
+                                           sc, vscale, vc, g_gate);
+  ASGK_LAUNCHED();
+  return ASGK_OK;
+}
+
+template<typename R, int D, int M>
+int apply_dm(line_data const &ld, double *v, double *z, const double *sc,
+             float *vc, cudaStream_t s)
+{
+  int64_t const n = int64_t(ld.rows) * ld.ts;
+  R *w0 = reinterpret_cast<R *>(ld.work);
+  R *w1 = w0 + n;
+  R *cur = nullptr;
+  for (int q = 0; q < M; q++)
+  {
+    bool const first = q == 0, last = q == M - 1;
+    R *dst = (q % 2 == 0) ? w0 : w1;
+    if (int rc = launch_factor<R, D, M>(ld, *ld.factors[q], q, first ? v : nullptr,
+                                        first ? nullptr : cur, last ? z : nullptr,
+                                        last ? nullptr : dst, !first,
+                                        first ? sc : nullptr, first && sc ? v : nullptr,
+                                        first ? vc : nullptr, s))
+      return rc;
+    cur = dst;
+  }
+  return ASGK_OK;
+}
+
+template<typename R, int D>
+int apply_d(line_data const &ld, double *v, double *z, const double *sc,
+            float *vc, cudaStream_t s)
+{
+  switch (ld.m)
+  {
+  case 1: return apply_dm<R, D, 1>(ld, v, z, sc, vc, s);
+  case 2:
+    if constexpr (D >= 2)
+      return apply_dm<R, D, 2>(ld, v, z, sc, vc, s);
+    break;
+  case 3:
+    if constexpr (D >= 3)
+      return apply_dm<R, D, 3>(ld, v, z, sc, vc, s);
+    break;
+  default: break;
+  }
+  return ASGK_ERR_UNSUPPORTED;
+}
+} // namespace
+
+int line_apply(line_data const &ld, bool low, double *v, double *z,
+               const double *scale_state, float *vcopy, cudaStream_t s)
+{
+  auto go = [&](auto tag) -> int {
+    using R = decltype(tag);
+    switch (ld.d)
+    {
+    case 1: return apply_d<R, 1>(ld, v, z, scale_state, vcopy, s);
+    case 2: return apply_d<R, 2>(ld, v, z, scale_state, vcopy, s);
+    case 3: return apply_d<R, 3>(ld, v, z, scale_state, vcopy, s);
+    case 4: return apply_d<R, 4>(ld, v, z, scale_state, vcopy, s);
+    case 5: return apply_d<R, 5>(ld, v, z, scale_state, vcopy, s);
+    case 6: return apply_d<R, 6>(ld, v, z, scale_state, vcopy, s);
+    default: return ASGK_ERR_UNSUPPORTED;
+    }
+  };
+  return low ? go(float{}) : go(double{});
+}
+
+int line_info(line_data const &ld, int *dims)
+{
+  for (int q = 0; q < ld.m; q++)
+    dims[q] = ld.line[q];
+  return ld.m;
+}
+
+} // namespace asgk

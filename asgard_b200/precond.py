@@ -33,7 +33,7 @@ from ._lib import check, lib
 
 _MAGIC = b"ASGKMLP1"
 
-JACOBI_KINDS = {"point": 0, "block": 1, "kron": 2}
+JACOBI_KINDS = {"point": 0, "block": 1, "kron": 2, "line": 3}
 
 
 class JacobiPreconditioner:
@@ -41,7 +41,9 @@ class JacobiPreconditioner:
     kronmult_matrix (see asgk_jacobi_create in include/asgard_b200.h).
     kind "kron": the cell-block inverse through the eigendecompositions of
     its one-dimensional factors (global plans whose terms act in one
-    dimension each; raises AsgkError otherwise)."""
+    dimension each; raises AsgkError otherwise).  kind "line": exact solves
+    along the pencils of the dimensions with symmetric 1D operators, chained
+    (ASGK_JACOBI_LINE; global plans)."""
 
     def __init__(self, mat, dt, kind="block"):
         if kind not in JACOBI_KINDS:

@@ -30,7 +30,7 @@ def main():
                     help="connected pairs found on the GPU (from_grid) instead of "
                          "by the host builder; mode pairs only")
     ap.add_argument("--mode", default="global", choices=["pairs", "global"])
-    ap.add_argument("--precond", default="block", choices=["none", "point", "block", "kron"])
+    ap.add_argument("--precond", default="block", choices=["none", "point", "block", "kron", "line"])
     ap.add_argument("--precision", default="fp32", choices=["fp64", "fp32"])
     ap.add_argument("--restart", type=int, default=50)
     ap.add_argument("--tol", type=float, default=1e-10)

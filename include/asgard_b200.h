@@ -303,9 +303,16 @@ typedef enum asgk_jacobi_kind
 {
   ASGK_JACOBI_POINT = 0, /* the reference's diagonal preconditioner */
   ASGK_JACOBI_BLOCK = 1, /* inverse of each cell's n^d x n^d diagonal block */
-  ASGK_JACOBI_KRON  = 2  /* the same inverse through the eigendecompositions of
+  ASGK_JACOBI_KRON  = 2, /* the same inverse through the eigendecompositions of
                             the block's 1D factors (global plans whose terms act
                             in one dimension each; any d <= 6) */
+  ASGK_JACOBI_LINE  = 3  /* no counterpart in the reference: exact solves along
+                            the pencils of every dimension whose 1D operator is
+                            symmetric (1 to 3 such dimensions), chained
+                            M_km^-1 B ... B M_k1^-1 with B the cell-diagonal
+                            part of those dimensions' terms; global plans whose
+                            terms act in one dimension each, n = 3, d <= 6;
+                            ASGK_ERR_UNSUPPORTED without such a dimension */
 } asgk_jacobi_kind;
 
 /* Builds a Jacobi preconditioner of I - dt*K for a square plan, on the

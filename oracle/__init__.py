@@ -691,3 +691,122 @@ def diagonal_blocks(d, n, pntr, indx, terms, iA, vA):
                 m = np.kron(m, A)
             out[r] += m
     return out
+
+
+# ---------------------------------------------------------------- line Jacobi
+# The definition of this library's line preconditioner (ASGK_JACOBI_LINE;
+# no counterpart in the reference), stated with dense algebra at small sizes
+# so that it checks the device's eigendecomposition-based apply
+# independently.  Operators are sparse-grid operators in the global form
+# (every term acts in one dimension or is the identity), factors in the
+# per-1D-connection layout [conn][term][dim][n*n] of connect_1d(level).
+
+def _global_1d_operators(d, level, terms, vA, n=3):
+    """Per dimension the full 1D operator (n*2^level square) summed over the
+    terms acting in that dimension, and the number of identity terms."""
+    pntr, indx = connect_1d(level)
+    R = len(pntr) - 1
+    rows1 = np.repeat(np.arange(R), np.diff(pntr))
+    blocks = np.asarray(vA, dtype=np.float64).reshape(len(indx), terms, d, n, n)
+    blocks = blocks.transpose(0, 1, 2, 4, 3)  # [..., row i, col j]
+    eye = np.eye(n)
+    F = [np.zeros((n * R, n * R)) for _ in range(d)]
+    n_id = 0
+    for t in range(terms):
+        act = []
+        for k in range(d):
+            b = blocks[:, t, k]
+            ident = all(np.array_equal(b[j], eye if rows1[j] == indx[j] else 0 * eye)
+                        for j in range(len(indx)))
+            if not ident:
+                act.append(k)
+        if not act:
+            n_id += 1
+            continue
+        if len(act) > 1:
+            raise ValueError("terms acting in several dimensions are not supported")
+        k = act[0]
+        for j in range(len(indx)):
+            r, c = rows1[j], indx[j]
+            F[k][n * r:n * r + n, n * c:n * c + n] += blocks[j, t, k]
+    return F, n_id
+
+
+def line_dimensions(d, level, terms, vA, n=3):
+    """Dimensions with a nonzero symmetric 1D operator: the ones the line
+    preconditioner solves along (increasing order)."""
+    F, _ = _global_1d_operators(d, level, terms, vA, n)
+    out = []
+    for k in range(d):
+        s = np.abs(F[k]).max()
+        if s > 0 and np.abs(F[k] - F[k].T).max() <= 1e-12 * s:
+            out.append(k)
+    return out
+
+
+def line_jacobi_apply(d, level, table, terms, vA, dt, v, n=3):
+    """z = M_{k_m}^-1 B ... B M_{k_2}^-1 B M_{k_1}^-1 v over the line
+    dimensions k_1 < ... < k_m, with (s = 1 - dt * identity terms)
+      M_k = s I - dt (K_k + sum_{j line, j != k} D_j),   B = s I - dt sum_{j line} D_j,
+    K_k the operator of the terms acting in dimension k (block diagonal over
+    the pencils of cells that agree outside k) and D_j its cell-diagonal
+    part.  Each pencil system of M_k is assembled densely and solved."""
+    F, n_id = _global_1d_operators(d, level, terms, vA, n)
+    line = line_dimensions(d, level, terms, vA, n)
+    if not line:
+        raise ValueError("no dimension with a symmetric operator")
+    s = 1.0 - dt * n_id
+    table = np.asarray(table)
+    lev, pos = table[:, :d].astype(np.int64), table[:, d:].astype(np.int64)
+    c1 = np.where(lev == 0, 0, (1 << np.maximum(lev - 1, 0)) + pos)
+    cells = table.shape[0]
+    z = np.asarray(v, dtype=np.float64).reshape((cells,) + (n,) * d).copy()
+
+    def selfblock(j, c):
+        return F[j][n * c:n * c + n, n * c:n * c + n]
+
+    def along(M, x, axis):
+        return np.moveaxis(np.tensordot(M, x, axes=([1], [axis])), 0, axis)
+
+    def bj(z):
+        out = s * z
+        for cell in range(cells):
+            for j in line:
+                out[cell] -= dt * along(selfblock(j, c1[cell, j]), z[cell], j)
+        return out
+
+    def solve_k(z, k):
+        out = np.empty_like(z)
+        others = [j for j in range(d) if j != k]
+        keys = {}
+        for cell in range(cells):
+            keys.setdefault(tuple(c1[cell, others]), []).append(cell)
+        rest = n ** (d - 1)
+        for key, mem in keys.items():
+            mem = sorted(mem, key=lambda c: c1[c, k])
+            idx = np.concatenate([np.arange(n * c1[c, k], n * c1[c, k] + n) for c in mem])
+            AP = F[k][np.ix_(idx, idx)]
+            # the other line dimensions' self blocks, on the rest axes
+            # (dimensions != k in increasing order, the first slowest)
+            S = np.zeros((rest, rest))
+            for j in line:
+                if j == k:
+                    continue
+                m = np.ones((1, 1))
+                for jj in others:
+                    m = np.kron(m, selfblock(j, key[others.index(jj)]) if jj == j else np.eye(n))
+                S += m
+            M = s * np.eye(len(idx) * rest) - dt * (np.kron(AP, np.eye(rest)) +
+                                                    np.kron(np.eye(len(idx)), S))
+            # gather: rows (member, poly_k), columns the rest axes
+            X = np.stack([np.moveaxis(z[c], k, 0).reshape(n, rest) for c in mem])
+            U = np.linalg.solve(M, X.reshape(-1)).reshape(len(mem), n, rest)
+            for i, c in enumerate(mem):
+                out[c] = np.moveaxis(U[i].reshape((n,) + (n,) * (d - 1)), 0, k)
+        return out
+
+    for i, k in enumerate(line):
+        if i > 0:
+            z = bj(z)
+        z = solve_k(z, k)
+    return z.reshape(-1)

@@ -157,7 +157,7 @@ def test_cgs_step_against_fp64_reference(cuda, n, k):
 @pytest.mark.parametrize("mode,precond,precision", [
     ("pairs", None, "fp64"), ("pairs", "point", "fp64"),
     ("global", "block", "fp32"), ("global", None, "fp32"), ("global", "kron", "fp32"),
-    ("dense", "block", "fp64")])
+    ("global", "line", "fp32"), ("global", "line", "fp64"), ("dense", "block", "fp64")])
 def test_recorded_cycles_match_host_driven_cycles(cuda, mode, precond, precision):
     """Restart cycles run as recorded CUDA graphs (device-side Givens steps,
     one launch per cycle) give the host-driven loop's iterates bit for bit:
@@ -227,7 +227,7 @@ def test_fp32_basis_gram_schmidt(cuda, precond):
 
 
 @pytest.mark.parametrize("precond,precision", [(None, "fp32"), ("kron", "fp32"),
-                                               ("block", "fp64")])
+                                               ("block", "fp64"), ("line", "fp32")])
 def test_node_steps_give_the_same_iterates(cuda, precond, precision):
     """Recorded cycles with several Arnoldi steps per graph node (the kernels
     of steps after the cycle stopped skip themselves) give the iterates of
