@@ -1972,14 +1972,16 @@ int asgk_gmres_dense_precond(int n, const double *A, double *x, const double *b,
     if (!(tol > 0))
       tol = 1e-12;
     // the reference's dense_preconditioner (src/solver.cpp:11-38) factors M
-    // and applies M^-1 on the left to every residual and new basis vector,
-    // which is GMRES on (M^-1 A) x = M^-1 b: M^-1 is formed once here (LU
-    // with partial pivoting on the host) and applied after A on the device
-    std::vector<double> Minv, bp;
+    // (getrf) and solves with the factors (getrs) on the left of every
+    // residual b - A x and every new basis vector A v -- for device vectors
+    // on a host copy (:27-33); the same here: LU with partial pivoting on the
+    // host, the product on the device, the solve on the host
+    std::vector<double> lu;
+    std::vector<int> piv;
     if (M != nullptr)
     {
-      std::vector<double> lu(M, M + int64_t(n) * n);
-      std::vector<int> piv(n);
+      lu.assign(M, M + int64_t(n) * n);
+      piv.assign(n, 0);
       for (int c = 0; c < n; c++)
       {
         int p = c;
@@ -1992,9 +1994,8 @@ int asgk_gmres_dense_precond(int n, const double *A, double *x, const double *b,
         if (p != c)
           for (int j = 0; j < n; j++)
             std::swap(lu[c + int64_t(j) * n], lu[p + int64_t(j) * n]);
-        double const inv = 1.0 / lu[c + int64_t(c) * n];
         for (int r = c + 1; r < n; r++)
-          lu[r + int64_t(c) * n] *= inv;
+          lu[r + int64_t(c) * n] /= lu[c + int64_t(c) * n];
         for (int j = c + 1; j < n; j++)
         {
           double const u = lu[c + int64_t(j) * n];
@@ -2003,70 +2004,56 @@ int asgk_gmres_dense_precond(int n, const double *A, double *x, const double *b,
               lu[r + int64_t(j) * n] -= lu[r + int64_t(c) * n] * u;
         }
       }
-      auto solve = [&](double *v) {
-        for (int c = 0; c < n; c++)
-          if (piv[c] != c)
-            std::swap(v[c], v[piv[c]]);
-        for (int c = 0; c < n; c++)
-          for (int r = c + 1; r < n; r++)
-            v[r] -= lu[r + int64_t(c) * n] * v[c];
-        for (int c = n - 1; c >= 0; c--)
-        {
-          v[c] /= lu[c + int64_t(c) * n];
-          for (int r = 0; r < c; r++)
-            v[r] -= lu[r + int64_t(c) * n] * v[c];
-        }
-      };
-      Minv.assign(int64_t(n) * n, 0.0);
-      for (int j = 0; j < n; j++)
-      {
-        double *col = Minv.data() + int64_t(j) * n;
-        col[j]      = 1.0;
-        solve(col);
-      }
-      bp.assign(b, b + n);
-      solve(bp.data());
-      b = bp.data();
     }
-    double *dA = nullptr, *dx = nullptr, *db = nullptr, *dM = nullptr,
-           *dt = nullptr;
+    std::vector<double> hv(M != nullptr ? n : 0);
+    auto lu_solve = [&](double *v) {
+      for (int c = 0; c < n; c++)
+        if (piv[c] != c)
+          std::swap(v[c], v[piv[c]]);
+      for (int c = 0; c < n; c++)
+        for (int r = c + 1; r < n; r++)
+          v[r] -= lu[r + int64_t(c) * n] * v[c];
+      for (int c = n - 1; c >= 0; c--)
+      {
+        v[c] /= lu[c + int64_t(c) * n];
+        for (int r = 0; r < c; r++)
+          v[r] -= lu[r + int64_t(c) * n] * v[c];
+      }
+    };
+    double *dA = nullptr, *dx = nullptr, *db = nullptr;
     int64_t bytes = 0;
     int rc;
     if ((rc = dev_alloc(&dA, int64_t(n) * n, bytes)) ||
-        (rc = dev_alloc(&dx, n, bytes)) || (rc = dev_alloc(&db, n, bytes)) ||
-        (M != nullptr && ((rc = dev_alloc(&dM, int64_t(n) * n, bytes)) ||
-                          (rc = dev_alloc(&dt, n, bytes)))))
+        (rc = dev_alloc(&dx, n, bytes)) || (rc = dev_alloc(&db, n, bytes)))
     {
       cudaFree(dA);
       cudaFree(dx);
       cudaFree(db);
-      cudaFree(dM);
       return rc;
     }
     cudaStream_t s = nullptr;
     gmres_ws ws;
     core_stats st;
+    // y = beta*y + alpha*A*x, then y = M^-1 y with a preconditioner
     auto mat = [&](double a, const double *xin, double bb, double *yout,
                    cudaStream_t ss) -> int {
-      if (dM == nullptr)
-      {
-        k_dense_gemv<<<(n + 3) / 4, 128, 0, ss>>>(n, dA, a, xin, bb, yout);
-        ASGK_LAUNCHED();
+      k_dense_gemv<<<(n + 3) / 4, 128, 0, ss>>>(n, dA, a, xin, bb, yout);
+      ASGK_LAUNCHED();
+      if (M == nullptr)
         return ASGK_OK;
-      }
-      k_dense_gemv<<<(n + 3) / 4, 128, 0, ss>>>(n, dA, 1.0, xin, 0.0, dt);
-      ASGK_LAUNCHED();
-      k_dense_gemv<<<(n + 3) / 4, 128, 0, ss>>>(n, dM, a, dt, bb, yout);
-      ASGK_LAUNCHED();
+      ASGK_CUDA(cudaMemcpyAsync(hv.data(), yout, sizeof(double) * n,
+                                cudaMemcpyDeviceToHost, ss));
+      ASGK_CUDA(cudaStreamSynchronize(ss));
+      lu_solve(hv.data());
+      ASGK_CUDA(cudaMemcpyAsync(yout, hv.data(), sizeof(double) * n,
+                                cudaMemcpyHostToDevice, ss));
+      ASGK_CUDA(cudaStreamSynchronize(ss));
       return ASGK_OK;
     };
     rc = ASGK_OK;
     if (cudaMemcpy(dA, A, sizeof(double) * n * int64_t(n), cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMemcpy(dx, x, sizeof(double) * n, cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemcpy(db, b, sizeof(double) * n, cudaMemcpyHostToDevice) != cudaSuccess ||
-        (dM != nullptr &&
-         cudaMemcpy(dM, Minv.data(), sizeof(double) * n * int64_t(n),
-                    cudaMemcpyHostToDevice) != cudaSuccess))
+        cudaMemcpy(db, b, sizeof(double) * n, cudaMemcpyHostToDevice) != cudaSuccess)
       rc = ASGK_ERR_CUDA;
     if (rc == ASGK_OK)
       rc = gmres_core(ws, n, mat, nullptr, dx, db, restart, max_outer, tol, st, s);
@@ -2076,8 +2063,6 @@ int asgk_gmres_dense_precond(int n, const double *A, double *x, const double *b,
     cudaFree(dA);
     cudaFree(dx);
     cudaFree(db);
-    cudaFree(dM);
-    cudaFree(dt);
     if (rc == ASGK_OK && info)
     {
       *info              = asgk_gmres_info{};

@@ -10,11 +10,11 @@ dt = 5e-4, b uniform in [-1, 1] (seeded, a new b every step), GMRES restart
 
 A step is one solve by the framework's method: the operator in its global
 Kronecker form (the reference's global_kron_matrix; the same operator as
-the connected-pair kronmult, its terms acting in one dimension each),
-block-Jacobi right preconditioning (each cell's diagonal block inverted
-through the eigendecompositions of its 3x3 1D factors; the learned correction
-on top of it is trained and kept only if its validation solve gains), FP32
-operator inside FP64 iterative refinement.  Timed beside it: the plain
+the connected-pair kronmult, its terms acting in one dimension each), right
+preconditioning by exact solves along the pencils of the diffusion
+dimensions, chained (the learned correction on top of it is trained and kept
+only if its validation solve gains), FP32 operator inside FP64 iterative
+refinement.  Timed beside it: the plain
 baseline -- FP64 GMRES with the connected-pair FP64 kronmult (one solve by
 default: about four minutes at d=6) -- and, at d <= 4, the same method on the
 connected-pair operator.  Inputs are resident in HBM when the timed region
@@ -346,24 +346,29 @@ def reference_arm(args):
 
 def build_method(args, ab, op, mat, gmat, mmat, dt, rank):
     """Setup of the method, not timed (as the reference's matrix setup is
-    not part of solves/s): block-Jacobi inverse -- through the
-    eigendecompositions of each cell's 1D factors on the global form (any
-    d), else the dense per-cell inverses (n^d <= 81) -- and the learned
-    network's training.  Returns (method dict, training info)."""
+    not part of solves/s): the base preconditioner -- on the global form the
+    line preconditioner (exact solves along the pencils of the diffusion
+    dimensions, chained), else the cell-block inverse through the
+    eigendecompositions of each cell's 1D factors, else the dense per-cell
+    inverses (n^d <= 81) -- and the learned network's training.  Returns
+    (method dict, training info)."""
     import torch
     d = op.d
     precision = "fp64" if args.method.endswith("fp64") else "fp32"
     base, base_form = None, None
     if "block" in args.method:
         if gmat is not None:
-            try:
-                base = ab.JacobiPreconditioner(gmat, dt, kind="kron")
-                base_form = "Kronecker-sum form"
-            except ab.AsgkError:
-                base = None
+            for kind, form in (("line", "line solves along the diffusion dimensions"),
+                               ("kron", "block-Jacobi, Kronecker-sum form")):
+                try:
+                    base = ab.JacobiPreconditioner(gmat, dt, kind=kind)
+                    base_form = form
+                    break
+                except ab.AsgkError:
+                    base = None
         if base is None and 3 ** d <= 81:
             base = ab.JacobiPreconditioner(mmat, dt, kind="block")
-            base_form = "dense cell inverses"
+            base_form = "block-Jacobi, dense cell inverses"
     pc, train_info = base, None
     if args.method.startswith("learned"):
         # plain FP64 GMRES solves of random right-hand sides give (v, e)
@@ -393,10 +398,9 @@ def build_method(args, ab, op, mat, gmat, mmat, dt, rank):
     dropped = " (learned correction dropped: no gain in its validation solve)"
     parts = []
     if learned and pc is not None and pc is not base:
-        parts.append("learned preconditioner" + (" on block-Jacobi" if base is not None else ""))
+        parts.append("learned preconditioner" + (f" on {base_form}" if base is not None else ""))
     elif base is not None:
-        parts.append(f"block-Jacobi preconditioner ({base_form})"
-                     + (dropped if learned else ""))
+        parts.append(f"preconditioner: {base_form}" + (dropped if learned else ""))
     elif learned:
         parts.append("no preconditioner" + dropped)
     parts.append("FP32 operator, FP64 refinement" if precision == "fp32" else "FP64")
