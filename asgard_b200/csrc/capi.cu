@@ -62,6 +62,9 @@ void free_plan(plan_data &p)
   cudaFree(p.row_nslice);
   cudaFree(p.gscratch);
   cudaFree(p.gtickets);
+  cudaFree(p.gseg);
+  cudaFree(p.gcell_order);
+  cudaFree(p.gx32);
   cudaFree(p.gjobs);
   cudaFree(p.gchain_last);
   cudaFree(p.gd_ptr);
@@ -1743,6 +1746,40 @@ int asgk_plan_create_global(asgk_plan **plan, int d, int n, int level,
           (rc = up(p.gd_col, dcol.data(), sizeof(int) * dcol.size())) ||
           (rc = up(p.gd_conn, dconn.data(), sizeof(int) * dconn.size())) ||
           (rc = up(p.gd_rel, drel.data(), drel.size())))
+      {
+        asgk_plan_destroy(*plan);
+        *plan = nullptr;
+        return rc;
+      }
+    }
+    // d >= 5: per-cell dimension segments (the entries of a cell come in
+    // dimension order) and the cells by decreasing longest segment
+    if (d >= 5)
+    {
+      std::vector<int> seg(size_t(num_cells) * (d + 1));
+      std::vector<int> longest(num_cells, 0);
+      for (int r = 0; r < num_cells; r++)
+      {
+        int64_t e = gptr[r];
+        for (int k = 0; k <= d; k++)
+        {
+          while (e < gptr[r + 1] && gkb[e] % d < k)
+            ++e;
+          seg[size_t(r) * (d + 1) + k] = int(e - gptr[r]);
+        }
+        for (int k = 0; k < d; k++)
+          longest[r] = std::max(longest[r], seg[size_t(r) * (d + 1) + k + 1] -
+                                                seg[size_t(r) * (d + 1) + k]);
+      }
+      std::vector<int> corder(num_cells);
+      std::iota(corder.begin(), corder.end(), 0);
+      std::stable_sort(corder.begin(), corder.end(),
+                       [&](int a, int b) { return longest[a] > longest[b]; });
+      if ((rc = dev_alloc(&p.gseg, int64_t(seg.size()), bytes)) ||
+          (rc = dev_alloc(&p.gcell_order, num_cells, bytes)) ||
+          (rc = dev_alloc(&p.gx32, int64_t(num_cells) * p.tensor, bytes)) ||
+          (rc = up(p.gseg, seg.data(), sizeof(int) * seg.size())) ||
+          (rc = up(p.gcell_order, corder.data(), sizeof(int) * corder.size())))
       {
         asgk_plan_destroy(*plan);
         *plan = nullptr;

@@ -36,6 +36,7 @@
 #include <memory>
 #include <new>
 #include <numeric>
+#include <type_traits>
 #include <vector>
 
 namespace asgk
@@ -171,7 +172,31 @@ __device__ void dense_rows(const R *__restrict__ Mt, int Rr, int Rp, int G,
         acc[i][c] = R(0);
     const R *xr = in + g * NCP;
     const R *mr = Mt + 4 * rb;
-    for (int t = 0; t < Rr; t++)
+    // eight matrix rows' loads issued together (the pencil matrices come
+    // from L2); Rr is a multiple of 3, the remainder loop takes the rest
+    constexpr int U = 8;
+    int t = 0;
+    for (; t + U <= Rr; t += U)
+    {
+      R q[U][4];
+#pragma unroll
+      for (int u = 0; u < U; u++)
+        vec4_of<R>::load(mr + int64_t(t + u) * Rp, q[u]);
+#pragma unroll
+      for (int u = 0; u < U; u++)
+      {
+        R x[NC];
+#pragma unroll
+        for (int c = 0; c < NC; c++)
+          x[c] = xr[int64_t(t + u) * G * NCP + c];
+#pragma unroll
+        for (int i = 0; i < 4; i++)
+#pragma unroll
+          for (int c = 0; c < NC; c++)
+            acc[i][c] = fma(q[u][i], x[c], acc[i][c]);
+      }
+    }
+    for (; t < Rr; t++)
     {
       R q[4];
       vec4_of<R>::load(mr + int64_t(t) * Rp, q);
@@ -210,7 +235,7 @@ __device__ void dense_rows(const R *__restrict__ Mt, int Rr, int Rp, int G,
 // D dimensions, M line dimensions; NC = 3^(M-1) columns per group (the other
 // line dimensions' polynomials), groups: the 3^(D-M) polynomial indices of
 // the non-line dimensions.
-template<typename R, int D, int M>
+template<typename R, int D, int M, int KIDX>
 __global__ void __launch_bounds__(kLineThreads)
     k_line_factor(line_args<R> a, const double *in64,
                   const R *__restrict__ inR, double *__restrict__ out64,
@@ -257,7 +282,7 @@ __global__ void __launch_bounds__(kLineThreads)
     R lam = R(0);
     for (int q = M - 1; q >= 0; q--)
     {
-      if (q == a.kidx)
+      if (q == KIDX)
         continue;
       int const j  = a.line[q];
       int const dg = c % 3;
@@ -321,7 +346,7 @@ __global__ void __launch_bounds__(kLineThreads)
           v[pk][c] = X[((int64_t(i) * 3 + pk) * G + g) * NCP + c];
       // this member's own self block along k
       R Sk[9];
-      const R *sf = a.self + (int64_t(a.kidx) * a.r1 +
+      const R *sf = a.self + (int64_t(KIDX) * a.r1 +
                               a.c1[int64_t(cells[i]) * D + a.k]) * kSelfEntry + 12;
 #pragma unroll
       for (int e = 0; e < 9; e++)
@@ -339,7 +364,7 @@ __global__ void __launch_bounds__(kLineThreads)
 #pragma unroll
           for (int q = M - 1; q >= 0; q--)
           {
-            if (q == a.kidx)
+            if (q == KIDX)
               continue;
             int const dg = (c / stride) % 3;
             int const cb = c - dg * stride;
@@ -375,7 +400,7 @@ __global__ void __launch_bounds__(kLineThreads)
 #pragma unroll
         for (int q = M - 1; q >= 0; q--)
         {
-          if (q == a.kidx)
+          if (q == KIDX)
             continue;
           R w[NC];
 #pragma unroll
@@ -428,6 +453,210 @@ __global__ void __launch_bounds__(kLineThreads)
   }
 }
 
+// Pencils of at most kSmallMaxM cells: a CTA stages whole cells (up to
+// kSmallCells, from pencils of one size) in shared memory with coalesced
+// loads and, per pencil column -- one fibre along k in every cell of the
+// pencil -- runs the pencil solve in registers.  With W the other line
+// dimensions' eigenvector transform, M_k^-1 B = W (Q D^-1 Q^T) Bt W^T where
+// Bt = mu I - dt S_k along k (mu = s - dt sum_{j line, j != k} lambda_j of the
+// column's polynomial indices, S_k the cell's own self block along k): W^T
+// as fibre stages over the staged cells, then Bt, Q^T, the division by
+// mu - dt theta and Q in registers per column, then W.
+constexpr int kSmallThreads = 256;
+constexpr int kSmallCells   = 16;
+constexpr int kSmallMaxM    = 8;
+
+template<typename R, int D, int M, int KIDX, int MC>
+__device__ __forceinline__ void small_column(line_args<R> const &a, R *buf,
+                                             int slot0, int fb, unsigned dig,
+                                             int stk, int tab, bool bj,
+                                             const R (*s_Sk)[9],
+                                             const R (*s_lam)[2][3])
+{
+  constexpr int TS = ipow3l(D);
+  constexpr int RR = 3 * MC;
+  R x[RR];
+#pragma unroll
+  for (int i = 0; i < MC; i++)
+#pragma unroll
+    for (int pk = 0; pk < 3; pk++)
+      x[3 * i + pk] = buf[(slot0 + i) * TS + fb + pk * stk];
+  // mu from the other line dimensions' polynomial indices of this column
+  R mu = a.shift;
+#pragma unroll
+  for (int qq = 0; qq < M - 1; qq++)
+    mu -= a.dt * s_lam[slot0][qq][(dig >> (2 * qq)) & 3u];
+  if (bj)
+  {
+#pragma unroll
+    for (int i = 0; i < MC; i++)
+    {
+      R const x0 = x[3 * i], x1 = x[3 * i + 1], x2 = x[3 * i + 2];
+      const R *S = s_Sk[slot0 + i];
+#pragma unroll
+      for (int pk = 0; pk < 3; pk++)
+        x[3 * i + pk] = mu * x[3 * i + pk] - a.dt * (S[pk] * x0 + S[pk + 3] * x1 + S[pk + 6] * x2);
+    }
+  }
+  int const Rp  = a.tab_rp[tab];
+  const R *Qm   = a.Q + a.tab_off[tab];
+  const R *th   = a.theta + a.tab_th[tab];
+  R u[RR];
+#pragma unroll
+  for (int r = 0; r < RR; r++)
+  {
+    R acc = R(0);
+#pragma unroll
+    for (int t = 0; t < RR; t++)
+      acc = fma(__ldg(Qm + t * Rp + r), x[t], acc);
+    u[r] = acc / (mu - a.dt * __ldg(th + r));
+  }
+#pragma unroll
+  for (int t = 0; t < RR; t++)
+  {
+    R acc = R(0);
+#pragma unroll
+    for (int r = 0; r < RR; r++)
+      acc = fma(__ldg(Qm + t * Rp + r), u[r], acc);
+    x[t] = acc;
+  }
+#pragma unroll
+  for (int i = 0; i < MC; i++)
+#pragma unroll
+    for (int pk = 0; pk < 3; pk++)
+      buf[(slot0 + i) * TS + fb + pk * stk] = x[3 * i + pk];
+}
+
+template<typename R, int D, int M, int KIDX, int MC>
+__global__ void __launch_bounds__(kSmallThreads, 2)
+    k_line_small(line_args<R> a, const int4 *__restrict__ batches,
+                 const double *in64, const R *__restrict__ inR,
+                 double *__restrict__ out64, R *__restrict__ outR, int bj,
+                 const double *scale_state, double *vscale, float *vcopy,
+                 const double *gate)
+{
+  if (gate_closed(gate))
+    return;
+  constexpr int TS = ipow3l(D);
+  constexpr int NF = TS / 3;
+  extern __shared__ __align__(16) unsigned char line_small_smem[];
+  R *buf = reinterpret_cast<R *>(line_small_smem);
+  __shared__ int s_cell[kSmallCells];
+  // per fibre index: the first entry of the fibre along k and along each
+  // other line dimension, and the column's polynomial digits in the other
+  // line dimensions (packed two bits each) -- computed once, so the loops
+  // below do no integer division by run-time strides
+  __shared__ short s_fbk[NF];
+  __shared__ short s_fbo[2][NF];
+  __shared__ unsigned char s_dig[NF];
+  __shared__ R s_P[kSmallCells][2][9];
+  __shared__ R s_lam[kSmallCells][2][3];
+  __shared__ R s_Sk[kSmallCells][9];
+  int4 const bt  = batches[blockIdx.x];
+  int const pen0 = bt.x, npen = bt.y, m = MC;
+  int const nc   = npen * m;
+  int const tid  = threadIdx.x;
+  if (tid < nc)
+    s_cell[tid] = a.pen_cells[a.pen_off[pen0 + tid / m] + tid % m];
+  int const stk = ipow3l(D - 1 - a.k);
+  for (int fi = tid; fi < NF; fi += blockDim.x)
+  {
+    int const fb = (fi / stk) * 3 * stk + fi % stk;
+    s_fbk[fi]    = short(fb);
+    unsigned dg  = 0;
+    for (int qq = 0; qq < M - 1; qq++)
+    {
+      int const q  = qq < KIDX ? qq : qq + 1;
+      int const sj = ipow3l(D - 1 - a.line[q]);
+      s_fbo[qq][fi] = short((fi / sj) * 3 * sj + fi % sj);
+      dg |= unsigned((fb / sj) % 3) << (2 * qq);
+    }
+    s_dig[fi] = (unsigned char)dg;
+  }
+  __syncthreads();
+  // other line dimensions' eigen data (constant over a pencil) and each
+  // cell's own self block along k
+  for (int e = tid; e < nc * 2 * 12; e += blockDim.x)
+  {
+    int const slot = e / 24, qq = (e / 12) % 2, ee = e % 12;
+    if (qq >= M - 1)
+      continue;
+    int const q = qq < KIDX ? qq : qq + 1; // qq-th line index other than KIDX
+    const R *sf = a.self + (int64_t(q) * a.r1 +
+                            a.c1[int64_t(s_cell[slot]) * D + a.line[q]]) * kSelfEntry;
+    if (ee < 9)
+      s_P[slot][qq][ee] = sf[ee];
+    else
+      s_lam[slot][qq][ee - 9] = sf[ee];
+  }
+  for (int e = tid; e < nc * 9; e += blockDim.x)
+  {
+    int const slot = e / 9;
+    s_Sk[slot][e % 9] = a.self[(int64_t(KIDX) * a.r1 +
+                                a.c1[int64_t(s_cell[slot]) * D + a.k]) * kSelfEntry + 12 + e % 9];
+  }
+  // stage the cells
+  double const f = scale_state ? scale_state[1] : 1.0;
+  for (int e = tid; e < nc * TS; e += blockDim.x)
+  {
+    int64_t const gi = int64_t(s_cell[e / TS]) * TS + e % TS;
+    if (in64)
+    {
+      double vv = in64[gi];
+      if (scale_state)
+      {
+        vv *= f;
+        vscale[gi] = vv;
+        if (vcopy)
+          vcopy[gi] = float(vv);
+      }
+      buf[e] = R(vv);
+    }
+    else
+      buf[e] = inR[gi];
+  }
+  __syncthreads();
+  // W^T (forward) or W (backward): fibre stages along the other line dimensions
+  auto other_stages = [&](bool forward) {
+    for (int qq = 0; qq < M - 1; qq++)
+    {
+      int const q  = qq < KIDX ? qq : qq + 1;
+      int const sj = ipow3l(D - 1 - a.line[q]);
+      for (int it = tid; it < nc * NF; it += blockDim.x)
+      {
+        int const slot = it / NF, fi = it - slot * NF;
+        int const base = slot * TS + s_fbo[qq][fi];
+        R const x0 = buf[base], x1 = buf[base + sj], x2 = buf[base + 2 * sj];
+        const R *P = s_P[slot][qq];
+#pragma unroll
+        for (int o = 0; o < 3; o++)
+          buf[base + o * sj] = forward ? P[3 * o] * x0 + P[3 * o + 1] * x1 + P[3 * o + 2] * x2
+                                       : P[o] * x0 + P[o + 3] * x1 + P[o + 6] * x2;
+      }
+      __syncthreads();
+    }
+  };
+  other_stages(true);
+  // the pencil solves, one column (fibre along k) per item
+  int const tab = a.pen_tab[pen0];
+  for (int it = tid; it < npen * NF; it += blockDim.x)
+  {
+    int const pi = it / NF, fi = it - pi * NF;
+    small_column<R, D, M, KIDX, MC>(a, buf, pi * MC, s_fbk[fi], s_dig[fi], stk, tab,
+                                    bj, s_Sk, s_lam);
+  }
+  __syncthreads();
+  other_stages(false);
+  for (int e = tid; e < nc * TS; e += blockDim.x)
+  {
+    int64_t const gi = int64_t(s_cell[e / TS]) * TS + e % TS;
+    if (out64)
+      out64[gi] = double(buf[e]);
+    else
+      outR[gi] = buf[e];
+  }
+}
+
 template<typename R>
 struct line_tables
 {
@@ -444,13 +673,16 @@ struct line_tables
 struct line_factor
 {
   int k = 0;
-  int nunits = 0;
+  int nunits = 0;   // (pencil, group range) units of the larger pencils
   int max_rows = 0; // largest Rp * G of its units (shared memory)
-  int4 *units = nullptr;
+  int nbatches = 0; // batches of pencils of 1, 2, 4 or 8 cells
+  int bfirst[4] = {0, 0, 0, 0}, bcount[4] = {0, 0, 0, 0}; // per size 1, 2, 4, 8
+  int4 *units = nullptr, *batches = nullptr;
   int *pen_off = nullptr, *pen_m = nullptr, *pen_tab = nullptr, *pen_cells = nullptr;
   ~line_factor()
   {
     cudaFree(units);
+    cudaFree(batches);
     cudaFree(pen_off);
     cudaFree(pen_m);
     cudaFree(pen_tab);
@@ -662,34 +894,75 @@ int line_build(plan_data const &p, double dt, line_data **out, int64_t &bytes)
       pen_tab.push_back(it->second);
       s = e;
     }
-    // units: pencils cut into group ranges, larger pencils first
-    int rpmax = 0;
-    for (int t : pen_tab)
-      rpmax = std::max(rpmax, trp[t]);
-    int const budget = std::max(256, rpmax);
-    std::vector<int> order(pen_m.size());
-    std::iota(order.begin(), order.end(), 0);
-    std::stable_sort(order.begin(), order.end(),
-                     [&](int x, int y) { return pen_m[x] > pen_m[y]; });
-    std::vector<int4> units;
-    int max_rows = 0;
-    for (int pe : order)
+    // pencils ordered by size (larger first), then by matrix; pencils of
+    // 1, 2, 4 or 8 cells go in batches of up to kSmallCells cells of one
+    // matrix (k_line_small), the others are cut into group-range units
     {
+      std::vector<int> order(pen_m.size());
+      std::iota(order.begin(), order.end(), 0);
+      std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+        if (pen_m[x] != pen_m[y])
+          return pen_m[x] > pen_m[y];
+        return pen_tab[x] < pen_tab[y];
+      });
+      std::vector<int> o_off, o_m, o_tab;
+      for (int pe : order)
+      {
+        o_off.push_back(pen_off[pe]);
+        o_m.push_back(pen_m[pe]);
+        o_tab.push_back(pen_tab[pe]);
+      }
+      pen_off.swap(o_off);
+      pen_m.swap(o_m);
+      pen_tab.swap(o_tab);
+    }
+    auto small = [](int m) { return m == 1 || m == 2 || m == 4 || m == kSmallMaxM; };
+    int rpmax = 0;
+    for (size_t pe = 0; pe < pen_m.size(); pe++)
+      if (!small(pen_m[pe]))
+        rpmax = std::max(rpmax, trp[pen_tab[pe]]);
+    int const budget = std::max(256, rpmax);
+    std::vector<int4> units, batches;
+    int max_rows = 0;
+    for (size_t pe = 0; pe < pen_m.size();)
+    {
+      int const m = pen_m[pe];
+      if (small(m))
+      {
+        int const per = kSmallCells / m;
+        size_t e      = pe;
+        while (e < pen_m.size() && e - pe < size_t(per) && pen_m[e] == m &&
+               pen_tab[e] == pen_tab[pe])
+          ++e;
+        batches.push_back(make_int4(int(pe), int(e - pe), m, 0));
+        pe = e;
+        continue;
+      }
       int const Rp = trp[pen_tab[pe]];
       int const G  = std::max(1, std::min(std::min(ng, 27), budget / Rp));
       for (int g0 = 0; g0 < ng; g0 += G)
       {
         int const gc = std::min(G, ng - g0);
-        units.push_back(make_int4(pe, g0, gc, 0));
+        units.push_back(make_int4(int(pe), g0, gc, 0));
         max_rows = std::max(max_rows, Rp * gc);
       }
+      ++pe;
     }
     auto fac      = std::make_unique<line_factor>();
     fac->k        = k;
     fac->nunits   = int(units.size());
     fac->max_rows = max_rows;
+    fac->nbatches = int(batches.size());
+    for (size_t b = 0; b < batches.size(); b++)
+    {
+      int const sz = batches[b].z == 1 ? 0 : batches[b].z == 2 ? 1 : batches[b].z == 4 ? 2 : 3;
+      if (fac->bcount[sz] == 0)
+        fac->bfirst[sz] = int(b);
+      ++fac->bcount[sz];
+    }
     int rc;
-    if ((rc = upload(&fac->units, units, bytes)) || (rc = upload(&fac->pen_off, pen_off, bytes)) ||
+    if ((rc = upload(&fac->units, units, bytes)) || (rc = upload(&fac->batches, batches, bytes)) ||
+        (rc = upload(&fac->pen_off, pen_off, bytes)) ||
         (rc = upload(&fac->pen_m, pen_m, bytes)) || (rc = upload(&fac->pen_tab, pen_tab, bytes)) ||
         (rc = upload(&fac->pen_cells, pen_cells, bytes)))
       return rc;
@@ -714,11 +987,10 @@ int line_build(plan_data const &p, double dt, line_data **out, int64_t &bytes)
 
 namespace
 {
-template<typename R, int D, int M>
-int launch_factor(line_data const &ld, line_factor const &f, int q,
-                  const double *in64, const R *inR, double *out64, R *outR,
-                  bool bj, const double *sc, double *vscale, float *vc,
-                  cudaStream_t s)
+template<typename R, int D, int M, int KIDX>
+int launch_factor(line_data const &ld, line_factor const &f, const double *in64,
+                  const R *inR, double *out64, R *outR, bool bj,
+                  const double *sc, double *vscale, float *vc, cudaStream_t s)
 {
   constexpr int NC  = ipow3l(M - 1);
   constexpr int NCP = NC == 1 ? 1 : (NC == 3 ? 4 : 12);
@@ -733,21 +1005,54 @@ int launch_factor(line_data const &ld, line_factor const &f, int q,
   a.pen_cells = f.pen_cells, a.c1 = ld.c1, a.tab_off = ld.tab_off, a.tab_th = ld.tab_th;
   a.tab_rp = ld.tab_rp;
   a.Q = t.Q, a.QT = t.QT, a.theta = t.theta, a.self = t.self, a.r1 = ld.r1;
-  a.k = f.k, a.kidx = q;
+  a.k = f.k, a.kidx = KIDX;
   for (int i = 0; i < 3; i++)
     a.line[i] = ld.line[i];
   for (int i = 0; i < 6; i++)
     a.nonline[i] = ld.nonline[i];
   a.shift = R(ld.shift), a.dt = R(ld.dt);
-  size_t const shm = 2 * sizeof(R) * size_t(f.max_rows) * NCP;
-  auto kern        = k_line_factor<R, D, M>;
-  if (shm > 48 * 1024)
+  auto small = [&](auto mc, int sz) -> int {
+    constexpr int MC = decltype(mc)::value;
+    if (f.bcount[sz] == 0)
+      return ASGK_OK;
+    size_t const shm = sizeof(R) * size_t(kSmallCells) * ipow3l(D);
+    auto kern        = k_line_small<R, D, M, KIDX, MC>;
     ASGK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    int(shm)));
-  kern<<<f.nunits, kLineThreads, shm, s>>>(a, in64, inR, out64, outR, bj ? 1 : 0,
-                                           sc, vscale, vc, g_gate);
-  ASGK_LAUNCHED();
+    kern<<<f.bcount[sz], kSmallThreads, shm, s>>>(a, f.batches + f.bfirst[sz], in64, inR,
+                                                  out64, outR, bj ? 1 : 0, sc, vscale,
+                                                  vc, g_gate);
+    ASGK_LAUNCHED();
+    return ASGK_OK;
+  };
+  if (int rc = small(std::integral_constant<int, 8>{}, 3))
+    return rc;
+  if (int rc = small(std::integral_constant<int, 4>{}, 2))
+    return rc;
+  if (int rc = small(std::integral_constant<int, 2>{}, 1))
+    return rc;
+  if (int rc = small(std::integral_constant<int, 1>{}, 0))
+    return rc;
+  if (f.nunits > 0)
+  {
+    size_t const shm = 2 * sizeof(R) * size_t(f.max_rows) * NCP;
+    auto kern        = k_line_factor<R, D, M, KIDX>;
+    ASGK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   int(shm)));
+    kern<<<f.nunits, kLineThreads, shm, s>>>(a, in64, inR, out64, outR, bj ? 1 : 0,
+                                             sc, vscale, vc, g_gate);
+    ASGK_LAUNCHED();
+  }
   return ASGK_OK;
+}
+
+template<typename R, int D, int M, int KIDX>
+int factor_q(line_data const &ld, const double *in64, const R *inR, double *out64,
+             R *outR, bool bj, const double *sc, double *vscale, float *vc,
+             cudaStream_t s)
+{
+  return launch_factor<R, D, M, KIDX>(ld, *ld.factors[KIDX], in64, inR, out64, outR,
+                                      bj, sc, vscale, vc, s);
 }
 
 template<typename R, int D, int M>
@@ -762,11 +1067,24 @@ int apply_dm(line_data const &ld, double *v, double *z, const double *sc,
   {
     bool const first = q == 0, last = q == M - 1;
     R *dst = (q % 2 == 0) ? w0 : w1;
-    if (int rc = launch_factor<R, D, M>(ld, *ld.factors[q], q, first ? v : nullptr,
-                                        first ? nullptr : cur, last ? z : nullptr,
-                                        last ? nullptr : dst, !first,
-                                        first ? sc : nullptr, first && sc ? v : nullptr,
-                                        first ? vc : nullptr, s))
+    const double *i64 = first ? v : nullptr;
+    const R *iR       = first ? nullptr : cur;
+    double *o64       = last ? z : nullptr;
+    R *oR             = last ? nullptr : dst;
+    const double *fsc = first ? sc : nullptr;
+    double *fvs       = first && sc ? v : nullptr;
+    float *fvc        = first ? vc : nullptr;
+    int rc            = ASGK_ERR_UNSUPPORTED;
+    if (q == 0)
+      rc = factor_q<R, D, M, 0>(ld, i64, iR, o64, oR, !first, fsc, fvs, fvc, s);
+    else if constexpr (M >= 2)
+    {
+      if (q == 1)
+        rc = factor_q<R, D, M, 1>(ld, i64, iR, o64, oR, !first, fsc, fvs, fvc, s);
+      else if constexpr (M >= 3)
+        rc = factor_q<R, D, M, 2>(ld, i64, iR, o64, oR, !first, fsc, fvs, fvc, s);
+    }
+    if (rc)
       return rc;
     cur = dst;
   }

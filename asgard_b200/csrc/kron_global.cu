@@ -20,6 +20,9 @@
 // 2 * 3^(d+1) flops per entry; the neighbour tensors come from L2.
 #include "internal.cuh"
 
+#include <algorithm>
+#include <cstdint>
+
 namespace asgk
 {
 namespace
@@ -234,6 +237,135 @@ __global__ void __launch_bounds__(NW * 32)
     tickets[row] = 0u; // ready for the next launch
 }
 
+// d >= 5: one CTA per output cell, warp k takes the cell's neighbours
+// along dimension k (no barrier until the end): lane f owns fibres f,
+// f + 32, ... of the 3^d tensor along k, loads each neighbour's fibre (from
+// the FP32 copy of x in the FP32 apply: 47 MB at d=6, level 7, held in L2
+// across the re-reads) and accumulates the 3x3 block's product in
+// registers; the warps' results meet in shared memory and are added in
+// dimension order with the Euler and beta terms (FP64 x and y).
+template<int D, typename TC, typename TX>
+__global__ void __launch_bounds__(D * 32)
+    kron_global_cell(const int *__restrict__ order,
+                     const int64_t *__restrict__ gptr,
+                     const int *__restrict__ gseg, const int *__restrict__ gcol,
+                     const int *__restrict__ gkb, const TC *__restrict__ B,
+                     double alpha, const TX *__restrict__ xs,
+                     const double *__restrict__ x, double beta,
+                     double *__restrict__ y, double ex,
+                     const double *__restrict__ gate)
+{
+  if (gate_closed(gate))
+    return;
+  constexpr int TS  = ipow3g(D);
+  constexpr int NF  = TS / 3;
+  constexpr int FPL = (NF + 31) / 32;
+  constexpr int PAD = padG<TC>::value;
+  __shared__ TC rows[D * TS];
+  int const k    = threadIdx.x >> 5;
+  int const lane = threadIdx.x & 31;
+  int const cell = order[blockIdx.x];
+  int64_t const e0 = gptr[cell];
+  int const sa = gseg[cell * (D + 1) + k], sb = gseg[cell * (D + 1) + k + 1];
+  int const stride = dim_stride<D>(k);
+  int fb[FPL];
+  TC acc[FPL][3];
+#pragma unroll
+  for (int m = 0; m < FPL; m++)
+  {
+    int const f = lane + 32 * m;
+    fb[m]       = (f / stride) * 3 * stride + (f % stride);
+    acc[m][0] = acc[m][1] = acc[m][2] = TC(0);
+  }
+  auto entry = [&](int64_t j) {
+    const TC *b  = B + int64_t(__ldg(gkb + j)) * PAD;
+    const TX *xc = xs + int64_t(__ldg(gcol + j)) * TS;
+    TC b0, b1, b2, b3, b4, b5, b6, b7, b8;
+    if constexpr (sizeof(TC) == 4)
+    {
+      const float4 *q = reinterpret_cast<const float4 *>(b);
+      float4 const q0 = __ldg(q), q1 = __ldg(q + 1), q2 = __ldg(q + 2);
+      b0 = q0.x, b1 = q0.y, b2 = q0.z, b3 = q0.w;
+      b4 = q1.x, b5 = q1.y, b6 = q1.z, b7 = q1.w;
+      b8 = q2.x;
+    }
+    else
+    {
+      const double2 *q = reinterpret_cast<const double2 *>(b);
+      double2 const q0 = __ldg(q), q1 = __ldg(q + 1), q2 = __ldg(q + 2);
+      double2 const q3 = __ldg(q + 3), q4 = __ldg(q + 4);
+      b0 = q0.x, b1 = q0.y, b2 = q1.x, b3 = q1.y, b4 = q2.x;
+      b5 = q2.y, b6 = q3.x, b7 = q3.y, b8 = q4.x;
+    }
+    TC v[FPL][3];
+#pragma unroll
+    for (int m = 0; m < FPL; m++)
+      if (lane + 32 * m < NF)
+#pragma unroll
+        for (int p = 0; p < 3; p++)
+          v[m][p] = static_cast<TC>(__ldg(xc + fb[m] + p * stride));
+#pragma unroll
+    for (int m = 0; m < FPL; m++)
+      if (lane + 32 * m < NF)
+      {
+        // column-major block: out_q += sum_p A(q, p) v_p, A(q, p) = b[q + 3p]
+        acc[m][0] = fma(b6, v[m][2], fma(b3, v[m][1], fma(b0, v[m][0], acc[m][0])));
+        acc[m][1] = fma(b7, v[m][2], fma(b4, v[m][1], fma(b1, v[m][0], acc[m][1])));
+        acc[m][2] = fma(b8, v[m][2], fma(b5, v[m][1], fma(b2, v[m][0], acc[m][2])));
+      }
+  };
+  for (int j = sa; j < sb; j++)
+    entry(e0 + j);
+  TC *row = rows + k * TS;
+#pragma unroll
+  for (int m = 0; m < FPL; m++)
+    if (lane + 32 * m < NF)
+    {
+      row[fb[m]]              = acc[m][0];
+      row[fb[m] + stride]     = acc[m][1];
+      row[fb[m] + 2 * stride] = acc[m][2];
+    }
+  __syncthreads();
+  int64_t const base = int64_t(cell) * TS;
+  for (int i = threadIdx.x; i < TS; i += D * 32)
+  {
+    TC s = TC(0);
+#pragma unroll
+    for (int kk = 0; kk < D; kk++)
+      s += rows[kk * TS + i];
+    double v = alpha * static_cast<double>(s) + ex * x[base + i];
+    if (beta != 0.0)
+      v += beta * y[base + i];
+    y[base + i] = v;
+  }
+}
+
+// the FP32 copy of x the FP32 cell kernel reads; pairs of values when x is
+// 16-byte aligned, single values otherwise (a basis column of an odd-length
+// system)
+__global__ void k_copy_to_f32(int64_t n, const double *__restrict__ x,
+                              float *__restrict__ x32, int pairs,
+                              const double *__restrict__ gate)
+{
+  if (gate_closed(gate))
+    return;
+  int64_t const t0 = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  int64_t const ts = int64_t(gridDim.x) * blockDim.x;
+  if (pairs)
+  {
+    for (int64_t i = t0; i < n / 2; i += ts)
+    {
+      double2 const v = reinterpret_cast<const double2 *>(x)[i];
+      reinterpret_cast<float2 *>(x32)[i] = make_float2(float(v.x), float(v.y));
+    }
+    if (t0 == 0 && (n & 1))
+      x32[n - 1] = float(x[n - 1]);
+  }
+  else
+    for (int64_t i = t0; i < n; i += ts)
+      x32[i] = float(x[i]);
+}
+
 // One stage of the chains of the terms acting in several dimensions
 // (src/device/asgard_glkronmult_cpu.cpp:103-181): for job (chain, dimension
 // k, fill, term) and output cell r,
@@ -361,6 +493,31 @@ int launch_global_d(plan_data const &p, double alpha, const double *x,
     B = p.gB64;
   else
     B = p.gB32;
+  if constexpr (D >= 5)
+  {
+    if (p.gseg != nullptr)
+    {
+      int64_t const n = int64_t(p.rows) * TS;
+      if constexpr (sizeof(TC) == 4)
+      {
+        int const pairs  = (reinterpret_cast<uintptr_t>(x) % 16) == 0 ? 1 : 0;
+        int const blocks = int(std::min<int64_t>((n / 2 + 255) / 256, 4 * 148));
+        k_copy_to_f32<<<blocks, 256, 0, s>>>(n, x, p.gx32, pairs, g_gate);
+        ASGK_LAUNCHED();
+        kron_global_cell<D, TC, float><<<p.rows, D * 32, 0, s>>>(
+            p.gcell_order, p.gptr, p.gseg, p.gcol, p.gkb, B, alpha, p.gx32, x, beta, y,
+            ex, g_gate);
+      }
+      else
+        kron_global_cell<D, TC, double><<<p.rows, D * 32, 0, s>>>(
+            p.gcell_order, p.gptr, p.gseg, p.gcol, p.gkb, B, alpha, x, x, beta, y, ex,
+            g_gate);
+      ASGK_LAUNCHED();
+      if (p.gchains > 0)
+        return launch_chains<D, TC>(p, alpha, x, y, s);
+      return ASGK_OK;
+    }
+  }
   kron_global_rows<D, TC, NW, SLICE><<<p.gslices, NW * 32, 0, s>>>(
       p.slice_row, p.slice_beg, p.slice_len, p.row_slice0, p.row_nslice, p.gcol, p.gkb, B,
       p.gscratch, p.gtickets, alpha, x, beta, y, ex, g_gate);

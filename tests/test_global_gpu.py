@@ -230,3 +230,24 @@ def test_value_update_changing_identity_terms_drops_recorded_cycles(cuda):
     x_new, it_new = solve(ab.kronmult_matrix.from_global(d, 3, L, table, T, v1))
     assert it_upd == it_new
     assert np.array_equal(x_upd, x_new)
+
+
+def test_global_cell_kernel_misaligned_and_aliasing_free_input(cuda):
+    """d >= 5 applies read x through an FP32 copy in FP32: an input that is
+    only 8-byte aligned (a column of an odd-length system) gives the same
+    result as an aligned copy of it."""
+    import asgard_b200 as ab
+    import torch
+    op = ab.SparseGridOperator(5, 3, 4, kind="advdiff")
+    g = op.kronmult_matrix(mode="global")
+    x = np.random.default_rng(9).uniform(-1, 1, op.N)
+    buf = torch.zeros(op.N + 1, dtype=torch.float64, device="cuda")
+    buf[1:] = _dev(x)
+    xs = buf[1:]                      # 8 bytes past a 256-byte boundary
+    assert xs.data_ptr() % 16 == 8
+    for prec in ("fp32", "fp64"):
+        ya, yb = torch.zeros_like(xs), torch.zeros_like(xs)
+        g.apply(1.0, xs, 0.0, ya, precision=prec)
+        g.apply(1.0, _dev(x), 0.0, yb, precision=prec)
+        torch.cuda.synchronize()
+        assert torch.equal(ya, yb), prec
