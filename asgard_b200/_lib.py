@@ -28,7 +28,8 @@ EXPORTS = [
     "asgk_mlp_num_params", "asgk_mlp_get_params", "asgk_mlp_set_params",
     "asgk_mlp_forward_backward", "asgk_mlp_train", "asgk_mlp_apply",
     "asgk_mlp_train_residual", "asgk_jacobi_create", "asgk_jacobi_destroy",
-    "asgk_jacobi_apply", "asgk_jacobi_info", "asgk_gmres_euler_jacobi",
+    "asgk_jacobi_apply", "asgk_jacobi_apply_precision", "asgk_jacobi_info",
+    "asgk_gmres_euler_jacobi",
     "asgk_mlp_set_base", "asgk_implicit_advance", "asgk_set_gmres_graphs",
     "asgk_set_gmres_basis", "asgk_set_gmres_node_steps", "asgk_imex_advance",
 ]
@@ -105,6 +106,7 @@ def _load():
         "asgk_jacobi_destroy": ([_vp], None),
         "asgk_mlp_set_base": ([_vp, _vp], _i),
         "asgk_jacobi_apply": ([_vp, _vp, _vp, _vp], _i),
+        "asgk_jacobi_apply_precision": ([_vp, _i, _vp, _vp, _vp], _i),
         "asgk_jacobi_info": ([_vp, C.POINTER(_i), C.POINTER(_d), C.POINTER(_i64)], _i),
         "asgk_gmres_euler_jacobi": ([_vp, _d, _vp, _vp, _i, _i, _d, _i, _i, _vp, C.POINTER(GmresInfo), _vp], _i),
         "asgk_set_gmres_graphs": ([_i], _i),

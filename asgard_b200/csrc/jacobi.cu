@@ -917,6 +917,28 @@ int asgk_jacobi_apply(asgk_jacobi *pc, const double *v, double *z,
   }
 }
 
+int asgk_jacobi_apply_precision(asgk_jacobi *pc, int precision,
+                                const double *v, double *z, asgk_stream stream)
+{
+  try
+  {
+    if (pc == nullptr || v == nullptr || z == nullptr ||
+        (precision != ASGK_FP64 && precision != ASGK_FP32))
+      return ASGK_ERR_INVALID;
+    return asgk::jacobi_apply(pc->jd, precision == ASGK_FP32,
+                              const_cast<double *>(v), z, nullptr, nullptr,
+                              static_cast<cudaStream_t>(stream));
+  }
+  catch (std::bad_alloc const &)
+  {
+    return ASGK_ERR_ALLOC;
+  }
+  catch (...)
+  {
+    return ASGK_ERR_INVALID;
+  }
+}
+
 uint64_t asgk::jacobi_serial(const asgk_jacobi *pc) { return pc ? pc->jd.serial : 0; }
 
 int asgk::jacobi_check_shape(const asgk_jacobi *pc, int rows, int tensor)

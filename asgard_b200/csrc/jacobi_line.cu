@@ -151,65 +151,113 @@ template<> struct vec4_of<double>
   }
 };
 
+// 16-byte asynchronous global->shared copies (no L1 allocation), in
+// groups the waits below count
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem)
+{
+  unsigned const sa = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit()
+{
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+template<int N>
+__device__ __forceinline__ void cp_async_wait()
+{
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+constexpr int kLineTile = 16; // matrix rows per staged tile
+
 // out[r][g][c] = sum_{t < Rr} Mt[t][r] in[t][g][c] for r < Rr (Mt rows of
-// Rp entries, zero beyond Rr), divided by den(r, c) when theta is given.
+// Rp entries, zero beyond Rr, in global memory), divided by den(r, c) when
+// theta is given.  Mt streams through shared memory in tiles of kLineTile
+// rows, double-buffered with cp.async; every thread owns at most two
+// (4-row block, group) items, their sums in registers across the tiles.
 template<typename R, int NC, int NCP>
 __device__ void dense_rows(const R *__restrict__ Mt, int Rr, int Rp, int G,
                            const R *__restrict__ in, R *__restrict__ out,
                            const R *__restrict__ theta, const R *lamc, R shift,
-                           R dt)
+                           R dt, R *qbuf)
 {
   int const rb_n  = Rp / 4;
   int const items = rb_n * G;
-  for (int it = threadIdx.x; it < items; it += blockDim.x)
+  int const tiles = (Rr + kLineTile - 1) / kLineTile;
+  int const chunks_per_row = Rp * int(sizeof(R)) / 16;
+  auto issue = [&](int tile) {
+    int const t0 = tile * kLineTile;
+    int const nr = min(kLineTile, Rr - t0);
+    R *dst       = qbuf + (tile & 1) * kLineTile * Rp;
+    const char *src = reinterpret_cast<const char *>(Mt + int64_t(t0) * Rp);
+    for (int c = threadIdx.x; c < nr * chunks_per_row; c += blockDim.x)
+      cp_async16(reinterpret_cast<char *>(dst) + 16 * c, src + 16 * c);
+    cp_async_commit();
+  };
+  int const it0 = threadIdx.x, it1 = threadIdx.x + blockDim.x;
+  bool const has0 = it0 < items, has1 = it1 < items;
+  int const rb0 = has0 ? it0 % rb_n : 0, g0 = has0 ? it0 / rb_n : 0;
+  int const rb1 = has1 ? it1 % rb_n : 0, g1 = has1 ? it1 / rb_n : 0;
+  R acc0[4][NC], acc1[4][NC];
+#pragma unroll
+  for (int i = 0; i < 4; i++)
+#pragma unroll
+    for (int c = 0; c < NC; c++)
+      acc0[i][c] = acc1[i][c] = R(0);
+  issue(0);
+  for (int tile = 0; tile < tiles; tile++)
   {
-    int const rb = it % rb_n, g = it / rb_n;
-    R acc[4][NC];
-#pragma unroll
-    for (int i = 0; i < 4; i++)
-#pragma unroll
-      for (int c = 0; c < NC; c++)
-        acc[i][c] = R(0);
-    const R *xr = in + g * NCP;
-    const R *mr = Mt + 4 * rb;
-    // eight matrix rows' loads issued together (the pencil matrices come
-    // from L2); Rr is a multiple of 3, the remainder loop takes the rest
-    constexpr int U = 8;
-    int t = 0;
-    for (; t + U <= Rr; t += U)
+    if (tile + 1 < tiles)
     {
-      R q[U][4];
-#pragma unroll
-      for (int u = 0; u < U; u++)
-        vec4_of<R>::load(mr + int64_t(t + u) * Rp, q[u]);
-#pragma unroll
-      for (int u = 0; u < U; u++)
+      issue(tile + 1);
+      cp_async_wait<1>();
+    }
+    else
+      cp_async_wait<0>();
+    __syncthreads();
+    int const t0 = tile * kLineTile;
+    int const nr = min(kLineTile, Rr - t0);
+    const R *qt  = qbuf + (tile & 1) * kLineTile * Rp;
+    for (int tt = 0; tt < nr; tt++)
+    {
+      int const t = t0 + tt;
+      if (has0)
       {
-        R x[NC];
-#pragma unroll
-        for (int c = 0; c < NC; c++)
-          x[c] = xr[int64_t(t + u) * G * NCP + c];
+        R q[4];
 #pragma unroll
         for (int i = 0; i < 4; i++)
-#pragma unroll
-          for (int c = 0; c < NC; c++)
-            acc[i][c] = fma(q[u][i], x[c], acc[i][c]);
-      }
-    }
-    for (; t < Rr; t++)
-    {
-      R q[4];
-      vec4_of<R>::load(mr + int64_t(t) * Rp, q);
-      R x[NC];
-#pragma unroll
-      for (int c = 0; c < NC; c++)
-        x[c] = xr[int64_t(t) * G * NCP + c];
-#pragma unroll
-      for (int i = 0; i < 4; i++)
+          q[i] = qt[tt * Rp + 4 * rb0 + i];
+        const R *xr = in + (int64_t(t) * G + g0) * NCP;
 #pragma unroll
         for (int c = 0; c < NC; c++)
-          acc[i][c] = fma(q[i], x[c], acc[i][c]);
+        {
+          R const x = xr[c];
+#pragma unroll
+          for (int i = 0; i < 4; i++)
+            acc0[i][c] = fma(q[i], x, acc0[i][c]);
+        }
+      }
+      if (has1)
+      {
+        R q[4];
+#pragma unroll
+        for (int i = 0; i < 4; i++)
+          q[i] = qt[tt * Rp + 4 * rb1 + i];
+        const R *xr = in + (int64_t(t) * G + g1) * NCP;
+#pragma unroll
+        for (int c = 0; c < NC; c++)
+        {
+          R const x = xr[c];
+#pragma unroll
+          for (int i = 0; i < 4; i++)
+            acc1[i][c] = fma(q[i], x, acc1[i][c]);
+        }
+      }
     }
+    __syncthreads(); // the buffer is refilled two tiles on
+  }
+  auto finish = [&](int rb, int g, R (&acc)[4][NC]) {
 #pragma unroll
     for (int i = 0; i < 4; i++)
     {
@@ -228,7 +276,11 @@ __device__ void dense_rows(const R *__restrict__ Mt, int Rr, int Rp, int G,
         out[(int64_t(r) * G + g) * NCP + c] = v;
       }
     }
-  }
+  };
+  if (has0)
+    finish(rb0, g0, acc0);
+  if (has1)
+    finish(rb1, g1, acc1);
 }
 
 // One factor M_k^-1 (after B when bj) on the (pencil, group range) units.
@@ -256,8 +308,9 @@ __global__ void __launch_bounds__(kLineThreads)
   int const Rr   = 3 * m;
   int const Rp   = a.tab_rp[tab];
   const int *cells = a.pen_cells + a.pen_off[pen];
-  R *X = reinterpret_cast<R *>(line_smem);
-  R *Y = X + int64_t(Rp) * G * NCP;
+  R *X    = reinterpret_cast<R *>(line_smem);
+  R *Y    = X + int64_t(Rp) * G * NCP;
+  R *qbuf = Y + int64_t(Rp) * G * NCP; // 2 tiles of kLineTile matrix rows
   __shared__ int s_offg[27];
   __shared__ int s_offc[NC];
   __shared__ R s_lamc[NC];
@@ -431,10 +484,10 @@ __global__ void __launch_bounds__(kLineThreads)
   int64_t const to = a.tab_off[tab];
   // rows: Y = Q^T X, divided; then X = Q Y
   dense_rows<R, NC, NCP>(a.Q + to, Rr, Rp, G, X, Y, a.theta + a.tab_th[tab], s_lamc,
-                         a.shift, a.dt);
+                         a.shift, a.dt, qbuf);
   __syncthreads();
   dense_rows<R, NC, NCP>(a.QT + to, Rr, Rp, G, Y, X, nullptr, s_lamc, a.shift,
-                         a.dt);
+                         a.dt, qbuf);
   __syncthreads();
   columns(X, false);
   // scatter
@@ -462,15 +515,16 @@ __global__ void __launch_bounds__(kLineThreads)
 // column's polynomial indices, S_k the cell's own self block along k): W^T
 // as fibre stages over the staged cells, then Bt, Q^T, the division by
 // mu - dt theta and Q in registers per column, then W.
-constexpr int kSmallThreads = 256;
-constexpr int kSmallCells   = 16;
+constexpr int kSmallThreads = 128;
+constexpr int kSmallCells   = 8;
 constexpr int kSmallMaxM    = 8;
+constexpr int kSmallMaxR    = 3 * kSmallMaxM;
 
 template<typename R, int D, int M, int KIDX, int MC>
 __device__ __forceinline__ void small_column(line_args<R> const &a, R *buf,
                                              int slot0, int fb, unsigned dig,
-                                             int stk, int tab, bool bj,
-                                             const R (*s_Sk)[9],
+                                             int stk, const R *Qm, const R *th,
+                                             bool bj, const R (*s_Sk)[9],
                                              const R (*s_lam)[2][3])
 {
   constexpr int TS = ipow3l(D);
@@ -498,28 +552,29 @@ __device__ __forceinline__ void small_column(line_args<R> const &a, R *buf,
         x[3 * i + pk] = mu * x[3 * i + pk] - a.dt * (S[pk] * x0 + S[pk + 3] * x1 + S[pk + 6] * x2);
     }
   }
-  int const Rp  = a.tab_rp[tab];
-  const R *Qm   = a.Q + a.tab_off[tab];
-  const R *th   = a.theta + a.tab_th[tab];
-  R u[RR];
+  // Qm: the pencil matrix's eigenvectors staged in shared memory, [t][r]
+  // with rows of RR entries.  Per eigenmode r: u_r = (Q^T x)_r / (mu - dt
+  // theta_r), then out += Q[:, r] u_r -- register arrays indexed only by
+  // unrolled loops
+  R out[RR];
 #pragma unroll
+  for (int t = 0; t < RR; t++)
+    out[t] = R(0);
+#pragma unroll(MC <= 2 ? RR : 1)
   for (int r = 0; r < RR; r++)
   {
     R acc = R(0);
 #pragma unroll
     for (int t = 0; t < RR; t++)
-      acc = fma(__ldg(Qm + t * Rp + r), x[t], acc);
-    u[r] = acc / (mu - a.dt * __ldg(th + r));
+      acc = fma(Qm[t * RR + r], x[t], acc);
+    R const u = acc / (mu - a.dt * th[r]);
+#pragma unroll
+    for (int t = 0; t < RR; t++)
+      out[t] = fma(Qm[t * RR + r], u, out[t]);
   }
 #pragma unroll
   for (int t = 0; t < RR; t++)
-  {
-    R acc = R(0);
-#pragma unroll
-    for (int r = 0; r < RR; r++)
-      acc = fma(__ldg(Qm + t * Rp + r), u[r], acc);
-    x[t] = acc;
-  }
+    x[t] = out[t];
 #pragma unroll
   for (int i = 0; i < MC; i++)
 #pragma unroll
@@ -528,7 +583,7 @@ __device__ __forceinline__ void small_column(line_args<R> const &a, R *buf,
 }
 
 template<typename R, int D, int M, int KIDX, int MC>
-__global__ void __launch_bounds__(kSmallThreads, 2)
+__global__ void __launch_bounds__(kSmallThreads, 4)
     k_line_small(line_args<R> a, const int4 *__restrict__ batches,
                  const double *in64, const R *__restrict__ inR,
                  double *__restrict__ out64, R *__restrict__ outR, int bj,
@@ -549,6 +604,8 @@ __global__ void __launch_bounds__(kSmallThreads, 2)
   __shared__ short s_fbk[NF];
   __shared__ short s_fbo[2][NF];
   __shared__ unsigned char s_dig[NF];
+  __shared__ R s_Q[kSmallMaxR * kSmallMaxR];
+  __shared__ R s_th[kSmallMaxR];
   __shared__ R s_P[kSmallCells][2][9];
   __shared__ R s_lam[kSmallCells][2][3];
   __shared__ R s_Sk[kSmallCells][9];
@@ -559,6 +616,17 @@ __global__ void __launch_bounds__(kSmallThreads, 2)
   if (tid < nc)
     s_cell[tid] = a.pen_cells[a.pen_off[pen0 + tid / m] + tid % m];
   int const stk = ipow3l(D - 1 - a.k);
+  {
+    // the batch's pencil matrix (every pencil of a batch has the same one)
+    constexpr int RR = 3 * MC;
+    int const tab    = a.pen_tab[pen0];
+    int const Rp     = a.tab_rp[tab];
+    const R *Qg      = a.Q + a.tab_off[tab];
+    for (int e = tid; e < RR * RR; e += blockDim.x)
+      s_Q[e] = Qg[(e / RR) * Rp + e % RR];
+    if (tid < RR)
+      s_th[tid] = a.theta[a.tab_th[tab] + tid];
+  }
   for (int fi = tid; fi < NF; fi += blockDim.x)
   {
     int const fb = (fi / stk) * 3 * stk + fi % stk;
@@ -638,12 +706,11 @@ __global__ void __launch_bounds__(kSmallThreads, 2)
   };
   other_stages(true);
   // the pencil solves, one column (fibre along k) per item
-  int const tab = a.pen_tab[pen0];
   for (int it = tid; it < npen * NF; it += blockDim.x)
   {
     int const pi = it / NF, fi = it - pi * NF;
-    small_column<R, D, M, KIDX, MC>(a, buf, pi * MC, s_fbk[fi], s_dig[fi], stk, tab,
-                                    bj, s_Sk, s_lam);
+    small_column<R, D, M, KIDX, MC>(a, buf, pi * MC, s_fbk[fi], s_dig[fi], stk, s_Q,
+                                    s_th, bj, s_Sk, s_lam);
   }
   __syncthreads();
   other_stages(false);
@@ -675,6 +742,7 @@ struct line_factor
   int k = 0;
   int nunits = 0;   // (pencil, group range) units of the larger pencils
   int max_rows = 0; // largest Rp * G of its units (shared memory)
+  int max_rp   = 0; // largest padded pencil size (matrix tiles)
   int nbatches = 0; // batches of pencils of 1, 2, 4 or 8 cells
   int bfirst[4] = {0, 0, 0, 0}, bcount[4] = {0, 0, 0, 0}; // per size 1, 2, 4, 8
   int4 *units = nullptr, *batches = nullptr;
@@ -921,7 +989,10 @@ int line_build(plan_data const &p, double dt, line_data **out, int64_t &bytes)
     for (size_t pe = 0; pe < pen_m.size(); pe++)
       if (!small(pen_m[pe]))
         rpmax = std::max(rpmax, trp[pen_tab[pe]]);
-    int const budget = std::max(256, rpmax);
+    // a unit's (4-row block, group) items: at most two per thread; its
+    // rows x groups bound its shared memory
+    int const budget = std::max(rpmax, 4 * kLineThreads);
+    int max_rp       = 0;
     std::vector<int4> units, batches;
     int max_rows = 0;
     for (size_t pe = 0; pe < pen_m.size();)
@@ -940,6 +1011,7 @@ int line_build(plan_data const &p, double dt, line_data **out, int64_t &bytes)
       }
       int const Rp = trp[pen_tab[pe]];
       int const G  = std::max(1, std::min(std::min(ng, 27), budget / Rp));
+      max_rp       = std::max(max_rp, Rp);
       for (int g0 = 0; g0 < ng; g0 += G)
       {
         int const gc = std::min(G, ng - g0);
@@ -952,6 +1024,7 @@ int line_build(plan_data const &p, double dt, line_data **out, int64_t &bytes)
     fac->k        = k;
     fac->nunits   = int(units.size());
     fac->max_rows = max_rows;
+    fac->max_rp   = max_rp;
     fac->nbatches = int(batches.size());
     for (size_t b = 0; b < batches.size(); b++)
     {
@@ -1035,7 +1108,8 @@ int launch_factor(line_data const &ld, line_factor const &f, const double *in64,
     return rc;
   if (f.nunits > 0)
   {
-    size_t const shm = 2 * sizeof(R) * size_t(f.max_rows) * NCP;
+    size_t const shm = sizeof(R) * (2 * size_t(f.max_rows) * NCP +
+                                    2 * size_t(kLineTile) * f.max_rp);
     auto kern        = k_line_factor<R, D, M, KIDX>;
     ASGK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    int(shm)));

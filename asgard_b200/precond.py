@@ -69,11 +69,17 @@ class JacobiPreconditioner:
         check(lib.asgk_jacobi_info(self._h, None, None, C.byref(b)))
         return b.value
 
-    def apply(self, v, z, stream=None):
-        """z = M v on CUDA float64 tensors."""
-        from .kronmult import _ptr, _stream
-        check(lib.asgk_jacobi_apply(self._h, _ptr(v), _ptr(z), _stream(stream)),
-              "jacobi_apply")
+    def apply(self, v, z, stream=None, precision="fp64"):
+        """z = M v on CUDA float64 tensors; precision "fp32" applies it in
+        the arithmetic of the FP32 inner solves."""
+        from .kronmult import _precision, _ptr, _stream
+        if precision == "fp64":
+            check(lib.asgk_jacobi_apply(self._h, _ptr(v), _ptr(z), _stream(stream)),
+                  "jacobi_apply")
+        else:
+            check(lib.asgk_jacobi_apply_precision(self._h, _precision(precision), _ptr(v),
+                                                  _ptr(z), _stream(stream)),
+                  "jacobi_apply")
         return z
 
 

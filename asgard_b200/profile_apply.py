@@ -2,6 +2,7 @@
 
     python -m asgard_b200.profile_apply --d 4 --level 7 --terms 4 \
         --precision fp64 --reps 3 [--warmup 1] [--mode global|dense]
+        [--jacobi point|block|kron|line]
 
 Builds the operator (advection/diffusion factors unless --kind random), runs
 --warmup untimed applies of the fused backward-Euler operator
@@ -32,6 +33,9 @@ def main():
     ap.add_argument("--device-build", action="store_true",
                     help="connected pairs found on the GPU (from_grid) instead of "
                          "by the host builder; mode pairs only")
+    ap.add_argument("--jacobi", default=None, choices=["point", "block", "kron", "line"],
+                    help="time the Jacobi preconditioner of that kind (built on the "
+                         "--mode plan, dt 5e-4 at d >= 6 else 1e-3) instead of the operator")
     ap.add_argument("--mode", default="pairs", choices=["pairs", "global", "dense"],
                     help="connected-pair kronmult, the global Kronecker form, "
                          "or the dense form (every cell pair)")
@@ -56,6 +60,28 @@ def main():
     g = torch.Generator(device="cuda").manual_seed(0)
     x = torch.rand(op.N, dtype=torch.float64, device="cuda", generator=g) * 2 - 1
     y = torch.zeros_like(x)
+    if args.jacobi:
+        t0 = time.perf_counter()
+        pc = ab.JacobiPreconditioner(mat, 5e-4 if args.d >= 6 else 1e-3, kind=args.jacobi)
+        torch.cuda.synchronize()
+        t_pc = time.perf_counter() - t0
+        for _ in range(args.warmup):
+            pc.apply(x, y, precision=args.precision)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.reps):
+            pc.apply(x, y, precision=args.precision)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / args.reps
+        print(json.dumps({"d": args.d, "level": args.level, "terms": args.terms,
+                          "jacobi": args.jacobi, "precision": args.precision,
+                          "dofs": op.N, "ms_per_apply": ms, "setup_s": t_pc,
+                          "algorithmic_GBps": 16 * op.N / ms / 1e6,
+                          "device_bytes": pc.device_bytes()}))
+        return
     for _ in range(args.warmup):
         mat.apply_euler(1e-3, 1.0, x, 0.0, y, precision=args.precision)
     torch.cuda.synchronize()

@@ -336,6 +336,13 @@ void asgk_jacobi_destroy(asgk_jacobi *pc);
 /* z = M v on device vectors of the plan's size (z != v). */
 int asgk_jacobi_apply(asgk_jacobi *pc, const double *v, double *z,
                       asgk_stream stream);
+/* z = M v as the solves of the given precision apply it: ASGK_FP64 as
+ * asgk_jacobi_apply, ASGK_FP32 in the FP32 arithmetic (FP16 block inverses
+ * for ASGK_JACOBI_BLOCK) of the FP32 inner solves of asgk_gmres_euler_jacobi.
+ * No counterpart in the reference (its diagonal preconditioner has one
+ * precision). */
+int asgk_jacobi_apply_precision(asgk_jacobi *pc, int precision,
+                                const double *v, double *z, asgk_stream stream);
 int asgk_jacobi_info(asgk_jacobi *pc, int *kind, double *dt,
                      int64_t *device_bytes);
 /* asgk_gmres_euler with a Jacobi preconditioner applied on the right
