@@ -129,6 +129,8 @@ struct line_args
   int k, kidx;        // this factor's dimension and its index among the line dims
   int line[3];        // line dimensions (increasing)
   int nonline[6];     // the other dimensions (increasing)
+  int st_k;           // tensor stride of dimension k, 3^(D-1-k)
+  int st_line[3];     // tensor strides of the line dimensions
   R shift, dt;
 };
 
@@ -582,13 +584,18 @@ __device__ __forceinline__ void small_column(line_args<R> const &a, R *buf,
       buf[(slot0 + i) * TS + fb + pk * stk] = x[3 * i + pk];
 }
 
-template<typename R, int D, int M, int KIDX, int MC>
+// One launch per factor for every batch of small pencils.  A batch record
+// holds (pencils, cells per pencil, matrix offset, eigenvalue offset); its
+// cells' records (cell, offsets of the cell's self-block entries in the
+// line dimensions) follow in batch order, so the staging needs no chain of
+// dependent lookups.
+template<typename R, int D, int M, int KIDX>
 __global__ void __launch_bounds__(kSmallThreads, 4)
     k_line_small(line_args<R> a, const int4 *__restrict__ batches,
-                 const double *in64, const R *__restrict__ inR,
-                 double *__restrict__ out64, R *__restrict__ outR, int bj,
-                 const double *scale_state, double *vscale, float *vcopy,
-                 const double *gate)
+                 const int4 *__restrict__ bcells, const double *in64,
+                 const R *__restrict__ inR, double *__restrict__ out64,
+                 R *__restrict__ outR, int bj, const double *scale_state,
+                 double *vscale, float *vcopy, const double *gate)
 {
   if (gate_closed(gate))
     return;
@@ -610,23 +617,35 @@ __global__ void __launch_bounds__(kSmallThreads, 4)
   __shared__ R s_lam[kSmallCells][2][3];
   __shared__ R s_Sk[kSmallCells][9];
   int4 const bt  = batches[blockIdx.x];
-  int const pen0 = bt.x, npen = bt.y, m = MC;
-  int const nc   = npen * m;
+  int const npen = bt.x, MC = bt.y;
+  int const nc   = npen * MC;
+  int const RR   = 3 * MC, Rp = (RR + 3) / 4 * 4;
   int const tid  = threadIdx.x;
+  int const stk  = a.st_k;
   if (tid < nc)
-    s_cell[tid] = a.pen_cells[a.pen_off[pen0 + tid / m] + tid % m];
-  int const stk = ipow3l(D - 1 - a.k);
   {
-    // the batch's pencil matrix (every pencil of a batch has the same one)
-    constexpr int RR = 3 * MC;
-    int const tab    = a.pen_tab[pen0];
-    int const Rp     = a.tab_rp[tab];
-    const R *Qg      = a.Q + a.tab_off[tab];
-    for (int e = tid; e < RR * RR; e += blockDim.x)
-      s_Q[e] = Qg[(e / RR) * Rp + e % RR];
-    if (tid < RR)
-      s_th[tid] = a.theta[a.tab_th[tab] + tid];
+    int4 const cr = bcells[blockIdx.x * kSmallCells + tid];
+    s_cell[tid]   = cr.x;
+    int const so[3] = {cr.y, cr.z, cr.w};
+    // the other line dimensions' eigenvectors and eigenvalues (constant over
+    // a pencil) and the cell's own self block along k
+    for (int qq = 0; qq < M - 1; qq++)
+    {
+      const R *sf = a.self + so[qq < KIDX ? qq : qq + 1];
+      for (int e = 0; e < 9; e++)
+        s_P[tid][qq][e] = sf[e];
+      for (int e = 0; e < 3; e++)
+        s_lam[tid][qq][e] = sf[9 + e];
+    }
+    const R *sk = a.self + so[KIDX] + 12;
+    for (int e = 0; e < 9; e++)
+      s_Sk[tid][e] = sk[e];
   }
+  // the batch's pencil matrix (every pencil of a batch has the same one)
+  for (int e = tid; e < RR * RR; e += blockDim.x)
+    s_Q[e] = a.Q[bt.z + (e / RR) * Rp + e % RR];
+  if (tid < RR)
+    s_th[tid] = a.theta[bt.w + tid];
   for (int fi = tid; fi < NF; fi += blockDim.x)
   {
     int const fb = (fi / stk) * 3 * stk + fi % stk;
@@ -634,35 +653,13 @@ __global__ void __launch_bounds__(kSmallThreads, 4)
     unsigned dg  = 0;
     for (int qq = 0; qq < M - 1; qq++)
     {
-      int const q  = qq < KIDX ? qq : qq + 1;
-      int const sj = ipow3l(D - 1 - a.line[q]);
+      int const sj  = a.st_line[qq < KIDX ? qq : qq + 1];
       s_fbo[qq][fi] = short((fi / sj) * 3 * sj + fi % sj);
       dg |= unsigned((fb / sj) % 3) << (2 * qq);
     }
     s_dig[fi] = (unsigned char)dg;
   }
   __syncthreads();
-  // other line dimensions' eigen data (constant over a pencil) and each
-  // cell's own self block along k
-  for (int e = tid; e < nc * 2 * 12; e += blockDim.x)
-  {
-    int const slot = e / 24, qq = (e / 12) % 2, ee = e % 12;
-    if (qq >= M - 1)
-      continue;
-    int const q = qq < KIDX ? qq : qq + 1; // qq-th line index other than KIDX
-    const R *sf = a.self + (int64_t(q) * a.r1 +
-                            a.c1[int64_t(s_cell[slot]) * D + a.line[q]]) * kSelfEntry;
-    if (ee < 9)
-      s_P[slot][qq][ee] = sf[ee];
-    else
-      s_lam[slot][qq][ee - 9] = sf[ee];
-  }
-  for (int e = tid; e < nc * 9; e += blockDim.x)
-  {
-    int const slot = e / 9;
-    s_Sk[slot][e % 9] = a.self[(int64_t(KIDX) * a.r1 +
-                                a.c1[int64_t(s_cell[slot]) * D + a.k]) * kSelfEntry + 12 + e % 9];
-  }
   // stage the cells
   double const f = scale_state ? scale_state[1] : 1.0;
   for (int e = tid; e < nc * TS; e += blockDim.x)
@@ -688,8 +685,7 @@ __global__ void __launch_bounds__(kSmallThreads, 4)
   auto other_stages = [&](bool forward) {
     for (int qq = 0; qq < M - 1; qq++)
     {
-      int const q  = qq < KIDX ? qq : qq + 1;
-      int const sj = ipow3l(D - 1 - a.line[q]);
+      int const sj = a.st_line[qq < KIDX ? qq : qq + 1];
       for (int it = tid; it < nc * NF; it += blockDim.x)
       {
         int const slot = it / NF, fi = it - slot * NF;
@@ -709,8 +705,13 @@ __global__ void __launch_bounds__(kSmallThreads, 4)
   for (int it = tid; it < npen * NF; it += blockDim.x)
   {
     int const pi = it / NF, fi = it - pi * NF;
-    small_column<R, D, M, KIDX, MC>(a, buf, pi * MC, s_fbk[fi], s_dig[fi], stk, s_Q,
-                                    s_th, bj, s_Sk, s_lam);
+    switch (MC)
+    {
+    case 1: small_column<R, D, M, KIDX, 1>(a, buf, pi, s_fbk[fi], s_dig[fi], stk, s_Q, s_th, bj, s_Sk, s_lam); break;
+    case 2: small_column<R, D, M, KIDX, 2>(a, buf, pi * 2, s_fbk[fi], s_dig[fi], stk, s_Q, s_th, bj, s_Sk, s_lam); break;
+    case 4: small_column<R, D, M, KIDX, 4>(a, buf, pi * 4, s_fbk[fi], s_dig[fi], stk, s_Q, s_th, bj, s_Sk, s_lam); break;
+    default: small_column<R, D, M, KIDX, 8>(a, buf, pi * 8, s_fbk[fi], s_dig[fi], stk, s_Q, s_th, bj, s_Sk, s_lam); break;
+    }
   }
   __syncthreads();
   other_stages(false);
@@ -744,13 +745,13 @@ struct line_factor
   int max_rows = 0; // largest Rp * G of its units (shared memory)
   int max_rp   = 0; // largest padded pencil size (matrix tiles)
   int nbatches = 0; // batches of pencils of 1, 2, 4 or 8 cells
-  int bfirst[4] = {0, 0, 0, 0}, bcount[4] = {0, 0, 0, 0}; // per size 1, 2, 4, 8
-  int4 *units = nullptr, *batches = nullptr;
+  int4 *units = nullptr, *batches = nullptr, *bcells = nullptr;
   int *pen_off = nullptr, *pen_m = nullptr, *pen_tab = nullptr, *pen_cells = nullptr;
   ~line_factor()
   {
     cudaFree(units);
     cudaFree(batches);
+    cudaFree(bcells);
     cudaFree(pen_off);
     cudaFree(pen_m);
     cudaFree(pen_tab);
@@ -993,7 +994,7 @@ int line_build(plan_data const &p, double dt, line_data **out, int64_t &bytes)
     // rows x groups bound its shared memory
     int const budget = std::max(rpmax, 4 * kLineThreads);
     int max_rp       = 0;
-    std::vector<int4> units, batches;
+    std::vector<int4> units, batches, bcells;
     int max_rows = 0;
     for (size_t pe = 0; pe < pen_m.size();)
     {
@@ -1005,7 +1006,19 @@ int line_build(plan_data const &p, double dt, line_data **out, int64_t &bytes)
         while (e < pen_m.size() && e - pe < size_t(per) && pen_m[e] == m &&
                pen_tab[e] == pen_tab[pe])
           ++e;
-        batches.push_back(make_int4(int(pe), int(e - pe), m, 0));
+        int const tb = pen_tab[pe];
+        batches.push_back(make_int4(int(e - pe), m, toff[tb], tth[tb]));
+        for (size_t p2 = pe; p2 < e; p2++)
+          for (int i = 0; i < m; i++)
+          {
+            int const cell = pen_cells[pen_off[p2] + i];
+            int so[3]      = {0, 0, 0};
+            for (int q2 = 0; q2 < M; q2++)
+              so[q2] = (q2 * r1 + c1[size_t(cell) * d + line[q2]]) * kSelfEntry;
+            bcells.push_back(make_int4(cell, so[0], so[1], so[2]));
+          }
+        while (bcells.size() % kSmallCells)
+          bcells.push_back(make_int4(0, 0, 0, 0));
         pe = e;
         continue;
       }
@@ -1026,15 +1039,9 @@ int line_build(plan_data const &p, double dt, line_data **out, int64_t &bytes)
     fac->max_rows = max_rows;
     fac->max_rp   = max_rp;
     fac->nbatches = int(batches.size());
-    for (size_t b = 0; b < batches.size(); b++)
-    {
-      int const sz = batches[b].z == 1 ? 0 : batches[b].z == 2 ? 1 : batches[b].z == 4 ? 2 : 3;
-      if (fac->bcount[sz] == 0)
-        fac->bfirst[sz] = int(b);
-      ++fac->bcount[sz];
-    }
     int rc;
     if ((rc = upload(&fac->units, units, bytes)) || (rc = upload(&fac->batches, batches, bytes)) ||
+        (rc = upload(&fac->bcells, bcells, bytes)) ||
         (rc = upload(&fac->pen_off, pen_off, bytes)) ||
         (rc = upload(&fac->pen_m, pen_m, bytes)) || (rc = upload(&fac->pen_tab, pen_tab, bytes)) ||
         (rc = upload(&fac->pen_cells, pen_cells, bytes)))
@@ -1084,28 +1091,19 @@ int launch_factor(line_data const &ld, line_factor const &f, const double *in64,
   for (int i = 0; i < 6; i++)
     a.nonline[i] = ld.nonline[i];
   a.shift = R(ld.shift), a.dt = R(ld.dt);
-  auto small = [&](auto mc, int sz) -> int {
-    constexpr int MC = decltype(mc)::value;
-    if (f.bcount[sz] == 0)
-      return ASGK_OK;
+  a.st_k = ipow3l(D - 1 - f.k);
+  for (int q = 0; q < 3; q++)
+    a.st_line[q] = q < M ? ipow3l(D - 1 - ld.line[q]) : 0;
+  if (f.nbatches > 0)
+  {
     size_t const shm = sizeof(R) * size_t(kSmallCells) * ipow3l(D);
-    auto kern        = k_line_small<R, D, M, KIDX, MC>;
+    auto kern        = k_line_small<R, D, M, KIDX>;
     ASGK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    int(shm)));
-    kern<<<f.bcount[sz], kSmallThreads, shm, s>>>(a, f.batches + f.bfirst[sz], in64, inR,
-                                                  out64, outR, bj ? 1 : 0, sc, vscale,
-                                                  vc, g_gate);
+    kern<<<f.nbatches, kSmallThreads, shm, s>>>(a, f.batches, f.bcells, in64, inR, out64,
+                                                outR, bj ? 1 : 0, sc, vscale, vc, g_gate);
     ASGK_LAUNCHED();
-    return ASGK_OK;
-  };
-  if (int rc = small(std::integral_constant<int, 8>{}, 3))
-    return rc;
-  if (int rc = small(std::integral_constant<int, 4>{}, 2))
-    return rc;
-  if (int rc = small(std::integral_constant<int, 2>{}, 1))
-    return rc;
-  if (int rc = small(std::integral_constant<int, 1>{}, 0))
-    return rc;
+  }
   if (f.nunits > 0)
   {
     size_t const shm = sizeof(R) * (2 * size_t(f.max_rows) * NCP +
