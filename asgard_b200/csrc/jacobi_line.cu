@@ -783,8 +783,22 @@ struct line_data
   line_tables<float> t32;
   std::vector<std::unique_ptr<line_factor>> factors;
   double *work = nullptr; // two intermediate vectors (rows * ts doubles each)
+  // a factor's small-pencil and larger-pencil launches touch disjoint cells:
+  // the larger ones run on a second stream, forked from and joined back to
+  // the caller's (parallel branches when the caller records a graph)
+  cudaStream_t side = nullptr;
+  cudaEvent_t fork[3] = {nullptr, nullptr, nullptr}, join[3] = {nullptr, nullptr, nullptr};
   ~line_data()
   {
+    for (int q = 0; q < 3; q++)
+    {
+      if (fork[q])
+        cudaEventDestroy(fork[q]);
+      if (join[q])
+        cudaEventDestroy(join[q]);
+    }
+    if (side)
+      cudaStreamDestroy(side);
     cudaFree(c1);
     cudaFree(tab_off);
     cudaFree(tab_th);
@@ -1060,6 +1074,12 @@ int line_build(plan_data const &p, double dt, line_data **out, int64_t &bytes)
     return rc;
   size_t const wb = sizeof(double) * 2 * size_t(p.rows) * p.tensor;
   ASGK_CUDA(cudaMalloc(&ld->work, wb));
+  ASGK_CUDA(cudaStreamCreateWithFlags(&ld->side, cudaStreamNonBlocking));
+  for (int q = 0; q < M; q++)
+  {
+    ASGK_CUDA(cudaEventCreateWithFlags(&ld->fork[q], cudaEventDisableTiming));
+    ASGK_CUDA(cudaEventCreateWithFlags(&ld->join[q], cudaEventDisableTiming));
+  }
   bytes += int64_t(wb);
   *out = ld.release();
   return ASGK_OK;
@@ -1094,6 +1114,25 @@ int launch_factor(line_data const &ld, line_factor const &f, const double *in64,
   a.st_k = ipow3l(D - 1 - f.k);
   for (int q = 0; q < 3; q++)
     a.st_line[q] = q < M ? ipow3l(D - 1 - ld.line[q]) : 0;
+  bool const both = f.nbatches > 0 && f.nunits > 0;
+  cudaStream_t sb = s;
+  if (both)
+  {
+    sb = ld.side;
+    ASGK_CUDA(cudaEventRecord(ld.fork[KIDX], s));
+    ASGK_CUDA(cudaStreamWaitEvent(sb, ld.fork[KIDX], 0));
+  }
+  if (f.nunits > 0)
+  {
+    size_t const shm = sizeof(R) * (2 * size_t(f.max_rows) * NCP +
+                                    2 * size_t(kLineTile) * f.max_rp);
+    auto kern        = k_line_factor<R, D, M, KIDX>;
+    ASGK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   int(shm)));
+    kern<<<f.nunits, kLineThreads, shm, sb>>>(a, in64, inR, out64, outR, bj ? 1 : 0,
+                                              sc, vscale, vc, g_gate);
+    ASGK_LAUNCHED();
+  }
   if (f.nbatches > 0)
   {
     size_t const shm = sizeof(R) * size_t(kSmallCells) * ipow3l(D);
@@ -1104,16 +1143,10 @@ int launch_factor(line_data const &ld, line_factor const &f, const double *in64,
                                                 outR, bj ? 1 : 0, sc, vscale, vc, g_gate);
     ASGK_LAUNCHED();
   }
-  if (f.nunits > 0)
+  if (both)
   {
-    size_t const shm = sizeof(R) * (2 * size_t(f.max_rows) * NCP +
-                                    2 * size_t(kLineTile) * f.max_rp);
-    auto kern        = k_line_factor<R, D, M, KIDX>;
-    ASGK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   int(shm)));
-    kern<<<f.nunits, kLineThreads, shm, s>>>(a, in64, inR, out64, outR, bj ? 1 : 0,
-                                             sc, vscale, vc, g_gate);
-    ASGK_LAUNCHED();
+    ASGK_CUDA(cudaEventRecord(ld.join[KIDX], sb));
+    ASGK_CUDA(cudaStreamWaitEvent(s, ld.join[KIDX], 0));
   }
   return ASGK_OK;
 }
