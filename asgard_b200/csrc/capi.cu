@@ -1753,11 +1753,11 @@ int asgk_plan_create_global(asgk_plan **plan, int d, int n, int level,
       }
     }
     // d >= 5: per-cell dimension segments (the entries of a cell come in
-    // dimension order) and the cells by decreasing longest segment
+    // dimension order) and two cell orders
     if (d >= 5)
     {
       std::vector<int> seg(size_t(num_cells) * (d + 1));
-      std::vector<int> longest(num_cells, 0);
+      std::vector<int> longest(num_cells, 0), total(num_cells, 0);
       for (int r = 0; r < num_cells; r++)
       {
         int64_t e = gptr[r];
@@ -1770,13 +1770,19 @@ int asgk_plan_create_global(asgk_plan **plan, int d, int n, int level,
         for (int k = 0; k < d; k++)
           longest[r] = std::max(longest[r], seg[size_t(r) * (d + 1) + k + 1] -
                                                 seg[size_t(r) * (d + 1) + k]);
+        total[r] = seg[size_t(r) * (d + 1) + d];
       }
-      std::vector<int> corder(num_cells);
-      std::iota(corder.begin(), corder.end(), 0);
-      std::stable_sort(corder.begin(), corder.end(),
+      // the FP32 kernel's warps take one dimension each (longest segment
+      // first), the FP64 kernel's equal ranges (most entries first)
+      std::vector<int> corder(2 * size_t(num_cells));
+      std::iota(corder.begin(), corder.begin() + num_cells, 0);
+      std::iota(corder.begin() + num_cells, corder.end(), 0);
+      std::stable_sort(corder.begin(), corder.begin() + num_cells,
                        [&](int a, int b) { return longest[a] > longest[b]; });
+      std::stable_sort(corder.begin() + num_cells, corder.end(),
+                       [&](int a, int b) { return total[a] > total[b]; });
       if ((rc = dev_alloc(&p.gseg, int64_t(seg.size()), bytes)) ||
-          (rc = dev_alloc(&p.gcell_order, num_cells, bytes)) ||
+          (rc = dev_alloc(&p.gcell_order, 2 * int64_t(num_cells), bytes)) ||
           (rc = dev_alloc(&p.gx32, int64_t(num_cells) * p.tensor, bytes)) ||
           (rc = up(p.gseg, seg.data(), sizeof(int) * seg.size())) ||
           (rc = up(p.gcell_order, corder.data(), sizeof(int) * corder.size())))

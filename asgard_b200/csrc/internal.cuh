@@ -127,12 +127,12 @@ struct plan_data
   int *row_slice0 = nullptr, *row_nslice = nullptr; // [rows]
   double *gscratch = nullptr;  // [gslices * n^d] partial tensors
   unsigned *gtickets = nullptr; // [rows], zero between launches
-  // d >= 5: one CTA per cell, one warp per dimension (kron_global_cell):
-  // each cell's segment of its neighbour list per dimension, the cells in
-  // order of decreasing longest segment, and the FP32 copy of x the FP32
-  // apply reads its neighbour tensors from (L2-resident)
+  // d >= 5: one CTA per cell, its warps sharing the cell's neighbour list
+  // (kron_global_cell): each cell's segment of the list per dimension, the
+  // cell orders the FP32 and FP64 kernels take, and the FP32 copy of x
+  // the FP32 apply reads its neighbour tensors from (L2-resident)
   int *gseg = nullptr;         // [rows][d + 1] offsets within the cell's list
-  int *gcell_order = nullptr;  // [rows]
+  int *gcell_order = nullptr;  // [2][rows]: by longest segment, by entries
   float *gx32 = nullptr;       // [rows * n^d]
   // terms acting in several dimensions (the reference's upper/lower
   // permutations): chains of masked 1D passes over per-dimension neighbour

@@ -237,7 +237,7 @@ __global__ void __launch_bounds__(NW * 32)
     tickets[row] = 0u; // ready for the next launch
 }
 
-// d >= 5: one CTA per output cell, warp k takes the cell's neighbours
+// d >= 5, FP32: one CTA per output cell, warp k takes the cell's neighbours
 // along dimension k (no barrier until the end): lane f owns fibres f,
 // f + 32, ... of the 3^d tensor along k, loads each neighbour's fibre (from
 // the FP32 copy of x in the FP32 apply: 47 MB at d=6, level 7, held in L2
@@ -246,7 +246,7 @@ __global__ void __launch_bounds__(NW * 32)
 // dimension order with the Euler and beta terms (FP64 x and y).
 template<int D, typename TC, typename TX>
 __global__ void __launch_bounds__(D * 32)
-    kron_global_cell(const int *__restrict__ order,
+    kron_global_cell_dims(const int *__restrict__ order,
                      const int64_t *__restrict__ gptr,
                      const int *__restrict__ gseg, const int *__restrict__ gcol,
                      const int *__restrict__ gkb, const TC *__restrict__ B,
@@ -333,6 +333,129 @@ __global__ void __launch_bounds__(D * 32)
 #pragma unroll
     for (int kk = 0; kk < D; kk++)
       s += rows[kk * TS + i];
+    double v = alpha * static_cast<double>(s) + ex * x[base + i];
+    if (beta != 0.0)
+      v += beta * y[base + i];
+    y[base + i] = v;
+  }
+}
+
+// d >= 5, FP64: one CTA per output cell, D warps sharing the cell's
+// neighbour list (in dimension order) in equal contiguous ranges, so no
+// warp waits on another's long dimension (measured at d=6, level 7: 0.64 ->
+// 0.46 ms; the FP32 apply, which reads from L2, is faster with a warp per
+// dimension).  Within a dimension k lane f owns fibres f,
+// f + 32, ... of the 3^d tensor along k, loads each neighbour's fibre (from
+// the FP32 copy of x in the FP32 apply: 47 MB at d=6, level 7, held in L2
+// across the re-reads) and accumulates the 3x3 block's product in
+// registers; when its range moves on to the next dimension the warp adds
+// its sums into its own row of shared memory.  The rows are added in warp
+// order with the Euler and beta terms (FP64 x and y): a fixed order, the
+// same result whichever warp finishes first.
+template<int D, typename TC, typename TX>
+__global__ void __launch_bounds__(D * 32)
+    kron_global_cell_ranges(const int *__restrict__ order,
+                     const int64_t *__restrict__ gptr,
+                     const int *__restrict__ gseg, const int *__restrict__ gcol,
+                     const int *__restrict__ gkb, const TC *__restrict__ B,
+                     double alpha, const TX *__restrict__ xs,
+                     const double *__restrict__ x, double beta,
+                     double *__restrict__ y, double ex,
+                     const double *__restrict__ gate)
+{
+  if (gate_closed(gate))
+    return;
+  constexpr int TS  = ipow3g(D);
+  constexpr int NF  = TS / 3;
+  constexpr int FPL = (NF + 31) / 32;
+  constexpr int PAD = padG<TC>::value;
+  __shared__ TC rows[D * TS];
+  int const w    = threadIdx.x >> 5;
+  int const lane = threadIdx.x & 31;
+  int const cell = order[blockIdx.x];
+  int64_t const e0 = gptr[cell];
+  int const E  = gseg[cell * (D + 1) + D];
+  int const ja = int(int64_t(E) * w / D), jb = int(int64_t(E) * (w + 1) / D);
+  int k = 0; // the dimension of the range's first entry
+  while (k < D - 1 && gseg[cell * (D + 1) + k + 1] <= ja)
+    ++k;
+  TC *row = rows + w * TS;
+  for (int i = lane; i < TS; i += 32)
+    row[i] = TC(0);
+  __syncwarp();
+  int j = ja;
+  while (j < jb)
+  {
+    int const send   = min(jb, gseg[cell * (D + 1) + k + 1]);
+    int const stride = dim_stride<D>(k);
+    int fb[FPL];
+    TC acc[FPL][3];
+#pragma unroll
+    for (int m = 0; m < FPL; m++)
+    {
+      int const f = lane + 32 * m;
+      fb[m]       = (f / stride) * 3 * stride + (f % stride);
+      acc[m][0] = acc[m][1] = acc[m][2] = TC(0);
+    }
+    for (; j < send; j++)
+    {
+      int64_t const e = e0 + j;
+      const TC *b  = B + int64_t(__ldg(gkb + e)) * PAD;
+      const TX *xc = xs + int64_t(__ldg(gcol + e)) * TS;
+      TC b0, b1, b2, b3, b4, b5, b6, b7, b8;
+      if constexpr (sizeof(TC) == 4)
+      {
+        const float4 *q = reinterpret_cast<const float4 *>(b);
+        float4 const q0 = __ldg(q), q1 = __ldg(q + 1), q2 = __ldg(q + 2);
+        b0 = q0.x, b1 = q0.y, b2 = q0.z, b3 = q0.w;
+        b4 = q1.x, b5 = q1.y, b6 = q1.z, b7 = q1.w;
+        b8 = q2.x;
+      }
+      else
+      {
+        const double2 *q = reinterpret_cast<const double2 *>(b);
+        double2 const q0 = __ldg(q), q1 = __ldg(q + 1), q2 = __ldg(q + 2);
+        double2 const q3 = __ldg(q + 3), q4 = __ldg(q + 4);
+        b0 = q0.x, b1 = q0.y, b2 = q1.x, b3 = q1.y, b4 = q2.x;
+        b5 = q2.y, b6 = q3.x, b7 = q3.y, b8 = q4.x;
+      }
+      TC v[FPL][3];
+#pragma unroll
+      for (int m = 0; m < FPL; m++)
+        if (lane + 32 * m < NF)
+#pragma unroll
+          for (int p = 0; p < 3; p++)
+            v[m][p] = static_cast<TC>(__ldg(xc + fb[m] + p * stride));
+#pragma unroll
+      for (int m = 0; m < FPL; m++)
+        if (lane + 32 * m < NF)
+        {
+          // column-major block: out_q += sum_p A(q, p) v_p, A(q, p) = b[q + 3p]
+          acc[m][0] = fma(b6, v[m][2], fma(b3, v[m][1], fma(b0, v[m][0], acc[m][0])));
+          acc[m][1] = fma(b7, v[m][2], fma(b4, v[m][1], fma(b1, v[m][0], acc[m][1])));
+          acc[m][2] = fma(b8, v[m][2], fma(b5, v[m][1], fma(b2, v[m][0], acc[m][2])));
+        }
+    }
+    // lanes own distinct fibres of dimension k: no two lanes touch an entry
+#pragma unroll
+    for (int m = 0; m < FPL; m++)
+      if (lane + 32 * m < NF)
+      {
+        row[fb[m]] += acc[m][0];
+        row[fb[m] + stride] += acc[m][1];
+        row[fb[m] + 2 * stride] += acc[m][2];
+      }
+    __syncwarp(); // before the next dimension's fibres touch these entries
+    ++k;
+  }
+  __syncthreads();
+  int64_t const base = int64_t(cell) * TS;
+  for (int i = threadIdx.x; i < TS; i += D * 32)
+  {
+    TC s = TC(0);
+#pragma unroll
+    for (int ww = 0; ww < D; ww++)
+      s += rows[ww * TS + i];
     double v = alpha * static_cast<double>(s) + ex * x[base + i];
     if (beta != 0.0)
       v += beta * y[base + i];
@@ -504,14 +627,14 @@ int launch_global_d(plan_data const &p, double alpha, const double *x,
         int const blocks = int(std::min<int64_t>((n / 2 + 255) / 256, 4 * 148));
         k_copy_to_f32<<<blocks, 256, 0, s>>>(n, x, p.gx32, pairs, g_gate);
         ASGK_LAUNCHED();
-        kron_global_cell<D, TC, float><<<p.rows, D * 32, 0, s>>>(
+        kron_global_cell_dims<D, TC, float><<<p.rows, D * 32, 0, s>>>(
             p.gcell_order, p.gptr, p.gseg, p.gcol, p.gkb, B, alpha, p.gx32, x, beta, y,
             ex, g_gate);
       }
       else
-        kron_global_cell<D, TC, double><<<p.rows, D * 32, 0, s>>>(
-            p.gcell_order, p.gptr, p.gseg, p.gcol, p.gkb, B, alpha, x, x, beta, y, ex,
-            g_gate);
+        kron_global_cell_ranges<D, TC, double><<<p.rows, D * 32, 0, s>>>(
+            p.gcell_order + p.rows, p.gptr, p.gseg, p.gcol, p.gkb, B, alpha, x, x, beta,
+            y, ex, g_gate);
       ASGK_LAUNCHED();
       if (p.gchains > 0)
         return launch_chains<D, TC>(p, alpha, x, y, s);
