@@ -62,6 +62,7 @@ TOL = 1e-10
 KERNEL_TRAFFIC = {
     ("pairs", "d4"): 254_243_328 + 4_232_704,
     ("global", "d4"): 3_930_368,
+    ("global", "d6"): 192_652_288 + 68_899_584,
 }
 
 
@@ -620,8 +621,12 @@ def rooflines(ab, op, mat, gmat, method, dt, workload, xs):
     nbytes = (16 * N + 8 * gmat.num_pairs() + 8 * (op.rows + 1)
               + 48 * len(op.vA) // (9 * op.terms))
     hbm, src = _measured_hbm_gbs()
+    gk = ("kron_global_cell_dims" if method["precision"] == "fp32"
+          else "kron_global_cell_ranges") if d >= 5 else "kron_global_rows"
     return {"bound": "hbm",
-            "kernel": f"kron_global_rows<d={d}, {method['precision']}>",
+            "kernel": f"{gk}<d={d}, {method['precision']}>"
+                      + (" (+ FP32 copy of x)" if d >= 5 and method["precision"] == "fp32"
+                         else ""),
             "achieved": nbytes / tg / 1e9, "peak": hbm, "peak_source": src,
             "unit": "GB/s", "frac": nbytes / tg / 1e9 / hbm,
             "traffic": KERNEL_TRAFFIC.get(("global", workload)),
