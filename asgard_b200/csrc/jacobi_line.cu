@@ -44,6 +44,7 @@ namespace asgk
 namespace
 {
 constexpr int kLineThreads = 128;
+constexpr int kGatherLoads = 8; // loads in flight per thread while gathering
 constexpr int kSelfEntry   = 21; // P (3x3 col-major), lambda (3), S (3x3 col-major)
 
 constexpr int ipow3l(int k) { return k <= 0 ? 1 : 3 * ipow3l(k - 1); }
@@ -173,6 +174,41 @@ __device__ __forceinline__ void cp_async_wait()
 
 constexpr int kLineTile = 16; // matrix rows per staged tile
 
+// shared-memory rows read in 16-byte pieces (rows start 16-byte aligned)
+__device__ __forceinline__ void smem_row4(const float *p, float (&q)[4])
+{
+  float4 const v = *reinterpret_cast<const float4 *>(p);
+  q[0] = v.x, q[1] = v.y, q[2] = v.z, q[3] = v.w;
+}
+__device__ __forceinline__ void smem_row4(const double *p, double (&q)[4])
+{
+  double2 const a = reinterpret_cast<const double2 *>(p)[0];
+  double2 const b = reinterpret_cast<const double2 *>(p)[1];
+  q[0] = a.x, q[1] = a.y, q[2] = b.x, q[3] = b.y;
+}
+template<typename R, int N>
+__device__ __forceinline__ void smem_row(const R *p, R (&q)[N])
+{
+  if constexpr (N % 4 == 0)
+  {
+#pragma unroll
+    for (int i = 0; i < N / 4; i++)
+    {
+      R t[4];
+      smem_row4(p + 4 * i, t);
+#pragma unroll
+      for (int e = 0; e < 4; e++)
+        q[4 * i + e] = t[e];
+    }
+  }
+  else
+  {
+#pragma unroll
+    for (int i = 0; i < N; i++)
+      q[i] = p[i];
+  }
+}
+
 // out[r][g][c] = sum_{t < Rr} Mt[t][r] in[t][g][c] for r < Rr (Mt rows of
 // Rp entries, zero beyond Rr, in global memory), divided by den(r, c) when
 // theta is given.  Mt streams through shared memory in tiles of kLineTile
@@ -226,35 +262,25 @@ __device__ void dense_rows(const R *__restrict__ Mt, int Rr, int Rp, int G,
       int const t = t0 + tt;
       if (has0)
       {
-        R q[4];
-#pragma unroll
-        for (int i = 0; i < 4; i++)
-          q[i] = qt[tt * Rp + 4 * rb0 + i];
-        const R *xr = in + (int64_t(t) * G + g0) * NCP;
+        R q[4], xv[NCP];
+        smem_row4(qt + tt * Rp + 4 * rb0, q);
+        smem_row<R, NCP>(in + (int64_t(t) * G + g0) * NCP, xv);
 #pragma unroll
         for (int c = 0; c < NC; c++)
-        {
-          R const x = xr[c];
 #pragma unroll
           for (int i = 0; i < 4; i++)
-            acc0[i][c] = fma(q[i], x, acc0[i][c]);
-        }
+            acc0[i][c] = fma(q[i], xv[c], acc0[i][c]);
       }
       if (has1)
       {
-        R q[4];
-#pragma unroll
-        for (int i = 0; i < 4; i++)
-          q[i] = qt[tt * Rp + 4 * rb1 + i];
-        const R *xr = in + (int64_t(t) * G + g1) * NCP;
+        R q[4], xv[NCP];
+        smem_row4(qt + tt * Rp + 4 * rb1, q);
+        smem_row<R, NCP>(in + (int64_t(t) * G + g1) * NCP, xv);
 #pragma unroll
         for (int c = 0; c < NC; c++)
-        {
-          R const x = xr[c];
 #pragma unroll
           for (int i = 0; i < 4; i++)
-            acc1[i][c] = fma(q[i], x, acc1[i][c]);
-        }
+            acc1[i][c] = fma(q[i], xv[c], acc1[i][c]);
       }
     }
     __syncthreads(); // the buffer is refilled two tiles on
@@ -359,31 +385,62 @@ __global__ void __launch_bounds__(kLineThreads)
   __syncthreads();
   int const stk = ipow3l(D - 1 - a.k);
   double const f = scale_state ? scale_state[1] : 1.0;
-  // gather (row = member * 3 + k polynomial, group, column)
+  // gather (row = member * 3 + k polynomial, group, column); kGatherLoads
+  // independent loads per thread are issued before their values are used
   int const nload = m * G * 3 * NC;
-  for (int e = threadIdx.x; e < nload; e += blockDim.x)
-  {
+  auto gidx = [&](int e, int &xo) {
     int const c  = e % NC;
     int const pk = (e / NC) % 3;
     int const g  = (e / (3 * NC)) % G;
     int const i  = e / (3 * NC * G);
-    int64_t const gi = int64_t(cells[i]) * TS + s_offg[g] + s_offc[c] + pk * stk;
-    R val;
+    xo           = ((i * 3 + pk) * G + g) * NCP + c;
+    return int64_t(__ldg(cells + i)) * TS + s_offg[g] + s_offc[c] + pk * stk;
+  };
+  for (int e0 = threadIdx.x; e0 < nload; e0 += kGatherLoads * kLineThreads)
+  {
+    int64_t gi[kGatherLoads];
+    int xo[kGatherLoads];
+#pragma unroll
+    for (int u = 0; u < kGatherLoads; u++)
+    {
+      int const e = e0 + u * kLineThreads;
+      gi[u]       = e < nload ? gidx(e, xo[u]) : 0;
+    }
     if (in64)
     {
-      double vv = in64[gi];
-      if (scale_state)
+      double v[kGatherLoads];
+#pragma unroll
+      for (int u = 0; u < kGatherLoads; u++)
+        if (e0 + u * kLineThreads < nload)
+          v[u] = in64[gi[u]];
+#pragma unroll
+      for (int u = 0; u < kGatherLoads; u++)
       {
-        vv *= f;
-        vscale[gi] = vv;
-        if (vcopy)
-          vcopy[gi] = float(vv);
+        if (e0 + u * kLineThreads >= nload)
+          break;
+        double vv = v[u];
+        if (scale_state)
+        {
+          vv *= f;
+          vscale[gi[u]] = vv;
+          if (vcopy)
+            vcopy[gi[u]] = float(vv);
+        }
+        X[xo[u]] = R(vv);
       }
-      val = R(vv);
     }
     else
-      val = inR[gi];
-    X[((int64_t(i) * 3 + pk) * G + g) * NCP + c] = val;
+    {
+      R v[kGatherLoads];
+#pragma unroll
+      for (int u = 0; u < kGatherLoads; u++)
+        if (e0 + u * kLineThreads < nload)
+          v[u] = inR[gi[u]];
+#pragma unroll
+      for (int u = 0; u < kGatherLoads; u++)
+        if (e0 + u * kLineThreads < nload)
+          X[xo[u]] = v[u];
+    }
   }
   __syncthreads();
   // B = s - dt sum_{line j} S_j along j, on each (member, group): its 3 x NC
@@ -521,6 +578,29 @@ constexpr int kSmallThreads = 128;
 constexpr int kSmallCells   = 8;
 constexpr int kSmallMaxM    = 8;
 constexpr int kSmallMaxR    = 3 * kSmallMaxM;
+constexpr int kStageLoads   = 8; // loads in flight per thread while staging
+
+// four consecutive entries of a shared-memory row (16-byte aligned).  The
+// loads are volatile so that the compiler reloads the matrix for every
+// column instead of hoisting all of it out of the column loop into
+// registers (which spills)
+__device__ __forceinline__ void lds4(const float *p, float (&q)[4])
+{
+  unsigned const a = static_cast<unsigned>(__cvta_generic_to_shared(p));
+  asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];\n"
+               : "=f"(q[0]), "=f"(q[1]), "=f"(q[2]), "=f"(q[3])
+               : "r"(a));
+}
+__device__ __forceinline__ void lds4(const double *p, double (&q)[4])
+{
+  unsigned const a = static_cast<unsigned>(__cvta_generic_to_shared(p));
+  asm volatile("ld.shared.v2.f64 {%0, %1}, [%2];\n"
+               : "=d"(q[0]), "=d"(q[1])
+               : "r"(a));
+  asm volatile("ld.shared.v2.f64 {%0, %1}, [%2];\n"
+               : "=d"(q[2]), "=d"(q[3])
+               : "r"(a + 16u));
+}
 
 template<typename R, int D, int M, int KIDX, int MC>
 __device__ __forceinline__ void small_column(line_args<R> const &a, R *buf,
@@ -531,6 +611,7 @@ __device__ __forceinline__ void small_column(line_args<R> const &a, R *buf,
 {
   constexpr int TS = ipow3l(D);
   constexpr int RR = 3 * MC;
+  constexpr int RP = (RR + 3) / 4 * 4;
   R x[RR];
 #pragma unroll
   for (int i = 0; i < MC; i++)
@@ -555,33 +636,43 @@ __device__ __forceinline__ void small_column(line_args<R> const &a, R *buf,
     }
   }
   // Qm: the pencil matrix's eigenvectors staged in shared memory, [t][r]
-  // with rows of RR entries.  Per eigenmode r: u_r = (Q^T x)_r / (mu - dt
-  // theta_r), then out += Q[:, r] u_r -- register arrays indexed only by
-  // unrolled loops
-  R out[RR];
+  // with rows of RP entries.  u = Q^T x row by row of Qm (four entries per
+  // load), u_r /= mu - dt theta_r, then out_t = Qm[t, :] u; every sum runs
+  // over increasing t (resp. r)
+  R u[RP];
+#pragma unroll
+  for (int r = 0; r < RP; r++)
+    u[r] = R(0);
 #pragma unroll
   for (int t = 0; t < RR; t++)
-    out[t] = R(0);
-#pragma unroll(MC <= 2 ? RR : 1)
+#pragma unroll
+    for (int r4 = 0; r4 < RP / 4; r4++)
+    {
+      R q[4];
+      lds4(Qm + t * RP + 4 * r4, q);
+#pragma unroll
+      for (int i = 0; i < 4; i++)
+        u[4 * r4 + i] = fma(q[i], x[t], u[4 * r4 + i]);
+    }
+#pragma unroll
   for (int r = 0; r < RR; r++)
-  {
-    R acc = R(0);
-#pragma unroll
-    for (int t = 0; t < RR; t++)
-      acc = fma(Qm[t * RR + r], x[t], acc);
-    R const u = acc / (mu - a.dt * th[r]);
-#pragma unroll
-    for (int t = 0; t < RR; t++)
-      out[t] = fma(Qm[t * RR + r], u, out[t]);
-  }
+    u[r] = u[r] / (mu - a.dt * th[r]);
 #pragma unroll
   for (int t = 0; t < RR; t++)
-    x[t] = out[t];
+  {
+    R o = R(0);
 #pragma unroll
-  for (int i = 0; i < MC; i++)
+    for (int r4 = 0; r4 < RP / 4; r4++)
+    {
+      R q[4];
+      lds4(Qm + t * RP + 4 * r4, q);
 #pragma unroll
-    for (int pk = 0; pk < 3; pk++)
-      buf[(slot0 + i) * TS + fb + pk * stk] = x[3 * i + pk];
+      for (int i = 0; i < 4; i++)
+        if (4 * r4 + i < RR)
+          o = fma(q[i], u[4 * r4 + i], o);
+    }
+    buf[(slot0 + t / 3) * TS + fb + (t % 3) * stk] = o;
+  }
 }
 
 // One launch per factor for every batch of small pencils.  A batch record
@@ -611,7 +702,7 @@ __global__ void __launch_bounds__(kSmallThreads, 4)
   __shared__ short s_fbk[NF];
   __shared__ short s_fbo[2][NF];
   __shared__ unsigned char s_dig[NF];
-  __shared__ R s_Q[kSmallMaxR * kSmallMaxR];
+  __shared__ __align__(16) R s_Q[kSmallMaxR * kSmallMaxR];
   __shared__ R s_th[kSmallMaxR];
   __shared__ R s_P[kSmallCells][2][9];
   __shared__ R s_lam[kSmallCells][2][3];
@@ -642,8 +733,8 @@ __global__ void __launch_bounds__(kSmallThreads, 4)
       s_Sk[tid][e] = sk[e];
   }
   // the batch's pencil matrix (every pencil of a batch has the same one)
-  for (int e = tid; e < RR * RR; e += blockDim.x)
-    s_Q[e] = a.Q[bt.z + (e / RR) * Rp + e % RR];
+  for (int e = tid; e < RR * Rp; e += blockDim.x)
+    s_Q[e] = a.Q[bt.z + e];
   if (tid < RR)
     s_th[tid] = a.theta[bt.w + tid];
   for (int fi = tid; fi < NF; fi += blockDim.x)
@@ -660,25 +751,61 @@ __global__ void __launch_bounds__(kSmallThreads, 4)
     s_dig[fi] = (unsigned char)dg;
   }
   __syncthreads();
-  // stage the cells
-  double const f = scale_state ? scale_state[1] : 1.0;
-  for (int e = tid; e < nc * TS; e += blockDim.x)
+  // stage the cells: kStageLoads independent loads per thread are issued
+  // before their values are used, so enough of them are in flight
+  int const ntot = nc * TS;
+  if (in64)
   {
-    int64_t const gi = int64_t(s_cell[e / TS]) * TS + e % TS;
-    if (in64)
+    double const f = scale_state ? scale_state[1] : 1.0;
+    for (int e0 = tid; e0 < ntot; e0 += kStageLoads * kSmallThreads)
     {
-      double vv = in64[gi];
-      if (scale_state)
+      double v[kStageLoads];
+#pragma unroll
+      for (int u = 0; u < kStageLoads; u++)
       {
-        vv *= f;
-        vscale[gi] = vv;
-        if (vcopy)
-          vcopy[gi] = float(vv);
+        int const e = e0 + u * kSmallThreads;
+        if (e < ntot)
+          v[u] = in64[int64_t(s_cell[e / TS]) * TS + e % TS];
       }
-      buf[e] = R(vv);
+#pragma unroll
+      for (int u = 0; u < kStageLoads; u++)
+      {
+        int const e = e0 + u * kSmallThreads;
+        if (e >= ntot)
+          break;
+        double vv = v[u];
+        if (scale_state)
+        {
+          int64_t const gi = int64_t(s_cell[e / TS]) * TS + e % TS;
+          vv *= f;
+          vscale[gi] = vv;
+          if (vcopy)
+            vcopy[gi] = float(vv);
+        }
+        buf[e] = R(vv);
+      }
     }
-    else
-      buf[e] = inR[gi];
+  }
+  else
+  {
+    for (int e0 = tid; e0 < ntot; e0 += kStageLoads * kSmallThreads)
+    {
+      R v[kStageLoads];
+#pragma unroll
+      for (int u = 0; u < kStageLoads; u++)
+      {
+        int const e = e0 + u * kSmallThreads;
+        if (e < ntot)
+          v[u] = inR[int64_t(s_cell[e / TS]) * TS + e % TS];
+      }
+#pragma unroll
+      for (int u = 0; u < kStageLoads; u++)
+      {
+        int const e = e0 + u * kSmallThreads;
+        if (e < ntot)
+          buf[e] = v[u];
+      }
+    }
   }
   __syncthreads();
   // W^T (forward) or W (backward): fibre stages along the other line dimensions

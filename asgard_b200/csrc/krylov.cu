@@ -215,7 +215,10 @@ __global__ void __launch_bounds__(kThreads)
     part[blockIdx.x] = v[0];
 }
 
-// x += V[:, :k] y
+// x += V[:, :k] y; VEC = 2 takes two rows per 16-byte load, with each row's
+// sum in the order of dot_row (four chains by column mod 4), so both forms
+// give the same bits
+template<int VEC>
 __global__ void __launch_bounds__(kThreads)
     k_gemv_add(const double *__restrict__ V, int64_t ldv, int k,
                const double *__restrict__ y, double *__restrict__ x, int64_t n)
@@ -224,9 +227,44 @@ __global__ void __launch_bounds__(kThreads)
   for (int j = threadIdx.x; j < k; j += blockDim.x)
     ys[j] = y[j];
   __syncthreads();
-  for (int64_t r = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; r < n;
-       r += int64_t(gridDim.x) * blockDim.x)
-    x[r] += dot_row(V, ldv, k, r, ys);
+  if constexpr (VEC == 1)
+  {
+    for (int64_t r = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; r < n;
+         r += int64_t(gridDim.x) * blockDim.x)
+      x[r] += dot_row(V, ldv, k, r, ys);
+  }
+  else
+  {
+    const double2 *V2 = reinterpret_cast<const double2 *>(V);
+    int64_t const ld2 = ldv / 2;
+    for (int64_t r = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; r < n / 2;
+         r += int64_t(gridDim.x) * blockDim.x)
+    {
+      double a[4] = {0.0, 0.0, 0.0, 0.0}, b[4] = {0.0, 0.0, 0.0, 0.0};
+      int j = 0;
+      for (; j + 4 <= k; j += 4)
+      {
+#pragma unroll
+        for (int q = 0; q < 4; q++)
+        {
+          double2 const v = V2[r + (j + q) * ld2];
+          a[q]            = fma(v.x, ys[j + q], a[q]);
+          b[q]            = fma(v.y, ys[j + q], b[q]);
+        }
+      }
+      for (; j < k; j++)
+      {
+        double2 const v = V2[r + j * ld2];
+        a[0]            = fma(v.x, ys[j], a[0]);
+        b[0]            = fma(v.y, ys[j], b[0]);
+      }
+      double2 *x2 = reinterpret_cast<double2 *>(x);
+      double2 t   = x2[r];
+      t.x += (a[0] + a[1]) + (a[2] + a[3]);
+      t.y += (b[0] + b[1]) + (b[2] + b[3]);
+      x2[r] = t;
+    }
+  }
 }
 
 // ---- Gram-Schmidt kernels that finish their own reductions -------------
@@ -785,16 +823,16 @@ int launch_store_basis(double *w, float *vf, int64_t n, const double *state,
   bool const v2 = (n % 2 == 0) && (reinterpret_cast<uintptr_t>(w) % 16 == 0) &&
                   (reinterpret_cast<uintptr_t>(vf) % 8 == 0);
   if (v2)
-    k_store_basis<2><<<grid_for(n / 2), kThreads, 0, s>>>(w, vf, n, state, scale, g_gate);
+    k_store_basis<2><<<grid_wide(n / 2), kThreads, 0, s>>>(w, vf, n, state, scale, g_gate);
   else
-    k_store_basis<1><<<grid_for(n), kThreads, 0, s>>>(w, vf, n, state, scale, g_gate);
+    k_store_basis<1><<<grid_wide(n), kThreads, 0, s>>>(w, vf, n, state, scale, g_gate);
   ASGK_LAUNCHED();
   return ASGK_OK;
 }
 
 int launch_scale_by(double *v, int64_t n, const double *state, cudaStream_t s)
 {
-  k_scale_by<<<grid_for(n), kThreads, 0, s>>>(v, n, state, g_gate);
+  k_scale_by<<<grid_wide(n), kThreads, 0, s>>>(v, n, state, g_gate);
   ASGK_LAUNCHED();
   return ASGK_OK;
 }
@@ -809,35 +847,35 @@ int launch_norm2_h(const double *v, int64_t n, double *part, unsigned *ticket,
 
 int launch_fill(double *v, int64_t n, double a, cudaStream_t s)
 {
-  k_fill<<<grid_for(n), kThreads, 0, s>>>(v, n, a);
+  k_fill<<<grid_wide(n), kThreads, 0, s>>>(v, n, a);
   ASGK_LAUNCHED();
   return ASGK_OK;
 }
 
 int launch_copy(double *d, const double *src, int64_t n, cudaStream_t s)
 {
-  k_copy<<<grid_for(n), kThreads, 0, s>>>(d, src, n);
+  k_copy<<<grid_wide(n), kThreads, 0, s>>>(d, src, n);
   ASGK_LAUNCHED();
   return ASGK_OK;
 }
 
 int launch_scale(double *v, int64_t n, double a, cudaStream_t s)
 {
-  k_scale<<<grid_for(n), kThreads, 0, s>>>(v, n, a);
+  k_scale<<<grid_wide(n), kThreads, 0, s>>>(v, n, a);
   ASGK_LAUNCHED();
   return ASGK_OK;
 }
 
 int launch_axpy(double *y, const double *x, int64_t n, double a, cudaStream_t s)
 {
-  k_axpy<<<grid_for(n), kThreads, 0, s>>>(y, x, n, a);
+  k_axpy<<<grid_wide(n), kThreads, 0, s>>>(y, x, n, a);
   ASGK_LAUNCHED();
   return ASGK_OK;
 }
 
 int launch_xpby(double *y, const double *x, int64_t n, double b, cudaStream_t s)
 {
-  k_xpby<<<grid_for(n), kThreads, 0, s>>>(y, x, n, b);
+  k_xpby<<<grid_wide(n), kThreads, 0, s>>>(y, x, n, b);
   ASGK_LAUNCHED();
   return ASGK_OK;
 }
@@ -886,8 +924,11 @@ int launch_norm2(const double *v, int64_t n, double *part, int *blocks,
 int launch_gemv_add(const double *V, int64_t ldv, int k, const double *y,
                     double *x, int64_t n, cudaStream_t s)
 {
-  k_gemv_add<<<grid_for(n), kThreads, sizeof(double) * std::max(k, 1), s>>>(
-      V, ldv, k, y, x, n);
+  size_t const sh = sizeof(double) * std::max(k, 1);
+  if (n % 2 == 0 && vec2_ok(V, ldv, x))
+    k_gemv_add<2><<<grid_wide(n / 2), kThreads, sh, s>>>(V, ldv, k, y, x, n);
+  else
+    k_gemv_add<1><<<grid_wide(n), kThreads, sh, s>>>(V, ldv, k, y, x, n);
   ASGK_LAUNCHED();
   return ASGK_OK;
 }
