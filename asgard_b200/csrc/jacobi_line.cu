@@ -174,6 +174,22 @@ __device__ __forceinline__ void cp_async_wait()
 
 constexpr int kLineTile = 16; // matrix rows per staged tile
 
+// a = fma(qa, x, a), b = fma(qb, x, b): for FP32 one packed two-lane FMA
+// (fma.rn.f32x2, each lane rounded as the scalar FMA, so the same bits)
+__device__ __forceinline__ void fma_pair(float qa, float qb, float x, float &a, float &b)
+{
+  asm("{\n\t.reg .b64 rq, rx, ra;\n\t"
+      "mov.b64 rq, {%2, %3};\n\tmov.b64 rx, {%4, %4};\n\tmov.b64 ra, {%0, %1};\n\t"
+      "fma.rn.f32x2 ra, rq, rx, ra;\n\tmov.b64 {%0, %1}, ra;\n\t}"
+      : "+f"(a), "+f"(b)
+      : "f"(qa), "f"(qb), "f"(x));
+}
+__device__ __forceinline__ void fma_pair(double qa, double qb, double x, double &a, double &b)
+{
+  a = fma(qa, x, a);
+  b = fma(qb, x, b);
+}
+
 // shared-memory rows read in 16-byte pieces (rows start 16-byte aligned)
 __device__ __forceinline__ void smem_row4(const float *p, float (&q)[4])
 {
@@ -267,9 +283,10 @@ __device__ void dense_rows(const R *__restrict__ Mt, int Rr, int Rp, int G,
         smem_row<R, NCP>(in + (int64_t(t) * G + g0) * NCP, xv);
 #pragma unroll
         for (int c = 0; c < NC; c++)
-#pragma unroll
-          for (int i = 0; i < 4; i++)
-            acc0[i][c] = fma(q[i], xv[c], acc0[i][c]);
+        {
+          fma_pair(q[0], q[1], xv[c], acc0[0][c], acc0[1][c]);
+          fma_pair(q[2], q[3], xv[c], acc0[2][c], acc0[3][c]);
+        }
       }
       if (has1)
       {
@@ -278,9 +295,10 @@ __device__ void dense_rows(const R *__restrict__ Mt, int Rr, int Rp, int G,
         smem_row<R, NCP>(in + (int64_t(t) * G + g1) * NCP, xv);
 #pragma unroll
         for (int c = 0; c < NC; c++)
-#pragma unroll
-          for (int i = 0; i < 4; i++)
-            acc1[i][c] = fma(q[i], xv[c], acc1[i][c]);
+        {
+          fma_pair(q[0], q[1], xv[c], acc1[0][c], acc1[1][c]);
+          fma_pair(q[2], q[3], xv[c], acc1[2][c], acc1[3][c]);
+        }
       }
     }
     __syncthreads(); // the buffer is refilled two tiles on
@@ -650,28 +668,37 @@ __device__ __forceinline__ void small_column(line_args<R> const &a, R *buf,
     {
       R q[4];
       lds4(Qm + t * RP + 4 * r4, q);
-#pragma unroll
-      for (int i = 0; i < 4; i++)
-        u[4 * r4 + i] = fma(q[i], x[t], u[4 * r4 + i]);
+      fma_pair(q[0], q[1], x[t], u[4 * r4], u[4 * r4 + 1]);
+      fma_pair(q[2], q[3], x[t], u[4 * r4 + 2], u[4 * r4 + 3]);
     }
 #pragma unroll
   for (int r = 0; r < RR; r++)
     u[r] = u[r] / (mu - a.dt * th[r]);
+  // two outputs (rows t, t + 1 of Qm) per pass
 #pragma unroll
-  for (int t = 0; t < RR; t++)
+  for (int t = 0; t < RR; t += 2)
   {
-    R o = R(0);
+    R o0 = R(0), o1 = R(0);
 #pragma unroll
     for (int r4 = 0; r4 < RP / 4; r4++)
     {
-      R q[4];
-      lds4(Qm + t * RP + 4 * r4, q);
+      R qa[4], qb[4];
+      lds4(Qm + t * RP + 4 * r4, qa);
+      if (t + 1 < RR)
+        lds4(Qm + (t + 1) * RP + 4 * r4, qb);
 #pragma unroll
       for (int i = 0; i < 4; i++)
         if (4 * r4 + i < RR)
-          o = fma(q[i], u[4 * r4 + i], o);
+        {
+          if (t + 1 < RR)
+            fma_pair(qa[i], qb[i], u[4 * r4 + i], o0, o1);
+          else
+            o0 = fma(qa[i], u[4 * r4 + i], o0);
+        }
     }
-    buf[(slot0 + t / 3) * TS + fb + (t % 3) * stk] = o;
+    buf[(slot0 + t / 3) * TS + fb + (t % 3) * stk] = o0;
+    if (t + 1 < RR)
+      buf[(slot0 + (t + 1) / 3) * TS + fb + ((t + 1) % 3) * stk] = o1;
   }
 }
 
