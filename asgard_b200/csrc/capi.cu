@@ -486,7 +486,7 @@ inline int pos_from_indices(int i, int j) { return i + j * (j + 1) / 2; }
 // What a recorded GMRES cycle depends on besides the workspace buffers: the
 // operator (plan, dt, arithmetic), the preconditioner, the restart length,
 // the basis precision of the Gram-Schmidt passes, the Arnoldi steps per
-// graph node.
+// graph node, whether the preconditioner writes the operator's FP32 input.
 struct graph_key
 {
   const void *plan = nullptr; // the workspace dies with its plan
@@ -496,16 +496,18 @@ struct graph_key
   int restart      = 0;
   bool low_basis   = false;
   int node_steps   = 1;
+  bool fused_copy  = false;
   bool operator==(graph_key const &o) const
   {
     return plan == o.plan && dt == o.dt && precision == o.precision &&
            pc == o.pc && restart == o.restart && low_basis == o.low_basis &&
-           node_steps == o.node_steps;
+           node_steps == o.node_steps && fused_copy == o.fused_copy;
   }
 };
 
 bool g_gmres_graphs     = true; // asgk_set_gmres_graphs
 bool g_gmres_low_basis  = true; // asgk_set_gmres_basis
+bool g_gmres_fused_copy = true; // asgk_set_gmres_fused_copy
 // steps per node of a recorded cycle (asgk_set_gmres_node_steps): at d=4
 // level 7 a 138-iteration solve took 9.85 / 8.49 / 8.33 / 8.23 ms with 1 / 4
 // / 8 / 16 (node boundaries cost ~10 us, a skipped launch ~1 us)
@@ -2279,11 +2281,23 @@ int gmres_euler_impl(asgk_plan *plan, double dt, double *x, const double *b,
     status = ASGK_ERR_NOT_CONVERGED;
     for (;;)
     {
+      // a zero initial guess (||x|| = 0) needs no product: r = b
+      bool x_zero = false;
+      if (steps == 0)
+      {
+        double xn = 0;
+        if (int rc = norm2(ws, x, n, xn, s))
+          return rc;
+        x_zero = (xn == 0.0);
+      }
       if (int rc = launch_copy(ws.r, b, n, s))
         return rc;
-      if (int rc = op64(-1.0, x, 1.0, ws.r, s))
-        return rc;
-      ++fp64;
+      if (!x_zero)
+      {
+        if (int rc = op64(-1.0, x, 1.0, ws.r, s))
+          return rc;
+        ++fp64;
+      }
       if (int rc = norm2(ws, ws.r, n, rnorm, s))
         return rc;
       if (!std::isfinite(rnorm))
@@ -2315,7 +2329,7 @@ int gmres_euler_impl(asgk_plan *plan, double dt, double *x, const double *b,
       // FP32 inner solves: Gram-Schmidt over an FP32 copy of the basis
       bool const low_basis = (precision != ASGK_FP64) && g_gmres_low_basis;
       graph_key const gk{plan, dt, precision, use_pc ? pc_serial : 0, restart,
-                         low_basis, node_steps};
+                         low_basis, node_steps, use_pc != nullptr && g_gmres_fused_copy};
       bool const recordable = (use_pc == nullptr || pc_graph_ok);
       if (int rc = gmres_core(ws, n, (precision == ASGK_FP64) ? matvec_t(op64) : matvec_t(oplow),
                               use_pc, ws.e, ws.r, restart, inner_outer, itol, ist, s,
@@ -2437,10 +2451,21 @@ int asgk_gmres_euler_jacobi(asgk_plan *plan, double dt, double *x,
     if (int rc = jacobi_check_shape(precond, plan->p.rows, plan->p.tensor))
       return rc;
     cudaStream_t s = as_stream(stream);
+    // with the FP32 global apply at d >= 5 next, the line preconditioner
+    // also writes the FP32 copy of its output that apply reads
+    plan_data const &pp = plan->p;
+    float *zc = (precision == ASGK_FP32 && pp.gx32 != nullptr && g_gmres_fused_copy &&
+                 jacobi_writes_zcopy(precond))
+                    ? pp.gx32
+                    : nullptr;
     make_pc_t const mk = [&](bool low) -> precond_t {
-      return [=](double *v, double *z, const double *sc, float *vc,
-                 cudaStream_t ss) -> int {
-        return jacobi_apply_handle(precond, low, v, z, sc, vc, ss);
+      return [=, &pp](double *v, double *z, const double *sc, float *vc,
+                      cudaStream_t ss) -> int {
+        float *c = low ? zc : nullptr;
+        int const rc = jacobi_apply_handle(precond, low, v, z, sc, vc, ss, c);
+        if (rc == ASGK_OK && c != nullptr)
+          pp.gx32_src = z;
+        return rc;
       };
     };
     return gmres_euler_impl(plan, dt, x, b, restart, max_outer, tol, tol_mode,
@@ -2523,6 +2548,13 @@ int asgk_set_gmres_basis(int fp32)
 {
   int const old     = g_gmres_low_basis ? 1 : 0;
   g_gmres_low_basis = (fp32 != 0);
+  return old;
+}
+
+int asgk_set_gmres_fused_copy(int on)
+{
+  int const old      = g_gmres_fused_copy ? 1 : 0;
+  g_gmres_fused_copy = (on != 0);
   return old;
 }
 

@@ -134,6 +134,9 @@ struct plan_data
   int *gseg = nullptr;         // [rows][d + 1] offsets within the cell's list
   int *gcell_order = nullptr;  // [2][rows]: by longest segment, by entries
   float *gx32 = nullptr;       // [rows * n^d]
+  // the vector whose FP32 copy gx32 holds when a preconditioner wrote it
+  // with its output (consumed, and cleared, by the next FP32 global apply)
+  mutable const double *gx32_src = nullptr;
   // terms acting in several dimensions (the reference's upper/lower
   // permutations): chains of masked 1D passes over per-dimension neighbour
   // lists.  Stage s runs the jobs gjobs[stage_job0[s] ..] (chain, dimension,
@@ -198,12 +201,17 @@ int launch_fill_pairs(int d, int cells, const int *oned, const int *cand,
 struct jacobi_data;
 // z = M v; with scale_state, v *= scale_state[1] in place first (the
 // normalisation of a recorded GMRES step's new basis vector, fused), and
-// with vcopy also vcopy = FP32(v) (the basis copy of FP32 inner solves)
+// with vcopy also vcopy = FP32(v) (the basis copy of FP32 inner solves).
+// zcopy (the line preconditioner only, else ignored): also zcopy = FP32(z),
+// the FP32 copy of x the next FP32 global apply reads
 int jacobi_apply(jacobi_data const &jd, bool low, double *v, double *z,
-                 const double *scale_state, float *vcopy, cudaStream_t s);
+                 const double *scale_state, float *vcopy, cudaStream_t s,
+                 float *zcopy = nullptr);
 int jacobi_apply_handle(asgk_jacobi *pc, bool low, double *v, double *z,
                         const double *scale_state, float *vcopy,
-                        cudaStream_t s);
+                        cudaStream_t s, float *zcopy = nullptr);
+// whether jacobi_apply writes zcopy
+bool jacobi_writes_zcopy(const asgk_jacobi *pc);
 // never reused within a process: identifies a preconditioner in caches
 uint64_t jacobi_serial(const asgk_jacobi *pc);
 // ASGK_OK when the preconditioner applies to vectors of rows * tensor
@@ -219,7 +227,8 @@ struct line_data;
 int line_build(plan_data const &p, double dt, line_data **out, int64_t &bytes);
 void line_free(line_data *ld);
 int line_apply(line_data const &ld, bool low, double *v, double *z,
-               const double *scale_state, float *vcopy, cudaStream_t s);
+               const double *scale_state, float *vcopy, float *zcopy,
+               cudaStream_t s);
 // the line dimensions (up to 3) into dims; returns how many
 int line_info(line_data const &ld, int *dims);
 

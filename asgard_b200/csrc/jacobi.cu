@@ -822,11 +822,12 @@ int jacobi_build(plan_data const &p, double dt, int kind, jacobi_data &jd)
 }
 
 int jacobi_apply(jacobi_data const &jd, bool low, double *v, double *z,
-                 const double *scale_state, float *vcopy, cudaStream_t s)
+                 const double *scale_state, float *vcopy, cudaStream_t s,
+                 float *zcopy)
 {
   int64_t const n = int64_t(jd.rows) * jd.ts;
   if (jd.kind == ASGK_JACOBI_LINE)
-    return line_apply(*jd.line, low, v, z, scale_state, vcopy, s);
+    return line_apply(*jd.line, low, v, z, scale_state, vcopy, zcopy, s);
   if (jd.kind == ASGK_JACOBI_KRON)
   {
     if (low)
@@ -952,9 +953,14 @@ double asgk::jacobi_dt(const asgk_jacobi *pc) { return pc ? pc->jd.dt : 0.0; }
 
 int asgk::jacobi_apply_handle(asgk_jacobi *pc, bool low, double *v, double *z,
                               const double *scale_state, float *vcopy,
-                              cudaStream_t s)
+                              cudaStream_t s, float *zcopy)
 {
-  return asgk::jacobi_apply(pc->jd, low, v, z, scale_state, vcopy, s);
+  return asgk::jacobi_apply(pc->jd, low, v, z, scale_state, vcopy, s, zcopy);
+}
+
+bool asgk::jacobi_writes_zcopy(const asgk_jacobi *pc)
+{
+  return pc != nullptr && pc->jd.kind == ASGK_JACOBI_LINE;
 }
 
 int asgk_jacobi_info(asgk_jacobi *pc, int *kind, double *dt,

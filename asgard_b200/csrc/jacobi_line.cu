@@ -338,7 +338,8 @@ __global__ void __launch_bounds__(kLineThreads)
     k_line_factor(line_args<R> a, const double *in64,
                   const R *__restrict__ inR, double *__restrict__ out64,
                   R *__restrict__ outR, int bj, const double *scale_state,
-                  double *vscale, float *vcopy, const double *gate)
+                  double *vscale, float *vcopy, float *__restrict__ zcopy,
+                  const double *gate)
 {
   if (gate_closed(gate))
     return;
@@ -577,7 +578,11 @@ __global__ void __launch_bounds__(kLineThreads)
     int64_t const gi = int64_t(cells[i]) * TS + s_offg[g] + s_offc[c] + pk * stk;
     R const val = X[((int64_t(i) * 3 + pk) * G + g) * NCP + c];
     if (out64)
+    {
       out64[gi] = double(val);
+      if (zcopy)
+        zcopy[gi] = float(val);
+    }
     else
       outR[gi] = val;
   }
@@ -713,7 +718,8 @@ __global__ void __launch_bounds__(kSmallThreads, 4)
                  const int4 *__restrict__ bcells, const double *in64,
                  const R *__restrict__ inR, double *__restrict__ out64,
                  R *__restrict__ outR, int bj, const double *scale_state,
-                 double *vscale, float *vcopy, const double *gate)
+                 double *vscale, float *vcopy, float *__restrict__ zcopy,
+                 const double *gate)
 {
   if (gate_closed(gate))
     return;
@@ -873,7 +879,11 @@ __global__ void __launch_bounds__(kSmallThreads, 4)
   {
     int64_t const gi = int64_t(s_cell[e / TS]) * TS + e % TS;
     if (out64)
+    {
       out64[gi] = double(buf[e]);
+      if (zcopy)
+        zcopy[gi] = float(buf[e]);
+    }
     else
       outR[gi] = buf[e];
   }
@@ -1244,7 +1254,8 @@ namespace
 template<typename R, int D, int M, int KIDX>
 int launch_factor(line_data const &ld, line_factor const &f, const double *in64,
                   const R *inR, double *out64, R *outR, bool bj,
-                  const double *sc, double *vscale, float *vc, cudaStream_t s)
+                  const double *sc, double *vscale, float *vc, float *zc,
+                  cudaStream_t s)
 {
   constexpr int NC  = ipow3l(M - 1);
   constexpr int NCP = NC == 1 ? 1 : (NC == 3 ? 4 : 12);
@@ -1284,7 +1295,7 @@ int launch_factor(line_data const &ld, line_factor const &f, const double *in64,
     ASGK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    int(shm)));
     kern<<<f.nunits, kLineThreads, shm, sb>>>(a, in64, inR, out64, outR, bj ? 1 : 0,
-                                              sc, vscale, vc, g_gate);
+                                              sc, vscale, vc, zc, g_gate);
     ASGK_LAUNCHED();
   }
   if (f.nbatches > 0)
@@ -1294,7 +1305,7 @@ int launch_factor(line_data const &ld, line_factor const &f, const double *in64,
     ASGK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    int(shm)));
     kern<<<f.nbatches, kSmallThreads, shm, s>>>(a, f.batches, f.bcells, in64, inR, out64,
-                                                outR, bj ? 1 : 0, sc, vscale, vc, g_gate);
+                                                outR, bj ? 1 : 0, sc, vscale, vc, zc, g_gate);
     ASGK_LAUNCHED();
   }
   if (both)
@@ -1308,15 +1319,15 @@ int launch_factor(line_data const &ld, line_factor const &f, const double *in64,
 template<typename R, int D, int M, int KIDX>
 int factor_q(line_data const &ld, const double *in64, const R *inR, double *out64,
              R *outR, bool bj, const double *sc, double *vscale, float *vc,
-             cudaStream_t s)
+             float *zc, cudaStream_t s)
 {
   return launch_factor<R, D, M, KIDX>(ld, *ld.factors[KIDX], in64, inR, out64, outR,
-                                      bj, sc, vscale, vc, s);
+                                      bj, sc, vscale, vc, zc, s);
 }
 
 template<typename R, int D, int M>
 int apply_dm(line_data const &ld, double *v, double *z, const double *sc,
-             float *vc, cudaStream_t s)
+             float *vc, float *zc, cudaStream_t s)
 {
   int64_t const n = int64_t(ld.rows) * ld.ts;
   R *w0 = reinterpret_cast<R *>(ld.work);
@@ -1333,15 +1344,16 @@ int apply_dm(line_data const &ld, double *v, double *z, const double *sc,
     const double *fsc = first ? sc : nullptr;
     double *fvs       = first && sc ? v : nullptr;
     float *fvc        = first ? vc : nullptr;
+    float *lzc        = last ? zc : nullptr;
     int rc            = ASGK_ERR_UNSUPPORTED;
     if (q == 0)
-      rc = factor_q<R, D, M, 0>(ld, i64, iR, o64, oR, !first, fsc, fvs, fvc, s);
+      rc = factor_q<R, D, M, 0>(ld, i64, iR, o64, oR, !first, fsc, fvs, fvc, lzc, s);
     else if constexpr (M >= 2)
     {
       if (q == 1)
-        rc = factor_q<R, D, M, 1>(ld, i64, iR, o64, oR, !first, fsc, fvs, fvc, s);
+        rc = factor_q<R, D, M, 1>(ld, i64, iR, o64, oR, !first, fsc, fvs, fvc, lzc, s);
       else if constexpr (M >= 3)
-        rc = factor_q<R, D, M, 2>(ld, i64, iR, o64, oR, !first, fsc, fvs, fvc, s);
+        rc = factor_q<R, D, M, 2>(ld, i64, iR, o64, oR, !first, fsc, fvs, fvc, lzc, s);
     }
     if (rc)
       return rc;
@@ -1352,18 +1364,18 @@ int apply_dm(line_data const &ld, double *v, double *z, const double *sc,
 
 template<typename R, int D>
 int apply_d(line_data const &ld, double *v, double *z, const double *sc,
-            float *vc, cudaStream_t s)
+            float *vc, float *zc, cudaStream_t s)
 {
   switch (ld.m)
   {
-  case 1: return apply_dm<R, D, 1>(ld, v, z, sc, vc, s);
+  case 1: return apply_dm<R, D, 1>(ld, v, z, sc, vc, zc, s);
   case 2:
     if constexpr (D >= 2)
-      return apply_dm<R, D, 2>(ld, v, z, sc, vc, s);
+      return apply_dm<R, D, 2>(ld, v, z, sc, vc, zc, s);
     break;
   case 3:
     if constexpr (D >= 3)
-      return apply_dm<R, D, 3>(ld, v, z, sc, vc, s);
+      return apply_dm<R, D, 3>(ld, v, z, sc, vc, zc, s);
     break;
   default: break;
   }
@@ -1372,18 +1384,19 @@ int apply_d(line_data const &ld, double *v, double *z, const double *sc,
 } // namespace
 
 int line_apply(line_data const &ld, bool low, double *v, double *z,
-               const double *scale_state, float *vcopy, cudaStream_t s)
+               const double *scale_state, float *vcopy, float *zcopy,
+               cudaStream_t s)
 {
   auto go = [&](auto tag) -> int {
     using R = decltype(tag);
     switch (ld.d)
     {
-    case 1: return apply_d<R, 1>(ld, v, z, scale_state, vcopy, s);
-    case 2: return apply_d<R, 2>(ld, v, z, scale_state, vcopy, s);
-    case 3: return apply_d<R, 3>(ld, v, z, scale_state, vcopy, s);
-    case 4: return apply_d<R, 4>(ld, v, z, scale_state, vcopy, s);
-    case 5: return apply_d<R, 5>(ld, v, z, scale_state, vcopy, s);
-    case 6: return apply_d<R, 6>(ld, v, z, scale_state, vcopy, s);
+    case 1: return apply_d<R, 1>(ld, v, z, scale_state, vcopy, zcopy, s);
+    case 2: return apply_d<R, 2>(ld, v, z, scale_state, vcopy, zcopy, s);
+    case 3: return apply_d<R, 3>(ld, v, z, scale_state, vcopy, zcopy, s);
+    case 4: return apply_d<R, 4>(ld, v, z, scale_state, vcopy, zcopy, s);
+    case 5: return apply_d<R, 5>(ld, v, z, scale_state, vcopy, zcopy, s);
+    case 6: return apply_d<R, 6>(ld, v, z, scale_state, vcopy, zcopy, s);
     default: return ASGK_ERR_UNSUPPORTED;
     }
   };

@@ -623,10 +623,15 @@ int launch_global_d(plan_data const &p, double alpha, const double *x,
       int64_t const n = int64_t(p.rows) * TS;
       if constexpr (sizeof(TC) == 4)
       {
-        int const pairs  = (reinterpret_cast<uintptr_t>(x) % 16) == 0 ? 1 : 0;
-        int const blocks = int(std::min<int64_t>((n / 2 + 255) / 256, 4 * 148));
-        k_copy_to_f32<<<blocks, 256, 0, s>>>(n, x, p.gx32, pairs, g_gate);
-        ASGK_LAUNCHED();
+        // the copy is already there when the preconditioner wrote it with x
+        if (p.gx32_src != x)
+        {
+          int const pairs  = (reinterpret_cast<uintptr_t>(x) % 16) == 0 ? 1 : 0;
+          int const blocks = int(std::min<int64_t>((n / 2 + 255) / 256, 4 * 148));
+          k_copy_to_f32<<<blocks, 256, 0, s>>>(n, x, p.gx32, pairs, g_gate);
+          ASGK_LAUNCHED();
+        }
+        p.gx32_src = nullptr;
         kron_global_cell_dims<D, TC, float><<<p.rows, D * 32, 0, s>>>(
             p.gcell_order, p.gptr, p.gseg, p.gcol, p.gkb, B, alpha, p.gx32, x, beta, y,
             ex, g_gate);
@@ -676,11 +681,13 @@ int launch_global(plan_data const &p, int precision, double alpha,
     return ASGK_ERR_UNSUPPORTED; // the chain kernels take no gate
   // terms that are the identity in every dimension add n_identity * x
   double const ex_eff = ex + alpha * p.g_identity;
+  int rc = ASGK_ERR_UNSUPPORTED;
   if (precision == ASGK_FP64)
-    return launch_global_t<double>(p, alpha, x, beta, y, ex_eff, s);
-  if (precision == ASGK_FP32)
-    return launch_global_t<float>(p, alpha, x, beta, y, ex_eff, s);
-  return ASGK_ERR_UNSUPPORTED;
+    rc = launch_global_t<double>(p, alpha, x, beta, y, ex_eff, s);
+  else if (precision == ASGK_FP32)
+    rc = launch_global_t<float>(p, alpha, x, beta, y, ex_eff, s);
+  p.gx32_src = nullptr; // a preconditioner's copy serves the next apply only
+  return rc;
 }
 
 } // namespace asgk

@@ -385,6 +385,14 @@ int asgk_set_gmres_node_steps(int steps);
  * in the reference. */
 int asgk_set_gmres_basis(int fp32);
 
+/* Solves with the line preconditioner and the FP32 global operator at
+ * d >= 5 (asgk_gmres_euler_jacobi): with on = 1 (the default) the
+ * preconditioner's last pass also writes the FP32 copy of its output that
+ * the operator reads, instead of a separate conversion pass over the vector;
+ * on = 0 keeps the separate pass.  Both give the same bits.  Process-wide;
+ * returns the previous setting.  No counterpart in the reference. */
+int asgk_set_gmres_fused_copy(int on);
+
 /* ------------------------------------------------ implicit time loop */
 
 typedef enum asgk_pc_kind

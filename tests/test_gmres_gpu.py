@@ -266,3 +266,38 @@ def test_node_steps_give_the_same_iterates(cuda, precond, precision):
         assert np.array_equal(xs, x1)
         assert i_s.error == i1.error and i_s.true_relres == i1.true_relres
         assert ls == l1  # skipped launches are not counted as work
+
+
+@pytest.mark.parametrize("graphs", [0, 1])
+def test_line_preconditioner_fused_fp32_copy(cuda, graphs):
+    """At d >= 5 the line preconditioner's last pass also writes the FP32
+    copy of its output that the FP32 global operator reads (no separate
+    conversion pass): the iterates equal those with the separate pass bit
+    for bit, host-driven and recorded."""
+    import asgard_b200 as ab
+    import torch
+    op = ab.SparseGridOperator(5, 4, 5, kind="advdiff", nu=0.1)
+    mat = op.kronmult_matrix(mode="global")
+    dt = 1e-3
+    pc = ab.JacobiPreconditioner(mat, dt, kind="line")
+    b = to_dev(np.random.default_rng(21).uniform(-1, 1, op.N))
+    res = {}
+    old_graphs = ab.lib.asgk_set_gmres_graphs(graphs)
+    try:
+        for fused in (0, 1):
+            ab.lib.asgk_set_gmres_fused_copy(fused)
+            x = torch.zeros_like(b)
+            l0 = ab.launch_count()
+            info = ab.simple_gmres_euler(dt, mat, x, b, 30, 200, 1e-10, tol_mode="rel",
+                                         precision="fp32", precond=pc)
+            torch.cuda.synchronize()
+            assert info.status == 0 and info.true_relres <= 1e-10
+            res[fused] = (x.cpu().numpy(), info, ab.launch_count() - l0)
+    finally:
+        ab.lib.asgk_set_gmres_fused_copy(1)
+        ab.lib.asgk_set_gmres_graphs(old_graphs)
+    (xs, i_s, ls), (xf, i_f, lf) = res[0], res[1]
+    assert i_f.iterations == i_s.iterations and np.array_equal(xf, xs)
+    assert i_f.true_relres == i_s.true_relres
+    # one conversion launch fewer per preconditioned operator apply
+    assert lf < ls
