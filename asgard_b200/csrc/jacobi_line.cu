@@ -43,7 +43,8 @@ namespace asgk
 {
 namespace
 {
-constexpr int kLineThreads = 128;
+constexpr int kLineItems   = 128;            // item slots of a factor CTA
+constexpr int kLineThreads = 2 * kLineItems; // two halves share each item
 constexpr int kGatherLoads = 8; // loads in flight per thread while gathering
 constexpr int kSelfEntry   = 21; // P (3x3 col-major), lambda (3), S (3x3 col-major)
 
@@ -228,18 +229,25 @@ __device__ __forceinline__ void smem_row(const R *p, R (&q)[N])
 // out[r][g][c] = sum_{t < Rr} Mt[t][r] in[t][g][c] for r < Rr (Mt rows of
 // Rp entries, zero beyond Rr, in global memory), divided by den(r, c) when
 // theta is given.  Mt streams through shared memory in tiles of kLineTile
-// rows, double-buffered with cp.async; every thread owns at most two
-// (4-row block, group) items, their sums in registers across the tiles.
+// rows, double-buffered with cp.async.  The (4-row block, group) items go
+// to kLineItems thread slots, at most two each, their sums in registers
+// across the tiles; the two halves of the block take the first and second
+// half of every tile's rows for the same items, so each thread's chain of
+// dependent tiles is half as long.  The second half leaves its partial
+// sums in out, where the first adds them to its own (a fixed order) and
+// finishes.
 template<typename R, int NC, int NCP>
 __device__ void dense_rows(const R *__restrict__ Mt, int Rr, int Rp, int G,
                            const R *__restrict__ in, R *__restrict__ out,
                            const R *__restrict__ theta, const R *lamc, R shift,
                            R dt, R *qbuf)
 {
+  constexpr int TH = kLineTile / 2; // rows of a tile per half
   int const rb_n  = Rp / 4;
   int const items = rb_n * G;
   int const tiles = (Rr + kLineTile - 1) / kLineTile;
   int const chunks_per_row = Rp * int(sizeof(R)) / 16;
+  int const half = threadIdx.x / kLineItems, slot = threadIdx.x % kLineItems;
   auto issue = [&](int tile) {
     int const t0 = tile * kLineTile;
     int const nr = min(kLineTile, Rr - t0);
@@ -249,7 +257,7 @@ __device__ void dense_rows(const R *__restrict__ Mt, int Rr, int Rp, int G,
       cp_async16(reinterpret_cast<char *>(dst) + 16 * c, src + 16 * c);
     cp_async_commit();
   };
-  int const it0 = threadIdx.x, it1 = threadIdx.x + blockDim.x;
+  int const it0 = slot, it1 = slot + kLineItems;
   bool const has0 = it0 < items, has1 = it1 < items;
   int const rb0 = has0 ? it0 % rb_n : 0, g0 = has0 ? it0 / rb_n : 0;
   int const rb1 = has1 ? it1 % rb_n : 0, g1 = has1 ? it1 / rb_n : 0;
@@ -273,8 +281,12 @@ __device__ void dense_rows(const R *__restrict__ Mt, int Rr, int Rp, int G,
     int const t0 = tile * kLineTile;
     int const nr = min(kLineTile, Rr - t0);
     const R *qt  = qbuf + (tile & 1) * kLineTile * Rp;
-    for (int tt = 0; tt < nr; tt++)
+#pragma unroll
+    for (int th = 0; th < TH; th++)
     {
+      int const tt = half * TH + th;
+      if (tt >= nr)
+        break;
       int const t = t0 + tt;
       if (has0)
       {
@@ -303,6 +315,19 @@ __device__ void dense_rows(const R *__restrict__ Mt, int Rr, int Rp, int G,
     }
     __syncthreads(); // the buffer is refilled two tiles on
   }
+  auto at = [&](int r, int g, int c) { return out + (int64_t(r) * G + g) * NCP + c; };
+  auto park = [&](int rb, int g, R (&acc)[4][NC]) {
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+    {
+      int const r = 4 * rb + i;
+      if (r >= Rr)
+        break;
+#pragma unroll
+      for (int c = 0; c < NC; c++)
+        *at(r, g, c) = acc[i][c];
+    }
+  };
   auto finish = [&](int rb, int g, R (&acc)[4][NC]) {
 #pragma unroll
     for (int i = 0; i < 4; i++)
@@ -316,17 +341,28 @@ __device__ void dense_rows(const R *__restrict__ Mt, int Rr, int Rp, int G,
 #pragma unroll
       for (int c = 0; c < NC; c++)
       {
-        R v = acc[i][c];
+        R v = acc[i][c] + *at(r, g, c);
         if (theta)
           v = v / (shift - dt * (th + lamc[c]));
-        out[(int64_t(r) * G + g) * NCP + c] = v;
+        *at(r, g, c) = v;
       }
     }
   };
-  if (has0)
-    finish(rb0, g0, acc0);
-  if (has1)
-    finish(rb1, g1, acc1);
+  if (half == 1)
+  {
+    if (has0)
+      park(rb0, g0, acc0);
+    if (has1)
+      park(rb1, g1, acc1);
+  }
+  __syncthreads();
+  if (half == 0)
+  {
+    if (has0)
+      finish(rb0, g0, acc0);
+    if (has1)
+      finish(rb1, g1, acc1);
+  }
 }
 
 // One factor M_k^-1 (after B when bj) on the (pencil, group range) units.
@@ -1168,9 +1204,9 @@ int line_build(plan_data const &p, double dt, line_data **out, int64_t &bytes)
     for (size_t pe = 0; pe < pen_m.size(); pe++)
       if (!small(pen_m[pe]))
         rpmax = std::max(rpmax, trp[pen_tab[pe]]);
-    // a unit's (4-row block, group) items: at most two per thread; its
+    // a unit's (4-row block, group) items: at most two per item slot; its
     // rows x groups bound its shared memory
-    int const budget = std::max(rpmax, 4 * kLineThreads);
+    int const budget = std::max(rpmax, 4 * kLineItems);
     int max_rp       = 0;
     std::vector<int4> units, batches, bcells;
     int max_rows = 0;
