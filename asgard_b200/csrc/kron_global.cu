@@ -243,9 +243,13 @@ __global__ void __launch_bounds__(NW * 32)
 // the FP32 copy of x in the FP32 apply: 47 MB at d=6, level 7, held in L2
 // across the re-reads) and accumulates the 3x3 block's product in
 // registers; the warps' results meet in shared memory and are added in
-// dimension order with the Euler and beta terms (FP64 x and y).
-template<int D, typename TC, typename TX>
-__global__ void __launch_bounds__(D * 32)
+// dimension order with the Euler and beta terms (FP64 x and y).  The lane's
+// fibres are taken in PASSES passes over the warp's entries: with two, half
+// the accumulators are live, so six CTAs fit on an SM instead of four
+// (measured at d=6, level 7: 0.344 -> 0.317 ms with the conversion pass;
+// three or four passes spill and are slower).
+template<int D, typename TC, typename TX, int PASSES>
+__global__ void __launch_bounds__(D * 32, PASSES == 1 ? 4 : 6)
     kron_global_cell_dims(const int *__restrict__ order,
                      const int64_t *__restrict__ gptr,
                      const int *__restrict__ gseg, const int *__restrict__ gcol,
@@ -268,15 +272,23 @@ __global__ void __launch_bounds__(D * 32)
   int64_t const e0 = gptr[cell];
   int const sa = gseg[cell * (D + 1) + k], sb = gseg[cell * (D + 1) + k + 1];
   int const stride = dim_stride<D>(k);
-  int fb[FPL];
-  TC acc[FPL][3];
-#pragma unroll
-  for (int m = 0; m < FPL; m++)
+  // the lane's fibres f = lane + 32 m, m < FPL, in PASSES passes over the
+  // warp's entries (fewer live registers per pass, more warps per SM)
+  constexpr int FPP = (FPL + PASSES - 1) / PASSES;
+  TC *row = rows + k * TS;
+#pragma unroll 1
+  for (int pass = 0; pass < PASSES; pass++)
   {
-    int const f = lane + 32 * m;
+  int fb[FPP];
+  TC acc[FPP][3];
+#pragma unroll
+  for (int m = 0; m < FPP; m++)
+  {
+    int const f = lane + 32 * (pass * FPP + m);
     fb[m]       = (f / stride) * 3 * stride + (f % stride);
     acc[m][0] = acc[m][1] = acc[m][2] = TC(0);
   }
+  auto live = [&](int m) { return pass * FPP + m < FPL && lane + 32 * (pass * FPP + m) < NF; };
   auto entry = [&](int64_t j) {
     const TC *b  = B + int64_t(__ldg(gkb + j)) * PAD;
     const TX *xc = xs + int64_t(__ldg(gcol + j)) * TS;
@@ -297,16 +309,16 @@ __global__ void __launch_bounds__(D * 32)
       b0 = q0.x, b1 = q0.y, b2 = q1.x, b3 = q1.y, b4 = q2.x;
       b5 = q2.y, b6 = q3.x, b7 = q3.y, b8 = q4.x;
     }
-    TC v[FPL][3];
+    TC v[FPP][3];
 #pragma unroll
-    for (int m = 0; m < FPL; m++)
-      if (lane + 32 * m < NF)
+    for (int m = 0; m < FPP; m++)
+      if (live(m))
 #pragma unroll
         for (int p = 0; p < 3; p++)
           v[m][p] = static_cast<TC>(__ldg(xc + fb[m] + p * stride));
 #pragma unroll
-    for (int m = 0; m < FPL; m++)
-      if (lane + 32 * m < NF)
+    for (int m = 0; m < FPP; m++)
+      if (live(m))
       {
         // column-major block: out_q += sum_p A(q, p) v_p, A(q, p) = b[q + 3p]
         acc[m][0] = fma(b6, v[m][2], fma(b3, v[m][1], fma(b0, v[m][0], acc[m][0])));
@@ -316,15 +328,15 @@ __global__ void __launch_bounds__(D * 32)
   };
   for (int j = sa; j < sb; j++)
     entry(e0 + j);
-  TC *row = rows + k * TS;
 #pragma unroll
-  for (int m = 0; m < FPL; m++)
-    if (lane + 32 * m < NF)
+  for (int m = 0; m < FPP; m++)
+    if (live(m))
     {
       row[fb[m]]              = acc[m][0];
       row[fb[m] + stride]     = acc[m][1];
       row[fb[m] + 2 * stride] = acc[m][2];
     }
+  }
   __syncthreads();
   int64_t const base = int64_t(cell) * TS;
   for (int i = threadIdx.x; i < TS; i += D * 32)
@@ -632,7 +644,7 @@ int launch_global_d(plan_data const &p, double alpha, const double *x,
           ASGK_LAUNCHED();
         }
         p.gx32_src = nullptr;
-        kron_global_cell_dims<D, TC, float><<<p.rows, D * 32, 0, s>>>(
+        kron_global_cell_dims<D, TC, float, 2><<<p.rows, D * 32, 0, s>>>(
             p.gcell_order, p.gptr, p.gseg, p.gcol, p.gkb, B, alpha, p.gx32, x, beta, y,
             ex, g_gate);
       }
