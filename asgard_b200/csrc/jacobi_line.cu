@@ -749,7 +749,7 @@ __device__ __forceinline__ void small_column(line_args<R> const &a, R *buf,
 // line dimensions) follow in batch order, so the staging needs no chain of
 // dependent lookups.
 template<typename R, int D, int M, int KIDX>
-__global__ void __launch_bounds__(kSmallThreads, 4)
+__global__ void __launch_bounds__(kSmallThreads, 6)
     k_line_small(line_args<R> a, const int4 *__restrict__ batches,
                  const int4 *__restrict__ bcells, const double *in64,
                  const R *__restrict__ inR, double *__restrict__ out64,
