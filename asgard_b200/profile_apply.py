@@ -10,7 +10,7 @@ y = x - dt*K*x, then --reps timed applies (CUDA events on the launching
 stream) and prints one JSON line: ms per launch, algorithmic TFLOP/s
 (2*d*T*n^(d+1) flops per pair -- every cell pair in the dense form;
 2*n^(d+1) per single-direction pair in the global form) and the fraction of the measured FMA peak.
-This is the command the ncu summaries under profiles/ were taken with.
+The kernel summaries of this repository were taken with this command under ncu.
 """
 from __future__ import annotations
 

@@ -474,7 +474,7 @@ int asgk_imex_advance(asgk_plan *explicit_plan, asgk_plan *implicit_plan,
 /* ------------------------------------------------ learned preconditioner */
 
 /* A per-cell learned preconditioner (no counterpart in the reference, which
- * has none on this path; BASELINE's learned form).  4 layers of width
+ * has none on this path).  4 layers of width
  * `hidden` with GELU: the cell's residual block (scaled to unit norm) passes
  * through 4 linear layers whose hidden activations are gated elementwise by
  * GELU gates computed from the cell's level multi-index, so the network is
