@@ -664,7 +664,7 @@ __device__ __forceinline__ void lds4(const double *p, double (&q)[4])
 template<typename R, int D, int M, int KIDX, int MC>
 __device__ __forceinline__ void small_column(line_args<R> const &a, R *buf,
                                              int slot0, int fb, unsigned dig,
-                                             int stk, const R *Qm, const R *th,
+                                             int stk, const R *Qm, const R *inv,
                                              bool bj, const R (*s_Sk)[9],
                                              const R (*s_lam)[2][3])
 {
@@ -712,9 +712,13 @@ __device__ __forceinline__ void small_column(line_args<R> const &a, R *buf,
       fma_pair(q[0], q[1], x[t], u[4 * r4], u[4 * r4 + 1]);
       fma_pair(q[2], q[3], x[t], u[4 * r4 + 2], u[4 * r4 + 3]);
     }
+  // 1 / (mu - dt theta_r) from the batch's table: this pencil, this
+  // column's digits in the other line dimensions
+  unsigned const combo = (M == 3) ? (dig & 3u) + 3u * ((dig >> 2) & 3u) : (M == 2 ? (dig & 3u) : 0u);
+  const R *iv = inv + combo * (3 * kSmallCells) + (slot0 / MC) * RR;
 #pragma unroll
   for (int r = 0; r < RR; r++)
-    u[r] = u[r] / (mu - a.dt * th[r]);
+    u[r] = u[r] * iv[r];
   // two outputs (rows t, t + 1 of Qm) per pass
 #pragma unroll
   for (int t = 0; t < RR; t += 2)
@@ -776,6 +780,13 @@ __global__ void __launch_bounds__(kSmallThreads, 6)
   __shared__ R s_P[kSmallCells][2][9];
   __shared__ R s_lam[kSmallCells][2][3];
   __shared__ R s_Sk[kSmallCells][9];
+  // 1 / (mu - dt theta_r) per digit combination of the other line
+  // dimensions, pencil and eigenmode (pencils x modes = 3 x cells <= 24)
+  __shared__ R s_inv[9 * 3 * kSmallCells];
+  // with three line dimensions: the first entries of the 3 x 3 blocks the
+  // two other line dimensions span (one item of the merged column stage)
+  constexpr int NB9 = TS / 9 > 0 ? TS / 9 : 1;
+  __shared__ short s_b9[NB9];
   int4 const bt  = batches[blockIdx.x];
   int const npen = bt.x, MC = bt.y;
   int const nc   = npen * MC;
@@ -819,66 +830,138 @@ __global__ void __launch_bounds__(kSmallThreads, 6)
     }
     s_dig[fi] = (unsigned char)dg;
   }
-  __syncthreads();
-  // stage the cells: kStageLoads independent loads per thread are issued
-  // before their values are used, so enough of them are in flight
-  int const ntot = nc * TS;
-  if (in64)
+  int const o0 = 0 < KIDX ? 0 : 1, o1 = 1 < KIDX ? 1 : 2; // the other line dims
+  if constexpr (M == 3)
   {
-    double const f = scale_state ? scale_state[1] : 1.0;
-    for (int e0 = tid; e0 < ntot; e0 += kStageLoads * kSmallThreads)
+    for (int u = tid; u < NB9; u += blockDim.x)
     {
-      double v[kStageLoads];
-#pragma unroll
-      for (int u = 0; u < kStageLoads; u++)
+      int rem = u, idx = 0;
+      for (int dim = D - 1; dim >= 0; dim--)
       {
-        int const e = e0 + u * kSmallThreads;
-        if (e < ntot)
-          v[u] = in64[int64_t(s_cell[e / TS]) * TS + e % TS];
+        if (dim == a.line[o0] || dim == a.line[o1])
+          continue;
+        idx += (rem % 3) * ipow3l(D - 1 - dim);
+        rem /= 3;
       }
-#pragma unroll
-      for (int u = 0; u < kStageLoads; u++)
-      {
-        int const e = e0 + u * kSmallThreads;
-        if (e >= ntot)
-          break;
-        double vv = v[u];
-        if (scale_state)
-        {
-          int64_t const gi = int64_t(s_cell[e / TS]) * TS + e % TS;
-          vv *= f;
-          vscale[gi] = vv;
-          if (vcopy)
-            vcopy[gi] = float(vv);
-        }
-        buf[e] = R(vv);
-      }
+      s_b9[u] = short(idx);
     }
   }
-  else
+  __syncthreads();
   {
-    for (int e0 = tid; e0 < ntot; e0 += kStageLoads * kSmallThreads)
+    constexpr int NCMB = M == 3 ? 9 : (M == 2 ? 3 : 1);
+    int const per = npen * RR;
+    for (int e = tid; e < NCMB * per; e += blockDim.x)
     {
-      R v[kStageLoads];
-#pragma unroll
-      for (int u = 0; u < kStageLoads; u++)
+      int const combo = e / per, rem = e - combo * per;
+      int const pi = rem / RR, r = rem - pi * RR;
+      int const slot0 = pi * MC;
+      unsigned const dig = (M == 3) ? unsigned(combo % 3) | (unsigned(combo / 3) << 2)
+                                    : unsigned(combo);
+      R mu = a.shift;
+      for (int qq = 0; qq < M - 1; qq++)
+        mu -= a.dt * s_lam[slot0][qq][(dig >> (2 * qq)) & 3u];
+      s_inv[combo * (3 * kSmallCells) + rem] = R(1) / (mu - a.dt * s_th[r]);
+    }
+  }
+  // stage the cells, a warp per cell: kStageLoads independent loads per
+  // thread are issued before their values are used, so enough of them are
+  // in flight
+  constexpr int PER = (TS + 31) / 32;
+  int const warp = tid >> 5, lane = tid & 31;
+  for (int c = warp; c < nc; c += kSmallThreads / 32)
+  {
+    int64_t const gb = int64_t(s_cell[c]) * TS;
+    R *bc            = buf + c * TS;
+    for (int j0 = 0; j0 < PER; j0 += kStageLoads)
+    {
+      if (in64)
       {
-        int const e = e0 + u * kSmallThreads;
-        if (e < ntot)
-          v[u] = inR[int64_t(s_cell[e / TS]) * TS + e % TS];
+        double v[kStageLoads];
+#pragma unroll
+        for (int u = 0; u < kStageLoads; u++)
+        {
+          int const i = lane + 32 * (j0 + u);
+          if (j0 + u < PER && i < TS)
+            v[u] = in64[gb + i];
+        }
+        double const f = scale_state ? scale_state[1] : 1.0;
+#pragma unroll
+        for (int u = 0; u < kStageLoads; u++)
+        {
+          int const i = lane + 32 * (j0 + u);
+          if (j0 + u < PER && i < TS)
+          {
+            double vv = v[u];
+            if (scale_state)
+            {
+              vv *= f;
+              vscale[gb + i] = vv;
+              if (vcopy)
+                vcopy[gb + i] = float(vv);
+            }
+            bc[i] = R(vv);
+          }
+        }
       }
-#pragma unroll
-      for (int u = 0; u < kStageLoads; u++)
+      else
       {
-        int const e = e0 + u * kSmallThreads;
-        if (e < ntot)
-          buf[e] = v[u];
+        R v[kStageLoads];
+#pragma unroll
+        for (int u = 0; u < kStageLoads; u++)
+        {
+          int const i = lane + 32 * (j0 + u);
+          if (j0 + u < PER && i < TS)
+            v[u] = inR[gb + i];
+        }
+#pragma unroll
+        for (int u = 0; u < kStageLoads; u++)
+        {
+          int const i = lane + 32 * (j0 + u);
+          if (j0 + u < PER && i < TS)
+            bc[i] = v[u];
+        }
       }
     }
   }
   __syncthreads();
   // W^T (forward) or W (backward): fibre stages along the other line dimensions
   auto other_stages = [&](bool forward) {
+    if constexpr (M == 3)
+    {
+      // both other line dimensions in one pass over 3 x 3 blocks: along the
+      // first (qq = 0), then the second, the same sums as two passes
+      int const s1 = a.st_line[o0], s2 = a.st_line[o1];
+      for (int it = tid; it < nc * NB9; it += blockDim.x)
+      {
+        int const slot = it / NB9, u = it - slot * NB9;
+        int const base = slot * TS + s_b9[u];
+        R v[3][3];
+#pragma unroll
+        for (int d1 = 0; d1 < 3; d1++)
+#pragma unroll
+          for (int d2 = 0; d2 < 3; d2++)
+            v[d1][d2] = buf[base + d1 * s1 + d2 * s2];
+        const R *P = s_P[slot][0];
+        R w[3][3];
+#pragma unroll
+        for (int d2 = 0; d2 < 3; d2++)
+#pragma unroll
+          for (int o = 0; o < 3; o++)
+            w[o][d2] = forward ? P[3 * o] * v[0][d2] + P[3 * o + 1] * v[1][d2] + P[3 * o + 2] * v[2][d2]
+                               : P[o] * v[0][d2] + P[o + 3] * v[1][d2] + P[o + 6] * v[2][d2];
+        P = s_P[slot][1];
+#pragma unroll
+        for (int d1 = 0; d1 < 3; d1++)
+#pragma unroll
+          for (int o = 0; o < 3; o++)
+            buf[base + d1 * s1 + o * s2] =
+                forward ? P[3 * o] * w[d1][0] + P[3 * o + 1] * w[d1][1] + P[3 * o + 2] * w[d1][2]
+                        : P[o] * w[d1][0] + P[o + 3] * w[d1][1] + P[o + 6] * w[d1][2];
+      }
+      __syncthreads();
+    }
+    else
+    {
     for (int qq = 0; qq < M - 1; qq++)
     {
       int const sj = a.st_line[qq < KIDX ? qq : qq + 1];
@@ -895,6 +978,7 @@ __global__ void __launch_bounds__(kSmallThreads, 6)
       }
       __syncthreads();
     }
+    }
   };
   other_stages(true);
   // the pencil solves, one column (fibre along k) per item
@@ -903,25 +987,29 @@ __global__ void __launch_bounds__(kSmallThreads, 6)
     int const pi = it / NF, fi = it - pi * NF;
     switch (MC)
     {
-    case 1: small_column<R, D, M, KIDX, 1>(a, buf, pi, s_fbk[fi], s_dig[fi], stk, s_Q, s_th, bj, s_Sk, s_lam); break;
-    case 2: small_column<R, D, M, KIDX, 2>(a, buf, pi * 2, s_fbk[fi], s_dig[fi], stk, s_Q, s_th, bj, s_Sk, s_lam); break;
-    case 4: small_column<R, D, M, KIDX, 4>(a, buf, pi * 4, s_fbk[fi], s_dig[fi], stk, s_Q, s_th, bj, s_Sk, s_lam); break;
-    default: small_column<R, D, M, KIDX, 8>(a, buf, pi * 8, s_fbk[fi], s_dig[fi], stk, s_Q, s_th, bj, s_Sk, s_lam); break;
+    case 1: small_column<R, D, M, KIDX, 1>(a, buf, pi, s_fbk[fi], s_dig[fi], stk, s_Q, s_inv, bj, s_Sk, s_lam); break;
+    case 2: small_column<R, D, M, KIDX, 2>(a, buf, pi * 2, s_fbk[fi], s_dig[fi], stk, s_Q, s_inv, bj, s_Sk, s_lam); break;
+    case 4: small_column<R, D, M, KIDX, 4>(a, buf, pi * 4, s_fbk[fi], s_dig[fi], stk, s_Q, s_inv, bj, s_Sk, s_lam); break;
+    default: small_column<R, D, M, KIDX, 8>(a, buf, pi * 8, s_fbk[fi], s_dig[fi], stk, s_Q, s_inv, bj, s_Sk, s_lam); break;
     }
   }
   __syncthreads();
   other_stages(false);
-  for (int e = tid; e < nc * TS; e += blockDim.x)
+  for (int c = warp; c < nc; c += kSmallThreads / 32)
   {
-    int64_t const gi = int64_t(s_cell[e / TS]) * TS + e % TS;
-    if (out64)
+    int64_t const gb = int64_t(s_cell[c]) * TS;
+    const R *bc      = buf + c * TS;
+    for (int i = lane; i < TS; i += 32)
     {
-      out64[gi] = double(buf[e]);
-      if (zcopy)
-        zcopy[gi] = float(buf[e]);
+      if (out64)
+      {
+        out64[gb + i] = double(bc[i]);
+        if (zcopy)
+          zcopy[gb + i] = float(bc[i]);
+      }
+      else
+        outR[gb + i] = bc[i];
     }
-    else
-      outR[gi] = buf[e];
   }
 }
 
