@@ -391,7 +391,12 @@ __global__ void __launch_bounds__(kLineThreads)
   int const Rr   = 3 * m;
   int const Rp   = a.tab_rp[tab];
   const int *cells = a.pen_cells + a.pen_off[pen];
-  R *X    = reinterpret_cast<R *>(line_smem);
+  // per (member, group): its cell's offset plus the group's digits in the
+  // vector, and its first row of X -- so gathering and scattering divide by
+  // no run-time size
+  int64_t *s_rowoff = reinterpret_cast<int64_t *>(line_smem);
+  int *s_xrow       = reinterpret_cast<int *>(s_rowoff + m * G);
+  R *X = reinterpret_cast<R *>(line_smem + ((12 * size_t(m) * G + 15) / 16) * 16);
   R *Y    = X + int64_t(Rp) * G * NCP;
   R *qbuf = Y + int64_t(Rp) * G * NCP; // 2 tiles of kLineTile matrix rows
   __shared__ int s_offg[27];
@@ -438,18 +443,23 @@ __global__ void __launch_bounds__(kLineThreads)
     s_S[q][e] = sf[12 + e];
   }
   __syncthreads();
+  for (int it = threadIdx.x; it < m * G; it += blockDim.x)
+  {
+    int const i  = it / G, g = it - i * G;
+    s_rowoff[it] = int64_t(__ldg(cells + i)) * TS + s_offg[g];
+    s_xrow[it]   = (i * 3 * G + g) * NCP;
+  }
+  __syncthreads();
   int const stk = ipow3l(D - 1 - a.k);
   double const f = scale_state ? scale_state[1] : 1.0;
   // gather (row = member * 3 + k polynomial, group, column); kGatherLoads
   // independent loads per thread are issued before their values are used
   int const nload = m * G * 3 * NC;
   auto gidx = [&](int e, int &xo) {
-    int const c  = e % NC;
-    int const pk = (e / NC) % 3;
-    int const g  = (e / (3 * NC)) % G;
-    int const i  = e / (3 * NC * G);
-    xo           = ((i * 3 + pk) * G + g) * NCP + c;
-    return int64_t(__ldg(cells + i)) * TS + s_offg[g] + s_offc[c] + pk * stk;
+    int const ig = e / (3 * NC), w = e - ig * (3 * NC);
+    int const pk = w / NC, c = w - pk * NC;
+    xo           = s_xrow[ig] + pk * G * NCP + c;
+    return s_rowoff[ig] + s_offc[c] + pk * stk;
   };
   for (int e0 = threadIdx.x; e0 < nload; e0 += kGatherLoads * kLineThreads)
   {
@@ -607,12 +617,9 @@ __global__ void __launch_bounds__(kLineThreads)
   // scatter
   for (int e = threadIdx.x; e < nload; e += blockDim.x)
   {
-    int const c  = e % NC;
-    int const pk = (e / NC) % 3;
-    int const g  = (e / (3 * NC)) % G;
-    int const i  = e / (3 * NC * G);
-    int64_t const gi = int64_t(cells[i]) * TS + s_offg[g] + s_offc[c] + pk * stk;
-    R const val = X[((int64_t(i) * 3 + pk) * G + g) * NCP + c];
+    int xo;
+    int64_t const gi = gidx(e, xo);
+    R const val      = X[xo];
     if (out64)
     {
       out64[gi] = double(val);
@@ -1413,7 +1420,10 @@ int launch_factor(line_data const &ld, line_factor const &f, const double *in64,
   }
   if (f.nunits > 0)
   {
-    size_t const shm = sizeof(R) * (2 * size_t(f.max_rows) * NCP +
+    // the (member, group) tables (members x groups <= max_rows / 3), X, Y and
+    // the matrix tiles
+    size_t const shm = ((12 * (size_t(f.max_rows) / 3 + 1) + 15) / 16) * 16 +
+                       sizeof(R) * (2 * size_t(f.max_rows) * NCP +
                                     2 * size_t(kLineTile) * f.max_rp);
     auto kern        = k_line_factor<R, D, M, KIDX>;
     ASGK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
