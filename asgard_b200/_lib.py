@@ -32,7 +32,7 @@ EXPORTS = [
     "asgk_gmres_euler_jacobi",
     "asgk_mlp_set_base", "asgk_implicit_advance", "asgk_set_gmres_graphs",
     "asgk_set_gmres_basis", "asgk_set_gmres_node_steps", "asgk_imex_advance",
-    "asgk_set_gmres_fused_copy",
+    "asgk_set_gmres_fused_copy", "asgk_set_bf16_inner_tol",
 ]
 
 
@@ -113,6 +113,7 @@ def _load():
         "asgk_set_gmres_graphs": ([_i], _i),
         "asgk_set_gmres_basis": ([_i], _i),
         "asgk_set_gmres_fused_copy": ([_i], _i),
+        "asgk_set_bf16_inner_tol": ([_d], _d),
         "asgk_set_gmres_node_steps": ([_i], _i),
         "asgk_implicit_advance": ([_vp, _d, _vp, _i, _vp, _i64, _i, _i, _d, _i, _i, _i, _vp, C.POINTER(GmresInfo), _vp], _i),
         "asgk_imex_advance": ([_vp, _vp, _d, _vp, _i, _i, _i, _d, _i, _i, _vp, _vp, _vp, _vp,

@@ -74,6 +74,7 @@ void free_plan(plan_data &p)
   cudaFree(p.gwork);
   cudaFree(p.vP64);
   cudaFree(p.vP32);
+  tc_free(p.tc);
   p = plan_data{};
 }
 
@@ -199,6 +200,8 @@ int upload_global_blocks(plan_data &p, std::vector<double> const &B)
                        cudaMemcpyHostToDevice));
   ASGK_CUDA(cudaMemcpy(p.gB32, B32.data(), sizeof(float) * B32.size(),
                        cudaMemcpyHostToDevice));
+  if (p.tc != nullptr)
+    return tc_refresh(p, *p.tc);
   return ASGK_OK;
 }
 
@@ -512,6 +515,10 @@ bool g_gmres_fused_copy = true; // asgk_set_gmres_fused_copy
 // level 7 a 138-iteration solve took 9.85 / 8.49 / 8.33 / 8.23 ms with 1 / 4
 // / 8 / 16 (node boundaries cost ~10 us, a skipped launch ~1 us)
 int g_gmres_node_steps  = 16;
+// relative tolerance of the inner solves with the BF16 tensor-core operator
+// (asgk_set_bf16_inner_tol): its products carry BF16-rounded operands, so an
+// inner solve far below that rounding gains the refinement nothing
+double g_bf16_inner_rtol = 1e-3;
 
 // Device workspace of a GMRES solve, kept on the plan between solves.
 struct gmres_ws
@@ -2204,8 +2211,13 @@ int gmres_euler_impl(asgk_plan *plan, double dt, double *x, const double *b,
   auto &p = plan->p;
   if (p.rows != p.cols)
     return ASGK_ERR_INVALID;
-  if (precision != ASGK_FP64 && precision != ASGK_FP32)
+  if (precision != ASGK_FP64 && precision != ASGK_FP32 && precision != ASGK_BF16)
     return ASGK_ERR_UNSUPPORTED;
+  // the tensor-core operator exists for global plans; its set-up (host work,
+  // allocations) happens here, before any cycle is recorded
+  if (precision == ASGK_BF16)
+    if (int rc = tc_prepare(p))
+      return rc;
   int64_t const n = int64_t(p.rows) * p.tensor;
   if (restart <= 0)
     restart = asgk_default_gmres_restarts(n);
@@ -2273,7 +2285,10 @@ int gmres_euler_impl(asgk_plan *plan, double dt, double *x, const double *b,
   {
     // FP64 iterative refinement: r = b - A x in FP64, inner (flexible) GMRES
     // on A e = r with the low-precision operator, x += e.
-    double const inner_rtol = (precision == ASGK_FP64) ? 1e-10 : 1e-5;
+    // inner tolerances: about the operator's rounding (FP32 2^-24, BF16
+    // operands 2^-9), below which an inner solve gains nothing
+    double const inner_rtol =
+        (precision == ASGK_FP64) ? 1e-10 : (precision == ASGK_FP32 ? 1e-5 : g_bf16_inner_rtol);
     int total = 0, low = 0, fp64 = 0, pcalls = 0, steps = 0, fallback = 0;
     double rnorm = 0, prev_rnorm = 0;
     int const max_steps = 50;
@@ -2555,6 +2570,14 @@ int asgk_set_gmres_fused_copy(int on)
 {
   int const old      = g_gmres_fused_copy ? 1 : 0;
   g_gmres_fused_copy = (on != 0);
+  return old;
+}
+
+double asgk_set_bf16_inner_tol(double rtol)
+{
+  double const old = g_bf16_inner_rtol;
+  if (rtol > 0 && rtol < 1)
+    g_bf16_inner_rtol = rtol;
   return old;
 }
 

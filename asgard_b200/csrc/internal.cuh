@@ -76,6 +76,9 @@ enum class index_mode : int
   conn     = 1  // conn[p*d + k]*(d*T*n*n) + (t*d + k)*n*n: sparse-grid layout
 };
 
+// kron_tc.cu: the tensor-core (BF16) form of a global plan's operator
+struct tc_data;
+
 // Device-resident operator.  Pairs are grouped by output cell (CSR) and the
 // cells are visited in order of decreasing pair count.
 struct plan_data
@@ -153,6 +156,10 @@ struct plan_data
   unsigned char *gd_rel = nullptr; // neighbour's 1D cell: 0 before, 1 same, 2 after
   double *gwork = nullptr;         // 2 * gchains * rows * n^d values
   int64_t gchain_entries = 0;      // neighbour entries the chains' stages visit
+
+  // the tensor-core form of a global plan (precision ASGK_BF16): pencils,
+  // their BF16 class matrices and its vectors, built on first use
+  mutable tc_data *tc = nullptr;
 
   // dense mode (every (row, col) pair): a conn-mode plan whose connection
   // index in dimension k is elem_col[k] * dense_nb + elem_row[k], the factors
@@ -236,6 +243,18 @@ int line_info(line_data const &ld, int *dims);
 int launch_global(plan_data const &p, int precision, double alpha,
                   const double *x, double beta, double *y, double ex,
                   cudaStream_t s);
+
+// kron_tc.cu: the tensor-core form (tcgen05, BF16 operands, FP32 TMEM
+// accumulators) of a global plan whose terms act in one dimension each.
+// tc_prepare builds it once (host work and allocations: call it outside
+// stream capture); tc_refresh rewrites its matrices after new values.
+int tc_build(plan_data const &p, tc_data **out);
+int tc_prepare(plan_data const &p);
+int tc_refresh(plan_data const &p, tc_data &t);
+void tc_free(tc_data *t);
+int tc_read_error(int reset, int *code);
+int launch_global_tc(plan_data const &p, double alpha, const double *x, double beta,
+                     double *y, double ex, cudaStream_t s);
 
 // kron_staged.cu: n = 3, d = 3/4 apply with bulk-copied x tensors
 bool staged_supported(plan_data const &p);

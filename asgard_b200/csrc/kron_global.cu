@@ -727,6 +727,12 @@ int launch_global(plan_data const &p, int precision, double alpha,
     rc = launch_global_t<double>(p, alpha, x, beta, y, ex_eff, s);
   else if (precision == ASGK_FP32)
     rc = launch_global_t<float>(p, alpha, x, beta, y, ex_eff, s);
+  else if (precision == ASGK_BF16)
+  {
+    rc = tc_prepare(p);
+    if (rc == ASGK_OK)
+      rc = launch_global_tc(p, alpha, x, beta, y, ex_eff, s);
+  }
   p.gx32_src = nullptr; // a preconditioner's copy serves the next apply only
   return rc;
 }

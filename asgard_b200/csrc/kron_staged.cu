@@ -559,7 +559,11 @@ int read_device_error(int reset, int *code)
     int const zero = 0;
     ASGK_CUDA(cudaMemcpyToSymbol(g_device_error, &zero, sizeof(int)));
   }
-  *code = v;
+  // the tensor-core kernels keep their own word
+  int w = 0;
+  if (int rc = tc_read_error(reset, &w))
+    return rc;
+  *code = (v != 0) ? v : w;
   return ASGK_OK;
 }
 

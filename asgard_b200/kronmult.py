@@ -453,14 +453,18 @@ def launch_count() -> int:
     return lib.asgk_launch_count()
 
 
-def gmres_settings(graphs=None, node_steps=None, fp32_basis=None) -> dict:
+def gmres_settings(graphs=None, node_steps=None, fp32_basis=None,
+                   bf16_inner_tol=None) -> dict:
     """Process-wide settings of the device GMRES (asgk_set_gmres_graphs,
-    asgk_set_gmres_node_steps, asgk_set_gmres_basis): restart cycles recorded
-    as CUDA graphs, Arnoldi steps per recorded graph node, and whether the
-    FP32 inner solves orthogonalise against an FP32 copy of the basis.  The
-    arguments given are set; returns the settings in force before the call
-    (pass the dict back as keyword arguments to restore them).  None of them
-    changes iterates except fp32_basis."""
+    asgk_set_gmres_node_steps, asgk_set_gmres_basis,
+    asgk_set_bf16_inner_tol): restart cycles recorded as CUDA graphs, Arnoldi
+    steps per recorded graph node, whether the FP32 inner solves orthogonalise
+    against an FP32 copy of the basis, and the inner tolerance of the BF16
+    tensor-core solves.  The arguments given are set; returns the settings in
+    force before the call (pass the dict back as keyword arguments to restore
+    them).  None of them changes iterates except fp32_basis and
+    bf16_inner_tol."""
+    old_tol = lib.asgk_set_bf16_inner_tol(bf16_inner_tol if bf16_inner_tol is not None else 0.0)
     old_steps = lib.asgk_set_gmres_node_steps(node_steps if node_steps is not None else 0)
     if graphs is None:
         old_graphs = lib.asgk_set_gmres_graphs(1)
@@ -473,7 +477,7 @@ def gmres_settings(graphs=None, node_steps=None, fp32_basis=None) -> dict:
     else:
         old_basis = lib.asgk_set_gmres_basis(1 if fp32_basis else 0)
     return {"graphs": bool(old_graphs), "node_steps": old_steps,
-            "fp32_basis": bool(old_basis)}
+            "fp32_basis": bool(old_basis), "bf16_inner_tol": old_tol}
 
 
 __all__ = ["kronmult_matrix", "simple_gmres_euler", "simple_gmres", "cgs_step",

@@ -100,6 +100,13 @@ def main():
            "dofs": op.N, "ms_per_launch": ms, "tflops": flops / ms / 1e9,
            "flops_per_launch": flops, "setup_s": t_setup,
            "device_bytes": mat.device_bytes()}
+    if args.precision != "fp64":
+        # the low-precision product K x against the FP64 one on the same x
+        y64, ylo = torch.zeros_like(x), torch.zeros_like(x)
+        mat.apply(1.0, x, 0.0, y64, precision="fp64")
+        mat.apply(1.0, x, 0.0, ylo, precision=args.precision)
+        torch.cuda.synchronize()
+        out["rel_err_vs_fp64"] = float(torch.linalg.norm(ylo - y64) / torch.linalg.norm(y64))
     if args.peak:
         pk = C.c_double()
         ab.lib.asgk_measure_fma_peak(0 if args.precision == "fp64" else 1, C.byref(pk))

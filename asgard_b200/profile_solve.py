@@ -31,7 +31,9 @@ def main():
                          "by the host builder; mode pairs only")
     ap.add_argument("--mode", default="global", choices=["pairs", "global"])
     ap.add_argument("--precond", default="block", choices=["none", "point", "block", "kron", "line"])
-    ap.add_argument("--precision", default="fp32", choices=["fp64", "fp32"])
+    ap.add_argument("--precision", default="fp32", choices=["fp64", "fp32", "bf16"])
+    ap.add_argument("--bf16-inner-tol", type=float, default=0.0,
+                    help="inner relative tolerance of the bf16 solves (0: the default)")
     ap.add_argument("--restart", type=int, default=50)
     ap.add_argument("--tol", type=float, default=1e-10)
     ap.add_argument("--solves", type=int, default=3)
@@ -65,7 +67,8 @@ def main():
     import asgard_b200 as ab
 
     ab.gmres_settings(graphs=not args.no_graphs, fp32_basis=args.basis == "fp32",
-                      node_steps=args.node_steps if args.node_steps > 0 else None)
+                      node_steps=args.node_steps if args.node_steps > 0 else None,
+                      bf16_inner_tol=args.bf16_inner_tol if args.bf16_inner_tol > 0 else None)
     t0 = time.perf_counter()
     if args.device_build:
         from asgard_b200.operators import factor_values
@@ -174,6 +177,7 @@ def main():
                       "precision": args.precision, "dofs": op.N,
                       "s_per_solve": s, "solves_per_s": 1.0 / s,
                       "iterations": [i.iterations for i in infos],
+                      "outer_steps": [i.outer_steps for i in infos],
                       "true_relres": max(i.true_relres for i in infos),
                       "ms_per_iteration": s * 1e3 / (sum(i.iterations for i in infos) / len(infos)),
                       "setup_s": setup}))

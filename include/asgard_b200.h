@@ -393,6 +393,15 @@ int asgk_set_gmres_basis(int fp32);
  * returns the previous setting.  No counterpart in the reference. */
 int asgk_set_gmres_fused_copy(int on);
 
+/* Relative tolerance of each inner solve of iterative refinement with the
+ * BF16 tensor-core operator (precision ASGK_BF16; default 1e-3): the
+ * operator's products use BF16-rounded operands (relative rounding 2^-9), so
+ * every refinement step removes about that fraction of the residual, and an
+ * inner solve far below it only adds iterations.  rtol outside (0, 1) only
+ * reads the setting.  Process-wide; returns the previous setting.  No
+ * counterpart in the reference. */
+double asgk_set_bf16_inner_tol(double rtol);
+
 /* ------------------------------------------------ implicit time loop */
 
 typedef enum asgk_pc_kind

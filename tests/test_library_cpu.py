@@ -57,13 +57,17 @@ def test_gmres_settings_set_and_restore():
     reported back, and the restore from the returned dict."""
     import asgard_b200 as ab
     old = ab.gmres_settings()
-    assert old == {"graphs": True, "node_steps": 16, "fp32_basis": True}
+    assert old == {"graphs": True, "node_steps": 16, "fp32_basis": True,
+                   "bf16_inner_tol": 1e-3}
     try:
-        assert ab.gmres_settings(graphs=False, node_steps=3, fp32_basis=False) == old
+        assert ab.gmres_settings(graphs=False, node_steps=3, fp32_basis=False,
+                                 bf16_inner_tol=1e-2) == old
         assert ab.gmres_settings() == {"graphs": False, "node_steps": 3,
-                                       "fp32_basis": False}
+                                       "fp32_basis": False, "bf16_inner_tol": 1e-2}
         ab.gmres_settings(node_steps=0)  # below 1: only read
         assert ab.gmres_settings()["node_steps"] == 3
+        ab.gmres_settings(bf16_inner_tol=2.0)  # outside (0, 1): only read
+        assert ab.gmres_settings()["bf16_inner_tol"] == 1e-2
     finally:
         ab.gmres_settings(**old)
     assert ab.gmres_settings() == old
