@@ -92,6 +92,9 @@ def parse():
                              "learned-fp64", "fp32", "fp64"])
     ap.add_argument("--operator", default="global", choices=["global", "pairs"],
                     help="the method's operator form (plain FP64 always uses pairs)")
+    ap.add_argument("--form-steps", type=int, default=3,
+                    help="timed solves of the method with its inner operator in "
+                         "FP32 and in BF16 on the tensor cores (0: skip)")
     ap.add_argument("--train-solves", type=int, default=1)
     ap.add_argument("--train-epochs", type=int, default=60)
     return ap.parse_args()
@@ -558,6 +561,13 @@ def main():
                        "iterations": [i.iterations for i in qinfos],
                        "true_relres": max(i.true_relres for i in qinfos)}
 
+    # ---- the inner operator in FP32 (CUDA cores) and in BF16 (tensor
+    # cores): its error against the FP64 product and the method's solves
+    forms = None
+    if gmat is not None and args.form_steps > 0:
+        forms = precision_forms(op, gmat, method, dt, B, args.form_steps, solve,
+                                plain_value)
+
     roofline = rooflines(ab, op, mat, gmat, method, dt, args.workload, B[0])
 
     # ---- CPU baseline (rank 0, N = 1): the reference's own solve
@@ -596,11 +606,88 @@ def main():
                     "steps": e2e_steps},
             "gpu_launches": launches,
             "pair_operator_method": pair_method,
+            "precision_forms": forms,
             "roofline": roofline,
             "cpu_baseline": cpu,
         }
         print(json.dumps(line))
     replicas.shutdown()
+
+
+def pencil_gemm_flops(op):
+    """Useful flops of the tensor-core form per apply: along each dimension
+    with terms, every pencil of p cells is a (3p x 3p) by (3p x 3^(d-1))
+    product (2 flops per multiply-add; padding not counted)."""
+    import numpy as np
+    t = op.table.astype(np.int64)
+    d, fib = op.d, 3 ** (op.d - 1)
+    total = 0
+    for k in sorted({tt % d for tt in range(op.terms)}):
+        keep = [j for j in range(d) if j != k] + [d + j for j in range(d) if j != k]
+        _, counts = np.unique(t[:, keep], axis=0, return_counts=True)
+        total += int((2 * (3 * counts) ** 2 * fib).sum())
+    return total
+
+
+def _bf16_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["bf16_tflops"]), "MEASURED_PEAKS.json bf16_tflops"
+    except (OSError, KeyError, ValueError):
+        return 1590.0, "fallback 1.59 PFLOP/s"
+
+
+def precision_forms(op, gmat, method, dt, B, steps, solve, plain_value):
+    """The method (its preconditioner, FP64 refinement, recorded cycles) with
+    the inner operator in FP32 on the CUDA cores and in BF16 on the tensor
+    cores (FP32 accumulation): the inner product's relative error against
+    the FP64 product on a seeded x, the apply time, and `steps` timed solves
+    to the FP64 relative residual (each recomputed in FP64)."""
+    import torch
+    x = B[0]
+    y64 = torch.zeros_like(x)
+    gmat.apply(1.0, x, 0.0, y64, precision="fp64")
+    ys = torch.zeros_like(x)
+    out = {}
+    for prec in ("fp32", "bf16"):
+        gmat.apply(1.0, x, 0.0, ys, precision=prec)
+        torch.cuda.synchronize()
+        err = float(torch.linalg.norm(ys - y64) / torch.linalg.norm(y64))
+        a0 = torch.cuda.Event(enable_timing=True)
+        a1 = torch.cuda.Event(enable_timing=True)
+        a0.record()
+        for _ in range(10):
+            gmat.apply_euler(dt, 1.0, x, 0.0, ys, precision=prec)
+        a1.record()
+        torch.cuda.synchronize()
+        apply_ms = a0.elapsed_time(a1) / 10
+        solve(B[0], prec, method["precond"])        # warm-up: records the cycles
+        torch.cuda.synchronize()
+        a0.record()
+        infos = [solve(B[(1 + i) % len(B)], prec, method["precond"])[1]
+                 for i in range(steps)]
+        a1.record()
+        torch.cuda.synchronize()
+        sec = a0.elapsed_time(a1) / 1e3
+        out[prec] = {"operator_rel_err_vs_fp64": err, "apply_ms": apply_ms,
+                     "value": steps / sec, "unit": "solves/s",
+                     "iterations": [i.iterations for i in infos],
+                     "outer_steps": [i.outer_steps for i in infos],
+                     "true_relres": max(i.true_relres for i in infos),
+                     "speedup_vs_plain": (steps / sec / plain_value
+                                          if plain_value else None)}
+    flops = pencil_gemm_flops(op)
+    peak, src = _bf16_peak()
+    ms = out["bf16"]["apply_ms"]
+    out["bf16"]["tensor"] = {"kernel": f"k_tc_pencil<d={op.d}> (tcgen05.mma kind::f16, "
+                                       f"+ BF16 conversion of x)",
+                             "useful_flops_per_apply": flops,
+                             "achieved": flops / ms / 1e9, "peak": peak,
+                             "peak_source": src, "unit": "TFLOP/s",
+                             "frac": flops / ms / 1e9 / peak}
+    out["inner"] = ("FP64 iterative refinement; inner flexible GMRES to 1e-5 (fp32) / "
+                    "1e-3 (bf16) relative with the method's preconditioner")
+    return out
 
 
 def rooflines(ab, op, mat, gmat, method, dt, workload, xs):
