@@ -52,7 +52,6 @@ using namespace bulk;
 constexpr int kTcRows    = 128; // rows per tile: M of the MMA, TMEM lanes
 constexpr int kTcK       = 64;  // K columns per staged chunk (four MMAs)
 constexpr int kTcThreads = 128;
-constexpr int kTcAbytes  = kTcRows * kTcK * 2; // one A chunk buffer
 
 constexpr int ipow3t(int k) { return k <= 0 ? 1 : 3 * ipow3t(k - 1); }
 
@@ -151,7 +150,8 @@ struct tc_group
 // columns (a power of two >= Np)
 struct tc_launch
 {
-  int k = 0, cols = 0, ntiles = 0, np_max = 0;
+  int k = 0, cols = 0, ntiles = 0, np_max = 0, kp_max = 0;
+  int abytes = 0, bbytes = 0, nbuf = 0; // chunk buffers sized for this launch
   size_t smem       = 0;
   int2 *tiles       = nullptr; // (group, first row)
 };
@@ -211,7 +211,8 @@ __global__ void __launch_bounds__(kTcThreads)
     k_tc_pencil(const int2 *__restrict__ tiles, const tc_group *__restrict__ groups,
                 const int *__restrict__ pen_start, const int *__restrict__ pen_cells,
                 const __nv_bfloat16 *__restrict__ img, const __nv_bfloat16 *__restrict__ xb,
-                float *__restrict__ acc, int post, uint32_t cols, int bbytes, int mode,
+                float *__restrict__ acc, int post, uint32_t cols, int abytes, int bbytes,
+                int nbuf, int mode,
                 double alpha, const double *__restrict__ x, double beta,
                 double *__restrict__ y, double ex, const double *gate)
 {
@@ -227,7 +228,7 @@ __global__ void __launch_bounds__(kTcThreads)
   tc_group const g = groups[tile.x];
   int const nch    = (g.Kp + kTcK - 1) / kTcK;
   unsigned char *const Abuf = smem;
-  unsigned char *const Bbuf = smem + 2 * kTcAbytes;
+  unsigned char *const Bbuf = smem + nbuf * abytes;
 
   if (tid == 0)
   {
@@ -273,7 +274,7 @@ __global__ void __launch_bounds__(kTcThreads)
     __syncthreads();
     if (s_abort)
       break;
-    unsigned char *const A = Abuf + b * kTcAbytes;
+    unsigned char *const A = Abuf + b * abytes;
     unsigned char *const B = Bbuf + b * bbytes;
     if (tid == 0)
     {
@@ -475,13 +476,20 @@ void class_images(std::vector<tc_class_host> const &classes, int r1,
   }
 }
 
-// shared memory for a launch: two A chunks and two B chunks of np_max rows;
-// raised until at most 512 / cols CTAs fit on an SM, so the resident CTAs'
-// TMEM allocations never exceed the SM's 512 columns
-int launch_smem(int d, int cols, int np_max, size_t &smem)
+// shared memory for a launch: A and B chunk buffers of the launch's widest
+// chunk (K columns) and largest matrix, two of each when some matrix needs
+// several chunks (double buffering), one otherwise; raised until at most
+// 512 / cols CTAs fit on an SM, so the resident CTAs' TMEM allocations never
+// exceed the SM's 512 columns
+int launch_smem(int d, tc_launch &l)
 {
+  int const cols = l.cols;
+  int const kc   = std::min(kTcK, l.kp_max);
+  l.nbuf         = l.kp_max > kTcK ? 2 : 1;
+  l.abytes       = kTcRows * kc * 2;
+  l.bbytes       = l.np_max * kc * 2;
   void *fn = tc_kernel_d(d);
-  size_t s = size_t(2) * kTcAbytes + size_t(2) * np_max * kTcK * 2;
+  size_t s = size_t(l.nbuf) * (l.abytes + l.bbytes);
   int const allowed = 512 / cols;
   int dev = 0, optin = 0;
   ASGK_CUDA(cudaGetDevice(&dev));
@@ -503,7 +511,7 @@ int launch_smem(int d, int cols, int np_max, size_t &smem)
       return ASGK_ERR_UNSUPPORTED;
     s += 4096;
   }
-  smem = s;
+  l.smem = s;
   return ASGK_OK;
 }
 
@@ -653,7 +661,7 @@ int tc_build(plan_data const &p, tc_data **out)
       return t->classes[a].R > t->classes[b].R;
     });
     std::map<int, std::vector<int2>, std::greater<int>> tiles_by_cols;
-    std::map<int, int> npmax_by_cols;
+    std::map<int, int> npmax_by_cols, kpmax_by_cols;
     for (int ci : cls)
     {
       auto const &ch = t->classes[ci];
@@ -676,6 +684,7 @@ int tc_build(plan_data const &p, tc_data **out)
       for (int64_t r0 = 0; r0 < nr; r0 += kTcRows)
         tiles_by_cols[cols].push_back(make_int2(gid, int(r0)));
       npmax_by_cols[cols] = std::max(npmax_by_cols[cols], ch.Np);
+      kpmax_by_cols[cols] = std::max(kpmax_by_cols[cols], ch.Kp);
       groups.push_back(g);
     }
     for (auto &kv : tiles_by_cols)
@@ -684,8 +693,9 @@ int tc_build(plan_data const &p, tc_data **out)
       l.k      = k;
       l.cols   = kv.first;
       l.np_max = npmax_by_cols[kv.first];
+      l.kp_max = kpmax_by_cols[kv.first];
       l.ntiles = int(kv.second.size());
-      if (int rc = launch_smem(d, l.cols, l.np_max, l.smem))
+      if (int rc = launch_smem(d, l))
         return rc;
       if (int rc = upload_tc(&l.tiles, kv.second, t->bytes))
         return rc;
@@ -743,11 +753,10 @@ int launch_global_tc(plan_data const &p, double alpha, const double *x, double b
   {
     int const mode = (kfirst == klast) ? 3 : (l.k == kfirst ? 0 : (l.k == klast ? 2 : 1));
     int const post = ipow3t(t.d - 1 - l.k);
-    int const bbytes = l.np_max * kTcK * 2;
 #define ASGK_TC_LAUNCH(DD)                                                                  \
   k_tc_pencil<DD><<<l.ntiles, kTcThreads, l.smem, s>>>(                                     \
       l.tiles, t.groups, t.pen_start, t.pen_cells, t.img, t.xb, t.acc, post,               \
-      uint32_t(l.cols), bbytes, mode, alpha, x, beta, y, ex, g_gate)
+      uint32_t(l.cols), l.abytes, l.bbytes, l.nbuf, mode, alpha, x, beta, y, ex, g_gate)
     switch (t.d)
     {
     case 1: ASGK_TC_LAUNCH(1); break;
