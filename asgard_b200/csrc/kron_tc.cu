@@ -23,8 +23,11 @@
 // double-buffered, their reuse ordered by tcgen05.commit on mbarriers.  The
 // epilogue reads the accumulators (tcgen05.ld, each warp its 32 lanes) and
 // adds them into the cells' values.  Every cell lies in exactly one pencil
-// per dimension, so the launches of one dimension write disjoint values;
-// dimensions follow one another on the stream through an FP32 sum vector and
+// per dimension, so the launches of one dimension (one per TMEM size) write
+// disjoint values and run concurrently on side streams; matrices of 3 x 32
+// cells and more take 512-thread CTAs whose four thread groups split each
+// tile's gather and epilogue; dimensions follow one another through an FP32
+// sum vector and
 // the last one forms
 //   y = beta y + alpha (sum_k K_k x + n_identity x) + ex x
 // in FP64.  x is rounded to BF16 once per apply (a conversion pass); the
@@ -51,7 +54,8 @@ using namespace bulk;
 
 constexpr int kTcRows    = 128; // rows per tile: M of the MMA, TMEM lanes
 constexpr int kTcK       = 64;  // K columns per staged chunk (four MMAs)
-constexpr int kTcThreads = 128;
+constexpr int kTcThreads = 128;     // small matrices (up to 64 TMEM columns)
+constexpr int kTcThreadsWide = 512; // matrices of 3 x 32 cells and more
 
 constexpr int ipow3t(int k) { return k <= 0 ? 1 : 3 * ipow3t(k - 1); }
 
@@ -150,7 +154,7 @@ struct tc_group
 // columns (a power of two >= Np)
 struct tc_launch
 {
-  int k = 0, cols = 0, ntiles = 0, np_max = 0, kp_max = 0;
+  int k = 0, cols = 0, ntiles = 0, np_max = 0, kp_max = 0, nt = 0;
   int abytes = 0, bbytes = 0, nbuf = 0; // chunk buffers sized for this launch
   size_t smem       = 0;
   int2 *tiles       = nullptr; // (group, first row)
@@ -177,8 +181,20 @@ struct tc_data
   __nv_bfloat16 *xb     = nullptr; // x rounded to BF16
   float *acc            = nullptr; // FP32 sum over the dimensions
   int64_t bytes         = 0;
+  // the launches of one dimension touch disjoint cells and run concurrently:
+  // the first on the caller's stream, the others on side streams forked and
+  // joined by events (parallel branches when recorded into a graph)
+  std::vector<cudaStream_t> side;
+  cudaEvent_t fork = nullptr;
+  std::vector<cudaEvent_t> join;
   ~tc_data()
   {
+    for (auto st : side)
+      cudaStreamDestroy(st);
+    for (auto ev : join)
+      cudaEventDestroy(ev);
+    if (fork)
+      cudaEventDestroy(fork);
     for (auto &l : launches)
       cudaFree(l.tiles);
     cudaFree(groups);
@@ -205,9 +221,13 @@ __global__ void k_to_bf16(const double *__restrict__ x, __nv_bfloat16 *__restric
 // mode 0: acc = K_k x (first dimension); 1: acc += K_k x; 2 (last): y = beta
 // y + alpha (acc + K_k x) + ex x; 3 (the only dimension): y = beta y + alpha
 // K_k x + ex x.  post = 3^(D-1-k): fibre f of dimension k holds the values
-// (f / post) * 3 post + c post + f % post, c = 0, 1, 2.
-template<int D>
-__global__ void __launch_bounds__(kTcThreads)
+// (f / post) * 3 post + c post + f % post, c = 0, 1, 2.  NT threads: NT / 128
+// groups of 128 share a tile, thread t owning row t % 128 (the TMEM lane of
+// its warp's lane quarter) and group t / 128 taking every (NT / 128)-th
+// 8-column piece of the gather and 16-column piece of the epilogue, so the
+// long chains of the large pencils are split.
+template<int D, int NT>
+__global__ void __launch_bounds__(NT)
     k_tc_pencil(const int2 *__restrict__ tiles, const tc_group *__restrict__ groups,
                 const int *__restrict__ pen_start, const int *__restrict__ pen_cells,
                 const __nv_bfloat16 *__restrict__ img, const __nv_bfloat16 *__restrict__ xb,
@@ -217,6 +237,7 @@ __global__ void __launch_bounds__(kTcThreads)
                 double *__restrict__ y, double ex, const double *gate)
 {
   constexpr int T = ipow3t(D), F = T / 3;
+  constexpr int NP = NT / kTcRows;
   extern __shared__ __align__(1024) unsigned char smem[];
   __shared__ __align__(8) uint64_t bbar[2], mbar[2];
   __shared__ uint32_t tslot;
@@ -224,6 +245,7 @@ __global__ void __launch_bounds__(kTcThreads)
   if (gate_closed(gate))
     return;
   int const tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  int const row = tid & (kTcRows - 1), part = tid / kTcRows;
   int2 const tile  = tiles[blockIdx.x];
   tc_group const g = groups[tile.x];
   int const nch    = (g.Kp + kTcK - 1) / kTcK;
@@ -250,7 +272,7 @@ __global__ void __launch_bounds__(kTcThreads)
   uint32_t const tmem = tslot;
 
   // this thread's row: pencil P of the class, fibre f
-  int const rowg   = tile.y + tid;
+  int const rowg   = tile.y + row;
   bool const valid = rowg < g.npen * F;
   int const P      = valid ? rowg / F : 0;
   int const f      = valid ? rowg - P * F : 0;
@@ -284,8 +306,9 @@ __global__ void __launch_bounds__(kTcThreads)
     }
     // gather the rows' chunk of X: core matrix (row / 8, column / 8) at
     // (row / 8) * kc * 16 + (column / 8) * 128 bytes, 16 bytes per row
-    unsigned char *const arow = A + (tid >> 3) * (kc * 16) + (tid & 7) * 16;
-    for (int e8 = 0; e8 < kc / 8; e8++)
+    unsigned char *const arow = A + (row >> 3) * (kc * 16) + (row & 7) * 16;
+#pragma unroll 2
+    for (int e8 = part; e8 < kc / 8; e8 += NP)
     {
       unsigned short v[8];
 #pragma unroll
@@ -353,8 +376,8 @@ __global__ void __launch_bounds__(kTcThreads)
   tc_fence_after();
   if (done && !s_abort)
   {
-    uint32_t const lanebase = tmem + (uint32_t(warp * 32) << 16);
-    for (int n0 = 0; n0 < g.R; n0 += 16)
+    uint32_t const lanebase = tmem + (uint32_t((warp & 3) * 32) << 16);
+    for (int n0 = 16 * part; n0 < g.R; n0 += 16 * NP)
     {
       uint32_t r[16];
       tmem_ld16(lanebase + uint32_t(n0), r);
@@ -392,21 +415,22 @@ __global__ void __launch_bounds__(kTcThreads)
 }
 
 template<int D>
-void *tc_kernel()
+void *tc_kernel(int nt)
 {
-  return reinterpret_cast<void *>(&k_tc_pencil<D>);
+  return nt == kTcThreadsWide ? reinterpret_cast<void *>(&k_tc_pencil<D, kTcThreadsWide>)
+                              : reinterpret_cast<void *>(&k_tc_pencil<D, kTcThreads>);
 }
 
-void *tc_kernel_d(int d)
+void *tc_kernel_d(int d, int nt)
 {
   switch (d)
   {
-  case 1: return tc_kernel<1>();
-  case 2: return tc_kernel<2>();
-  case 3: return tc_kernel<3>();
-  case 4: return tc_kernel<4>();
-  case 5: return tc_kernel<5>();
-  case 6: return tc_kernel<6>();
+  case 1: return tc_kernel<1>(nt);
+  case 2: return tc_kernel<2>(nt);
+  case 3: return tc_kernel<3>(nt);
+  case 4: return tc_kernel<4>(nt);
+  case 5: return tc_kernel<5>(nt);
+  case 6: return tc_kernel<6>(nt);
   default: return nullptr;
   }
 }
@@ -488,7 +512,8 @@ int launch_smem(int d, tc_launch &l)
   l.nbuf         = l.kp_max > kTcK ? 2 : 1;
   l.abytes       = kTcRows * kc * 2;
   l.bbytes       = l.np_max * kc * 2;
-  void *fn = tc_kernel_d(d);
+  l.nt     = cols >= 128 ? kTcThreadsWide : kTcThreads;
+  void *fn = tc_kernel_d(d, l.nt);
   size_t s = size_t(l.nbuf) * (l.abytes + l.bbytes);
   int const allowed = 512 / cols;
   int dev = 0, optin = 0;
@@ -504,7 +529,7 @@ int launch_smem(int d, tc_launch &l)
     if (s > size_t(dyn_max))
       return ASGK_ERR_UNSUPPORTED;
     int nb = 0;
-    ASGK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, kTcThreads, s));
+    ASGK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, l.nt, s));
     if (nb >= 1 && nb <= allowed)
       break;
     if (nb < 1)
@@ -713,6 +738,24 @@ int tc_build(plan_data const &p, tc_data **out)
       (rc = upload_tc(&t->pen_cells, pen_cells, t->bytes)) ||
       (rc = upload_tc(&t->img, img, t->bytes)))
     return rc;
+  int per_dim = 0;
+  for (int k : t->dims)
+  {
+    int c = 0;
+    for (auto const &l : t->launches)
+      c += (l.k == k);
+    per_dim = std::max(per_dim, c);
+  }
+  ASGK_CUDA(cudaEventCreateWithFlags(&t->fork, cudaEventDisableTiming));
+  for (int i = 1; i < per_dim; i++)
+  {
+    cudaStream_t st = nullptr;
+    cudaEvent_t ev  = nullptr;
+    ASGK_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    t->side.push_back(st);
+    ASGK_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    t->join.push_back(ev);
+  }
   int64_t const n = int64_t(p.rows) * p.tensor;
   ASGK_CUDA(cudaMalloc(&t->xb, sizeof(__nv_bfloat16) * std::max<int64_t>(n, 1)));
   ASGK_CUDA(cudaMalloc(&t->acc, sizeof(float) * std::max<int64_t>(n, 1)));
@@ -749,26 +792,48 @@ int launch_global_tc(plan_data const &p, double alpha, const double *x, double b
     ASGK_LAUNCHED();
   }
   int const kfirst = t.dims.front(), klast = t.dims.back();
-  for (auto const &l : t.launches)
+  size_t li = 0;
+  for (int k : t.dims)
   {
-    int const mode = (kfirst == klast) ? 3 : (l.k == kfirst ? 0 : (l.k == klast ? 2 : 1));
-    int const post = ipow3t(t.d - 1 - l.k);
-#define ASGK_TC_LAUNCH(DD)                                                                  \
-  k_tc_pencil<DD><<<l.ntiles, kTcThreads, l.smem, s>>>(                                     \
-      l.tiles, t.groups, t.pen_start, t.pen_cells, t.img, t.xb, t.acc, post,               \
-      uint32_t(l.cols), l.abytes, l.bbytes, l.nbuf, mode, alpha, x, beta, y, ex, g_gate)
-    switch (t.d)
+    size_t le = li;
+    while (le < t.launches.size() && t.launches[le].k == k)
+      ++le;
+    int const nl = int(le - li);
+    if (nl > 1)
     {
-    case 1: ASGK_TC_LAUNCH(1); break;
-    case 2: ASGK_TC_LAUNCH(2); break;
-    case 3: ASGK_TC_LAUNCH(3); break;
-    case 4: ASGK_TC_LAUNCH(4); break;
-    case 5: ASGK_TC_LAUNCH(5); break;
-    case 6: ASGK_TC_LAUNCH(6); break;
-    default: return ASGK_ERR_UNSUPPORTED;
+      ASGK_CUDA(cudaEventRecord(t.fork, s));
+      for (int i = 1; i < nl; i++)
+        ASGK_CUDA(cudaStreamWaitEvent(t.side[i - 1], t.fork, 0));
     }
+    int const mode = (kfirst == klast) ? 3 : (k == kfirst ? 0 : (k == klast ? 2 : 1));
+    int const post = ipow3t(t.d - 1 - k);
+    for (int i = 0; i < nl; i++)
+    {
+      tc_launch const &l = t.launches[li + i];
+      cudaStream_t const ls = (i == 0) ? s : t.side[i - 1];
+#define ASGK_TC_LAUNCH(DD, NT)                                                                k_tc_pencil<DD, NT><<<l.ntiles, NT, l.smem, ls>>>(                                             l.tiles, t.groups, t.pen_start, t.pen_cells, t.img, t.xb, t.acc, post,                     uint32_t(l.cols), l.abytes, l.bbytes, l.nbuf, mode, alpha, x, beta, y, ex, g_gate)
+#define ASGK_TC_LAUNCH_D(DD)                                                                  if (l.nt == kTcThreadsWide)                                                                   ASGK_TC_LAUNCH(DD, kTcThreadsWide);                                                       else                                                                                          ASGK_TC_LAUNCH(DD, kTcThreads)
+      switch (t.d)
+      {
+      case 1: ASGK_TC_LAUNCH_D(1); break;
+      case 2: ASGK_TC_LAUNCH_D(2); break;
+      case 3: ASGK_TC_LAUNCH_D(3); break;
+      case 4: ASGK_TC_LAUNCH_D(4); break;
+      case 5: ASGK_TC_LAUNCH_D(5); break;
+      case 6: ASGK_TC_LAUNCH_D(6); break;
+      default: return ASGK_ERR_UNSUPPORTED;
+      }
+#undef ASGK_TC_LAUNCH_D
 #undef ASGK_TC_LAUNCH
-    ASGK_LAUNCHED();
+      ASGK_LAUNCHED();
+    }
+    if (nl > 1)
+      for (int i = 1; i < nl; i++)
+      {
+        ASGK_CUDA(cudaEventRecord(t.join[i - 1], t.side[i - 1]));
+        ASGK_CUDA(cudaStreamWaitEvent(s, t.join[i - 1], 0));
+      }
+    li = le;
   }
   return ASGK_OK;
 }
