@@ -503,8 +503,11 @@ void class_images(std::vector<tc_class_host> const &classes, int r1,
 // shared memory for a launch: A and B chunk buffers of the launch's widest
 // chunk (K columns) and largest matrix, two of each when some matrix needs
 // several chunks (double buffering), one otherwise; raised until at most
-// 512 / cols CTAs fit on an SM, so the resident CTAs' TMEM allocations never
-// exceed the SM's 512 columns
+// 512 / cols CTAs fit on an SM, so the resident CTAs of one launch never ask
+// for more than the SM's 512 columns.  CTAs of the concurrent launches of the
+// same dimension can share an SM; a tcgen05.alloc that finds too few free
+// columns then waits until a resident CTA deallocates, which every CTA does
+// without waiting on any other CTA, so the wait always ends
 int launch_smem(int d, tc_launch &l)
 {
   int const cols = l.cols;
