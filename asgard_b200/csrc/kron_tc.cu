@@ -27,8 +27,7 @@
 // disjoint values and run concurrently on side streams; matrices of 3 x 32
 // cells and more take 512-thread CTAs whose four thread groups split each
 // tile's gather and epilogue; dimensions follow one another through an FP32
-// sum vector and
-// the last one forms
+// sum vector and the last one forms
 //   y = beta y + alpha (sum_k K_k x + n_identity x) + ex x
 // in FP64.  x is rounded to BF16 once per apply (a conversion pass); the
 // same summation order every call, so results are bit-reproducible.
@@ -307,19 +306,31 @@ __global__ void __launch_bounds__(NT)
     // gather the rows' chunk of X: core matrix (row / 8, column / 8) at
     // (row / 8) * kc * 16 + (column / 8) * 128 bytes, 16 bytes per row
     unsigned char *const arow = A + (row >> 3) * (kc * 16) + (row & 7) * 16;
-#pragma unroll 2
+    // columns of this chunk that hold values of this row (the rest is the
+    // zero padding up to Kp): pieces past them are stored as zeros without
+    // loads; (cell, polynomial) of a column advance without divisions
+    int const kvalid = valid ? min(kc, g.R - kk0) : 0;
     for (int e8 = part; e8 < kc / 8; e8 += NP)
     {
-      unsigned short v[8];
-#pragma unroll
-      for (int q = 0; q < 8; q++)
+      unsigned short v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+      if (e8 * 8 < kvalid)
       {
-        int const kk = kk0 + e8 * 8 + q;
-        v[q]         = 0;
-        if (valid && kk < g.R)
+        int const kk = kk0 + e8 * 8;
+        int i        = kk / 3;
+        int c        = kk - 3 * i;
+        int64_t off  = int64_t(cells[i]) * T + base;
+#pragma unroll
+        for (int q = 0; q < 8; q++)
         {
-          int const i = kk / 3, c = kk - 3 * i;
-          v[q] = __bfloat16_as_ushort(xb[int64_t(cells[i]) * T + base + c * post]);
+          if (e8 * 8 + q < kvalid)
+            v[q] = __bfloat16_as_ushort(xb[off + c * post]);
+          if (++c == 3 && q < 7)
+          {
+            c = 0;
+            ++i;
+            if (kk + q + 1 < g.R)
+              off = int64_t(cells[i]) * T + base;
+          }
         }
       }
       uint4 pk;
