@@ -15,7 +15,8 @@
 //   Y[(P, f), n] = sum_kk X[(P, f), kk] A_P[n, kk],
 // rows (pencil, fibre f: the 3^(d-1) index combinations of the other
 // dimensions), kk = (cell i of P, polynomial c along k), n = (cell i', c').
-// A CTA takes 128 rows (M = 128, one TMEM lane each): its threads gather the
+// A tile is 128 rows (M = 128, one TMEM lane each; a CTA takes one tile, or
+// four of one class for pencils of up to 8 cells): its threads gather the
 // rows' X into shared memory as BF16 in the no-swizzle K-major layout, the
 // class matrix arrives in 64-column chunks by bulk copy (laid out on the
 // host in the same layout), and one thread issues the MMAs (K = 16 each; N
@@ -55,6 +56,7 @@ constexpr int kTcRows    = 128; // rows per tile: M of the MMA, TMEM lanes
 constexpr int kTcK       = 64;  // K columns per staged chunk (four MMAs)
 constexpr int kTcThreads = 128;     // small matrices (up to 64 TMEM columns)
 constexpr int kTcThreadsWide = 512; // matrices of 3 x 32 cells and more
+constexpr int kTcTilesSmall  = 4;   // tiles per CTA for matrices of up to 3 x 8 cells
 
 constexpr int ipow3t(int k) { return k <= 0 ? 1 : 3 * ipow3t(k - 1); }
 
@@ -153,7 +155,7 @@ struct tc_group
 // columns (a power of two >= Np)
 struct tc_launch
 {
-  int k = 0, cols = 0, ntiles = 0, np_max = 0, kp_max = 0, nt = 0;
+  int k = 0, cols = 0, ntiles = 0, np_max = 0, kp_max = 0, nt = 0, tpc = 1;
   int abytes = 0, bbytes = 0, nbuf = 0; // chunk buffers sized for this launch
   size_t smem       = 0;
   int2 *tiles       = nullptr; // (group, first row)
@@ -220,12 +222,16 @@ __global__ void k_to_bf16(const double *__restrict__ x, __nv_bfloat16 *__restric
 // mode 0: acc = K_k x (first dimension); 1: acc += K_k x; 2 (last): y = beta
 // y + alpha (acc + K_k x) + ex x; 3 (the only dimension): y = beta y + alpha
 // K_k x + ex x.  post = 3^(D-1-k): fibre f of dimension k holds the values
-// (f / post) * 3 post + c post + f % post, c = 0, 1, 2.  NT threads: NT / 128
-// groups of 128 share a tile, thread t owning row t % 128 (the TMEM lane of
-// its warp's lane quarter) and group t / 128 taking every (NT / 128)-th
-// 8-column piece of the gather and 16-column piece of the epilogue, so the
-// long chains of the large pencils are split.
-template<int D, int NT>
+// (f / post) * 3 post + c post + f % post, c = 0, 1, 2.  A CTA takes TILES
+// consecutive tiles of 128 rows of one class (its MMAs share the class
+// matrix; tile i accumulates in TMEM columns i * Np on), and NT / (128 TILES)
+// thread groups share each row: thread t owns row t % (128 TILES) (the TMEM
+// lane of its warp's lane quarter in tile (t % (128 TILES)) / 128) and group
+// t / (128 TILES) takes every NP-th 8-column piece of the gather and
+// 16-column piece of the epilogue.  Large pencils: one tile, four groups
+// (their long chains split); pencils of 1-8 cells: four tiles, one group
+// (the per-CTA set-up, matrix copy and MMA round trip shared).
+template<int D, int NT, int TILES>
 __global__ void __launch_bounds__(NT)
     k_tc_pencil(const int2 *__restrict__ tiles, const tc_group *__restrict__ groups,
                 const int *__restrict__ pen_start, const int *__restrict__ pen_cells,
@@ -236,7 +242,9 @@ __global__ void __launch_bounds__(NT)
                 double *__restrict__ y, double ex, const double *gate)
 {
   constexpr int T = ipow3t(D), F = T / 3;
-  constexpr int NP = NT / kTcRows;
+  constexpr int ROWS = kTcRows * TILES;
+  constexpr int NP   = NT / ROWS;
+  static_assert(NP >= 1 && NT % ROWS == 0, "thread groups");
   extern __shared__ __align__(1024) unsigned char smem[];
   __shared__ __align__(8) uint64_t bbar[2], mbar[2];
   __shared__ uint32_t tslot;
@@ -244,7 +252,8 @@ __global__ void __launch_bounds__(NT)
   if (gate_closed(gate))
     return;
   int const tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  int const row = tid & (kTcRows - 1), part = tid / kTcRows;
+  int const row = tid % ROWS, part = tid / ROWS;
+  int const ti  = row / kTcRows, r128 = row % kTcRows; // tile, lane
   int2 const tile  = tiles[blockIdx.x];
   tc_group const g = groups[tile.x];
   int const nch    = (g.Kp + kTcK - 1) / kTcK;
@@ -305,7 +314,9 @@ __global__ void __launch_bounds__(NT)
     }
     // gather the rows' chunk of X: core matrix (row / 8, column / 8) at
     // (row / 8) * kc * 16 + (column / 8) * 128 bytes, 16 bytes per row
-    unsigned char *const arow = A + (row >> 3) * (kc * 16) + (row & 7) * 16;
+    int const tbytes = kTcRows * kc * 2; // one tile's rows of the chunk
+    unsigned char *const arow =
+        A + ti * tbytes + (r128 >> 3) * (kc * 16) + (r128 & 7) * 16;
     // columns of this chunk that hold values of this row (the rest is the
     // zero padding up to Kp): pieces past them are stored as zeros without
     // loads; (cell, polynomial) of a column advance without divisions
@@ -357,14 +368,17 @@ __global__ void __launch_bounds__(NT)
         uint32_t const a0 = smem_u32(A), b0 = smem_u32(B);
         uint32_t const sbo = uint32_t(kc) * 16u;
         for (int s = 0; s < kc / 16; s++)
-        {
-          uint64_t const ad = smem_desc(a0 + s * 256, 128, sbo);
-          for (int h = 0; h < nh; h++)
+          for (int t2 = 0; t2 < TILES; t2++)
           {
-            uint64_t const bd = smem_desc(b0 + h * (Nh / 8) * sbo + s * 256, 128, sbo);
-            mma_bf16(tmem + uint32_t(h * Nh), ad, bd, idesc, (j > 0 || s > 0) ? 1u : 0u);
+            uint64_t const ad =
+                smem_desc(a0 + t2 * kTcRows * kc * 2 + s * 256, 128, sbo);
+            for (int h = 0; h < nh; h++)
+            {
+              uint64_t const bd = smem_desc(b0 + h * (Nh / 8) * sbo + s * 256, 128, sbo);
+              mma_bf16(tmem + uint32_t(t2 * g.Np + h * Nh), ad, bd, idesc,
+                       (j > 0 || s > 0) ? 1u : 0u);
+            }
           }
-        }
         mma_commit(&mbar[b]);
       }
     }
@@ -387,7 +401,8 @@ __global__ void __launch_bounds__(NT)
   tc_fence_after();
   if (done && !s_abort)
   {
-    uint32_t const lanebase = tmem + (uint32_t((warp & 3) * 32) << 16);
+    uint32_t const lanebase =
+        tmem + (uint32_t((warp & 3) * 32) << 16) + uint32_t(ti * g.Np);
     for (int n0 = 16 * part; n0 < g.R; n0 += 16 * NP)
     {
       uint32_t r[16];
@@ -426,22 +441,24 @@ __global__ void __launch_bounds__(NT)
 }
 
 template<int D>
-void *tc_kernel(int nt)
+void *tc_kernel(int nt, int tiles)
 {
-  return nt == kTcThreadsWide ? reinterpret_cast<void *>(&k_tc_pencil<D, kTcThreadsWide>)
-                              : reinterpret_cast<void *>(&k_tc_pencil<D, kTcThreads>);
+  if (tiles == kTcTilesSmall)
+    return reinterpret_cast<void *>(&k_tc_pencil<D, kTcThreadsWide, kTcTilesSmall>);
+  return nt == kTcThreadsWide ? reinterpret_cast<void *>(&k_tc_pencil<D, kTcThreadsWide, 1>)
+                              : reinterpret_cast<void *>(&k_tc_pencil<D, kTcThreads, 1>);
 }
 
-void *tc_kernel_d(int d, int nt)
+void *tc_kernel_d(int d, int nt, int tiles)
 {
   switch (d)
   {
-  case 1: return tc_kernel<1>(nt);
-  case 2: return tc_kernel<2>(nt);
-  case 3: return tc_kernel<3>(nt);
-  case 4: return tc_kernel<4>(nt);
-  case 5: return tc_kernel<5>(nt);
-  case 6: return tc_kernel<6>(nt);
+  case 1: return tc_kernel<1>(nt, tiles);
+  case 2: return tc_kernel<2>(nt, tiles);
+  case 3: return tc_kernel<3>(nt, tiles);
+  case 4: return tc_kernel<4>(nt, tiles);
+  case 5: return tc_kernel<5>(nt, tiles);
+  case 6: return tc_kernel<6>(nt, tiles);
   default: return nullptr;
   }
 }
@@ -524,10 +541,9 @@ int launch_smem(int d, tc_launch &l)
   int const cols = l.cols;
   int const kc   = std::min(kTcK, l.kp_max);
   l.nbuf         = l.kp_max > kTcK ? 2 : 1;
-  l.abytes       = kTcRows * kc * 2;
+  l.abytes       = l.tpc * kTcRows * kc * 2;
   l.bbytes       = l.np_max * kc * 2;
-  l.nt     = cols >= 128 ? kTcThreadsWide : kTcThreads;
-  void *fn = tc_kernel_d(d, l.nt);
+  void *fn = tc_kernel_d(d, l.nt, l.tpc);
   size_t s = size_t(l.nbuf) * (l.abytes + l.bbytes);
   int const allowed = 512 / cols;
   int dev = 0, optin = 0;
@@ -720,7 +736,9 @@ int tc_build(plan_data const &p, tc_data **out)
       int64_t const nr = int64_t(g.npen) * fib;
       if (nr > (int64_t(1) << 30))
         return ASGK_ERR_UNSUPPORTED;
-      for (int64_t r0 = 0; r0 < nr; r0 += kTcRows)
+      // matrices of up to 3 x 8 cells: four tiles per CTA
+      int64_t const step = int64_t(kTcRows) * (cols == 32 ? kTcTilesSmall : 1);
+      for (int64_t r0 = 0; r0 < nr; r0 += step)
         tiles_by_cols[cols].push_back(make_int2(gid, int(r0)));
       npmax_by_cols[cols] = std::max(npmax_by_cols[cols], ch.Np);
       kpmax_by_cols[cols] = std::max(kpmax_by_cols[cols], ch.Kp);
@@ -734,6 +752,13 @@ int tc_build(plan_data const &p, tc_data **out)
       l.np_max = npmax_by_cols[kv.first];
       l.kp_max = kpmax_by_cols[kv.first];
       l.ntiles = int(kv.second.size());
+      // 1-8-cell pencils: four tiles per 512-thread CTA; 16-cell pencils:
+      // one tile per 128-thread CTA; larger: one tile per 512-thread CTA
+      l.tpc = (kv.first == 32) ? kTcTilesSmall : 1;
+      l.nt  = (kv.first == 32 || kv.first >= 128) ? kTcThreadsWide : kTcThreads;
+      l.cols = 32;
+      while (l.cols < l.tpc * l.np_max)
+        l.cols *= 2;
       if (int rc = launch_smem(d, l))
         return rc;
       if (int rc = upload_tc(&l.tiles, kv.second, t->bytes))
@@ -825,8 +850,17 @@ int launch_global_tc(plan_data const &p, double alpha, const double *x, double b
     {
       tc_launch const &l = t.launches[li + i];
       cudaStream_t const ls = (i == 0) ? s : t.side[i - 1];
-#define ASGK_TC_LAUNCH(DD, NT)                                                                k_tc_pencil<DD, NT><<<l.ntiles, NT, l.smem, ls>>>(                                             l.tiles, t.groups, t.pen_start, t.pen_cells, t.img, t.xb, t.acc, post,                     uint32_t(l.cols), l.abytes, l.bbytes, l.nbuf, mode, alpha, x, beta, y, ex, g_gate)
-#define ASGK_TC_LAUNCH_D(DD)                                                                  if (l.nt == kTcThreadsWide)                                                                   ASGK_TC_LAUNCH(DD, kTcThreadsWide);                                                       else                                                                                          ASGK_TC_LAUNCH(DD, kTcThreads)
+#define ASGK_TC_LAUNCH(DD, NT, TL)                                                          \
+  k_tc_pencil<DD, NT, TL><<<l.ntiles, NT, l.smem, ls>>>(                                   \
+      l.tiles, t.groups, t.pen_start, t.pen_cells, t.img, t.xb, t.acc, post,               \
+      uint32_t(l.cols), l.abytes, l.bbytes, l.nbuf, mode, alpha, x, beta, y, ex, g_gate)
+#define ASGK_TC_LAUNCH_D(DD)                                                                \
+  if (l.tpc == kTcTilesSmall)                                                               \
+    ASGK_TC_LAUNCH(DD, kTcThreadsWide, kTcTilesSmall);                                      \
+  else if (l.nt == kTcThreadsWide)                                                          \
+    ASGK_TC_LAUNCH(DD, kTcThreadsWide, 1);                                                  \
+  else                                                                                      \
+    ASGK_TC_LAUNCH(DD, kTcThreads, 1)
       switch (t.d)
       {
       case 1: ASGK_TC_LAUNCH_D(1); break;
