@@ -141,3 +141,30 @@ def test_bf16_refinement_reaches_fp64_residual(cuda, d, L, T, dt):
         assert ib.status == 0 and ib.true_relres <= 1e-10, ib
         assert ib.matvecs_low > 0 and ib.outer_steps >= 2
         assert rel_err(xb.cpu().numpy(), x64.cpu().numpy()) < 1e-8
+
+
+def test_bf16_refused_where_the_pencil_form_does_not_apply(cuda):
+    """The tensor-core form needs a global plan whose terms act in one
+    dimension each: a connected-pair plan, and a global plan with a term
+    acting in several dimensions (upper/lower chains), refuse precision
+    "bf16" with ASGK_ERR_UNSUPPORTED in the apply and in the solve, and the
+    solve leaves x untouched."""
+    import asgard_b200 as ab
+    import torch
+    from asgard_b200._lib import AsgkError
+    op = ab.SparseGridOperator(3, 4, 3, kind="advdiff")
+    pairs = op.kronmult_matrix()
+    opr = ab.SparseGridOperator(3, 4, 2, kind="random", seed=3)  # all-direction terms
+    chains = opr.kronmult_matrix(mode="global")
+    x = torch.rand(op.N, dtype=torch.float64, device="cuda")
+    for m in (pairs, chains):
+        y = torch.zeros_like(x)
+        with pytest.raises(AsgkError) as e:
+            m.apply(1.0, x, 0.0, y, precision="bf16")
+        assert e.value.status == 2   # ASGK_ERR_UNSUPPORTED
+        x0 = torch.zeros_like(x)
+        with pytest.raises(AsgkError) as e:
+            ab.simple_gmres_euler(1e-3, m, x0, x, 20, 5, 1e-10, tol_mode="rel",
+                                  precision="bf16")
+        assert e.value.status == 2
+        assert not x0.any()
