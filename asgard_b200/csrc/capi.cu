@@ -529,6 +529,15 @@ struct gmres_ws
   double *V = nullptr, *Z = nullptr, *part = nullptr, *h = nullptr,
          *y = nullptr, *r = nullptr, *e = nullptr;
   double *hh = nullptr; // pinned host mirror of h
+  // The solver's scalar reads (norms, Gram-Schmidt sums, the recorded
+  // cycle's state) and its write of the least-squares solution go through
+  // mapped pinned memory, moved by one-block kernels: a caller streaming
+  // large copies on another stream (x out, the next b in) occupies the copy
+  // engines, and a small cudaMemcpyAsync would queue behind those copies.
+  // Device aliases of hh, hstate and hy (null: mapping unavailable, plain
+  // copies instead).
+  double *hh_dev = nullptr, *hstate_dev = nullptr;
+  double *hy = nullptr, *hy_dev = nullptr; // pinned staging of the LS solution
   // FP32 copy of the basis for the Gram-Schmidt passes of FP32 inner solves
   // (allocated on first use, n * (m + 1))
   float *Vf = nullptr;
@@ -570,7 +579,11 @@ struct gmres_ws
     dstate = nullptr;
     if (hstate)
       cudaFreeHost(hstate);
-    hstate = nullptr;
+    hstate     = nullptr;
+    hstate_dev = nullptr;
+    if (hy)
+      cudaFreeHost(hy);
+    hy = hy_dev = nullptr;
     cudaFree(V);
     cudaFree(Vf);
     Vf = nullptr;
@@ -584,7 +597,7 @@ struct gmres_ws
     tickets = nullptr;
     if (hh)
       cudaFreeHost(hh);
-    V = Z = part = h = y = r = e = hh = nullptr;
+    V = Z = part = h = y = r = e = hh = hh_dev = nullptr;
     N = 0;
     m = 0;
   }
@@ -625,14 +638,24 @@ struct gmres_ws
       release();
       return rc;
     }
-    if (cudaMallocHost(reinterpret_cast<void **>(&hh),
-                       sizeof(double) * (restart + 2)) != cudaSuccess ||
-        cudaMallocHost(reinterpret_cast<void **>(&hstate),
-                       sizeof(double) * state_len(restart)) != cudaSuccess)
+    if (cudaHostAlloc(reinterpret_cast<void **>(&hh), sizeof(double) * (restart + 2),
+                      cudaHostAllocMapped) != cudaSuccess ||
+        cudaHostAlloc(reinterpret_cast<void **>(&hstate),
+                      sizeof(double) * state_len(restart), cudaHostAllocMapped) != cudaSuccess ||
+        cudaHostAlloc(reinterpret_cast<void **>(&hy), sizeof(double) * (restart + 1),
+                      cudaHostAllocMapped) != cudaSuccess)
     {
       cudaGetLastError();
       release();
       return ASGK_ERR_ALLOC;
+    }
+    if (cudaHostGetDevicePointer(reinterpret_cast<void **>(&hh_dev), hh, 0) != cudaSuccess ||
+        cudaHostGetDevicePointer(reinterpret_cast<void **>(&hstate_dev), hstate, 0) !=
+            cudaSuccess ||
+        cudaHostGetDevicePointer(reinterpret_cast<void **>(&hy_dev), hy, 0) != cudaSuccess)
+    {
+      cudaGetLastError();
+      hh_dev = hstate_dev = hy_dev = nullptr;
     }
     N        = n;
     m        = restart;
@@ -680,12 +703,37 @@ __global__ void k_cycle_start(double *st, double inner_res, double tol)
   }
 }
 
+// dst[0..n) = src[0..n): one block, for the few values the solver moves
+// between device memory and mapped pinned host memory
+__global__ void k_move_small(double *__restrict__ dst, const double *__restrict__ src,
+                             int n)
+{
+  for (int i = threadIdx.x; i < n; i += blockDim.x)
+    dst[i] = src[i];
+}
+
+// host = src[0..n) (read after the next synchronisation of s): through the
+// mapped alias when there is one, else a copy
+int read_small(double *host, double *host_dev, const double *src, int n,
+               cudaStream_t s)
+{
+  if (host_dev != nullptr)
+  {
+    k_move_small<<<1, 64, 0, s>>>(host_dev, src, n);
+    ASGK_LAUNCHED();
+    return ASGK_OK;
+  }
+  ASGK_CUDA(cudaMemcpyAsync(host, src, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+  return ASGK_OK;
+}
+
 int norm2(gmres_ws &ws, const double *v, int64_t n, double &out,
           cudaStream_t s)
 {
   if (int rc = launch_norm2_h(v, n, ws.part, ws.tickets + 1, ws.h, s))
     return rc;
-  ASGK_CUDA(cudaMemcpyAsync(ws.hh, ws.h, sizeof(double), cudaMemcpyDeviceToHost, s));
+  if (int rc = read_small(ws.hh, ws.hh_dev, ws.h, 1, s))
+    return rc;
   ASGK_CUDA(cudaStreamSynchronize(s));
   out = std::sqrt(ws.hh[0]);
   return ASGK_OK;
@@ -926,9 +974,8 @@ int gmres_core(gmres_ws &ws, int64_t n, matvec_t const &mat,
       k_cycle_start<<<1, 32, 0, s>>>(ws.dstate, inner_res, tol);
       ASGK_LAUNCHED();
       ASGK_CUDA(cudaGraphLaunch(cg->exec, s));
-      ASGK_CUDA(cudaMemcpyAsync(ws.hstate, ws.dstate,
-                                sizeof(double) * state_len(restart),
-                                cudaMemcpyDeviceToHost, s));
+      if (int rc = read_small(ws.hstate, ws.hstate_dev, ws.dstate, state_len(restart), s))
+        return rc;
       ASGK_CUDA(cudaStreamSynchronize(s));
       const double *hs = ws.hstate;
       inner            = int(hs[3]);
@@ -977,8 +1024,8 @@ int gmres_core(gmres_ws &ws, int64_t n, matvec_t const &mat,
                        : launch_update_norm_h(ws.V, n, k, ws.h, w, n, ws.part,
                                               ws.tickets, ws.h + k, s))
         return rc;
-      ASGK_CUDA(cudaMemcpyAsync(ws.hh, ws.h, sizeof(double) * (k + 1),
-                                cudaMemcpyDeviceToHost, s));
+      if (int rc = read_small(ws.hh, ws.hh_dev, ws.h, k + 1, s))
+        return rc;
       ASGK_CUDA(cudaStreamSynchronize(s));
       double const nrm = std::sqrt(ws.hh[k]);
       if (!std::isfinite(nrm))
@@ -1022,8 +1069,15 @@ int gmres_core(gmres_ws &ws, int64_t n, matvec_t const &mat,
             ksol[i] -= tmp * proj[pos_from_indices(i, j)];
         }
       }
-      ASGK_CUDA(cudaMemcpyAsync(ws.y, ksol.data(), sizeof(double) * inner,
-                                cudaMemcpyHostToDevice, s));
+      std::memcpy(ws.hy, ksol.data(), sizeof(double) * inner);
+      if (ws.hy_dev != nullptr)
+      {
+        k_move_small<<<1, 64, 0, s>>>(ws.y, ws.hy_dev, inner);
+        ASGK_LAUNCHED();
+      }
+      else
+        ASGK_CUDA(cudaMemcpyAsync(ws.y, ws.hy, sizeof(double) * inner,
+                                  cudaMemcpyHostToDevice, s));
       if (int rc = launch_gemv_add(flex ? ws.Z : ws.V, n, inner, ws.y, x, n, s))
         return rc;
       // ksol is read by the copy above before it is reused
