@@ -65,7 +65,7 @@ TOL = 1e-10
 KERNEL_TRAFFIC = {
     ("pairs", "d4"): 254_243_328 + 4_232_704,
     ("global", "d4"): 3_930_368,
-    ("global", "d6"): 193_600_768 + 68_187_648,
+    ("global", "d6"): 71_265_792 + 54_134_016,
 }
 
 
