@@ -1904,7 +1904,7 @@ int asgk_plan_info(const asgk_plan *plan, int64_t *num_batch,
       *flops = p.global ? int64_t(p.tensor) * p.n * (p.gnnz + p.gchain_entries) * 2
                         : int64_t(p.tensor) * p.n * p.d * p.terms * p.nnz * 2;
     if (device_bytes)
-      *device_bytes = p.device_bytes;
+      *device_bytes = p.device_bytes + tc_bytes(p.tc);
     return ASGK_OK;
   }
   catch (std::bad_alloc const &)

@@ -252,6 +252,8 @@ int tc_build(plan_data const &p, tc_data **out);
 int tc_prepare(plan_data const &p);
 int tc_refresh(plan_data const &p, tc_data &t);
 void tc_free(tc_data *t);
+// device memory the tensor-core form holds (0 before its first use)
+int64_t tc_bytes(const tc_data *t);
 int tc_read_error(int reset, int *code);
 int launch_global_tc(plan_data const &p, double alpha, const double *x, double beta,
                      double *y, double ex, cudaStream_t s);

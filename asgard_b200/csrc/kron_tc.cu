@@ -574,6 +574,8 @@ int launch_smem(int d, tc_launch &l)
 
 void tc_free(tc_data *t) { delete t; }
 
+int64_t tc_bytes(const tc_data *t) { return t != nullptr ? t->bytes : 0; }
+
 int tc_prepare(plan_data const &p)
 {
   if (p.tc != nullptr)

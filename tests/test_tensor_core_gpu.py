@@ -78,10 +78,14 @@ def test_bf16_general_inputs_within_rounding(cuda, d, L, T):
     x = rng.uniform(-1, 1, op.N)
     y0 = rng.uniform(-1, 1, op.N)
     ref = _apply(g, 1.0, x, 0.5, y0, "fp64")
+    held = g.device_bytes()
     a = _apply(g, 1.0, x, 0.5, y0, "bf16")
     b = _apply(g, 1.0, x, 0.5, y0, "bf16")
     assert rel_err(a, ref) < 1e-2
     assert np.array_equal(a, b)
+    # the tensor-core tables built by the first BF16 call are reported:
+    # at least the BF16 copy of x and the FP32 sum vector
+    assert g.device_bytes() >= held + 6 * op.N
 
 
 def test_bf16_euler_form_and_value_update(cuda):
