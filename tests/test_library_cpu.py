@@ -200,3 +200,21 @@ def test_direction_pairs_are_the_single_dimension_pairs(d, L):
             elif not diff:
                 want |= {(c, k, int(conn[p, k])) for k in range(d)}
         assert got == want, r
+
+
+@pytest.mark.parametrize("d,L,T", [(2, 5, 2), (3, 4, 3), (4, 3, 2)])
+def test_bench_pencil_gemm_flops(d, L, T):
+    """The bench's count of the tensor-core form's useful flops: along each
+    dimension with terms, a cell of a standard sparse grid lies in a pencil
+    of 2^(L - s) cells (s: its levels summed over the other dimensions), so
+    sum over pencils of 2 (3p)^2 3^(d-1) = sum over cells of 2 * 9 p * 3^(d-1)."""
+    import bench
+    import asgard_b200 as ab
+    op = ab.SparseGridOperator(d, L, T, kind="advdiff")
+    lev = op.table[:, :d].astype(np.int64)
+    expect = 0
+    for k in sorted({t % d for t in range(T)}):
+        s = lev.sum(axis=1) - lev[:, k]
+        p = 2 ** (L - s)
+        expect += int((2 * 9 * p * 3 ** (d - 1)).sum())
+    assert bench.pencil_gemm_flops(op) == expect
