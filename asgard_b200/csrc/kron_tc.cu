@@ -763,9 +763,11 @@ int tc_build(plan_data const &p, tc_data **out)
         l.cols *= 2;
       if (int rc = launch_smem(d, l))
         return rc;
-      if (int rc = upload_tc(&l.tiles, kv.second, t->bytes))
-        return rc;
+      // recorded before the upload, so the destructor frees its tiles on
+      // every error path
       t->launches.push_back(l);
+      if (int rc = upload_tc(&t->launches.back().tiles, kv.second, t->bytes))
+        return rc;
     }
   }
   pen_start.push_back(int(pen_cells.size()));
